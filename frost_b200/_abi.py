@@ -1,0 +1,135 @@
+"""ctypes mirrors of the plain-C types declared in include/frost_b200.h.
+
+Field order and widths follow the header exactly; the header is the
+contract, this module only restates it for Python callers.
+"""
+
+import ctypes as C
+
+# status codes (enum frost_status)
+OK = 0
+ERR_INVALID_ARGUMENT = -1
+ERR_OUT_OF_MEMORY = -2
+ERR_DEVICE = -3
+ERR_TIMEOUT = -4
+ERR_STATE = -5
+ERR_OVERFLOW = -6
+ERR_IO = -7
+ERR_INTERNAL = -8
+
+# enum frost_dtype (include/frost/common/policies.hpp:52-60)
+UINT1, UINT2, UINT4, UINT8, UINT16, UINT32, FLOAT32 = range(7)
+DTYPE_BITS = {UINT1: 1, UINT2: 2, UINT4: 4, UINT8: 8, UINT16: 16, UINT32: 32, FLOAT32: 32}
+
+FILL_NEIGHBOUR, FILL_MEAN, FILL_NOISE = range(3)
+ZERO_DM_OFF, ZERO_DM_SUBTRACT, ZERO_DM_ZDOT = range(3)
+
+# enum frost_peak_mode (dmt::PeakFindingMode as frost names it,
+# docs/user_guide/search.md:43-49)
+PEAK_PER_WIDTH, PEAK_ACROSS_WIDTHS, PEAK_ALL = range(3)
+
+# enum frost_storage: FDMT intermediate plane storage
+STORAGE_FP32, STORAGE_FP16 = range(2)
+
+
+class ChannelRange(C.Structure):
+    _fields_ = [("start", C.c_uint64), ("end", C.c_uint64)]
+
+
+class FrequencyRange(C.Structure):
+    _fields_ = [("lo", C.c_double), ("hi", C.c_double)]
+
+
+class RfiConfigC(C.Structure):
+    _fields_ = [
+        ("zap_chans", C.POINTER(ChannelRange)),
+        ("n_zap_chans", C.c_uint64),
+        ("zap_freqs", C.POINTER(FrequencyRange)),
+        ("n_zap_freqs", C.c_uint64),
+        ("narrow_enabled", C.c_int32),
+        ("narrow_threshold", C.c_float),
+        ("broad_enabled", C.c_int32),
+        ("broad_threshold", C.c_float),
+        ("broad_boxcar_max", C.c_uint64),
+        ("dropout_enabled", C.c_int32),
+        ("dropout_min_std_fraction", C.c_float),
+        ("moments_enabled", C.c_int32),
+        ("moments_threshold", C.c_float),
+        ("moments_mean", C.c_int32),
+        ("moments_std", C.c_int32),
+        ("moments_skewness", C.c_int32),
+        ("moments_kurtosis", C.c_int32),
+        ("moments_autocorr", C.c_int32),
+        ("moments_kurtosis_max", C.c_float),
+        ("iqrm_enabled", C.c_int32),
+        ("iqrm_threshold", C.c_float),
+        ("iqrm_radius", C.c_uint64),
+        ("mask_grow", C.c_uint64),
+        ("kadane_channel_enabled", C.c_int32),
+        ("kadane_channel_threshold", C.c_float),
+        ("kadane_channel_min_duration", C.c_float),
+        ("kadane_spectrum_enabled", C.c_int32),
+        ("kadane_spectrum_threshold", C.c_float),
+        ("kadane_spectrum_min_bandwidth", C.c_float),
+        ("kadane_spectrum_whole_band_fraction", C.c_float),
+        ("zero_dm", C.c_int32),
+        ("equalize", C.c_int32),
+        ("fill", C.c_int32),
+        ("seed", C.c_uint64),
+    ]
+
+
+class BlockLayoutC(C.Structure):
+    _fields_ = [
+        ("nchans", C.c_uint64),
+        ("max_nsamps", C.c_uint64),
+        ("dtype", C.c_int32),
+        ("tsamp", C.c_double),
+        ("f0", C.c_double),
+        ("df", C.c_double),
+    ]
+
+
+class RfiReportC(C.Structure):
+    _fields_ = [
+        ("calibration_reused", C.c_int32),
+        ("nsamps", C.c_uint64),
+        ("chans_zapped", C.c_uint64),
+        ("chans_dead", C.c_uint64),
+        ("chans_moments", C.c_uint64),
+        ("chans_iqrm", C.c_uint64),
+        ("chans_grown", C.c_uint64),
+        ("chans_masked", C.c_uint64),
+        ("samps_broad", C.c_uint64),
+        ("samps_dropout", C.c_uint64),
+        ("samps_kadane", C.c_uint64),
+        ("samps_flagged", C.c_uint64),
+        ("cells_narrow", C.c_uint64),
+        ("cells_kadane_spectrum", C.c_uint64),
+        ("cells_kadane_channel", C.c_uint64),
+        ("fill_fallbacks", C.c_uint64),
+        ("t_bandpass", C.c_double),
+        ("t_moments", C.c_double),
+        ("t_scan", C.c_double),
+        ("t_flags", C.c_double),
+        ("t_apply", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class DedispPlanConfigC(C.Structure):
+    _fields_ = [
+        ("nchans", C.c_uint64),
+        ("dt", C.c_float),
+        ("f0", C.c_float),
+        ("df", C.c_float),
+        ("dm_min", C.c_float),
+        ("dm_max", C.c_float),
+        ("dm_pulse_width", C.c_float),
+        ("dm_tol", C.c_float),
+        ("dm_dtype", C.c_int32),
+        ("block_nsamps", C.c_uint64),
+        ("subband_depth", C.c_uint64),
+    ]

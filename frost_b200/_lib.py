@@ -1,0 +1,75 @@
+"""Loads the in-tree C-ABI library (frost_b200/lib/libfrost_b200.so) and
+declares the signatures of include/frost_b200.h. There is no fallback: a
+missing library raises, so every call in this package runs the CUDA path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libfrost_b200.so")
+
+_lib = None
+
+
+class FrostError(RuntimeError):
+    """A frost_b200 call failed with a status other than INVALID_ARGUMENT."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+# Every symbol include/frost_b200.h declares, with (restype, argtypes).
+_vp, _sz, _u8p, _f32p, _u64 = C.c_void_p, C.c_size_t, C.POINTER(C.c_uint8), C.POINTER(C.c_float), C.c_uint64
+SIGNATURES = {
+    "frost_last_error": (C.c_char_p, []),
+    "frost_version": (C.c_char_p, []),
+    "frost_rfi_config_default": (None, [C.POINTER(_abi.RfiConfigC)]),
+    "frost_rfi_config_validate": (C.c_int, [C.POINTER(_abi.RfiConfigC)]),
+    "frost_rfi_create": (C.c_int, [C.POINTER(_abi.RfiConfigC), C.POINTER(_abi.BlockLayoutC),
+                                   C.c_float, C.c_int, C.POINTER(_vp)]),
+    "frost_rfi_destroy": (C.c_int, [_vp]),
+    "frost_rfi_execute_normalized": (C.c_int, [_vp, _vp, _sz, _sz, C.c_int, _vp, C.POINTER(_vp)]),
+    "frost_rfi_download_normalized": (C.c_int, [_vp, _f32p, _sz]),
+    "frost_rfi_channel_mask": (C.c_int, [_vp, _u8p, _sz]),
+    "frost_rfi_get_report": (C.c_int, [_vp, C.POINTER(_abi.RfiReportC)]),
+    "frost_rfi_time_flags": (C.c_int, [_vp, _u8p, _sz]),
+    "frost_rfi_memory_usage": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "frost_iqrm_mask": (C.c_int, [_f32p, _sz, _u64, C.c_float, _u8p, _u8p]),
+    "frost_apply_manual_killmask": (C.c_int, [_u8p, _sz, C.POINTER(_abi.ChannelRange), _sz]),
+    "frost_read_kill_file": (C.c_int, [C.c_char_p, _sz, C.POINTER(_abi.ChannelRange), _sz,
+                                       C.POINTER(_sz)]),
+    "frost_generate_dm_list": (C.c_int, [C.POINTER(_abi.DedispPlanConfigC), _f32p, _sz, C.POINTER(_sz)]),
+    "frost_fdmt_band_edges": (C.c_int, [C.POINTER(_abi.DedispPlanConfigC), _f32p, _f32p]),
+}
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"frost_b200: {LIB_PATH} is not built; run "
+                          "`python -c 'import __graft_entry__ as g; g.build()'` or "
+                          "`make -C frost_b200/csrc`")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc: int) -> int:
+    if rc == _abi.OK:
+        return rc
+    msg = lib().frost_last_error().decode(errors="replace")
+    if rc == _abi.ERR_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    raise FrostError(rc, msg)

@@ -1,0 +1,224 @@
+// extern "C" entry points of include/frost_b200.h. Each wraps the C++
+// implementation, converts exceptions to frost_status codes and records the
+// message for frost_last_error(); nothing throws across this boundary.
+
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "common.hpp"
+#include "dedisp.hpp"
+#include "host_stats.hpp"
+#include "rfi_cleaner.hpp"
+
+namespace fb {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+bool is_finite(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, sizeof(b));
+    return is_finite_bits32(b);
+}
+
+bool is_finite(double x) {
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof(b));
+    return is_finite_bits64(b);
+}
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return FROST_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code();
+    } catch (const std::bad_alloc& e) {
+        set_last_error(std::string("host allocation failed: ") + e.what());
+        return FROST_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return FROST_ERR_INTERNAL;
+    } catch (...) {
+        set_last_error("unknown error");
+        return FROST_ERR_INTERNAL;
+    }
+}
+
+} // namespace fb
+
+struct frost_rfi {
+    fb::rfi::Cleaner impl;
+    template <class... A> explicit frost_rfi(A&&... a) : impl(std::forward<A>(a)...) {}
+};
+
+using fb::guarded;
+using fb::invalid;
+
+extern "C" {
+
+const char* frost_last_error(void) { return fb::g_last_error.c_str(); }
+
+const char* frost_version(void) { return "frost_b200 0.1.0 (sm_100a)"; }
+
+void frost_rfi_config_default(frost_rfi_config* cfg) {
+    if (cfg != nullptr)
+        fb::rfi::config_default(cfg);
+}
+
+int frost_rfi_config_validate(const frost_rfi_config* cfg) {
+    return guarded([&] {
+        if (cfg == nullptr)
+            invalid("null config");
+        fb::rfi::Config::from(*cfg).validate();
+    });
+}
+
+int frost_rfi_create(const frost_rfi_config* cfg, const frost_block_layout* layout,
+                     float baseline_length, int device, frost_rfi** out) {
+    return guarded([&] {
+        if (cfg == nullptr || layout == nullptr || out == nullptr)
+            invalid("frost_rfi_create: null argument");
+        *out = nullptr;
+        *out = new frost_rfi(*cfg, *layout, baseline_length, device);
+    });
+}
+
+int frost_rfi_destroy(frost_rfi* rfi) {
+    return guarded([&] { delete rfi; });
+}
+
+int frost_rfi_execute_normalized(frost_rfi* rfi, const uint8_t* block, size_t block_bytes,
+                                 size_t nsamps, int block_on_device, void* stream,
+                                 const float** out_device) {
+    return guarded([&] {
+        if (rfi == nullptr)
+            invalid("frost_rfi_execute_normalized: null handle");
+        const float* out = rfi->impl.execute_normalized(block, block_bytes, nsamps,
+                                                        block_on_device != 0,
+                                                        static_cast<cudaStream_t>(stream));
+        if (out_device != nullptr)
+            *out_device = out;
+    });
+}
+
+int frost_rfi_download_normalized(frost_rfi* rfi, float* host, size_t count) {
+    return guarded([&] {
+        if (rfi == nullptr || (host == nullptr && count != 0))
+            invalid("frost_rfi_download_normalized: null argument");
+        const size_t have = rfi->impl.capacity() * rfi->impl.nchans();
+        if (count < have)
+            invalid("frost_rfi_download_normalized: buffer holds " + std::to_string(count) +
+                    " floats, need " + std::to_string(have));
+        fb::DeviceGuard g(rfi->impl.device());
+        if (have)
+            FB_CUDA(cudaMemcpy(host, rfi->impl.output(), have * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
+int frost_rfi_channel_mask(const frost_rfi* rfi, uint8_t* out, size_t nchans) {
+    return guarded([&] {
+        if (rfi == nullptr || out == nullptr)
+            invalid("frost_rfi_channel_mask: null argument");
+        const auto& m = rfi->impl.channel_mask();
+        if (nchans < m.size())
+            invalid("frost_rfi_channel_mask: buffer too small");
+        std::memcpy(out, m.data(), m.size());
+    });
+}
+
+int frost_rfi_get_report(const frost_rfi* rfi, frost_rfi_report* out) {
+    return guarded([&] {
+        if (rfi == nullptr || out == nullptr)
+            invalid("frost_rfi_get_report: null argument");
+        *out = rfi->impl.report();
+    });
+}
+
+int frost_rfi_time_flags(const frost_rfi* rfi, uint8_t* out, size_t nsamps) {
+    return guarded([&] {
+        if (rfi == nullptr || out == nullptr)
+            invalid("frost_rfi_time_flags: null argument");
+        const auto& f = rfi->impl.time_flags();
+        if (nsamps < f.size())
+            invalid("frost_rfi_time_flags: buffer too small");
+        std::memcpy(out, f.data(), f.size());
+    });
+}
+
+int frost_rfi_memory_usage(const frost_rfi* rfi, size_t* bytes) {
+    return guarded([&] {
+        if (rfi == nullptr || bytes == nullptr)
+            invalid("frost_rfi_memory_usage: null argument");
+        *bytes = rfi->impl.memory_usage();
+    });
+}
+
+int frost_iqrm_mask(const float* x, size_t n, uint64_t radius, float threshold,
+                    const uint8_t* ignore, uint8_t* out) {
+    return guarded([&] {
+        if ((x == nullptr || out == nullptr) && n != 0)
+            invalid("frost_iqrm_mask: null argument");
+        std::span<const uint8_t> ig;
+        if (ignore != nullptr)
+            ig = {ignore, n};
+        const auto m = fb::stats::iqrm_mask({x, n}, radius, threshold, ig);
+        if (n)
+            std::memcpy(out, m.data(), n);
+    });
+}
+
+int frost_apply_manual_killmask(uint8_t* killmask, size_t nchans, const frost_channel_range* zaps,
+                                size_t nzaps) {
+    return guarded([&] {
+        if ((killmask == nullptr && nchans) || (zaps == nullptr && nzaps))
+            invalid("frost_apply_manual_killmask: null argument");
+        fb::rfi::apply_manual_killmask({killmask, nchans}, {zaps, nzaps});
+    });
+}
+
+int frost_read_kill_file(const char* path, size_t nchans, frost_channel_range* out,
+                         size_t capacity, size_t* count) {
+    return guarded([&] {
+        if (path == nullptr || count == nullptr)
+            invalid("frost_read_kill_file: null argument");
+        const auto r = fb::rfi::read_kill_file(path, nchans);
+        *count       = r.size();
+        if (out != nullptr) {
+            if (capacity < r.size())
+                invalid("frost_read_kill_file: output holds too few ranges");
+            std::memcpy(out, r.data(), r.size() * sizeof(frost_channel_range));
+        }
+    });
+}
+
+int frost_generate_dm_list(const frost_dedisp_plan_config* cfg, float* out, size_t capacity,
+                           size_t* count) {
+    return guarded([&] {
+        if (cfg == nullptr || count == nullptr)
+            invalid("frost_generate_dm_list: null argument");
+        const auto dms = fb::dedisp::generate_dm_list(*cfg);
+        *count         = dms.size();
+        if (out != nullptr) {
+            if (capacity < dms.size())
+                invalid("frost_generate_dm_list: output holds too few trials");
+            std::memcpy(out, dms.data(), dms.size() * sizeof(float));
+        }
+    });
+}
+
+int frost_fdmt_band_edges(const frost_dedisp_plan_config* cfg, float* f_min, float* f_max) {
+    return guarded([&] {
+        if (cfg == nullptr || f_min == nullptr || f_max == nullptr)
+            invalid("frost_fdmt_band_edges: null argument");
+        fb::dedisp::band_edges(*cfg, *f_min, *f_max);
+    });
+}
+
+} // extern "C"

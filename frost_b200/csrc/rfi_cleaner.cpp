@@ -1,0 +1,825 @@
+// GPU RFICleaner orchestration. Per gulp:
+//   decode checks -> bandpass (sampled remedian + clipped refinement) ->
+//   moments -> channel mask (moments IQR outliers, IQRM, growth) ->
+//   row scan + column scan -> flags -> apply (fills, transforms) ->
+//   optional Welford re-measure -> normalise + transpose to [channel][time].
+// Every T x C pass is a kernel (rfi_kernels.cu); the per-gulp decisions use
+// the O(T) / O(C) series the kernels reduce the block to, as frost's own
+// device cleaner does (lib/cuda/device_rfi_cuda.cu:187-262). Semantics follow
+// RFICleaner::Impl (lib/cpu/rfi_cpu.cpp, lib/cpu/rfi_cpu_measure.cpp).
+
+#include "rfi_cleaner.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <limits>
+#include <string_view>
+
+#include "host_stats.hpp"
+
+namespace fb::rfi {
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double since(Clock::time_point t) {
+    return std::chrono::duration<double>(Clock::now() - t).count();
+}
+
+template <class T> void h2d(DeviceBuffer& dst, const T* src, SizeType count, cudaStream_t s) {
+    dst.reserve(std::max<SizeType>(count * sizeof(T), 1));
+    if (count)
+        FB_CUDA(cudaMemcpyAsync(dst.get(), src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+template <class T> void d2h(std::vector<T>& dst, const DeviceBuffer& src, SizeType count, cudaStream_t s) {
+    dst.resize(count);
+    if (count)
+        FB_CUDA(cudaMemcpyAsync(dst.data(), src.get(), count * sizeof(T), cudaMemcpyDeviceToHost, s));
+}
+
+SizeType count_zeros(const std::vector<uint8_t>& v) {
+    return static_cast<SizeType>(std::count(v.begin(), v.end(), uint8_t{0}));
+}
+
+} // namespace
+
+// ---- configuration ---------------------------------------------------------
+
+void config_default(frost_rfi_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->narrow_enabled                      = 1;
+    c->narrow_threshold                    = 5.0F;
+    c->broad_enabled                       = 1;
+    c->broad_threshold                     = 5.0F;
+    c->broad_boxcar_max                    = 1;
+    c->dropout_enabled                     = 0;
+    c->dropout_min_std_fraction            = 0.1F;
+    c->moments_enabled                     = 0;
+    c->moments_threshold                   = 4.0F;
+    c->moments_mean                        = 1;
+    c->moments_std                         = 1;
+    c->moments_skewness                    = 1;
+    c->moments_kurtosis                    = 1;
+    c->moments_autocorr                    = 1;
+    c->moments_kurtosis_max                = 0.0F;
+    c->iqrm_enabled                        = 0;
+    c->iqrm_threshold                      = 3.0F;
+    c->iqrm_radius                         = 0;
+    c->mask_grow                           = 0;
+    c->kadane_channel_enabled              = 0;
+    c->kadane_channel_threshold            = 7.0F;
+    c->kadane_channel_min_duration         = 0.05F;
+    c->kadane_spectrum_enabled             = 0;
+    c->kadane_spectrum_threshold           = 7.0F;
+    c->kadane_spectrum_min_bandwidth       = 10.0F;
+    c->kadane_spectrum_whole_band_fraction = 0.8F;
+    c->zero_dm                             = FROST_ZERO_DM_OFF;
+    c->equalize                            = 0;
+    c->fill                                = FROST_FILL_NEIGHBOUR;
+    c->seed                                = 0x5EED;
+}
+
+Config Config::from(const frost_rfi_config& in) {
+    Config out;
+    out.c = in;
+    if (in.n_zap_chans && in.zap_chans == nullptr)
+        invalid("rfi.zap_chans is null");
+    if (in.n_zap_freqs && in.zap_freqs == nullptr)
+        invalid("rfi.zap_freqs is null");
+    out.zap_chans.assign(in.zap_chans, in.zap_chans + in.n_zap_chans);
+    out.zap_freqs.assign(in.zap_freqs, in.zap_freqs + in.n_zap_freqs);
+    out.c.zap_chans = nullptr;
+    out.c.zap_freqs = nullptr;
+    return out;
+}
+
+// RfiConfig::validate (lib/prepare/rfi_config.cpp:14-77).
+void Config::validate() const {
+    auto positive = [](float v, const char* name) {
+        if (!is_positive_finite(v))
+            invalid(std::string("rfi.") + name + " must be finite and > 0");
+    };
+    auto nonnegative = [](float v, const char* name) {
+        if (!is_finite(v) || v < 0.0F)
+            invalid(std::string("rfi.") + name + " must be finite and >= 0");
+    };
+    auto fraction = [](float v, const char* name) {
+        if (!is_finite(v) || v < 0.0F || v > 1.0F)
+            invalid(std::string("rfi.") + name + " must be finite and in [0, 1]");
+    };
+    positive(c.narrow_threshold, "narrow.threshold");
+    positive(c.broad_threshold, "broad.threshold");
+    positive(c.moments_threshold, "moments.threshold");
+    positive(c.iqrm_threshold, "iqrm.threshold");
+    positive(c.kadane_channel_threshold, "kadane_channel.threshold");
+    positive(c.kadane_spectrum_threshold, "kadane_spectrum.threshold");
+    nonnegative(c.moments_kurtosis_max, "moments.kurtosis_max");
+    nonnegative(c.kadane_channel_min_duration, "kadane_channel.min_duration");
+    nonnegative(c.kadane_spectrum_min_bandwidth, "kadane_spectrum.min_bandwidth");
+    fraction(c.dropout_min_std_fraction, "dropout.min_std_fraction");
+    fraction(c.kadane_spectrum_whole_band_fraction, "kadane_spectrum.whole_band_fraction");
+    if (c.broad_boxcar_max == 0)
+        invalid("rfi.broad.boxcar_max must be >= 1");
+    for (const auto& r : zap_chans)
+        if (r.start > r.end)
+            invalid("rfi.zap_chans ranges need start <= end");
+    for (const auto& r : zap_freqs)
+        if (!is_finite(r.lo) || !is_finite(r.hi) || r.lo > r.hi)
+            invalid("rfi.zap_freqs ranges must be finite with lo <= hi");
+    if (c.fill < FROST_FILL_NEIGHBOUR || c.fill > FROST_FILL_NOISE)
+        invalid("Invalid rfi.fill");
+    if (c.zero_dm < FROST_ZERO_DM_OFF || c.zero_dm > FROST_ZERO_DM_ZDOT)
+        invalid("Invalid rfi.zero_dm");
+}
+
+// validate_layout (lib/prepare/rfi_config.cpp:79-110).
+void validate_layout(const frost_block_layout& l, float baseline_length) {
+    if (l.nchans == 0 || l.max_nsamps == 0)
+        invalid("RFI: nchans and max_nsamps must be > 0");
+    if (l.dtype < FROST_UINT1 || l.dtype > FROST_FLOAT32)
+        invalid("RFI: unsupported dtype");
+    const auto width    = static_cast<SizeType>(bits_of(l.dtype));
+    constexpr auto kMax = std::numeric_limits<SizeType>::max();
+    if (l.nchans > kMax / width || l.nchans > (kMax / sizeof(float)) / l.max_nsamps)
+        invalid("RFI: packed or normalized block geometry overflows");
+    if ((l.nchans * width) % 8 != 0)
+        invalid("RFI: each time sample must be a whole number of bytes");
+    if (!is_positive_finite(l.tsamp) || !is_positive_finite(baseline_length))
+        invalid("RFI: tsamp and baseline_length must be finite and > 0");
+    if (!is_finite(l.f0) || !is_finite(l.df))
+        invalid("RFI: f0 and df must be finite");
+    if (l.tsamp <= static_cast<double>(baseline_length) / static_cast<double>(kMax))
+        invalid("RFI: baseline sample count is not representable");
+}
+
+// apply_manual_killmask (lib/cpu/rfi_masks_cpu.cpp:16-27).
+void apply_manual_killmask(std::span<uint8_t> mask, std::span<const frost_channel_range> zaps) {
+    if (mask.empty())
+        return;
+    for (const auto& r : zaps) {
+        const auto end = std::min<uint64_t>(r.end, mask.size() - 1);
+        for (uint64_t c = r.start; c <= end; ++c)
+            mask[c] = 0;
+    }
+}
+
+// read_kill_file (lib/prepare/kill_file.cpp:15-65): one 0/1 per line,
+// '#' comments and blank lines ignored, exactly nchans entries.
+std::vector<frost_channel_range> read_kill_file(const std::string& path, SizeType nchans) {
+    std::ifstream in(path);
+    if (!in)
+        throw Error(FROST_ERR_IO, "cannot read kill file " + path);
+    std::vector<frost_channel_range> killed;
+    SizeType channel = 0;
+    std::string line;
+    for (SizeType number = 1; std::getline(in, line); ++number) {
+        std::string_view text(line);
+        if (const auto hash = text.find('#'); hash != std::string_view::npos)
+            text = text.substr(0, hash);
+        constexpr std::string_view kSpace = " \t\r\f\v";
+        const auto first                  = text.find_first_not_of(kSpace);
+        if (first == std::string_view::npos)
+            continue;
+        text = text.substr(first, text.find_last_not_of(kSpace) - first + 1);
+        if (text != "0" && text != "1")
+            invalid("kill file " + path + " line " + std::to_string(number) +
+                    ": expected 0 (kill) or 1 (keep), got '" + std::string(text) + "'");
+        if (channel == nchans)
+            invalid("kill file " + path + " has more than " + std::to_string(nchans) +
+                    " channel entries");
+        if (text == "0") {
+            if (!killed.empty() && killed.back().end + 1 == channel)
+                killed.back().end = channel;
+            else
+                killed.push_back({channel, channel});
+        }
+        ++channel;
+    }
+    if (in.bad())
+        throw Error(FROST_ERR_IO, "error reading kill file " + path);
+    if (channel != nchans)
+        invalid("kill file " + path + " has " + std::to_string(channel) +
+                " channel entries; the input has " + std::to_string(nchans));
+    return killed;
+}
+
+// ---- cleaner -----------------------------------------------------------------
+
+Cleaner::Cleaner(const frost_rfi_config& cfg, const frost_block_layout& layout,
+                 float baseline_length, int device)
+    : m_cfg(Config::from(cfg)), m_layout(layout), m_device(device), m_n(layout.nchans),
+      m_row_bytes(0) {
+    m_cfg.validate();
+    validate_layout(layout, baseline_length);
+    const auto& c = m_cfg.c;
+    if ((c.zero_dm != FROST_ZERO_DM_OFF || c.equalize) && layout.dtype != FROST_FLOAT32 &&
+        bits_of(layout.dtype) < 8)
+        invalid("RFICleaner: zero_dm and equalize need >= 8-bit data");
+    if ((c.kadane_spectrum_enabled || !m_cfg.zap_freqs.empty()) && layout.df == 0.0)
+        invalid("RFICleaner: zap_freqs and kadane_spectrum need the channel spacing (df)");
+    int ndev = 0;
+    FB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev)
+        invalid("RFICleaner: device " + std::to_string(device) + " does not exist");
+    DeviceGuard g(device);
+
+    m_row_bytes = layout.nchans * static_cast<SizeType>(bits_of(layout.dtype)) / 8;
+    const double window_samples = static_cast<double>(baseline_length) / layout.tsamp;
+    m_window_len       = std::max(static_cast<SizeType>(window_samples), SizeType{kMinWindow});
+    m_smooth_radius    = std::max<SizeType>(static_cast<SizeType>(window_samples / 2), 1);
+    m_time_fill_radius = std::max<SizeType>(m_smooth_radius / 4, 1);
+    m_chan_fill_radius = std::max<SizeType>(m_n / 60, 1);
+    m_clip             = c.narrow_threshold;
+    m_narrow_active    = c.narrow_enabled && (layout.dtype == FROST_FLOAT32 || bits_of(layout.dtype) > 4);
+    m_transform        = c.zero_dm != FROST_ZERO_DM_OFF || c.equalize;
+    m_need_moments     = c.moments_enabled || c.iqrm_enabled || c.kadane_channel_enabled;
+    if (layout.dtype == FROST_FLOAT32) {
+        m_eq_loc   = 0.0F;
+        m_eq_scale = 1.0F;
+    } else {
+        const int nbits = bits_of(layout.dtype);
+        m_eq_loc        = static_cast<float>(uint64_t{1} << (nbits - 1));
+        m_eq_scale      = static_cast<float>(uint64_t{1} << nbits) / 16.0F;
+    }
+    build_static_mask();
+    m_mask                = m_static_mask;
+    m_report              = frost_rfi_report{};
+    m_report.chans_zapped = count_zeros(m_static_mask);
+    m_report.chans_masked = m_report.chans_zapped;
+    m_zdot_a.assign(m_n, 0.0F);
+    m_zdot_b.assign(m_n, 0.0F);
+    FB_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
+    h2d(m_static_mask_d, m_static_mask.data(), m_n, m_stream);
+    FB_CUDA(cudaStreamSynchronize(m_stream));
+}
+
+Cleaner::~Cleaner() {
+    if (m_stream != nullptr) {
+        cudaSetDevice(m_device);
+        cudaStreamSynchronize(m_stream);
+        cudaStreamDestroy(m_stream);
+    }
+}
+
+void Cleaner::build_static_mask() {
+    m_static_mask.assign(m_n, 1U);
+    apply_manual_killmask(m_static_mask, m_cfg.zap_chans);
+    for (SizeType c = 0; c < m_n; ++c) {
+        const double f = m_layout.f0 + (static_cast<double>(c) * m_layout.df);
+        for (const auto& r : m_cfg.zap_freqs)
+            if (f >= r.lo && f <= r.hi)
+                m_static_mask[c] = 0;
+    }
+}
+
+SizeType Cleaner::memory_usage() const {
+    const DeviceBuffer* all[] = {
+        &m_raw, &m_samples, &m_loc, &m_scale, &m_inv, &m_loc2, &m_scale2, &m_unmeasured,
+        &m_moments, &m_clip_mean, &m_clip_inv, &m_mask_d, &m_static_mask_d, &m_good_prefix,
+        &m_s_det, &m_s_keep_d, &m_s_keep_f, &m_row_std, &m_kspec_pos, &m_kspec_neg,
+        &m_kspec_whole, &m_chunk_min, &m_chunk_max, &m_chunk_zdot, &m_chunk_kpos, &m_chunk_kneg,
+        &m_lo, &m_hi, &m_zdot_sum, &m_kpos_best, &m_kneg_best, &m_time_flags_d, &m_zdot_a_d,
+        &m_zdot_b_d, &m_kchan_pos_d, &m_kchan_neg_d, &m_flagged_d, &m_work, &m_out, &m_counters,
+        &m_first_bad, &m_tail_loc, &m_tail_scale, &m_tail_out_loc, &m_tail_out_scale};
+    SizeType total = 0;
+    for (const auto* b : all)
+        total += b->bytes();
+    return total;
+}
+
+Dims Cleaner::dims(SizeType nsamps, int dtype) const {
+    Dims d{};
+    d.dtype     = dtype;
+    d.nchans    = m_n;
+    d.row_bytes = m_row_bytes;
+    d.nsamps    = nsamps;
+    d.window    = m_window_len;
+    d.nwin      = std::max<SizeType>(nsamps / m_window_len, 1);
+    const SizeType by_rows = (nsamps + kMinChunkRows - 1) / kMinChunkRows;
+    d.nchunks   = std::clamp<SizeType>(by_rows, 1, kMaxChunks);
+    d.chunk     = (nsamps + d.nchunks - 1) / d.nchunks;
+    return d;
+}
+
+ApplyParams Cleaner::apply_params() const {
+    const auto& c = m_cfg.c;
+    ApplyParams p{};
+    p.seed             = c.seed;
+    p.block_index      = m_block_index;
+    p.chan_fill_radius = m_chan_fill_radius;
+    p.time_fill_radius = m_time_fill_radius;
+    p.clip             = m_clip;
+    p.eq_loc           = m_eq_loc;
+    p.eq_scale         = m_eq_scale;
+    p.narrow_active    = m_narrow_active ? 1 : 0;
+    p.kspec            = c.kadane_spectrum_enabled ? 1 : 0;
+    p.kchan            = c.kadane_channel_enabled ? 1 : 0;
+    p.neighbour        = c.fill == FROST_FILL_NEIGHBOUR ? 1 : 0;
+    p.noise            = c.fill == FROST_FILL_NOISE ? 1 : 0;
+    p.zero_dm          = c.zero_dm;
+    p.equalize         = c.equalize;
+    p.transform        = m_transform ? 1 : 0;
+    return p;
+}
+
+void Cleaner::ensure_capacity(SizeType capacity, SizeType valid) {
+    const SizeType n = m_n;
+    m_raw.reserve(std::max<SizeType>(capacity * m_row_bytes, 16));
+    m_work.reserve(std::max<SizeType>(valid * n * sizeof(float), 16));
+    m_out.reserve(std::max<SizeType>(capacity * n * sizeof(float), 16));
+    const SizeType nwin_max = std::max<SizeType>(valid / m_window_len, 1);
+    m_loc.reserve(nwin_max * n * sizeof(float));
+    m_scale.reserve(nwin_max * n * sizeof(float));
+    m_inv.reserve(nwin_max * n * sizeof(float));
+    m_loc2.reserve(nwin_max * n * sizeof(float));
+    m_scale2.reserve(nwin_max * n * sizeof(float));
+    m_tail_loc.reserve(n * sizeof(float));
+    m_tail_scale.reserve(n * sizeof(float));
+    m_tail_out_loc.reserve(n * sizeof(float));
+    m_tail_out_scale.reserve(n * sizeof(float));
+    m_counters.reserve(kCountSlots * sizeof(unsigned long long));
+    m_first_bad.reserve(sizeof(unsigned long long));
+}
+
+const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, SizeType valid,
+                                         bool on_device, cudaStream_t stream) {
+    if (bytes % m_row_bytes != 0 || bytes / m_row_bytes > m_layout.max_nsamps)
+        invalid("RFICleaner: invalid normalized block size");
+    if (block == nullptr && bytes != 0)
+        invalid("RFICleaner: null block");
+    const SizeType capacity = bytes / m_row_bytes;
+    if (valid == 0)
+        valid = capacity;
+    if (valid > capacity)
+        invalid("RFICleaner: nsamps exceeds block");
+    DeviceGuard g(m_device);
+    cudaStream_t s = stream != nullptr ? stream : m_stream;
+    ensure_capacity(capacity, valid);
+    m_capacity = capacity;
+
+    // Raw block on the device.
+    const uint8_t* raw = block;
+    if (!on_device) {
+        if (bytes)
+            FB_CUDA(cudaMemcpyAsync(m_raw.get(), block, bytes, cudaMemcpyHostToDevice, s));
+        raw = m_raw.as<uint8_t>();
+    }
+    // Non-finite float32 input is rejected before any statistics.
+    if (m_layout.dtype == FROST_FLOAT32 && valid > 0) {
+        const uint64_t words = valid * m_n;
+        unsigned long long first = words;
+        FB_CUDA(cudaMemcpyAsync(m_first_bad.get(), &first, sizeof(first), cudaMemcpyHostToDevice, s));
+        launch_check_finite(raw, words, m_first_bad.as<unsigned long long>(), s);
+        FB_CUDA(cudaMemcpyAsync(&first, m_first_bad.get(), sizeof(first), cudaMemcpyDeviceToHost, s));
+        FB_CUDA(cudaStreamSynchronize(s));
+        if (first != words)
+            invalid("RFI: non-finite float32 input at sample " + std::to_string(first / m_n) +
+                    ", channel " + std::to_string(first % m_n));
+    }
+
+    const bool short_block = valid < static_cast<SizeType>(std::max(kMinWindow, kMinBlockSamps));
+    const int flip         = m_layout.df < 0.0 ? 1 : 0;
+    FB_CUDA(cudaMemsetAsync(m_out.get(), 0, capacity * m_n * sizeof(float), s));
+    if (short_block && m_tail_ready) {
+        Dims d = dims(valid, m_layout.dtype);
+        launch_unpack(d, raw, m_work.as<float>(), s);
+        normalize_short(capacity, valid, s);
+        FB_CUDA(cudaStreamSynchronize(s));
+        return m_out.as<float>();
+    }
+
+    // The full suite on float samples (lib/cpu/rfi_cpu.cpp:191-208).
+    m_report              = frost_rfi_report{};
+    m_report.nsamps       = valid;
+    m_mask                = m_static_mask;
+    m_report.chans_zapped = count_zeros(m_static_mask);
+    m_report.chans_masked = m_report.chans_zapped;
+    m_raw_ptr           = raw;
+    Dims d                = dims(valid, m_layout.dtype);
+    const float* loc      = m_loc.as<float>();
+    const float* scale    = m_scale.as<float>();
+    if (short_block) {
+        // Too short for statistics: data unchanged, static mask; calibrate
+        // each channel by its own mean/std.
+        ++m_block_index;
+        d.nwin = 1;
+        launch_unpack(d, raw, m_work.as<float>(), s);
+        h2d(m_mask_d, m_mask.data(), m_n, s);
+        launch_welford(d, m_work.as<float>(), m_loc2.as<float>(), m_scale2.as<float>(), s);
+        loc   = m_loc2.as<float>();
+        scale = m_scale2.as<float>();
+        m_time_flags.assign(valid, 0);
+    } else {
+        run_full(d, s);
+        ++m_block_index;
+        if (m_transform) {
+            launch_welford(d, m_work.as<float>(), m_loc2.as<float>(), m_scale2.as<float>(), s);
+            loc   = m_loc2.as<float>();
+            scale = m_scale2.as<float>();
+        }
+        const SizeType last = (d.nwin - 1) * m_n;
+        FB_CUDA(cudaMemcpyAsync(m_tail_loc.get(), m_loc.as<float>() + last, m_n * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+        FB_CUDA(cudaMemcpyAsync(m_tail_scale.get(), m_scale.as<float>() + last, m_n * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+        FB_CUDA(cudaMemcpyAsync(m_tail_out_loc.get(), loc + last, m_n * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+        FB_CUDA(cudaMemcpyAsync(m_tail_out_scale.get(), scale + last, m_n * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+    }
+    launch_normalize(d, m_work.as<float>(), loc, scale, m_mask_d.as<uint8_t>(), flip, capacity,
+                     m_out.as<float>(), s);
+    FB_CUDA(cudaStreamSynchronize(s));
+    m_tail_ready = !short_block;
+    return m_out.as<float>();
+}
+
+void Cleaner::normalize_short(SizeType capacity, SizeType valid, cudaStream_t s) {
+    m_report                    = frost_rfi_report{};
+    m_report.nsamps             = valid;
+    m_report.chans_zapped       = count_zeros(m_static_mask);
+    m_report.chans_masked       = count_zeros(m_mask);
+    m_report.calibration_reused = 1;
+    Dims d                      = dims(valid, m_layout.dtype);
+    h2d(m_mask_d, m_mask.data(), m_n, s);
+    h2d(m_zdot_a_d, m_zdot_a.data(), m_n, s);
+    h2d(m_zdot_b_d, m_zdot_b.data(), m_n, s);
+    launch_normalize_short(d, apply_params(), m_work.as<float>(), m_tail_loc.as<float>(),
+                           m_tail_scale.as<float>(), m_tail_out_loc.as<float>(),
+                           m_tail_out_scale.as<float>(), m_mask_d.as<uint8_t>(),
+                           m_zdot_a_d.as<float>(), m_zdot_b_d.as<float>(),
+                           m_layout.df < 0.0 ? 1 : 0, capacity, m_out.as<float>(), s);
+    m_time_flags.assign(valid, 0);
+    ++m_block_index;
+}
+
+// Channel mask from the static zaps, moments outliers, IQRM and growth
+// (lib/cpu/rfi_cpu_measure.cpp:140-300).
+void Cleaner::build_channel_mask(const Dims& d, const std::vector<uint32_t>& unmeasured,
+                                 const std::vector<float>& scale,
+                                 const std::vector<MomentSums>& mom) {
+    const SizeType n    = m_n;
+    const SizeType nwin = d.nwin;
+    const auto& c       = m_cfg.c;
+    std::vector<uint8_t> dynamic(n, 0U);
+    if (c.moments_enabled) {
+        std::vector<double> mean(n, 0.0), stdev(n, 0.0), skew(n, 0.0), kurt(n, 0.0), acf(n, 0.0);
+        std::vector<uint8_t> good(n, 0U);
+        for (SizeType ch = 0; ch < n; ++ch) {
+            if (m_mask[ch] == 0)
+                continue;
+            MomentSums s{};
+            double lag_pairs = 0.0;
+            for (SizeType w = 0; w < nwin; ++w) {
+                const auto& sw = mom[w * n + ch];
+                s.n += sw.n;
+                s.s1 += sw.s1;
+                s.s2 += sw.s2;
+                s.s3 += sw.s3;
+                s.s4 += sw.s4;
+                s.lag += sw.lag;
+                lag_pairs += std::max(sw.n - 1.0, 0.0);
+            }
+            if (s.n < 2.0)
+                continue;
+            const double m1  = s.s1 / s.n;
+            const double m2  = s.s2 / s.n;
+            const double m3  = s.s3 / s.n;
+            const double m4  = s.s4 / s.n;
+            const double var = m2 - (m1 * m1);
+            if (!(var > 0.0))
+                continue;
+            good[ch]  = 1;
+            mean[ch]  = m1;
+            stdev[ch] = std::sqrt(var);
+            skew[ch]  = (m3 - (3.0 * m1 * m2) + (2.0 * m1 * m1 * m1)) / (var * stdev[ch]);
+            kurt[ch]  = ((m4 - (4.0 * m1 * m3) + (6.0 * m1 * m1 * m2) - (3.0 * m1 * m1 * m1 * m1)) /
+                        (var * var)) -
+                       3.0;
+            acf[ch] = lag_pairs > 0.0 ? ((s.lag / lag_pairs) - (m1 * m1)) / var : 0.0;
+        }
+        const double k = c.moments_threshold;
+        if (c.moments_mean)
+            stats::flag_iqr_outliers(mean, good, k, dynamic);
+        if (c.moments_std)
+            stats::flag_iqr_outliers(stdev, good, k, dynamic);
+        if (c.moments_skewness)
+            stats::flag_iqr_outliers(skew, good, k, dynamic);
+        if (c.moments_kurtosis)
+            stats::flag_iqr_outliers(kurt, good, k, dynamic);
+        if (c.moments_autocorr)
+            stats::flag_iqr_outliers(acf, good, k, dynamic);
+        if (c.moments_kurtosis_max > 0.0F)
+            for (SizeType ch = 0; ch < n; ++ch)
+                if (good[ch] && std::abs(kurt[ch]) > c.moments_kurtosis_max)
+                    dynamic[ch] = 1;
+        m_report.chans_moments = static_cast<SizeType>(std::count(dynamic.begin(), dynamic.end(), 1U));
+    }
+    if (c.iqrm_enabled) {
+        std::vector<float> std_data(n, 0.0F);
+        std::vector<uint8_t> ignore(n, 0U);
+        for (SizeType ch = 0; ch < n; ++ch) {
+            ignore[ch]    = (m_mask[ch] == 0 || unmeasured[ch] > 0) ? 1 : 0;
+            double weight = 0.0, acc = 0.0;
+            for (SizeType w = 0; w < nwin; ++w) {
+                const auto& s = mom[w * n + ch];
+                if (s.n > 1.0) {
+                    const double mean = s.s1 / s.n;
+                    const double var  = (s.s2 / s.n) - (mean * mean);
+                    const double sc   = scale[w * n + ch];
+                    acc += s.n * std::max(var, 0.0) * sc * sc;
+                    weight += s.n;
+                }
+            }
+            std_data[ch] = weight > 0.0 ? static_cast<float>(std::sqrt(acc / weight)) : 0.0F;
+        }
+        const SizeType radius = c.iqrm_radius > 0 ? c.iqrm_radius : std::max<SizeType>(n / 10, 1);
+        const auto flags      = stats::iqrm_mask(std_data, radius, c.iqrm_threshold, ignore);
+        for (SizeType ch = 0; ch < n; ++ch) {
+            if (flags[ch] != 0 && ignore[ch] == 0 && dynamic[ch] == 0) {
+                dynamic[ch] = 1;
+                ++m_report.chans_iqrm;
+            }
+        }
+    }
+    if (c.mask_grow > 0) {
+        std::vector<uint8_t> grown = dynamic;
+        const SizeType g           = c.mask_grow;
+        for (SizeType ch = 0; ch < n; ++ch) {
+            if (dynamic[ch] == 0)
+                continue;
+            const SizeType first = ch > g ? ch - g : 0;
+            const SizeType last  = ch + std::min(g, n - 1 - ch);
+            for (SizeType k = first; k <= last; ++k)
+                grown[k] = 1;
+        }
+        for (SizeType ch = 0; ch < n; ++ch)
+            if (grown[ch] != 0 && dynamic[ch] == 0 && m_mask[ch] != 0)
+                ++m_report.chans_grown;
+        dynamic = std::move(grown);
+    }
+    for (SizeType ch = 0; ch < n; ++ch)
+        if (dynamic[ch] != 0)
+            m_mask[ch] = 0;
+    m_report.chans_masked = count_zeros(m_mask);
+}
+
+void Cleaner::run_full(const Dims& d, cudaStream_t s) {
+    const SizeType n     = m_n;
+    const SizeType nwin  = d.nwin;
+    const SizeType T     = d.nsamps;
+    const auto& c        = m_cfg.c;
+    const uint8_t* raw   = m_raw_ptr;
+    const bool zdot      = c.zero_dm == FROST_ZERO_DM_ZDOT;
+    const bool kchan     = c.kadane_channel_enabled != 0;
+    const bool kspec     = c.kadane_spectrum_enabled != 0;
+
+    // ---- bandpass ----
+    auto t = Clock::now();
+    m_samples.reserve(nwin * kMaxBandpassRows * n * sizeof(float));
+    m_unmeasured.reserve(n * sizeof(uint32_t));
+    FB_CUDA(cudaMemsetAsync(m_unmeasured.get(), 0, n * sizeof(uint32_t), s));
+    launch_sample_rows(d, raw, m_samples.as<float>(), s);
+    launch_bandpass(d, m_samples.as<float>(), m_loc.as<float>(), m_scale.as<float>(),
+                    m_inv.as<float>(), m_unmeasured.as<uint32_t>(), s);
+    std::vector<uint32_t> unmeasured;
+    std::vector<float> scale_h;
+    d2h(unmeasured, m_unmeasured, n, s);
+    if (c.iqrm_enabled)
+        d2h(scale_h, m_scale, nwin * n, s);
+    FB_CUDA(cudaStreamSynchronize(s));
+    m_report.t_bandpass = since(t);
+
+    // ---- moments and channel mask ----
+    t = Clock::now();
+    std::vector<MomentSums> mom;
+    if (m_need_moments) {
+        m_moments.reserve(nwin * n * sizeof(MomentSums));
+        launch_moments(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_static_mask_d.as<uint8_t>(),
+                       m_clip, m_moments.as<MomentSums>(), s);
+        d2h(mom, m_moments, nwin * n, s);
+        FB_CUDA(cudaStreamSynchronize(s));
+        std::vector<float> cmean(nwin * n, 0.0F), cinv(nwin * n, 0.0F);
+        for (SizeType i = 0; i < nwin * n; ++i) {
+            const auto& sm = mom[i];
+            if (sm.nc > 1.0) {
+                const double mean = sm.c1 / sm.nc;
+                const double var  = (sm.c2 / sm.nc) - (mean * mean);
+                cmean[i]          = static_cast<float>(mean);
+                cinv[i]           = var > 0.0 ? static_cast<float>(1.0 / std::sqrt(var)) : 0.0F;
+            }
+        }
+        h2d(m_clip_mean, cmean.data(), nwin * n, s);
+        h2d(m_clip_inv, cinv.data(), nwin * n, s);
+    }
+    build_channel_mask(d, unmeasured, scale_h, mom);
+    std::vector<uint64_t> good_prefix(n + 1, 0);
+    for (SizeType ch = 0; ch < n; ++ch)
+        good_prefix[ch + 1] = good_prefix[ch] + (m_mask[ch] != 0 ? 1 : 0);
+    h2d(m_mask_d, m_mask.data(), n, s);
+    h2d(m_good_prefix, good_prefix.data(), n + 1, s);
+    m_report.t_moments = since(t);
+
+    // ---- scan ----
+    t = Clock::now();
+    m_s_det.reserve(T * sizeof(float));
+    m_s_keep_d.reserve(T * sizeof(double));
+    m_s_keep_f.reserve(T * sizeof(float));
+    m_row_std.reserve(T * sizeof(float));
+    m_kspec_pos.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
+    m_kspec_neg.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
+    m_kspec_whole.reserve(std::max<SizeType>(T, 1));
+    const SizeType nck = d.nchunks * n;
+    m_chunk_min.reserve(nck * sizeof(float));
+    m_chunk_max.reserve(nck * sizeof(float));
+    m_chunk_zdot.reserve(std::max<SizeType>(zdot ? nck : 1, 1) * sizeof(ZdotSums));
+    m_chunk_kpos.reserve(std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState));
+    m_chunk_kneg.reserve(std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState));
+    m_lo.reserve(n * sizeof(float));
+    m_hi.reserve(n * sizeof(float));
+    m_zdot_sum.reserve(n * sizeof(ZdotSums));
+    m_kpos_best.reserve(n * sizeof(Run));
+    m_kneg_best.reserve(n * sizeof(Run));
+    m_clip_mean.reserve(sizeof(float));
+    m_clip_inv.reserve(sizeof(float));
+
+    std::vector<float> s_det, row_std, lo, hi;
+    std::vector<uint8_t> kwhole;
+    std::vector<ZdotSums> zsum;
+    std::vector<Run> kpb, knb;
+    const bool any_good = good_prefix[n] != 0;
+    if (any_good) {
+        KspecParams kp{};
+        kp.enabled      = kspec ? 1 : 0;
+        kp.min_bw_chans = kspec ? static_cast<double>(c.kadane_spectrum_min_bandwidth) /
+                                      std::abs(m_layout.df)
+                                : 0.0;
+        kp.whole_chans = static_cast<double>(c.kadane_spectrum_whole_band_fraction) *
+                         static_cast<double>(n);
+        kp.threshold = c.kadane_spectrum_threshold;
+        launch_scan_rows(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(),
+                         m_clip, kp, m_good_prefix.as<uint64_t>(), m_s_det.as<float>(),
+                         m_s_keep_d.as<double>(), m_s_keep_f.as<float>(), m_row_std.as<float>(),
+                         m_kspec_pos.as<Span32>(), m_kspec_neg.as<Span32>(),
+                         m_kspec_whole.as<uint8_t>(), s);
+        launch_scan_cols(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(),
+                         m_clip, m_s_keep_d.as<double>(), zdot ? 1 : 0, kchan ? 1 : 0,
+                         m_clip_mean.as<float>(), m_clip_inv.as<float>(), m_chunk_min.as<float>(),
+                         m_chunk_max.as<float>(), m_chunk_zdot.as<ZdotSums>(),
+                         m_chunk_kpos.as<KadaneState>(), m_chunk_kneg.as<KadaneState>(),
+                         m_lo.as<float>(), m_hi.as<float>(), m_zdot_sum.as<ZdotSums>(),
+                         m_kpos_best.as<Run>(), m_kneg_best.as<Run>(), s);
+        d2h(s_det, m_s_det, T, s);
+        if (c.dropout_enabled)
+            d2h(row_std, m_row_std, T, s);
+        if (kspec)
+            d2h(kwhole, m_kspec_whole, T, s);
+        d2h(lo, m_lo, n, s);
+        d2h(hi, m_hi, n, s);
+        if (zdot)
+            d2h(zsum, m_zdot_sum, n, s);
+        if (kchan) {
+            d2h(kpb, m_kpos_best, n, s);
+            d2h(knb, m_kneg_best, n, s);
+        }
+    } else {
+        FB_CUDA(cudaMemsetAsync(m_s_keep_f.get(), 0, T * sizeof(float), s));
+        if (kspec) {
+            FB_CUDA(cudaMemsetAsync(m_kspec_pos.get(), 0xFF, T * sizeof(Span32), s));
+            FB_CUDA(cudaMemsetAsync(m_kspec_neg.get(), 0xFF, T * sizeof(Span32), s));
+        }
+    }
+    FB_CUDA(cudaStreamSynchronize(s));
+    m_report.t_scan = since(t);
+
+    // ---- flags (lib/cpu/rfi_cpu.cpp:347-468) ----
+    t = Clock::now();
+    if (any_good) {
+        for (SizeType ch = 0; ch < n; ++ch) {
+            if (m_mask[ch] == 0 || unmeasured[ch] < nwin)
+                continue;
+            if (!(hi[ch] > lo[ch])) {
+                m_mask[ch] = 0;
+                ++m_report.chans_dead;
+            }
+        }
+    }
+    m_report.chans_masked = count_zeros(m_mask);
+    m_time_flags.assign(T, 0U);
+    std::vector<Segment> kcp, kcn;
+    if (any_good) {
+        if (c.broad_enabled)
+            m_report.samps_broad = stats::broadband_time_flags(
+                s_det, m_smooth_radius, c.broad_threshold, c.broad_boxcar_max, m_time_flags);
+        if (c.dropout_enabled) {
+            std::vector<float> spread = row_std;
+            const auto mid = spread.begin() + static_cast<IndexType>(T / 2);
+            std::nth_element(spread.begin(), mid, spread.end());
+            const float cut = c.dropout_min_std_fraction * *mid;
+            std::vector<uint8_t> drop(T, 0U);
+            for (SizeType i = 0; i < T; ++i) {
+                if (row_std[i] < cut) {
+                    drop[i] = 1;
+                    if (i > 0)
+                        drop[i - 1] = 1;
+                    if (i + 1 < T)
+                        drop[i + 1] = 1;
+                }
+            }
+            for (SizeType i = 0; i < T; ++i) {
+                if (drop[i] != 0 && m_time_flags[i] == 0) {
+                    m_time_flags[i] = 1;
+                    ++m_report.samps_dropout;
+                }
+            }
+        }
+        if (kspec) {
+            for (SizeType i = 0; i < T; ++i) {
+                if (kwhole[i] != 0 && m_time_flags[i] == 0) {
+                    m_time_flags[i] = 1;
+                    ++m_report.samps_kadane;
+                }
+            }
+        }
+        m_report.samps_flagged =
+            static_cast<SizeType>(std::count(m_time_flags.begin(), m_time_flags.end(), 1U));
+        if (zdot) {
+            m_zdot_a.assign(n, 0.0F);
+            m_zdot_b.assign(n, 0.0F);
+            for (SizeType ch = 0; ch < n; ++ch) {
+                const ZdotSums& sm = zsum[ch];
+                if (sm.n < 2.0)
+                    continue;
+                const double mz    = sm.sz / sm.n;
+                const double ms    = sm.ss / sm.n;
+                const double var_s = (sm.sss / sm.n) - (ms * ms);
+                const double cov   = (sm.szs / sm.n) - (mz * ms);
+                const double a     = var_s > 0.0 ? cov / var_s : 0.0;
+                m_zdot_a[ch]       = static_cast<float>(a);
+                m_zdot_b[ch]       = static_cast<float>(mz - (a * ms));
+            }
+        }
+        if (kchan) {
+            const double min_len = static_cast<double>(c.kadane_channel_min_duration) / m_layout.tsamp;
+            kcp.assign(n, Segment{0, -1});
+            kcn.assign(n, Segment{0, -1});
+            auto accept = [&](const Run& r, Segment& out) {
+                const auto len = static_cast<double>(r.length());
+                if (len > 0.0 && len >= min_len && r.sum / std::sqrt(len) > c.kadane_channel_threshold)
+                    out = {r.start, r.end};
+            };
+            for (SizeType ch = 0; ch < n; ++ch) {
+                if (m_mask[ch] == 0)
+                    continue;
+                accept(kpb[ch], kcp[ch]);
+                accept(knb[ch], kcn[ch]);
+            }
+        }
+    }
+    m_report.t_flags = since(t);
+
+    // ---- apply (lib/cpu/rfi_cpu.cpp:526-720) ----
+    t = Clock::now();
+    std::vector<uint64_t> flagged;
+    for (SizeType i = 0; i < T; ++i)
+        if (m_time_flags[i] != 0)
+            flagged.push_back(i);
+    h2d(m_time_flags_d, m_time_flags.data(), T, s);
+    h2d(m_mask_d, m_mask.data(), n, s);
+    h2d(m_zdot_a_d, m_zdot_a.data(), n, s);
+    h2d(m_zdot_b_d, m_zdot_b.data(), n, s);
+    if (kchan) {
+        h2d(m_kchan_pos_d, kcp.data(), n, s);
+        h2d(m_kchan_neg_d, kcn.data(), n, s);
+    } else {
+        m_kchan_pos_d.reserve(sizeof(Segment));
+        m_kchan_neg_d.reserve(sizeof(Segment));
+    }
+    h2d(m_flagged_d, flagged.data(), flagged.size(), s);
+    FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, kCountSlots * sizeof(unsigned long long), s));
+    const ApplyParams p = apply_params();
+    launch_apply_unflagged(d, p, raw, m_loc.as<float>(), m_scale.as<float>(), m_inv.as<float>(),
+                           m_mask_d.as<uint8_t>(), m_time_flags_d.as<uint8_t>(),
+                           m_kspec_pos.as<Span32>(), m_kspec_neg.as<Span32>(),
+                           m_kchan_pos_d.as<Segment>(), m_kchan_neg_d.as<Segment>(),
+                           m_s_keep_f.as<float>(), m_zdot_a_d.as<float>(), m_zdot_b_d.as<float>(),
+                           m_work.as<float>(), m_counters.as<unsigned long long>(), s);
+    launch_apply_flagged(d, p, m_flagged_d.as<uint64_t>(), flagged.size(), m_loc.as<float>(),
+                         m_scale.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(),
+                         m_time_flags_d.as<uint8_t>(), m_work.as<float>(),
+                         m_counters.as<unsigned long long>(), s);
+    unsigned long long counts[kCountSlots];
+    FB_CUDA(cudaMemcpyAsync(counts, m_counters.get(), sizeof(counts), cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
+    m_report.cells_narrow          = counts[kCountNarrow];
+    m_report.cells_kadane_spectrum = counts[kCountKspec];
+    m_report.cells_kadane_channel  = counts[kCountKchan];
+    m_report.fill_fallbacks        = counts[kCountFallback];
+    m_report.t_apply               = since(t);
+}
+
+} // namespace fb::rfi

@@ -1,0 +1,958 @@
+// RFI excision kernels for sm_100a.
+//
+// The cleaner's decisions (masks, time flags, cell states) must agree bit for
+// bit with frost's CPU cleaner, so every threshold-deciding sum keeps the
+// reference's summation order: per (window, channel) over time for the
+// bandpass refinement, moments and Welford statistics; per row over channels
+// for the detection series; per (chunk, channel) over time for zdot and
+// Kadane-along-time. Parallelism comes from the many independent
+// (window, channel), row and (chunk, channel) sequences instead of from
+// splitting any one of them. This file is compiled with --fmad=false so no
+// multiply-add is contracted and each float/double operation rounds exactly
+// as the IEEE host build does.
+//
+// Packed samples are decoded on the fly from the raw time-major block (LSB
+// first below 8 bits, lib/prepare/sample_codec.hpp:18-109), so the 1/4-byte
+// raw block is what every statistics pass reads from HBM.
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+#include <cstring>
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "rfi_kernels.hpp"
+
+namespace fb::rfi {
+
+namespace {
+
+// ---- sample decoding --------------------------------------------------
+
+template <int D> __device__ __forceinline__ float rd(const uint8_t* __restrict__ row, uint64_t c) {
+    if constexpr (D == FROST_UINT8) {
+        return static_cast<float>(row[c]);
+    } else if constexpr (D == FROST_UINT16) {
+        return static_cast<float>(reinterpret_cast<const uint16_t*>(row)[c]);
+    } else if constexpr (D == FROST_UINT32) {
+        return static_cast<float>(reinterpret_cast<const uint32_t*>(row)[c]);
+    } else if constexpr (D == FROST_FLOAT32) {
+        return reinterpret_cast<const float*>(row)[c];
+    } else {
+        constexpr unsigned kBits = D == FROST_UINT1 ? 1U : D == FROST_UINT2 ? 2U : 4U;
+        constexpr unsigned kMask = (1U << kBits) - 1U;
+        const uint64_t bit       = c * kBits;
+        return static_cast<float>((row[bit >> 3U] >> (bit & 7U)) & kMask);
+    }
+}
+
+#define FB_DTYPE_CASE(DT, ...)                                                                    \
+    case DT: {                                                                                    \
+        constexpr int D = DT;                                                                     \
+        __VA_ARGS__;                                                                              \
+    } break;
+
+#define FB_DISPATCH(dtype, ...)                                                                   \
+    switch (dtype) {                                                                              \
+        FB_DTYPE_CASE(FROST_UINT1, __VA_ARGS__)                                                   \
+        FB_DTYPE_CASE(FROST_UINT2, __VA_ARGS__)                                                   \
+        FB_DTYPE_CASE(FROST_UINT4, __VA_ARGS__)                                                   \
+        FB_DTYPE_CASE(FROST_UINT8, __VA_ARGS__)                                                   \
+        FB_DTYPE_CASE(FROST_UINT16, __VA_ARGS__)                                                  \
+        FB_DTYPE_CASE(FROST_UINT32, __VA_ARGS__)                                                  \
+        FB_DTYPE_CASE(FROST_FLOAT32, __VA_ARGS__)                                                 \
+    default: throw ::fb::Error(FROST_ERR_INVALID_ARGUMENT, "unsupported dtype");                 \
+    }
+
+// ---- order-exact helpers ------------------------------------------------
+
+// std::min / std::max semantics (first argument kept on ties), which the
+// remedian's median network relies on for bit-identical results.
+template <class T> __device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
+template <class T> __device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ float median3(float a, float b, float c) {
+    return a < b ? (b < c ? b : (a < c ? c : a)) : (a < c ? a : (b < c ? c : b));
+}
+
+// Median of five: drop the extremes of the first four, then the median of
+// the remaining pair and the fifth value.
+__device__ __forceinline__ float median5(float a, float b, float c, float d, float e) {
+    const float f = smax(smin(a, b), smin(c, d));
+    const float g = smin(smax(a, b), smax(c, d));
+    return median3(e, f, g);
+}
+
+__device__ __forceinline__ float clampf(float v, float lo, float hi) {
+    return (v < lo) ? lo : (hi < v) ? hi : v;
+}
+
+__device__ __forceinline__ uint64_t window_of(uint64_t t, uint64_t window, uint64_t nwin) {
+    const uint64_t w = t / window;
+    return w < nwin - 1 ? w : nwin - 1;
+}
+
+__device__ __forceinline__ uint64_t window_begin(uint64_t w, uint64_t window) { return w * window; }
+__device__ __forceinline__ uint64_t window_end(uint64_t w, const Dims& d) {
+    return w + 1 == d.nwin ? d.nsamps : (w + 1) * d.window;
+}
+
+__device__ __forceinline__ float normal_deviate(uint64_t h) {
+    constexpr double kTwoPi = 6.283185307179586;
+    const double u1         = uniform_open(h);
+    const double u2         = uniform_open(splitmix64(h));
+    return static_cast<float>(sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2));
+}
+
+__device__ __forceinline__ uint64_t draw(const ApplyParams& p, uint64_t stream, uint64_t t,
+                                         uint64_t c, uint64_t attempt) {
+    return hash5(p.seed, p.block_index, (stream << 56U) ^ t, c, attempt);
+}
+
+// ---- finite check ---------------------------------------------------------
+
+__global__ void k_check_finite(const uint32_t* __restrict__ w, uint64_t n,
+                               unsigned long long* first_bad) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        if ((w[i] & 0x7F800000U) == 0x7F800000U)
+            atomicMin(first_bad, static_cast<unsigned long long>(i));
+    }
+}
+
+// ---- bandpass -------------------------------------------------------------
+
+template <int D>
+__global__ void k_sample_rows(Dims d, const uint8_t* __restrict__ raw, float* __restrict__ out) {
+    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t i = blockIdx.y;
+    const uint64_t w = blockIdx.z;
+    if (c >= d.nchans)
+        return;
+    const uint64_t b   = window_begin(w, d.window);
+    const uint64_t len = window_end(w, d) - b;
+    const uint64_t m   = largest_power_of_five_leq(len < kMaxBandpassRows ? len : kMaxBandpassRows);
+    if (i >= m)
+        return;
+    const uint64_t t = b + (i * len) / m;
+    out[(w * kMaxBandpassRows + i) * d.nchans + c] = rd<D>(raw + t * d.row_bytes, c);
+}
+
+// Recursive median-of-5 over m = 5^k values streamed in order: the same
+// groups of five, level by level, as the batch remedian in
+// lib/cpu/spectra_cpu.cpp:43-69.
+struct Remedian {
+    float buf[5][5];
+    int cnt[5];
+    int depth;
+    float result;
+
+    __device__ void init(int levels) {
+        depth = levels;
+        for (int l = 0; l < 5; ++l)
+            cnt[l] = 0;
+        result = 0.0F;
+    }
+    __device__ void push(float x) {
+        int l = 0;
+        while (true) {
+            if (l == depth) {
+                result = x;
+                return;
+            }
+            buf[l][cnt[l]++] = x;
+            if (cnt[l] < 5)
+                return;
+            cnt[l] = 0;
+            x      = median5(buf[l][0], buf[l][1], buf[l][2], buf[l][3], buf[l][4]);
+            ++l;
+        }
+    }
+};
+
+__global__ void k_bandpass(Dims d, const float* __restrict__ samples, float* __restrict__ loc_out,
+                           float* __restrict__ scale_out, float* __restrict__ inv_out,
+                           uint32_t* __restrict__ unmeasured) {
+    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t w = blockIdx.y;
+    if (c >= d.nchans)
+        return;
+    const uint64_t b   = window_begin(w, d.window);
+    const uint64_t len = window_end(w, d) - b;
+    const uint64_t m   = largest_power_of_five_leq(len < kMaxBandpassRows ? len : kMaxBandpassRows);
+    int levels         = 0;
+    for (uint64_t p = m; p > 1; p /= 5)
+        ++levels;
+    const uint64_t n = d.nchans;
+    const float* v   = samples + w * kMaxBandpassRows * n + c;
+
+    // Level: remedian over the sampled rows; scale: remedian of |x - level|
+    // times 1.4826 (lib/cpu/spectra_cpu.cpp:73-130).
+    Remedian r;
+    r.init(levels);
+    for (uint64_t i = 0; i < m; ++i)
+        r.push(v[i * n]);
+    const float level = r.result;
+    r.init(levels);
+    for (uint64_t i = 0; i < m; ++i)
+        r.push(fabsf(v[i * n] - level));
+    const float rms = r.result * kMadToStd;
+
+    // Clipped refinement in double (lib/cpu/bandpass_kernels.hpp:17-76).
+    float lo = v[0], hi = v[0];
+    for (uint64_t i = 1; i < m; ++i) {
+        lo = smin(lo, v[i * n]);
+        hi = smax(hi, v[i * n]);
+    }
+    const uint64_t o = w * n + c;
+    if (!(hi > lo)) {
+        loc_out[o]   = lo;
+        scale_out[o] = 0.0F;
+        inv_out[o]   = 0.0F;
+        atomicAdd(&unmeasured[c], 1U);
+        return;
+    }
+    double centre = level;
+    double s      = rms;
+    const double dm = static_cast<double>(m);
+    if (!(s > 0.0)) {
+        double mean = 0.0;
+        for (uint64_t i = 0; i < m; ++i)
+            mean += v[i * n];
+        mean /= dm;
+        double ss = 0.0;
+        for (uint64_t i = 0; i < m; ++i)
+            ss += (v[i * n] - mean) * (v[i * n] - mean);
+        s = sqrt(ss / dm);
+    }
+    for (int it = 0; it < kClipIterations; ++it) {
+        const double cut = kClipSigma * s;
+        double count = 0.0, sum = 0.0;
+        for (uint64_t i = 0; i < m; ++i) {
+            const double dv = v[i * n] - centre;
+            if (fabs(dv) <= cut) {
+                count += 1.0;
+                sum += dv;
+            }
+        }
+        if (count < 2.0)
+            break;
+        const double shift = sum / count;
+        double ss          = 0.0;
+        for (uint64_t i = 0; i < m; ++i) {
+            const double dv = v[i * n] - centre;
+            if (fabs(dv) <= cut)
+                ss += (dv - shift) * (dv - shift);
+        }
+        const double clipped = sqrt(ss / count);
+        if (!(clipped > 0.0))
+            break;
+        centre += shift;
+        s = clipped;
+    }
+    const float fl = static_cast<float>(centre);
+    const float fs = static_cast<float>(s);
+    loc_out[o]     = fl;
+    scale_out[o]   = fs;
+    inv_out[o]     = 1.0F / fs;
+}
+
+// ---- moments --------------------------------------------------------------
+
+template <int D>
+__global__ void k_moments(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
+                          const float* __restrict__ inv, const uint8_t* __restrict__ static_mask,
+                          float clip, MomentSums* __restrict__ out) {
+    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t w = blockIdx.y;
+    if (c >= d.nchans)
+        return;
+    const uint64_t o = w * d.nchans + c;
+    MomentSums s{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const float l = loc[o], iv = inv[o];
+    if (static_mask[c] != 0 && iv != 0.0F) {
+        const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
+        double prev      = 0.0;
+        for (uint64_t t = b; t < e; ++t) {
+            const float x   = rd<D>(raw + t * d.row_bytes, c);
+            const double z  = (x - l) * iv;
+            const double z2 = z * z;
+            s.n += 1.0;
+            s.s1 += z;
+            s.s2 += z2;
+            s.s3 += z2 * z;
+            s.s4 += z2 * z2;
+            if (t > b)
+                s.lag += z * prev;
+            prev = z;
+            if (fabs(z) <= clip) {
+                s.nc += 1.0;
+                s.c1 += z;
+                s.c2 += z2;
+            }
+        }
+    }
+    out[o] = s;
+}
+
+// ---- row scan ---------------------------------------------------------------
+
+constexpr int kScanRows  = 128; // rows per CTA (one thread each)
+constexpr int kScanChans = 64;  // channel tile staged in shared memory
+
+template <int D>
+__global__ void __launch_bounds__(kScanRows)
+    k_scan_rows(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
+                const float* __restrict__ inv, const uint8_t* __restrict__ mask, float clip,
+                KspecParams kp, const uint64_t* __restrict__ good_prefix, float* __restrict__ s_det,
+                double* __restrict__ s_keep_d, float* __restrict__ s_keep_f,
+                float* __restrict__ row_std, Span32* __restrict__ kspec_pos,
+                Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole) {
+    __shared__ float tile[kScanRows][kScanChans + 1];
+    const uint64_t t0    = static_cast<uint64_t>(blockIdx.x) * kScanRows;
+    const uint64_t t     = t0 + threadIdx.x;
+    const bool active    = t < d.nsamps;
+    const uint64_t n     = d.nchans;
+    const uint64_t w     = active ? window_of(t, d.window, d.nwin) : 0;
+    const float* lw      = loc + w * n;
+    const float* iw      = inv + w * n;
+    double sum_det = 0.0, sum_keep = 0.0, n_keep = 0.0, sx = 0.0, sxx = 0.0, n_meas = 0.0;
+    KadaneState sp = KadaneState::make(), sn = KadaneState::make();
+
+    for (uint64_t c0 = 0; c0 < n; c0 += kScanChans) {
+        const unsigned cl_ = threadIdx.x % kScanChans;
+        const uint64_t cc  = c0 + cl_;
+        __syncthreads();
+        for (int r = threadIdx.x / kScanChans; r < kScanRows; r += kScanRows / kScanChans) {
+            const uint64_t tr = t0 + r;
+            tile[r][cl_] = (tr < d.nsamps && cc < n) ? rd<D>(raw + tr * d.row_bytes, cc) : 0.0F;
+        }
+        __syncthreads();
+        if (!active)
+            continue;
+        const uint64_t cend = (c0 + kScanChans < n) ? c0 + kScanChans : n;
+        for (uint64_t c = c0; c < cend; ++c) {
+            if (mask[c] == 0)
+                continue;
+            const float ic = iw[c];
+            if (ic == 0.0F)
+                continue;
+            const float x = tile[threadIdx.x][c - c0];
+            n_meas += 1.0;
+            const float zc = (x - lw[c]) * ic;
+            const float cl = clampf(zc, -clip, clip);
+            sum_det += cl;
+            if (fabsf(zc) <= clip) {
+                sum_keep += zc;
+                n_keep += 1.0;
+            }
+            sx += x;
+            sxx += static_cast<double>(x) * x;
+            if (kp.enabled) {
+                sp.append(static_cast<int64_t>(c), cl);
+                sn.append(static_cast<int64_t>(c), -cl);
+            }
+        }
+    }
+    if (!active)
+        return;
+    const double dn     = n_meas > 1.0 ? n_meas : 1.0;
+    const double s_keep = n_keep > 0.0 ? sum_keep / n_keep : 0.0;
+    s_det[t]            = static_cast<float>(sum_det / dn);
+    s_keep_f[t]         = static_cast<float>(s_keep);
+    s_keep_d[t]         = s_keep;
+    const double mx     = sx / dn;
+    const double var    = (sxx / dn) - (mx * mx);
+    row_std[t]          = static_cast<float>(sqrt(var < 0.0 ? 0.0 : var));
+    if (kp.enabled) {
+        // accept_span (lib/cpu/rfi_cpu_measure.cpp:335-349)
+        auto accept = [&](const Run& r, Span32& out) -> bool {
+            out = {-1, -1};
+            if (r.length() <= 0)
+                return false;
+            const uint64_t lo    = static_cast<uint64_t>(r.start);
+            const uint64_t hi    = static_cast<uint64_t>(r.end);
+            const uint64_t count = good_prefix[hi + 1] - good_prefix[lo];
+            const double nspan   = static_cast<double>(hi - lo + 1);
+            const double snr     = r.sum / sqrt(static_cast<double>(count));
+            if (snr > kp.threshold && nspan >= kp.min_bw_chans) {
+                out = {static_cast<int32_t>(lo), static_cast<int32_t>(hi)};
+                return nspan > kp.whole_chans;
+            }
+            return false;
+        };
+        Span32 a, b;
+        bool whole = accept(sp.best, a);
+        whole      = accept(sn.best, b) || whole;
+        kspec_pos[t]   = a;
+        kspec_neg[t]   = b;
+        kspec_whole[t] = whole ? 1 : 0;
+    }
+}
+
+template <int D>
+__global__ void k_scan_cols(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
+                            const float* __restrict__ inv, const uint8_t* __restrict__ mask,
+                            float clip, const double* __restrict__ s_keep_d, int zdot, int kchan,
+                            const float* __restrict__ clip_mean,
+                            const float* __restrict__ clip_inv_std, float* __restrict__ cmin_out,
+                            float* __restrict__ cmax_out, ZdotSums* __restrict__ zs_out,
+                            KadaneState* __restrict__ kp_out, KadaneState* __restrict__ kn_out) {
+    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t k = blockIdx.y;
+    if (c >= d.nchans)
+        return;
+    const uint64_t n = d.nchans;
+    float cmin = FLT_MAX, cmax = -FLT_MAX;
+    ZdotSums zs{0, 0, 0, 0, 0};
+    KadaneState kpos = KadaneState::make(), kneg = KadaneState::make();
+    if (mask[c] != 0) {
+        const uint64_t t0 = k * d.chunk;
+        const uint64_t t1 = (t0 + d.chunk < d.nsamps) ? t0 + d.chunk : d.nsamps;
+        for (uint64_t t = t0; t < t1; ++t) {
+            const uint64_t w = window_of(t, d.window, d.nwin);
+            const uint64_t o = w * n + c;
+            const float x    = rd<D>(raw + t * d.row_bytes, c);
+            const float iv   = inv[o];
+            float z          = 0.0F;
+            if (iv == 0.0F) {
+                cmin = smin(cmin, x);
+                cmax = smax(cmax, x);
+            } else {
+                z = (x - loc[o]) * iv;
+            }
+            const bool outlier = fabsf(z) > clip;
+            if (zdot && !outlier && iv != 0.0F) {
+                const double sk = s_keep_d[t];
+                zs.n += 1.0;
+                zs.sz += z;
+                zs.ss += sk;
+                zs.sss += sk * sk;
+                zs.szs += z * sk;
+            }
+            if (kchan) {
+                const double u = outlier ? 0.0 : static_cast<double>((z - clip_mean[o]) * clip_inv_std[o]);
+                kpos.append(static_cast<int64_t>(t), u);
+                kneg.append(static_cast<int64_t>(t), -u);
+            }
+        }
+    }
+    const uint64_t o = k * n + c;
+    cmin_out[o]      = cmin;
+    cmax_out[o]      = cmax;
+    if (zdot)
+        zs_out[o] = zs;
+    if (kchan) {
+        kp_out[o] = kpos;
+        kn_out[o] = kneg;
+    }
+}
+
+// Per channel, in chunk order: the block min/max of unmeasured cells, the
+// zdot sums and the combined Kadane-along-time states
+// (lib/cpu/rfi_cpu.cpp:352-366, 413-466).
+__global__ void k_combine_chunks(Dims d, int zdot, int kchan, const float* __restrict__ cmin,
+                                 const float* __restrict__ cmax, const ZdotSums* __restrict__ zs,
+                                 const KadaneState* __restrict__ kp,
+                                 const KadaneState* __restrict__ kn, float* __restrict__ lo_out,
+                                 float* __restrict__ hi_out, ZdotSums* __restrict__ zs_out,
+                                 Run* __restrict__ kp_best, Run* __restrict__ kn_best) {
+    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (c >= d.nchans)
+        return;
+    const uint64_t n = d.nchans;
+    float lo = FLT_MAX, hi = -FLT_MAX;
+    ZdotSums s{0, 0, 0, 0, 0};
+    KadaneState pos = KadaneState::make(), neg = KadaneState::make();
+    for (uint64_t k = 0; k < d.nchunks; ++k) {
+        lo = smin(lo, cmin[k * n + c]);
+        hi = smax(hi, cmax[k * n + c]);
+        if (zdot) {
+            const ZdotSums& p = zs[k * n + c];
+            s.n += p.n;
+            s.sz += p.sz;
+            s.ss += p.ss;
+            s.sss += p.sss;
+            s.szs += p.szs;
+        }
+        if (kchan) {
+            pos = KadaneState::combine(pos, kp[k * n + c]);
+            neg = KadaneState::combine(neg, kn[k * n + c]);
+        }
+    }
+    lo_out[c] = lo;
+    hi_out[c] = hi;
+    if (zdot)
+        zs_out[c] = s;
+    if (kchan) {
+        kp_best[c] = pos.best;
+        kn_best[c] = neg.best;
+    }
+}
+
+// ---- apply ------------------------------------------------------------------
+
+__device__ __forceinline__ float level_of(const ApplyParams& p, float loc, float scale, float v) {
+    return p.equalize ? p.eq_loc + (p.eq_scale * v) : loc + (scale * v);
+}
+
+// Unflagged rows (lib/cpu/rfi_cpu.cpp:537-624): one CTA per row; the row's
+// samples and cell states are staged in shared memory so neighbour draws
+// read them without touching HBM again. Masked cells are not written: the
+// normalized output zeroes them, so their fill values are never observed.
+template <int D>
+__global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restrict__ raw,
+                                  const float* __restrict__ loc, const float* __restrict__ scale,
+                                  const float* __restrict__ inv, const uint8_t* __restrict__ mask,
+                                  const uint8_t* __restrict__ time_flags,
+                                  const Span32* __restrict__ kspec_pos,
+                                  const Span32* __restrict__ kspec_neg,
+                                  const Segment* __restrict__ kchan_pos,
+                                  const Segment* __restrict__ kchan_neg,
+                                  const float* __restrict__ s_keep_f,
+                                  const float* __restrict__ zdot_a,
+                                  const float* __restrict__ zdot_b, float* __restrict__ work,
+                                  unsigned long long* __restrict__ counters) {
+    extern __shared__ unsigned char smem[];
+    const uint64_t n = d.nchans;
+    float* sv        = reinterpret_cast<float*>(smem);           // v = z - zero-DM term
+    uint8_t* state   = reinterpret_cast<uint8_t*>(sv + n);
+    __shared__ unsigned long long cnt[kCountSlots];
+    if (threadIdx.x < kCountSlots)
+        cnt[threadIdx.x] = 0;
+
+    const uint64_t t = blockIdx.x;
+    if (time_flags[t] != 0)
+        return;
+    const uint64_t w  = window_of(t, d.window, d.nwin);
+    const float* lw   = loc + w * n;
+    const float* sw   = scale + w * n;
+    const float* iw   = inv + w * n;
+    const uint8_t* in = raw + t * d.row_bytes;
+    float* out        = work + t * n;
+    const float sk    = s_keep_f[t];
+    const Span32 ksp  = p.kspec ? kspec_pos[t] : Span32{-1, -1};
+    const Span32 ksn  = p.kspec ? kspec_neg[t] : Span32{-1, -1};
+    auto span_has     = [](const Span32& s, uint64_t c) {
+        return s.lo >= 0 && static_cast<int32_t>(c) >= s.lo && static_cast<int32_t>(c) <= s.hi;
+    };
+    auto seg_has = [](const Segment& s, uint64_t tt) {
+        const int64_t i = static_cast<int64_t>(tt);
+        return i >= s.start && i <= s.end;
+    };
+
+    for (uint64_t c = threadIdx.x; c < n; c += blockDim.x) {
+        const float x = rd<D>(in, c);
+        uint8_t st;
+        float v = 0.0F;
+        if (mask[c] == 0) {
+            st = kMasked;
+        } else if (iw[c] == 0.0F) {
+            st = kUnmeasured;
+            out[c] = x;
+        } else {
+            const float z = (x - lw[c]) * iw[c];
+            if (p.narrow_active && fabsf(z) > p.clip) {
+                st = kNarrow;
+            } else if (p.kspec && (span_has(ksp, c) || span_has(ksn, c))) {
+                st = kKadaneSpectrum;
+            } else if (p.kchan && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
+                st = kKadaneChannel;
+            } else {
+                st = kClean;
+                float term = 0.0F;
+                if (p.zero_dm == FROST_ZERO_DM_SUBTRACT)
+                    term = sk;
+                else if (p.zero_dm == FROST_ZERO_DM_ZDOT)
+                    term = (zdot_a[c] * sk) + zdot_b[c];
+                v      = z - term;
+                out[c] = p.transform ? level_of(p, lw[c], sw[c], v) : x;
+            }
+        }
+        state[c] = st;
+        sv[c]    = v;
+    }
+    __syncthreads();
+
+    unsigned long long narrow = 0, nks = 0, nkc = 0, fallbacks = 0;
+    for (uint64_t c = threadIdx.x; c < n; c += blockDim.x) {
+        const uint8_t st = state[c];
+        if (st == kClean || st == kUnmeasured || st == kMasked)
+            continue;
+        if (st == kNarrow)
+            ++narrow;
+        else if (st == kKadaneSpectrum)
+            ++nks;
+        else
+            ++nkc;
+        if (!p.neighbour) {
+            const float v = p.noise ? normal_deviate(draw(p, kStreamNoise, t, c, 0)) : 0.0F;
+            out[c]        = level_of(p, lw[c], sw[c], v);
+            continue;
+        }
+        const uint64_t r  = p.chan_fill_radius;
+        const uint64_t lo = c > r ? c - r : 0;
+        const uint64_t hi = (c + r < n - 1) ? c + r : n - 1;
+        float value       = 0.0F;
+        bool found        = false;
+        for (int a = 0; a < kMaxDraws && !found; ++a) {
+            const uint64_t src = uniform_index(draw(p, kStreamCell, t, c, a), lo, hi);
+            if (state[src] == kClean) {
+                value = sv[src];
+                found = true;
+            }
+        }
+        fallbacks += found ? 0 : 1;
+        out[c] = level_of(p, lw[c], sw[c], value);
+    }
+    if (narrow | nks | nkc | fallbacks) {
+        atomicAdd(&cnt[kCountNarrow], narrow);
+        atomicAdd(&cnt[kCountKspec], nks);
+        atomicAdd(&cnt[kCountKchan], nkc);
+        atomicAdd(&cnt[kCountFallback], fallbacks);
+    }
+    __syncthreads();
+    if (threadIdx.x < kCountSlots && cnt[threadIdx.x] != 0)
+        atomicAdd(&counters[threadIdx.x], cnt[threadIdx.x]);
+}
+
+// Flagged rows (lib/cpu/rfi_cpu.cpp:626-715): each copies, per channel,
+// from a random unflagged row within the time-fill radius (already final),
+// or rebuilds the spectrum in noise units and removes its band mean when a
+// zero-DM transform is on. The band-mean sum keeps channel order.
+__global__ void k_apply_flagged(Dims d, ApplyParams p, const uint64_t* __restrict__ flagged,
+                                const float* __restrict__ loc, const float* __restrict__ scale,
+                                const float* __restrict__ inv, const uint8_t* __restrict__ mask,
+                                const uint8_t* __restrict__ time_flags, float* __restrict__ work,
+                                unsigned long long* __restrict__ counters) {
+    extern __shared__ unsigned char smem[];
+    const uint64_t n  = d.nchans;
+    float* sv         = reinterpret_cast<float*>(smem);
+    uint8_t* contrib  = reinterpret_cast<uint8_t*>(sv + n);
+    __shared__ float s_mean;
+    __shared__ unsigned long long s_fallbacks;
+    if (threadIdx.x == 0)
+        s_fallbacks = 0;
+    __syncthreads();
+    const uint64_t t  = flagged[blockIdx.x];
+    const uint64_t w  = window_of(t, d.window, d.nwin);
+    const uint64_t r  = p.time_fill_radius;
+    const uint64_t lo = t > r ? t - r : 0;
+    const uint64_t hi = (t + r < d.nsamps - 1) ? t + r : d.nsamps - 1;
+    const bool rezero = p.zero_dm != FROST_ZERO_DM_OFF;
+    float* out        = work + t * n;
+    unsigned long long fallbacks = 0;
+
+    for (uint64_t c = threadIdx.x; c < n; c += blockDim.x) {
+        contrib[c] = 0;
+        sv[c]      = 0.0F;
+        if (mask[c] == 0)
+            continue;
+        float v = 0.0F;
+        if (!p.neighbour) {
+            v = p.noise ? normal_deviate(draw(p, kStreamNoise, t, c, 0)) : 0.0F;
+        } else {
+            bool found = false;
+            for (int a = 0; a < kMaxDraws && !found; ++a) {
+                const uint64_t src = uniform_index(draw(p, kStreamTime, t, c, a), lo, hi);
+                if (time_flags[src] != 0)
+                    continue;
+                found = true;
+                const float sval = work[src * n + c];
+                if (rezero) {
+                    const uint64_t ws = window_of(src, d.window, d.nwin);
+                    v = p.equalize ? (sval - p.eq_loc) / p.eq_scale
+                                   : (sval - loc[ws * n + c]) * inv[ws * n + c];
+                } else {
+                    out[c] = sval;
+                }
+            }
+            if (!found)
+                ++fallbacks;
+            if (found && !rezero)
+                continue;
+        }
+        sv[c] = v;
+        if (rezero) {
+            contrib[c] = inv[w * n + c] != 0.0F ? 1 : 0;
+        } else {
+            out[c] = level_of(p, loc[w * n + c], scale[w * n + c], v);
+        }
+    }
+    if (fallbacks)
+        atomicAdd(&s_fallbacks, fallbacks);
+    __syncthreads();
+    if (rezero) {
+        if (threadIdx.x == 0) {
+            double sum = 0.0, count = 0.0;
+            for (uint64_t c = 0; c < n; ++c) {
+                if (contrib[c]) {
+                    sum += sv[c];
+                    count += 1.0;
+                }
+            }
+            s_mean = static_cast<float>(count > 0.0 ? sum / count : 0.0);
+        }
+        __syncthreads();
+        // Float samples: quantisation is the identity, so the carried
+        // rounding error of lib/cpu/rfi_cpu.cpp:704-713 stays +0.
+        for (uint64_t c = threadIdx.x; c < n; c += blockDim.x) {
+            if (mask[c] == 0)
+                continue;
+            out[c] = level_of(p, loc[w * n + c], scale[w * n + c], sv[c] - s_mean) + 0.0F;
+        }
+    }
+    if (threadIdx.x == 0 && s_fallbacks)
+        atomicAdd(&counters[kCountFallback], s_fallbacks);
+}
+
+// ---- re-measure and normalise ---------------------------------------------
+
+template <int D>
+__global__ void k_unpack(Dims d, const uint8_t* __restrict__ raw, float* __restrict__ work) {
+    const uint64_t i      = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t total  = d.nsamps * d.nchans;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t j = i; j < total; j += stride) {
+        const uint64_t t = j / d.nchans, c = j % d.nchans;
+        work[j]          = rd<D>(raw + t * d.row_bytes, c);
+    }
+}
+
+__global__ void k_welford(Dims d, const float* __restrict__ work, float* __restrict__ loc,
+                          float* __restrict__ scale) {
+    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t w = blockIdx.y;
+    if (c >= d.nchans)
+        return;
+    const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
+    double mean = 0.0, var = 0.0;
+    for (uint64_t t = b; t < e; ++t) {
+        const double x     = work[t * d.nchans + c];
+        const double delta = x - mean;
+        mean += delta / static_cast<double>(t - b + 1);
+        var += delta * (x - mean);
+    }
+    loc[w * d.nchans + c]   = static_cast<float>(mean);
+    scale[w * d.nchans + c] = e > b ? static_cast<float>(sqrt(var / static_cast<double>(e - b))) : 0.0F;
+}
+
+constexpr int kTile = 32;
+
+__global__ void k_normalize(Dims d, const float* __restrict__ work, const float* __restrict__ loc,
+                            const float* __restrict__ scale, const uint8_t* __restrict__ mask,
+                            int flip, uint64_t capacity, float* __restrict__ out) {
+    __shared__ float tile[kTile][kTile + 1];
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kTile;
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.y) * kTile;
+    const uint64_t n  = d.nchans;
+    // Load [t][c] tile, already normalised.
+    for (int k = threadIdx.y; k < kTile; k += blockDim.y) {
+        const uint64_t t = t0 + k, c = c0 + threadIdx.x;
+        float v          = 0.0F;
+        if (t < d.nsamps && c < n && mask[c] != 0) {
+            const uint64_t i = window_of(t, d.window, d.nwin) * n + c;
+            const float s    = scale[i] > 0.0F ? 1.0F / scale[i] : 1.0F;
+            v                = (work[t * n + c] - loc[i]) * s;
+        }
+        tile[k][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < kTile; k += blockDim.y) {
+        const uint64_t c = c0 + k, t = t0 + threadIdx.x;
+        if (c < n && t < capacity) {
+            const uint64_t dst     = flip ? n - 1 - c : c;
+            out[dst * capacity + t] = tile[threadIdx.x][k];
+        }
+    }
+}
+
+__global__ void k_normalize_short(Dims d, ApplyParams p, const float* __restrict__ work,
+                                  const float* __restrict__ tl, const float* __restrict__ ts,
+                                  const float* __restrict__ tol, const float* __restrict__ tos,
+                                  const uint8_t* __restrict__ mask, const float* __restrict__ za,
+                                  const float* __restrict__ zb, int flip, uint64_t capacity,
+                                  float* __restrict__ out) {
+    extern __shared__ unsigned char smem[];
+    const uint64_t n = d.nchans;
+    float* z         = reinterpret_cast<float*>(smem);
+    __shared__ float band_mean;
+    const uint64_t t = blockIdx.x;
+    for (uint64_t c = threadIdx.x; c < n; c += blockDim.x)
+        z[c] = (work[t * n + c] - tl[c]) * (ts[c] > 0.0F ? 1.0F / ts[c] : 1.0F);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum     = 0.0;
+        uint64_t count = 0;
+        for (uint64_t c = 0; c < n; ++c) {
+            if (mask[c] && ts[c] > 0.0F && fabsf(z[c]) <= p.clip) {
+                sum += z[c];
+                ++count;
+            }
+        }
+        band_mean = count ? static_cast<float>(sum / static_cast<double>(count)) : 0.0F;
+    }
+    __syncthreads();
+    for (uint64_t c = threadIdx.x; c < n; c += blockDim.x) {
+        if (!mask[c])
+            continue;
+        float term = 0.0F;
+        if (p.zero_dm == FROST_ZERO_DM_SUBTRACT)
+            term = band_mean;
+        else if (p.zero_dm == FROST_ZERO_DM_ZDOT)
+            term = za[c] * band_mean + zb[c];
+        const float x = work[t * n + c];
+        const float transformed = ts[c] <= 0.0F ? x
+                                  : p.equalize  ? p.eq_loc + p.eq_scale * (z[c] - term)
+                                  : p.transform ? tl[c] + ts[c] * (z[c] - term)
+                                                : x;
+        const float s      = tos[c] > 0.0F ? 1.0F / tos[c] : 1.0F;
+        const uint64_t dst = flip ? n - 1 - c : c;
+        out[dst * capacity + t] = (transformed - tol[c]) * s;
+    }
+}
+
+unsigned grid1(uint64_t n, unsigned block) { return static_cast<unsigned>((n + block - 1) / block); }
+
+} // namespace
+
+// ---- launchers ----------------------------------------------------------------
+
+void launch_check_finite(const uint8_t* raw, uint64_t nwords, unsigned long long* first_bad,
+                         cudaStream_t s) {
+    if (nwords == 0)
+        return;
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((nwords + 255) / 256, 148 * 16));
+    k_check_finite<<<blocks, 256, 0, s>>>(reinterpret_cast<const uint32_t*>(raw), nwords, first_bad);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_sample_rows(const Dims& d, const uint8_t* raw, float* samples, cudaStream_t s) {
+    const dim3 grid(grid1(d.nchans, 128), kMaxBandpassRows, static_cast<unsigned>(d.nwin));
+    FB_DISPATCH(d.dtype, k_sample_rows<D><<<grid, 128, 0, s>>>(d, raw, samples));
+    FB_LAUNCH_CHECK();
+}
+
+void launch_bandpass(const Dims& d, const float* samples, float* loc, float* scale, float* inv,
+                     uint32_t* unmeasured, cudaStream_t s) {
+    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
+    k_bandpass<<<grid, 64, 0, s>>>(d, samples, loc, scale, inv, unmeasured);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_moments(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
+                    const uint8_t* static_mask, float clip, MomentSums* out, cudaStream_t s) {
+    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
+    FB_DISPATCH(d.dtype, k_moments<D><<<grid, 64, 0, s>>>(d, raw, loc, inv, static_mask, clip, out));
+    FB_LAUNCH_CHECK();
+}
+
+void launch_scan_rows(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
+                      const uint8_t* mask, float clip, const KspecParams& kp,
+                      const uint64_t* good_prefix, float* s_det, double* s_keep_d, float* s_keep_f,
+                      float* row_std, Span32* kspec_pos, Span32* kspec_neg, uint8_t* kspec_whole,
+                      cudaStream_t s) {
+    const unsigned grid = grid1(d.nsamps, kScanRows);
+    FB_DISPATCH(d.dtype, k_scan_rows<D><<<grid, kScanRows, 0, s>>>(
+                             d, raw, loc, inv, mask, clip, kp, good_prefix, s_det, s_keep_d,
+                             s_keep_f, row_std, kspec_pos, kspec_neg, kspec_whole));
+    FB_LAUNCH_CHECK();
+}
+
+void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
+                      const uint8_t* mask, float clip, const double* s_keep_d, int zdot, int kchan,
+                      const float* clip_mean, const float* clip_inv_std, float* chunk_min,
+                      float* chunk_max, ZdotSums* chunk_zdot, KadaneState* chunk_kpos,
+                      KadaneState* chunk_kneg, float* lo, float* hi, ZdotSums* zdot_sum,
+                      Run* kpos_best, Run* kneg_best, cudaStream_t s) {
+    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nchunks));
+    FB_DISPATCH(d.dtype, k_scan_cols<D><<<grid, 64, 0, s>>>(
+                             d, raw, loc, inv, mask, clip, s_keep_d, zdot, kchan, clip_mean,
+                             clip_inv_std, chunk_min, chunk_max, chunk_zdot, chunk_kpos,
+                             chunk_kneg));
+    FB_LAUNCH_CHECK();
+    k_combine_chunks<<<grid1(d.nchans, 128), 128, 0, s>>>(d, zdot, kchan, chunk_min, chunk_max,
+                                                          chunk_zdot, chunk_kpos, chunk_kneg, lo,
+                                                          hi, zdot_sum, kpos_best, kneg_best);
+    FB_LAUNCH_CHECK();
+}
+
+static void set_smem(const void* fn, size_t bytes) {
+    if (bytes > 48 * 1024)
+        FB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(bytes)));
+}
+
+void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* raw,
+                            const float* loc, const float* scale, const float* inv,
+                            const uint8_t* mask, const uint8_t* time_flags, const Span32* kspec_pos,
+                            const Span32* kspec_neg, const Segment* kchan_pos,
+                            const Segment* kchan_neg, const float* s_keep_f, const float* zdot_a,
+                            const float* zdot_b, float* work, unsigned long long* counters,
+                            cudaStream_t s) {
+    const size_t smem = d.nchans * (sizeof(float) + 1);
+    if (d.nsamps == 0)
+        return;
+    FB_DISPATCH(d.dtype, {
+        set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D>), smem);
+        k_apply_unflagged<D><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
+            d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
+            kchan_neg, s_keep_f, zdot_a, zdot_b, work, counters);
+    });
+    FB_LAUNCH_CHECK();
+}
+
+void launch_apply_flagged(const Dims& d, const ApplyParams& p, const uint64_t* flagged,
+                          uint64_t nflagged, const float* loc, const float* scale,
+                          const float* inv, const uint8_t* mask, const uint8_t* time_flags,
+                          float* work, unsigned long long* counters, cudaStream_t s) {
+    if (nflagged == 0)
+        return;
+    const size_t smem = d.nchans * (sizeof(float) + 1);
+    set_smem(reinterpret_cast<const void*>(&k_apply_flagged), smem);
+    k_apply_flagged<<<static_cast<unsigned>(nflagged), 256, smem, s>>>(
+        d, p, flagged, loc, scale, inv, mask, time_flags, work, counters);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_unpack(const Dims& d, const uint8_t* raw, float* work, cudaStream_t s) {
+    const uint64_t total = d.nsamps * d.nchans;
+    if (total == 0)
+        return;
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((total + 255) / 256, 148 * 32));
+    FB_DISPATCH(d.dtype, k_unpack<D><<<blocks, 256, 0, s>>>(d, raw, work));
+    FB_LAUNCH_CHECK();
+}
+
+void launch_welford(const Dims& d, const float* work, float* loc, float* scale, cudaStream_t s) {
+    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
+    k_welford<<<grid, 64, 0, s>>>(d, work, loc, scale);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_normalize(const Dims& d, const float* work, const float* loc, const float* scale,
+                      const uint8_t* mask, int flip, uint64_t capacity, float* out, cudaStream_t s) {
+    const dim3 grid(grid1(capacity, kTile), grid1(d.nchans, kTile));
+    k_normalize<<<grid, dim3(kTile, 8), 0, s>>>(d, work, loc, scale, mask, flip, capacity, out);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_normalize_short(const Dims& d, const ApplyParams& p, const float* work,
+                            const float* tail_loc, const float* tail_scale,
+                            const float* tail_out_loc, const float* tail_out_scale,
+                            const uint8_t* mask, const float* zdot_a, const float* zdot_b,
+                            int flip, uint64_t capacity, float* out, cudaStream_t s) {
+    if (d.nsamps == 0)
+        return;
+    const size_t smem = d.nchans * sizeof(float);
+    set_smem(reinterpret_cast<const void*>(&k_normalize_short), smem);
+    k_normalize_short<<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
+        d, p, work, tail_loc, tail_scale, tail_out_loc, tail_out_scale, mask, zdot_a, zdot_b, flip,
+        capacity, out);
+    FB_LAUNCH_CHECK();
+}
+
+} // namespace fb::rfi

@@ -1,0 +1,269 @@
+/*
+ * frost_b200 — C ABI of the B200 (sm_100a) per-gulp search path of frost:
+ * RFI excision and normalisation, the DM trial grid, and the streaming
+ * FDMT + boxcar/trapezoid search with exact noise.
+ *
+ * Plain C types only: no C++ or torch types cross this boundary. Every entry
+ * point returns an int status (FROST_OK == 0, negative on failure) and never
+ * throws; frost_last_error() gives the calling thread's last message.
+ * Arguments are validated before any state changes. Handles own their device
+ * buffers; device pointers they return stay valid until the next call on the
+ * same handle. A NULL stream argument selects the handle's own stream.
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * file:line within pravirkr/frost.
+ */
+#ifndef FROST_B200_H
+#define FROST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status --------------------------------------------------------- */
+
+/* Status codes. The C++ wrapper maps INVALID_ARGUMENT to
+ * std::invalid_argument and the rest to std::runtime_error, as frost's
+ * FROST_CUDA_CHECK does (lib/cuda/gpu_utils.cuh:13-20). */
+enum frost_status {
+    FROST_OK                   = 0,
+    FROST_ERR_INVALID_ARGUMENT = -1,
+    FROST_ERR_OUT_OF_MEMORY    = -2,
+    FROST_ERR_DEVICE           = -3,
+    FROST_ERR_TIMEOUT          = -4,
+    FROST_ERR_STATE            = -5,
+    FROST_ERR_OVERFLOW         = -6,
+    FROST_ERR_IO               = -7,
+    FROST_ERR_INTERNAL         = -8
+};
+
+/* Message of the calling thread's last failing call ("" if none). */
+const char* frost_last_error(void);
+
+/* Library version string. */
+const char* frost_version(void);
+
+/* ---- common types (include/frost/common/policies.hpp:52-60) ---------- */
+
+enum frost_dtype {
+    FROST_UINT1   = 0,
+    FROST_UINT2   = 1,
+    FROST_UINT4   = 2,
+    FROST_UINT8   = 3,
+    FROST_UINT16  = 4,
+    FROST_UINT32  = 5,
+    FROST_FLOAT32 = 6
+};
+
+/* Inclusive channel range (include/frost/prepare/rfi.hpp:14-18). */
+typedef struct {
+    uint64_t start;
+    uint64_t end;
+} frost_channel_range;
+
+/* Inclusive frequency range in MHz (include/frost/prepare/rfi.hpp:21-25). */
+typedef struct {
+    double lo;
+    double hi;
+} frost_frequency_range;
+
+/* ---- RFI excision (include/frost/prepare/rfi.hpp) -------------------- */
+
+enum frost_fill_mode { FROST_FILL_NEIGHBOUR = 0, FROST_FILL_MEAN = 1, FROST_FILL_NOISE = 2 };
+enum frost_zero_dm { FROST_ZERO_DM_OFF = 0, FROST_ZERO_DM_SUBTRACT = 1, FROST_ZERO_DM_ZDOT = 2 };
+
+/* Flat form of RfiConfig (include/frost/prepare/rfi.hpp:167-191) with
+ * every strategy's switch and thresholds. frost_rfi_config_default() gives
+ * the reference defaults (narrow + broad, neighbour fill). Arrays are
+ * borrowed for the duration of the create call only. */
+typedef struct {
+    const frost_channel_range* zap_chans;
+    uint64_t n_zap_chans;
+    const frost_frequency_range* zap_freqs;
+    uint64_t n_zap_freqs;
+    int32_t narrow_enabled;
+    float narrow_threshold;
+    int32_t broad_enabled;
+    float broad_threshold;
+    uint64_t broad_boxcar_max;
+    int32_t dropout_enabled;
+    float dropout_min_std_fraction;
+    int32_t moments_enabled;
+    float moments_threshold;
+    int32_t moments_mean;
+    int32_t moments_std;
+    int32_t moments_skewness;
+    int32_t moments_kurtosis;
+    int32_t moments_autocorr;
+    float moments_kurtosis_max;
+    int32_t iqrm_enabled;
+    float iqrm_threshold;
+    uint64_t iqrm_radius;
+    uint64_t mask_grow;
+    int32_t kadane_channel_enabled;
+    float kadane_channel_threshold;
+    float kadane_channel_min_duration;
+    int32_t kadane_spectrum_enabled;
+    float kadane_spectrum_threshold;
+    float kadane_spectrum_min_bandwidth;
+    float kadane_spectrum_whole_band_fraction;
+    int32_t zero_dm;  /* enum frost_zero_dm */
+    int32_t equalize;
+    int32_t fill;     /* enum frost_fill_mode */
+    uint64_t seed;
+} frost_rfi_config;
+
+/* BlockLayout (include/frost/prepare/rfi.hpp:194-201). */
+typedef struct {
+    uint64_t nchans;
+    uint64_t max_nsamps;
+    int32_t dtype; /* enum frost_dtype */
+    double tsamp;  /* seconds */
+    double f0;     /* centre frequency of channel 0, MHz */
+    double df;     /* channel spacing, MHz, may be negative */
+} frost_block_layout;
+
+/* RfiReport (include/frost/prepare/rfi.hpp:204-227). Stage times are
+ * device (CUDA event) seconds. */
+typedef struct {
+    int32_t calibration_reused;
+    uint64_t nsamps;
+    uint64_t chans_zapped;
+    uint64_t chans_dead;
+    uint64_t chans_moments;
+    uint64_t chans_iqrm;
+    uint64_t chans_grown;
+    uint64_t chans_masked;
+    uint64_t samps_broad;
+    uint64_t samps_dropout;
+    uint64_t samps_kadane;
+    uint64_t samps_flagged;
+    uint64_t cells_narrow;
+    uint64_t cells_kadane_spectrum;
+    uint64_t cells_kadane_channel;
+    uint64_t fill_fallbacks;
+    double t_bandpass;
+    double t_moments;
+    double t_scan;
+    double t_flags;
+    double t_apply;
+} frost_rfi_report;
+
+/* Opaque RFICleaner handle (include/frost/prepare/rfi.hpp:243-297). */
+typedef struct frost_rfi frost_rfi;
+
+/* Fills `cfg` with RfiConfig's defaults (include/frost/prepare/rfi.hpp:167-191). */
+void frost_rfi_config_default(frost_rfi_config* cfg);
+
+/* RfiConfig::validate (lib/prepare/rfi_config.cpp:14-77). */
+int frost_rfi_config_validate(const frost_rfi_config* cfg);
+
+/* RFICleaner(RfiConfig, BlockLayout, baseline_length)
+ * (include/frost/prepare/rfi.hpp:250-254, lib/cpu/rfi_cpu.cpp:24-60).
+ * Validates configuration and geometry (lib/prepare/rfi_config.cpp:79-110)
+ * before allocating device workspace on `device`. */
+int frost_rfi_create(const frost_rfi_config* cfg,
+                     const frost_block_layout* layout,
+                     float baseline_length,
+                     int device,
+                     frost_rfi** out);
+
+int frost_rfi_destroy(frost_rfi* rfi);
+
+/* RFICleaner::execute_normalized (include/frost/prepare/rfi.hpp:266-282,
+ * lib/cpu/rfi_cpu.cpp:161-260): cleans the packed time-major block in float
+ * precision on the GPU and writes calibrated float32 in [channel][time]
+ * order, low frequency first, `capacity = block_bytes / row_bytes` samples
+ * per channel, masked channels and padding zero. `block` is host memory
+ * (copied to the device inside the call) when `block_on_device` is 0, else a
+ * device pointer. `nsamps` = 0 uses every row. The device result is returned
+ * in `*out_device` (valid until the next call); the call does not
+ * synchronise the stream except to read back the small per-gulp statistics
+ * the flag logic needs. */
+int frost_rfi_execute_normalized(frost_rfi* rfi,
+                                 const uint8_t* block,
+                                 size_t block_bytes,
+                                 size_t nsamps,
+                                 int block_on_device,
+                                 void* stream,
+                                 const float** out_device);
+
+/* Copies the last normalized waterfall ([nchans][capacity] floats) to host
+ * memory; synchronises the stream. */
+int frost_rfi_download_normalized(frost_rfi* rfi, float* host, size_t count);
+
+/* RFICleaner::channel_mask (include/frost/prepare/rfi.hpp:284-287). */
+int frost_rfi_channel_mask(const frost_rfi* rfi, uint8_t* out, size_t nchans);
+
+/* RFICleaner::report (include/frost/prepare/rfi.hpp:289). */
+int frost_rfi_get_report(const frost_rfi* rfi, frost_rfi_report* out);
+
+/* Per-sample time flags of the last full block (1 = flagged), as built by
+ * RFICleaner::Impl::build_flags (lib/cpu/rfi_cpu.cpp:347-468). */
+int frost_rfi_time_flags(const frost_rfi* rfi, uint8_t* out, size_t nsamps);
+
+/* RFICleaner::memory_usage (include/frost/prepare/rfi.hpp:291): device bytes. */
+int frost_rfi_memory_usage(const frost_rfi* rfi, size_t* bytes);
+
+/* IQRM channel mask (include/frost/prepare/rfi.hpp:56-59,
+ * lib/cpu/rfi_masks_cpu.cpp:29-122) on an n-channel host statistic.
+ * `ignore` may be NULL. Writes n flags (1 = flagged) to host `out`. */
+int frost_iqrm_mask(const float* x,
+                    size_t n,
+                    uint64_t radius,
+                    float threshold,
+                    const uint8_t* ignore,
+                    uint8_t* out);
+
+/* apply_manual_killmask (include/frost/prepare/rfi.hpp:48-49,
+ * lib/cpu/rfi_masks_cpu.cpp:16-27). */
+int frost_apply_manual_killmask(uint8_t* killmask,
+                                size_t nchans,
+                                const frost_channel_range* zaps,
+                                size_t nzaps);
+
+/* read_kill_file (include/frost/prepare/rfi.hpp:40-41,
+ * lib/prepare/kill_file.cpp:15-65). Writes merged inclusive ranges. */
+int frost_read_kill_file(const char* path,
+                         size_t nchans,
+                         frost_channel_range* out,
+                         size_t capacity,
+                         size_t* count);
+
+/* ---- dedispersion plan (include/frost/dedisp/dedisp.hpp) ------------- */
+
+/* DedispPlanConfig (include/frost/dedisp/dedisp.hpp:12-27). */
+typedef struct {
+    uint64_t nchans;
+    float dt;             /* seconds */
+    float f0;             /* MHz, channel 0 */
+    float df;             /* MHz, may be negative */
+    float dm_min;
+    float dm_max;
+    float dm_pulse_width; /* microseconds */
+    float dm_tol;
+    int32_t dm_dtype;     /* enum frost_dtype of the DM-time output */
+    uint64_t block_nsamps;
+    uint64_t subband_depth;
+} frost_dedisp_plan_config;
+
+/* generate_dm_list (include/frost/dedisp/dedisp.hpp:29-30,
+ * lib/dedisp/dedisp.cpp:16-69). With out == NULL only *count is set. */
+int frost_generate_dm_list(const frost_dedisp_plan_config* cfg,
+                           float* out,
+                           size_t capacity,
+                           size_t* count);
+
+/* Ascending band edges of make_dmt_fdmt_plan (lib/dedisp/dedisp.cpp:71-89). */
+int frost_fdmt_band_edges(const frost_dedisp_plan_config* cfg,
+                          float* f_min,
+                          float* f_max);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* FROST_B200_H */
