@@ -119,6 +119,74 @@ class RfiReportC(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class BoxcarConfigC(C.Structure):
+    _fields_ = [
+        ("max_boxcar", C.c_uint64),
+        ("wtsp", C.c_float),
+        ("use_trapezoid", C.c_int32),
+        ("detect_thresh", C.c_float),
+        ("noise_sigma", C.c_float),
+        ("peak_mode", C.c_int32),
+        ("max_candidates", C.c_uint64),
+        ("max_cands_per_dm", C.c_uint64),
+        ("skip_cold_prefix", C.c_int32),
+        ("input_nbits", C.c_int32),
+        ("input_mean", C.c_float),
+        ("storage", C.c_int32),
+        ("tile_nsamps", C.c_uint64),
+    ]
+
+
+class CandidateC(C.Structure):
+    _fields_ = [
+        ("peak_sample", C.c_uint64),
+        ("begin_sample", C.c_uint64),
+        ("end_sample", C.c_uint64),
+        ("snr", C.c_float),
+        ("dm", C.c_float),
+        ("f_low_mhz", C.c_float),
+        ("f_high_mhz", C.c_float),
+        ("filter_idx", C.c_uint32),
+        ("width", C.c_uint32),
+        ("dm_idx", C.c_uint32),
+        ("chan_begin", C.c_uint32),
+        ("chan_end", C.c_uint32),
+        ("beam_idx", C.c_uint32),
+        ("subband_level", C.c_uint32),
+        ("subband_idx", C.c_uint32),
+    ]
+
+
+class SearchInfoC(C.Structure):
+    _fields_ = [
+        ("nchans", C.c_uint64),
+        ("block_nsamps", C.c_uint64),
+        ("tile_nsamps", C.c_uint64),
+        ("dt_max", C.c_uint64),
+        ("ndm", C.c_uint64),
+        ("nplanes", C.c_uint64),
+        ("nwidths", C.c_uint64),
+        ("levels", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("f_min", C.c_double),
+        ("f_max", C.c_double),
+    ]
+
+
+class SearchPlaneC(C.Structure):
+    _fields_ = [
+        ("subband_level", C.c_uint32),
+        ("subband_idx", C.c_uint32),
+        ("level", C.c_uint32),
+        ("chan_begin", C.c_uint32),
+        ("chan_end", C.c_uint32),
+        ("staggered", C.c_uint32),
+        ("ndm", C.c_uint64),
+        ("f_low", C.c_double),
+        ("f_high", C.c_double),
+    ]
+
+
 class DedispPlanConfigC(C.Structure):
     _fields_ = [
         ("nchans", C.c_uint64),

@@ -46,6 +46,21 @@ SIGNATURES = {
                                        C.POINTER(_sz)]),
     "frost_generate_dm_list": (C.c_int, [C.POINTER(_abi.DedispPlanConfigC), _f32p, _sz, C.POINTER(_sz)]),
     "frost_fdmt_band_edges": (C.c_int, [C.POINTER(_abi.DedispPlanConfigC), _f32p, _f32p]),
+    "frost_search_create": (C.c_int, [C.POINTER(_abi.DedispPlanConfigC), C.POINTER(_abi.BoxcarConfigC),
+                                      _u8p, _sz, C.c_int, C.POINTER(_vp)]),
+    "frost_search_destroy": (C.c_int, [_vp]),
+    "frost_search_execute": (C.c_int, [_vp, _f32p, _sz, C.c_int, _u8p, _vp]),
+    "frost_search_drain": (C.c_int, [_vp]),
+    "frost_search_result_count": (C.c_int, [_vp, C.POINTER(_sz), C.POINTER(_u64), C.POINTER(_u64)]),
+    "frost_search_results": (C.c_int, [_vp, C.POINTER(_abi.CandidateC), _sz, C.POINTER(_sz)]),
+    "frost_search_frontier": (C.c_int, [_vp, C.POINTER(_u64)]),
+    "frost_search_get_info": (C.c_int, [_vp, C.POINTER(_abi.SearchInfoC)]),
+    "frost_search_plane_info": (C.c_int, [_vp, _sz, C.POINTER(_abi.SearchPlaneC), _f32p,
+                                          C.POINTER(C.c_uint32)]),
+    "frost_search_widths": (C.c_int, [_vp, C.POINTER(C.c_uint32), _sz, C.POINTER(_sz)]),
+    "frost_search_variance_grid": (C.c_int, [_vp, _sz, C.c_uint32, _u8p, C.POINTER(C.c_double), _sz]),
+    "frost_search_capture_planes": (C.c_int, [_vp, C.c_int]),
+    "frost_search_plane_data": (C.c_int, [_vp, _sz, _f32p, _sz]),
 }
 
 

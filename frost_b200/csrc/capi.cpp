@@ -11,6 +11,7 @@
 #include "dedisp.hpp"
 #include "host_stats.hpp"
 #include "rfi_cleaner.hpp"
+#include "search_engine.hpp"
 
 namespace fb {
 
@@ -56,6 +57,11 @@ template <class F> int guarded(F&& f) {
 struct frost_rfi {
     fb::rfi::Cleaner impl;
     template <class... A> explicit frost_rfi(A&&... a) : impl(std::forward<A>(a)...) {}
+};
+
+struct frost_search {
+    fb::fdmt::Engine impl;
+    template <class... A> explicit frost_search(A&&... a) : impl(std::forward<A>(a)...) {}
 };
 
 using fb::guarded;
@@ -218,6 +224,159 @@ int frost_fdmt_band_edges(const frost_dedisp_plan_config* cfg, float* f_min, flo
         if (cfg == nullptr || f_min == nullptr || f_max == nullptr)
             invalid("frost_fdmt_band_edges: null argument");
         fb::dedisp::band_edges(*cfg, *f_min, *f_max);
+    });
+}
+
+} // extern "C"
+
+extern "C" {
+
+int frost_search_create(const frost_dedisp_plan_config* plan, const frost_boxcar_config* cfg,
+                        const uint8_t* kill_mask, size_t memory_budget, int device,
+                        frost_search** out) {
+    return guarded([&] {
+        if (plan == nullptr || cfg == nullptr || out == nullptr)
+            invalid("frost_search_create: null argument");
+        *out = nullptr;
+        *out = new frost_search(*plan, *cfg, kill_mask, memory_budget, device);
+    });
+}
+
+int frost_search_destroy(frost_search* s) {
+    return guarded([&] { delete s; });
+}
+
+int frost_search_execute(frost_search* s, const float* waterfall, size_t nsamps, int on_device,
+                         const uint8_t* mask, void* stream) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_execute: null handle");
+        s->impl.execute(waterfall, nsamps, on_device != 0, mask, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int frost_search_drain(frost_search* s) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_drain: null handle");
+        s->impl.drain();
+    });
+}
+
+int frost_search_result_count(const frost_search* s, size_t* count, uint64_t* dropped_global,
+                              uint64_t* dropped_per_dm) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_result_count: null handle");
+        if (count != nullptr)
+            *count = s->impl.results().size();
+        if (dropped_global != nullptr)
+            *dropped_global = s->impl.dropped_global();
+        if (dropped_per_dm != nullptr)
+            *dropped_per_dm = s->impl.dropped_per_dm();
+    });
+}
+
+int frost_search_results(const frost_search* s, frost_candidate* out, size_t capacity,
+                         size_t* count) {
+    return guarded([&] {
+        if (s == nullptr || count == nullptr)
+            invalid("frost_search_results: null argument");
+        const auto& r = s->impl.results();
+        *count        = r.size();
+        if (out != nullptr) {
+            if (capacity < r.size())
+                invalid("frost_search_results: output holds too few candidates");
+            std::memcpy(out, r.data(), r.size() * sizeof(frost_candidate));
+        }
+    });
+}
+
+int frost_search_frontier(const frost_search* s, uint64_t* sample) {
+    return guarded([&] {
+        if (s == nullptr || sample == nullptr)
+            invalid("frost_search_frontier: null argument");
+        *sample = const_cast<frost_search*>(s)->impl.frontier();
+    });
+}
+
+int frost_search_get_info(const frost_search* s, frost_search_info* out) {
+    return guarded([&] {
+        if (s == nullptr || out == nullptr)
+            invalid("frost_search_get_info: null argument");
+        *out = s->impl.info();
+    });
+}
+
+int frost_search_plane_info(const frost_search* s, size_t plane, frost_search_plane* out,
+                            float* dm_grid, uint32_t* warmup) {
+    return guarded([&] {
+        if (s == nullptr || out == nullptr)
+            invalid("frost_search_plane_info: null argument");
+        const auto& planes = s->impl.plan().planes();
+        if (plane >= planes.size())
+            invalid("frost_search_plane_info: plane index out of range");
+        const auto& p     = planes[plane];
+        out->subband_level = static_cast<uint32_t>(p.subband_level);
+        out->subband_idx   = static_cast<uint32_t>(p.subband_idx);
+        out->level         = static_cast<uint32_t>(p.height);
+        out->chan_begin    = static_cast<uint32_t>(p.chan_begin);
+        out->chan_end      = static_cast<uint32_t>(p.chan_end);
+        out->staggered     = static_cast<uint32_t>(p.staggered);
+        out->ndm           = p.delay.size();
+        out->f_low         = p.f_lo;
+        out->f_high        = p.f_hi;
+        for (size_t i = 0; i < p.delay.size(); ++i) {
+            if (dm_grid != nullptr)
+                dm_grid[i] = p.dm[i];
+            if (warmup != nullptr)
+                warmup[i] = static_cast<uint32_t>(p.delay[i]);
+        }
+    });
+}
+
+int frost_search_widths(const frost_search* s, uint32_t* out, size_t capacity, size_t* count) {
+    return guarded([&] {
+        if (s == nullptr || count == nullptr)
+            invalid("frost_search_widths: null argument");
+        const auto& w = s->impl.plan().widths();
+        *count        = w.size();
+        if (out != nullptr) {
+            if (capacity < w.size())
+                invalid("frost_search_widths: output too small");
+            for (size_t i = 0; i < w.size(); ++i)
+                out[i] = static_cast<uint32_t>(w[i]);
+        }
+    });
+}
+
+int frost_search_variance_grid(const frost_search* s, size_t plane, uint32_t width,
+                               const uint8_t* mask, double* out, size_t capacity) {
+    return guarded([&] {
+        if (s == nullptr || out == nullptr)
+            invalid("frost_search_variance_grid: null argument");
+        if (width == 0)
+            invalid("frost_search_variance_grid: width must be > 0");
+        const auto v = s->impl.variance_grid(plane, width, mask);
+        if (capacity < v.size())
+            invalid("frost_search_variance_grid: output too small");
+        std::memcpy(out, v.data(), v.size() * sizeof(double));
+    });
+}
+
+int frost_search_capture_planes(frost_search* s, int enable) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_capture_planes: null handle");
+        s->impl.capture(enable != 0);
+    });
+}
+
+int frost_search_plane_data(const frost_search* s, size_t plane, float* out, size_t capacity) {
+    return guarded([&] {
+        if (s == nullptr || out == nullptr)
+            invalid("frost_search_plane_data: null argument");
+        s->impl.plane_data(plane, out, capacity);
     });
 }
 

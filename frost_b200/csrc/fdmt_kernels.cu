@@ -1,0 +1,275 @@
+// FDMT level kernels for sm_100a.
+//
+// Every level is one streaming pass: read two child rows, write one parent
+// row, HBM-bound. Level 1 is fused with the leaf initialisation (the
+// per-channel window sums are prefix-sum differences in shared memory), so
+// the ~C * (1 + d) leaf rows are never materialised. Rows live in level
+// buffers with a per-level history prefix (see LevelView), so a shifted read
+// t - d_lo before the tile start lands in the history columns without a
+// branch. The shifted (high-child) row segment of each CTA is staged in
+// shared memory with aligned 16-byte loads; the unshifted row is read
+// directly, coalesced. Storage is float or __half; arithmetic is float.
+
+#include <algorithm>
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "fdmt_kernels.hpp"
+
+namespace fb::fdmt {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPer     = kTimePerCta / kThreads; // 8 samples per thread
+
+template <class S> __device__ __forceinline__ float ld(const S* p);
+template <> __device__ __forceinline__ float ld<float>(const float* p) { return *p; }
+template <> __device__ __forceinline__ float ld<__half>(const __half* p) { return __half2float(*p); }
+
+template <class S> __device__ __forceinline__ void st(S* p, float v);
+template <> __device__ __forceinline__ void st<float>(float* p, float v) { *p = v; }
+template <> __device__ __forceinline__ void st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
+
+// Inclusive block scan of smem[0..n) in place (float), n <= kThreads * 64.
+__device__ void block_scan(float* a, int n) {
+    __shared__ float warp_tot[kThreads / 32];
+    const int per  = (n + kThreads - 1) / kThreads;
+    const int beg  = threadIdx.x * per;
+    const int end  = min(beg + per, n);
+    float run      = 0.0F;
+    for (int i = beg; i < end; ++i) {
+        run += a[i];
+        a[i] = run;
+    }
+    // exclusive scan of the per-thread totals
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float v        = run;
+    for (int o = 1; o < 32; o <<= 1) {
+        const float u = __shfl_up_sync(0xFFFFFFFFU, v, o);
+        if (lane >= o)
+            v += u;
+    }
+    if (lane == 31)
+        warp_tot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        float w = lane < kThreads / 32 ? warp_tot[lane] : 0.0F;
+        for (int o = 1; o < 32; o <<= 1) {
+            const float u = __shfl_up_sync(0xFFFFFFFFU, w, o);
+            if (lane >= o)
+                w += u;
+        }
+        if (lane < kThreads / 32)
+            warp_tot[lane] = w;
+    }
+    __syncthreads();
+    const float offset = (v - run) + (warp > 0 ? warp_tot[warp - 1] : 0.0F);
+    for (int i = beg; i < end; ++i)
+        a[i] += offset;
+    __syncthreads();
+}
+
+template <class S>
+__global__ void __launch_bounds__(kThreads)
+    k_level1(const LeafOp* __restrict__ ops, const int32_t* __restrict__ node_first_op,
+             int32_t H, const float* __restrict__ wf, int64_t wpitch, int64_t t0, int32_t n_valid,
+             const float* __restrict__ hist, int32_t hist_len, S* __restrict__ out,
+             int64_t pitch, int32_t base) {
+    extern __shared__ float smem[];
+    const int32_t node = blockIdx.x;
+    const int32_t op0 = node_first_op[node], op1 = node_first_op[node + 1];
+    const int32_t ca  = ops[op0].chan_lo;
+    const int32_t cb  = ops[op0].chan_hi;
+    const int32_t k0  = blockIdx.y * kTimePerCta;
+    const int32_t N   = kTimePerCta + H + 1;
+    float* Pa         = smem;
+    float* Pb         = smem + N;
+    // x(i) for tile-relative time t = k0 + i - H - 1; x(0) is the scan base.
+    for (int i = threadIdx.x; i < N; i += kThreads) {
+        const int64_t t = static_cast<int64_t>(k0) + i - H - 1;
+        float a = 0.0F, b = 0.0F;
+        if (i > 0) {
+            if (t < 0) {
+                a = hist[static_cast<int64_t>(ca) * hist_len + hist_len + t];
+                if (cb >= 0)
+                    b = hist[static_cast<int64_t>(cb) * hist_len + hist_len + t];
+            } else if (t < n_valid) {
+                a = wf[static_cast<int64_t>(ca) * wpitch + t0 + t];
+                if (cb >= 0)
+                    b = wf[static_cast<int64_t>(cb) * wpitch + t0 + t];
+            }
+        }
+        Pa[i] = a;
+        Pb[i] = b;
+    }
+    __syncthreads();
+    block_scan(Pa, N);
+    if (cb >= 0)
+        block_scan(Pb, N);
+    for (int32_t r = op0; r < op1; ++r) {
+        const LeafOp op = ops[r];
+        S* row          = out + static_cast<int64_t>(r) * pitch + base + k0;
+        for (int j = 0; j < kPer; ++j) {
+            const int k = threadIdx.x + j * kThreads;
+            const int i = k + H + 1;
+            float v     = Pa[i] - Pa[i - op.d_lo - 1];
+            if (cb >= 0)
+                v += Pb[i - op.d_lo] - Pb[i - op.d_lo - op.d_hi - 1];
+            st<S>(row + k, v);
+        }
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(kThreads)
+    k_level(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
+            int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base) {
+    constexpr int VEC = 16 / sizeof(S);
+    __shared__ __align__(16) S stage[kTimePerCta + VEC];
+    const RowOp op = ops[blockIdx.x];
+    const int32_t k0 = blockIdx.y * kTimePerCta;
+    const S* lo = in + static_cast<int64_t>(op.lo_row) * in_pitch + in_base + k0;
+    S* dst      = out + static_cast<int64_t>(blockIdx.x) * out_pitch + out_base + k0;
+    if (op.hi_row < 0) {
+        for (int j = 0; j < kPer; ++j) {
+            const int k = threadIdx.x + j * kThreads;
+            dst[k]      = lo[k];
+        }
+        return;
+    }
+    // Stage hi[k0 - shift, k0 - shift + kTimePerCta) with aligned vectors.
+    const S* hrow    = in + static_cast<int64_t>(op.hi_row) * in_pitch;
+    const int64_t e0 = static_cast<int64_t>(in_base) + k0 - op.shift;
+    const int64_t v0 = e0 / VEC;
+    const int off    = static_cast<int>(e0 - v0 * VEC);
+    const int nvec   = kTimePerCta / VEC + (off > 0 ? 1 : 0);
+    const uint4* src = reinterpret_cast<const uint4*>(hrow) + v0;
+    uint4* sv        = reinterpret_cast<uint4*>(stage);
+    for (int i = threadIdx.x; i < nvec; i += kThreads)
+        sv[i] = src[i];
+    __syncthreads();
+    for (int j = 0; j < kPer; ++j) {
+        const int k = threadIdx.x + j * kThreads;
+        st<S>(dst + k, ld<S>(lo + k) + ld<S>(stage + off + k));
+    }
+}
+
+template <class S>
+__global__ void k_capture(const S* __restrict__ in, int64_t pitch, int32_t base,
+                          const int64_t* __restrict__ rows, float* __restrict__ out,
+                          int64_t out_pitch, int64_t t_off, int32_t n_valid) {
+    const int64_t r = blockIdx.y;
+    const S* src    = in + rows[r] * pitch + base;
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n_valid;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[r * out_pitch + t_off + k] = ld<S>(src + k);
+}
+
+} // namespace
+
+void launch_capture_rows(LevelView v, const int64_t* rows, int64_t nrows, float* out,
+                         int64_t out_pitch, int64_t t_off, int32_t n_valid, cudaStream_t s) {
+    if (nrows == 0 || n_valid <= 0)
+        return;
+    const dim3 grid(static_cast<unsigned>(std::min<int64_t>((n_valid + 255) / 256, 64)),
+                    static_cast<unsigned>(nrows));
+    if (v.fp16)
+        k_capture<__half><<<grid, 256, 0, s>>>(static_cast<const __half*>(v.data), v.pitch, v.base,
+                                               rows, out, out_pitch, t_off, n_valid);
+    else
+        k_capture<float><<<grid, 256, 0, s>>>(static_cast<const float*>(v.data), v.pitch, v.base,
+                                              rows, out, out_pitch, t_off, n_valid);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnodes,
+                   int32_t max_node_delay, const float* waterfall, int64_t waterfall_pitch,
+                   int64_t t0, int32_t n_valid, const float* input_hist, int32_t hist_len,
+                   LevelView out, int32_t ncols, cudaStream_t s) {
+    if (ncols % kTimePerCta != 0 || max_node_delay > hist_len)
+        throw Error(FROST_ERR_INTERNAL, "level1: bad geometry");
+    const dim3 grid(static_cast<unsigned>(nnodes), static_cast<unsigned>(ncols / kTimePerCta));
+    const size_t smem = 2 * sizeof(float) * (kTimePerCta + max_node_delay + 1);
+    if (smem > 200 * 1024)
+        throw Error(FROST_ERR_INVALID_ARGUMENT, "level1: leaf windows too long for shared memory");
+    if (out.fp16) {
+        FB_CUDA(cudaFuncSetAttribute(k_level1<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_level1<__half><<<grid, kThreads, smem, s>>>(
+            ops, node_first_op, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
+            input_hist, hist_len, static_cast<__half*>(out.data), out.pitch, out.base);
+    } else {
+        FB_CUDA(cudaFuncSetAttribute(k_level1<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_level1<float><<<grid, kThreads, smem, s>>>(
+            ops, node_first_op, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
+            input_hist, hist_len, static_cast<float*>(out.data), out.pitch, out.base);
+    }
+    FB_LAUNCH_CHECK();
+}
+
+void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
+                  cudaStream_t s) {
+    if (nrows == 0)
+        return;
+    if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
+        out.pitch % 8 != 0)
+        throw Error(FROST_ERR_INTERNAL, "level: bad geometry");
+    const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>(ncols / kTimePerCta));
+    if (out.fp16)
+        k_level<__half><<<grid, kThreads, 0, s>>>(ops, static_cast<const __half*>(in.data), in.pitch,
+                                                  in.base, static_cast<__half*>(out.data),
+                                                  out.pitch, out.base);
+    else
+        k_level<float><<<grid, kThreads, 0, s>>>(ops, static_cast<const float*>(in.data), in.pitch,
+                                                 in.base, static_cast<float*>(out.data), out.pitch,
+                                                 out.base);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_save_history(LevelView v, int64_t rows, int32_t hist, int32_t n_valid, void* hist_buf,
+                         cudaStream_t s) {
+    if (rows == 0 || hist == 0)
+        return;
+    const size_t es  = v.fp16 ? 2 : 4;
+    const char* src  = static_cast<const char*>(v.data) + (v.base + n_valid - hist) * es;
+    FB_CUDA(cudaMemcpy2DAsync(hist_buf, hist * es, src, v.pitch * es, hist * es,
+                              static_cast<size_t>(rows), cudaMemcpyDeviceToDevice, s));
+}
+
+void launch_load_history(LevelView v, int64_t rows, int32_t hist, const void* hist_buf,
+                         cudaStream_t s) {
+    if (rows == 0 || hist == 0)
+        return;
+    const size_t es = v.fp16 ? 2 : 4;
+    char* dst       = static_cast<char*>(v.data) + (v.base - hist) * es;
+    FB_CUDA(cudaMemcpy2DAsync(dst, v.pitch * es, hist_buf, hist * es, hist * es,
+                              static_cast<size_t>(rows), cudaMemcpyDeviceToDevice, s));
+}
+
+void launch_save_input_history(const float* wf, int64_t pitch, int64_t t0, int32_t n_valid,
+                               int32_t nchans, float* hist, float* scratch, int32_t hist_len,
+                               cudaStream_t s) {
+    if (hist_len == 0)
+        return;
+    const size_t es = sizeof(float);
+    if (n_valid >= hist_len) {
+        FB_CUDA(cudaMemcpy2DAsync(hist, hist_len * es, wf + t0 + n_valid - hist_len, pitch * es,
+                                  hist_len * es, nchans, cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    // Keep the newest hist_len - n_valid old samples, then append the tile.
+    const int32_t keep = hist_len - n_valid;
+    FB_CUDA(cudaMemcpy2DAsync(scratch, hist_len * es, hist + n_valid, hist_len * es, keep * es,
+                              nchans, cudaMemcpyDeviceToDevice, s));
+    if (n_valid > 0)
+        FB_CUDA(cudaMemcpy2DAsync(scratch + keep, hist_len * es, wf + t0, pitch * es, n_valid * es,
+                                  nchans, cudaMemcpyDeviceToDevice, s));
+    FB_CUDA(cudaMemcpyAsync(hist, scratch, static_cast<size_t>(nchans) * hist_len * es,
+                            cudaMemcpyDeviceToDevice, s));
+}
+
+} // namespace fb::fdmt

@@ -1,0 +1,56 @@
+// Launchers of the FDMT level kernels and the boxcar/trapezoid search
+// (fdmt_kernels.cu, search_kernels.cu).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime_api.h>
+
+#include "fdmt_plan.hpp"
+
+namespace fb::fdmt {
+
+/** A level buffer: rows of `pitch` elements; time t of the current tile is
+ * column `base + t`, its history occupies columns [base - H, base). */
+struct LevelView {
+    void* data;
+    int64_t pitch;
+    int32_t base;
+    int32_t fp16; // element type: 0 float, 1 __half
+};
+
+constexpr int kTimePerCta = 2048; // samples per CTA in the level kernels
+
+/** Level 1 straight from the input channels: each row is the sum of two
+ * leaf windows read from the waterfall (columns t0 .. t0 + n_valid) and,
+ * for times before the tile, the input history [C][hist_len]. */
+void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnodes,
+                   int32_t max_node_delay, const float* waterfall, int64_t waterfall_pitch,
+                   int64_t t0, int32_t n_valid, const float* input_hist, int32_t hist_len,
+                   LevelView out, int32_t ncols, cudaStream_t s);
+
+/** Level h >= 2: out[row] = in[lo] + in[hi] shifted. */
+void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
+                  cudaStream_t s);
+
+/** Copies the last `hist` columns ending at column base + n_valid of every
+ * row of `view` into hist_buf[rows][hist]. */
+void launch_save_history(LevelView view, int64_t rows, int32_t hist, int32_t n_valid,
+                         void* hist_buf, cudaStream_t s);
+
+/** Copies hist_buf[rows][hist] into columns [base - hist, base). */
+void launch_load_history(LevelView view, int64_t rows, int32_t hist, const void* hist_buf,
+                         cudaStream_t s);
+
+/** Copies level rows `rows[0..nrows)` (tile columns [0, n_valid)) to
+ * out[i][t_off + k] as float. */
+void launch_capture_rows(LevelView view, const int64_t* rows, int64_t nrows, float* out,
+                         int64_t out_pitch, int64_t t_off, int32_t n_valid, cudaStream_t s);
+
+/** Input history update: last hist columns of (old history ++ waterfall
+ * columns [t0, t0 + n_valid)). */
+void launch_save_input_history(const float* waterfall, int64_t pitch, int64_t t0, int32_t n_valid,
+                               int32_t nchans, float* hist, float* scratch, int32_t hist_len,
+                               cudaStream_t s);
+
+} // namespace fb::fdmt

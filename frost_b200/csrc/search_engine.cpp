@@ -1,0 +1,508 @@
+// Search engine orchestration (see search_engine.hpp).
+
+#include "search_engine.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "dedisp.hpp"
+
+namespace fb::fdmt {
+
+namespace {
+
+template <class T> void upload(DeviceBuffer& b, const std::vector<T>& v, cudaStream_t s) {
+    b.reserve(std::max<SizeType>(v.size() * sizeof(T), 16));
+    if (!v.empty())
+        FB_CUDA(cudaMemcpyAsync(b.get(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+PlanConfig plan_config(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc) {
+    float f_min = 0, f_max = 0;
+    dedisp::band_edges(dd, f_min, f_max);
+    if (dd.block_nsamps == 0)
+        invalid("search: block_nsamps must be > 0");
+    PlanConfig pc;
+    pc.nchans        = dd.nchans;
+    pc.f_min         = f_min;
+    pc.f_max         = f_max;
+    pc.tsamp         = dd.dt;
+    pc.block_nsamps  = dd.block_nsamps;
+    pc.subband_depth = dd.subband_depth;
+    pc.max_boxcar    = bc.max_boxcar;
+    pc.wtsp          = bc.wtsp;
+    pc.dm_list       = dedisp::generate_dm_list(dd);
+    return pc;
+}
+
+} // namespace
+
+Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc,
+               const uint8_t* kill_mask, SizeType memory_budget, int device)
+    : m_plan(plan_config(dd, bc)), m_cfg(bc), m_device(device),
+      m_fp16(bc.storage == FROST_STORAGE_FP16) {
+    if (bc.storage != FROST_STORAGE_FP32 && bc.storage != FROST_STORAGE_FP16)
+        invalid("search: storage must be fp32 or fp16");
+    if (bc.peak_mode < FROST_PEAK_PER_WIDTH || bc.peak_mode > FROST_PEAK_ALL)
+        invalid("search: invalid peak_mode");
+    if (!is_finite(bc.detect_thresh))
+        invalid("search: detect_thresh must be finite");
+    if (!(bc.noise_sigma == 1.0F) || bc.input_nbits != 32 || !(bc.input_mean == 0.0F))
+        invalid("search: the engine takes calibrated float32 input (noise_sigma 1, "
+                "input_nbits 32, input_mean 0)");
+    if (m_plan.widths().size() > 32)
+        invalid("search: more than 32 boxcar widths (raise wtsp)");
+    if (dd.block_nsamps <= static_cast<uint64_t>(m_plan.dt_max()) + bc.max_boxcar)
+        invalid("nsamps_gulp must exceed the dedispersion max_delay (" +
+                std::to_string(m_plan.dt_max()) + ") plus boxcar_max (" +
+                std::to_string(bc.max_boxcar) + ")");
+    int ndev = 0;
+    FB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev)
+        invalid("search: device " + std::to_string(device) + " does not exist");
+    DeviceGuard g(device);
+    FB_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
+    cudaStream_t s = m_stream;
+
+    const int32_t C = m_plan.nchans();
+    m_mask.assign(C, 1U);
+    if (kill_mask != nullptr)
+        for (int32_t c = 0; c < C; ++c)
+            m_mask[c] = kill_mask[c] != 0 ? 1 : 0;
+
+    // Level ops.
+    const int L = m_plan.levels();
+    std::vector<int32_t> first;
+    {
+        const auto& ops = m_plan.leaf_ops();
+        // nodes of height 1 own contiguous op ranges with one channel pair
+        first.push_back(0);
+        for (size_t i = 1; i < ops.size(); ++i)
+            if (ops[i].chan_lo != ops[i - 1].chan_lo || ops[i].chan_hi != ops[i - 1].chan_hi)
+                first.push_back(static_cast<int32_t>(i));
+        first.push_back(static_cast<int32_t>(ops.size()));
+        m_node_first_op = first;
+        upload(m_leaf_ops, ops, s);
+        upload(m_node_first_op_d, first, s);
+    }
+    std::vector<RowOp> all_ops;
+    m_row_op_offset.assign(L + 2, 0);
+    for (int h = 2; h <= L; ++h) {
+        m_row_op_offset[h] = static_cast<int64_t>(all_ops.size());
+        const auto& ops    = m_plan.row_ops(h);
+        all_ops.insert(all_ops.end(), ops.begin(), ops.end());
+    }
+    upload(m_row_ops, all_ops, s);
+
+    // Searched rows, grouped by height.
+    const auto& planes = m_plan.planes();
+    std::vector<int32_t> order(planes.size());
+    for (size_t i = 0; i < order.size(); ++i)
+        order[i] = static_cast<int32_t>(i);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return planes[a].height < planes[b].height; });
+    std::vector<SearchRow> rows;
+    std::vector<PlaneInfo> pinfo(planes.size());
+    std::vector<uint16_t> leaf;
+    std::vector<int64_t> leaf_off;
+    std::vector<int64_t> cap_rows;
+    m_height_g0.assign(L + 1, 0);
+    m_height_g1.assign(L + 1, 0);
+    for (size_t i = 0; i < planes.size(); ++i) {
+        const Plane& p = planes[i];
+        pinfo[i]       = {static_cast<float>(p.f_lo), static_cast<float>(p.f_hi),
+                          static_cast<uint32_t>(p.chan_begin), static_cast<uint32_t>(p.chan_end),
+                          static_cast<uint32_t>(p.subband_level), static_cast<uint32_t>(p.subband_idx)};
+    }
+    int cur_h = -1;
+    for (const int32_t pi : order) {
+        const Plane& p = planes[pi];
+        if (p.height != cur_h) {
+            cur_h                = p.height;
+            m_height_g0[cur_h]   = static_cast<int64_t>(rows.size());
+        }
+        const auto len    = m_plan.leaf_lengths(pi);
+        const int32_t nch = p.chan_end - p.chan_begin;
+        for (size_t r = 0; r < p.delay.size(); ++r) {
+            rows.push_back({p.level_row[r], pi, static_cast<int32_t>(r), p.delay[r], p.dm[r]});
+            leaf_off.push_back(static_cast<int64_t>(leaf.size()));
+            leaf.insert(leaf.end(), len.begin() + r * nch, len.begin() + (r + 1) * nch);
+        }
+        m_height_g1[cur_h] = static_cast<int64_t>(rows.size());
+    }
+    m_nsearch = rows.size();
+    upload(m_rows, rows, s);
+    upload(m_planes, pinfo, s);
+    upload(m_leaf_len, leaf, s);
+    upload(m_leaf_offset, leaf_off, s);
+    upload(m_widths, m_plan.widths(), s);
+
+    // Window-box variance table g[L][w].
+    m_max_len          = m_plan.max_leaf_length();
+    const auto& widths = m_plan.widths();
+    std::vector<double> gtab((m_max_len + 1) * widths.size(), 0.0);
+    for (int32_t Lc = 1; Lc <= m_max_len; ++Lc)
+        for (size_t w = 0; w < widths.size(); ++w)
+            gtab[Lc * widths.size() + w] =
+                window_box_variance(Lc, widths[w], bc.use_trapezoid != 0);
+    upload(m_gtab, gtab, s);
+    const SizeType nw = widths.size();
+    m_var.reserve(std::max<SizeType>(m_nsearch * nw * sizeof(double), 16));
+    m_inv.reserve(std::max<SizeType>(m_nsearch * nw * sizeof(float), 16));
+    m_inv_or.reserve(std::max<SizeType>(m_nsearch * nw * sizeof(float), 16));
+    const SizeType nruns = bc.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : nw;
+    m_carry.reserve(std::max<SizeType>(m_nsearch * nruns * sizeof(RunState), 16));
+    FB_CUDA(cudaMemsetAsync(m_carry.get(), 0, m_nsearch * nruns * sizeof(RunState), s));
+    m_row_counts.reserve(std::max<SizeType>(m_nsearch * sizeof(uint32_t), 16));
+    const SizeType maxc = std::max<uint64_t>(bc.max_candidates, 1);
+    m_cands.reserve(maxc * sizeof(frost_candidate));
+    m_counters.reserve(4 * sizeof(unsigned long long));
+    m_frontier.reserve(sizeof(unsigned long long));
+    m_mask_d.reserve(C);
+    m_mask_or_d.reserve(C);
+
+    // Tile length: the whole gulp unless the budget (or the device) is short.
+    int64_t tile = bc.tile_nsamps != 0 ? static_cast<int64_t>(bc.tile_nsamps)
+                                       : static_cast<int64_t>(dd.block_nsamps);
+    if (bc.tile_nsamps != 0 && bc.tile_nsamps % kTimePerCta != 0)
+        invalid("search: tile_nsamps must be a multiple of 2048");
+    tile = round_up(std::min<int64_t>(tile, static_cast<int64_t>(dd.block_nsamps)), kTimePerCta);
+    size_t free_b = 0, total_b = 0;
+    FB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const SizeType limit = memory_budget != 0 ? memory_budget
+                                              : static_cast<SizeType>(0.85 * static_cast<double>(free_b));
+    while (plan_bytes(tile) > limit && tile > kTimePerCta)
+        tile = round_up(tile / 2, kTimePerCta);
+    if (plan_bytes(tile) > limit)
+        throw Error(FROST_ERR_OUT_OF_MEMORY,
+                    "search: plan needs " + std::to_string(plan_bytes(tile)) +
+                        " device bytes at the smallest tile; budget " + std::to_string(limit));
+    allocate(tile);
+    FB_CUDA(cudaStreamSynchronize(s));
+}
+
+Engine::~Engine() {
+    if (m_stream != nullptr) {
+        cudaSetDevice(m_device);
+        cudaStreamSynchronize(m_stream);
+        cudaStreamDestroy(m_stream);
+    }
+}
+
+SizeType Engine::plan_bytes(int64_t tile) const {
+    const SizeType es    = m_fp16 ? 2 : 4;
+    const int L          = m_plan.levels();
+    int32_t maxh         = 0;
+    for (int h = 1; h <= L; ++h)
+        maxh = std::max(maxh, m_plan.level_history(h));
+    const int64_t base   = round_up(std::max<int64_t>(maxh, m_plan.widths().back()), 8);
+    const int64_t pitch  = base + round_up(tile, kTimePerCta);
+    SizeType bytes       = 2 * static_cast<SizeType>(m_plan.max_level_rows()) * pitch * es;
+    for (int h = 1; h <= L; ++h)
+        bytes += static_cast<SizeType>(m_plan.level_rows(h)) * m_plan.level_history(h) * es;
+    bytes += 2 * static_cast<SizeType>(m_plan.nchans()) * m_plan.level_history(0) * sizeof(float);
+    bytes += m_leaf_len.bytes() + m_rows.bytes() + m_var.bytes() + m_inv.bytes() * 2 +
+             m_carry.bytes() + m_cands.bytes() + m_row_ops.bytes() + m_leaf_ops.bytes();
+    return bytes;
+}
+
+void Engine::allocate(int64_t tile) {
+    const SizeType es = m_fp16 ? 2 : 4;
+    const int L       = m_plan.levels();
+    int32_t maxh      = 0;
+    for (int h = 1; h <= L; ++h)
+        maxh = std::max(maxh, m_plan.level_history(h));
+    m_tile  = tile;
+    m_ncols = round_up(tile, kTimePerCta);
+    m_base  = static_cast<int32_t>(round_up(std::max<int64_t>(maxh, m_plan.widths().back()), 8));
+    m_pitch = m_base + m_ncols;
+    const SizeType buf = static_cast<SizeType>(m_plan.max_level_rows()) * m_pitch * es;
+    for (auto& b : m_buf) {
+        b.reserve(buf);
+        FB_CUDA(cudaMemsetAsync(b.get(), 0, buf, m_stream));
+    }
+    m_hist.clear();
+    m_hist.resize(L + 1);
+    for (int h = 1; h <= L; ++h) {
+        const SizeType bytes = static_cast<SizeType>(m_plan.level_rows(h)) * m_plan.level_history(h) * es;
+        m_hist[h].reserve(std::max<SizeType>(bytes, 16));
+        FB_CUDA(cudaMemsetAsync(m_hist[h].get(), 0, std::max<SizeType>(bytes, 16), m_stream));
+    }
+    const SizeType in_bytes = static_cast<SizeType>(m_plan.nchans()) * m_plan.level_history(0) * sizeof(float);
+    m_in_hist.reserve(std::max<SizeType>(in_bytes, 16));
+    m_in_scratch.reserve(std::max<SizeType>(in_bytes, 16));
+    FB_CUDA(cudaMemsetAsync(m_in_hist.get(), 0, std::max<SizeType>(in_bytes, 16), m_stream));
+}
+
+SizeType Engine::device_bytes() const {
+    SizeType total = m_buf[0].bytes() + m_buf[1].bytes();
+    for (const auto& b : m_hist)
+        total += b.bytes();
+    const DeviceBuffer* rest[] = {&m_in_hist, &m_in_scratch, &m_wf_stage, &m_leaf_ops,
+                                  &m_node_first_op_d, &m_row_ops, &m_rows, &m_planes, &m_widths,
+                                  &m_leaf_len, &m_leaf_offset, &m_gtab, &m_var, &m_inv, &m_inv_or,
+                                  &m_mask_d, &m_mask_or_d, &m_carry, &m_row_counts, &m_cands,
+                                  &m_counters, &m_frontier, &m_capture_rows};
+    for (const auto* b : rest)
+        total += b->bytes();
+    for (const auto& b : m_capture)
+        total += b.bytes();
+    return total;
+}
+
+LevelView Engine::view(int h) const {
+    return LevelView{m_buf[h % 2].get(), m_pitch, m_base, m_fp16 ? 1 : 0};
+}
+
+SearchParams Engine::params(int64_t tile_t0, int64_t gulp_t0, int32_t n_valid, bool or_active) const {
+    SearchParams p{};
+    p.rows         = m_rows.as<SearchRow>();
+    p.planes       = m_planes.as<PlaneInfo>();
+    p.widths       = m_widths.as<int32_t>();
+    p.nwidths      = static_cast<int32_t>(m_plan.widths().size());
+    p.wmax         = m_plan.widths().back();
+    p.thresh       = m_cfg.detect_thresh;
+    p.peak_mode    = m_cfg.peak_mode;
+    p.trapezoid    = m_cfg.use_trapezoid ? 1 : 0;
+    p.skip_cold    = m_cfg.skip_cold_prefix ? 1 : 0;
+    p.or_active    = or_active ? 1 : 0;
+    p.tile_t0      = tile_t0;
+    p.gulp_t0      = gulp_t0;
+    p.n_valid      = n_valid;
+    p.inv_sigma    = m_inv.as<float>();
+    p.inv_sigma_or = m_inv_or.as<float>();
+    p.carry        = m_carry.as<RunState>();
+    p.cands        = m_cands.as<frost_candidate>();
+    p.ncands       = m_counters.as<unsigned long long>();
+    p.max_cands    = m_cfg.max_candidates;
+    p.row_counts   = m_row_counts.as<uint32_t>();
+    p.max_per_dm   = static_cast<uint32_t>(std::min<uint64_t>(m_cfg.max_cands_per_dm, 0xFFFFFFFFULL));
+    p.dropped      = m_counters.as<unsigned long long>() + 1;
+    return p;
+}
+
+void Engine::update_variance(const std::vector<uint8_t>& cur, const std::vector<uint8_t>& orm) {
+    if (m_var_ready && cur == m_var_mask && orm == m_var_mask_or)
+        return;
+    const int32_t C = m_plan.nchans();
+    FB_CUDA(cudaMemcpyAsync(m_mask_d.get(), cur.data(), C, cudaMemcpyHostToDevice, m_stream));
+    FB_CUDA(cudaMemcpyAsync(m_mask_or_d.get(), orm.data(), C, cudaMemcpyHostToDevice, m_stream));
+    launch_variance(m_rows.as<SearchRow>(), m_planes.as<PlaneInfo>(), m_leaf_offset.as<int64_t>(),
+                    m_leaf_len.as<uint16_t>(), static_cast<int64_t>(m_nsearch), m_gtab.as<double>(),
+                    m_max_len, static_cast<int32_t>(m_plan.widths().size()),
+                    m_mask_d.as<uint8_t>(), m_mask_or_d.as<uint8_t>(), m_var.as<double>(),
+                    m_inv.as<float>(), m_inv_or.as<float>(), m_stream);
+    ++m_launches;
+    m_var_mask    = cur;
+    m_var_mask_or = orm;
+    m_var_ready   = true;
+}
+
+void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, const uint8_t* mask,
+                     cudaStream_t stream) {
+    if (waterfall == nullptr)
+        invalid("search: null waterfall");
+    if (nsamps == 0 || nsamps > m_plan.config().block_nsamps)
+        invalid("search: nsamps must be in [1, block_nsamps]");
+    DeviceGuard g(m_device);
+    cudaStream_t s  = m_stream;
+    m_launches      = 0;
+    const int32_t C = m_plan.nchans();
+    std::vector<uint8_t> cur = m_mask;
+    if (mask != nullptr)
+        for (int32_t c = 0; c < C; ++c)
+            cur[c] = mask[c] != 0 ? 1 : 0;
+    const bool or_active = cur != m_mask;
+    std::vector<uint8_t> orm(C);
+    for (int32_t c = 0; c < C; ++c)
+        orm[c] = (cur[c] | m_mask[c]) ? 1 : 0;
+    // Order the caller's stream before the engine's.
+    if (stream != nullptr && stream != s) {
+        cudaEvent_t ev;
+        FB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        FB_CUDA(cudaEventRecord(ev, stream));
+        FB_CUDA(cudaStreamWaitEvent(s, ev, 0));
+        FB_CUDA(cudaEventDestroy(ev));
+    }
+    update_variance(cur, orm);
+
+    const float* wf = waterfall;
+    if (!on_device) {
+        const SizeType bytes = static_cast<SizeType>(C) * nsamps * sizeof(float);
+        m_wf_stage.reserve(bytes);
+        FB_CUDA(cudaMemcpyAsync(m_wf_stage.get(), waterfall, bytes, cudaMemcpyHostToDevice, s));
+        wf = m_wf_stage.as<float>();
+    }
+    FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, 4 * sizeof(unsigned long long), s));
+    FB_CUDA(cudaMemsetAsync(m_row_counts.get(), 0, m_nsearch * sizeof(uint32_t), s));
+    if (m_capture_on) {
+        const auto& planes = m_plan.planes();
+        m_capture.resize(planes.size());
+        m_capture_cols = static_cast<int64_t>(nsamps);
+        for (size_t p = 0; p < planes.size(); ++p)
+            m_capture[p].reserve(std::max<SizeType>(planes[p].delay.size() * nsamps * sizeof(float), 16));
+    }
+
+    const int L          = m_plan.levels();
+    const int64_t gulp0  = static_cast<int64_t>(m_samples);
+    const auto& planes   = m_plan.planes();
+    for (int64_t t_off = 0; t_off < static_cast<int64_t>(nsamps); t_off += m_tile) {
+        const int32_t n_valid = static_cast<int32_t>(std::min<int64_t>(m_tile, nsamps - t_off));
+        const SearchParams sp = params(gulp0 + t_off, gulp0, n_valid, or_active);
+        for (int h = 1; h <= L; ++h) {
+            const LevelView out = view(h);
+            if (h == 1) {
+                launch_level1(m_leaf_ops.as<LeafOp>(), m_node_first_op_d.as<int32_t>(),
+                              static_cast<int32_t>(m_node_first_op.size() - 1),
+                              m_plan.level_history(0), wf, static_cast<int64_t>(nsamps), t_off,
+                              n_valid, m_in_hist.as<float>(), m_plan.level_history(0), out,
+                              static_cast<int32_t>(m_ncols), s);
+                launch_save_input_history(wf, static_cast<int64_t>(nsamps), t_off, n_valid, C,
+                                          m_in_hist.as<float>(), m_in_scratch.as<float>(),
+                                          m_plan.level_history(0), s);
+                m_launches += 1;
+            } else {
+                launch_level(m_row_ops.as<RowOp>() + m_row_op_offset[h], m_plan.level_rows(h),
+                             view(h - 1), out, static_cast<int32_t>(m_ncols), s);
+                m_launches += 1;
+            }
+            launch_load_history(out, m_plan.level_rows(h), m_plan.level_history(h),
+                                m_hist[h].get(), s);
+            if (m_height_g1[h] > m_height_g0[h]) {
+                launch_search(sp, out, m_height_g0[h], m_height_g1[h], s);
+                m_launches += 1;
+                if (m_capture_on) {
+                    for (size_t p = 0; p < planes.size(); ++p) {
+                        if (planes[p].height != h)
+                            continue;
+                        std::vector<int64_t> rows(planes[p].level_row.begin(), planes[p].level_row.end());
+                        upload(m_capture_rows, rows, s);
+                        launch_capture_rows(out, m_capture_rows.as<int64_t>(),
+                                            static_cast<int64_t>(rows.size()),
+                                            m_capture[p].as<float>(), m_capture_cols, t_off,
+                                            n_valid, s);
+                        FB_CUDA(cudaStreamSynchronize(s));
+                    }
+                }
+            }
+            if (h >= 2)
+                launch_save_history(view(h - 1), m_plan.level_rows(h - 1),
+                                    m_plan.level_history(h - 1), n_valid, m_hist[h - 1].get(), s);
+        }
+        launch_save_history(view(L), m_plan.level_rows(L), m_plan.level_history(L), n_valid,
+                            m_hist[L].get(), s);
+    }
+    m_samples += nsamps;
+    m_mask = cur;
+    collect(s);
+}
+
+void Engine::collect(cudaStream_t s) {
+    unsigned long long counters[4];
+    FB_CUDA(cudaMemcpyAsync(counters, m_counters.get(), sizeof(counters), cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
+    const uint64_t n = std::min<uint64_t>(counters[0], m_cfg.max_candidates);
+    m_results.resize(n);
+    if (n)
+        FB_CUDA(cudaMemcpy(m_results.data(), m_cands.get(), n * sizeof(frost_candidate),
+                           cudaMemcpyDeviceToHost));
+    m_dropped_global = counters[1];
+    m_dropped_per_dm = counters[2];
+    std::sort(m_results.begin(), m_results.end(), [](const frost_candidate& a, const frost_candidate& b) {
+        if (a.subband_level != b.subband_level)
+            return a.subband_level < b.subband_level;
+        if (a.subband_idx != b.subband_idx)
+            return a.subband_idx < b.subband_idx;
+        if (a.dm_idx != b.dm_idx)
+            return a.dm_idx < b.dm_idx;
+        if (a.peak_sample != b.peak_sample)
+            return a.peak_sample < b.peak_sample;
+        return a.filter_idx < b.filter_idx;
+    });
+}
+
+void Engine::drain() {
+    DeviceGuard g(m_device);
+    cudaStream_t s = m_stream;
+    FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, 4 * sizeof(unsigned long long), s));
+    FB_CUDA(cudaMemsetAsync(m_row_counts.get(), 0, m_nsearch * sizeof(uint32_t), s));
+    const SearchParams sp = params(static_cast<int64_t>(m_samples), static_cast<int64_t>(m_samples), 0, false);
+    launch_flush_runs(sp, static_cast<int64_t>(m_nsearch), s);
+    collect(s);
+}
+
+uint64_t Engine::frontier() {
+    DeviceGuard g(m_device);
+    // Earliest start of a still-open run, else the samples processed so far.
+    const SizeType nruns = m_cfg.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : m_plan.widths().size();
+    if (m_cfg.peak_mode == FROST_PEAK_ALL)
+        return m_samples;
+    std::vector<RunState> runs(m_nsearch * nruns);
+    FB_CUDA(cudaStreamSynchronize(m_stream));
+    if (!runs.empty())
+        FB_CUDA(cudaMemcpy(runs.data(), m_carry.get(), runs.size() * sizeof(RunState), cudaMemcpyDeviceToHost));
+    uint64_t f = m_samples;
+    for (const auto& r : runs)
+        if (r.open)
+            f = std::min<uint64_t>(f, static_cast<uint64_t>(r.start));
+    return f;
+}
+
+frost_search_info Engine::info() const {
+    frost_search_info i{};
+    i.nchans       = static_cast<uint64_t>(m_plan.nchans());
+    i.block_nsamps = m_plan.config().block_nsamps;
+    i.tile_nsamps  = static_cast<uint64_t>(m_tile);
+    i.dt_max       = static_cast<uint64_t>(m_plan.dt_max());
+    i.ndm          = m_plan.config().dm_list.size();
+    i.nplanes      = m_plan.planes().size();
+    i.nwidths      = m_plan.widths().size();
+    i.levels       = static_cast<uint64_t>(m_plan.levels());
+    i.device_bytes = device_bytes();
+    i.f_min        = m_plan.config().f_min;
+    i.f_max        = m_plan.config().f_max;
+    return i;
+}
+
+std::vector<double> Engine::variance_grid(SizeType plane, uint32_t width, const uint8_t* mask) const {
+    const auto& planes = m_plan.planes();
+    if (plane >= planes.size())
+        invalid("search: plane index out of range");
+    const Plane& p    = planes[plane];
+    const auto len    = m_plan.leaf_lengths(static_cast<int>(plane));
+    const int32_t nch = p.chan_end - p.chan_begin;
+    const uint8_t* m  = mask != nullptr ? mask : m_mask.data();
+    std::vector<double> g(m_plan.max_leaf_length() + 2, 0.0);
+    for (int32_t L = 1; L < static_cast<int32_t>(g.size()); ++L)
+        g[L] = window_box_variance(L, static_cast<int32_t>(width), m_cfg.use_trapezoid != 0);
+    std::vector<double> out(p.delay.size(), 0.0);
+    for (size_t r = 0; r < p.delay.size(); ++r) {
+        double v = 0.0;
+        for (int32_t c = 0; c < nch; ++c)
+            if (m[p.chan_begin + c])
+                v += g[len[r * nch + c]];
+        out[r] = v;
+    }
+    return out;
+}
+
+void Engine::capture(bool on) {
+    m_capture_on = on;
+    if (!on)
+        m_capture.clear();
+}
+
+void Engine::plane_data(SizeType plane, float* out, SizeType capacity) const {
+    if (!m_capture_on || plane >= m_capture.size())
+        fail_state("search: plane capture is off or no execute has run");
+    const SizeType n = m_plan.planes()[plane].delay.size() * static_cast<SizeType>(m_capture_cols);
+    if (capacity < n)
+        invalid("search: plane buffer too small");
+    DeviceGuard g(m_device);
+    FB_CUDA(cudaMemcpy(out, m_capture[plane].get(), n * sizeof(float), cudaMemcpyDeviceToHost));
+}
+
+} // namespace fb::fdmt

@@ -1,0 +1,86 @@
+// The search engine: a frost-owned replacement for dmt::FDMTBoxcar with its
+// call shape (lib/pipeline/pipeline.cpp:346-367, 493, 517, 598-608).
+// Streaming FDMT (per-level history carried across tiles and gulps) feeding
+// the boxcar/trapezoid search with exact per-DM/width/mask noise.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime_api.h>
+
+#include "common.hpp"
+#include "fdmt_plan.hpp"
+#include "search_kernels.hpp"
+
+namespace fb::fdmt {
+
+class Engine {
+public:
+    Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc,
+           const uint8_t* kill_mask, SizeType memory_budget, int device);
+    ~Engine();
+    Engine(const Engine&)            = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    void execute(const float* waterfall, SizeType nsamps, bool on_device, const uint8_t* mask,
+                 cudaStream_t stream);
+    void drain();
+
+    const std::vector<frost_candidate>& results() const { return m_results; }
+    uint64_t dropped_global() const { return m_dropped_global; }
+    uint64_t dropped_per_dm() const { return m_dropped_per_dm; }
+    uint64_t frontier();
+    frost_search_info info() const;
+    const Plan& plan() const { return m_plan; }
+    std::vector<double> variance_grid(SizeType plane, uint32_t width, const uint8_t* mask) const;
+    void capture(bool on);
+    void plane_data(SizeType plane, float* out, SizeType capacity) const;
+    int device() const { return m_device; }
+    SizeType device_bytes() const;
+    /** Stream of the engine's kernels (for callers timing them). */
+    cudaStream_t stream() const { return m_stream; }
+    /** Kernel launches of the last execute call. */
+    uint64_t last_launches() const { return m_launches; }
+
+private:
+    Plan m_plan;
+    frost_boxcar_config m_cfg;
+    int m_device;
+    cudaStream_t m_stream = nullptr;
+    bool m_fp16;
+    int64_t m_tile = 0, m_ncols = 0, m_pitch = 0;
+    int32_t m_base = 0;
+    SizeType m_nsearch = 0; // searched rows over all planes
+    std::vector<int64_t> m_height_g0, m_height_g1; // searched rows per height
+    std::vector<int32_t> m_node_first_op;
+
+    DeviceBuffer m_buf[2];
+    std::vector<DeviceBuffer> m_hist;
+    DeviceBuffer m_in_hist, m_in_scratch, m_wf_stage;
+    DeviceBuffer m_leaf_ops, m_node_first_op_d, m_row_ops, m_rows, m_planes, m_widths, m_leaf_len,
+        m_leaf_offset, m_gtab, m_var, m_inv, m_inv_or, m_mask_d, m_mask_or_d, m_carry,
+        m_row_counts, m_cands, m_counters, m_frontier, m_capture_rows;
+    std::vector<int64_t> m_row_op_offset;
+    std::vector<DeviceBuffer> m_capture;
+    bool m_capture_on = false;
+    int64_t m_capture_cols = 0;
+
+    std::vector<uint8_t> m_mask;     // mask of the previous gulp (FDMT order)
+    std::vector<uint8_t> m_var_mask, m_var_mask_or;
+    bool m_var_ready = false;
+    uint64_t m_samples = 0;          // absolute samples processed
+    std::vector<frost_candidate> m_results;
+    uint64_t m_dropped_global = 0, m_dropped_per_dm = 0;
+    uint64_t m_launches = 0;
+    int32_t m_max_len = 1;
+
+    SizeType plan_bytes(int64_t tile) const;
+    void allocate(int64_t tile);
+    SearchParams params(int64_t tile_t0, int64_t gulp_t0, int32_t n_valid, bool or_active) const;
+    LevelView view(int h) const;
+    void update_variance(const std::vector<uint8_t>& cur, const std::vector<uint8_t>& orm);
+    void collect(cudaStream_t s);
+};
+
+} // namespace fb::fdmt

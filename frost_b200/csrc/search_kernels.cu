@@ -1,0 +1,391 @@
+// Boxcar/trapezoid matched filter, exact noise and peak finding on sm_100a.
+//
+// One CTA per searched (plane, DM) row walks the tile in 2048-sample chunks:
+// the chunk plus a (wmax - 1)-sample halo is staged in shared memory and
+// prefix-summed, every width's S/N is a difference of two (four for the
+// trapezoid) prefix values times 1/sigma, and above-threshold samples become
+// ballot bitmasks. Runs (contiguous set bits) are rare, so one lane walks
+// only the set bits in time order, extending or closing the run carried
+// from the previous chunk (and tile, and gulp) and emitting each closed
+// run's peak. The DM-time rows are never re-read and the run state is the
+// only thing carried between calls.
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "search_kernels.hpp"
+
+namespace fb::fdmt {
+
+namespace {
+
+constexpr int kThreads   = 256;
+constexpr int kChunk     = 2048;
+constexpr int kWords     = kChunk / 32;
+constexpr int kMaxWidths = 32;
+#define FB_NEG_INF (-__int_as_float(0x7f800000))
+
+template <class S> __device__ __forceinline__ float ldf(const S* p);
+template <> __device__ __forceinline__ float ldf<float>(const float* p) { return *p; }
+template <> __device__ __forceinline__ float ldf<__half>(const __half* p) { return __half2float(*p); }
+
+__device__ void scan_inplace(float* a, int n) {
+    __shared__ float warp_tot[kThreads / 32];
+    const int per = (n + kThreads - 1) / kThreads;
+    const int beg = threadIdx.x * per;
+    const int end = min(beg + per, n);
+    float run     = 0.0F;
+    for (int i = beg; i < end; ++i) {
+        run += a[i];
+        a[i] = run;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float v        = run;
+    for (int o = 1; o < 32; o <<= 1) {
+        const float u = __shfl_up_sync(0xFFFFFFFFU, v, o);
+        if (lane >= o)
+            v += u;
+    }
+    if (lane == 31)
+        warp_tot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        float w = lane < kThreads / 32 ? warp_tot[lane] : 0.0F;
+        for (int o = 1; o < 32; o <<= 1) {
+            const float u = __shfl_up_sync(0xFFFFFFFFU, w, o);
+            if (lane >= o)
+                w += u;
+        }
+        if (lane < kThreads / 32)
+            warp_tot[lane] = w;
+    }
+    __syncthreads();
+    const float offset = (v - run) + (warp > 0 ? warp_tot[warp - 1] : 0.0F);
+    for (int i = beg; i < end; ++i)
+        a[i] += offset;
+    __syncthreads();
+}
+
+struct Ctx {
+    const SearchParams* p;
+    const float* P;      // prefix sums: P[i] covers columns up to c0 - wmax + i
+    const float* inv;    // 1/sigma per width (shared memory)
+    const float* inv_or; // 1/sigma under the OR of the last two masks
+    int wmax;
+    int64_t c0;          // chunk start column in the tile
+    int32_t delay;
+};
+
+// Sum of the width-W window ending at chunk sample k (boxcar or trapezoid).
+__device__ __forceinline__ float window_sum(const Ctx& c, int k, int W, int trap) {
+    const int i = k + c.wmax;
+    float s     = c.P[i] - c.P[i - W];
+    if (trap && W >= 3) {
+        const int e = (W + 1) / 4;
+        s -= 0.5F * ((c.P[i] - c.P[i - e]) + (c.P[i - W + e] - c.P[i - W]));
+    }
+    return s;
+}
+
+// S/N of chunk sample k at width index wi, or -inf where the sample is not
+// searchable (past the valid columns, or in the cold prefix).
+__device__ __forceinline__ float snr_at(const Ctx& c, int k, int wi) {
+    const SearchParams& p = *c.p;
+    const int W           = p.widths[wi];
+    const int64_t col     = c.c0 + k;
+    if (col >= p.n_valid)
+        return FB_NEG_INF;
+    const int64_t t = p.tile_t0 + col;
+    if (p.skip_cold && t < static_cast<int64_t>(c.delay) + W - 1)
+        return FB_NEG_INF;
+    const bool use_or = p.or_active && (t - p.gulp_t0) < static_cast<int64_t>(c.delay) + W - 1;
+    const float inv   = use_or ? c.inv_or[wi] : c.inv[wi];
+    if (inv == 0.0F)
+        return FB_NEG_INF;
+    return window_sum(c, k, W, p.trapezoid) * inv;
+}
+
+// `count` (shared or global) is the row's emitted total this call.
+__device__ void emit(const SearchParams& p, const SearchRow& row, int64_t g, const RunState& r,
+                     uint32_t* count) {
+    const uint32_t before = atomicAdd(count, 1U);
+    if (p.max_per_dm != 0 && before >= p.max_per_dm) {
+        atomicAdd(&p.dropped[1], 1ULL);
+        return;
+    }
+    const unsigned long long idx = atomicAdd(p.ncands, 1ULL);
+    if (idx >= p.max_cands) {
+        atomicAdd(&p.dropped[0], 1ULL);
+        return;
+    }
+    const PlaneInfo& pl = p.planes[row.plane];
+    frost_candidate c;
+    c.peak_sample   = static_cast<uint64_t>(r.best_t);
+    c.begin_sample  = static_cast<uint64_t>(r.start);
+    c.end_sample    = static_cast<uint64_t>(r.last_t);
+    c.snr           = r.best;
+    c.dm            = row.dm;
+    c.f_low_mhz     = pl.f_low;
+    c.f_high_mhz    = pl.f_high;
+    c.filter_idx    = static_cast<uint32_t>(r.best_w);
+    c.width         = static_cast<uint32_t>(p.widths[r.best_w]);
+    c.dm_idx        = static_cast<uint32_t>(row.prow);
+    c.chan_begin    = pl.chan_begin;
+    c.chan_end      = pl.chan_end;
+    c.beam_idx      = 0;
+    c.subband_level = pl.subband_level;
+    c.subband_idx   = pl.subband_idx;
+    p.cands[idx]    = c;
+}
+
+// Walks the set bits of one chunk's mask in time order (one lane).
+// For across-widths mode `wi` < 0: the peak is the best S/N over widths.
+__device__ void walk_runs(const Ctx& c, const uint32_t* bits, int wi, RunState& run,
+                          const SearchRow& row, int64_t g, uint32_t* local_count) {
+    const SearchParams& p = *c.p;
+    int64_t last          = run.open ? c.c0 - 1 : -2; // tile column of the last set bit
+    for (int wd = 0; wd < kWords; ++wd) {
+        uint32_t b = bits[wd];
+        while (b) {
+            const int bit   = __ffs(b) - 1;
+            b &= b - 1;
+            const int k     = wd * 32 + bit;
+            const int64_t col = c.c0 + k;
+            float best = FB_NEG_INF;
+            int bw     = 0;
+            if (wi >= 0) {
+                best = snr_at(c, k, wi);
+                bw   = wi;
+            } else {
+                for (int w = 0; w < p.nwidths; ++w) {
+                    const float s = snr_at(c, k, w);
+                    if (s > best) {
+                        best = s;
+                        bw   = w;
+                    }
+                }
+            }
+            const int64_t t = p.tile_t0 + col;
+            if (run.open && col == last + 1) {
+                if (best > run.best) {
+                    run.best   = best;
+                    run.best_t = t;
+                    run.best_w = bw;
+                }
+                run.last_t = t;
+            } else {
+                if (run.open)
+                    emit(p, row, g, run, local_count);
+                run.open   = 1;
+                run.start  = t;
+                run.best   = best;
+                run.best_t = t;
+                run.best_w = bw;
+                run.last_t = t;
+            }
+            last = col;
+        }
+    }
+    // A run that does not reach the chunk's last valid column has closed.
+    const int64_t chunk_end = min(c.c0 + kChunk, static_cast<int64_t>(p.n_valid));
+    if (run.open && last != chunk_end - 1) {
+        emit(p, row, g, run, local_count);
+        run.open = 0;
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(kThreads)
+    k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0) {
+    extern __shared__ float P[];
+    __shared__ uint32_t bits[kMaxWidths][kWords];
+    __shared__ uint32_t any_bits[kWords];
+    __shared__ RunState runs[kMaxWidths];
+    __shared__ float s_inv[kMaxWidths], s_inv_or[kMaxWidths];
+    __shared__ uint32_t local_count;
+
+    const int64_t g     = g0 + blockIdx.x;
+    const SearchRow row = p.rows[g];
+    const int nw        = p.nwidths;
+    const bool across   = p.peak_mode == FROST_PEAK_ACROSS_WIDTHS;
+    const bool all      = p.peak_mode == FROST_PEAK_ALL;
+    if (threadIdx.x == 0)
+        local_count = p.row_counts[g];
+    if (threadIdx.x < nw) {
+        s_inv[threadIdx.x]    = p.inv_sigma[g * nw + threadIdx.x];
+        s_inv_or[threadIdx.x] = p.inv_sigma_or[g * nw + threadIdx.x];
+    }
+    const int nruns = across ? 1 : nw;
+    if (threadIdx.x < nruns && !all)
+        runs[threadIdx.x] = p.carry[g * nruns + threadIdx.x];
+    __syncthreads();
+    Ctx c;
+    c.p      = &p;
+    c.P      = P;
+    c.inv    = s_inv;
+    c.inv_or = s_inv_or;
+    c.wmax   = p.wmax;
+    c.c0     = 0;
+    c.delay  = row.delay;
+
+    const S* src   = level + row.level_row * pitch + base;
+    const int N    = kChunk + p.wmax;
+    for (int64_t c0 = 0; c0 < p.n_valid; c0 += kChunk) {
+        c.c0 = c0;
+        // P[i] <- column c0 - wmax + i (i = 0 is the scan base).
+        for (int i = threadIdx.x; i < N; i += kThreads)
+            P[i] = i == 0 ? 0.0F : ldf<S>(src + c0 - p.wmax + i);
+        __syncthreads();
+        scan_inplace(P, N);
+
+        uint32_t any = 0;
+        for (int wi = 0; wi < nw; ++wi) {
+            for (int j = 0; j < kChunk / kThreads; ++j) {
+                const int k   = threadIdx.x + j * kThreads;
+                const float s = snr_at(c, k, wi);
+                const bool up = s > p.thresh;
+                if (all && up) {
+                    RunState r{};
+                    r.best   = s;
+                    r.best_w = wi;
+                    r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
+                    emit(p, row, g, r, &local_count);
+                }
+                const uint32_t m = __ballot_sync(0xFFFFFFFFU, up);
+                if ((threadIdx.x & 31) == 0)
+                    bits[wi][j * (kThreads / 32) + (threadIdx.x >> 5)] = m;
+                any |= m;
+            }
+        }
+        if (across) {
+            __syncthreads();
+            for (int wd = threadIdx.x; wd < kWords; wd += kThreads) {
+                uint32_t m = 0;
+                for (int wi = 0; wi < nw; ++wi)
+                    m |= bits[wi][wd];
+                any_bits[wd] = m;
+            }
+        }
+        // Skip the walk when nothing fired and no run is open.
+        const int fired = __syncthreads_or(any != 0);
+        if (!all && threadIdx.x == 0) {
+            if (across) {
+                if (fired || runs[0].open)
+                    walk_runs(c, any_bits, -1, runs[0], row, g, &local_count);
+            } else {
+                for (int wi = 0; wi < nw; ++wi)
+                    if (fired || runs[wi].open)
+                        walk_runs(c, bits[wi], wi, runs[wi], row, g, &local_count);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < nruns && !all)
+        p.carry[g * nruns + threadIdx.x] = runs[threadIdx.x];
+    if (threadIdx.x == 0)
+        p.row_counts[g] = local_count;
+}
+
+__global__ void k_flush(SearchParams p, int64_t nrows) {
+    const int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (g >= nrows)
+        return;
+    const int nruns     = p.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : p.nwidths;
+    const SearchRow row = p.rows[g];
+    for (int i = 0; i < nruns; ++i) {
+        RunState& r = p.carry[g * nruns + i];
+        if (r.open) {
+            emit(p, row, g, r, &p.row_counts[g]);
+            r.open = 0;
+        }
+    }
+}
+
+__global__ void k_variance(const SearchRow* __restrict__ rows, const PlaneInfo* __restrict__ planes,
+                           const int64_t* __restrict__ leaf_offset,
+                           const uint16_t* __restrict__ leaf_len, int64_t nrows,
+                           const double* __restrict__ gtab, int32_t max_len, int32_t nw,
+                           const uint8_t* __restrict__ mask, const uint8_t* __restrict__ mask_or,
+                           double* __restrict__ var, float* __restrict__ inv,
+                           float* __restrict__ inv_or) {
+    const int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (g >= nrows)
+        return;
+    const SearchRow r   = rows[g];
+    const PlaneInfo pl  = planes[r.plane];
+    const int32_t nch   = static_cast<int32_t>(pl.chan_end - pl.chan_begin);
+    const uint16_t* len = leaf_len + leaf_offset[g];
+    double v[kMaxWidths], vo[kMaxWidths];
+    for (int w = 0; w < nw; ++w) {
+        v[w]  = 0.0;
+        vo[w] = 0.0;
+    }
+    for (int32_t c = 0; c < nch; ++c) {
+        const int L     = min(static_cast<int>(len[c]), max_len);
+        const bool on   = mask[pl.chan_begin + c] != 0;
+        const bool on_o = mask_or[pl.chan_begin + c] != 0;
+        if (!on && !on_o)
+            continue;
+        const double* gt = gtab + static_cast<int64_t>(L) * nw;
+        for (int w = 0; w < nw; ++w) {
+            if (on)
+                v[w] += gt[w];
+            if (on_o)
+                vo[w] += gt[w];
+        }
+    }
+    for (int w = 0; w < nw; ++w) {
+        var[g * nw + w]    = v[w];
+        inv[g * nw + w]    = v[w] > 0.0 ? static_cast<float>(1.0 / sqrt(v[w])) : 0.0F;
+        inv_or[g * nw + w] = vo[w] > 0.0 ? static_cast<float>(1.0 / sqrt(vo[w])) : 0.0F;
+    }
+}
+
+} // namespace
+
+void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1, cudaStream_t s) {
+    if (g1 <= g0 || p.n_valid <= 0)
+        return;
+    if (p.nwidths > kMaxWidths)
+        throw Error(FROST_ERR_INVALID_ARGUMENT, "search: more than 32 boxcar widths");
+    if (level.base < p.wmax)
+        throw Error(FROST_ERR_INTERNAL, "search: level history shorter than the widest boxcar");
+    const size_t smem = sizeof(float) * (kChunk + p.wmax);
+    const dim3 grid(static_cast<unsigned>(g1 - g0));
+    if (level.fp16) {
+        FB_CUDA(cudaFuncSetAttribute(k_search<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_search<__half><<<grid, kThreads, smem, s>>>(p, static_cast<const __half*>(level.data),
+                                                      level.pitch, level.base, g0);
+    } else {
+        FB_CUDA(cudaFuncSetAttribute(k_search<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_search<float><<<grid, kThreads, smem, s>>>(p, static_cast<const float*>(level.data),
+                                                     level.pitch, level.base, g0);
+    }
+    FB_LAUNCH_CHECK();
+}
+
+void launch_variance(const SearchRow* rows, const PlaneInfo* planes, const int64_t* leaf_offset,
+                     const uint16_t* leaf_len, int64_t nrows, const double* gtab, int32_t max_len,
+                     int32_t nwidths, const uint8_t* mask, const uint8_t* mask_or, double* var,
+                     float* inv_sigma, float* inv_sigma_or, cudaStream_t s) {
+    if (nrows == 0)
+        return;
+    if (nwidths > kMaxWidths)
+        throw Error(FROST_ERR_INVALID_ARGUMENT, "variance: more than 32 boxcar widths");
+    k_variance<<<static_cast<unsigned>((nrows + 127) / 128), 128, 0, s>>>(
+        rows, planes, leaf_offset, leaf_len, nrows, gtab, max_len, nwidths, mask, mask_or, var,
+        inv_sigma, inv_sigma_or);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_flush_runs(const SearchParams& p, int64_t nrows, cudaStream_t s) {
+    if (nrows == 0 || p.peak_mode == FROST_PEAK_ALL)
+        return;
+    k_flush<<<static_cast<unsigned>((nrows + 127) / 128), 128, 0, s>>>(p, nrows);
+    FB_LAUNCH_CHECK();
+}
+
+} // namespace fb::fdmt

@@ -1,0 +1,82 @@
+// Boxcar/trapezoid matched-filter search with exact per-DM/width noise and
+// run-based peak finding (search_kernels.cu).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime_api.h>
+
+#include "fdmt_kernels.hpp"
+#include "frost_b200.h"
+
+namespace fb::fdmt {
+
+/** One searched row: a DM trial of one plane. */
+struct SearchRow {
+    int64_t level_row; // row in its level buffer
+    int32_t plane;
+    int32_t prow;      // index in the plane's DM grid (dm_idx)
+    int32_t delay;     // warm-up samples of the row
+    float dm;
+};
+
+/** Per-plane constants copied into every candidate. */
+struct PlaneInfo {
+    float f_low, f_high;
+    uint32_t chan_begin, chan_end;
+    uint32_t subband_level, subband_idx;
+};
+
+/** Open above-threshold run carried across chunks, tiles and gulps. */
+struct RunState {
+    int32_t open;
+    int32_t best_w;
+    float best;
+    int32_t pad;
+    int64_t start;
+    int64_t best_t;
+    int64_t last_t;
+};
+
+struct SearchParams {
+    const SearchRow* rows;   // indexed by global searched-row g
+    const PlaneInfo* planes;
+    const int32_t* widths;
+    int32_t nwidths;
+    int32_t wmax;
+    float thresh;
+    int32_t peak_mode;       // enum frost_peak_mode
+    int32_t trapezoid;
+    int32_t skip_cold;
+    int32_t or_active;       // this gulp's mask differs from the previous one
+    int64_t tile_t0;         // absolute sample of tile column 0
+    int64_t gulp_t0;         // absolute sample of the gulp's first column
+    int32_t n_valid;         // valid columns in this tile
+    const float* inv_sigma;  // [g][nwidths]
+    const float* inv_sigma_or;
+    RunState* carry;         // [g][nwidths] (per width) or [g] (across widths)
+    frost_candidate* cands;
+    unsigned long long* ncands;
+    uint64_t max_cands;
+    uint32_t* row_counts;    // [g]
+    uint32_t max_per_dm;     // 0 = unlimited
+    unsigned long long* dropped; // [0] global, [1] per DM
+};
+
+/** Searches rows [g0, g1) (all in `level`) over the tile's valid columns. */
+void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1,
+                   cudaStream_t s);
+
+/** Exact variance of every searched row and width for `mask` and for
+ * `mask_or`: var = sum over active channels of g[L_c][w]; writes
+ * inv_sigma = 1/sqrt(var) (0 where var = 0) and the FP64 variances. */
+void launch_variance(const SearchRow* rows, const PlaneInfo* planes, const int64_t* leaf_offset,
+                     const uint16_t* leaf_len, int64_t nrows, const double* gtab,
+                     int32_t max_len, int32_t nwidths, const uint8_t* mask,
+                     const uint8_t* mask_or, double* var, float* inv_sigma, float* inv_sigma_or,
+                     cudaStream_t s);
+
+/** Emits every open run as a candidate and closes it (drain). */
+void launch_flush_runs(const SearchParams& p, int64_t nrows, cudaStream_t s);
+
+} // namespace fb::fdmt

@@ -1,0 +1,192 @@
+"""The streaming FDMT + boxcar search engine with dmt::FDMTBoxcar's call
+shape as frost uses it (lib/pipeline/pipeline.cpp:346-367, 493, 517,
+598-608), running on the GPU through the C ABI."""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, lib
+from .config import BoxcarConfig, DedispPlanConfig
+
+CANDIDATE_DTYPE = np.dtype([
+    ("peak_sample", np.uint64), ("begin_sample", np.uint64), ("end_sample", np.uint64),
+    ("snr", np.float32), ("dm", np.float32), ("f_low_mhz", np.float32), ("f_high_mhz", np.float32),
+    ("filter_idx", np.uint32), ("width", np.uint32), ("dm_idx", np.uint32),
+    ("chan_begin", np.uint32), ("chan_end", np.uint32), ("beam_idx", np.uint32),
+    ("subband_level", np.uint32), ("subband_idx", np.uint32)])
+
+
+@dataclass
+class SearchPlane:
+    """get_search_plans()[p] (tests/cpp/api/calibration_test.cpp:53-134)."""
+    subband_level: int
+    subband_idx: int
+    level: int
+    chan_begin: int
+    chan_end: int
+    staggered: bool
+    f_low: float
+    f_high: float
+    dm_grid: np.ndarray
+    warmup_samples: np.ndarray
+    widths: List[int]
+
+
+@dataclass
+class CandidateResult:
+    """CandidateResultView: candidates plus drop counters."""
+    candidates: np.ndarray
+    dropped_global: int
+    dropped_per_dm: int
+
+    def overflowed(self) -> bool:
+        return self.dropped_global > 0 or self.dropped_per_dm > 0
+
+
+def _boxcar_c(bc: BoxcarConfig, tile_nsamps: int = 0) -> _abi.BoxcarConfigC:
+    c = _abi.BoxcarConfigC()
+    c.max_boxcar = int(bc.max_boxcar)
+    c.wtsp = float(bc.wtsp)
+    c.use_trapezoid = int(bc.use_trapezoid)
+    c.detect_thresh = float(bc.detect_thresh)
+    c.noise_sigma = float(bc.noise_sigma)
+    c.peak_mode = int(bc.peak_mode)
+    c.max_candidates = int(bc.max_candidates)
+    c.max_cands_per_dm = int(bc.max_cands_per_dm)
+    c.skip_cold_prefix = int(bc.skip_cold_prefix)
+    c.input_nbits = 32
+    c.input_mean = 0.0
+    c.storage = int(bc.storage)
+    c.tile_nsamps = int(tile_nsamps)
+    return c
+
+
+class FDMTBoxcar:
+    """Streaming search of one beam. execute() takes the calibrated
+    [nchans][nsamps] float32 waterfall (low frequency first) as a host numpy
+    array or a device pointer, plus an optional per-gulp channel mask in FDMT
+    order (1 = keep)."""
+
+    def __init__(self, plan: DedispPlanConfig, cfg: BoxcarConfig, kill_mask=None,
+                 memory_budget: int = 0, device: int = 0, tile_nsamps: int = 0):
+        L = lib()
+        pc = plan.to_c()
+        bc = _boxcar_c(cfg, tile_nsamps)
+        km = None
+        if kill_mask is not None:
+            km = np.ascontiguousarray(kill_mask, np.uint8)
+            if km.size != plan.nchans:
+                raise ValueError("kill_mask must have nchans entries")
+        h = C.c_void_p()
+        check(L.frost_search_create(C.byref(pc), C.byref(bc),
+                                    km.ctypes.data_as(C.POINTER(C.c_uint8)) if km is not None else None,
+                                    memory_budget, device, C.byref(h)))
+        self._h = h
+        self.plan_config = plan
+        self.config = cfg
+        self.nchans = plan.nchans
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().frost_search_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _mask_ptr(self, mask):
+        if mask is None or (hasattr(mask, "__len__") and len(mask) == 0):
+            return None, None
+        m = np.ascontiguousarray(mask, np.uint8)
+        if m.size != self.nchans:
+            raise ValueError("mask must have nchans entries")
+        return m, m.ctypes.data_as(C.POINTER(C.c_uint8))
+
+    def execute(self, waterfall: np.ndarray, mask=None) -> CandidateResult:
+        wf = np.ascontiguousarray(waterfall, np.float32)
+        if wf.ndim != 2 or wf.shape[0] != self.nchans:
+            raise ValueError("waterfall must be [nchans][nsamps]")
+        keep, mp = self._mask_ptr(mask)
+        check(lib().frost_search_execute(self._h, wf.ctypes.data_as(C.POINTER(C.c_float)),
+                                         wf.shape[1], 0, mp, None))
+        return self.result()
+
+    def execute_device(self, ptr: int, nsamps: int, mask=None, stream: Optional[int] = None):
+        keep, mp = self._mask_ptr(mask)
+        check(lib().frost_search_execute(self._h, C.cast(C.c_void_p(ptr), C.POINTER(C.c_float)),
+                                         nsamps, 1, mp, C.c_void_p(stream) if stream else None))
+        return self.result()
+
+    def drain(self) -> CandidateResult:
+        check(lib().frost_search_drain(self._h))
+        return self.result()
+
+    def result(self) -> CandidateResult:
+        n, dg, dd = C.c_size_t(), C.c_uint64(), C.c_uint64()
+        check(lib().frost_search_result_count(self._h, C.byref(n), C.byref(dg), C.byref(dd)))
+        out = np.zeros(n.value, CANDIDATE_DTYPE)
+        if n.value:
+            check(lib().frost_search_results(self._h, out.ctypes.data_as(C.POINTER(_abi.CandidateC)),
+                                             n.value, C.byref(n)))
+        return CandidateResult(out, dg.value, dd.value)
+
+    def get_candidate_frontier(self) -> int:
+        v = C.c_uint64()
+        check(lib().frost_search_frontier(self._h, C.byref(v)))
+        return v.value
+
+    def info(self) -> dict:
+        i = _abi.SearchInfoC()
+        check(lib().frost_search_get_info(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in i._fields_}
+
+    def widths(self) -> List[int]:
+        n = C.c_size_t()
+        check(lib().frost_search_widths(self._h, None, 0, C.byref(n)))
+        out = (C.c_uint32 * max(n.value, 1))()
+        check(lib().frost_search_widths(self._h, out, n.value, C.byref(n)))
+        return [int(out[i]) for i in range(n.value)]
+
+    def get_search_plans(self) -> List[SearchPlane]:
+        info = self.info()
+        ws = self.widths()
+        planes = []
+        for p in range(info["nplanes"]):
+            pi = _abi.SearchPlaneC()
+            check(lib().frost_search_plane_info(self._h, p, C.byref(pi), None, None))
+            dm = np.zeros(pi.ndm, np.float32)
+            warm = np.zeros(pi.ndm, np.uint32)
+            check(lib().frost_search_plane_info(self._h, p, C.byref(pi),
+                                                dm.ctypes.data_as(C.POINTER(C.c_float)),
+                                                warm.ctypes.data_as(C.POINTER(C.c_uint32))))
+            planes.append(SearchPlane(pi.subband_level, pi.subband_idx, pi.level, pi.chan_begin,
+                                      pi.chan_end, bool(pi.staggered), pi.f_low, pi.f_high, dm,
+                                      warm, ws))
+        return planes
+
+    def get_subband_variance_grid(self, plane: int, width: int, mask=None) -> np.ndarray:
+        ndm = self.get_search_plans()[plane].dm_grid.size
+        out = np.zeros(ndm, np.float64)
+        keep, mp = self._mask_ptr(mask)
+        check(lib().frost_search_variance_grid(self._h, plane, width, mp,
+                                               out.ctypes.data_as(C.POINTER(C.c_double)), ndm))
+        return out
+
+    def capture_planes(self, enable: bool = True):
+        check(lib().frost_search_capture_planes(self._h, int(enable)))
+
+    def plane_data(self, plane: int, nsamps: int) -> np.ndarray:
+        ndm = self.get_search_plans()[plane].dm_grid.size
+        out = np.zeros((ndm, nsamps), np.float32)
+        check(lib().frost_search_plane_data(self._h, plane, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                            out.size))
+        return out

@@ -262,6 +262,174 @@ int frost_fdmt_band_edges(const frost_dedisp_plan_config* cfg,
                           float* f_min,
                           float* f_max);
 
+/* ---- search engine: streaming FDMT + boxcar (replaces dmt::FDMTBoxcar) -- */
+
+/* dmt::PeakFindingMode as frost exposes it (docs/user_guide/search.md:43-49). */
+enum frost_peak_mode {
+    FROST_PEAK_PER_WIDTH     = 0, /* one peak per above-threshold run, per width */
+    FROST_PEAK_ACROSS_WIDTHS = 1, /* one peak per run over all widths together */
+    FROST_PEAK_ALL           = 2  /* every sample above threshold */
+};
+
+/* Storage of the FDMT intermediate planes (arithmetic is always float). */
+enum frost_storage { FROST_STORAGE_FP32 = 0, FROST_STORAGE_FP16 = 1 };
+
+/* dmt::BoxcarConfig as frost fills it (lib/pipeline/pipeline.cpp:316-330),
+ * plus this engine's storage precision and time-tile length (0 = the whole
+ * gulp, else a multiple of 2048 samples that bounds device memory). */
+typedef struct {
+    uint64_t max_boxcar;
+    float wtsp;
+    int32_t use_trapezoid;
+    float detect_thresh;
+    float noise_sigma;
+    int32_t peak_mode;         /* enum frost_peak_mode */
+    uint64_t max_candidates;   /* per execute call, over all planes */
+    uint64_t max_cands_per_dm; /* per plane and DM trial; 0 = unlimited */
+    int32_t skip_cold_prefix;
+    int32_t input_nbits;       /* 32: float input */
+    float input_mean;
+    int32_t storage;           /* enum frost_storage */
+    uint64_t tile_nsamps;
+} frost_boxcar_config;
+
+/* One detection (the RawCandidate fields frost reads,
+ * lib/search/postprocess.cpp:79-116). Samples are absolute stream indices,
+ * referenced to the bottom (lowest frequency) of the plane's band;
+ * [begin, end] is the above-threshold run; channels are in FDMT (ascending
+ * frequency) order, end exclusive. */
+typedef struct {
+    uint64_t peak_sample;
+    uint64_t begin_sample;
+    uint64_t end_sample;
+    float snr;
+    float dm;
+    float f_low_mhz;
+    float f_high_mhz;
+    uint32_t filter_idx;
+    uint32_t width;
+    uint32_t dm_idx;
+    uint32_t chan_begin;
+    uint32_t chan_end;
+    uint32_t beam_idx;
+    uint32_t subband_level;
+    uint32_t subband_idx;
+} frost_candidate;
+
+/* Plan-level facts (FDMTPlan queries used at lib/pipeline/pipeline.cpp:405,
+ * 433-436). */
+typedef struct {
+    uint64_t nchans;
+    uint64_t block_nsamps;
+    uint64_t tile_nsamps;
+    uint64_t dt_max;
+    uint64_t ndm;          /* full-band DM trials */
+    uint64_t nplanes;
+    uint64_t nwidths;
+    uint64_t levels;
+    uint64_t device_bytes; /* device memory held by the engine */
+    double f_min;
+    double f_max;
+} frost_search_info;
+
+/* One search plane (get_search_plans()[p], tests/cpp/api/calibration_test.cpp:
+ * 53-134). */
+typedef struct {
+    uint32_t subband_level;
+    uint32_t subband_idx;
+    uint32_t level;        /* FDMT height of the plane's node */
+    uint32_t chan_begin;
+    uint32_t chan_end;
+    uint32_t staggered;
+    uint64_t ndm;
+    double f_low;
+    double f_high;
+} frost_search_plane;
+
+typedef struct frost_search frost_search;
+
+/* FDMTBoxcar(plan, BoxcarConfig, ..., memory budget, kill mask)
+ * (lib/pipeline/pipeline.cpp:346-367). `kill_mask` has nchans entries in
+ * FDMT order, 1 = keep, 0 = killed; NULL keeps every channel. Fails with
+ * FROST_ERR_OUT_OF_MEMORY when the plan cannot fit in `memory_budget` bytes
+ * (0 = no limit) at any tile length. */
+int frost_search_create(const frost_dedisp_plan_config* plan,
+                        const frost_boxcar_config* cfg,
+                        const uint8_t* kill_mask,
+                        size_t memory_budget,
+                        int device,
+                        frost_search** out);
+
+int frost_search_destroy(frost_search* s);
+
+/* FDMTBoxcar::execute (host span: lib/pipeline/pipeline.cpp:608; device
+ * span + copy_result: :603-605). `waterfall` is [nchans][nsamps] float32,
+ * low frequency first, nsamps <= block_nsamps, on the device when
+ * `on_device` else host memory. `mask` (nchans bytes, FDMT order) replaces
+ * the constructor mask for this and later calls; NULL keeps the current one.
+ * Results are complete when the call returns. */
+int frost_search_execute(frost_search* s,
+                         const float* waterfall,
+                         size_t nsamps,
+                         int on_device,
+                         const uint8_t* mask,
+                         void* stream);
+
+/* FDMTBoxcar::drain (lib/pipeline/pipeline.cpp:517): closes every open
+ * above-threshold run; its peaks become the current results. */
+int frost_search_drain(frost_search* s);
+
+/* CandidateResultView of the last execute/drain: count and drop counters. */
+int frost_search_result_count(const frost_search* s,
+                              size_t* count,
+                              uint64_t* dropped_global,
+                              uint64_t* dropped_per_dm);
+
+/* Copies the last results, sorted by (plane, dm_idx, peak_sample, width). */
+int frost_search_results(const frost_search* s,
+                         frost_candidate* out,
+                         size_t capacity,
+                         size_t* count);
+
+/* get_candidate_frontier (lib/pipeline/pipeline.cpp:493): the earliest
+ * absolute sample a later call can still report a peak at. */
+int frost_search_frontier(const frost_search* s, uint64_t* sample);
+
+int frost_search_get_info(const frost_search* s, frost_search_info* out);
+
+/* Plane p's facts; `dm_grid` and `warmup` (ndm entries each) may be NULL. */
+int frost_search_plane_info(const frost_search* s,
+                            size_t plane,
+                            frost_search_plane* out,
+                            float* dm_grid,
+                            uint32_t* warmup);
+
+/* Boxcar widths (shared by all planes). */
+int frost_search_widths(const frost_search* s,
+                        uint32_t* out,
+                        size_t capacity,
+                        size_t* count);
+
+/* get_subband_variance_grid (tests/cpp/api/calibration_test.cpp:105-106):
+ * exact FP64 noise variance of every DM row of `plane` at `width` for
+ * `mask` (FDMT order; NULL = current mask). */
+int frost_search_variance_grid(const frost_search* s,
+                               size_t plane,
+                               uint32_t width,
+                               const uint8_t* mask,
+                               double* out,
+                               size_t capacity);
+
+/* Keeps a float copy of every plane's DM-time rows of the next execute
+ * calls (for checks against the FP64 oracle; costs memory and time). */
+int frost_search_capture_planes(frost_search* s, int enable);
+
+/* Copies plane p's captured rows of the last execute: [ndm][nsamps]. */
+int frost_search_plane_data(const frost_search* s,
+                            size_t plane,
+                            float* out,
+                            size_t capacity);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

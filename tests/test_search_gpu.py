@@ -1,0 +1,153 @@
+"""GPU parity of the streaming FDMT + boxcar search against the FP64 oracle
+(oracle/fdmt_oracle.c): DM-time planes within 1e-5 of each row's RMS (FP32
+storage), candidate plane/DM/width/peak indices identical and S/N within
+1e-3 for every peak clear of the threshold; FP16 storage recovers the same
+candidates above S/N 7 with its S/N error stated; noise S/N is unit in every
+plane; tiling, masks, drain and the peak modes keep the same answers."""
+
+import numpy as np
+import pytest
+
+from frost_b200.config import BoxcarConfig, PeakMode, Storage
+from frost_b200.dedisp import band_edges, generate_dm_list
+from oracle.fdmt import Oracle
+from tests.search_cases import compare, make_stream, plan_config, run_engine
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_for(pc, bc):
+    f_min, f_max = band_edges(pc)
+    return Oracle(pc.nchans, f_min, f_max, pc.dt, generate_dm_list(pc), pc.subband_depth,
+                  bc.max_boxcar, bc.wtsp, bc.use_trapezoid, bc.detect_thresh, int(bc.peak_mode),
+                  bc.skip_cold_prefix)
+
+
+PULSES = ((1500, 20.0, 3.0, 1.2), (5000, 45.0, 8.0, 0.5), (9300, 5.0, 1.0, 2.5),
+          (8190, 33.0, 4.0, 0.8))  # the last straddles the gulp boundary at 8192
+
+
+@pytest.mark.parametrize("depth", [0, 2])
+def test_planes_and_candidates_match_oracle(depth):
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=depth)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0)
+    stream = make_stream(pc, 3, seed=7 + depth, pulses=PULSES)
+    eng = FDMTBoxcar(pc, bc)
+    eng.capture_planes(True)
+    orc = oracle_for(pc, bc)
+    gulp = pc.block_nsamps
+    # planes of the last gulp vs the oracle's rows over the whole stream
+    cands = run_engine(eng, stream, gulp, drain=False)
+    planes = eng.get_search_plans()
+    assert len(planes) == (1 if depth == 0 else 11)
+    for p, band in enumerate(orc.bands):
+        assert (planes[p].chan_begin, planes[p].chan_end) == (band.a, band.b)
+        assert np.array_equal(planes[p].warmup_samples, band.delays)
+        rows = orc.dedisperse(stream, band)[:, -gulp:]
+        mine = eng.plane_data(p, gulp)
+        rms = np.sqrt(np.mean(rows ** 2, axis=1, keepdims=True)) + 1e-12
+        err = np.max(np.abs(mine - rows) / rms)
+        assert err < 1e-5, (p, err)
+    cands = np.concatenate([cands, eng.drain().candidates])
+    ref = orc.search(stream, gulp, [np.ones(pc.nchans, np.uint8)] * 3)
+    n, missing, extra, bad = compare(cands, ref, bc.detect_thresh)
+    assert n > 10
+    assert not missing and not extra and not bad, (missing[:5], extra[:5], bad[:5])
+
+
+def test_tiles_and_peak_modes_match():
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=1)
+    stream = make_stream(pc, 2, seed=11, pulses=PULSES)
+    for mode in (PeakMode.PER_WIDTH, PeakMode.ACROSS_WIDTHS, PeakMode.ALL):
+        bc = BoxcarConfig(max_boxcar=16, detect_thresh=7.0, peak_mode=mode, use_trapezoid=True)
+        whole = run_engine(FDMTBoxcar(pc, bc), stream, pc.block_nsamps)
+        tiled = run_engine(FDMTBoxcar(pc, bc, tile_nsamps=2048), stream, pc.block_nsamps)
+        assert np.array_equal(whole, tiled), mode
+        ref = oracle_for(pc, bc).search(stream, pc.block_nsamps, [np.ones(pc.nchans, np.uint8)] * 2)
+        n, missing, extra, bad = compare(whole, ref, bc.detect_thresh)
+        assert n > 0 and not missing and not extra and not bad, (mode, missing[:3], extra[:3], bad[:3])
+
+
+def test_changing_masks_use_or_variance():
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=2)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0)
+    stream = make_stream(pc, 3, seed=5, pulses=PULSES)
+    rng = np.random.default_rng(3)
+    masks = [(rng.random(pc.nchans) > p).astype(np.uint8) for p in (0.0, 0.2, 0.2)]
+    masks[2][:8] = 0
+    masked = stream.copy()
+    for g, m in enumerate(masks):
+        masked[:, g * pc.block_nsamps:(g + 1) * pc.block_nsamps] *= m[:, None]
+    cands = run_engine(FDMTBoxcar(pc, bc), stream, pc.block_nsamps, masks=masks)
+    ref = oracle_for(pc, bc).search(masked, pc.block_nsamps, masks)
+    n, missing, extra, bad = compare(cands, ref, bc.detect_thresh)
+    assert n > 0 and not missing and not extra and not bad, (missing[:3], extra[:3], bad[:3])
+
+
+def test_fp16_storage_recovers_candidates_above_7():
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=2)
+    bc32 = BoxcarConfig(max_boxcar=16, detect_thresh=6.0)
+    bc16 = BoxcarConfig(max_boxcar=16, detect_thresh=6.0, storage=Storage.FP16)
+    stream = make_stream(pc, 2, seed=21, pulses=PULSES)
+    e32, e16 = FDMTBoxcar(pc, bc32), FDMTBoxcar(pc, bc16)
+    e16.capture_planes(True)
+    c32 = run_engine(e32, stream, pc.block_nsamps)
+    c16 = run_engine(e16, stream, pc.block_nsamps)
+    orc = oracle_for(pc, bc32)
+    worst = 0.0
+    for p, band in enumerate(orc.bands):
+        rows = orc.dedisperse(stream, band)[:, -pc.block_nsamps:]
+        rms = np.sqrt(np.mean(rows ** 2, axis=1, keepdims=True)) + 1e-12
+        worst = max(worst, float(np.max(np.abs(e16.plane_data(p, pc.block_nsamps) - rows) / rms)))
+    assert worst < 5e-3, worst
+    strong = lambda cs: {(c["subband_level"], c["subband_idx"], c["dm_idx"], c["filter_idx"],
+                          c["peak_sample"]): float(c["snr"]) for c in cs if c["snr"] >= 7.0}
+    s32, s16 = strong(c32), strong(c16)
+    common = set(s32) & set(s16)
+    # same list above 7 except peaks whose S/N sits within the FP16 error of 7
+    diff = [k for k in set(s32) ^ set(s16) if abs(s32.get(k, s16.get(k)) - 7.0) > 0.05]
+    assert not diff, diff[:5]
+    err = max(abs(s32[k] - s16[k]) / s32[k] for k in common)
+    assert err < 1e-2, err
+
+
+def test_unit_noise_snr_in_every_plane():
+    """calibration_test.cpp:159-168 on the GPU engine: S/N of pure noise has
+    sigma 1 +- 0.15 per plane and width (all-sample peak mode, threshold -inf
+    equivalent via a low threshold on a short stream)."""
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=2, gulp=8192)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=-1e30, peak_mode=PeakMode.ALL,
+                      max_candidates=1 << 26, max_cands_per_dm=0)
+    stream = make_stream(pc, 1, seed=0xCA11B)
+    eng = FDMTBoxcar(pc, bc)
+    res = eng.execute(stream)
+    c = res.candidates
+    assert not res.overflowed()
+    for lvl, idx in {(int(a), int(b)) for a, b in zip(c["subband_level"], c["subband_idx"])}:
+        for fi in np.unique(c["filter_idx"]):
+            s = c["snr"][(c["subband_level"] == lvl) & (c["subband_idx"] == idx) & (c["filter_idx"] == fi)]
+            assert abs(float(np.mean(s))) < 0.15 and abs(float(np.std(s)) - 1.0) < 0.15, (lvl, idx, fi)
+
+
+def test_variance_grid_matches_oracle_and_errors():
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=2)
+    bc = BoxcarConfig(max_boxcar=16, use_trapezoid=True)
+    eng = FDMTBoxcar(pc, bc)
+    orc = oracle_for(pc, bc)
+    mask = (np.arange(pc.nchans) % 3 != 0).astype(np.uint8)
+    for p, band in enumerate(orc.bands):
+        for W in (1, 4, 16):
+            assert np.allclose(eng.get_subband_variance_grid(p, W, mask), orc.variance(band, mask, W),
+                               rtol=1e-12)
+    with pytest.raises(ValueError):
+        FDMTBoxcar(plan_config(gulp=256), bc)  # gulp must exceed dt_max + boxcar_max
+    with pytest.raises(ValueError):
+        eng.execute(np.zeros((pc.nchans, pc.block_nsamps + 1), np.float32))
+    info = eng.info()
+    assert info["nplanes"] == 11 and info["dt_max"] > 0
