@@ -1,0 +1,364 @@
+#!/usr/bin/env python3
+"""Benchmark of the per-gulp search path at the 4096-channel, DM 0-2000
+workload: beam-seconds searched per second (whole job), p50/p99 gulp
+latency, FP16-storage vs plain FP32, end-to-end through the public API,
+the FDMT level kernels' HBM roofline, and the CPU baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl frost|reference]
+
+A step is one 262144-sample gulp of one beam through RFI excision (moments,
+IQRM, Kadane along time and frequency, zero-DM subtract, narrow/broad-band
+neighbour fills) -> normalisation -> streaming FDMT -> boxcar search of 11
+sub-band planes (widths 1-256). Each rank streams its own beam (replicas,
+weak scaling; no collective is needed: beams are independent). Inputs are
+seeded synthetic filterbanks with the workload's noise, RFI and pulse
+recipe; every step reads a 1 GiB raw gulp and writes/reads multi-GiB
+planes, so inputs exceed the 126 MB L2 without a flush.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "beam-s searched/s @4096ch DM2000"
+UNIT = "beam-s/s"
+NCHANS, GULP, TSAMP = 4096, 262144, 64e-6
+FCH1, FOFF = 1535.958984375, -0.08203125
+DM_MAX, MAX_BOXCAR, DEPTH = 2000.0, 256, 2
+WORKLOAD = ("4096ch 1200-1536MHz 64us uint8, 262144-sample gulps, DM 0-2000 (3625 trials), "
+            "boxcar 1-256, 11 sub-band planes, moments+IQRM+Kadane(time,freq)+zero-DM RFI")
+
+
+def rfi_config():
+    from frost_b200.config import RfiConfig, ZeroDMMode
+    cfg = RfiConfig()
+    cfg.moments.enabled = True
+    cfg.iqrm.enabled = True
+    cfg.kadane_channel.enabled = True
+    cfg.kadane_spectrum.enabled = True
+    cfg.zero_dm = ZeroDMMode.SUBTRACT
+    return cfg
+
+
+def layout(nsamps=GULP):
+    from frost_b200.config import BlockLayout, DataType
+    return BlockLayout(NCHANS, nsamps, DataType.UINT8, TSAMP, FCH1, FOFF)
+
+
+def search_config(storage):
+    from frost_b200.config import BoxcarConfig
+    return BoxcarConfig(max_boxcar=MAX_BOXCAR, wtsp=2.0, detect_thresh=6.0, storage=storage)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.lines, self.proc = device, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """Level-kernel DRAM bytes per launch from the committed ncu summary,
+    scaled to the full gulp (profiles/fdmt_level_config2.md), or None."""
+    path = os.path.join(ROOT, "profiles", "fdmt_level_config2.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch_full_gulp")
+    except (OSError, ValueError):
+        return None
+
+
+def make_gulp(seed):
+    from frost_b200.synth import config2_gulp
+    return config2_gulp(seed=seed).data  # [T][C] uint8
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    from frost_b200.config import Storage
+    from frost_b200.pipeline import GulpPipeline, plan_for
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+
+    raw_host = make_gulp(0x46524F5354 ^ rank)
+    nbytes = raw_host.size
+    raw_dev = torch.from_numpy(raw_host.reshape(-1)).to(dev)
+    pinned = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    pinned.copy_(torch.from_numpy(raw_host.reshape(-1)))
+    del raw_host
+    lay = layout()
+    plan = plan_for(lay, 0.0, DM_MAX, DEPTH)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def measure(storage, e2e=False, sample_clocks=False):
+        pipe = GulpPipeline(rfi_config(), lay, 2.0, plan, search_config(storage), device=local)
+        step = (lambda: pipe.execute_device(pinned.data_ptr(), GULP, on_device=False)) if e2e else \
+               (lambda: pipe.execute_device(raw_dev.data_ptr(), GULP, on_device=True))
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        pipe.search.enable_timing(True)
+        l0 = pipe.rfi.launches()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        ncands, d2h = 0, 0
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.__enter__()
+        torch.cuda.synchronize()
+        starts[0].record()
+        for i in range(args.steps):
+            res = step()
+            ncands += res.candidates.size
+            d2h += res.candidates.nbytes
+            starts[i + 1].record()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.__exit__(None, None, None)
+        barrier()
+        lat = [starts[i].elapsed_time(starts[i + 1]) for i in range(args.steps)]
+        total_ms = starts[0].elapsed_time(starts[-1])
+        timing = pipe.search.timing()
+        launches = timing["total_launches"] + (pipe.rfi.launches() - l0)
+        out = {"total_ms": max_over_ranks(total_ms), "lat": lat, "timing": timing,
+               "launches": launches, "ncands": ncands, "d2h": d2h,
+               "clocks": sampler.summary() if sampler else None,
+               "rfi_report": pipe.rfi.report(), "device_bytes": pipe.search.info()["device_bytes"]}
+        del pipe
+        torch.cuda.empty_cache()
+        return out
+
+    fp16 = measure(Storage.FP16, sample_clocks=True)
+    fp32 = measure(Storage.FP32)
+    e2e = measure(Storage.FP16, e2e=True)
+
+    beam_s = args.steps * GULP * TSAMP * world
+    value = beam_s / (fp16["total_ms"] / 1e3)
+    t = fp16["timing"]
+    peak, peak_kind = measured_peaks()
+    level_gbs = t["algorithmic_level_bytes"] / (t["level_ms"] / 1e3) / 1e9 if t["level_ms"] else 0.0
+    traffic = ncu_traffic_per_launch()
+    roofline = {
+        "bound": "hbm",
+        "kernel": "k_level<__half> (FDMT levels 2-12)",
+        "achieved": round(level_gbs, 1),
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": round(level_gbs / peak, 4),
+        "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
+        "traffic": traffic,
+        "algorithmic_bytes_per_launch": int(t["algorithmic_level_bytes"] / max(t["level_launches"], 1)),
+        "launches": int(t["level_launches"]),
+        "phase_ms_per_step": {k: round(t[k] / args.steps, 3) for k in
+                              ("level1_ms", "level_ms", "search_ms", "history_ms", "variance_ms")},
+    }
+    lat = sorted(fp16["lat"])
+    p = lambda q: lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(fp16["total_ms"] / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (fp16 plane storage)",
+        "data": "synthetic (seeded filterbank, config-2 noise/RFI/pulse recipe)",
+        "config": {"workload": WORKLOAD, "storage": "fp16", "beams_per_gpu": 1,
+                   "l2": "inputs larger than L2 (1 GiB raw gulp per step)",
+                   "parallelism": f"replicas x{world}"},
+        "latency_ms": {"p50": round(p(0.5), 2), "p99": round(p(0.99), 2),
+                       "realtime_gulp_ms": GULP * TSAMP * 1e3},
+        "plain_fp32": {"value": round(beam_s / (fp32["total_ms"] / 1e3), 3),
+                       "ms_per_step": round(fp32["total_ms"] / args.steps, 3)},
+        "e2e": {"value": round(beam_s / (e2e["total_ms"] / 1e3), 3), "unit": UNIT,
+                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": int(e2e["d2h"] / args.steps)},
+        "gpu_launches": int(fp16["launches"]),
+        "roofline": roofline,
+        "clocks": fp16["clocks"],
+        "candidates_per_step": round(fp16["ncands"] / args.steps, 1),
+        "device_bytes": fp16["device_bytes"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+CPU_SAMPLE = 16384  # rows of the gulp timed on the host cores
+
+
+def cpu_baseline(sample=CPU_SAMPLE, steps=1):
+    """The reference's CPU RFI cleaner (oracle/_ref, shipped -O3 -ffast-math
+    build) plus this project's CPU port of the FDMT + boxcar search
+    (oracle/cpu_fdmt.c; the reference's own engine, dmt, is not available)
+    on a `sample`-row block of the same recipe; beam-s/s of that work."""
+    from frost_b200.dedisp import band_edges, generate_dm_list
+    from frost_b200.pipeline import plan_for
+    from frost_b200.synth import config2_gulp
+    from oracle import ref
+    from oracle.fdmt import cpu_search, widths
+
+    raw = config2_gulp(seed=0x46524F5354, nsamps=sample, n_pulses=2).data
+    lay = layout(sample)
+    plan = plan_for(layout(), 0.0, DM_MAX, DEPTH)
+    f_min, f_max = band_edges(plan)
+    dms = generate_dm_list(plan)
+    ws = widths(MAX_BOXCAR, 2.0)
+    fast = ref.available(fast=True)
+    cleaner = ref.RefRFICleaner(rfi_config(), lay, 2.0, fast=fast)
+    t_rfi = t_fdmt = 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        wf = cleaner.execute_normalized(raw.reshape(-1))
+        t1 = time.perf_counter()
+        cpu_search(wf, f_min, f_max, TSAMP, dms, DEPTH, ws, 6.0)
+        t2 = time.perf_counter()
+        t_rfi += t1 - t0
+        t_fdmt += t2 - t1
+    beam_s = steps * sample * TSAMP
+    return {"value": round(beam_s / (t_rfi + t_fdmt), 4), "unit": UNIT,
+            "cores": os.cpu_count(), "kind": "port",
+            "sample": (f"{steps} x {sample} rows x 4096 ch: reference RFICleaner "
+                       f"({'shipped -ffast-math' if fast else 'strict'} build of its own sources) "
+                       f"{t_rfi:.2f} s + CPU port of FDMT+boxcar (11 planes, widths 1-256, zero "
+                       f"history) {t_fdmt:.2f} s; OpenMP threads={os.cpu_count()}")}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    if args.warmup > 0:
+        cpu_baseline(steps=1)
+    cb = cpu_baseline(steps=args.steps)
+    value = cb["value"]
+    total = args.steps * CPU_SAMPLE * TSAMP / value
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * total / args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD + f"; each step a {CPU_SAMPLE}-row sample",
+                       "parallelism": "host cores"},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": os.cpu_count(),
+                             "kind": "port", "sample": cb["sample"] if cb else ""},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["frost", "reference"], default="frost")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "frost":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -187,6 +187,23 @@ class SearchPlaneC(C.Structure):
     ]
 
 
+class SearchTimingC(C.Structure):
+    _fields_ = [
+        ("level1_ms", C.c_double),
+        ("level_ms", C.c_double),
+        ("search_ms", C.c_double),
+        ("history_ms", C.c_double),
+        ("variance_ms", C.c_double),
+        ("level_launches", C.c_uint64),
+        ("search_launches", C.c_uint64),
+        ("total_launches", C.c_uint64),
+        ("algorithmic_level_bytes", C.c_uint64),
+        ("algorithmic_level1_bytes", C.c_uint64),
+        ("algorithmic_search_bytes", C.c_uint64),
+        ("executes", C.c_uint64),
+    ]
+
+
 class DedispPlanConfigC(C.Structure):
     _fields_ = [
         ("nchans", C.c_uint64),

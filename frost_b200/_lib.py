@@ -40,6 +40,7 @@ SIGNATURES = {
     "frost_rfi_get_report": (C.c_int, [_vp, C.POINTER(_abi.RfiReportC)]),
     "frost_rfi_time_flags": (C.c_int, [_vp, _u8p, _sz]),
     "frost_rfi_memory_usage": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "frost_rfi_launch_count": (C.c_int, [_vp, C.POINTER(_u64)]),
     "frost_iqrm_mask": (C.c_int, [_f32p, _sz, _u64, C.c_float, _u8p, _u8p]),
     "frost_apply_manual_killmask": (C.c_int, [_u8p, _sz, C.POINTER(_abi.ChannelRange), _sz]),
     "frost_read_kill_file": (C.c_int, [C.c_char_p, _sz, C.POINTER(_abi.ChannelRange), _sz,
@@ -61,6 +62,8 @@ SIGNATURES = {
     "frost_search_variance_grid": (C.c_int, [_vp, _sz, C.c_uint32, _u8p, C.POINTER(C.c_double), _sz]),
     "frost_search_capture_planes": (C.c_int, [_vp, C.c_int]),
     "frost_search_plane_data": (C.c_int, [_vp, _sz, _f32p, _sz]),
+    "frost_search_enable_timing": (C.c_int, [_vp, C.c_int]),
+    "frost_search_get_timing": (C.c_int, [_vp, C.POINTER(_abi.SearchTimingC)]),
 }
 
 

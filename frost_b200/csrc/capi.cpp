@@ -166,6 +166,14 @@ int frost_rfi_memory_usage(const frost_rfi* rfi, size_t* bytes) {
     });
 }
 
+int frost_rfi_launch_count(const frost_rfi* rfi, uint64_t* launches) {
+    return guarded([&] {
+        if (rfi == nullptr || launches == nullptr)
+            invalid("frost_rfi_launch_count: null argument");
+        *launches = rfi->impl.launches();
+    });
+}
+
 int frost_iqrm_mask(const float* x, size_t n, uint64_t radius, float threshold,
                     const uint8_t* ignore, uint8_t* out) {
     return guarded([&] {
@@ -369,6 +377,22 @@ int frost_search_capture_planes(frost_search* s, int enable) {
         if (s == nullptr)
             invalid("frost_search_capture_planes: null handle");
         s->impl.capture(enable != 0);
+    });
+}
+
+int frost_search_enable_timing(frost_search* s, int enable) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_enable_timing: null handle");
+        s->impl.enable_timing(enable != 0);
+    });
+}
+
+int frost_search_get_timing(const frost_search* s, frost_search_timing* out) {
+    return guarded([&] {
+        if (s == nullptr || out == nullptr)
+            invalid("frost_search_get_timing: null argument");
+        *out = s->impl.timing();
     });
 }
 

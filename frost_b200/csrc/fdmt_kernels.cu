@@ -31,7 +31,11 @@ template <> __device__ __forceinline__ float ld<__half>(const __half* p) { retur
 
 template <class S> __device__ __forceinline__ void st(S* p, float v);
 template <> __device__ __forceinline__ void st<float>(float* p, float v) { *p = v; }
-template <> __device__ __forceinline__ void st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
+// FP16 storage saturates at the largest finite half instead of overflowing
+// to infinity (a strong unexcised burst must not poison a whole DM row).
+template <> __device__ __forceinline__ void st<__half>(__half* p, float v) {
+    *p = __float2half_rn(fminf(fmaxf(v, -65504.0F), 65504.0F));
+}
 
 // Inclusive block scan of smem[0..n) in place (float), n <= kThreads * 64.
 __device__ void block_scan(float* a, int n) {

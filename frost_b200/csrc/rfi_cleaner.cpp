@@ -360,6 +360,11 @@ const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, S
     cudaStream_t s = stream != nullptr ? stream : m_stream;
     ensure_capacity(capacity, valid);
     m_capacity = capacity;
+    struct CountLaunches {
+        uint64_t& total;
+        uint64_t before = launch_counter();
+        ~CountLaunches() { total += launch_counter() - before; }
+    } counting{m_launches};
 
     // Raw block on the device.
     const uint8_t* raw = block;

@@ -52,8 +52,10 @@ public:
     int device() const { return m_device; }
     cudaStream_t stream() const { return m_stream; }
     SizeType memory_usage() const;
+    uint64_t launches() const { return m_launches; }
 
 private:
+    uint64_t m_launches = 0;
     Config m_cfg;
     frost_block_layout m_layout;
     int m_device;

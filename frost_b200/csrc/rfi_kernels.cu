@@ -16,6 +16,7 @@
 // raw block is what every statistics pass reads from HBM.
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cstdint>
 #include <cstring>
@@ -817,7 +818,17 @@ __global__ void k_normalize_short(Dims d, ApplyParams p, const float* __restrict
 
 unsigned grid1(uint64_t n, unsigned block) { return static_cast<unsigned>((n + block - 1) / block); }
 
+std::atomic<uint64_t> g_launches{0};
+
 } // namespace
+
+#define FB_COUNT_LAUNCH()                                                                         \
+    do {                                                                                          \
+        FB_LAUNCH_CHECK();                                                                        \
+        g_launches.fetch_add(1, std::memory_order_relaxed);                                       \
+    } while (0)
+
+uint64_t launch_counter() { return g_launches.load(std::memory_order_relaxed); }
 
 // ---- launchers ----------------------------------------------------------------
 
@@ -827,27 +838,27 @@ void launch_check_finite(const uint8_t* raw, uint64_t nwords, unsigned long long
         return;
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((nwords + 255) / 256, 148 * 16));
     k_check_finite<<<blocks, 256, 0, s>>>(reinterpret_cast<const uint32_t*>(raw), nwords, first_bad);
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_sample_rows(const Dims& d, const uint8_t* raw, float* samples, cudaStream_t s) {
     const dim3 grid(grid1(d.nchans, 128), kMaxBandpassRows, static_cast<unsigned>(d.nwin));
     FB_DISPATCH(d.dtype, k_sample_rows<D><<<grid, 128, 0, s>>>(d, raw, samples));
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_bandpass(const Dims& d, const float* samples, float* loc, float* scale, float* inv,
                      uint32_t* unmeasured, cudaStream_t s) {
     const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
     k_bandpass<<<grid, 64, 0, s>>>(d, samples, loc, scale, inv, unmeasured);
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_moments(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
                     const uint8_t* static_mask, float clip, MomentSums* out, cudaStream_t s) {
     const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
     FB_DISPATCH(d.dtype, k_moments<D><<<grid, 64, 0, s>>>(d, raw, loc, inv, static_mask, clip, out));
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_scan_rows(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
@@ -859,7 +870,7 @@ void launch_scan_rows(const Dims& d, const uint8_t* raw, const float* loc, const
     FB_DISPATCH(d.dtype, k_scan_rows<D><<<grid, kScanRows, 0, s>>>(
                              d, raw, loc, inv, mask, clip, kp, good_prefix, s_det, s_keep_d,
                              s_keep_f, row_std, kspec_pos, kspec_neg, kspec_whole));
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
@@ -873,11 +884,11 @@ void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const
                              d, raw, loc, inv, mask, clip, s_keep_d, zdot, kchan, clip_mean,
                              clip_inv_std, chunk_min, chunk_max, chunk_zdot, chunk_kpos,
                              chunk_kneg));
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
     k_combine_chunks<<<grid1(d.nchans, 128), 128, 0, s>>>(d, zdot, kchan, chunk_min, chunk_max,
                                                           chunk_zdot, chunk_kpos, chunk_kneg, lo,
                                                           hi, zdot_sum, kpos_best, kneg_best);
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 static void set_smem(const void* fn, size_t bytes) {
@@ -902,7 +913,7 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
             d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
             kchan_neg, s_keep_f, zdot_a, zdot_b, work, counters);
     });
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_apply_flagged(const Dims& d, const ApplyParams& p, const uint64_t* flagged,
@@ -915,7 +926,7 @@ void launch_apply_flagged(const Dims& d, const ApplyParams& p, const uint64_t* f
     set_smem(reinterpret_cast<const void*>(&k_apply_flagged), smem);
     k_apply_flagged<<<static_cast<unsigned>(nflagged), 256, smem, s>>>(
         d, p, flagged, loc, scale, inv, mask, time_flags, work, counters);
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_unpack(const Dims& d, const uint8_t* raw, float* work, cudaStream_t s) {
@@ -924,20 +935,20 @@ void launch_unpack(const Dims& d, const uint8_t* raw, float* work, cudaStream_t 
         return;
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((total + 255) / 256, 148 * 32));
     FB_DISPATCH(d.dtype, k_unpack<D><<<blocks, 256, 0, s>>>(d, raw, work));
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_welford(const Dims& d, const float* work, float* loc, float* scale, cudaStream_t s) {
     const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
     k_welford<<<grid, 64, 0, s>>>(d, work, loc, scale);
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_normalize(const Dims& d, const float* work, const float* loc, const float* scale,
                       const uint8_t* mask, int flip, uint64_t capacity, float* out, cudaStream_t s) {
     const dim3 grid(grid1(capacity, kTile), grid1(d.nchans, kTile));
     k_normalize<<<grid, dim3(kTile, 8), 0, s>>>(d, work, loc, scale, mask, flip, capacity, out);
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 void launch_normalize_short(const Dims& d, const ApplyParams& p, const float* work,
@@ -952,7 +963,7 @@ void launch_normalize_short(const Dims& d, const ApplyParams& p, const float* wo
     k_normalize_short<<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
         d, p, work, tail_loc, tail_scale, tail_out_loc, tail_out_scale, mask, zdot_a, zdot_b, flip,
         capacity, out);
-    FB_LAUNCH_CHECK();
+    FB_COUNT_LAUNCH();
 }
 
 } // namespace fb::rfi

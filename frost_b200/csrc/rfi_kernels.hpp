@@ -50,6 +50,9 @@ struct KspecParams {
     double threshold;
 };
 
+/** Kernels launched by this file's launchers in this process. */
+uint64_t launch_counter();
+
 /** Counters the apply passes accumulate (device, 4 x uint64). */
 enum { kCountNarrow = 0, kCountKspec = 1, kCountKchan = 2, kCountFallback = 3, kCountSlots = 4 };
 

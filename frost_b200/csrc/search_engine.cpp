@@ -188,8 +188,54 @@ Engine::~Engine() {
     if (m_stream != nullptr) {
         cudaSetDevice(m_device);
         cudaStreamSynchronize(m_stream);
+        for (auto e : m_event_pool)
+            cudaEventDestroy(e);
         cudaStreamDestroy(m_stream);
     }
+}
+
+void Engine::enable_timing(bool on) {
+    m_timing_on = on;
+    m_timing    = frost_search_timing{};
+}
+
+cudaEvent_t Engine::next_event() {
+    if (m_events_used == m_event_pool.size()) {
+        cudaEvent_t e;
+        FB_CUDA(cudaEventCreate(&e));
+        m_event_pool.push_back(e);
+    }
+    return m_event_pool[m_events_used++];
+}
+
+template <class F> void Engine::timed(Phase ph, cudaStream_t s, F&& f) {
+    if (!m_timing_on) {
+        f();
+        return;
+    }
+    Mark m{ph, next_event(), next_event()};
+    FB_CUDA(cudaEventRecord(m.a, s));
+    f();
+    FB_CUDA(cudaEventRecord(m.b, s));
+    m_marks.push_back(m);
+}
+
+// Accumulates the marked phases' device time (the stream is synchronised).
+void Engine::harvest() {
+    for (const auto& m : m_marks) {
+        float ms = 0.0F;
+        FB_CUDA(cudaEventElapsedTime(&ms, m.a, m.b));
+        switch (m.phase) {
+        case kLevel1: m_timing.level1_ms += ms; break;
+        case kLevel: m_timing.level_ms += ms; break;
+        case kSearch: m_timing.search_ms += ms; break;
+        case kHistory: m_timing.history_ms += ms; break;
+        case kVariance: m_timing.variance_ms += ms; break;
+        default: break;
+        }
+    }
+    m_marks.clear();
+    m_events_used = 0;
 }
 
 SizeType Engine::plan_bytes(int64_t tile) const {
@@ -327,7 +373,7 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
         FB_CUDA(cudaStreamWaitEvent(s, ev, 0));
         FB_CUDA(cudaEventDestroy(ev));
     }
-    update_variance(cur, orm);
+    timed(kVariance, s, [&] { update_variance(cur, orm); });
 
     const float* wf = waterfall;
     if (!on_device) {
@@ -349,31 +395,49 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
     const int L          = m_plan.levels();
     const int64_t gulp0  = static_cast<int64_t>(m_samples);
     const auto& planes   = m_plan.planes();
+    const uint64_t es    = m_fp16 ? 2 : 4;
     for (int64_t t_off = 0; t_off < static_cast<int64_t>(nsamps); t_off += m_tile) {
         const int32_t n_valid = static_cast<int32_t>(std::min<int64_t>(m_tile, nsamps - t_off));
         const SearchParams sp = params(gulp0 + t_off, gulp0, n_valid, or_active);
         for (int h = 1; h <= L; ++h) {
             const LevelView out = view(h);
             if (h == 1) {
-                launch_level1(m_leaf_ops.as<LeafOp>(), m_node_first_op_d.as<int32_t>(),
-                              static_cast<int32_t>(m_node_first_op.size() - 1),
-                              m_plan.level_history(0), wf, static_cast<int64_t>(nsamps), t_off,
-                              n_valid, m_in_hist.as<float>(), m_plan.level_history(0), out,
-                              static_cast<int32_t>(m_ncols), s);
-                launch_save_input_history(wf, static_cast<int64_t>(nsamps), t_off, n_valid, C,
-                                          m_in_hist.as<float>(), m_in_scratch.as<float>(),
-                                          m_plan.level_history(0), s);
+                timed(kLevel1, s, [&] {
+                    launch_level1(m_leaf_ops.as<LeafOp>(), m_node_first_op_d.as<int32_t>(),
+                                  static_cast<int32_t>(m_node_first_op.size() - 1),
+                                  m_plan.level_history(0), wf, static_cast<int64_t>(nsamps), t_off,
+                                  n_valid, m_in_hist.as<float>(), m_plan.level_history(0), out,
+                                  static_cast<int32_t>(m_ncols), s);
+                });
+                timed(kHistory, s, [&] {
+                    launch_save_input_history(wf, static_cast<int64_t>(nsamps), t_off, n_valid, C,
+                                              m_in_hist.as<float>(), m_in_scratch.as<float>(),
+                                              m_plan.level_history(0), s);
+                });
                 m_launches += 1;
+                m_timing.algorithmic_level1_bytes +=
+                    static_cast<uint64_t>(C) * m_ncols * sizeof(float) +
+                    static_cast<uint64_t>(m_plan.level_rows(1)) * m_ncols * es;
             } else {
-                launch_level(m_row_ops.as<RowOp>() + m_row_op_offset[h], m_plan.level_rows(h),
-                             view(h - 1), out, static_cast<int32_t>(m_ncols), s);
+                timed(kLevel, s, [&] {
+                    launch_level(m_row_ops.as<RowOp>() + m_row_op_offset[h], m_plan.level_rows(h),
+                                 view(h - 1), out, static_cast<int32_t>(m_ncols), s);
+                });
                 m_launches += 1;
+                m_timing.level_launches += 1;
+                m_timing.algorithmic_level_bytes +=
+                    static_cast<uint64_t>(m_plan.level_rows(h - 1) + m_plan.level_rows(h)) * m_ncols * es;
             }
-            launch_load_history(out, m_plan.level_rows(h), m_plan.level_history(h),
-                                m_hist[h].get(), s);
+            timed(kHistory, s, [&] {
+                launch_load_history(out, m_plan.level_rows(h), m_plan.level_history(h),
+                                    m_hist[h].get(), s);
+            });
             if (m_height_g1[h] > m_height_g0[h]) {
-                launch_search(sp, out, m_height_g0[h], m_height_g1[h], s);
+                timed(kSearch, s, [&] { launch_search(sp, out, m_height_g0[h], m_height_g1[h], s); });
                 m_launches += 1;
+                m_timing.search_launches += 1;
+                m_timing.algorithmic_search_bytes +=
+                    static_cast<uint64_t>(m_height_g1[h] - m_height_g0[h]) * m_ncols * es;
                 if (m_capture_on) {
                     for (size_t p = 0; p < planes.size(); ++p) {
                         if (planes[p].height != h)
@@ -389,15 +453,22 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
                 }
             }
             if (h >= 2)
-                launch_save_history(view(h - 1), m_plan.level_rows(h - 1),
-                                    m_plan.level_history(h - 1), n_valid, m_hist[h - 1].get(), s);
+                timed(kHistory, s, [&] {
+                    launch_save_history(view(h - 1), m_plan.level_rows(h - 1),
+                                        m_plan.level_history(h - 1), n_valid, m_hist[h - 1].get(), s);
+                });
         }
-        launch_save_history(view(L), m_plan.level_rows(L), m_plan.level_history(L), n_valid,
-                            m_hist[L].get(), s);
+        timed(kHistory, s, [&] {
+            launch_save_history(view(L), m_plan.level_rows(L), m_plan.level_history(L), n_valid,
+                                m_hist[L].get(), s);
+        });
     }
     m_samples += nsamps;
     m_mask = cur;
     collect(s);
+    m_timing.total_launches += m_launches;
+    m_timing.executes += 1;
+    harvest();
 }
 
 void Engine::collect(cudaStream_t s) {

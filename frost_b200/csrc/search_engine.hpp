@@ -42,8 +42,24 @@ public:
     cudaStream_t stream() const { return m_stream; }
     /** Kernel launches of the last execute call. */
     uint64_t last_launches() const { return m_launches; }
+    void enable_timing(bool on);
+    const frost_search_timing& timing() const { return m_timing; }
 
 private:
+    enum Phase { kLevel1, kLevel, kSearch, kHistory, kVariance, kPhases };
+    struct Mark {
+        Phase phase;
+        cudaEvent_t a, b;
+    };
+    bool m_timing_on = false;
+    frost_search_timing m_timing{};
+    std::vector<cudaEvent_t> m_event_pool;
+    std::vector<Mark> m_marks;
+    size_t m_events_used = 0;
+    cudaEvent_t next_event();
+    template <class F> void timed(Phase ph, cudaStream_t s, F&& f);
+    void harvest();
+
     Plan m_plan;
     frost_boxcar_config m_cfg;
     int m_device;

@@ -90,6 +90,11 @@ class RFICleaner:
         check(lib().frost_rfi_get_report(self._h, C.byref(r)))
         return r.as_dict()
 
+    def launches(self) -> int:
+        n = C.c_uint64()
+        check(lib().frost_rfi_launch_count(self._h, C.byref(n)))
+        return n.value
+
     def memory_usage(self) -> int:
         n = C.c_size_t()
         check(lib().frost_rfi_memory_usage(self._h, C.byref(n)))

@@ -181,6 +181,14 @@ class FDMTBoxcar:
                                                out.ctypes.data_as(C.POINTER(C.c_double)), ndm))
         return out
 
+    def enable_timing(self, enable: bool = True):
+        check(lib().frost_search_enable_timing(self._h, int(enable)))
+
+    def timing(self) -> dict:
+        t = _abi.SearchTimingC()
+        check(lib().frost_search_get_timing(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     def capture_planes(self, enable: bool = True):
         check(lib().frost_search_capture_planes(self._h, int(enable)))
 

@@ -208,6 +208,9 @@ int frost_rfi_time_flags(const frost_rfi* rfi, uint8_t* out, size_t nsamps);
 /* RFICleaner::memory_usage (include/frost/prepare/rfi.hpp:291): device bytes. */
 int frost_rfi_memory_usage(const frost_rfi* rfi, size_t* bytes);
 
+/* Kernels this cleaner has launched since it was created. */
+int frost_rfi_launch_count(const frost_rfi* rfi, uint64_t* launches);
+
 /* IQRM channel mask (include/frost/prepare/rfi.hpp:56-59,
  * lib/cpu/rfi_masks_cpu.cpp:29-122) on an n-channel host statistic.
  * `ignore` may be NULL. Writes n flags (1 = flagged) to host `out`. */
@@ -429,6 +432,30 @@ int frost_search_plane_data(const frost_search* s,
                             size_t plane,
                             float* out,
                             size_t capacity);
+
+/* Per-phase device time of the execute calls since timing was enabled
+ * (CUDA events on the engine's stream), the stage profile frost keeps in
+ * RunProfile (include/frost/pipeline/profile.hpp:27-61) at kernel level.
+ * `algorithmic_level_bytes` counts one read of every input row and one write
+ * of every output row of the FDMT levels >= 2 (the HBM roofline's traffic). */
+typedef struct {
+    double level1_ms;
+    double level_ms;
+    double search_ms;
+    double history_ms;
+    double variance_ms;
+    uint64_t level_launches;
+    uint64_t search_launches;
+    uint64_t total_launches;
+    uint64_t algorithmic_level_bytes;
+    uint64_t algorithmic_level1_bytes;
+    uint64_t algorithmic_search_bytes;
+    uint64_t executes;
+} frost_search_timing;
+
+/* Enables (and zeroes) or disables per-phase timing. */
+int frost_search_enable_timing(frost_search* s, int enable);
+int frost_search_get_timing(const frost_search* s, frost_search_timing* out);
 
 #ifdef __cplusplus
 } /* extern "C" */

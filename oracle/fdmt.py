@@ -44,6 +44,10 @@ def lib():
         L.oracle_dedisperse.argtypes = [f64p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, i64p, i64p,
                                         C.c_int64, f64p]
         L.oracle_variance.argtypes = [i64p, C.c_int64, C.c_int64, u8p, C.c_int64, C.c_int, f64p]
+        L.cpu_fdmt_search.restype = C.c_int64
+        L.cpu_fdmt_search.argtypes = [C.POINTER(C.c_float), C.c_int64, C.c_int64, C.c_double,
+                                      C.c_double, C.c_double, C.POINTER(C.c_float), C.c_int64,
+                                      C.c_int64, i64p, C.c_int64, C.c_double]
         L.oracle_search.restype = C.c_int64
         L.oracle_search.argtypes = [f64p, C.c_int64, C.c_int64, i64p, i64p, C.c_int64, f64p, f64p,
                                     C.c_int64, u8p, C.c_double, C.c_int, C.c_int, C.c_int,
@@ -277,3 +281,19 @@ class Oracle:
 
     def _cand(self, band, c):
         return self._mk(band, c.row, c.width_idx, c.peak, c.begin, c.end, c.snr)
+
+
+def cpu_search(waterfall: np.ndarray, f_min: float, f_max: float, tsamp: float, dm_list,
+               depth: int, widths_list, thresh: float = 6.0) -> int:
+    """The CPU port of the search (oracle/cpu_fdmt.c) on one [nchans][T]
+    float32 block with zero history; returns the peak count. Timed as the CPU
+    baseline; not a correctness oracle."""
+    x = np.ascontiguousarray(waterfall, np.float32)
+    dms = np.ascontiguousarray(dm_list, np.float32)
+    ws = np.ascontiguousarray(widths_list, np.int64)
+    n = lib().cpu_fdmt_search(_p(x, C.c_float), x.shape[0], x.shape[1], float(f_min), float(f_max),
+                              float(tsamp), _p(dms, C.c_float), dms.size, depth, _p(ws, C.c_int64),
+                              ws.size, float(thresh))
+    if n < 0:
+        raise RuntimeError("cpu_fdmt_search failed")
+    return int(n)
