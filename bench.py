@@ -32,21 +32,41 @@ sys.path.insert(0, ROOT)
 
 METRIC = "beam-s searched/s @4096ch DM2000"
 UNIT = "beam-s/s"
-NCHANS, GULP, TSAMP = 4096, 262144, 64e-6
-FCH1, FOFF = 1535.958984375, -0.08203125
-DM_MAX, MAX_BOXCAR, DEPTH = 2000.0, 256, 2
-WORKLOAD = ("4096ch 1200-1536MHz 64us uint8, 262144-sample gulps, DM 0-2000 (3625 trials), "
-            "boxcar 1-256, 11 sub-band planes, moments+IQRM+Kadane(time,freq)+zero-DM RFI")
+# The headline workload (4096 channels, DM 0-2000, 11 planes) and the small
+# 1024-channel DM 0-500 full-band workload used for profiling captures.
+WORKLOADS = {
+    "config2": dict(nchans=4096, gulp=262144, fch1=1535.958984375, foff=-0.08203125,
+                    dm_max=2000.0, max_boxcar=256, depth=2, full_rfi=True,
+                    text=("4096ch 1200-1536MHz 64us uint8, 262144-sample gulps, DM 0-2000 "
+                          "(3625 trials), boxcar 1-256, 11 sub-band planes, "
+                          "moments+IQRM+Kadane(time,freq)+zero-DM RFI")),
+    "config1": dict(nchans=1024, gulp=65536, fch1=1500.0, foff=-0.29296875, dm_max=500.0,
+                    max_boxcar=64, depth=0, full_rfi=False,
+                    text=("1024ch 1200-1500MHz 64us uint8, 65536-sample gulps, DM 0-500 "
+                          "(886 trials), boxcar 1-64, full band, default RFI")),
+}
+TSAMP = 64e-6
+W = dict(WORKLOADS["config2"])
+NCHANS, GULP, FCH1, FOFF = W["nchans"], W["gulp"], W["fch1"], W["foff"]
+DM_MAX, MAX_BOXCAR, DEPTH, WORKLOAD = W["dm_max"], W["max_boxcar"], W["depth"], W["text"]
+
+
+def select_workload(name):
+    global W, NCHANS, GULP, FCH1, FOFF, DM_MAX, MAX_BOXCAR, DEPTH, WORKLOAD
+    W = dict(WORKLOADS[name])
+    NCHANS, GULP, FCH1, FOFF = W["nchans"], W["gulp"], W["fch1"], W["foff"]
+    DM_MAX, MAX_BOXCAR, DEPTH, WORKLOAD = W["dm_max"], W["max_boxcar"], W["depth"], W["text"]
 
 
 def rfi_config():
     from frost_b200.config import RfiConfig, ZeroDMMode
     cfg = RfiConfig()
-    cfg.moments.enabled = True
-    cfg.iqrm.enabled = True
-    cfg.kadane_channel.enabled = True
-    cfg.kadane_spectrum.enabled = True
-    cfg.zero_dm = ZeroDMMode.SUBTRACT
+    if W["full_rfi"]:
+        cfg.moments.enabled = True
+        cfg.iqrm.enabled = True
+        cfg.kadane_channel.enabled = True
+        cfg.kadane_spectrum.enabled = True
+        cfg.zero_dm = ZeroDMMode.SUBTRACT
     return cfg
 
 
@@ -56,8 +76,11 @@ def layout(nsamps=GULP):
 
 
 def search_config(storage):
+    """frost's search defaults (threshold 6, one peak per run per width) with
+    room for every candidate of the 20 injected pulses in 11 planes."""
     from frost_b200.config import BoxcarConfig
-    return BoxcarConfig(max_boxcar=MAX_BOXCAR, wtsp=2.0, detect_thresh=6.0, storage=storage)
+    return BoxcarConfig(max_boxcar=MAX_BOXCAR, wtsp=2.0, detect_thresh=6.0, storage=storage,
+                        max_candidates=1 << 20, max_cands_per_dm=4096)
 
 
 def dist_env():
@@ -141,7 +164,9 @@ def ncu_traffic_per_launch():
 
 
 def make_gulp(seed):
-    from frost_b200.synth import config2_gulp
+    from frost_b200.synth import config1_gulp, config2_gulp
+    if NCHANS == 1024:
+        return config1_gulp(seed=seed, nsamps=GULP).data
     return config2_gulp(seed=seed).data  # [T][C] uint8
 
 
@@ -211,10 +236,16 @@ def run_gpu(args):
         total_ms = starts[0].elapsed_time(starts[-1])
         timing = pipe.search.timing()
         launches = timing["total_launches"] + (pipe.rfi.launches() - l0)
+        rep = pipe.rfi.report()
         out = {"total_ms": max_over_ranks(total_ms), "lat": lat, "timing": timing,
                "launches": launches, "ncands": ncands, "d2h": d2h,
+               "dropped": [res.dropped_global, res.dropped_per_dm],
                "clocks": sampler.summary() if sampler else None,
-               "rfi_report": pipe.rfi.report(), "device_bytes": pipe.search.info()["device_bytes"]}
+               "rfi_ms": {k: round(rep[k] * 1e3, 2) for k in
+                          ("t_bandpass", "t_moments", "t_scan", "t_flags", "t_apply")},
+               "rfi_counts": {k: rep[k] for k in ("chans_masked", "samps_flagged", "cells_narrow",
+                                                  "cells_kadane_channel", "cells_kadane_spectrum")},
+               "device_bytes": pipe.search.info()["device_bytes"]}
         del pipe
         torch.cuda.empty_cache()
         return out
@@ -271,6 +302,9 @@ def run_gpu(args):
         "roofline": roofline,
         "clocks": fp16["clocks"],
         "candidates_per_step": round(fp16["ncands"] / args.steps, 1),
+        "dropped_last_step": fp16["dropped"],
+        "rfi_stage_ms_last_step": fp16["rfi_ms"],
+        "rfi_counts_last_step": fp16["rfi_counts"],
         "device_bytes": fp16["device_bytes"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -351,7 +385,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["frost", "reference"], default="frost")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
+                    help="config2 (headline) or config1 (1024-channel profiling case)")
     args = ap.parse_args()
+    select_workload(args.workload)
     if args.warmup < 3 and args.impl == "frost":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":

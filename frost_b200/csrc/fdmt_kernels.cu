@@ -137,14 +137,18 @@ __global__ void __launch_bounds__(kThreads)
     const int32_t k0 = blockIdx.y * kTimePerCta;
     const S* lo = in + static_cast<int64_t>(op.lo_row) * in_pitch + in_base + k0;
     S* dst      = out + static_cast<int64_t>(blockIdx.x) * out_pitch + out_base + k0;
+    // Each thread owns 8 consecutive samples: one 16-byte (fp16) or two
+    // 16-byte (fp32) vectors of the unshifted row and of the output.
+    const int e = 8 * threadIdx.x;
     if (op.hi_row < 0) {
-        for (int j = 0; j < kPer; ++j) {
-            const int k = threadIdx.x + j * kThreads;
-            dst[k]      = lo[k];
-        }
+        const uint4* s4 = reinterpret_cast<const uint4*>(lo + e);
+        uint4* d4       = reinterpret_cast<uint4*>(dst + e);
+        for (int v = 0; v < 8 / VEC; ++v)
+            d4[v] = s4[v];
         return;
     }
-    // Stage hi[k0 - shift, k0 - shift + kTimePerCta) with aligned vectors.
+    // Stage hi[k0 - shift, k0 - shift + kTimePerCta) with aligned vectors;
+    // element k of the segment is stage[off + k].
     const S* hrow    = in + static_cast<int64_t>(op.hi_row) * in_pitch;
     const int64_t e0 = static_cast<int64_t>(in_base) + k0 - op.shift;
     const int64_t v0 = e0 / VEC;
@@ -155,9 +159,57 @@ __global__ void __launch_bounds__(kThreads)
     for (int i = threadIdx.x; i < nvec; i += kThreads)
         sv[i] = src[i];
     __syncthreads();
-    for (int j = 0; j < kPer; ++j) {
-        const int k = threadIdx.x + j * kThreads;
-        st<S>(dst + k, ld<S>(lo + k) + ld<S>(stage + off + k));
+    if constexpr (sizeof(S) == 4) {
+        const float4* l4 = reinterpret_cast<const float4*>(lo + e);
+        const float4 a0 = l4[0], a1 = l4[1];
+        const float4* h4 = reinterpret_cast<const float4*>(stage) + e / 4;
+        const float4 b0 = h4[0], b1 = h4[1], b2 = h4[2]; // b2 unused when off == 0
+        const float h[12] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
+        float g[8];
+        switch (off) {
+#define FB_PICK(O)                                                                                \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 8; ++i) g[i] = h[O + i];                             \
+        break;
+            FB_PICK(0) FB_PICK(1) FB_PICK(2) FB_PICK(3)
+#undef FB_PICK
+        }
+        float4* d4 = reinterpret_cast<float4*>(dst + e);
+        d4[0]      = make_float4(a0.x + g[0], a0.y + g[1], a0.z + g[2], a0.w + g[3]);
+        d4[1]      = make_float4(a1.x + g[4], a1.y + g[5], a1.z + g[6], a1.w + g[7]);
+    } else {
+        const uint4 a  = *reinterpret_cast<const uint4*>(lo + e);
+        const uint4 b0 = sv[threadIdx.x], b1 = sv[threadIdx.x + 1]; // b1 unused when off == 0
+        const uint32_t w[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        uint32_t g[4];
+        // 8 halves starting at half `off` of the 16 in w[]
+        switch (off) {
+#define FB_PICK_EVEN(O)                                                                           \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] = w[O / 2 + i];                         \
+        break;
+#define FB_PICK_ODD(O)                                                                            \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] =                                      \
+            __byte_perm(w[O / 2 + i], w[O / 2 + i + 1], 0x5432);                                  \
+        break;
+            FB_PICK_EVEN(0) FB_PICK_ODD(1) FB_PICK_EVEN(2) FB_PICK_ODD(3)
+            FB_PICK_EVEN(4) FB_PICK_ODD(5) FB_PICK_EVEN(6) FB_PICK_ODD(7)
+#undef FB_PICK_EVEN
+#undef FB_PICK_ODD
+        }
+        const uint32_t av[4] = {a.x, a.y, a.z, a.w};
+        uint32_t r[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 x = __half22float2(*reinterpret_cast<const __half2*>(&av[i]));
+            const float2 y = __half22float2(*reinterpret_cast<const __half2*>(&g[i]));
+            const float lo_sum = fminf(fmaxf(x.x + y.x, -65504.0F), 65504.0F);
+            const float hi_sum = fminf(fmaxf(x.y + y.y, -65504.0F), 65504.0F);
+            const __half2 s    = __floats2half2_rn(lo_sum, hi_sum);
+            r[i]               = *reinterpret_cast<const uint32_t*>(&s);
+        }
+        *reinterpret_cast<uint4*>(dst + e) = make_uint4(r[0], r[1], r[2], r[3]);
     }
 }
 

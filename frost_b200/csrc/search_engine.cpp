@@ -167,15 +167,15 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     // Tile length: the whole gulp unless the budget (or the device) is short.
     int64_t tile = bc.tile_nsamps != 0 ? static_cast<int64_t>(bc.tile_nsamps)
                                        : static_cast<int64_t>(dd.block_nsamps);
-    if (bc.tile_nsamps != 0 && bc.tile_nsamps % kTimePerCta != 0)
-        invalid("search: tile_nsamps must be a multiple of 2048");
-    tile = round_up(std::min<int64_t>(tile, static_cast<int64_t>(dd.block_nsamps)), kTimePerCta);
+    if (bc.tile_nsamps != 0 && bc.tile_nsamps % kTileQuantum != 0)
+        invalid("search: tile_nsamps must be a multiple of 4096");
+    tile = round_up(std::min<int64_t>(tile, static_cast<int64_t>(dd.block_nsamps)), kTileQuantum);
     size_t free_b = 0, total_b = 0;
     FB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const SizeType limit = memory_budget != 0 ? memory_budget
                                               : static_cast<SizeType>(0.85 * static_cast<double>(free_b));
-    while (plan_bytes(tile) > limit && tile > kTimePerCta)
-        tile = round_up(tile / 2, kTimePerCta);
+    while (plan_bytes(tile) > limit && tile > kTileQuantum)
+        tile = round_up(tile / 2, kTileQuantum);
     if (plan_bytes(tile) > limit)
         throw Error(FROST_ERR_OUT_OF_MEMORY,
                     "search: plan needs " + std::to_string(plan_bytes(tile)) +
@@ -245,7 +245,7 @@ SizeType Engine::plan_bytes(int64_t tile) const {
     for (int h = 1; h <= L; ++h)
         maxh = std::max(maxh, m_plan.level_history(h));
     const int64_t base   = round_up(std::max<int64_t>(maxh, m_plan.widths().back()), 8);
-    const int64_t pitch  = base + round_up(tile, kTimePerCta);
+    const int64_t pitch  = base + round_up(tile, kTileQuantum);
     SizeType bytes       = 2 * static_cast<SizeType>(m_plan.max_level_rows()) * pitch * es;
     for (int h = 1; h <= L; ++h)
         bytes += static_cast<SizeType>(m_plan.level_rows(h)) * m_plan.level_history(h) * es;
@@ -262,7 +262,7 @@ void Engine::allocate(int64_t tile) {
     for (int h = 1; h <= L; ++h)
         maxh = std::max(maxh, m_plan.level_history(h));
     m_tile  = tile;
-    m_ncols = round_up(tile, kTimePerCta);
+    m_ncols = round_up(tile, kTileQuantum);
     m_base  = static_cast<int32_t>(round_up(std::max<int64_t>(maxh, m_plan.widths().back()), 8));
     m_pitch = m_base + m_ncols;
     const SizeType buf = static_cast<SizeType>(m_plan.max_level_rows()) * m_pitch * es;

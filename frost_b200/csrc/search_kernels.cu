@@ -1,14 +1,18 @@
 // Boxcar/trapezoid matched filter, exact noise and peak finding on sm_100a.
 //
-// One CTA per searched (plane, DM) row walks the tile in 2048-sample chunks:
+// One CTA per searched (plane, DM) row walks the tile in 4096-sample chunks:
 // the chunk plus a (wmax - 1)-sample halo is staged in shared memory and
-// prefix-summed, every width's S/N is a difference of two (four for the
-// trapezoid) prefix values times 1/sigma, and above-threshold samples become
-// ballot bitmasks. Runs (contiguous set bits) are rare, so one lane walks
-// only the set bits in time order, extending or closing the run carried
-// from the previous chunk (and tile, and gulp) and emitting each closed
-// run's peak. The DM-time rows are never re-read and the run state is the
-// only thing carried between calls.
+// prefix-summed; every width's window sum is a difference of two (four for
+// the trapezoid) prefix values. In the steady state (no cold prefix, no mask
+// change in the chunk) a sample is above threshold when its window sum
+// exceeds thresh * sigma, precomputed per width, so the test is two shared
+// loads, a subtract and a compare; the first chunks of a stream or after a
+// mask change take the general path (cold prefix, OR-mask variance).
+// Above-threshold samples become ballot bitmasks. Runs (contiguous set bits)
+// are rare, so one lane walks only the set bits in time order, extending or
+// closing the run carried from the previous chunk (and tile, and gulp) and
+// emitting each closed run's peak. The DM-time rows are never re-read and
+// the run state is the only thing carried between calls.
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -21,10 +25,12 @@ namespace fb::fdmt {
 namespace {
 
 constexpr int kThreads   = 256;
-constexpr int kChunk     = 2048;
+constexpr int kChunk     = kSearchChunk;
+constexpr int kPerThread = kChunk / kThreads;
 constexpr int kWords     = kChunk / 32;
 constexpr int kMaxWidths = 32;
 #define FB_NEG_INF (-__int_as_float(0x7f800000))
+#define FB_POS_INF (__int_as_float(0x7f800000))
 
 template <class S> __device__ __forceinline__ float ldf(const S* p);
 template <> __device__ __forceinline__ float ldf<float>(const float* p) { return *p; }
@@ -67,47 +73,44 @@ __device__ void scan_inplace(float* a, int n) {
     __syncthreads();
 }
 
-struct Ctx {
-    const SearchParams* p;
-    const float* P;      // prefix sums: P[i] covers columns up to c0 - wmax + i
-    const float* inv;    // 1/sigma per width (shared memory)
-    const float* inv_or; // 1/sigma under the OR of the last two masks
-    int wmax;
-    int64_t c0;          // chunk start column in the tile
-    int32_t delay;
+/** Per-row constants, in shared memory. */
+struct RowConst {
+    int W[kMaxWidths];
+    int E[kMaxWidths];      // trapezoid half-weight edge, 0 for a boxcar
+    float inv[kMaxWidths];  // 1/sigma
+    float inv_or[kMaxWidths];
+    float thr[kMaxWidths];  // window-sum threshold thresh * sigma
 };
 
-// Sum of the width-W window ending at chunk sample k (boxcar or trapezoid).
-__device__ __forceinline__ float window_sum(const Ctx& c, int k, int W, int trap) {
-    const int i = k + c.wmax;
-    float s     = c.P[i] - c.P[i - W];
-    if (trap && W >= 3) {
-        const int e = (W + 1) / 4;
-        s -= 0.5F * ((c.P[i] - c.P[i - e]) + (c.P[i - W + e] - c.P[i - W]));
-    }
+// Window sum of width W (edge E) ending at prefix index i.
+__device__ __forceinline__ float wsum(const float* P, int i, int W, int E) {
+    float s = P[i] - P[i - W];
+    if (E > 0)
+        s -= 0.5F * ((P[i] - P[i - E]) + (P[i - W + E] - P[i - W]));
     return s;
 }
 
-// S/N of chunk sample k at width index wi, or -inf where the sample is not
-// searchable (past the valid columns, or in the cold prefix).
-__device__ __forceinline__ float snr_at(const Ctx& c, int k, int wi) {
-    const SearchParams& p = *c.p;
-    const int W           = p.widths[wi];
-    const int64_t col     = c.c0 + k;
+// General S/N of chunk sample k at width wi: -inf past the valid columns or
+// in the cold prefix; the OR-mask variance right after a mask change.
+__device__ __forceinline__ float snr_general(const SearchParams& p, const RowConst& rc,
+                                             const float* P, int wmax, int64_t c0, int k, int wi,
+                                             int32_t delay) {
+    const int64_t col = c0 + k;
     if (col >= p.n_valid)
         return FB_NEG_INF;
+    const int W     = rc.W[wi];
     const int64_t t = p.tile_t0 + col;
-    if (p.skip_cold && t < static_cast<int64_t>(c.delay) + W - 1)
+    if (p.skip_cold && t < static_cast<int64_t>(delay) + W - 1)
         return FB_NEG_INF;
-    const bool use_or = p.or_active && (t - p.gulp_t0) < static_cast<int64_t>(c.delay) + W - 1;
-    const float inv   = use_or ? c.inv_or[wi] : c.inv[wi];
+    const bool use_or = p.or_active && (t - p.gulp_t0) < static_cast<int64_t>(delay) + W - 1;
+    const float inv   = use_or ? rc.inv_or[wi] : rc.inv[wi];
     if (inv == 0.0F)
         return FB_NEG_INF;
-    return window_sum(c, k, W, p.trapezoid) * inv;
+    return wsum(P, k + wmax, W, rc.E[wi]) * inv;
 }
 
 // `count` (shared or global) is the row's emitted total this call.
-__device__ void emit(const SearchParams& p, const SearchRow& row, int64_t g, const RunState& r,
+__device__ void emit(const SearchParams& p, const SearchRow& row, const RunState& r,
                      uint32_t* count) {
     const uint32_t before = atomicAdd(count, 1U);
     if (p.max_per_dm != 0 && before >= p.max_per_dm) {
@@ -139,27 +142,27 @@ __device__ void emit(const SearchParams& p, const SearchRow& row, int64_t g, con
     p.cands[idx]    = c;
 }
 
-// Walks the set bits of one chunk's mask in time order (one lane).
-// For across-widths mode `wi` < 0: the peak is the best S/N over widths.
-__device__ void walk_runs(const Ctx& c, const uint32_t* bits, int wi, RunState& run,
-                          const SearchRow& row, int64_t g, uint32_t* local_count) {
-    const SearchParams& p = *c.p;
-    int64_t last          = run.open ? c.c0 - 1 : -2; // tile column of the last set bit
+// Walks the set bits of one chunk's mask in time order (one lane). For the
+// across-widths mode `wi` < 0: the peak is the best S/N over widths.
+__device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float* P, int wmax,
+                          int64_t c0, int32_t delay, const uint32_t* bits, int wi, RunState& run,
+                          const SearchRow& row, uint32_t* count) {
+    int64_t last = run.open ? c0 - 1 : -2; // tile column of the last set bit
     for (int wd = 0; wd < kWords; ++wd) {
         uint32_t b = bits[wd];
         while (b) {
-            const int bit   = __ffs(b) - 1;
+            const int bit     = __ffs(b) - 1;
             b &= b - 1;
-            const int k     = wd * 32 + bit;
-            const int64_t col = c.c0 + k;
-            float best = FB_NEG_INF;
-            int bw     = 0;
+            const int k       = wd * 32 + bit;
+            const int64_t col = c0 + k;
+            float best        = FB_NEG_INF;
+            int bw            = 0;
             if (wi >= 0) {
-                best = snr_at(c, k, wi);
+                best = snr_general(p, rc, P, wmax, c0, k, wi, delay);
                 bw   = wi;
             } else {
                 for (int w = 0; w < p.nwidths; ++w) {
-                    const float s = snr_at(c, k, w);
+                    const float s = snr_general(p, rc, P, wmax, c0, k, w, delay);
                     if (s > best) {
                         best = s;
                         bw   = w;
@@ -176,7 +179,7 @@ __device__ void walk_runs(const Ctx& c, const uint32_t* bits, int wi, RunState& 
                 run.last_t = t;
             } else {
                 if (run.open)
-                    emit(p, row, g, run, local_count);
+                    emit(p, row, run, count);
                 run.open   = 1;
                 run.start  = t;
                 run.best   = best;
@@ -188,9 +191,9 @@ __device__ void walk_runs(const Ctx& c, const uint32_t* bits, int wi, RunState& 
         }
     }
     // A run that does not reach the chunk's last valid column has closed.
-    const int64_t chunk_end = min(c.c0 + kChunk, static_cast<int64_t>(p.n_valid));
+    const int64_t chunk_end = min(c0 + kChunk, static_cast<int64_t>(p.n_valid));
     if (run.open && last != chunk_end - 1) {
-        emit(p, row, g, run, local_count);
+        emit(p, row, run, count);
         run.open = 0;
     }
 }
@@ -202,55 +205,64 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ uint32_t bits[kMaxWidths][kWords];
     __shared__ uint32_t any_bits[kWords];
     __shared__ RunState runs[kMaxWidths];
-    __shared__ float s_inv[kMaxWidths], s_inv_or[kMaxWidths];
+    __shared__ RowConst rc;
     __shared__ uint32_t local_count;
 
     const int64_t g     = g0 + blockIdx.x;
     const SearchRow row = p.rows[g];
     const int nw        = p.nwidths;
+    const int wmax      = p.wmax;
     const bool across   = p.peak_mode == FROST_PEAK_ACROSS_WIDTHS;
     const bool all      = p.peak_mode == FROST_PEAK_ALL;
     if (threadIdx.x == 0)
         local_count = p.row_counts[g];
     if (threadIdx.x < nw) {
-        s_inv[threadIdx.x]    = p.inv_sigma[g * nw + threadIdx.x];
-        s_inv_or[threadIdx.x] = p.inv_sigma_or[g * nw + threadIdx.x];
+        const int w  = threadIdx.x;
+        const int W  = p.widths[w];
+        rc.W[w]      = W;
+        rc.E[w]      = (p.trapezoid && W >= 3) ? (W + 1) / 4 : 0;
+        const float iv = p.inv_sigma[g * nw + w];
+        rc.inv[w]    = iv;
+        rc.inv_or[w] = p.inv_sigma_or[g * nw + w];
+        rc.thr[w]    = iv > 0.0F ? p.thresh / iv : FB_POS_INF;
     }
     const int nruns = across ? 1 : nw;
     if (threadIdx.x < nruns && !all)
         runs[threadIdx.x] = p.carry[g * nruns + threadIdx.x];
     __syncthreads();
-    Ctx c;
-    c.p      = &p;
-    c.P      = P;
-    c.inv    = s_inv;
-    c.inv_or = s_inv_or;
-    c.wmax   = p.wmax;
-    c.c0     = 0;
-    c.delay  = row.delay;
 
-    const S* src   = level + row.level_row * pitch + base;
-    const int N    = kChunk + p.wmax;
+    const S* src = level + row.level_row * pitch + base;
+    const int N  = kChunk + wmax;
+    const int64_t warm = static_cast<int64_t>(row.delay) + wmax - 1;
     for (int64_t c0 = 0; c0 < p.n_valid; c0 += kChunk) {
-        c.c0 = c0;
         // P[i] <- column c0 - wmax + i (i = 0 is the scan base).
         for (int i = threadIdx.x; i < N; i += kThreads)
-            P[i] = i == 0 ? 0.0F : ldf<S>(src + c0 - p.wmax + i);
+            P[i] = i == 0 ? 0.0F : ldf<S>(src + c0 - wmax + i);
         __syncthreads();
         scan_inplace(P, N);
 
+        const bool fast = c0 + kChunk <= p.n_valid && (!p.skip_cold || p.tile_t0 + c0 >= warm) &&
+                          (!p.or_active || p.tile_t0 + c0 - p.gulp_t0 >= warm);
         uint32_t any = 0;
         for (int wi = 0; wi < nw; ++wi) {
-            for (int j = 0; j < kChunk / kThreads; ++j) {
-                const int k   = threadIdx.x + j * kThreads;
-                const float s = snr_at(c, k, wi);
-                const bool up = s > p.thresh;
+            const int W     = rc.W[wi];
+            const int E     = rc.E[wi];
+            const float thr = rc.thr[wi];
+#pragma unroll 4
+            for (int j = 0; j < kPerThread; ++j) {
+                const int k = threadIdx.x + j * kThreads;
+                bool up;
+                if (fast) {
+                    up = wsum(P, k + wmax, W, E) > thr;
+                } else {
+                    up = snr_general(p, rc, P, wmax, c0, k, wi, row.delay) > p.thresh;
+                }
                 if (all && up) {
                     RunState r{};
-                    r.best   = s;
+                    r.best   = snr_general(p, rc, P, wmax, c0, k, wi, row.delay);
                     r.best_w = wi;
                     r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
-                    emit(p, row, g, r, &local_count);
+                    emit(p, row, r, &local_count);
                 }
                 const uint32_t m = __ballot_sync(0xFFFFFFFFU, up);
                 if ((threadIdx.x & 31) == 0)
@@ -272,11 +284,12 @@ __global__ void __launch_bounds__(kThreads)
         if (!all && threadIdx.x == 0) {
             if (across) {
                 if (fired || runs[0].open)
-                    walk_runs(c, any_bits, -1, runs[0], row, g, &local_count);
+                    walk_runs(p, rc, P, wmax, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
             } else {
                 for (int wi = 0; wi < nw; ++wi)
                     if (fired || runs[wi].open)
-                        walk_runs(c, bits[wi], wi, runs[wi], row, g, &local_count);
+                        walk_runs(p, rc, P, wmax, c0, row.delay, bits[wi], wi, runs[wi], row,
+                                  &local_count);
             }
         }
         __syncthreads();
@@ -296,7 +309,7 @@ __global__ void k_flush(SearchParams p, int64_t nrows) {
     for (int i = 0; i < nruns; ++i) {
         RunState& r = p.carry[g * nruns + i];
         if (r.open) {
-            emit(p, row, g, r, &p.row_counts[g]);
+            emit(p, row, r, &p.row_counts[g]);
             r.open = 0;
         }
     }
@@ -351,6 +364,8 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
         throw Error(FROST_ERR_INVALID_ARGUMENT, "search: more than 32 boxcar widths");
     if (level.base < p.wmax)
         throw Error(FROST_ERR_INTERNAL, "search: level history shorter than the widest boxcar");
+    if (level.pitch - level.base < ((p.n_valid + kChunk - 1) / kChunk) * kChunk)
+        throw Error(FROST_ERR_INTERNAL, "search: tile columns are not a whole number of chunks");
     const size_t smem = sizeof(float) * (kChunk + p.wmax);
     const dim3 grid(static_cast<unsigned>(g1 - g0));
     if (level.fp16) {

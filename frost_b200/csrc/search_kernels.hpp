@@ -11,6 +11,11 @@
 
 namespace fb::fdmt {
 
+/** Samples per search chunk; level tiles are a whole number of chunks. */
+constexpr int kSearchChunk = 4096;
+/** Column granularity of a level-buffer tile. */
+constexpr int kTileQuantum = kSearchChunk > kTimePerCta ? kSearchChunk : kTimePerCta;
+
 /** One searched row: a DM trial of one plane. */
 struct SearchRow {
     int64_t level_row; // row in its level buffer

@@ -279,7 +279,7 @@ enum frost_storage { FROST_STORAGE_FP32 = 0, FROST_STORAGE_FP16 = 1 };
 
 /* dmt::BoxcarConfig as frost fills it (lib/pipeline/pipeline.cpp:316-330),
  * plus this engine's storage precision and time-tile length (0 = the whole
- * gulp, else a multiple of 2048 samples that bounds device memory). */
+ * gulp, else a multiple of 4096 samples that bounds device memory). */
 typedef struct {
     uint64_t max_boxcar;
     float wtsp;
