@@ -70,9 +70,9 @@ def rfi_config():
     return cfg
 
 
-def layout(nsamps=GULP):
+def layout(nsamps=None):
     from frost_b200.config import BlockLayout, DataType
-    return BlockLayout(NCHANS, nsamps, DataType.UINT8, TSAMP, FCH1, FOFF)
+    return BlockLayout(NCHANS, nsamps or GULP, DataType.UINT8, TSAMP, FCH1, FOFF)
 
 
 def search_config(storage):

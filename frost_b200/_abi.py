@@ -218,3 +218,16 @@ class DedispPlanConfigC(C.Structure):
         ("block_nsamps", C.c_uint64),
         ("subband_depth", C.c_uint64),
     ]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [
+        ("completed", C.c_uint64),
+        ("beams", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("beam_seconds", C.c_double),
+        ("wall_seconds", C.c_double),
+        ("p50_latency_s", C.c_double),
+        ("p99_latency_s", C.c_double),
+        ("max_latency_s", C.c_double),
+    ]

@@ -64,6 +64,18 @@ SIGNATURES = {
     "frost_search_plane_data": (C.c_int, [_vp, _sz, _f32p, _sz]),
     "frost_search_enable_timing": (C.c_int, [_vp, C.c_int]),
     "frost_search_get_timing": (C.c_int, [_vp, C.POINTER(_abi.SearchTimingC)]),
+    "frost_server_create": (C.c_int, [C.c_int, _sz, C.c_uint32, C.POINTER(_vp)]),
+    "frost_server_destroy": (C.c_int, [_vp]),
+    "frost_server_add_beam": (C.c_int, [_vp, C.POINTER(_abi.RfiConfigC), C.POINTER(_abi.BlockLayoutC),
+                                        C.c_float, C.POINTER(_abi.DedispPlanConfigC),
+                                        C.POINTER(_abi.BoxcarConfigC), C.POINTER(C.c_uint32)]),
+    "frost_server_remove_beam": (C.c_int, [_vp, C.c_uint32]),
+    "frost_server_submit": (C.c_int, [_vp, C.c_uint32, _u8p, _sz, _sz, C.POINTER(_u64)]),
+    "frost_server_wait": (C.c_int, [_vp, _u64, C.POINTER(_abi.CandidateC), _sz, C.POINTER(_sz),
+                                    C.POINTER(C.c_double)]),
+    "frost_server_drain": (C.c_int, [_vp, C.c_uint32, C.POINTER(_abi.CandidateC), _sz,
+                                     C.POINTER(_sz)]),
+    "frost_server_get_stats": (C.c_int, [_vp, C.POINTER(_abi.ServerStatsC)]),
 }
 
 

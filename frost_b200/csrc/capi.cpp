@@ -2,6 +2,7 @@
 // implementation, converts exceptions to frost_status codes and records the
 // message for frost_last_error(); nothing throws across this boundary.
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -12,6 +13,7 @@
 #include "host_stats.hpp"
 #include "rfi_cleaner.hpp"
 #include "search_engine.hpp"
+#include "server.hpp"
 
 namespace fb {
 
@@ -63,6 +65,28 @@ struct frost_search {
     fb::fdmt::Engine impl;
     template <class... A> explicit frost_search(A&&... a) : impl(std::forward<A>(a)...) {}
 };
+
+struct frost_server {
+    fb::serve::Server impl;
+    template <class... A> explicit frost_server(A&&... a) : impl(std::forward<A>(a)...) {}
+};
+
+namespace {
+int copy_candidates(const std::vector<frost_candidate>& c, frost_candidate* out, size_t capacity,
+                    size_t* count) {
+    if (count != nullptr)
+        *count = c.size();
+    const size_t n = std::min(capacity, c.size());
+    if (out != nullptr && n)
+        std::memcpy(out, c.data(), n * sizeof(frost_candidate));
+    if (c.size() > capacity) {
+        fb::set_last_error("candidate buffer holds " + std::to_string(capacity) + " of " +
+                           std::to_string(c.size()));
+        return FROST_ERR_OVERFLOW;
+    }
+    return FROST_OK;
+}
+} // namespace
 
 using fb::guarded;
 using fb::invalid;
@@ -377,6 +401,89 @@ int frost_search_capture_planes(frost_search* s, int enable) {
         if (s == nullptr)
             invalid("frost_search_capture_planes: null handle");
         s->impl.capture(enable != 0);
+    });
+}
+
+int frost_server_create(int device, size_t memory_budget, uint32_t slots, frost_server** out) {
+    return guarded([&] {
+        if (out == nullptr)
+            invalid("frost_server_create: null argument");
+        *out = nullptr;
+        *out = new frost_server(device, memory_budget, slots);
+    });
+}
+
+int frost_server_destroy(frost_server* s) {
+    return guarded([&] { delete s; });
+}
+
+int frost_server_add_beam(frost_server* s, const frost_rfi_config* rfi,
+                          const frost_block_layout* layout, float baseline_length,
+                          const frost_dedisp_plan_config* plan, const frost_boxcar_config* search,
+                          uint32_t* beam) {
+    return guarded([&] {
+        if (s == nullptr || rfi == nullptr || layout == nullptr || plan == nullptr ||
+            search == nullptr || beam == nullptr)
+            invalid("frost_server_add_beam: null argument");
+        fb::serve::BeamSpec spec;
+        spec.rfi = *rfi;
+        if (rfi->n_zap_chans)
+            spec.zap_chans.assign(rfi->zap_chans, rfi->zap_chans + rfi->n_zap_chans);
+        if (rfi->n_zap_freqs)
+            spec.zap_freqs.assign(rfi->zap_freqs, rfi->zap_freqs + rfi->n_zap_freqs);
+        spec.layout          = *layout;
+        spec.baseline_length = baseline_length;
+        spec.plan            = *plan;
+        spec.search          = *search;
+        *beam                = s->impl.add_beam(spec);
+    });
+}
+
+int frost_server_remove_beam(frost_server* s, uint32_t beam) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_remove_beam: null handle");
+        s->impl.remove_beam(beam);
+    });
+}
+
+int frost_server_submit(frost_server* s, uint32_t beam, const uint8_t* block, size_t block_bytes,
+                        size_t nread, uint64_t* ticket) {
+    return guarded([&] {
+        if (s == nullptr || ticket == nullptr)
+            invalid("frost_server_submit: null argument");
+        *ticket = s->impl.submit(beam, block, block_bytes, nread);
+    });
+}
+
+int frost_server_wait(frost_server* s, uint64_t ticket, frost_candidate* out, size_t capacity,
+                      size_t* count, double* latency_s) {
+    int rc = FROST_OK;
+    const int g = guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_wait: null handle");
+        const auto c = s->impl.wait(ticket, latency_s);
+        rc           = copy_candidates(c, out, capacity, count);
+    });
+    return g != FROST_OK ? g : rc;
+}
+
+int frost_server_drain(frost_server* s, uint32_t beam, frost_candidate* out, size_t capacity,
+                       size_t* count) {
+    int rc = FROST_OK;
+    const int g = guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_drain: null handle");
+        rc = copy_candidates(s->impl.drain(beam), out, capacity, count);
+    });
+    return g != FROST_OK ? g : rc;
+}
+
+int frost_server_get_stats(frost_server* s, frost_server_stats* out) {
+    return guarded([&] {
+        if (s == nullptr || out == nullptr)
+            invalid("frost_server_get_stats: null argument");
+        *out = s->impl.stats();
     });
 }
 

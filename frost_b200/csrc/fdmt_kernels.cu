@@ -127,6 +127,196 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// dst[0..8) = lo[0..8) + stage[off + e .. off + e + 8): `lo` and `dst` are
+// 16-byte aligned (global or shared), `stage` is the 16-byte aligned staged
+// high-child segment, e = 8 * thread.
+template <class S>
+__device__ __forceinline__ void merge8(const S* lo, const S* stage, int e, int off, S* dst) {
+    if constexpr (sizeof(S) == 4) {
+        const float4* l4 = reinterpret_cast<const float4*>(lo);
+        const float4 a0 = l4[0], a1 = l4[1];
+        const float4* h4 = reinterpret_cast<const float4*>(stage) + e / 4;
+        const float4 b0 = h4[0], b1 = h4[1], b2 = h4[2]; // b2 unused when off == 0
+        const float h[12] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
+        float g[8];
+        switch (off) {
+#define FB_PICK(O)                                                                                \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 8; ++i) g[i] = h[O + i];                             \
+        break;
+            FB_PICK(0) FB_PICK(1) FB_PICK(2) FB_PICK(3)
+#undef FB_PICK
+        }
+        float4* d4 = reinterpret_cast<float4*>(dst);
+        d4[0]      = make_float4(a0.x + g[0], a0.y + g[1], a0.z + g[2], a0.w + g[3]);
+        d4[1]      = make_float4(a1.x + g[4], a1.y + g[5], a1.z + g[6], a1.w + g[7]);
+    } else {
+        const uint4 a   = *reinterpret_cast<const uint4*>(lo);
+        const uint4* sv = reinterpret_cast<const uint4*>(stage) + e / 8;
+        const uint4 b0 = sv[0], b1 = sv[1]; // b1 unused when off == 0
+        const uint32_t w[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        uint32_t g[4];
+        switch (off) {
+#define FB_PICK_EVEN(O)                                                                           \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] = w[O / 2 + i];                         \
+        break;
+#define FB_PICK_ODD(O)                                                                            \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] =                                      \
+            __byte_perm(w[O / 2 + i], w[O / 2 + i + 1], 0x5432);                                  \
+        break;
+            FB_PICK_EVEN(0) FB_PICK_ODD(1) FB_PICK_EVEN(2) FB_PICK_ODD(3)
+            FB_PICK_EVEN(4) FB_PICK_ODD(5) FB_PICK_EVEN(6) FB_PICK_ODD(7)
+#undef FB_PICK_EVEN
+#undef FB_PICK_ODD
+        }
+        const uint32_t av[4] = {a.x, a.y, a.z, a.w};
+        uint32_t r[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 x = __half22float2(*reinterpret_cast<const __half2*>(&av[i]));
+            const float2 y = __half22float2(*reinterpret_cast<const __half2*>(&g[i]));
+            const float lo_sum = fminf(fmaxf(x.x + y.x, -65504.0F), 65504.0F);
+            const float hi_sum = fminf(fmaxf(x.y + y.y, -65504.0F), 65504.0F);
+            const __half2 s    = __floats2half2_rn(lo_sum, hi_sum);
+            r[i]               = *reinterpret_cast<const uint32_t*>(&s);
+        }
+        *reinterpret_cast<uint4*>(dst) = make_uint4(r[0], r[1], r[2], r[3]);
+    }
+}
+
+// ---- TMA-pipelined level kernel ------------------------------------------
+//
+// One CTA per (output row, run of kTilesPerCta time tiles). Thread 0 keeps
+// kStages tiles in flight with 1-D bulk async copies (cp.async.bulk, local
+// global memory only, no multicast) of the unshifted child segment and the
+// 16-byte-aligned superset of the shifted one, each stage completing on its
+// own mbarrier; all threads combine a landed stage from shared memory and
+// store 16-byte vectors. Every wait is bounded: a wait that runs out sets
+// *err and the CTA drains its copies (again bounded) and returns.
+
+constexpr int kStages      = 4;
+constexpr int kTilesPerCta = 16;
+constexpr long kSpinLimit  = 1L << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t phase) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (long it = 0; it < kSpinLimit; ++it)
+        if (mbar_try(bar, phase))
+            return true;
+    return false;
+}
+
+template <class S>
+__global__ void __launch_bounds__(kThreads)
+    k_level_pipe(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
+                 int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
+                 int32_t ntiles, unsigned* __restrict__ err) {
+    constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
+    constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
+    constexpr int kHiBytes  = kLoBytes + 16;
+    constexpr int kStageBytes = kLoBytes + kHiBytes;
+    extern __shared__ __align__(128) unsigned char pipe_smem[];
+    __shared__ __align__(8) uint64_t bar[kStages];
+    __shared__ int abort_flag;
+
+    const RowOp op  = ops[blockIdx.x];
+    const int tile0 = blockIdx.y * kTilesPerCta;
+    const int nt    = min(kTilesPerCta, ntiles - tile0);
+    if (nt <= 0)
+        return;
+    const bool has_hi = op.hi_row >= 0;
+    const S* lo_row   = in + static_cast<int64_t>(op.lo_row) * in_pitch + in_base;
+    const S* hi_base  = in + static_cast<int64_t>(has_hi ? op.hi_row : op.lo_row) * in_pitch;
+    S* dst_row        = out + static_cast<int64_t>(blockIdx.x) * out_pitch + out_base;
+    // the shifted segment's offset inside its aligned superset is the same
+    // for every tile (tiles start at multiples of kTimePerCta)
+    const int64_t e_first = static_cast<int64_t>(in_base) - op.shift;
+    const int off         = static_cast<int>(((e_first % VEC) + VEC) % VEC);
+    const uint32_t hi_bytes = has_hi ? static_cast<uint32_t>((kTimePerCta / VEC + (off > 0 ? 1 : 0)) * 16) : 0U;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < kStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bar[s])), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    auto issue = [&](int i) {
+        const int s        = i % kStages;
+        const int64_t k0   = static_cast<int64_t>(tile0 + i) * kTimePerCta;
+        unsigned char* st  = pipe_smem + s * kStageBytes;
+        const uint32_t b   = smem_addr(&bar[s]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b),
+                     "r"(static_cast<uint32_t>(kLoBytes) + hi_bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_addr(st)),
+            "l"(lo_row + k0), "r"(static_cast<uint32_t>(kLoBytes)), "r"(b)
+            : "memory");
+        if (has_hi) {
+            const int64_t v0 = (e_first + k0 - off) / VEC; // aligned start, in vectors
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(st + kLoBytes)),
+                "l"(hi_base + v0 * VEC), "r"(hi_bytes), "r"(b)
+                : "memory");
+        }
+    };
+
+    if (threadIdx.x == 0)
+        for (int i = 0; i < min(kStages, nt); ++i)
+            issue(i);
+    const int e = 8 * threadIdx.x;
+    int i       = 0;
+    for (; i < nt; ++i) {
+        const int s           = i % kStages;
+        const uint32_t phase  = static_cast<uint32_t>((i / kStages) & 1);
+        if (!mbar_wait(smem_addr(&bar[s]), phase))
+            atomicExch(&abort_flag, 1);
+        __syncthreads();
+        if (abort_flag)
+            break;
+        const S* lo_s = reinterpret_cast<const S*>(pipe_smem + s * kStageBytes);
+        const S* hi_s = reinterpret_cast<const S*>(pipe_smem + s * kStageBytes + kLoBytes);
+        S* dst        = dst_row + static_cast<int64_t>(tile0 + i) * kTimePerCta + e;
+        if (has_hi) {
+            merge8<S>(lo_s + e, hi_s, e, off, dst);
+        } else {
+            const uint4* s4 = reinterpret_cast<const uint4*>(lo_s + e);
+            uint4* d4       = reinterpret_cast<uint4*>(dst);
+            for (int v = 0; v < 8 / VEC; ++v)
+                d4[v] = s4[v];
+        }
+        __syncthreads(); // every thread is done with stage s
+        if (threadIdx.x == 0 && i + kStages < nt)
+            issue(i + kStages);
+    }
+    if (i < nt && threadIdx.x == 0) {
+        // a wait ran out: report it, then let the copies still in flight land
+        atomicOr(err, 1U);
+        for (int j = i; j < min(nt, i + kStages); ++j)
+            (void)mbar_wait(smem_addr(&bar[j % kStages]), static_cast<uint32_t>((j / kStages) & 1));
+    }
+}
+
 template <class S>
 __global__ void __launch_bounds__(kThreads)
     k_level(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
@@ -268,21 +458,44 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
 }
 
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  cudaStream_t s) {
+                  unsigned* err, cudaStream_t s) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
-        out.pitch % 8 != 0)
+        out.pitch % 8 != 0 || in.fp16 != out.fp16)
         throw Error(FROST_ERR_INTERNAL, "level: bad geometry");
-    const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>(ncols / kTimePerCta));
-    if (out.fp16)
-        k_level<__half><<<grid, kThreads, 0, s>>>(ops, static_cast<const __half*>(in.data), in.pitch,
-                                                  in.base, static_cast<__half*>(out.data),
-                                                  out.pitch, out.base);
-    else
-        k_level<float><<<grid, kThreads, 0, s>>>(ops, static_cast<const float*>(in.data), in.pitch,
-                                                 in.base, static_cast<float*>(out.data), out.pitch,
-                                                 out.base);
+    const int ntiles = ncols / kTimePerCta;
+    if (err == nullptr) {
+        // direct form (no bulk copies): one CTA per (row, tile)
+        const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>(ntiles));
+        if (out.fp16)
+            k_level<__half><<<grid, kThreads, 0, s>>>(ops, static_cast<const __half*>(in.data), in.pitch,
+                                                      in.base, static_cast<__half*>(out.data),
+                                                      out.pitch, out.base);
+        else
+            k_level<float><<<grid, kThreads, 0, s>>>(ops, static_cast<const float*>(in.data), in.pitch,
+                                                     in.base, static_cast<float*>(out.data), out.pitch,
+                                                     out.base);
+        FB_LAUNCH_CHECK();
+        return;
+    }
+    const dim3 grid(static_cast<unsigned>(nrows),
+                    static_cast<unsigned>((ntiles + kTilesPerCta - 1) / kTilesPerCta));
+    const size_t es   = out.fp16 ? 2 : 4;
+    const size_t smem = kStages * (2 * kTimePerCta * es + 16);
+    if (out.fp16) {
+        FB_CUDA(cudaFuncSetAttribute(k_level_pipe<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_level_pipe<__half><<<grid, kThreads, smem, s>>>(
+            ops, static_cast<const __half*>(in.data), in.pitch, in.base,
+            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, err);
+    } else {
+        FB_CUDA(cudaFuncSetAttribute(k_level_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_level_pipe<float><<<grid, kThreads, smem, s>>>(
+            ops, static_cast<const float*>(in.data), in.pitch, in.base,
+            static_cast<float*>(out.data), out.pitch, out.base, ntiles, err);
+    }
     FB_LAUNCH_CHECK();
 }
 

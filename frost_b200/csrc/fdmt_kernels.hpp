@@ -29,9 +29,11 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
                    int64_t t0, int32_t n_valid, const float* input_hist, int32_t hist_len,
                    LevelView out, int32_t ncols, cudaStream_t s);
 
-/** Level h >= 2: out[row] = in[lo] + in[hi] shifted. */
+/** Level h >= 2: out[row] = in[lo] + in[hi] shifted. With `err` non-null
+ * the TMA-pipelined kernel runs and sets *err if a bounded wait ran out;
+ * with `err` null the direct (one CTA per row and tile) kernel runs. */
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  cudaStream_t s);
+                  unsigned* err, cudaStream_t s);
 
 /** Copies the last `hist` columns ending at column base + n_valid of every
  * row of `view` into hist_buf[rows][hist]. */

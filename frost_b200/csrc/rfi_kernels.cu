@@ -67,6 +67,10 @@ template <int D> __device__ __forceinline__ float rd(const uint8_t* __restrict__
     default: throw ::fb::Error(FROST_ERR_INVALID_ARGUMENT, "unsupported dtype");                 \
     }
 
+// Rows fetched ahead per thread in the time-ordered (window or chunk,
+// channel) loops: the loads are independent, only the sums are sequential.
+constexpr int kBlock = 16;
+
 // ---- order-exact helpers ------------------------------------------------
 
 // std::min / std::max semantics (first argument kept on ties), which the
@@ -277,22 +281,32 @@ __global__ void k_moments(Dims d, const uint8_t* __restrict__ raw, const float* 
     if (static_mask[c] != 0 && iv != 0.0F) {
         const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
         double prev      = 0.0;
-        for (uint64_t t = b; t < e; ++t) {
-            const float x   = rd<D>(raw + t * d.row_bytes, c);
-            const double z  = (x - l) * iv;
-            const double z2 = z * z;
-            s.n += 1.0;
-            s.s1 += z;
-            s.s2 += z2;
-            s.s3 += z2 * z;
-            s.s4 += z2 * z2;
-            if (t > b)
-                s.lag += z * prev;
-            prev = z;
-            if (fabs(z) <= clip) {
-                s.nc += 1.0;
-                s.c1 += z;
-                s.c2 += z2;
+        // Rows are fetched kBlock at a time (independent loads in flight),
+        // then consumed strictly in time order.
+        for (uint64_t t0 = b; t0 < e; t0 += kBlock) {
+            float xs[kBlock];
+#pragma unroll
+            for (int j = 0; j < kBlock; ++j)
+                xs[j] = t0 + j < e ? rd<D>(raw + (t0 + j) * d.row_bytes, c) : 0.0F;
+#pragma unroll
+            for (int j = 0; j < kBlock; ++j) {
+                if (t0 + j >= e)
+                    break;
+                const double z  = (xs[j] - l) * iv;
+                const double z2 = z * z;
+                s.n += 1.0;
+                s.s1 += z;
+                s.s2 += z2;
+                s.s3 += z2 * z;
+                s.s4 += z2 * z2;
+                if (t0 + j > b)
+                    s.lag += z * prev;
+                prev = z;
+                if (fabs(z) <= clip) {
+                    s.nc += 1.0;
+                    s.c1 += z;
+                    s.c2 += z2;
+                }
             }
         }
     }
@@ -413,31 +427,43 @@ __global__ void k_scan_cols(Dims d, const uint8_t* __restrict__ raw, const float
     if (mask[c] != 0) {
         const uint64_t t0 = k * d.chunk;
         const uint64_t t1 = (t0 + d.chunk < d.nsamps) ? t0 + d.chunk : d.nsamps;
-        for (uint64_t t = t0; t < t1; ++t) {
-            const uint64_t w = window_of(t, d.window, d.nwin);
-            const uint64_t o = w * n + c;
-            const float x    = rd<D>(raw + t * d.row_bytes, c);
-            const float iv   = inv[o];
-            float z          = 0.0F;
-            if (iv == 0.0F) {
-                cmin = smin(cmin, x);
-                cmax = smax(cmax, x);
-            } else {
-                z = (x - loc[o]) * iv;
-            }
-            const bool outlier = fabsf(z) > clip;
-            if (zdot && !outlier && iv != 0.0F) {
-                const double sk = s_keep_d[t];
-                zs.n += 1.0;
-                zs.sz += z;
-                zs.ss += sk;
-                zs.sss += sk * sk;
-                zs.szs += z * sk;
-            }
-            if (kchan) {
-                const double u = outlier ? 0.0 : static_cast<double>((z - clip_mean[o]) * clip_inv_std[o]);
-                kpos.append(static_cast<int64_t>(t), u);
-                kneg.append(static_cast<int64_t>(t), -u);
+        for (uint64_t tb = t0; tb < t1; tb += kBlock) {
+            // fetch kBlock rows ahead of their sequential use
+            float xs[kBlock];
+#pragma unroll
+            for (int q = 0; q < kBlock; ++q)
+                xs[q] = tb + q < t1 ? rd<D>(raw + (tb + q) * d.row_bytes, c) : 0.0F;
+#pragma unroll
+            for (int q = 0; q < kBlock; ++q) {
+                const uint64_t t = tb + q;
+                if (t >= t1)
+                    break;
+                const uint64_t w = window_of(t, d.window, d.nwin);
+                const uint64_t o = w * n + c;
+                const float x    = xs[q];
+                const float iv   = inv[o];
+                float z          = 0.0F;
+                if (iv == 0.0F) {
+                    cmin = smin(cmin, x);
+                    cmax = smax(cmax, x);
+                } else {
+                    z = (x - loc[o]) * iv;
+                }
+                const bool outlier = fabsf(z) > clip;
+                if (zdot && !outlier && iv != 0.0F) {
+                    const double sk = s_keep_d[t];
+                    zs.n += 1.0;
+                    zs.sz += z;
+                    zs.ss += sk;
+                    zs.sss += sk * sk;
+                    zs.szs += z * sk;
+                }
+                if (kchan) {
+                    const double u =
+                        outlier ? 0.0 : static_cast<double>((z - clip_mean[o]) * clip_inv_std[o]);
+                    kpos.append(static_cast<int64_t>(t), u);
+                    kneg.append(static_cast<int64_t>(t), -u);
+                }
             }
         }
     }
@@ -731,11 +757,21 @@ __global__ void k_welford(Dims d, const float* __restrict__ work, float* __restr
         return;
     const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
     double mean = 0.0, var = 0.0;
-    for (uint64_t t = b; t < e; ++t) {
-        const double x     = work[t * d.nchans + c];
-        const double delta = x - mean;
-        mean += delta / static_cast<double>(t - b + 1);
-        var += delta * (x - mean);
+    for (uint64_t tb = b; tb < e; tb += kBlock) {
+        float xs[kBlock];
+#pragma unroll
+        for (int q = 0; q < kBlock; ++q)
+            xs[q] = tb + q < e ? work[(tb + q) * d.nchans + c] : 0.0F;
+#pragma unroll
+        for (int q = 0; q < kBlock; ++q) {
+            const uint64_t t = tb + q;
+            if (t >= e)
+                break;
+            const double x     = xs[q];
+            const double delta = x - mean;
+            mean += delta / static_cast<double>(t - b + 1);
+            var += delta * (x - mean);
+        }
     }
     loc[w * d.nchans + c]   = static_cast<float>(mean);
     scale[w * d.nchans + c] = e > b ? static_cast<float>(sqrt(var / static_cast<double>(e - b))) : 0.0F;

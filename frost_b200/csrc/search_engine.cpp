@@ -421,7 +421,9 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
             } else {
                 timed(kLevel, s, [&] {
                     launch_level(m_row_ops.as<RowOp>() + m_row_op_offset[h], m_plan.level_rows(h),
-                                 view(h - 1), out, static_cast<int32_t>(m_ncols), s);
+                                 view(h - 1), out, static_cast<int32_t>(m_ncols),
+                                 reinterpret_cast<unsigned*>(m_counters.as<unsigned long long>() + 3),
+                                 s);
                 });
                 m_launches += 1;
                 m_timing.level_launches += 1;
@@ -475,6 +477,9 @@ void Engine::collect(cudaStream_t s) {
     unsigned long long counters[4];
     FB_CUDA(cudaMemcpyAsync(counters, m_counters.get(), sizeof(counters), cudaMemcpyDeviceToHost, s));
     FB_CUDA(cudaStreamSynchronize(s));
+    if (counters[3] != 0)
+        throw Error(FROST_ERR_TIMEOUT, "search: a level kernel's bounded wait for its bulk copies ran "
+                                       "out; this call's results are incomplete");
     const uint64_t n = std::min<uint64_t>(counters[0], m_cfg.max_candidates);
     m_results.resize(n);
     if (n)

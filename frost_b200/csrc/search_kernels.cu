@@ -198,8 +198,10 @@ __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float
     }
 }
 
-template <class S>
-__global__ void __launch_bounds__(kThreads)
+// NW > 0: the width count as a compile-time constant (steady-state fast
+// path in registers); NW == 0: any width count.
+template <class S, int NW>
+__global__ void __launch_bounds__(kThreads, 4)
     k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0) {
     extern __shared__ float P[];
     __shared__ uint32_t bits[kMaxWidths][kWords];
@@ -230,6 +232,16 @@ __global__ void __launch_bounds__(kThreads)
     if (threadIdx.x < nruns && !all)
         runs[threadIdx.x] = p.carry[g * nruns + threadIdx.x];
     __syncthreads();
+    int Wr[NW > 0 ? NW : 1], Er[NW > 0 ? NW : 1];
+    float Tr[NW > 0 ? NW : 1];
+    if constexpr (NW > 0) {
+#pragma unroll
+        for (int wi = 0; wi < NW; ++wi) {
+            Wr[wi] = rc.W[wi];
+            Er[wi] = rc.E[wi];
+            Tr[wi] = rc.thr[wi];
+        }
+    }
 
     const S* src = level + row.level_row * pitch + base;
     const int N  = kChunk + wmax;
@@ -244,16 +256,43 @@ __global__ void __launch_bounds__(kThreads)
         const bool fast = c0 + kChunk <= p.n_valid && (!p.skip_cold || p.tile_t0 + c0 >= warm) &&
                           (!p.or_active || p.tile_t0 + c0 - p.gulp_t0 >= warm);
         uint32_t any = 0;
-        for (int wi = 0; wi < nw; ++wi) {
-            const int W     = rc.W[wi];
-            const int E     = rc.E[wi];
-            const float thr = rc.thr[wi];
-#pragma unroll 4
-            for (int j = 0; j < kPerThread; ++j) {
-                const int k = threadIdx.x + j * kThreads;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if constexpr (NW > 0) {
+            if (fast && !all) {
+                // steady state with the width count known at compile time:
+                // widths and thresholds live in registers
+#pragma unroll 1
+                for (int j = 0; j < kPerThread; ++j) {
+                    const int i    = threadIdx.x + j * kThreads + wmax;
+                    const float pi = P[i];
+#pragma unroll
+                    for (int wi = 0; wi < NW; ++wi) {
+                        float s = pi - P[i - Wr[wi]];
+                        if (Er[wi] > 0)
+                            s -= 0.5F * ((pi - P[i - Er[wi]]) + (P[i - Wr[wi] + Er[wi]] - P[i - Wr[wi]]));
+                        const uint32_t m = __ballot_sync(0xFFFFFFFFU, s > Tr[wi]);
+                        if (lane == 0)
+                            bits[wi][j * (kThreads / 32) + warp] = m;
+                        any |= m;
+                    }
+                }
+            }
+        }
+        const bool generic = NW == 0 || !fast || all;
+        for (int j = 0; generic && j < kPerThread; ++j) {
+            // one sample, every width: its prefix value is read once
+            const int k  = threadIdx.x + j * kThreads;
+            const int i  = k + wmax;
+            const float pi = P[i];
+            for (int wi = 0; wi < nw; ++wi) {
                 bool up;
                 if (fast) {
-                    up = wsum(P, k + wmax, W, E) > thr;
+                    const int W = rc.W[wi];
+                    const int E = rc.E[wi];
+                    float s     = pi - P[i - W];
+                    if (E > 0)
+                        s -= 0.5F * ((pi - P[i - E]) + (P[i - W + E] - P[i - W]));
+                    up = s > rc.thr[wi];
                 } else {
                     up = snr_general(p, rc, P, wmax, c0, k, wi, row.delay) > p.thresh;
                 }
@@ -265,8 +304,8 @@ __global__ void __launch_bounds__(kThreads)
                     emit(p, row, r, &local_count);
                 }
                 const uint32_t m = __ballot_sync(0xFFFFFFFFU, up);
-                if ((threadIdx.x & 31) == 0)
-                    bits[wi][j * (kThreads / 32) + (threadIdx.x >> 5)] = m;
+                if (lane == 0)
+                    bits[wi][j * (kThreads / 32) + warp] = m;
                 any |= m;
             }
         }
@@ -368,16 +407,26 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
         throw Error(FROST_ERR_INTERNAL, "search: tile columns are not a whole number of chunks");
     const size_t smem = sizeof(float) * (kChunk + p.wmax);
     const dim3 grid(static_cast<unsigned>(g1 - g0));
-    if (level.fp16) {
-        FB_CUDA(cudaFuncSetAttribute(k_search<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    auto go = [&](auto kernel, auto data) {
+        FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-        k_search<__half><<<grid, kThreads, smem, s>>>(p, static_cast<const __half*>(level.data),
-                                                      level.pitch, level.base, g0);
-    } else {
-        FB_CUDA(cudaFuncSetAttribute(k_search<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-        k_search<float><<<grid, kThreads, smem, s>>>(p, static_cast<const float*>(level.data),
-                                                     level.pitch, level.base, g0);
+        kernel<<<grid, kThreads, smem, s>>>(p, data, level.pitch, level.base, g0);
+    };
+    // width counts of wtsp = 2 with max_boxcar 16, 64, 256 and 4096
+    switch (level.fp16 ? 100 + p.nwidths : p.nwidths) {
+    case 5: go(k_search<float, 5>, static_cast<const float*>(level.data)); break;
+    case 7: go(k_search<float, 7>, static_cast<const float*>(level.data)); break;
+    case 9: go(k_search<float, 9>, static_cast<const float*>(level.data)); break;
+    case 13: go(k_search<float, 13>, static_cast<const float*>(level.data)); break;
+    case 105: go(k_search<__half, 5>, static_cast<const __half*>(level.data)); break;
+    case 107: go(k_search<__half, 7>, static_cast<const __half*>(level.data)); break;
+    case 109: go(k_search<__half, 9>, static_cast<const __half*>(level.data)); break;
+    case 113: go(k_search<__half, 13>, static_cast<const __half*>(level.data)); break;
+    default:
+        if (level.fp16)
+            go(k_search<__half, 0>, static_cast<const __half*>(level.data));
+        else
+            go(k_search<float, 0>, static_cast<const float*>(level.data));
     }
     FB_LAUNCH_CHECK();
 }

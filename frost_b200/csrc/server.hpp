@@ -1,0 +1,106 @@
+// Serving loop: many beams on one GPU, each with its RFI calibration and
+// FDMT tails resident, gulps admitted as worker slots free up so one beam's
+// host-side phases overlap other beams' kernels (continuous batching at the
+// stream level), beams admitted by device memory, and per-gulp latency
+// (arrival -> candidates ready) recorded for p50/p99.
+#pragma once
+
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "common.hpp"
+#include "rfi_cleaner.hpp"
+#include "search_engine.hpp"
+
+namespace fb::serve {
+
+struct BeamSpec {
+    frost_rfi_config rfi;
+    std::vector<frost_channel_range> zap_chans;
+    std::vector<frost_frequency_range> zap_freqs;
+    frost_block_layout layout;
+    float baseline_length;
+    frost_dedisp_plan_config plan;
+    frost_boxcar_config search;
+};
+
+/** One beam's resident state and its per-gulp body (Pipeline::execute_block's
+ * hot path, lib/pipeline/pipeline.cpp:529-619). */
+class Beam {
+public:
+    Beam(const BeamSpec& spec, int device);
+    /** Cleans and searches one gulp (host block, block rows, nread valid). */
+    void process(const uint8_t* block, SizeType bytes, SizeType nread);
+    std::vector<frost_candidate> results() const { return m_engine->results(); }
+    std::vector<frost_candidate> drain();
+    uint64_t samples_searched() const { return m_searched; }
+    double tsamp() const { return m_spec.layout.tsamp; }
+    SizeType device_bytes() const;
+    SizeType block_bytes() const;
+
+private:
+    BeamSpec m_spec;
+    std::unique_ptr<rfi::Cleaner> m_cleaner;
+    std::unique_ptr<fdmt::Engine> m_engine;
+    bool m_descending;
+    std::vector<uint8_t> m_fdmt_mask;
+    uint64_t m_read = 0, m_searched = 0, m_max_delay = 0;
+};
+
+struct Request {
+    uint64_t ticket;
+    uint32_t beam;
+    const uint8_t* block;
+    SizeType bytes;
+    SizeType nread;
+    double arrival;  // steady seconds
+    double done = 0;
+    bool finished = false;
+    int status    = FROST_OK;
+    std::string error;
+    std::vector<frost_candidate> cands;
+};
+
+class Server {
+public:
+    Server(int device, SizeType memory_budget, uint32_t slots);
+    ~Server();
+    uint32_t add_beam(const BeamSpec& spec);
+    void remove_beam(uint32_t beam);
+    uint64_t submit(uint32_t beam, const uint8_t* block, SizeType bytes, SizeType nread);
+    /** Blocks until the ticket is done; moves its candidates out. */
+    std::vector<frost_candidate> wait(uint64_t ticket, double* latency_s);
+    frost_server_stats stats();
+    std::vector<frost_candidate> drain(uint32_t beam);
+
+private:
+    int m_device;
+    SizeType m_budget, m_used = 0;
+    std::mutex m_mu;
+    std::condition_variable m_work_cv, m_done_cv;
+    bool m_stop = false;
+    uint64_t m_next_ticket = 1;
+    uint32_t m_next_beam = 0;
+    std::map<uint32_t, std::unique_ptr<Beam>> m_beams;
+    std::map<uint32_t, std::deque<uint64_t>> m_queue; // per-beam FIFO of tickets
+    std::map<uint32_t, bool> m_busy;
+    std::map<uint32_t, SizeType> m_charge; // device bytes charged at admission
+    std::map<uint64_t, std::shared_ptr<Request>> m_requests;
+    std::vector<double> m_latencies;
+    double m_beam_seconds = 0, m_first_arrival = -1, m_last_done = 0;
+    uint64_t m_completed = 0;
+    std::vector<std::thread> m_workers;
+
+    void worker();
+    bool pick(uint32_t& beam, std::shared_ptr<Request>& req);
+};
+
+double now_seconds();
+
+} // namespace fb::serve

@@ -1,0 +1,112 @@
+"""Many beams searched on one GPU through the C ABI's server
+(frost_server_*): each beam keeps its RFI calibration and FDMT tails
+resident, beams are admitted by device memory, and queued gulps are taken by
+worker slots oldest first, one gulp per beam at a time. frost itself runs one
+beam per process and overlaps only the read of the next gulp
+(GulpPrefetch, lib/pipeline/pipeline.cpp:109-262)."""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Dict, Tuple
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, lib
+from .config import BlockLayout, BoxcarConfig, DedispPlanConfig, RfiConfig
+from .search import CANDIDATE_DTYPE, _boxcar_c
+
+
+@dataclass
+class ServerStats:
+    completed: int
+    beams: int
+    device_bytes: int
+    beam_seconds: float
+    wall_seconds: float
+    p50_latency_s: float
+    p99_latency_s: float
+    max_latency_s: float
+
+    @property
+    def beam_seconds_per_second(self) -> float:
+        return self.beam_seconds / self.wall_seconds if self.wall_seconds > 0 else 0.0
+
+
+class BeamServer:
+    def __init__(self, device: int = 0, memory_budget: int = 0, slots: int = 4):
+        h = C.c_void_p()
+        check(lib().frost_server_create(device, memory_budget, slots, C.byref(h)))
+        self._h = h
+        self._capacity: Dict[int, int] = {}
+        self._beam_of: Dict[int, int] = {}
+        self._blocks: Dict[int, np.ndarray] = {}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().frost_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_beam(self, rfi_cfg: RfiConfig, layout: BlockLayout, baseline_length: float,
+                 plan: DedispPlanConfig, search_cfg: BoxcarConfig) -> int:
+        """Admits a beam; raises FrostError(ERR_OUT_OF_MEMORY) when its
+        device memory would exceed the server's budget."""
+        c, keep = rfi_cfg.to_c()
+        lay, pc, bc = layout.to_c(), plan.to_c(), _boxcar_c(search_cfg)
+        beam = C.c_uint32()
+        check(lib().frost_server_add_beam(self._h, C.byref(c), C.byref(lay), C.c_float(baseline_length),
+                                          C.byref(pc), C.byref(bc), C.byref(beam)))
+        # results of one gulp never exceed the engine's max_candidates
+        self._capacity[beam.value] = max(1, int(search_cfg.max_candidates))
+        return beam.value
+
+    def remove_beam(self, beam: int):
+        check(lib().frost_server_remove_beam(self._h, beam))
+        self._capacity.pop(beam, None)
+
+    def submit(self, beam: int, block: np.ndarray, nread: int) -> int:
+        """Queues one gulp (a whole host block of max_nsamps rows, `nread`
+        valid); the block is kept alive until wait() returns its ticket."""
+        buf = np.ascontiguousarray(block).view(np.uint8).reshape(-1)
+        ticket = C.c_uint64()
+        check(lib().frost_server_submit(self._h, beam, buf.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                        buf.size, nread, C.byref(ticket)))
+        self._blocks[ticket.value] = buf
+        self._beam_of[ticket.value] = beam
+        return ticket.value
+
+    def wait(self, ticket: int) -> Tuple[np.ndarray, float]:
+        """Candidates of the gulp (sorted as the engine's results) and its
+        latency from submit to candidates ready, in seconds."""
+        cap = self._capacity[self._beam_of[ticket]]
+        out = np.zeros(cap, CANDIDATE_DTYPE)
+        n, lat = C.c_size_t(), C.c_double()
+        try:
+            check(lib().frost_server_wait(self._h, ticket, out.ctypes.data_as(C.POINTER(_abi.CandidateC)),
+                                          cap, C.byref(n), C.byref(lat)))
+        finally:
+            self._blocks.pop(ticket, None)
+            self._beam_of.pop(ticket, None)
+        return out[:n.value], lat.value
+
+    def drain(self, beam: int) -> np.ndarray:
+        cap = self._capacity[beam]
+        out = np.zeros(cap, CANDIDATE_DTYPE)
+        n = C.c_size_t()
+        check(lib().frost_server_drain(self._h, beam, out.ctypes.data_as(C.POINTER(_abi.CandidateC)),
+                                       cap, C.byref(n)))
+        return out[:n.value]
+
+    def stats(self) -> ServerStats:
+        s = _abi.ServerStatsC()
+        check(lib().frost_server_get_stats(self._h, C.byref(s)))
+        return ServerStats(s.completed, s.beams, s.device_bytes, s.beam_seconds, s.wall_seconds,
+                           s.p50_latency_s, s.p99_latency_s, s.max_latency_s)

@@ -457,6 +457,76 @@ typedef struct {
 int frost_search_enable_timing(frost_search* s, int enable);
 int frost_search_get_timing(const frost_search* s, frost_search_timing* out);
 
+/* ---- serving: many beams on one GPU -------------------------------------
+ *
+ * frost runs one beam per process and reads its next gulp on a side thread
+ * while the current one is searched (GulpPrefetch,
+ * lib/pipeline/pipeline.cpp:109-262). The server runs many beams on one
+ * GPU: each beam keeps its RFI calibration and FDMT tails resident; beams
+ * are admitted by device memory; gulps are taken by `slots` worker threads
+ * as they arrive, oldest first, one gulp per beam at a time (a beam's gulps
+ * stay in order), so one beam's host-side phases overlap other beams'
+ * kernels. Latency is measured from submit to candidates ready. */
+
+typedef struct {
+    uint64_t completed;
+    uint64_t beams;
+    uint64_t device_bytes; /* charged to admitted beams */
+    double beam_seconds;   /* data searched (valid samples x tsamp) */
+    double wall_seconds;   /* first arrival to last completion */
+    double p50_latency_s;
+    double p99_latency_s;
+    double max_latency_s;
+} frost_server_stats;
+
+typedef struct frost_server frost_server;
+
+/* memory_budget 0 = 90% of the device's free memory. */
+int frost_server_create(int device, size_t memory_budget, uint32_t slots, frost_server** out);
+int frost_server_destroy(frost_server* s);
+
+/* Admits a beam (RFICleaner + search engine, plan.block_nsamps ==
+ * layout.max_nsamps) or fails with FROST_ERR_OUT_OF_MEMORY when its device
+ * memory would exceed the budget. */
+int frost_server_add_beam(frost_server* s,
+                          const frost_rfi_config* rfi,
+                          const frost_block_layout* layout,
+                          float baseline_length,
+                          const frost_dedisp_plan_config* plan,
+                          const frost_boxcar_config* search,
+                          uint32_t* beam);
+
+/* Waits for the beam's queued gulps, then releases it. */
+int frost_server_remove_beam(frost_server* s, uint32_t beam);
+
+/* Queues one gulp (a host block of max_nsamps rows, `nread` valid); the
+ * block must stay valid until frost_server_wait returns for the ticket. */
+int frost_server_submit(frost_server* s,
+                        uint32_t beam,
+                        const uint8_t* block,
+                        size_t block_bytes,
+                        size_t nread,
+                        uint64_t* ticket);
+
+/* Blocks until the gulp is searched; copies up to `capacity` candidates
+ * (sorted as frost_search_results), sets *count to the total and returns
+ * FROST_ERR_OVERFLOW if some did not fit. */
+int frost_server_wait(frost_server* s,
+                      uint64_t ticket,
+                      frost_candidate* out,
+                      size_t capacity,
+                      size_t* count,
+                      double* latency_s);
+
+/* drain() of one beam's engine (end of its stream). */
+int frost_server_drain(frost_server* s,
+                       uint32_t beam,
+                       frost_candidate* out,
+                       size_t capacity,
+                       size_t* count);
+
+int frost_server_get_stats(frost_server* s, frost_server_stats* out);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

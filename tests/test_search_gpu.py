@@ -107,15 +107,39 @@ def test_fp16_storage_recovers_candidates_above_7():
     # relative to each row's RMS, stays well under 1e-2 (measured ~5e-3).
     assert worst < 1e-2, worst
     print(f"fp16 plane max error / row RMS: {worst:.3e}")
-    strong = lambda cs: {(c["subband_level"], c["subband_idx"], c["dm_idx"], c["filter_idx"],
-                          c["peak_sample"]): float(c["snr"]) for c in cs if c["snr"] >= 7.0}
-    s32, s16 = strong(c32), strong(c16)
-    common = set(s32) & set(s16)
-    # same list above 7 except peaks whose S/N sits within the FP16 error of 7
-    diff = [k for k in set(s32) ^ set(s16) if abs(s32.get(k, s16.get(k)) - 7.0) > 0.05]
-    assert not diff, diff[:5]
-    err = max(abs(s32[k] - s16[k]) / s32[k] for k in common)
-    assert err < 1e-2, err
+    # Same list above S/N 7: every FP32 detection (plane, DM, width) has an
+    # FP16 detection whose peak lies in the FP32 run (a near-tie inside a run
+    # may move the argmax by a sample), and vice versa, except detections
+    # whose S/N is within the FP16 error of 7.
+    def runs(cs):
+        out = {}
+        for c in cs:
+            if c["snr"] >= 7.0:
+                k = (int(c["subband_level"]), int(c["subband_idx"]), int(c["dm_idx"]), int(c["filter_idx"]))
+                out.setdefault(k, []).append((int(c["begin_sample"]), int(c["end_sample"]),
+                                              int(c["peak_sample"]), float(c["snr"])))
+        return out
+    r32, r16 = runs(c32), runs(c16)
+
+    def unmatched(a, b):
+        bad, errs = [], []
+        for k, lst in a.items():
+            for beg, end, pk, snr in lst:
+                hit = [x for x in b.get(k, []) if beg <= x[2] <= end or x[0] <= pk <= x[1]]
+                if not hit:
+                    if abs(snr - 7.0) > 0.05:
+                        bad.append((k, pk, snr))
+                else:
+                    errs.append(abs(hit[0][3] - snr) / snr)
+        return bad, errs
+    bad32, errs = unmatched(r32, r16)
+    bad16, _ = unmatched(r16, r32)
+    assert not bad32 and not bad16, (bad32[:5], bad16[:5])
+    exact = sum(1 for k, l in r32.items() for x in l if any(y[2] == x[2] for y in r16.get(k, [])))
+    total = sum(len(l) for l in r32.values())
+    print(f"fp16 vs fp32 above 7: {total} detections, {exact} identical peaks, "
+          f"max S/N error {max(errs):.2e}")
+    assert max(errs) < 1e-2
 
 
 def test_unit_noise_snr_in_every_plane():

@@ -1,0 +1,86 @@
+"""The multi-beam server on one GPU: beams served together, with gulps queued
+up front and taken by two worker slots, give exactly the candidates each beam
+gives alone through the single-beam pipeline; admission refuses a beam that
+would exceed the memory budget and takes it once another beam is removed;
+latency statistics and searched beam-seconds add up."""
+
+import numpy as np
+import pytest
+
+from frost_b200.config import BlockLayout, BoxcarConfig, DataType, RfiConfig
+from frost_b200.synth import make_filterbank
+
+pytestmark = pytest.mark.gpu
+
+NCHANS, GULP, NGULPS, TSAMP = 256, 8192, 3, 1e-3
+
+
+def _beam_stream(seed):
+    fb = make_filterbank(NCHANS, GULP * NGULPS, 1500.0, -1.0, TSAMP, seed, n_pulses=6,
+                         dm_range=(5.0, 60.0), snr_range=(10.0, 25.0), rfi_channel_fraction=0.03,
+                         n_bursts=2)
+    return fb.data
+
+
+def _setup():
+    from frost_b200.pipeline import plan_for
+    layout = BlockLayout(NCHANS, GULP, DataType.UINT8, TSAMP, 1500.0, -1.0)
+    plan = plan_for(layout, 0.0, 80.0, subband_depth=1)
+    bc = BoxcarConfig(max_boxcar=32, detect_thresh=7.0)
+    return RfiConfig(), layout, plan, bc
+
+
+def _nread(g):
+    return GULP if g < NGULPS - 1 else GULP - 1000  # a short last gulp
+
+
+def test_served_beams_match_each_beam_alone():
+    from frost_b200.pipeline import GulpPipeline
+    from frost_b200.serve import BeamServer
+    rfi, layout, plan, bc = _setup()
+    streams = [_beam_stream(s) for s in (21, 22, 23)]
+    alone = []
+    for st in streams:
+        p = GulpPipeline(rfi, layout, 1.0, plan, bc)
+        per = [p.execute(st[g * GULP:(g + 1) * GULP], _nread(g)).candidates for g in range(NGULPS)]
+        per.append(p.flush().candidates)
+        alone.append(per)
+    srv = BeamServer(slots=2)
+    beams = [srv.add_beam(rfi, layout, 1.0, plan, bc) for _ in streams]
+    tickets = [[srv.submit(b, st[g * GULP:(g + 1) * GULP], _nread(g)) for g in range(NGULPS)]
+               for b, st in zip(beams, streams)]
+    for i, b in enumerate(beams):
+        for g, t in enumerate(tickets[i]):
+            cands, latency = srv.wait(t)
+            assert latency > 0
+            assert np.array_equal(cands, alone[i][g]), (i, g)
+        assert np.array_equal(srv.drain(b), alone[i][NGULPS]), i
+    assert sum(len(c) for per in alone for c in per) > 0
+    s = srv.stats()
+    assert s.completed == 3 * NGULPS and s.beams == 3
+    expect = 3 * sum(_nread(g) for g in range(NGULPS)) * TSAMP
+    assert abs(s.beam_seconds - expect) < 1e-6 * expect
+    assert 0 < s.p50_latency_s <= s.p99_latency_s <= s.max_latency_s
+    assert s.wall_seconds > 0
+    srv.close()
+
+
+def test_admission_by_device_memory():
+    from frost_b200._abi import ERR_OUT_OF_MEMORY
+    from frost_b200._lib import FrostError
+    from frost_b200.serve import BeamServer
+    rfi, layout, plan, bc = _setup()
+    probe = BeamServer(slots=1)
+    probe.add_beam(rfi, layout, 1.0, plan, bc)
+    need = probe.stats().device_bytes
+    probe.close()
+    assert need > 0
+    srv = BeamServer(memory_budget=int(1.5 * need), slots=1)
+    first = srv.add_beam(rfi, layout, 1.0, plan, bc)
+    with pytest.raises(FrostError) as e:
+        srv.add_beam(rfi, layout, 1.0, plan, bc)
+    assert e.value.code == ERR_OUT_OF_MEMORY
+    srv.remove_beam(first)
+    second = srv.add_beam(rfi, layout, 1.0, plan, bc)
+    assert srv.stats().beams == 1 and second != first
+    srv.close()
