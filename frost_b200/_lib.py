@@ -41,6 +41,8 @@ SIGNATURES = {
     "frost_rfi_time_flags": (C.c_int, [_vp, _u8p, _sz]),
     "frost_rfi_memory_usage": (C.c_int, [_vp, C.POINTER(_sz)]),
     "frost_rfi_launch_count": (C.c_int, [_vp, C.POINTER(_u64)]),
+    "frost_rfi_normalize_static": (C.c_int, [C.POINTER(_abi.BlockLayoutC), C.c_float, _vp, _sz, _sz,
+                                             _vp, _sz, _vp]),
     "frost_iqrm_mask": (C.c_int, [_f32p, _sz, _u64, C.c_float, _u8p, _u8p]),
     "frost_apply_manual_killmask": (C.c_int, [_u8p, _sz, C.POINTER(_abi.ChannelRange), _sz]),
     "frost_read_kill_file": (C.c_int, [C.c_char_p, _sz, C.POINTER(_abi.ChannelRange), _sz,

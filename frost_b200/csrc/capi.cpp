@@ -190,6 +190,17 @@ int frost_rfi_memory_usage(const frost_rfi* rfi, size_t* bytes) {
     });
 }
 
+int frost_rfi_normalize_static(const frost_block_layout* layout, float baseline_length,
+                               const uint8_t* block, size_t block_bytes, size_t nsamps, float* out,
+                               size_t out_count, void* stream) {
+    return guarded([&] {
+        if (layout == nullptr)
+            invalid("frost_rfi_normalize_static: null layout");
+        fb::rfi::normalize_static(*layout, baseline_length, block, block_bytes, nsamps, out,
+                                  out_count, static_cast<cudaStream_t>(stream));
+    });
+}
+
 int frost_rfi_launch_count(const frost_rfi* rfi, uint64_t* launches) {
     return guarded([&] {
         if (rfi == nullptr || launches == nullptr)

@@ -30,6 +30,12 @@ void validate_layout(const frost_block_layout& l, float baseline_length);
 void apply_manual_killmask(std::span<uint8_t> mask, std::span<const frost_channel_range> zaps);
 std::vector<frost_channel_range> read_kill_file(const std::string& path, SizeType nchans);
 
+/** Quiet-configuration clean + normalise of one device block into `out`
+ * using only the static scratch array of rfi_static.cu (no allocation). */
+void normalize_static(const frost_block_layout& layout, float baseline_length, const uint8_t* block,
+                      size_t block_bytes, size_t nsamps, float* out, size_t out_count,
+                      cudaStream_t stream);
+
 class Cleaner {
 public:
     Cleaner(const frost_rfi_config& cfg, const frost_block_layout& layout, float baseline_length,

@@ -211,6 +211,33 @@ int frost_rfi_memory_usage(const frost_rfi* rfi, size_t* bytes);
 /* Kernels this cleaner has launched since it was created. */
 int frost_rfi_launch_count(const frost_rfi* rfi, uint64_t* launches);
 
+/* No counterpart in the reference. An allocation-free form of
+ * frost_rfi_execute_normalized for callers that cannot call cudaMalloc once
+ * they are processing (a real-time consumer that sizes all device memory at
+ * start-up and must never block in or fail inside the device allocator, or a
+ * host program whose device memory belongs to another framework's pool).
+ * It cleans and normalises one block with the quiet configuration (no
+ * automatic excision or zaps: per-window bandpass, dead channels zeroed,
+ * (x - loc) / scale in [channel][time] order, low frequency first, padding
+ * zero) — the same result as frost_rfi_execute_normalized with every
+ * strategy off. `block` and `out` are device pointers; out holds
+ * nchans * (block_bytes / row_bytes) floats; nsamps = 0 uses every row and
+ * must otherwise be >= 64. Scratch is a fixed 32 MiB + 256 KiB static device
+ * array in the library (held by every GPU that loads it until exit), limiting
+ * windows x channels to 2684; larger blocks are rejected with
+ * FROST_ERR_INVALID_ARGUMENT. The first call on a device looks up the
+ * array's address and should come before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race. Synchronises
+ * `stream` (NULL = the default stream) before returning. */
+int frost_rfi_normalize_static(const frost_block_layout* layout,
+                               float baseline_length,
+                               const uint8_t* block,
+                               size_t block_bytes,
+                               size_t nsamps,
+                               float* out,
+                               size_t out_count,
+                               void* stream);
+
 /* IQRM channel mask (include/frost/prepare/rfi.hpp:56-59,
  * lib/cpu/rfi_masks_cpu.cpp:29-122) on an n-channel host statistic.
  * `ignore` may be NULL. Writes n flags (1 = flagged) to host `out`. */
