@@ -1,19 +1,24 @@
 #!/usr/bin/env python3
 """Benchmark of the per-gulp search path at the 4096-channel, DM 0-2000
-workload: beam-seconds searched per second (whole job), p50/p99 gulp
-latency, FP16-storage vs plain FP32, end-to-end through the public API,
-the FDMT level kernels' HBM roofline, and the CPU baseline.
+workload: beam-seconds searched per second (whole job) of several beams
+served together on one GPU with FP16 plane storage, their p50/p99 gulp
+latency, the plain single-beam FP32 and FP16 paths beside them, the same
+served run fed from pinned host memory (e2e), the FDMT level kernel's HBM
+roofline, and the CPU baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl frost|reference]
+                    [--beams B] [--served-tile T] [--workload config2|config1]
 
-A step is one 262144-sample gulp of one beam through RFI excision (moments,
-IQRM, Kadane along time and frequency, zero-DM subtract, narrow/broad-band
-neighbour fills) -> normalisation -> streaming FDMT -> boxcar search of 11
-sub-band planes (widths 1-256). Each rank streams its own beam (replicas,
-weak scaling; no collective is needed: beams are independent). Inputs are
-seeded synthetic filterbanks with the workload's noise, RFI and pulse
-recipe; every step reads a 1 GiB raw gulp and writes/reads multi-GiB
-planes, so inputs exceed the 126 MB L2 without a flush.
+A beam-gulp is one 262144-sample gulp of one beam through RFI excision
+(moments, IQRM, Kadane along time and frequency, zero-DM subtract,
+narrow/broad-band neighbour fills) -> normalisation -> streaming FDMT ->
+boxcar search of 11 sub-band planes (widths 1-256). A step is one gulp of
+each served beam (B beams, admitted by device memory; each has one gulp in
+flight). Each rank serves its own beams (replicas, weak scaling; beams are
+independent, so no collective is needed). Inputs are seeded synthetic
+filterbanks with the workload's noise, RFI and pulse recipe; every
+beam-gulp reads a 1 GiB raw gulp and writes/reads multi-GiB planes, so
+inputs exceed the 126 MB L2 without a flush.
 """
 
 from __future__ import annotations
@@ -250,19 +255,87 @@ def run_gpu(args):
         torch.cuda.empty_cache()
         return out
 
-    fp16 = measure(Storage.FP16, sample_clocks=True)
-    fp32 = measure(Storage.FP32)
-    e2e = measure(Storage.FP16, e2e=True)
+    def measure_served(nbeams, on_device, sample_clocks=False):
+        """Beams of the workload on one GPU through the server: each beam has
+        one gulp in flight (the next is submitted when the previous one's
+        candidates are ready), so every beam is busy and its latency is
+        service time under contention. Beams are admitted by device memory;
+        the admitted count is reported."""
+        from frost_b200._lib import FrostError
+        from frost_b200.serve import BeamServer
+        srv = BeamServer(device=local, slots=nbeams)
+        bc = search_config(Storage.FP16)
+        bc.tile_nsamps = args.served_tile
+        beams = []
+        for _ in range(nbeams):
+            try:
+                beams.append(srv.add_beam(rfi_config(), lay, 2.0, plan, bc))
+            except FrostError as e:
+                if e.code != -2:  # ERR_OUT_OF_MEMORY: admission refused
+                    raise
+                break
+        src = raw_dev.data_ptr() if on_device else pinned.data_ptr()
+        counts = {b: [0, 0] for b in beams}  # candidates, bytes
 
-    beam_s = args.steps * GULP * TSAMP * world
-    value = beam_s / (fp16["total_ms"] / 1e3)
-    t = fp16["timing"]
+        def run_beam(b, n, keep):
+            for _ in range(n):
+                t = srv.submit_ptr(b, src, nbytes, GULP, on_device)
+                cands, _ = srv.wait(t)
+                if keep:
+                    counts[b][0] += cands.size
+                    counts[b][1] += cands.nbytes
+
+        def run_all(n, keep):
+            ths = [threading.Thread(target=run_beam, args=(b, n, keep)) for b in beams]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+
+        run_all(args.warmup, False)
+        torch.cuda.synchronize()
+        barrier()
+        srv.reset_stats()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.__enter__()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        run_all(args.steps, True)
+        torch.cuda.synchronize()
+        ev[1].record()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.__exit__(None, None, None)
+        barrier()
+        st = srv.stats()
+        out = {"total_ms": max_over_ranks(ev[0].elapsed_time(ev[1])), "beams": len(beams),
+               "stats": st, "ncands": sum(c[0] for c in counts.values()),
+               "d2h": sum(c[1] for c in counts.values()),
+               "clocks": sampler.summary() if sampler else None}
+        srv.close()
+        torch.cuda.empty_cache()
+        return out
+
+    single16 = measure(Storage.FP16)
+    single32 = measure(Storage.FP32)
+    served = measure_served(args.beams, on_device=True, sample_clocks=True)
+    e2e = measure_served(args.beams, on_device=False)
+
+    gulp_s = GULP * TSAMP
+    per_beam_steps = args.steps * world
+    value = served["beams"] * per_beam_steps * gulp_s / (served["total_ms"] / 1e3)
+    plain32 = per_beam_steps * gulp_s / (single32["total_ms"] / 1e3)
+    plain16 = per_beam_steps * gulp_s / (single16["total_ms"] / 1e3)
+    e2e_value = e2e["beams"] * per_beam_steps * gulp_s / (e2e["total_ms"] / 1e3)
+    t = single16["timing"]
     peak, peak_kind = measured_peaks()
     level_gbs = t["algorithmic_level_bytes"] / (t["level_ms"] / 1e3) / 1e9 if t["level_ms"] else 0.0
     traffic = ncu_traffic_per_launch()
     roofline = {
         "bound": "hbm",
-        "kernel": "k_level<__half> (FDMT levels 2-12)",
+        "kernel": "k_level_pipe<__half> (FDMT levels 2-12, plain FP16 single-beam run)",
         "achieved": round(level_gbs, 1),
         "peak": peak,
         "unit": "GB/s",
@@ -274,8 +347,10 @@ def run_gpu(args):
         "phase_ms_per_step": {k: round(t[k] / args.steps, 3) for k in
                               ("level1_ms", "level_ms", "search_ms", "history_ms", "variance_ms")},
     }
-    lat = sorted(fp16["lat"])
-    p = lambda q: lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
+    st = served["stats"]
+    lat1 = sorted(single16["lat"])
+    p = lambda q: lat1[min(len(lat1) - 1, int(round(q * (len(lat1) - 1))))]
+    n_gulps = served["beams"] * args.steps
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -283,29 +358,38 @@ def run_gpu(args):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(fp16["total_ms"] / args.steps, 3),
+        "ms_per_step": round(served["total_ms"] / args.steps, 3),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 (fp16 plane storage)",
-        "data": "synthetic (seeded filterbank, config-2 noise/RFI/pulse recipe)",
-        "config": {"workload": WORKLOAD, "storage": "fp16", "beams_per_gpu": 1,
-                   "l2": "inputs larger than L2 (1 GiB raw gulp per step)",
+        "data": "synthetic (seeded filterbank, config-2 noise/RFI/pulse recipe); every beam replays its gulp",
+        "config": {"workload": WORKLOAD, "storage": "fp16", "served_beams_per_gpu": served["beams"],
+                   "step": f"one gulp of each of the {served['beams']} served beams",
+                   "served_tile_nsamps": args.served_tile or GULP,
+                   "l2": "inputs larger than L2 (1 GiB raw gulp per beam-gulp)",
+                   "timing": "CUDA events bracketing device-wide synchronisations (beams run on their own streams)",
                    "parallelism": f"replicas x{world}"},
-        "latency_ms": {"p50": round(p(0.5), 2), "p99": round(p(0.99), 2),
-                       "realtime_gulp_ms": GULP * TSAMP * 1e3},
-        "plain_fp32": {"value": round(beam_s / (fp32["total_ms"] / 1e3), 3),
-                       "ms_per_step": round(fp32["total_ms"] / args.steps, 3)},
-        "e2e": {"value": round(beam_s / (e2e["total_ms"] / 1e3), 3), "unit": UNIT,
-                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": int(e2e["d2h"] / args.steps)},
-        "gpu_launches": int(fp16["launches"]),
+        "latency_ms": {"p50": round(st.p50_latency_s * 1e3, 2), "p99": round(st.p99_latency_s * 1e3, 2),
+                       "max": round(st.max_latency_s * 1e3, 2), "realtime_gulp_ms": gulp_s * 1e3,
+                       "what": "served gulp, submit to candidates ready, one gulp in flight per beam"},
+        "plain_fp32": {"value": round(plain32, 3), "ms_per_step": round(single32["total_ms"] / args.steps, 3),
+                       "what": "single beam, FP32 planes, no server"},
+        "plain_fp16": {"value": round(plain16, 3), "ms_per_step": round(single16["total_ms"] / args.steps, 3),
+                       "p50_ms": round(p(0.5), 2), "p99_ms": round(p(0.99), 2)},
+        "served_vs_plain_fp32": round(value / plain32, 3),
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
+                "h2d_bytes_per_step": nbytes * e2e["beams"],
+                "d2h_bytes_per_step": int(e2e["d2h"] / args.steps),
+                "what": "served beams fed from pinned host gulps through frost_server_submit"},
+        "gpu_launches": int(st.launches),
         "roofline": roofline,
-        "clocks": fp16["clocks"],
-        "candidates_per_step": round(fp16["ncands"] / args.steps, 1),
-        "dropped_last_step": fp16["dropped"],
-        "rfi_stage_ms_last_step": fp16["rfi_ms"],
-        "rfi_counts_last_step": fp16["rfi_counts"],
-        "device_bytes": fp16["device_bytes"],
+        "clocks": served["clocks"],
+        "candidates_per_beam_gulp": round(served["ncands"] / max(n_gulps, 1), 1),
+        "dropped_last_step": single16["dropped"],
+        "rfi_stage_ms_last_step": single16["rfi_ms"],
+        "rfi_counts_last_step": single16["rfi_counts"],
+        "device_bytes_served": int(st.device_bytes),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
@@ -387,6 +471,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
                     help="config2 (headline) or config1 (1024-channel profiling case)")
+    ap.add_argument("--beams", type=int, default=3, help="served beams per GPU (admitted by memory)")
+    ap.add_argument("--served-tile", type=int, default=0,
+                    help="FDMT tile of the served beams in samples (0 = the whole gulp)")
     args = ap.parse_args()
     select_workload(args.workload)
     if args.warmup < 3 and args.impl == "frost":

@@ -230,4 +230,5 @@ class ServerStatsC(C.Structure):
         ("p50_latency_s", C.c_double),
         ("p99_latency_s", C.c_double),
         ("max_latency_s", C.c_double),
+        ("launches", C.c_uint64),
     ]

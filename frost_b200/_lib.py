@@ -72,12 +72,13 @@ SIGNATURES = {
                                         C.c_float, C.POINTER(_abi.DedispPlanConfigC),
                                         C.POINTER(_abi.BoxcarConfigC), C.POINTER(C.c_uint32)]),
     "frost_server_remove_beam": (C.c_int, [_vp, C.c_uint32]),
-    "frost_server_submit": (C.c_int, [_vp, C.c_uint32, _u8p, _sz, _sz, C.POINTER(_u64)]),
+    "frost_server_submit": (C.c_int, [_vp, C.c_uint32, _vp, _sz, _sz, C.c_int, C.POINTER(_u64)]),
     "frost_server_wait": (C.c_int, [_vp, _u64, C.POINTER(_abi.CandidateC), _sz, C.POINTER(_sz),
                                     C.POINTER(C.c_double)]),
     "frost_server_drain": (C.c_int, [_vp, C.c_uint32, C.POINTER(_abi.CandidateC), _sz,
                                      C.POINTER(_sz)]),
     "frost_server_get_stats": (C.c_int, [_vp, C.POINTER(_abi.ServerStatsC)]),
+    "frost_server_reset_stats": (C.c_int, [_vp]),
 }
 
 

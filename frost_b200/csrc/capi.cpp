@@ -459,11 +459,11 @@ int frost_server_remove_beam(frost_server* s, uint32_t beam) {
 }
 
 int frost_server_submit(frost_server* s, uint32_t beam, const uint8_t* block, size_t block_bytes,
-                        size_t nread, uint64_t* ticket) {
+                        size_t nread, int on_device, uint64_t* ticket) {
     return guarded([&] {
         if (s == nullptr || ticket == nullptr)
             invalid("frost_server_submit: null argument");
-        *ticket = s->impl.submit(beam, block, block_bytes, nread);
+        *ticket = s->impl.submit(beam, block, block_bytes, nread, on_device != 0);
     });
 }
 
@@ -488,6 +488,14 @@ int frost_server_drain(frost_server* s, uint32_t beam, frost_candidate* out, siz
         rc = copy_candidates(s->impl.drain(beam), out, capacity, count);
     });
     return g != FROST_OK ? g : rc;
+}
+
+int frost_server_reset_stats(frost_server* s) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_reset_stats: null handle");
+        s->impl.reset_stats();
+    });
 }
 
 int frost_server_get_stats(frost_server* s, frost_server_stats* out) {

@@ -15,6 +15,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "bulk_copy.cuh"
 #include "common.hpp"
 #include "fdmt_kernels.hpp"
 
@@ -198,29 +199,7 @@ __device__ __forceinline__ void merge8(const S* lo, const S* stage, int e, int o
 
 constexpr int kStages      = 4;
 constexpr int kTilesPerCta = 16;
-constexpr long kSpinLimit  = 1L << 22;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t phase) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(phase)
-        : "memory");
-    return done != 0;
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    for (long it = 0; it < kSpinLimit; ++it)
-        if (mbar_try(bar, phase))
-            return true;
-    return false;
-}
+using bulk::mbar_wait;
 
 template <class S>
 __global__ void __launch_bounds__(kThreads)
@@ -253,31 +232,19 @@ __global__ void __launch_bounds__(kThreads)
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < kStages; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bar[s])), "r"(1));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            bulk::mbar_init(&bar[s]);
     }
     __syncthreads();
 
     auto issue = [&](int i) {
-        const int s        = i % kStages;
-        const int64_t k0   = static_cast<int64_t>(tile0 + i) * kTimePerCta;
-        unsigned char* st  = pipe_smem + s * kStageBytes;
-        const uint32_t b   = smem_addr(&bar[s]);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b),
-                     "r"(static_cast<uint32_t>(kLoBytes) + hi_bytes)
-                     : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                smem_addr(st)),
-            "l"(lo_row + k0), "r"(static_cast<uint32_t>(kLoBytes)), "r"(b)
-            : "memory");
+        const int s       = i % kStages;
+        const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
+        unsigned char* st = pipe_smem + s * kStageBytes;
+        bulk::mbar_expect(&bar[s], static_cast<uint32_t>(kLoBytes) + hi_bytes);
+        bulk::load(st, lo_row + k0, static_cast<uint32_t>(kLoBytes), &bar[s]);
         if (has_hi) {
             const int64_t v0 = (e_first + k0 - off) / VEC; // aligned start, in vectors
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    smem_addr(st + kLoBytes)),
-                "l"(hi_base + v0 * VEC), "r"(hi_bytes), "r"(b)
-                : "memory");
+            bulk::load(st + kLoBytes, hi_base + v0 * VEC, hi_bytes, &bar[s]);
         }
     };
 
@@ -289,7 +256,7 @@ __global__ void __launch_bounds__(kThreads)
     for (; i < nt; ++i) {
         const int s           = i % kStages;
         const uint32_t phase  = static_cast<uint32_t>((i / kStages) & 1);
-        if (!mbar_wait(smem_addr(&bar[s]), phase))
+        if (!mbar_wait(&bar[s], phase))
             atomicExch(&abort_flag, 1);
         __syncthreads();
         if (abort_flag)
@@ -313,7 +280,7 @@ __global__ void __launch_bounds__(kThreads)
         // a wait ran out: report it, then let the copies still in flight land
         atomicOr(err, 1U);
         for (int j = i; j < min(nt, i + kStages); ++j)
-            (void)mbar_wait(smem_addr(&bar[j % kStages]), static_cast<uint32_t>((j / kStages) & 1));
+            (void)mbar_wait(&bar[j % kStages], static_cast<uint32_t>((j / kStages) & 1));
     }
 }
 

@@ -573,7 +573,51 @@ void Cleaner::build_channel_mask(const Dims& d, const std::vector<uint32_t>& unm
     m_report.chans_masked = count_zeros(m_mask);
 }
 
+// Device buffers of the full cleaning path for a block of d.nsamps rows.
+void Cleaner::reserve_phase_buffers(const Dims& d) {
+    const SizeType n    = m_n;
+    const SizeType nwin = d.nwin;
+    const SizeType T    = d.nsamps;
+    const auto& c       = m_cfg.c;
+    const bool zdot     = c.zero_dm == FROST_ZERO_DM_ZDOT;
+    const bool kchan    = c.kadane_channel_enabled != 0;
+    m_samples.reserve(nwin * kMaxBandpassRows * n * sizeof(float));
+    m_unmeasured.reserve(n * sizeof(uint32_t));
+    if (m_need_moments) {
+        m_moments.reserve(nwin * n * sizeof(MomentSums));
+        m_clip_mean.reserve(nwin * n * sizeof(float));
+        m_clip_inv.reserve(nwin * n * sizeof(float));
+    }
+    m_s_det.reserve(T * sizeof(float));
+    m_s_keep_d.reserve(T * sizeof(double));
+    m_s_keep_f.reserve(T * sizeof(float));
+    m_row_std.reserve(T * sizeof(float));
+    m_kspec_pos.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
+    m_kspec_neg.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
+    m_kspec_whole.reserve(std::max<SizeType>(T, 1));
+    m_time_flags_d.reserve(std::max<SizeType>(T, 1));
+    const SizeType nck = d.nchunks * n;
+    m_chunk_min.reserve(nck * sizeof(float));
+    m_chunk_max.reserve(nck * sizeof(float));
+    m_chunk_zdot.reserve(std::max<SizeType>(zdot ? nck : 1, 1) * sizeof(ZdotSums));
+    m_chunk_kpos.reserve(std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState));
+    m_chunk_kneg.reserve(std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState));
+    m_lo.reserve(n * sizeof(float));
+    m_hi.reserve(n * sizeof(float));
+    m_zdot_sum.reserve(n * sizeof(ZdotSums));
+    m_kpos_best.reserve(n * sizeof(Run));
+    m_kneg_best.reserve(n * sizeof(Run));
+}
+
+void Cleaner::preallocate() {
+    DeviceGuard g(m_device);
+    const SizeType T = m_layout.max_nsamps;
+    ensure_capacity(T, T);
+    reserve_phase_buffers(dims(T, m_layout.dtype));
+}
+
 void Cleaner::run_full(const Dims& d, cudaStream_t s) {
+    reserve_phase_buffers(d);
     const SizeType n     = m_n;
     const SizeType nwin  = d.nwin;
     const SizeType T     = d.nsamps;
@@ -585,8 +629,6 @@ void Cleaner::run_full(const Dims& d, cudaStream_t s) {
 
     // ---- bandpass ----
     auto t = Clock::now();
-    m_samples.reserve(nwin * kMaxBandpassRows * n * sizeof(float));
-    m_unmeasured.reserve(n * sizeof(uint32_t));
     FB_CUDA(cudaMemsetAsync(m_unmeasured.get(), 0, n * sizeof(uint32_t), s));
     launch_sample_rows(d, raw, m_samples.as<float>(), s);
     launch_bandpass(d, m_samples.as<float>(), m_loc.as<float>(), m_scale.as<float>(),
@@ -603,7 +645,6 @@ void Cleaner::run_full(const Dims& d, cudaStream_t s) {
     t = Clock::now();
     std::vector<MomentSums> mom;
     if (m_need_moments) {
-        m_moments.reserve(nwin * n * sizeof(MomentSums));
         launch_moments(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_static_mask_d.as<uint8_t>(),
                        m_clip, m_moments.as<MomentSums>(), s);
         d2h(mom, m_moments, nwin * n, s);
@@ -631,24 +672,6 @@ void Cleaner::run_full(const Dims& d, cudaStream_t s) {
 
     // ---- scan ----
     t = Clock::now();
-    m_s_det.reserve(T * sizeof(float));
-    m_s_keep_d.reserve(T * sizeof(double));
-    m_s_keep_f.reserve(T * sizeof(float));
-    m_row_std.reserve(T * sizeof(float));
-    m_kspec_pos.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
-    m_kspec_neg.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
-    m_kspec_whole.reserve(std::max<SizeType>(T, 1));
-    const SizeType nck = d.nchunks * n;
-    m_chunk_min.reserve(nck * sizeof(float));
-    m_chunk_max.reserve(nck * sizeof(float));
-    m_chunk_zdot.reserve(std::max<SizeType>(zdot ? nck : 1, 1) * sizeof(ZdotSums));
-    m_chunk_kpos.reserve(std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState));
-    m_chunk_kneg.reserve(std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState));
-    m_lo.reserve(n * sizeof(float));
-    m_hi.reserve(n * sizeof(float));
-    m_zdot_sum.reserve(n * sizeof(ZdotSums));
-    m_kpos_best.reserve(n * sizeof(Run));
-    m_kneg_best.reserve(n * sizeof(Run));
     m_clip_mean.reserve(sizeof(float));
     m_clip_inv.reserve(sizeof(float));
 

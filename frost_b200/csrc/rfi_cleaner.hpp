@@ -58,6 +58,9 @@ public:
     int device() const { return m_device; }
     cudaStream_t stream() const { return m_stream; }
     SizeType memory_usage() const;
+    /** Allocates every device buffer a full block of max_nsamps rows needs,
+     * so memory_usage() is the cleaner's steady-state footprint. */
+    void preallocate();
     uint64_t launches() const { return m_launches; }
 
 private:
@@ -95,6 +98,7 @@ private:
 
     void build_static_mask();
     void ensure_capacity(SizeType capacity, SizeType valid);
+    void reserve_phase_buffers(const Dims& d);
     ApplyParams apply_params() const;
     Dims dims(SizeType nsamps, int dtype) const;
 

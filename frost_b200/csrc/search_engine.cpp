@@ -244,7 +244,7 @@ SizeType Engine::plan_bytes(int64_t tile) const {
     int32_t maxh         = 0;
     for (int h = 1; h <= L; ++h)
         maxh = std::max(maxh, m_plan.level_history(h));
-    const int64_t base   = round_up(std::max<int64_t>(maxh, m_plan.widths().back()), 8);
+    const int64_t base   = round_up(std::max<int64_t>(maxh, search_halo(m_plan.widths().back())), 8);
     const int64_t pitch  = base + round_up(tile, kTileQuantum);
     SizeType bytes       = 2 * static_cast<SizeType>(m_plan.max_level_rows()) * pitch * es;
     for (int h = 1; h <= L; ++h)
@@ -263,7 +263,7 @@ void Engine::allocate(int64_t tile) {
         maxh = std::max(maxh, m_plan.level_history(h));
     m_tile  = tile;
     m_ncols = round_up(tile, kTileQuantum);
-    m_base  = static_cast<int32_t>(round_up(std::max<int64_t>(maxh, m_plan.widths().back()), 8));
+    m_base  = static_cast<int32_t>(round_up(std::max<int64_t>(maxh, search_halo(m_plan.widths().back())), 8));
     m_pitch = m_base + m_ncols;
     const SizeType buf = static_cast<SizeType>(m_plan.max_level_rows()) * m_pitch * es;
     for (auto& b : m_buf) {
@@ -310,6 +310,8 @@ SearchParams Engine::params(int64_t tile_t0, int64_t gulp_t0, int32_t n_valid, b
     p.widths       = m_widths.as<int32_t>();
     p.nwidths      = static_cast<int32_t>(m_plan.widths().size());
     p.wmax         = m_plan.widths().back();
+    p.halo         = search_halo(p.wmax);
+    p.err          = reinterpret_cast<unsigned*>(m_counters.as<unsigned long long>() + 3);
     p.thresh       = m_cfg.detect_thresh;
     p.peak_mode    = m_cfg.peak_mode;
     p.trapezoid    = m_cfg.use_trapezoid ? 1 : 0;
@@ -478,7 +480,7 @@ void Engine::collect(cudaStream_t s) {
     FB_CUDA(cudaMemcpyAsync(counters, m_counters.get(), sizeof(counters), cudaMemcpyDeviceToHost, s));
     FB_CUDA(cudaStreamSynchronize(s));
     if (counters[3] != 0)
-        throw Error(FROST_ERR_TIMEOUT, "search: a level kernel's bounded wait for its bulk copies ran "
+        throw Error(FROST_ERR_TIMEOUT, "search: a level or search kernel's bounded wait for its bulk copies ran "
                                        "out; this call's results are incomplete");
     const uint64_t n = std::min<uint64_t>(counters[0], m_cfg.max_candidates);
     m_results.resize(n);

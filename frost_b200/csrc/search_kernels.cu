@@ -1,22 +1,26 @@
 // Boxcar/trapezoid matched filter, exact noise and peak finding on sm_100a.
 //
 // One CTA per searched (plane, DM) row walks the tile in 4096-sample chunks:
-// the chunk plus a (wmax - 1)-sample halo is staged in shared memory and
-// prefix-summed; every width's window sum is a difference of two (four for
-// the trapezoid) prefix values. In the steady state (no cold prefix, no mask
-// change in the chunk) a sample is above threshold when its window sum
-// exceeds thresh * sigma, precomputed per width, so the test is two shared
-// loads, a subtract and a compare; the first chunks of a stream or after a
-// mask change take the general path (cold prefix, OR-mask variance).
-// Above-threshold samples become ballot bitmasks. Runs (contiguous set bits)
-// are rare, so one lane walks only the set bits in time order, extending or
-// closing the run carried from the previous chunk (and tile, and gulp) and
-// emitting each closed run's peak. The DM-time rows are never re-read and
-// the run state is the only thing carried between calls.
+// the chunk plus a halo of the widest boxcar (rounded to 128 columns) is
+// loaded with vector loads, prefix-summed (warp shuffles, then one offset
+// per warp) into shared memory, and every width's window sum is a
+// difference of two (four for the trapezoid) prefix values. In the steady
+// state (no cold prefix, no mask change in the chunk) a sample is above
+// threshold when its window sum exceeds thresh * sigma, precomputed per
+// width; each thread tests 4 consecutive samples per 16-byte shared load
+// and ORs the outcomes into one predicate, so a chunk in which nothing
+// fires (almost all of them) costs one block vote. A chunk that fires, and
+// the first chunks of a stream or after a mask change (cold prefix,
+// OR-mask variance), build per-width ballot bitmasks; one lane walks only
+// the set bits in time order, extending or closing the run carried from
+// the previous chunk (and tile, and gulp) and emitting each closed run's
+// peak. The DM-time rows are never re-read and the run state is the only
+// thing carried between calls.
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "bulk_copy.cuh"
 #include "common.hpp"
 #include "search_kernels.hpp"
 
@@ -82,18 +86,24 @@ struct RowConst {
     float thr[kMaxWidths];  // window-sum threshold thresh * sigma
 };
 
-// Window sum of width W (edge E) ending at prefix index i.
-__device__ __forceinline__ float wsum(const float* P, int i, int W, int E) {
-    float s = P[i] - P[i - W];
-    if (E > 0)
-        s -= 0.5F * ((P[i] - P[i - E]) + (P[i - W + E] - P[i - W]));
-    return s;
+// Window sum of width W (trapezoid edge E, 0 for a boxcar) ending at chunk
+// sample k; Q[k] is the prefix sum through sample k.
+// The steady-state pre-test evaluates the same expression, so the trapezoid
+// correction is written with non-contractible intrinsics (no FMA) to give
+// bit-identical sums in both places.
+__device__ __forceinline__ float trap_sum(float qk, float qw, float qe, float qwe) {
+    return __fsub_rn(qk - qw, __fmul_rn(0.5F, (qk - qe) + (qwe - qw)));
+}
+
+__device__ __forceinline__ float wsum(const float* Q, int k, int W, int E) {
+    const float qk = Q[k], qw = Q[k - W];
+    return E > 0 ? trap_sum(qk, qw, Q[k - E], Q[k - W + E]) : qk - qw;
 }
 
 // General S/N of chunk sample k at width wi: -inf past the valid columns or
 // in the cold prefix; the OR-mask variance right after a mask change.
 __device__ __forceinline__ float snr_general(const SearchParams& p, const RowConst& rc,
-                                             const float* P, int wmax, int64_t c0, int k, int wi,
+                                             const float* Q, int64_t c0, int k, int wi,
                                              int32_t delay) {
     const int64_t col = c0 + k;
     if (col >= p.n_valid)
@@ -106,7 +116,36 @@ __device__ __forceinline__ float snr_general(const SearchParams& p, const RowCon
     const float inv   = use_or ? rc.inv_or[wi] : rc.inv[wi];
     if (inv == 0.0F)
         return FB_NEG_INF;
-    return wsum(P, k + wmax, W, rc.E[wi]) * inv;
+    return wsum(Q, k, W, rc.E[wi]) * inv;
+}
+
+// Q[idx .. idx + 4) with idx mod 4 the same across the warp: one or two
+// aligned 16-byte shared-memory loads (Q itself is 16-byte aligned).
+__device__ __forceinline__ float4 ld4(const float* Q, int idx) {
+    const int r     = idx & 3;
+    const float4* v = reinterpret_cast<const float4*>(Q + (idx - r));
+    const float4 a  = v[0];
+    if (r == 0)
+        return a;
+    const float4 b = v[1];
+    if (r == 1)
+        return make_float4(a.y, a.z, a.w, b.x);
+    if (r == 2)
+        return make_float4(a.z, a.w, b.x, b.y);
+    return make_float4(a.w, b.x, b.y, b.z);
+}
+
+// Four consecutive staged level samples as float (8-byte fp16 / 16-byte
+// fp32 shared-memory load).
+template <class S> __device__ __forceinline__ float4 ld4s(const S* p);
+template <> __device__ __forceinline__ float4 ld4s<float>(const float* p) {
+    return *reinterpret_cast<const float4*>(p);
+}
+template <> __device__ __forceinline__ float4 ld4s<__half>(const __half* p) {
+    const uint2 u  = *reinterpret_cast<const uint2*>(p);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
 }
 
 // `count` (shared or global) is the row's emitted total this call.
@@ -144,8 +183,8 @@ __device__ void emit(const SearchParams& p, const SearchRow& row, const RunState
 
 // Walks the set bits of one chunk's mask in time order (one lane). For the
 // across-widths mode `wi` < 0: the peak is the best S/N over widths.
-__device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float* P, int wmax,
-                          int64_t c0, int32_t delay, const uint32_t* bits, int wi, RunState& run,
+__device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float* Q, int64_t c0,
+                          int32_t delay, const uint32_t* bits, int wi, RunState& run,
                           const SearchRow& row, uint32_t* count) {
     int64_t last = run.open ? c0 - 1 : -2; // tile column of the last set bit
     for (int wd = 0; wd < kWords; ++wd) {
@@ -158,11 +197,11 @@ __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float
             float best        = FB_NEG_INF;
             int bw            = 0;
             if (wi >= 0) {
-                best = snr_general(p, rc, P, wmax, c0, k, wi, delay);
+                best = snr_general(p, rc, Q, c0, k, wi, delay);
                 bw   = wi;
             } else {
                 for (int w = 0; w < p.nwidths; ++w) {
-                    const float s = snr_general(p, rc, P, wmax, c0, k, w, delay);
+                    const float s = snr_general(p, rc, Q, c0, k, w, delay);
                     if (s > best) {
                         best = s;
                         bw   = w;
@@ -198,112 +237,209 @@ __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float
     }
 }
 
-// NW > 0: the width count as a compile-time constant (steady-state fast
-// path in registers); NW == 0: any width count.
-template <class S, int NW>
+// Closes the runs still open at the end of a chunk in which nothing fired
+// (what walk_runs does for an all-zero mask).
+__device__ void close_open_runs(const SearchParams& p, RunState* runs, int nruns,
+                                const SearchRow& row, uint32_t* count) {
+    for (int i = 0; i < nruns; ++i)
+        if (runs[i].open) {
+            emit(p, row, runs[i], count);
+            runs[i].open = 0;
+        }
+}
+
+template <class S>
 __global__ void __launch_bounds__(kThreads, 4)
     k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0) {
-    extern __shared__ float P[];
+    // Dynamic shared memory: Ps, the chunk's prefix sums over columns
+    // [c0 - halo, c0 + kChunk) after 4 floats of padding (Q = Ps + 4 + halo
+    // puts sample k of the chunk at Q[k], 16-byte aligned), then two staging
+    // buffers of the raw row segment, filled by bulk copies one chunk ahead.
+    extern __shared__ __align__(16) float Ps[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int abort_flag;
     __shared__ uint32_t bits[kMaxWidths][kWords];
     __shared__ uint32_t any_bits[kWords];
     __shared__ RunState runs[kMaxWidths];
     __shared__ RowConst rc;
     __shared__ uint32_t local_count;
+    __shared__ float warp_tot[kThreads / 32];
 
     const int64_t g     = g0 + blockIdx.x;
     const SearchRow row = p.rows[g];
     const int nw        = p.nwidths;
     const int wmax      = p.wmax;
+    const int halo      = p.halo;
     const bool across   = p.peak_mode == FROST_PEAK_ACROSS_WIDTHS;
     const bool all      = p.peak_mode == FROST_PEAK_ALL;
     if (threadIdx.x == 0)
         local_count = p.row_counts[g];
     if (threadIdx.x < nw) {
-        const int w  = threadIdx.x;
-        const int W  = p.widths[w];
-        rc.W[w]      = W;
-        rc.E[w]      = (p.trapezoid && W >= 3) ? (W + 1) / 4 : 0;
+        const int w    = threadIdx.x;
+        const int W    = p.widths[w];
+        rc.W[w]        = W;
+        rc.E[w]        = (p.trapezoid && W >= 3) ? (W + 1) / 4 : 0;
         const float iv = p.inv_sigma[g * nw + w];
-        rc.inv[w]    = iv;
-        rc.inv_or[w] = p.inv_sigma_or[g * nw + w];
-        rc.thr[w]    = iv > 0.0F ? p.thresh / iv : FB_POS_INF;
+        rc.inv[w]      = iv;
+        rc.inv_or[w]   = p.inv_sigma_or[g * nw + w];
+        rc.thr[w]      = iv > 0.0F ? p.thresh / iv : FB_POS_INF;
     }
     const int nruns = across ? 1 : nw;
     if (threadIdx.x < nruns && !all)
         runs[threadIdx.x] = p.carry[g * nruns + threadIdx.x];
     __syncthreads();
-    int Wr[NW > 0 ? NW : 1], Er[NW > 0 ? NW : 1];
-    float Tr[NW > 0 ? NW : 1];
-    if constexpr (NW > 0) {
-#pragma unroll
-        for (int wi = 0; wi < NW; ++wi) {
-            Wr[wi] = rc.W[wi];
-            Er[wi] = rc.E[wi];
-            Tr[wi] = rc.thr[wi];
-        }
-    }
 
-    const S* src = level + row.level_row * pitch + base;
-    const int N  = kChunk + wmax;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* Q       = Ps + 4 + halo;
+    const S* src   = level + row.level_row * pitch + base;
+    const int seg_cols      = halo + kChunk;
+    const uint32_t seg_bytes = static_cast<uint32_t>(seg_cols * sizeof(S));
+    S* const stage0 = reinterpret_cast<S*>(Ps + 4 + seg_cols + 4); // buffer b at stage0 + b * seg_cols
+    const int nchunks = (p.n_valid + kChunk - 1) / kChunk;
+    auto issue = [&](int ci) {
+        bulk::mbar_expect(&bar[ci & 1], seg_bytes);
+        bulk::load(stage0 + (ci & 1) * seg_cols, src + static_cast<int64_t>(ci) * kChunk - halo, seg_bytes,
+                   &bar[ci & 1]);
+    };
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        bulk::mbar_init(&bar[0]);
+        bulk::mbar_init(&bar[1]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int ci = 0; ci < min(2, nchunks); ++ci)
+            issue(ci);
+    // 128-column segments (4 per lane): warp w scans a contiguous run of them
+    const int nseg  = (halo + kChunk) / 128;
+    const int spw   = (nseg + kThreads / 32 - 1) / (kThreads / 32);
+    const int s_beg = warp * spw, s_end = min(s_beg + spw, nseg);
+    const int jmin  = halo - wmax + 1; // earlier columns never enter a window
     const int64_t warm = static_cast<int64_t>(row.delay) + wmax - 1;
-    for (int64_t c0 = 0; c0 < p.n_valid; c0 += kChunk) {
-        // P[i] <- column c0 - wmax + i (i = 0 is the scan base).
-        for (int i = threadIdx.x; i < N; i += kThreads)
-            P[i] = i == 0 ? 0.0F : ldf<S>(src + c0 - wmax + i);
+    int ci = 0;
+    for (int64_t c0 = 0; c0 < p.n_valid; c0 += kChunk, ++ci) {
+        // ---- wait for the chunk's segment (bounded; a timeout ends the row)
+        if (!bulk::mbar_wait(&bar[ci & 1], static_cast<uint32_t>((ci >> 1) & 1)))
+            atomicExch(&abort_flag, 1);
         __syncthreads();
-        scan_inplace(P, N);
+        if (abort_flag)
+            break;
+        // ---- prefix sum: warp-local scans, then warp offsets
+        const S* seg = stage0 + (ci & 1) * seg_cols;
+        float carry  = 0.0F;
+        for (int sg = s_beg; sg < s_end; ++sg) {
+            const int j = sg * 128 + 4 * lane;
+            float4 x    = ld4s<S>(seg + j);
+            if (j < jmin) {
+                x.x = j < jmin ? 0.0F : x.x;
+                x.y = j + 1 < jmin ? 0.0F : x.y;
+                x.z = j + 2 < jmin ? 0.0F : x.z;
+                x.w = j + 3 < jmin ? 0.0F : x.w;
+            }
+            x.y += x.x;
+            x.z += x.y;
+            x.w += x.z;
+            float t = x.w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float u = __shfl_up_sync(0xFFFFFFFFU, t, o);
+                if (lane >= o)
+                    t += u;
+            }
+            const float before = __shfl_up_sync(0xFFFFFFFFU, t, 1);
+            const float off    = carry + (lane > 0 ? before : 0.0F);
+            x.x += off;
+            x.y += off;
+            x.z += off;
+            x.w += off;
+            *reinterpret_cast<float4*>(Ps + 4 + j) = x;
+            carry += __shfl_sync(0xFFFFFFFFU, t, 31);
+        }
+        if (lane == 0)
+            warp_tot[warp] = carry;
+        __syncthreads();
+        // every thread has read this chunk's staging buffer: refill it
+        if (threadIdx.x == 0 && ci + 2 < nchunks)
+            issue(ci + 2);
+        if (warp > 0) {
+            float woff = 0.0F;
+            for (int w = 0; w < warp; ++w)
+                woff += warp_tot[w];
+            for (int sg = s_beg; sg < s_end; ++sg) {
+                float4* v = reinterpret_cast<float4*>(Ps + 4 + sg * 128 + 4 * lane);
+                float4 x  = *v;
+                x.x += woff;
+                x.y += woff;
+                x.z += woff;
+                x.w += woff;
+                *v = x;
+            }
+        }
+        __syncthreads();
 
         const bool fast = c0 + kChunk <= p.n_valid && (!p.skip_cold || p.tile_t0 + c0 >= warm) &&
                           (!p.or_active || p.tile_t0 + c0 - p.gulp_t0 >= warm);
-        uint32_t any = 0;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        if constexpr (NW > 0) {
-            if (fast && !all) {
-                // steady state with the width count known at compile time:
-                // widths and thresholds live in registers
-#pragma unroll 1
-                for (int j = 0; j < kPerThread; ++j) {
-                    const int i    = threadIdx.x + j * kThreads + wmax;
-                    const float pi = P[i];
+        if (fast) {
+            // ---- steady state: the exact threshold test of every sample and
+            // width (the same float expression as wsum), 4 samples per vector
+            float4 qv[kPerThread / 4];
 #pragma unroll
-                    for (int wi = 0; wi < NW; ++wi) {
-                        float s = pi - P[i - Wr[wi]];
-                        if (Er[wi] > 0)
-                            s -= 0.5F * ((pi - P[i - Er[wi]]) + (P[i - Wr[wi] + Er[wi]] - P[i - Wr[wi]]));
-                        const uint32_t m = __ballot_sync(0xFFFFFFFFU, s > Tr[wi]);
-                        if (lane == 0)
-                            bits[wi][j * (kThreads / 32) + warp] = m;
-                        any |= m;
+            for (int q = 0; q < kPerThread / 4; ++q)
+                qv[q] = *reinterpret_cast<const float4*>(Q + 4 * (threadIdx.x + q * kThreads));
+            bool up = false;
+            for (int wi = 0; wi < nw; ++wi) {
+                const int W   = rc.W[wi];
+                const int E   = rc.E[wi];
+                const float T = rc.thr[wi];
+#pragma unroll
+                for (int q = 0; q < kPerThread / 4; ++q) {
+                    const int k    = 4 * (threadIdx.x + q * kThreads);
+                    const float4 a = qv[q];
+                    const float4 b = ld4(Q, k - W);
+                    float s0, s1, s2, s3;
+                    if (E > 0) {
+                        const float4 c = ld4(Q, k - E);
+                        const float4 d = ld4(Q, k - W + E);
+                        s0 = trap_sum(a.x, b.x, c.x, d.x);
+                        s1 = trap_sum(a.y, b.y, c.y, d.y);
+                        s2 = trap_sum(a.z, b.z, c.z, d.z);
+                        s3 = trap_sum(a.w, b.w, c.w, d.w);
+                    } else {
+                        s0 = a.x - b.x;
+                        s1 = a.y - b.y;
+                        s2 = a.z - b.z;
+                        s3 = a.w - b.w;
                     }
+                    up |= (s0 > T) | (s1 > T) | (s2 > T) | (s3 > T);
                 }
             }
+            if (!__syncthreads_or(up)) {
+                // nothing fired: runs open at the chunk start close here
+                if (!all && threadIdx.x == 0)
+                    close_open_runs(p, runs, nruns, row, &local_count);
+                continue; // Ps is rewritten only after every thread passed the barrier
+            }
         }
-        const bool generic = NW == 0 || !fast || all;
-        for (int j = 0; generic && j < kPerThread; ++j) {
+
+        // ---- a chunk that fired (or is not steady): per-width bit masks
+        uint32_t any = 0;
+        for (int j = 0; j < kPerThread; ++j) {
             // one sample, every width: its prefix value is read once
-            const int k  = threadIdx.x + j * kThreads;
-            const int i  = k + wmax;
-            const float pi = P[i];
+            const int k = threadIdx.x + j * kThreads;
             for (int wi = 0; wi < nw; ++wi) {
-                bool up;
-                if (fast) {
-                    const int W = rc.W[wi];
-                    const int E = rc.E[wi];
-                    float s     = pi - P[i - W];
-                    if (E > 0)
-                        s -= 0.5F * ((pi - P[i - E]) + (P[i - W + E] - P[i - W]));
-                    up = s > rc.thr[wi];
-                } else {
-                    up = snr_general(p, rc, P, wmax, c0, k, wi, row.delay) > p.thresh;
-                }
-                if (all && up) {
+                bool hit;
+                if (fast)
+                    hit = wsum(Q, k, rc.W[wi], rc.E[wi]) > rc.thr[wi];
+                else
+                    hit = snr_general(p, rc, Q, c0, k, wi, row.delay) > p.thresh;
+                if (all && hit) {
                     RunState r{};
-                    r.best   = snr_general(p, rc, P, wmax, c0, k, wi, row.delay);
+                    r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
                     r.best_w = wi;
                     r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
                     emit(p, row, r, &local_count);
                 }
-                const uint32_t m = __ballot_sync(0xFFFFFFFFU, up);
+                const uint32_t m = __ballot_sync(0xFFFFFFFFU, hit);
                 if (lane == 0)
                     bits[wi][j * (kThreads / 32) + warp] = m;
                 any |= m;
@@ -323,15 +459,24 @@ __global__ void __launch_bounds__(kThreads, 4)
         if (!all && threadIdx.x == 0) {
             if (across) {
                 if (fired || runs[0].open)
-                    walk_runs(p, rc, P, wmax, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
+                    walk_runs(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
             } else {
                 for (int wi = 0; wi < nw; ++wi)
                     if (fired || runs[wi].open)
-                        walk_runs(p, rc, P, wmax, c0, row.delay, bits[wi], wi, runs[wi], row,
+                        walk_runs(p, rc, Q, c0, row.delay, bits[wi], wi, runs[wi], row,
                                   &local_count);
             }
         }
         __syncthreads();
+    }
+    if (abort_flag) {
+        // a segment never landed: report it and let the copies in flight end
+        if (threadIdx.x == 0) {
+            atomicOr(p.err, 1U);
+            for (int j = ci; j < min(ci + 2, nchunks); ++j)
+                (void)bulk::mbar_wait(&bar[j & 1], static_cast<uint32_t>((j >> 1) & 1));
+        }
+        return;
     }
     if (threadIdx.x < nruns && !all)
         p.carry[g * nruns + threadIdx.x] = runs[threadIdx.x];
@@ -401,33 +546,24 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
         return;
     if (p.nwidths > kMaxWidths)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "search: more than 32 boxcar widths");
-    if (level.base < p.wmax)
-        throw Error(FROST_ERR_INTERNAL, "search: level history shorter than the widest boxcar");
+    if (p.halo != search_halo(p.wmax) || level.base < p.halo)
+        throw Error(FROST_ERR_INTERNAL, "search: level history shorter than the search halo");
     if (level.pitch - level.base < ((p.n_valid + kChunk - 1) / kChunk) * kChunk)
         throw Error(FROST_ERR_INTERNAL, "search: tile columns are not a whole number of chunks");
-    const size_t smem = sizeof(float) * (kChunk + p.wmax);
+    if (p.err == nullptr)
+        throw Error(FROST_ERR_INTERNAL, "search: no error flag");
+    const size_t es   = level.fp16 ? 2 : 4;
+    const size_t smem = sizeof(float) * (4 + p.halo + kChunk + 4) + 2 * es * (p.halo + kChunk);
     const dim3 grid(static_cast<unsigned>(g1 - g0));
     auto go = [&](auto kernel, auto data) {
         FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         kernel<<<grid, kThreads, smem, s>>>(p, data, level.pitch, level.base, g0);
     };
-    // width counts of wtsp = 2 with max_boxcar 16, 64, 256 and 4096
-    switch (level.fp16 ? 100 + p.nwidths : p.nwidths) {
-    case 5: go(k_search<float, 5>, static_cast<const float*>(level.data)); break;
-    case 7: go(k_search<float, 7>, static_cast<const float*>(level.data)); break;
-    case 9: go(k_search<float, 9>, static_cast<const float*>(level.data)); break;
-    case 13: go(k_search<float, 13>, static_cast<const float*>(level.data)); break;
-    case 105: go(k_search<__half, 5>, static_cast<const __half*>(level.data)); break;
-    case 107: go(k_search<__half, 7>, static_cast<const __half*>(level.data)); break;
-    case 109: go(k_search<__half, 9>, static_cast<const __half*>(level.data)); break;
-    case 113: go(k_search<__half, 13>, static_cast<const __half*>(level.data)); break;
-    default:
-        if (level.fp16)
-            go(k_search<__half, 0>, static_cast<const __half*>(level.data));
-        else
-            go(k_search<float, 0>, static_cast<const float*>(level.data));
-    }
+    if (level.fp16)
+        go(k_search<__half>, static_cast<const __half*>(level.data));
+    else
+        go(k_search<float>, static_cast<const float*>(level.data));
     FB_LAUNCH_CHECK();
 }
 

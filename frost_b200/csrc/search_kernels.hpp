@@ -16,6 +16,11 @@ constexpr int kSearchChunk = 4096;
 /** Column granularity of a level-buffer tile. */
 constexpr int kTileQuantum = kSearchChunk > kTimePerCta ? kSearchChunk : kTimePerCta;
 
+/** Columns before a search chunk that the search stages: the widest boxcar
+ * rounded up to whole 128-column segments. Level buffers keep at least this
+ * many history columns. */
+constexpr int32_t search_halo(int32_t wmax) { return (wmax + 127) / 128 * 128; }
+
 /** One searched row: a DM trial of one plane. */
 struct SearchRow {
     int64_t level_row; // row in its level buffer
@@ -49,6 +54,7 @@ struct SearchParams {
     const int32_t* widths;
     int32_t nwidths;
     int32_t wmax;
+    int32_t halo;            // search_halo(wmax)
     float thresh;
     int32_t peak_mode;       // enum frost_peak_mode
     int32_t trapezoid;
@@ -66,6 +72,7 @@ struct SearchParams {
     uint32_t* row_counts;    // [g]
     uint32_t max_per_dm;     // 0 = unlimited
     unsigned long long* dropped; // [0] global, [1] per DM
+    unsigned* err;           // set when a bounded wait for staged data ran out
 };
 
 /** Searches rows [g0, g1) (all in `level`) over the tile's valid columns. */

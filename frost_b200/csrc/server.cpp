@@ -40,14 +40,16 @@ SizeType Beam::block_bytes() const {
 
 SizeType Beam::device_bytes() const { return m_cleaner->memory_usage() + m_engine->device_bytes(); }
 
-void Beam::process(const uint8_t* block, SizeType bytes, SizeType nread) {
+void Beam::process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device) {
     if (bytes != block_bytes())
         invalid("serve: a gulp must be a whole block of max_nsamps rows");
-    const float* wf = m_cleaner->execute_normalized(block, bytes, nread, false, nullptr);
+    const uint64_t l0 = m_cleaner->launches();
+    const float* wf   = m_cleaner->execute_normalized(block, bytes, nread, on_device, nullptr);
     m_fdmt_mask     = m_cleaner->channel_mask();
     if (m_descending)
         std::reverse(m_fdmt_mask.begin(), m_fdmt_mask.end());
     m_engine->execute(wf, m_spec.layout.max_nsamps, true, m_fdmt_mask.data(), m_cleaner->stream());
+    m_last_launches = (m_cleaner->launches() - l0) + m_engine->last_launches();
     // samples searched: frost's accounting, lib/pipeline/pipeline.cpp:610-614
     m_read += nread;
     const uint64_t previous = m_read - nread;
@@ -92,10 +94,11 @@ uint32_t Server::add_beam(const BeamSpec& spec) {
     // Admission by device memory: build the beam (its buffers are sized by
     // its plan), then keep it only if the server's budget still holds.
     DeviceGuard g(m_device);
-    auto beam           = std::make_unique<Beam>(spec, m_device);
-    // the cleaner sizes its buffers on the first gulp: charge a full block
-    const SizeType need = beam->device_bytes() + 10 * beam->block_bytes() +
-                          static_cast<SizeType>(spec.layout.nchans) * spec.layout.max_nsamps * 8;
+    auto beam = std::make_unique<Beam>(spec, m_device);
+    // every steady-state buffer is allocated now, so the charge is the
+    // beam's footprint (plus a margin for small per-gulp transfers)
+    beam->preallocate();
+    const SizeType need = beam->device_bytes() + (SizeType{16} << 20);
     std::lock_guard<std::mutex> lk(m_mu);
     if (m_used + need > m_budget)
         throw Error(FROST_ERR_OUT_OF_MEMORY,
@@ -123,7 +126,8 @@ void Server::remove_beam(uint32_t beam) {
     m_busy.erase(beam);
 }
 
-uint64_t Server::submit(uint32_t beam, const uint8_t* block, SizeType bytes, SizeType nread) {
+uint64_t Server::submit(uint32_t beam, const uint8_t* block, SizeType bytes, SizeType nread,
+                        bool on_device) {
     if (block == nullptr)
         invalid("serve: null block");
     std::lock_guard<std::mutex> lk(m_mu);
@@ -134,7 +138,8 @@ uint64_t Server::submit(uint32_t beam, const uint8_t* block, SizeType bytes, Siz
     req->beam    = beam;
     req->block   = block;
     req->bytes   = bytes;
-    req->nread   = nread;
+    req->nread     = nread;
+    req->on_device = on_device;
     req->arrival = now_seconds();
     if (m_first_arrival < 0)
         m_first_arrival = req->arrival;
@@ -183,9 +188,11 @@ void Server::worker() {
         int status = FROST_OK;
         std::string err;
         std::vector<frost_candidate> cands;
+        uint64_t launches = 0;
         try {
-            b->process(req->block, req->bytes, req->nread);
-            cands = b->results();
+            b->process(req->block, req->bytes, req->nread, req->on_device);
+            cands    = b->results();
+            launches = b->last_launches();
         } catch (const Error& e) {
             status = e.code();
             err    = e.what();
@@ -205,6 +212,7 @@ void Server::worker() {
                 m_latencies.push_back(req->done - req->arrival);
                 m_beam_seconds += static_cast<double>(req->nread) * b->tsamp();
                 m_last_done = std::max(m_last_done, req->done);
+                m_launches += launches;
                 ++m_completed;
             }
         }
@@ -251,6 +259,16 @@ std::vector<frost_candidate> Server::drain(uint32_t beam) {
     return out;
 }
 
+void Server::reset_stats() {
+    std::lock_guard<std::mutex> lk(m_mu);
+    m_latencies.clear();
+    m_beam_seconds  = 0;
+    m_first_arrival = -1;
+    m_last_done     = 0;
+    m_completed     = 0;
+    m_launches      = 0;
+}
+
 frost_server_stats Server::stats() {
     std::lock_guard<std::mutex> lk(m_mu);
     frost_server_stats s{};
@@ -258,7 +276,8 @@ frost_server_stats Server::stats() {
     s.beams        = m_beams.size();
     s.device_bytes = m_used;
     s.beam_seconds = m_beam_seconds;
-    s.wall_seconds = m_first_arrival >= 0 ? m_last_done - m_first_arrival : 0.0;
+    s.wall_seconds = m_first_arrival >= 0 && m_completed > 0 ? m_last_done - m_first_arrival : 0.0;
+    s.launches     = m_launches;
     if (!m_latencies.empty()) {
         std::vector<double> l = m_latencies;
         std::sort(l.begin(), l.end());

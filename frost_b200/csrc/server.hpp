@@ -35,11 +35,16 @@ struct BeamSpec {
 class Beam {
 public:
     Beam(const BeamSpec& spec, int device);
-    /** Cleans and searches one gulp (host block, block rows, nread valid). */
-    void process(const uint8_t* block, SizeType bytes, SizeType nread);
+    /** Allocates the beam's steady-state device buffers up front. */
+    void preallocate() { m_cleaner->preallocate(); }
+    /** Cleans and searches one gulp (a block of max_nsamps rows, nread
+     * valid, on the host or on the beam's device). */
+    void process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device);
     std::vector<frost_candidate> results() const { return m_engine->results(); }
     std::vector<frost_candidate> drain();
     uint64_t samples_searched() const { return m_searched; }
+    /** Kernels launched by the last process() call. */
+    uint64_t last_launches() const { return m_last_launches; }
     double tsamp() const { return m_spec.layout.tsamp; }
     SizeType device_bytes() const;
     SizeType block_bytes() const;
@@ -50,7 +55,7 @@ private:
     std::unique_ptr<fdmt::Engine> m_engine;
     bool m_descending;
     std::vector<uint8_t> m_fdmt_mask;
-    uint64_t m_read = 0, m_searched = 0, m_max_delay = 0;
+    uint64_t m_read = 0, m_searched = 0, m_max_delay = 0, m_last_launches = 0;
 };
 
 struct Request {
@@ -59,6 +64,7 @@ struct Request {
     const uint8_t* block;
     SizeType bytes;
     SizeType nread;
+    bool on_device;
     double arrival;  // steady seconds
     double done = 0;
     bool finished = false;
@@ -73,10 +79,12 @@ public:
     ~Server();
     uint32_t add_beam(const BeamSpec& spec);
     void remove_beam(uint32_t beam);
-    uint64_t submit(uint32_t beam, const uint8_t* block, SizeType bytes, SizeType nread);
+    uint64_t submit(uint32_t beam, const uint8_t* block, SizeType bytes, SizeType nread,
+                    bool on_device);
     /** Blocks until the ticket is done; moves its candidates out. */
     std::vector<frost_candidate> wait(uint64_t ticket, double* latency_s);
     frost_server_stats stats();
+    void reset_stats();
     std::vector<frost_candidate> drain(uint32_t beam);
 
 private:
@@ -94,7 +102,7 @@ private:
     std::map<uint64_t, std::shared_ptr<Request>> m_requests;
     std::vector<double> m_latencies;
     double m_beam_seconds = 0, m_first_arrival = -1, m_last_done = 0;
-    uint64_t m_completed = 0;
+    uint64_t m_completed = 0, m_launches = 0;
     std::vector<std::thread> m_workers;
 
     void worker();

@@ -29,6 +29,7 @@ class ServerStats:
     p50_latency_s: float
     p99_latency_s: float
     max_latency_s: float
+    launches: int
 
     @property
     def beam_seconds_per_second(self) -> float:
@@ -76,10 +77,17 @@ class BeamServer:
         """Queues one gulp (a whole host block of max_nsamps rows, `nread`
         valid); the block is kept alive until wait() returns its ticket."""
         buf = np.ascontiguousarray(block).view(np.uint8).reshape(-1)
+        ticket = self.submit_ptr(beam, buf.ctypes.data, buf.size, nread, on_device=False)
+        self._blocks[ticket] = buf
+        return ticket
+
+    def submit_ptr(self, beam: int, ptr: int, nbytes: int, nread: int, on_device: bool) -> int:
+        """Queues one gulp at `ptr` (device memory of the server's device
+        when on_device, else host memory, preferably pinned); the caller
+        keeps it valid until wait() returns the ticket."""
         ticket = C.c_uint64()
-        check(lib().frost_server_submit(self._h, beam, buf.ctypes.data_as(C.POINTER(C.c_uint8)),
-                                        buf.size, nread, C.byref(ticket)))
-        self._blocks[ticket.value] = buf
+        check(lib().frost_server_submit(self._h, beam, C.c_void_p(ptr), nbytes, nread,
+                                        1 if on_device else 0, C.byref(ticket)))
         self._beam_of[ticket.value] = beam
         return ticket.value
 
@@ -109,4 +117,7 @@ class BeamServer:
         s = _abi.ServerStatsC()
         check(lib().frost_server_get_stats(self._h, C.byref(s)))
         return ServerStats(s.completed, s.beams, s.device_bytes, s.beam_seconds, s.wall_seconds,
-                           s.p50_latency_s, s.p99_latency_s, s.max_latency_s)
+                           s.p50_latency_s, s.p99_latency_s, s.max_latency_s, s.launches)
+
+    def reset_stats(self):
+        check(lib().frost_server_reset_stats(self._h))

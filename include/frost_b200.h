@@ -504,6 +504,7 @@ typedef struct {
     double p50_latency_s;
     double p99_latency_s;
     double max_latency_s;
+    uint64_t launches;     /* kernels launched for the completed gulps */
 } frost_server_stats;
 
 typedef struct frost_server frost_server;
@@ -513,8 +514,9 @@ int frost_server_create(int device, size_t memory_budget, uint32_t slots, frost_
 int frost_server_destroy(frost_server* s);
 
 /* Admits a beam (RFICleaner + search engine, plan.block_nsamps ==
- * layout.max_nsamps) or fails with FROST_ERR_OUT_OF_MEMORY when its device
- * memory would exceed the budget. */
+ * layout.max_nsamps): allocates all of its steady-state device buffers and
+ * charges their size, or fails with FROST_ERR_OUT_OF_MEMORY when that would
+ * exceed the budget. */
 int frost_server_add_beam(frost_server* s,
                           const frost_rfi_config* rfi,
                           const frost_block_layout* layout,
@@ -526,13 +528,15 @@ int frost_server_add_beam(frost_server* s,
 /* Waits for the beam's queued gulps, then releases it. */
 int frost_server_remove_beam(frost_server* s, uint32_t beam);
 
-/* Queues one gulp (a host block of max_nsamps rows, `nread` valid); the
- * block must stay valid until frost_server_wait returns for the ticket. */
+/* Queues one gulp (a block of max_nsamps rows, `nread` valid) that is in
+ * host memory, or in the server device's memory when on_device is non-zero;
+ * the block must stay valid until frost_server_wait returns for the ticket. */
 int frost_server_submit(frost_server* s,
                         uint32_t beam,
                         const uint8_t* block,
                         size_t block_bytes,
                         size_t nread,
+                        int on_device,
                         uint64_t* ticket);
 
 /* Blocks until the gulp is searched; copies up to `capacity` candidates
@@ -552,7 +556,10 @@ int frost_server_drain(frost_server* s,
                        size_t capacity,
                        size_t* count);
 
+/* Statistics since the server was created or since the last reset; a
+ * reset while gulps are in flight counts them when they complete. */
 int frost_server_get_stats(frost_server* s, frost_server_stats* out);
+int frost_server_reset_stats(frost_server* s);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -61,7 +61,29 @@ def test_served_beams_match_each_beam_alone():
     expect = 3 * sum(_nread(g) for g in range(NGULPS)) * TSAMP
     assert abs(s.beam_seconds - expect) < 1e-6 * expect
     assert 0 < s.p50_latency_s <= s.p99_latency_s <= s.max_latency_s
-    assert s.wall_seconds > 0
+    assert s.wall_seconds > 0 and s.launches > 10 * s.completed
+    srv.reset_stats()
+    assert srv.stats().completed == 0 and srv.stats().launches == 0
+    srv.close()
+
+
+def test_device_resident_gulps_match_host_gulps():
+    import torch
+
+    from frost_b200.serve import BeamServer
+    rfi, layout, plan, bc = _setup()
+    st = _beam_stream(31)
+    srv = BeamServer(slots=2)
+    host_beam, dev_beam = srv.add_beam(rfi, layout, 1.0, plan, bc), srv.add_beam(rfi, layout, 1.0, plan, bc)
+    dev = torch.from_numpy(st.reshape(-1)).cuda()
+    gulp_bytes = GULP * NCHANS
+    for g in range(NGULPS):
+        th = srv.submit(host_beam, st[g * GULP:(g + 1) * GULP], _nread(g))
+        td = srv.submit_ptr(dev_beam, dev.data_ptr() + g * gulp_bytes, gulp_bytes, _nread(g), on_device=True)
+        a, _ = srv.wait(th)
+        b, _ = srv.wait(td)
+        assert np.array_equal(a, b), g
+    assert np.array_equal(srv.drain(host_beam), srv.drain(dev_beam))
     srv.close()
 
 
