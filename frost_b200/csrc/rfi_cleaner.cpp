@@ -254,6 +254,11 @@ Cleaner::Cleaner(const frost_rfi_config& cfg, const frost_block_layout& layout,
     m_zdot_b.assign(m_n, 0.0F);
     FB_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
     h2d(m_static_mask_d, m_static_mask.data(), m_n, m_stream);
+    // Reciprocals of the Welford counts (correctly rounded host divisions).
+    std::vector<double> recip(layout.max_nsamps + 1, 0.0);
+    for (SizeType n = 1; n < recip.size(); ++n)
+        recip[n] = 1.0 / static_cast<double>(n);
+    h2d(m_recip, recip.data(), recip.size(), m_stream);
     FB_CUDA(cudaStreamSynchronize(m_stream));
 }
 
@@ -284,7 +289,7 @@ SizeType Cleaner::memory_usage() const {
         &m_kspec_whole, &m_chunk_min, &m_chunk_max, &m_chunk_zdot, &m_chunk_kpos, &m_chunk_kneg,
         &m_lo, &m_hi, &m_zdot_sum, &m_kpos_best, &m_kneg_best, &m_time_flags_d, &m_zdot_a_d,
         &m_zdot_b_d, &m_kchan_pos_d, &m_kchan_neg_d, &m_flagged_d, &m_work, &m_out, &m_counters,
-        &m_first_bad, &m_tail_loc, &m_tail_scale, &m_tail_out_loc, &m_tail_out_scale};
+        &m_first_bad, &m_tail_loc, &m_tail_scale, &m_tail_out_loc, &m_tail_out_scale, &m_recip};
     SizeType total = 0;
     for (const auto* b : all)
         total += b->bytes();
@@ -367,10 +372,17 @@ const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, S
     } counting{m_launches};
 
     // Raw block on the device.
+    // A device block that does not start on a 16-byte boundary is copied
+    // into the cleaner's own buffer first: the kernels read whole samples
+    // and 16-byte row segments, which a misaligned pointer would fault.
     const uint8_t* raw = block;
     if (!on_device) {
         if (bytes)
             FB_CUDA(cudaMemcpyAsync(m_raw.get(), block, bytes, cudaMemcpyHostToDevice, s));
+        raw = m_raw.as<uint8_t>();
+    } else if (reinterpret_cast<uintptr_t>(block) % 16 != 0) {
+        if (bytes)
+            FB_CUDA(cudaMemcpyAsync(m_raw.get(), block, bytes, cudaMemcpyDeviceToDevice, s));
         raw = m_raw.as<uint8_t>();
     }
     // Non-finite float32 input is rejected before any statistics.
@@ -414,7 +426,7 @@ const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, S
         d.nwin = 1;
         launch_unpack(d, raw, m_work.as<float>(), s);
         h2d(m_mask_d, m_mask.data(), m_n, s);
-        launch_welford(d, m_work.as<float>(), m_loc2.as<float>(), m_scale2.as<float>(), s);
+        launch_welford(d, m_work.as<float>(), m_recip.as<double>(), m_loc2.as<float>(), m_scale2.as<float>(), s);
         loc   = m_loc2.as<float>();
         scale = m_scale2.as<float>();
         m_time_flags.assign(valid, 0);
@@ -422,7 +434,7 @@ const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, S
         run_full(d, s);
         ++m_block_index;
         if (m_transform) {
-            launch_welford(d, m_work.as<float>(), m_loc2.as<float>(), m_scale2.as<float>(), s);
+            launch_welford(d, m_work.as<float>(), m_recip.as<double>(), m_loc2.as<float>(), m_scale2.as<float>(), s);
             loc   = m_loc2.as<float>();
             scale = m_scale2.as<float>();
         }

@@ -25,6 +25,7 @@
 
 #include "common.hpp"
 #include "rfi_kernels.hpp"
+#include "rfi_stage.cuh"
 
 namespace fb::rfi {
 
@@ -48,6 +49,11 @@ template <int D> __device__ __forceinline__ float rd(const uint8_t* __restrict__
         return static_cast<float>((row[bit >> 3U] >> (bit & 7U)) & kMask);
     }
 }
+
+// Bits per packed sample of dtype D (usable in device code).
+template <int D>
+constexpr uint64_t kBitsOf = D == FROST_UINT1 ? 1 : D == FROST_UINT2 ? 2 : D == FROST_UINT4 ? 4
+                           : D == FROST_UINT8 ? 8 : D == FROST_UINT16 ? 16 : 32;
 
 #define FB_DTYPE_CASE(DT, ...)                                                                    \
     case DT: {                                                                                    \
@@ -265,7 +271,175 @@ __global__ void k_bandpass(Dims d, const float* __restrict__ samples, float* __r
     inv_out[o]     = 1.0F / fs;
 }
 
+// The same per-(window, channel) bandpass with the sampled rows streamed
+// through shared memory (rfi_stage.cuh), one thread per channel of a
+// 128-channel segment. Every pass over the rows is one staged sweep; the
+// block runs the optional passes (mean fallback, clip iterations) when any
+// of its channels needs them, and each channel updates only while its own
+// sequence of steps is still running, so every channel takes exactly the
+// steps of the direct kernel above.
+constexpr int kBandChans = 128;
+
+__global__ void __launch_bounds__(kBandChans)
+    k_bandpass_staged(Dims d, const float* __restrict__ samples, float* __restrict__ loc_out,
+                      float* __restrict__ scale_out, float* __restrict__ inv_out,
+                      uint32_t* __restrict__ unmeasured, int seg_bytes, int rows) {
+    extern __shared__ __align__(16) uint8_t stage_buf[];
+    const uint64_t c0  = static_cast<uint64_t>(blockIdx.x) * kBandChans;
+    const uint64_t c   = c0 + threadIdx.x;
+    const uint64_t w   = blockIdx.y;
+    const bool in      = c < d.nchans;
+    const uint64_t b   = window_begin(w, d.window);
+    const uint64_t len = window_end(w, d) - b;
+    const uint64_t m   = largest_power_of_five_leq(len < kMaxBandpassRows ? len : kMaxBandpassRows);
+    int levels         = 0;
+    for (uint64_t p = m; p > 1; p /= 5)
+        ++levels;
+    const uint64_t n     = d.nchans;
+    const uint64_t pitch = n * sizeof(float);
+    const uint64_t left  = pitch - c0 * sizeof(float);
+    const int copy       = static_cast<int>(left < static_cast<uint64_t>(seg_bytes) ? left : seg_bytes);
+    const int stride     = seg_bytes / static_cast<int>(sizeof(float));
+    const uint8_t* src   = reinterpret_cast<const uint8_t*>(samples + w * kMaxBandpassRows * n + c0);
+    // one sweep over rows 0 .. m-1: f(x, i) per row, in order
+    auto sweep = [&](auto&& f) {
+        stage::Stager st(stage_buf, src, pitch, seg_bytes, copy, rows, 0, m);
+        st.start();
+        for (int k = 0; k < st.nblk; ++k) {
+            st.wait(k);
+            const float* buf = reinterpret_cast<const float*>(st.buf(k));
+            const int nr     = st.rows_of(k);
+            const uint64_t i0 = st.t0(k);
+            if (in)
+                for (int r = 0; r < nr; ++r)
+                    f(buf[r * stride + threadIdx.x], i0 + r);
+            st.release(k);
+        }
+    };
+
+    // Level (remedian) and the sample range; then the scale (remedian of
+    // |x - level| times 1.4826) (lib/cpu/spectra_cpu.cpp:73-130).
+    Remedian r;
+    r.init(levels);
+    float lo = 0.0F, hi = 0.0F;
+    sweep([&](float x, uint64_t i) {
+        r.push(x);
+        if (i == 0) {
+            lo = x;
+            hi = x;
+        } else {
+            lo = smin(lo, x);
+            hi = smax(hi, x);
+        }
+    });
+    const float level = r.result;
+    r.init(levels);
+    sweep([&](float x, uint64_t) { r.push(fabsf(x - level)); });
+    const float rms = r.result * kMadToStd;
+
+    // Clipped refinement in double (lib/cpu/bandpass_kernels.hpp:17-76).
+    const uint64_t o = w * n + c;
+    const bool flat  = !(hi > lo);
+    if (in && flat) {
+        loc_out[o]   = lo;
+        scale_out[o] = 0.0F;
+        inv_out[o]   = 0.0F;
+        atomicAdd(&unmeasured[c], 1U);
+    }
+    bool live       = in && !flat;
+    double centre   = level;
+    double sd       = rms;
+    const double dm = static_cast<double>(m);
+    const bool need_mean = live && !(sd > 0.0);
+    if (__syncthreads_or(need_mean)) {
+        double mean = 0.0;
+        sweep([&](float x, uint64_t) {
+            if (need_mean)
+                mean += x;
+        });
+        mean /= dm;
+        double ss = 0.0;
+        sweep([&](float x, uint64_t) {
+            if (need_mean)
+                ss += (x - mean) * (x - mean);
+        });
+        if (need_mean)
+            sd = sqrt(ss / dm);
+    }
+    for (int it = 0; it < kClipIterations; ++it) {
+        if (!__syncthreads_or(live))
+            break;
+        const double cut = kClipSigma * sd;
+        double count = 0.0, sum = 0.0;
+        sweep([&](float x, uint64_t) {
+            if (live) {
+                const double dv = x - centre;
+                if (fabs(dv) <= cut) {
+                    count += 1.0;
+                    sum += dv;
+                }
+            }
+        });
+        if (live && count < 2.0)
+            live = false;
+        const double shift = live ? sum / count : 0.0;
+        if (!__syncthreads_or(live))
+            break;
+        double ss = 0.0;
+        sweep([&](float x, uint64_t) {
+            if (live) {
+                const double dv = x - centre;
+                if (fabs(dv) <= cut)
+                    ss += (dv - shift) * (dv - shift);
+            }
+        });
+        if (live) {
+            const double clipped = sqrt(ss / count);
+            if (!(clipped > 0.0)) {
+                live = false;
+            } else {
+                centre += shift;
+                sd = clipped;
+            }
+        }
+    }
+    if (in && !flat) {
+        const float fl = static_cast<float>(centre);
+        const float fs = static_cast<float>(sd);
+        loc_out[o]     = fl;
+        scale_out[o]   = fs;
+        inv_out[o]     = 1.0F / fs;
+    }
+}
+
 // ---- moments --------------------------------------------------------------
+
+// One (window, channel) sequence of the moments pass, fed in time order
+// (lib/cpu/rfi_cpu_measure.cpp:91-138).
+struct MomentsAcc {
+    MomentSums s{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double prev = 0.0;
+    float l, iv;
+    double clip;
+    uint64_t b;
+    __device__ __forceinline__ void step(float x, uint64_t t) {
+        const double z  = (x - l) * iv;
+        const double z2 = z * z;
+        s.n += 1.0;
+        s.s1 += z;
+        s.s2 += z2;
+        s.s3 += z2 * z;
+        s.s4 += z2 * z2;
+        if (t > b)
+            s.lag += z * prev;
+        prev = z;
+        if (fabs(z) <= clip) {
+            s.nc += 1.0;
+            s.c1 += z;
+            s.c2 += z2;
+        }
+    }
+};
 
 template <int D>
 __global__ void k_moments(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
@@ -276,11 +450,13 @@ __global__ void k_moments(Dims d, const uint8_t* __restrict__ raw, const float* 
     if (c >= d.nchans)
         return;
     const uint64_t o = w * d.nchans + c;
-    MomentSums s{0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const float l = loc[o], iv = inv[o];
-    if (static_mask[c] != 0 && iv != 0.0F) {
-        const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
-        double prev      = 0.0;
+    const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
+    MomentsAcc acc;
+    acc.l    = loc[o];
+    acc.iv   = inv[o];
+    acc.clip = clip;
+    acc.b    = b;
+    if (static_mask[c] != 0 && acc.iv != 0.0F) {
         // Rows are fetched kBlock at a time (independent loads in flight),
         // then consumed strictly in time order.
         for (uint64_t t0 = b; t0 < e; t0 += kBlock) {
@@ -292,31 +468,123 @@ __global__ void k_moments(Dims d, const uint8_t* __restrict__ raw, const float* 
             for (int j = 0; j < kBlock; ++j) {
                 if (t0 + j >= e)
                     break;
-                const double z  = (xs[j] - l) * iv;
-                const double z2 = z * z;
-                s.n += 1.0;
-                s.s1 += z;
-                s.s2 += z2;
-                s.s3 += z2 * z;
-                s.s4 += z2 * z2;
-                if (t0 + j > b)
-                    s.lag += z * prev;
-                prev = z;
-                if (fabs(z) <= clip) {
-                    s.nc += 1.0;
-                    s.c1 += z;
-                    s.c2 += z2;
-                }
+                acc.step(xs[j], t0 + j);
             }
         }
     }
-    out[o] = s;
+    out[o] = acc.s;
+}
+
+// The same sequences with the block's channel columns streamed through
+// shared memory (rfi_stage.cuh): one thread per channel of a
+// kStageChans-channel segment.
+constexpr int kStageChans = 128;
+
+template <int D>
+__global__ void __launch_bounds__(kStageChans)
+    k_moments_staged(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
+                     const float* __restrict__ inv, const uint8_t* __restrict__ static_mask,
+                     float clip, MomentSums* __restrict__ out, int seg_bytes, int rows) {
+    extern __shared__ __align__(16) uint8_t stage_buf[];
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kStageChans;
+    const uint64_t c  = c0 + threadIdx.x;
+    const uint64_t w  = blockIdx.y;
+    const bool in     = c < d.nchans;
+    const uint64_t o  = w * d.nchans + c;
+    const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
+    MomentsAcc acc;
+    acc.l    = in ? loc[o] : 0.0F;
+    acc.iv   = in ? inv[o] : 0.0F;
+    acc.clip = clip;
+    acc.b    = b;
+    const bool active   = in && static_mask[c] != 0 && acc.iv != 0.0F;
+    const uint64_t off  = c0 * kBitsOf<D> / 8;
+    const uint64_t left = d.row_bytes - off;
+    const int copy      = static_cast<int>(left < static_cast<uint64_t>(seg_bytes) ? left : seg_bytes);
+    stage::Stager st(stage_buf, raw + off, d.row_bytes, seg_bytes, copy, rows, b, e);
+    st.start();
+    for (int k = 0; k < st.nblk; ++k) {
+        st.wait(k);
+        const uint8_t* buf = st.buf(k);
+        const int nr       = st.rows_of(k);
+        const uint64_t t0  = st.t0(k);
+        if (active) {
+#pragma unroll 8
+            for (int r = 0; r < nr; ++r)
+                acc.step(rd<D>(buf + r * seg_bytes, threadIdx.x), t0 + r);
+        }
+        st.release(k);
+    }
+    if (in)
+        out[o] = acc.s;
 }
 
 // ---- row scan ---------------------------------------------------------------
 
 constexpr int kScanRows  = 128; // rows per CTA (one thread each)
 constexpr int kScanChans = 64;  // channel tile staged in shared memory
+
+// One row of the row scan (lib/cpu/rfi_cpu_measure.cpp:305-446), fed its
+// channels in ascending order: the detection series sums and the Kadane
+// states across frequency.
+struct ScanRowAcc {
+    double sum_det = 0.0, sum_keep = 0.0, n_keep = 0.0, sx = 0.0, sxx = 0.0, n_meas = 0.0;
+    KadaneState sp = KadaneState::make(), sn = KadaneState::make();
+    __device__ __forceinline__ void step(uint64_t c, float x, float l, float ic, float clip, int kspec) {
+        n_meas += 1.0;
+        const float zc = (x - l) * ic;
+        const float cl = clampf(zc, -clip, clip);
+        sum_det += cl;
+        if (fabsf(zc) <= clip) {
+            sum_keep += zc;
+            n_keep += 1.0;
+        }
+        sx += x;
+        sxx += static_cast<double>(x) * x;
+        if (kspec) {
+            sp.append(static_cast<int64_t>(c), cl);
+            sn.append(static_cast<int64_t>(c), -cl);
+        }
+    }
+    __device__ void finish(const Dims& d, uint64_t t, const KspecParams& kp,
+                           const uint64_t* __restrict__ good_prefix, float* __restrict__ s_det,
+                           double* __restrict__ s_keep_d, float* __restrict__ s_keep_f,
+                           float* __restrict__ row_std, Span32* __restrict__ kspec_pos,
+                           Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole) const {
+        const double dn     = n_meas > 1.0 ? n_meas : 1.0;
+        const double s_keep = n_keep > 0.0 ? sum_keep / n_keep : 0.0;
+        s_det[t]            = static_cast<float>(sum_det / dn);
+        s_keep_f[t]         = static_cast<float>(s_keep);
+        s_keep_d[t]         = s_keep;
+        const double mx     = sx / dn;
+        const double var    = (sxx / dn) - (mx * mx);
+        row_std[t]          = static_cast<float>(sqrt(var < 0.0 ? 0.0 : var));
+        if (kp.enabled) {
+            // accept_span (lib/cpu/rfi_cpu_measure.cpp:335-349)
+            auto accept = [&](const Run& r, Span32& out) -> bool {
+                out = {-1, -1};
+                if (r.length() <= 0)
+                    return false;
+                const uint64_t lo    = static_cast<uint64_t>(r.start);
+                const uint64_t hi    = static_cast<uint64_t>(r.end);
+                const uint64_t count = good_prefix[hi + 1] - good_prefix[lo];
+                const double nspan   = static_cast<double>(hi - lo + 1);
+                const double snr     = r.sum / sqrt(static_cast<double>(count));
+                if (snr > kp.threshold && nspan >= kp.min_bw_chans) {
+                    out = {static_cast<int32_t>(lo), static_cast<int32_t>(hi)};
+                    return nspan > kp.whole_chans;
+                }
+                return false;
+            };
+            Span32 a, b;
+            bool whole     = accept(sp.best, a);
+            whole          = accept(sn.best, b) || whole;
+            kspec_pos[t]   = a;
+            kspec_neg[t]   = b;
+            kspec_whole[t] = whole ? 1 : 0;
+        }
+    }
+};
 
 template <int D>
 __global__ void __launch_bounds__(kScanRows)
@@ -334,9 +602,7 @@ __global__ void __launch_bounds__(kScanRows)
     const uint64_t w     = active ? window_of(t, d.window, d.nwin) : 0;
     const float* lw      = loc + w * n;
     const float* iw      = inv + w * n;
-    double sum_det = 0.0, sum_keep = 0.0, n_keep = 0.0, sx = 0.0, sxx = 0.0, n_meas = 0.0;
-    KadaneState sp = KadaneState::make(), sn = KadaneState::make();
-
+    ScanRowAcc acc;
     for (uint64_t c0 = 0; c0 < n; c0 += kScanChans) {
         const unsigned cl_ = threadIdx.x % kScanChans;
         const uint64_t cc  = c0 + cl_;
@@ -355,58 +621,161 @@ __global__ void __launch_bounds__(kScanRows)
             const float ic = iw[c];
             if (ic == 0.0F)
                 continue;
-            const float x = tile[threadIdx.x][c - c0];
-            n_meas += 1.0;
-            const float zc = (x - lw[c]) * ic;
-            const float cl = clampf(zc, -clip, clip);
-            sum_det += cl;
-            if (fabsf(zc) <= clip) {
-                sum_keep += zc;
-                n_keep += 1.0;
-            }
-            sx += x;
-            sxx += static_cast<double>(x) * x;
-            if (kp.enabled) {
-                sp.append(static_cast<int64_t>(c), cl);
-                sn.append(static_cast<int64_t>(c), -cl);
-            }
+            acc.step(c, tile[threadIdx.x][c - c0], lw[c], ic, clip, kp.enabled);
         }
     }
-    if (!active)
-        return;
-    const double dn     = n_meas > 1.0 ? n_meas : 1.0;
-    const double s_keep = n_keep > 0.0 ? sum_keep / n_keep : 0.0;
-    s_det[t]            = static_cast<float>(sum_det / dn);
-    s_keep_f[t]         = static_cast<float>(s_keep);
-    s_keep_d[t]         = s_keep;
-    const double mx     = sx / dn;
-    const double var    = (sxx / dn) - (mx * mx);
-    row_std[t]          = static_cast<float>(sqrt(var < 0.0 ? 0.0 : var));
-    if (kp.enabled) {
-        // accept_span (lib/cpu/rfi_cpu_measure.cpp:335-349)
-        auto accept = [&](const Run& r, Span32& out) -> bool {
-            out = {-1, -1};
-            if (r.length() <= 0)
-                return false;
-            const uint64_t lo    = static_cast<uint64_t>(r.start);
-            const uint64_t hi    = static_cast<uint64_t>(r.end);
-            const uint64_t count = good_prefix[hi + 1] - good_prefix[lo];
-            const double nspan   = static_cast<double>(hi - lo + 1);
-            const double snr     = r.sum / sqrt(static_cast<double>(count));
-            if (snr > kp.threshold && nspan >= kp.min_bw_chans) {
-                out = {static_cast<int32_t>(lo), static_cast<int32_t>(hi)};
-                return nspan > kp.whole_chans;
-            }
-            return false;
-        };
-        Span32 a, b;
-        bool whole = accept(sp.best, a);
-        whole      = accept(sn.best, b) || whole;
-        kspec_pos[t]   = a;
-        kspec_neg[t]   = b;
-        kspec_whole[t] = whole ? 1 : 0;
-    }
+    if (active)
+        acc.finish(d, t, kp, good_prefix, s_det, s_keep_d, s_keep_f, row_std, kspec_pos, kspec_neg,
+                   kspec_whole);
 }
+
+// The same rows with 256-byte column tiles of all 128 rows bulk-copied
+// into shared memory (cp.async, two tiles deep; rows padded to 272 bytes so
+// that each thread's 16-byte reads of its own row are conflict-free).
+constexpr int kRowTileBytes  = 256;
+constexpr int kRowTileStride = kRowTileBytes + 16;
+
+template <int D>
+__global__ void __launch_bounds__(kScanRows)
+    k_scan_rows_staged(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
+                       const float* __restrict__ inv, const uint8_t* __restrict__ mask, float clip,
+                       KspecParams kp, const uint64_t* __restrict__ good_prefix,
+                       float* __restrict__ s_det, double* __restrict__ s_keep_d,
+                       float* __restrict__ s_keep_f, float* __restrict__ row_std,
+                       Span32* __restrict__ kspec_pos, Span32* __restrict__ kspec_neg,
+                       uint8_t* __restrict__ kspec_whole) {
+    extern __shared__ __align__(16) uint8_t tiles[]; // [2][kScanRows][kRowTileStride]
+    constexpr int kPerChunk = static_cast<int>(128 / kBitsOf<D>); // channels per 16 bytes
+    constexpr int kTileCh   = static_cast<int>(kRowTileBytes * 8 / kBitsOf<D>);
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kScanRows;
+    const uint64_t t  = t0 + threadIdx.x;
+    const bool active = t < d.nsamps;
+    const uint64_t n  = d.nchans;
+    const uint64_t w  = active ? window_of(t, d.window, d.nwin) : 0;
+    const float* lw   = loc + w * n;
+    const float* iw   = inv + w * n;
+    const int nrows   = static_cast<int>(d.nsamps - t0 < kScanRows ? d.nsamps - t0 : kScanRows);
+    const int ntiles  = static_cast<int>((d.row_bytes + kRowTileBytes - 1) / kRowTileBytes);
+    auto issue = [&](int j) {
+        const uint64_t b0  = static_cast<uint64_t>(j) * kRowTileBytes;
+        const int chunks   = static_cast<int>((d.row_bytes - b0 < kRowTileBytes ? d.row_bytes - b0 : kRowTileBytes) / 16);
+        uint8_t* dst       = tiles + (j & 1) * kScanRows * kRowTileStride;
+        for (int i = threadIdx.x; i < nrows * chunks; i += kScanRows) {
+            const int r = i / chunks, v = i - r * chunks;
+            stage::cp_async16(dst + r * kRowTileStride + v * 16, raw + (t0 + r) * d.row_bytes + b0 + v * 16);
+        }
+        stage::commit();
+    };
+    issue(0);
+    if (ntiles > 1)
+        issue(1);
+    ScanRowAcc acc;
+    for (int j = 0; j < ntiles; ++j) {
+        if (j + 1 < ntiles)
+            stage::wait_pending<1>();
+        else
+            stage::wait_pending<0>();
+        __syncthreads();
+        if (active) {
+            const uint8_t* row = tiles + (j & 1) * kScanRows * kRowTileStride + threadIdx.x * kRowTileStride;
+            const uint64_t cb  = static_cast<uint64_t>(j) * kTileCh;
+            const uint64_t ce  = cb + kTileCh < n ? cb + kTileCh : n;
+            for (uint64_t q = cb; q < ce; q += kPerChunk) {
+                union {
+                    uint4 v;
+                    uint8_t b[16];
+                } u;
+                u.v = *reinterpret_cast<const uint4*>(row + (q - cb) * kBitsOf<D> / 8);
+#pragma unroll
+                for (int e = 0; e < kPerChunk; ++e) {
+                    const uint64_t c = q + e;
+                    if (c >= ce)
+                        break;
+                    if (mask[c] == 0)
+                        continue;
+                    const float ic = iw[c];
+                    if (ic == 0.0F)
+                        continue;
+                    acc.step(c, rd<D>(u.b, static_cast<uint64_t>(e)), lw[c], ic, clip, kp.enabled);
+                }
+            }
+        }
+        __syncthreads(); // every thread is done with this tile's buffer
+        if (j + 2 < ntiles)
+            issue(j + 2);
+    }
+    if (active)
+        acc.finish(d, t, kp, good_prefix, s_det, s_keep_d, s_keep_f, row_std, kspec_pos, kspec_neg,
+                   kspec_whole);
+}
+
+// One (chunk, channel) sequence of the column scan
+// (lib/cpu/rfi_cpu_measure.cpp:305-446): the block min/max of unmeasured
+// cells, zdot sums and Kadane-along-time states. The per-(window, channel)
+// constants are reloaded only when the window changes.
+struct ScanColAcc {
+    const Dims* d;
+    const float* loc;
+    const float* inv;
+    const float* clip_mean;
+    const float* clip_inv_std;
+    const double* s_keep_d;
+    uint64_t c;
+    float clip;
+    int zdot, kchan;
+    uint64_t w = 0, wend = 0; // current window and its end (0: none yet)
+    float l = 0.0F, iv = 0.0F, cm = 0.0F, ci = 0.0F;
+    float cmin = FLT_MAX, cmax = -FLT_MAX;
+    ZdotSums zs{0, 0, 0, 0, 0};
+    KadaneState kpos = KadaneState::make(), kneg = KadaneState::make();
+    __device__ __forceinline__ void step(float x, uint64_t t) {
+        if (t >= wend) {
+            w                = window_of(t, d->window, d->nwin);
+            wend             = window_end(w, *d);
+            const uint64_t o = w * d->nchans + c;
+            l                = loc[o];
+            iv               = inv[o];
+            if (kchan) {
+                cm = clip_mean[o];
+                ci = clip_inv_std[o];
+            }
+        }
+        float z = 0.0F;
+        if (iv == 0.0F) {
+            cmin = smin(cmin, x);
+            cmax = smax(cmax, x);
+        } else {
+            z = (x - l) * iv;
+        }
+        const bool outlier = fabsf(z) > clip;
+        if (zdot && !outlier && iv != 0.0F) {
+            const double sk = s_keep_d[t];
+            zs.n += 1.0;
+            zs.sz += z;
+            zs.ss += sk;
+            zs.sss += sk * sk;
+            zs.szs += z * sk;
+        }
+        if (kchan) {
+            const double u = outlier ? 0.0 : static_cast<double>((z - cm) * ci);
+            kpos.append(static_cast<int64_t>(t), u);
+            kneg.append(static_cast<int64_t>(t), -u);
+        }
+    }
+    __device__ __forceinline__ void store(uint64_t k, float* cmin_out, float* cmax_out,
+                                          ZdotSums* zs_out, KadaneState* kp_out,
+                                          KadaneState* kn_out) const {
+        const uint64_t o = k * d->nchans + c;
+        cmin_out[o]      = cmin;
+        cmax_out[o]      = cmax;
+        if (zdot)
+            zs_out[o] = zs;
+        if (kchan) {
+            kp_out[o] = kpos;
+            kn_out[o] = kneg;
+        }
+    }
+};
 
 template <int D>
 __global__ void k_scan_cols(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
@@ -420,10 +789,7 @@ __global__ void k_scan_cols(Dims d, const uint8_t* __restrict__ raw, const float
     const uint64_t k = blockIdx.y;
     if (c >= d.nchans)
         return;
-    const uint64_t n = d.nchans;
-    float cmin = FLT_MAX, cmax = -FLT_MAX;
-    ZdotSums zs{0, 0, 0, 0, 0};
-    KadaneState kpos = KadaneState::make(), kneg = KadaneState::make();
+    ScanColAcc acc{&d, loc, inv, clip_mean, clip_inv_std, s_keep_d, c, clip, zdot, kchan};
     if (mask[c] != 0) {
         const uint64_t t0 = k * d.chunk;
         const uint64_t t1 = (t0 + d.chunk < d.nsamps) ? t0 + d.chunk : d.nsamps;
@@ -435,47 +801,52 @@ __global__ void k_scan_cols(Dims d, const uint8_t* __restrict__ raw, const float
                 xs[q] = tb + q < t1 ? rd<D>(raw + (tb + q) * d.row_bytes, c) : 0.0F;
 #pragma unroll
             for (int q = 0; q < kBlock; ++q) {
-                const uint64_t t = tb + q;
-                if (t >= t1)
+                if (tb + q >= t1)
                     break;
-                const uint64_t w = window_of(t, d.window, d.nwin);
-                const uint64_t o = w * n + c;
-                const float x    = xs[q];
-                const float iv   = inv[o];
-                float z          = 0.0F;
-                if (iv == 0.0F) {
-                    cmin = smin(cmin, x);
-                    cmax = smax(cmax, x);
-                } else {
-                    z = (x - loc[o]) * iv;
-                }
-                const bool outlier = fabsf(z) > clip;
-                if (zdot && !outlier && iv != 0.0F) {
-                    const double sk = s_keep_d[t];
-                    zs.n += 1.0;
-                    zs.sz += z;
-                    zs.ss += sk;
-                    zs.sss += sk * sk;
-                    zs.szs += z * sk;
-                }
-                if (kchan) {
-                    const double u =
-                        outlier ? 0.0 : static_cast<double>((z - clip_mean[o]) * clip_inv_std[o]);
-                    kpos.append(static_cast<int64_t>(t), u);
-                    kneg.append(static_cast<int64_t>(t), -u);
-                }
+                acc.step(xs[q], tb + q);
             }
         }
     }
-    const uint64_t o = k * n + c;
-    cmin_out[o]      = cmin;
-    cmax_out[o]      = cmax;
-    if (zdot)
-        zs_out[o] = zs;
-    if (kchan) {
-        kp_out[o] = kpos;
-        kn_out[o] = kneg;
+    acc.store(k, cmin_out, cmax_out, zs_out, kp_out, kn_out);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kStageChans)
+    k_scan_cols_staged(Dims d, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
+                       const float* __restrict__ inv, const uint8_t* __restrict__ mask, float clip,
+                       const double* __restrict__ s_keep_d, int zdot, int kchan,
+                       const float* __restrict__ clip_mean, const float* __restrict__ clip_inv_std,
+                       float* __restrict__ cmin_out, float* __restrict__ cmax_out,
+                       ZdotSums* __restrict__ zs_out, KadaneState* __restrict__ kp_out,
+                       KadaneState* __restrict__ kn_out, int seg_bytes, int rows) {
+    extern __shared__ __align__(16) uint8_t stage_buf[];
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kStageChans;
+    const uint64_t c  = c0 + threadIdx.x;
+    const uint64_t k  = blockIdx.y;
+    const bool in     = c < d.nchans;
+    const bool active = in && mask[c] != 0;
+    ScanColAcc acc{&d, loc, inv, clip_mean, clip_inv_std, s_keep_d, c, clip, zdot, kchan};
+    const uint64_t t0   = k * d.chunk;
+    const uint64_t t1   = (t0 + d.chunk < d.nsamps) ? t0 + d.chunk : d.nsamps;
+    const uint64_t off  = c0 * kBitsOf<D> / 8;
+    const uint64_t left = d.row_bytes - off;
+    const int copy      = static_cast<int>(left < static_cast<uint64_t>(seg_bytes) ? left : seg_bytes);
+    stage::Stager st(stage_buf, raw + off, d.row_bytes, seg_bytes, copy, rows, t0, t1);
+    st.start();
+    for (int kb = 0; kb < st.nblk; ++kb) {
+        st.wait(kb);
+        const uint8_t* buf = st.buf(kb);
+        const int nr       = st.rows_of(kb);
+        const uint64_t tb  = st.t0(kb);
+        if (active) {
+#pragma unroll 4
+            for (int r = 0; r < nr; ++r)
+                acc.step(rd<D>(buf + r * seg_bytes, threadIdx.x), tb + r);
+        }
+        st.release(kb);
     }
+    if (in)
+        acc.store(k, cmin_out, cmax_out, zs_out, kp_out, kn_out);
 }
 
 // Per channel, in chunk order: the block min/max of unmeasured cells, the
@@ -530,7 +901,7 @@ __device__ __forceinline__ float level_of(const ApplyParams& p, float loc, float
 // samples and cell states are staged in shared memory so neighbour draws
 // read them without touching HBM again. Masked cells are not written: the
 // normalized output zeroes them, so their fill values are never observed.
-template <int D>
+template <int D, int V>
 __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restrict__ raw,
                                   const float* __restrict__ loc, const float* __restrict__ scale,
                                   const float* __restrict__ inv, const uint8_t* __restrict__ mask,
@@ -571,36 +942,75 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
         return i >= s.start && i <= s.end;
     };
 
-    for (uint64_t c = threadIdx.x; c < n; c += blockDim.x) {
-        const float x = rd<D>(in, c);
-        uint8_t st;
-        float v = 0.0F;
-        if (mask[c] == 0) {
-            st = kMasked;
-        } else if (iw[c] == 0.0F) {
-            st = kUnmeasured;
-            out[c] = x;
-        } else {
-            const float z = (x - lw[c]) * iw[c];
-            if (p.narrow_active && fabsf(z) > p.clip) {
-                st = kNarrow;
-            } else if (p.kspec && (span_has(ksp, c) || span_has(ksn, c))) {
-                st = kKadaneSpectrum;
-            } else if (p.kchan && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
-                st = kKadaneChannel;
+    // V consecutive channels per thread (V = 4: 16-byte loads of the
+    // per-window constants and stores of the row, when nchans % 4 == 0)
+    for (uint64_t cb = threadIdx.x * V; cb < n; cb += blockDim.x * V) {
+        float xs[V], ls[V], ss[V], is[V], outv[V];
+        uint8_t ms[V];
+        if constexpr (V == 4) {
+            const float4 l4 = *reinterpret_cast<const float4*>(lw + cb);
+            const float4 s4 = *reinterpret_cast<const float4*>(sw + cb);
+            const float4 i4 = *reinterpret_cast<const float4*>(iw + cb);
+            const uchar4 m4 = *reinterpret_cast<const uchar4*>(mask + cb);
+            ls[0] = l4.x; ls[1] = l4.y; ls[2] = l4.z; ls[3] = l4.w;
+            ss[0] = s4.x; ss[1] = s4.y; ss[2] = s4.z; ss[3] = s4.w;
+            is[0] = i4.x; is[1] = i4.y; is[2] = i4.z; is[3] = i4.w;
+            ms[0] = m4.x; ms[1] = m4.y; ms[2] = m4.z; ms[3] = m4.w;
+            if constexpr (D == FROST_UINT8) {
+                const uchar4 x4 = *reinterpret_cast<const uchar4*>(in + cb);
+                xs[0] = static_cast<float>(x4.x); xs[1] = static_cast<float>(x4.y);
+                xs[2] = static_cast<float>(x4.z); xs[3] = static_cast<float>(x4.w);
             } else {
-                st = kClean;
-                float term = 0.0F;
-                if (p.zero_dm == FROST_ZERO_DM_SUBTRACT)
-                    term = sk;
-                else if (p.zero_dm == FROST_ZERO_DM_ZDOT)
-                    term = (zdot_a[c] * sk) + zdot_b[c];
-                v      = z - term;
-                out[c] = p.transform ? level_of(p, lw[c], sw[c], v) : x;
+#pragma unroll
+                for (int e = 0; e < V; ++e)
+                    xs[e] = rd<D>(in, cb + e);
             }
+        } else {
+            ls[0] = lw[cb];
+            ss[0] = sw[cb];
+            is[0] = iw[cb];
+            ms[0] = mask[cb];
+            xs[0] = rd<D>(in, cb);
         }
-        state[c] = st;
-        sv[c]    = v;
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const uint64_t c = cb + e;
+            const float x    = xs[e];
+            uint8_t st;
+            float v = 0.0F;
+            outv[e] = 0.0F;
+            if (ms[e] == 0) {
+                st = kMasked;
+            } else if (is[e] == 0.0F) {
+                st      = kUnmeasured;
+                outv[e] = x;
+            } else {
+                const float z = (x - ls[e]) * is[e];
+                if (p.narrow_active && fabsf(z) > p.clip) {
+                    st = kNarrow;
+                } else if (p.kspec && (span_has(ksp, c) || span_has(ksn, c))) {
+                    st = kKadaneSpectrum;
+                } else if (p.kchan && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
+                    st = kKadaneChannel;
+                } else {
+                    st = kClean;
+                    float term = 0.0F;
+                    if (p.zero_dm == FROST_ZERO_DM_SUBTRACT)
+                        term = sk;
+                    else if (p.zero_dm == FROST_ZERO_DM_ZDOT)
+                        term = (zdot_a[c] * sk) + zdot_b[c];
+                    v       = z - term;
+                    outv[e] = p.transform ? level_of(p, ls[e], ss[e], v) : x;
+                }
+            }
+            state[c] = st;
+            sv[c]    = v;
+        }
+        // masked and flagged cells are (re)written below or never read
+        if constexpr (V == 4)
+            *reinterpret_cast<float4*>(out + cb) = make_float4(outv[0], outv[1], outv[2], outv[3]);
+        else
+            out[cb] = outv[0];
     }
     __syncthreads();
 
@@ -749,14 +1159,55 @@ __global__ void k_unpack(Dims d, const uint8_t* __restrict__ raw, float* __restr
     }
 }
 
-__global__ void k_welford(Dims d, const float* __restrict__ work, float* __restrict__ loc,
-                          float* __restrict__ scale) {
+// a / n for a count n >= 1 with y = RN(1/n) precomputed, correctly
+// rounded (round to nearest even) with one fused multiply-add correction
+// (Markstein's theorem: P. Markstein, "Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Develop. 34, 1990;
+// Muller et al., Handbook of Floating-Point Arithmetic, ch. 4). q0 = a*y is
+// within 1.5 ulp of a/n, so r = a - q0*n is exact (a multiple of ulp(q0)
+// below 2n ulps); q0 + r*y then differs from a/n by at most ~2^-52 ulp, far
+// less than the distance ulp/(2n) that separates a quotient by an integer
+// n < 2^40 from a rounding midpoint (a/n is never exactly a midpoint), so
+// it rounds as a/n does. Zero and tiny |a| (where r could lose bits) take
+// the plain division.
+__device__ __forceinline__ double div_by_count(double a, double n, double y) {
+    if (!(fabs(a) > 0x1p-900))
+        return a / n;
+    const double q0 = a * y;
+    const double r  = fma(-q0, n, a);
+    return fma(r, y, q0);
+}
+
+// One (window, channel) Welford sequence of the re-measure after a
+// transform (lib/cpu/rfi_cpu.cpp:219-238).
+struct WelfordAcc {
+    double mean = 0.0, var = 0.0;
+    uint64_t b;
+    const double* recip; // recip[n] = RN(1/n), or null for the plain division
+    __device__ __forceinline__ void step(float xf, uint64_t t) {
+        const uint64_t n = t - b + 1;
+        if (recip != nullptr)
+            step_by(xf, static_cast<double>(n), recip[n]);
+        else
+            step_by(xf, static_cast<double>(n), 0.0);
+    }
+    /** The update for the n-th sample given y = RN(1/n) (y = 0: divide). */
+    __device__ __forceinline__ void step_by(float xf, double n, double y) {
+        const double x     = xf;
+        const double delta = x - mean;
+        mean += y != 0.0 ? div_by_count(delta, n, y) : delta / n;
+        var += delta * (x - mean);
+    }
+};
+
+__global__ void k_welford(Dims d, const float* __restrict__ work, const double* __restrict__ recip,
+                          float* __restrict__ loc, float* __restrict__ scale) {
     const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     const uint64_t w = blockIdx.y;
     if (c >= d.nchans)
         return;
     const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
-    double mean = 0.0, var = 0.0;
+    WelfordAcc acc{0.0, 0.0, b, recip};
     for (uint64_t tb = b; tb < e; tb += kBlock) {
         float xs[kBlock];
 #pragma unroll
@@ -764,46 +1215,114 @@ __global__ void k_welford(Dims d, const float* __restrict__ work, float* __restr
             xs[q] = tb + q < e ? work[(tb + q) * d.nchans + c] : 0.0F;
 #pragma unroll
         for (int q = 0; q < kBlock; ++q) {
-            const uint64_t t = tb + q;
-            if (t >= e)
+            if (tb + q >= e)
                 break;
-            const double x     = xs[q];
-            const double delta = x - mean;
-            mean += delta / static_cast<double>(t - b + 1);
-            var += delta * (x - mean);
+            acc.step(xs[q], tb + q);
         }
     }
-    loc[w * d.nchans + c]   = static_cast<float>(mean);
-    scale[w * d.nchans + c] = e > b ? static_cast<float>(sqrt(var / static_cast<double>(e - b))) : 0.0F;
+    loc[w * d.nchans + c]   = static_cast<float>(acc.mean);
+    scale[w * d.nchans + c] = e > b ? static_cast<float>(sqrt(acc.var / static_cast<double>(e - b))) : 0.0F;
+}
+
+__global__ void __launch_bounds__(kStageChans)
+    k_welford_staged(Dims d, const float* __restrict__ work, const double* __restrict__ recip,
+                     float* __restrict__ loc, float* __restrict__ scale, int seg_bytes, int rows) {
+    extern __shared__ __align__(16) uint8_t stage_buf[];
+    __shared__ double ys[2][256]; // reciprocal counts of each stage's rows (rows <= 256)
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kStageChans;
+    const uint64_t c  = c0 + threadIdx.x;
+    const uint64_t w  = blockIdx.y;
+    const bool in     = c < d.nchans;
+    const uint64_t b = window_begin(w, d.window), e = window_end(w, d);
+    WelfordAcc acc{0.0, 0.0, b, recip};
+    const uint64_t pitch = d.nchans * sizeof(float);
+    const uint64_t left  = pitch - c0 * sizeof(float);
+    const int copy       = static_cast<int>(left < static_cast<uint64_t>(seg_bytes) ? left : seg_bytes);
+    const int stride     = seg_bytes / static_cast<int>(sizeof(float));
+    stage::Stager st(stage_buf, reinterpret_cast<const uint8_t*>(work + c0), pitch, seg_bytes, copy,
+                     rows, b, e);
+    // The reciprocals of a stage's counts are read into shared memory with
+    // the stage, so no load sits on the sequential update chain.
+    auto load_recip = [&](int k) {
+        if (k < st.nblk && static_cast<int>(threadIdx.x) < st.rows_of(k)) {
+            const uint64_t n = st.t0(k) - b + 1 + threadIdx.x;
+            ys[k & 1][threadIdx.x] = recip != nullptr ? recip[n] : 0.0;
+        }
+    };
+    load_recip(0);
+    load_recip(1);
+    st.start();
+    for (int k = 0; k < st.nblk; ++k) {
+        st.wait(k);
+        const float* buf  = reinterpret_cast<const float*>(st.buf(k));
+        const int nr      = st.rows_of(k);
+        double nd         = static_cast<double>(st.t0(k) - b); // exact below 2^53
+        if (in) {
+#pragma unroll 8
+            for (int r = 0; r < nr; ++r) {
+                nd += 1.0;
+                acc.step_by(buf[r * stride + threadIdx.x], nd, ys[k & 1][r]);
+            }
+        }
+        st.release(k);
+        load_recip(k + 2);
+    }
+    if (in) {
+        loc[w * d.nchans + c] = static_cast<float>(acc.mean);
+        scale[w * d.nchans + c] =
+            e > b ? static_cast<float>(sqrt(acc.var / static_cast<double>(e - b))) : 0.0F;
+    }
 }
 
 constexpr int kTile = 32;
+
+// Normalise + transpose (lib/cpu/rfi_cpu.cpp:242-255): out[c][t] =
+// (work[t][c] - loc) * (scale > 0 ? 1 / scale : 1) per (window, channel),
+// masked channels zero. A block covers 32 channels and kNormSpan samples
+// in 32 x 32 tiles through shared memory; each thread keeps its channel's
+// window constants and reloads them only when its rows cross into the next
+// window.
+constexpr int kNormSpan = 256;
 
 __global__ void k_normalize(Dims d, const float* __restrict__ work, const float* __restrict__ loc,
                             const float* __restrict__ scale, const uint8_t* __restrict__ mask,
                             int flip, uint64_t capacity, float* __restrict__ out) {
     __shared__ float tile[kTile][kTile + 1];
-    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kTile;
-    const uint64_t c0 = static_cast<uint64_t>(blockIdx.y) * kTile;
     const uint64_t n  = d.nchans;
-    // Load [t][c] tile, already normalised.
-    for (int k = threadIdx.y; k < kTile; k += blockDim.y) {
-        const uint64_t t = t0 + k, c = c0 + threadIdx.x;
-        float v          = 0.0F;
-        if (t < d.nsamps && c < n && mask[c] != 0) {
-            const uint64_t i = window_of(t, d.window, d.nwin) * n + c;
-            const float s    = scale[i] > 0.0F ? 1.0F / scale[i] : 1.0F;
-            v                = (work[t * n + c] - loc[i]) * s;
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.y) * kTile;
+    const uint64_t c  = c0 + threadIdx.x;
+    const bool on     = c < n && mask[c] != 0;
+    uint64_t wend     = 0;
+    float l = 0.0F, is = 1.0F;
+    const uint64_t span0 = static_cast<uint64_t>(blockIdx.x) * kNormSpan;
+    for (uint64_t t0 = span0; t0 < span0 + kNormSpan && t0 < capacity; t0 += kTile) {
+        for (int k = threadIdx.y; k < kTile; k += blockDim.y) {
+            const uint64_t t = t0 + k;
+            float v          = 0.0F;
+            if (t < d.nsamps && on) {
+                if (t >= wend) {
+                    const uint64_t w = window_of(t, d.window, d.nwin);
+                    wend             = window_end(w, d);
+                    l                = loc[w * n + c];
+                    const float sc   = scale[w * n + c];
+                    is               = sc > 0.0F ? 1.0F / sc : 1.0F;
+                }
+                v = (work[t * n + c] - l) * is;
+            }
+            tile[k][threadIdx.x] = v;
         }
-        tile[k][threadIdx.x] = v;
-    }
-    __syncthreads();
-    for (int k = threadIdx.y; k < kTile; k += blockDim.y) {
-        const uint64_t c = c0 + k, t = t0 + threadIdx.x;
-        if (c < n && t < capacity) {
-            const uint64_t dst     = flip ? n - 1 - c : c;
-            out[dst * capacity + t] = tile[threadIdx.x][k];
+        __syncthreads();
+        const uint64_t t = t0 + threadIdx.x;
+        if (t < capacity) {
+            for (int k = threadIdx.y; k < kTile; k += blockDim.y) {
+                const uint64_t cc = c0 + k;
+                if (cc < n) {
+                    const uint64_t dst      = flip ? n - 1 - cc : cc;
+                    out[dst * capacity + t] = tile[threadIdx.x][k];
+                }
+            }
         }
+        __syncthreads();
     }
 }
 
@@ -868,6 +1387,12 @@ uint64_t launch_counter() { return g_launches.load(std::memory_order_relaxed); }
 
 // ---- launchers ----------------------------------------------------------------
 
+static void set_smem(const void* fn, size_t bytes) {
+    if (bytes > 48 * 1024)
+        FB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(bytes)));
+}
+
 void launch_check_finite(const uint8_t* raw, uint64_t nwords, unsigned long long* first_bad,
                          cudaStream_t s) {
     if (nwords == 0)
@@ -885,15 +1410,54 @@ void launch_sample_rows(const Dims& d, const uint8_t* raw, float* samples, cudaS
 
 void launch_bandpass(const Dims& d, const float* samples, float* loc, float* scale, float* inv,
                      uint32_t* unmeasured, cudaStream_t s) {
-    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
-    k_bandpass<<<grid, 64, 0, s>>>(d, samples, loc, scale, inv, unmeasured);
+    const uint64_t pitch = d.nchans * sizeof(float);
+    if (pitch % 16 != 0 || reinterpret_cast<uintptr_t>(samples) % 16 != 0) {
+        const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
+        k_bandpass<<<grid, 64, 0, s>>>(d, samples, loc, scale, inv, unmeasured);
+    } else {
+        const int seg  = static_cast<int>(std::min<uint64_t>(kBandChans * sizeof(float), pitch));
+        const int rows = std::max(8, 16384 / seg);
+        const dim3 grid(grid1(d.nchans, kBandChans), static_cast<unsigned>(d.nwin));
+        k_bandpass_staged<<<grid, kBandChans, 2 * static_cast<size_t>(seg) * rows, s>>>(
+            d, samples, loc, scale, inv, unmeasured, seg, rows);
+    }
     FB_COUNT_LAUNCH();
+}
+
+// Staging geometry of a kStageChans-channel column segment: bytes per row
+// and rows per stage (about kStageBytes per buffer), or seg_bytes = 0 when
+// the layout cannot be staged with 16-byte copies.
+constexpr int kStageBytes = 16 * 1024;
+
+struct StageGeom {
+    int seg_bytes = 0, rows = 0;
+    size_t smem() const { return 2 * static_cast<size_t>(seg_bytes) * rows; }
+};
+
+bool aligned16(const void* p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; }
+
+StageGeom stage_geom(const void* base, uint64_t row_bytes, int bits) {
+    StageGeom g;
+    const uint64_t full = static_cast<uint64_t>(kStageChans) * bits / 8;
+    if (!aligned16(base) || row_bytes % 16 != 0 || full % 16 != 0)
+        return g;
+    // every segment starts on a 16-byte boundary; the last may be shorter
+    g.seg_bytes = static_cast<int>(std::min<uint64_t>(full, row_bytes));
+    g.rows      = std::max(8, std::min(256, kStageBytes / g.seg_bytes));
+    return g;
 }
 
 void launch_moments(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
                     const uint8_t* static_mask, float clip, MomentSums* out, cudaStream_t s) {
-    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
-    FB_DISPATCH(d.dtype, k_moments<D><<<grid, 64, 0, s>>>(d, raw, loc, inv, static_mask, clip, out));
+    const StageGeom g = stage_geom(raw, d.row_bytes, bits_of(d.dtype));
+    if (g.seg_bytes == 0) {
+        const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
+        FB_DISPATCH(d.dtype, k_moments<D><<<grid, 64, 0, s>>>(d, raw, loc, inv, static_mask, clip, out));
+    } else {
+        const dim3 grid(grid1(d.nchans, kStageChans), static_cast<unsigned>(d.nwin));
+        FB_DISPATCH(d.dtype, k_moments_staged<D><<<grid, kStageChans, g.smem(), s>>>(
+                                 d, raw, loc, inv, static_mask, clip, out, g.seg_bytes, g.rows));
+    }
     FB_COUNT_LAUNCH();
 }
 
@@ -903,9 +1467,19 @@ void launch_scan_rows(const Dims& d, const uint8_t* raw, const float* loc, const
                       float* row_std, Span32* kspec_pos, Span32* kspec_neg, uint8_t* kspec_whole,
                       cudaStream_t s) {
     const unsigned grid = grid1(d.nsamps, kScanRows);
-    FB_DISPATCH(d.dtype, k_scan_rows<D><<<grid, kScanRows, 0, s>>>(
-                             d, raw, loc, inv, mask, clip, kp, good_prefix, s_det, s_keep_d,
-                             s_keep_f, row_std, kspec_pos, kspec_neg, kspec_whole));
+    if (d.row_bytes % 16 != 0 || reinterpret_cast<uintptr_t>(raw) % 16 != 0) {
+        FB_DISPATCH(d.dtype, k_scan_rows<D><<<grid, kScanRows, 0, s>>>(
+                                 d, raw, loc, inv, mask, clip, kp, good_prefix, s_det, s_keep_d,
+                                 s_keep_f, row_std, kspec_pos, kspec_neg, kspec_whole));
+    } else {
+        const size_t smem = 2 * static_cast<size_t>(kScanRows) * kRowTileStride;
+        FB_DISPATCH(d.dtype, {
+            set_smem(reinterpret_cast<const void*>(&k_scan_rows_staged<D>), smem);
+            k_scan_rows_staged<D><<<grid, kScanRows, smem, s>>>(
+                d, raw, loc, inv, mask, clip, kp, good_prefix, s_det, s_keep_d, s_keep_f, row_std,
+                kspec_pos, kspec_neg, kspec_whole);
+        });
+    }
     FB_COUNT_LAUNCH();
 }
 
@@ -915,11 +1489,20 @@ void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const
                       float* chunk_max, ZdotSums* chunk_zdot, KadaneState* chunk_kpos,
                       KadaneState* chunk_kneg, float* lo, float* hi, ZdotSums* zdot_sum,
                       Run* kpos_best, Run* kneg_best, cudaStream_t s) {
-    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nchunks));
-    FB_DISPATCH(d.dtype, k_scan_cols<D><<<grid, 64, 0, s>>>(
-                             d, raw, loc, inv, mask, clip, s_keep_d, zdot, kchan, clip_mean,
-                             clip_inv_std, chunk_min, chunk_max, chunk_zdot, chunk_kpos,
-                             chunk_kneg));
+    const StageGeom g = stage_geom(raw, d.row_bytes, bits_of(d.dtype));
+    if (g.seg_bytes == 0) {
+        const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nchunks));
+        FB_DISPATCH(d.dtype, k_scan_cols<D><<<grid, 64, 0, s>>>(
+                                 d, raw, loc, inv, mask, clip, s_keep_d, zdot, kchan, clip_mean,
+                                 clip_inv_std, chunk_min, chunk_max, chunk_zdot, chunk_kpos,
+                                 chunk_kneg));
+    } else {
+        const dim3 grid(grid1(d.nchans, kStageChans), static_cast<unsigned>(d.nchunks));
+        FB_DISPATCH(d.dtype, k_scan_cols_staged<D><<<grid, kStageChans, g.smem(), s>>>(
+                                 d, raw, loc, inv, mask, clip, s_keep_d, zdot, kchan, clip_mean,
+                                 clip_inv_std, chunk_min, chunk_max, chunk_zdot, chunk_kpos,
+                                 chunk_kneg, g.seg_bytes, g.rows));
+    }
     FB_COUNT_LAUNCH();
     k_combine_chunks<<<grid1(d.nchans, 128), 128, 0, s>>>(d, zdot, kchan, chunk_min, chunk_max,
                                                           chunk_zdot, chunk_kpos, chunk_kneg, lo,
@@ -927,11 +1510,6 @@ void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const
     FB_COUNT_LAUNCH();
 }
 
-static void set_smem(const void* fn, size_t bytes) {
-    if (bytes > 48 * 1024)
-        FB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(bytes)));
-}
 
 void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* raw,
                             const float* loc, const float* scale, const float* inv,
@@ -943,11 +1521,21 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
     const size_t smem = d.nchans * (sizeof(float) + 1);
     if (d.nsamps == 0)
         return;
+    // 4-channel vectors need nchans % 4 == 0 and, for the byte loads of the
+    // raw row, a 4-byte aligned block
+    const bool vec = d.nchans % 4 == 0 && reinterpret_cast<uintptr_t>(raw) % 4 == 0;
     FB_DISPATCH(d.dtype, {
-        set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D>), smem);
-        k_apply_unflagged<D><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
-            d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
-            kchan_neg, s_keep_f, zdot_a, zdot_b, work, counters);
+        if (vec) {
+            set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 4>), smem);
+            k_apply_unflagged<D, 4><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
+                d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
+                kchan_neg, s_keep_f, zdot_a, zdot_b, work, counters);
+        } else {
+            set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 1>), smem);
+            k_apply_unflagged<D, 1><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
+                d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
+                kchan_neg, s_keep_f, zdot_a, zdot_b, work, counters);
+        }
     });
     FB_COUNT_LAUNCH();
 }
@@ -974,15 +1562,25 @@ void launch_unpack(const Dims& d, const uint8_t* raw, float* work, cudaStream_t 
     FB_COUNT_LAUNCH();
 }
 
-void launch_welford(const Dims& d, const float* work, float* loc, float* scale, cudaStream_t s) {
-    const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
-    k_welford<<<grid, 64, 0, s>>>(d, work, loc, scale);
+void launch_welford(const Dims& d, const float* work, const double* recip, float* loc, float* scale,
+                    cudaStream_t s) {
+    const StageGeom g = stage_geom(work, d.nchans * sizeof(float), 32);
+    if (g.seg_bytes == 0) {
+        const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
+        k_welford<<<grid, 64, 0, s>>>(d, work, recip, loc, scale);
+    } else {
+        const dim3 grid(grid1(d.nchans, kStageChans), static_cast<unsigned>(d.nwin));
+        // a stage's reciprocals are loaded one per thread
+        const int rows = std::min(g.rows, kStageChans);
+        k_welford_staged<<<grid, kStageChans, 2 * static_cast<size_t>(g.seg_bytes) * rows, s>>>(
+            d, work, recip, loc, scale, g.seg_bytes, rows);
+    }
     FB_COUNT_LAUNCH();
 }
 
 void launch_normalize(const Dims& d, const float* work, const float* loc, const float* scale,
                       const uint8_t* mask, int flip, uint64_t capacity, float* out, cudaStream_t s) {
-    const dim3 grid(grid1(capacity, kTile), grid1(d.nchans, kTile));
+    const dim3 grid(grid1(capacity, kNormSpan), grid1(d.nchans, kTile));
     k_normalize<<<grid, dim3(kTile, 8), 0, s>>>(d, work, loc, scale, mask, flip, capacity, out);
     FB_COUNT_LAUNCH();
 }

@@ -111,7 +111,12 @@ void launch_apply_flagged(const Dims& d, const ApplyParams& p, const uint64_t* f
 void launch_unpack(const Dims& d, const uint8_t* raw, float* work, cudaStream_t s);
 
 // Per (window, channel) Welford mean/rms of work rows in that window.
-void launch_welford(const Dims& d, const float* work, float* loc, float* scale, cudaStream_t s);
+/** Per (window, channel) Welford mean / std of the cleaned float rows.
+ * `recip[n]` = RN(1/n) for n up to the longest window lets the update
+ * divide with one correction step instead of a full division (same bits);
+ * null uses the plain division. */
+void launch_welford(const Dims& d, const float* work, const double* recip, float* loc, float* scale,
+                    cudaStream_t s);
 
 // out[dst][t] = (work[t][c] - loc) / scale for t < nsamps and unmasked c;
 // zero elsewhere; dst = flip ? nchans-1-c : c; out has `capacity` columns.

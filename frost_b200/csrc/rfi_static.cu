@@ -164,6 +164,11 @@ void normalize_static(const frost_block_layout& layout, float baseline_length, c
     const uint64_t row_bytes = n * static_cast<uint64_t>(bits_of(layout.dtype)) / 8;
     if (block == nullptr || out == nullptr)
         invalid("normalize_static: null block or output");
+    // samples wider than a byte and the float output are read and written
+    // as whole words: a misaligned pointer would fault the kernels
+    const uintptr_t word = bits_of(layout.dtype) > 8 ? static_cast<uintptr_t>(bits_of(layout.dtype) / 8) : 1;
+    if (reinterpret_cast<uintptr_t>(block) % word != 0 || reinterpret_cast<uintptr_t>(out) % 4 != 0)
+        invalid("normalize_static: block and output must be aligned to their element size");
     if (block_bytes % row_bytes != 0 || block_bytes / row_bytes > layout.max_nsamps)
         invalid("normalize_static: invalid block size");
     const uint64_t capacity = block_bytes / row_bytes;

@@ -1,21 +1,24 @@
 // Boxcar/trapezoid matched filter, exact noise and peak finding on sm_100a.
 //
-// One CTA per searched (plane, DM) row walks the tile in 4096-sample chunks:
-// the chunk plus a halo of the widest boxcar (rounded to 128 columns) is
-// loaded with vector loads, prefix-summed (warp shuffles, then one offset
-// per warp) into shared memory, and every width's window sum is a
+// One CTA per searched (plane, DM) row walks the tile in 4096-sample chunks.
+// The chunk plus a halo of the widest boxcar (rounded to 256 columns) is
+// bulk-copied into shared memory one chunk ahead, prefix-summed (warp
+// shuffles, then one offset per warp), and every width's window sum is a
 // difference of two (four for the trapezoid) prefix values. In the steady
 // state (no cold prefix, no mask change in the chunk) a sample is above
 // threshold when its window sum exceeds thresh * sigma, precomputed per
-// width; each thread tests 4 consecutive samples per 16-byte shared load
-// and ORs the outcomes into one predicate, so a chunk in which nothing
-// fires (almost all of them) costs one block vote. A chunk that fires, and
-// the first chunks of a stream or after a mask change (cold prefix,
-// OR-mask variance), build per-width ballot bitmasks; one lane walks only
-// the set bits in time order, extending or closing the run carried from
-// the previous chunk (and tile, and gulp) and emitting each closed run's
-// peak. The DM-time rows are never re-read and the run state is the only
-// thing carried between calls.
+// width. Each thread covers groups of 4 consecutive samples: the group's
+// largest prefix value minus the least prefix value the group's windows
+// start from bounds all 4 window sums, so almost every (group, width) is
+// cleared by one shared load, a subtract and a compare; the rest take the
+// exact test, which also writes the per-width bit masks of the samples that
+// fired. A chunk where nothing fires costs one block vote. The first
+// chunks of a stream or after a mask change (cold prefix, OR-mask
+// variance) build the bit masks from the general S/N. One lane walks the
+// set bits of the widths that fired in time order, extending or closing
+// the run carried from the previous chunk (and tile, and gulp) and
+// emitting each closed run's peak. The DM-time rows are never re-read and
+// the run state is the only thing carried between calls.
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -148,6 +151,25 @@ template <> __device__ __forceinline__ float4 ld4s<__half>(const __half* p) {
     return make_float4(a.x, a.y, b.x, b.y);
 }
 
+// Eight consecutive staged samples (16-byte aligned) as float.
+template <class S> __device__ __forceinline__ void ld8s(const S* p, float (&x)[8]) {
+    if constexpr (sizeof(S) == 4) {
+        const float4 a = reinterpret_cast<const float4*>(p)[0];
+        const float4 b = reinterpret_cast<const float4*>(p)[1];
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+    } else {
+        const uint4 u       = *reinterpret_cast<const uint4*>(p);
+        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
+            x[2 * i]       = f.x;
+            x[2 * i + 1]   = f.y;
+        }
+    }
+}
+
 // `count` (shared or global) is the row's emitted total this call.
 __device__ void emit(const SearchParams& p, const SearchRow& row, const RunState& r,
                      uint32_t* count) {
@@ -248,21 +270,26 @@ __device__ void close_open_runs(const SearchParams& p, RunState* runs, int nruns
         }
 }
 
+// Words of the per-width bit masks [nw][kWords].
+__host__ __device__ constexpr int search_bits_words(int nw) { return nw * kWords; }
+
 template <class S>
 __global__ void __launch_bounds__(kThreads, 4)
     k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0) {
     // Dynamic shared memory: Ps, the chunk's prefix sums over columns
     // [c0 - halo, c0 + kChunk) after 4 floats of padding (Q = Ps + 4 + halo
-    // puts sample k of the chunk at Q[k], 16-byte aligned), then two staging
-    // buffers of the raw row segment, filled by bulk copies one chunk ahead.
+    // puts sample k of the chunk at Q[k], 16-byte aligned); gmin / gmax, the
+    // least and greatest of each aligned group of 4 prefix values; the
+    // per-width bit masks [nw][kWords]; two staging buffers of the raw row
+    // segment, filled by bulk copies one chunk ahead.
     extern __shared__ __align__(16) float Ps[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int abort_flag;
-    __shared__ uint32_t bits[kMaxWidths][kWords];
     __shared__ uint32_t any_bits[kWords];
     __shared__ RunState runs[kMaxWidths];
     __shared__ RowConst rc;
     __shared__ uint32_t local_count;
+    __shared__ uint32_t fired_w; // widths with a set bit in this chunk
     __shared__ float warp_tot[kThreads / 32];
 
     const int64_t g     = g0 + blockIdx.x;
@@ -292,9 +319,13 @@ __global__ void __launch_bounds__(kThreads, 4)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* Q       = Ps + 4 + halo;
     const S* src   = level + row.level_row * pitch + base;
-    const int seg_cols      = halo + kChunk;
+    const int seg_cols       = halo + kChunk;
     const uint32_t seg_bytes = static_cast<uint32_t>(seg_cols * sizeof(S));
-    S* const stage0 = reinterpret_cast<S*>(Ps + 4 + seg_cols + 4); // buffer b at stage0 + b * seg_cols
+    const int ngroups        = seg_cols / 4;
+    float* const gmin        = Ps + 4 + seg_cols + 4;
+    float* const gmax        = gmin + ngroups;
+    uint32_t* const bits     = reinterpret_cast<uint32_t*>(gmax + ngroups);
+    S* const stage0 = reinterpret_cast<S*>(bits + search_bits_words(nw)); // buffer b at stage0 + b * seg_cols
     const int nchunks = (p.n_valid + kChunk - 1) / kChunk;
     auto issue = [&](int ci) {
         bulk::mbar_expect(&bar[ci & 1], seg_bytes);
@@ -310,8 +341,8 @@ __global__ void __launch_bounds__(kThreads, 4)
     if (threadIdx.x == 0)
         for (int ci = 0; ci < min(2, nchunks); ++ci)
             issue(ci);
-    // 128-column segments (4 per lane): warp w scans a contiguous run of them
-    const int nseg  = (halo + kChunk) / 128;
+    // 256-column segments (8 per lane): warp w scans a contiguous run of them
+    const int nseg  = seg_cols / 256;
     const int spw   = (nseg + kThreads / 32 - 1) / (kThreads / 32);
     const int s_beg = warp * spw, s_end = min(s_beg + spw, nseg);
     const int jmin  = halo - wmax + 1; // earlier columns never enter a window
@@ -328,18 +359,18 @@ __global__ void __launch_bounds__(kThreads, 4)
         const S* seg = stage0 + (ci & 1) * seg_cols;
         float carry  = 0.0F;
         for (int sg = s_beg; sg < s_end; ++sg) {
-            const int j = sg * 128 + 4 * lane;
-            float4 x    = ld4s<S>(seg + j);
+            const int j = sg * 256 + 8 * lane;
+            float x[8];
+            ld8s<S>(seg + j, x);
             if (j < jmin) {
-                x.x = j < jmin ? 0.0F : x.x;
-                x.y = j + 1 < jmin ? 0.0F : x.y;
-                x.z = j + 2 < jmin ? 0.0F : x.z;
-                x.w = j + 3 < jmin ? 0.0F : x.w;
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    x[e] = j + e < jmin ? 0.0F : x[e];
             }
-            x.y += x.x;
-            x.z += x.y;
-            x.w += x.z;
-            float t = x.w;
+#pragma unroll
+            for (int e = 1; e < 8; ++e)
+                x[e] += x[e - 1];
+            float t = x[7];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const float u = __shfl_up_sync(0xFFFFFFFFU, t, o);
@@ -348,11 +379,12 @@ __global__ void __launch_bounds__(kThreads, 4)
             }
             const float before = __shfl_up_sync(0xFFFFFFFFU, t, 1);
             const float off    = carry + (lane > 0 ? before : 0.0F);
-            x.x += off;
-            x.y += off;
-            x.z += off;
-            x.w += off;
-            *reinterpret_cast<float4*>(Ps + 4 + j) = x;
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                x[e] += off;
+            float4* dst = reinterpret_cast<float4*>(Ps + 4 + j);
+            dst[0]      = make_float4(x[0], x[1], x[2], x[3]);
+            dst[1]      = make_float4(x[4], x[5], x[6], x[7]);
             carry += __shfl_sync(0xFFFFFFFFU, t, 31);
         }
         if (lane == 0)
@@ -361,18 +393,31 @@ __global__ void __launch_bounds__(kThreads, 4)
         // every thread has read this chunk's staging buffer: refill it
         if (threadIdx.x == 0 && ci + 2 < nchunks)
             issue(ci + 2);
-        if (warp > 0) {
+        // clear the bit masks (a steady chunk sets only the words of
+        // samples that fired)
+        for (int i = threadIdx.x; i < nw * kWords; i += kThreads)
+            bits[i] = 0U;
+        if (threadIdx.x == 0)
+            fired_w = 0U;
+        {
+            // add the preceding warps' totals; record each 4-group's range
             float woff = 0.0F;
             for (int w = 0; w < warp; ++w)
                 woff += warp_tot[w];
             for (int sg = s_beg; sg < s_end; ++sg) {
-                float4* v = reinterpret_cast<float4*>(Ps + 4 + sg * 128 + 4 * lane);
-                float4 x  = *v;
-                x.x += woff;
-                x.y += woff;
-                x.z += woff;
-                x.w += woff;
-                *v = x;
+                const int j = sg * 256 + 8 * lane;
+                float4* v   = reinterpret_cast<float4*>(Ps + 4 + j);
+                float4 a = v[0], b = v[1];
+                if (warp > 0) {
+                    a.x += woff; a.y += woff; a.z += woff; a.w += woff;
+                    b.x += woff; b.y += woff; b.z += woff; b.w += woff;
+                    v[0] = a;
+                    v[1] = b;
+                }
+                reinterpret_cast<float2*>(gmin)[j / 8] = make_float2(
+                    fminf(fminf(a.x, a.y), fminf(a.z, a.w)), fminf(fminf(b.x, b.y), fminf(b.z, b.w)));
+                reinterpret_cast<float2*>(gmax)[j / 8] = make_float2(
+                    fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)), fmaxf(fmaxf(b.x, b.y), fmaxf(b.z, b.w)));
             }
         }
         __syncthreads();
@@ -380,37 +425,57 @@ __global__ void __launch_bounds__(kThreads, 4)
         const bool fast = c0 + kChunk <= p.n_valid && (!p.skip_cold || p.tile_t0 + c0 >= warm) &&
                           (!p.or_active || p.tile_t0 + c0 - p.gulp_t0 >= warm);
         if (fast) {
-            // ---- steady state: the exact threshold test of every sample and
-            // width (the same float expression as wsum), 4 samples per vector
-            float4 qv[kPerThread / 4];
-#pragma unroll
-            for (int q = 0; q < kPerThread / 4; ++q)
-                qv[q] = *reinterpret_cast<const float4*>(Q + 4 * (threadIdx.x + q * kThreads));
+            // ---- steady state. Group gi = samples 4 gi .. 4 gi + 3. A window
+            // sum Q[k] - Q[k - W] of the group is at most gmax(group) minus
+            // gmin over the groups holding Q[4 gi - W .. 4 gi + 3 - W]
+            // (rounding is monotonic), so a (group, width) the bound clears
+            // cannot fire. The others take the exact test (the same float
+            // expression as wsum) and set the bits of the samples that fire.
+            // Trapezoids take the exact test throughout.
             bool up = false;
-            for (int wi = 0; wi < nw; ++wi) {
-                const int W   = rc.W[wi];
-                const int E   = rc.E[wi];
-                const float T = rc.thr[wi];
 #pragma unroll
-                for (int q = 0; q < kPerThread / 4; ++q) {
-                    const int k    = 4 * (threadIdx.x + q * kThreads);
-                    const float4 a = qv[q];
-                    const float4 b = ld4(Q, k - W);
-                    float s0, s1, s2, s3;
-                    if (E > 0) {
-                        const float4 c = ld4(Q, k - E);
-                        const float4 d = ld4(Q, k - W + E);
-                        s0 = trap_sum(a.x, b.x, c.x, d.x);
-                        s1 = trap_sum(a.y, b.y, c.y, d.y);
-                        s2 = trap_sum(a.z, b.z, c.z, d.z);
-                        s3 = trap_sum(a.w, b.w, c.w, d.w);
-                    } else {
-                        s0 = a.x - b.x;
-                        s1 = a.y - b.y;
-                        s2 = a.z - b.z;
-                        s3 = a.w - b.w;
+            for (int q = 0; q < kPerThread / 4; ++q) {
+                const int gi   = threadIdx.x + q * kThreads; // group in the chunk
+                const int k    = 4 * gi;
+                const float hi = gmax[gi + halo / 4];
+                for (int wi = 0; wi < nw; ++wi) {
+                    const int W   = rc.W[wi];
+                    const int E   = rc.E[wi];
+                    const float T = rc.thr[wi];
+                    bool maybe    = true;
+                    if (E == 0) {
+                        const int lo_g = (halo + k - W) >> 2; // group of Q[k - W]
+                        float lo       = gmin[lo_g];
+                        if ((W & 3) != 0)
+                            lo = fminf(lo, gmin[lo_g + 1]);
+                        maybe = hi - lo > T;
                     }
-                    up |= (s0 > T) | (s1 > T) | (s2 > T) | (s3 > T);
+                    if (maybe) {
+                        const float4 a = *reinterpret_cast<const float4*>(Q + k);
+                        const float4 b = ld4(Q, k - W);
+                        float s0, s1, s2, s3;
+                        if (E > 0) {
+                            const float4 c = ld4(Q, k - E);
+                            const float4 d = ld4(Q, k - W + E);
+                            s0 = trap_sum(a.x, b.x, c.x, d.x);
+                            s1 = trap_sum(a.y, b.y, c.y, d.y);
+                            s2 = trap_sum(a.z, b.z, c.z, d.z);
+                            s3 = trap_sum(a.w, b.w, c.w, d.w);
+                        } else {
+                            s0 = a.x - b.x;
+                            s1 = a.y - b.y;
+                            s2 = a.z - b.z;
+                            s3 = a.w - b.w;
+                        }
+                        const uint32_t nib = (s0 > T ? 1U : 0U) | (s1 > T ? 2U : 0U) |
+                                             (s2 > T ? 4U : 0U) | (s3 > T ? 8U : 0U);
+                        if (nib != 0U) {
+                            // samples 4 gi .. 4 gi + 3: word gi / 8, nibble gi % 8
+                            atomicOr(&bits[wi * kWords + (gi >> 3)], nib << ((gi & 7) * 4));
+                            atomicOr(&fired_w, 1U << wi);
+                            up = true;
+                        }
+                    }
                 }
             }
             if (!__syncthreads_or(up)) {
@@ -419,51 +484,61 @@ __global__ void __launch_bounds__(kThreads, 4)
                     close_open_runs(p, runs, nruns, row, &local_count);
                 continue; // Ps is rewritten only after every thread passed the barrier
             }
-        }
-
-        // ---- a chunk that fired (or is not steady): per-width bit masks
-        uint32_t any = 0;
-        for (int j = 0; j < kPerThread; ++j) {
-            // one sample, every width: its prefix value is read once
-            const int k = threadIdx.x + j * kThreads;
-            for (int wi = 0; wi < nw; ++wi) {
-                bool hit;
-                if (fast)
-                    hit = wsum(Q, k, rc.W[wi], rc.E[wi]) > rc.thr[wi];
-                else
-                    hit = snr_general(p, rc, Q, c0, k, wi, row.delay) > p.thresh;
-                if (all && hit) {
-                    RunState r{};
-                    r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
-                    r.best_w = wi;
-                    r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
-                    emit(p, row, r, &local_count);
+        } else {
+            // ---- not steady (cold prefix, mask change, partial chunk): the
+            // bit masks from the general S/N
+            for (int j = 0; j < kPerThread; ++j) {
+                const int k = threadIdx.x + j * kThreads;
+                for (int wi = 0; wi < nw; ++wi) {
+                    const bool hit   = snr_general(p, rc, Q, c0, k, wi, row.delay) > p.thresh;
+                    const uint32_t m = __ballot_sync(0xFFFFFFFFU, hit);
+                    if (lane == 0) {
+                        bits[wi * kWords + j * (kThreads / 32) + warp] = m;
+                        if (m != 0U)
+                            atomicOr(&fired_w, 1U << wi);
+                    }
                 }
-                const uint32_t m = __ballot_sync(0xFFFFFFFFU, hit);
-                if (lane == 0)
-                    bits[wi][j * (kThreads / 32) + warp] = m;
-                any |= m;
             }
-        }
-        if (across) {
             __syncthreads();
+        }
+        // bits now hold exactly the above-threshold samples of every width
+        const uint32_t fw = fired_w;
+        if (across) {
             for (int wd = threadIdx.x; wd < kWords; wd += kThreads) {
                 uint32_t m = 0;
                 for (int wi = 0; wi < nw; ++wi)
-                    m |= bits[wi][wd];
+                    if ((fw >> wi) & 1U)
+                        m |= bits[wi * kWords + wd];
                 any_bits[wd] = m;
             }
+            __syncthreads();
         }
-        // Skip the walk when nothing fired and no run is open.
-        const int fired = __syncthreads_or(any != 0);
-        if (!all && threadIdx.x == 0) {
-            if (across) {
-                if (fired || runs[0].open)
+        if (threadIdx.x == 0) {
+            if (all) {
+                // every above-threshold sample and width is a candidate
+                for (int wi = 0; wi < nw; ++wi) {
+                    if (((fw >> wi) & 1U) == 0U)
+                        continue;
+                    for (int wd = 0; wd < kWords; ++wd) {
+                        uint32_t m = bits[wi * kWords + wd];
+                        while (m) {
+                            const int k = wd * 32 + __ffs(m) - 1;
+                            m &= m - 1;
+                            RunState r{};
+                            r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
+                            r.best_w = wi;
+                            r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
+                            emit(p, row, r, &local_count);
+                        }
+                    }
+                }
+            } else if (across) {
+                if (fw != 0U || runs[0].open)
                     walk_runs(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
             } else {
                 for (int wi = 0; wi < nw; ++wi)
-                    if (fired || runs[wi].open)
-                        walk_runs(p, rc, Q, c0, row.delay, bits[wi], wi, runs[wi], row,
+                    if (((fw >> wi) & 1U) != 0U || runs[wi].open)
+                        walk_runs(p, rc, Q, c0, row.delay, bits + wi * kWords, wi, runs[wi], row,
                                   &local_count);
             }
         }
@@ -553,7 +628,9 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
     if (p.err == nullptr)
         throw Error(FROST_ERR_INTERNAL, "search: no error flag");
     const size_t es   = level.fp16 ? 2 : 4;
-    const size_t smem = sizeof(float) * (4 + p.halo + kChunk + 4) + 2 * es * (p.halo + kChunk);
+    const size_t seg  = static_cast<size_t>(p.halo) + kChunk;
+    const size_t smem = sizeof(float) * (4 + seg + 4 + 2 * (seg / 4)) +
+                        sizeof(uint32_t) * search_bits_words(p.nwidths) + 2 * es * seg;
     const dim3 grid(static_cast<unsigned>(g1 - g0));
     auto go = [&](auto kernel, auto data) {
         FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -17,9 +17,9 @@ constexpr int kSearchChunk = 4096;
 constexpr int kTileQuantum = kSearchChunk > kTimePerCta ? kSearchChunk : kTimePerCta;
 
 /** Columns before a search chunk that the search stages: the widest boxcar
- * rounded up to whole 128-column segments. Level buffers keep at least this
+ * rounded up to whole 256-column segments. Level buffers keep at least this
  * many history columns. */
-constexpr int32_t search_halo(int32_t wmax) { return (wmax + 127) / 128 * 128; }
+constexpr int32_t search_halo(int32_t wmax) { return (wmax + 255) / 256 * 256; }
 
 /** One searched row: a DM trial of one plane. */
 struct SearchRow {

@@ -97,3 +97,25 @@ def test_rfi_full_size_channel_mask_and_flags_match_reference(ref):
         assert rep_m[k] == rep_t[k], f"report.{k}: {rep_m[k]} vs {rep_t[k]}"
     assert np.array_equal(gpu.channel_mask(), cpu.channel_mask())
     assert np.array_equal(mine.view(np.uint32), theirs.view(np.uint32)), describe_diff(mine, theirs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["zdot_equalize_u8", "all_strategies_f32"])
+def test_rfi_unaligned_device_block_matches_aligned(name):
+    """A device block that does not start on a 16-byte boundary (here one
+    byte past it) is copied to an aligned buffer first; the result is the
+    same bits as from the aligned block."""
+    import torch
+
+    from frost_b200.rfi import RFICleaner
+    cfg, layout, baseline, blocks = make_case(name)
+    block, nsamps = blocks[0]
+    buf = torch.zeros(block.size + 16, dtype=torch.uint8, device="cuda")
+    outs = []
+    for off in (0, 1):
+        buf[off:off + block.size].copy_(torch.from_numpy(block))
+        gpu = RFICleaner(cfg, layout, baseline)
+        gpu.execute_normalized_device(buf.data_ptr() + off, block.size, nsamps, on_device=True)
+        outs.append((gpu.download().copy(), gpu.channel_mask().copy()))
+    assert np.array_equal(outs[0][0].view(np.uint32), outs[1][0].view(np.uint32))
+    assert np.array_equal(outs[0][1], outs[1][1])

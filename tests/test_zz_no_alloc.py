@@ -88,3 +88,8 @@ def test_static_scratch_refuses_oversize_and_short_blocks():
     rc = L.frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr()),
                                       64 * 4096, 40, C.c_void_p(out.data_ptr()), out.numel(), None)
     assert rc == -1 and "at least 64" in L.frost_last_error().decode()
+    f32 = BlockLayout(64, 4096, DataType.FLOAT32, 1e-3, 1500.0, -1.0)
+    lay = f32.to_c()
+    rc = L.frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr() + 2),
+                                      64 * 4096 * 4, 0, C.c_void_p(out.data_ptr()), out.numel(), None)
+    assert rc == -1 and "aligned" in L.frost_last_error().decode()
