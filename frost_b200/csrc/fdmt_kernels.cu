@@ -284,6 +284,185 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// ---- two levels in one pass ---------------------------------------------
+//
+// A row of level h+1 is a row of level h plus a shifted one, and each of
+// those is a row of level h-1 plus a shifted one, so it is the sum of up to
+// four level h-1 rows read at shifts 0, s1, s2, s3 (FusedOp). Computing
+// (x0 + x1) + (x2 + x3) in float is what the two single levels compute
+// (with float storage the same bits; with fp16 storage the middle sums stay
+// in float), and level h is never written or read back. Staging as in
+// k_level_pipe: one unshifted segment and up to three 16-byte-aligned
+// supersets of the shifted ones per tile, kStages2 tiles in flight.
+
+// 8 consecutive values starting at element off + e of a staged aligned
+// segment (off < 16 / sizeof(S)), as float.
+template <class S>
+__device__ __forceinline__ void load8(const S* stage, int e, int off, float (&x)[8]) {
+    if constexpr (sizeof(S) == 4) {
+        const float4* h4 = reinterpret_cast<const float4*>(stage) + e / 4;
+        const float4 b0 = h4[0], b1 = h4[1], b2 = h4[2]; // b2 unused when off == 0
+        const float h[12] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
+        switch (off) {
+#define FB_PICK(O)                                                                                \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 8; ++i) x[i] = h[O + i];                             \
+        break;
+            FB_PICK(0) FB_PICK(1) FB_PICK(2) FB_PICK(3)
+#undef FB_PICK
+        }
+    } else {
+        const uint4* sv = reinterpret_cast<const uint4*>(stage) + e / 8;
+        const uint4 b0 = sv[0], b1 = sv[1]; // b1 unused when off == 0
+        const uint32_t w[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        uint32_t g[4];
+        switch (off) {
+#define FB_PICK_EVEN(O)                                                                           \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] = w[O / 2 + i];                         \
+        break;
+#define FB_PICK_ODD(O)                                                                            \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] =                                      \
+            __byte_perm(w[O / 2 + i], w[O / 2 + i + 1], 0x5432);                                  \
+        break;
+            FB_PICK_EVEN(0) FB_PICK_ODD(1) FB_PICK_EVEN(2) FB_PICK_ODD(3)
+            FB_PICK_EVEN(4) FB_PICK_ODD(5) FB_PICK_EVEN(6) FB_PICK_ODD(7)
+#undef FB_PICK_EVEN
+#undef FB_PICK_ODD
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&g[i]));
+            x[2 * i]       = f.x;
+            x[2 * i + 1]   = f.y;
+        }
+    }
+}
+
+template <class S> constexpr int kStages2 = sizeof(S) == 2 ? 4 : 3;
+
+template <class S>
+__global__ void __launch_bounds__(kThreads)
+    k_level2_pipe(const FusedOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
+                  int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
+                  int32_t ntiles, unsigned* __restrict__ err) {
+    constexpr int NS        = kStages2<S>;
+    constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
+    constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
+    constexpr int kHiBytes  = kLoBytes + 16;
+    constexpr int kStageBytes = kLoBytes + 3 * kHiBytes;
+    extern __shared__ __align__(128) unsigned char pipe2_smem[];
+    __shared__ __align__(8) uint64_t bar[NS];
+    __shared__ int abort_flag;
+
+    const FusedOp op = ops[blockIdx.x];
+    const int tile0  = blockIdx.y * kTilesPerCta;
+    const int nt     = min(kTilesPerCta, ntiles - tile0);
+    if (nt <= 0)
+        return;
+    const S* rows[4];
+    int off[4];
+    uint32_t bytes[4];
+    int64_t first[4];
+    uint32_t total = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const bool has = op.row[j] >= 0;
+        rows[j]        = in + static_cast<int64_t>(has ? op.row[j] : op.row[0]) * in_pitch;
+        first[j]       = static_cast<int64_t>(in_base) - op.shift[j];
+        off[j]         = static_cast<int>(((first[j] % VEC) + VEC) % VEC);
+        bytes[j]       = !has ? 0U
+                         : j == 0 ? static_cast<uint32_t>(kLoBytes)
+                                  : static_cast<uint32_t>((kTimePerCta / VEC + (off[j] > 0 ? 1 : 0)) * 16);
+        total += bytes[j];
+    }
+    S* dst_row = out + static_cast<int64_t>(blockIdx.x) * out_pitch + out_base;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int st = 0; st < NS; ++st)
+            bulk::mbar_init(&bar[st]);
+    }
+    __syncthreads();
+
+    auto issue = [&](int i) {
+        const int st      = i % NS;
+        const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
+        unsigned char* sb = pipe2_smem + st * kStageBytes;
+        bulk::mbar_expect(&bar[st], total);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (bytes[j] == 0U)
+                continue;
+            const int64_t v0 = (first[j] + k0 - off[j]) / VEC; // aligned start, in vectors
+            bulk::load(sb + (j == 0 ? 0 : kLoBytes + (j - 1) * kHiBytes), rows[j] + v0 * VEC, bytes[j],
+                       &bar[st]);
+        }
+    };
+
+    if (threadIdx.x == 0)
+        for (int i = 0; i < min(NS, nt); ++i)
+            issue(i);
+    const int e = 8 * threadIdx.x;
+    int i       = 0;
+    for (; i < nt; ++i) {
+        const int st         = i % NS;
+        const uint32_t phase = static_cast<uint32_t>((i / NS) & 1);
+        if (!mbar_wait(&bar[st], phase))
+            atomicExch(&abort_flag, 1);
+        __syncthreads();
+        if (abort_flag)
+            break;
+        const unsigned char* sb = pipe2_smem + st * kStageBytes;
+        float a[8], x[8];
+        load8<S>(reinterpret_cast<const S*>(sb), e, 0, a);
+        if (bytes[1] != 0U) {
+            load8<S>(reinterpret_cast<const S*>(sb + kLoBytes), e, off[1], x);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                a[q] = a[q] + x[q];
+        }
+        if (bytes[2] != 0U) {
+            float b[8];
+            load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + kHiBytes), e, off[2], b);
+            if (bytes[3] != 0U) {
+                load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], x);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    b[q] = b[q] + x[q];
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                a[q] = a[q] + b[q];
+        }
+        S* dst = dst_row + static_cast<int64_t>(tile0 + i) * kTimePerCta + e;
+        if constexpr (sizeof(S) == 4) {
+            float4* d4 = reinterpret_cast<float4*>(dst);
+            d4[0]      = make_float4(a[0], a[1], a[2], a[3]);
+            d4[1]      = make_float4(a[4], a[5], a[6], a[7]);
+        } else {
+            uint32_t r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const __half2 h = __floats2half2_rn(fminf(fmaxf(a[2 * q], -65504.0F), 65504.0F),
+                                                    fminf(fmaxf(a[2 * q + 1], -65504.0F), 65504.0F));
+                r[q] = *reinterpret_cast<const uint32_t*>(&h);
+            }
+            *reinterpret_cast<uint4*>(dst) = make_uint4(r[0], r[1], r[2], r[3]);
+        }
+        __syncthreads(); // every thread is done with stage st
+        if (threadIdx.x == 0 && i + NS < nt)
+            issue(i + NS);
+    }
+    if (i < nt && threadIdx.x == 0) {
+        // a wait ran out: report it, then let the copies still in flight land
+        atomicOr(err, 1U);
+        for (int j = i; j < min(nt, i + NS); ++j)
+            (void)mbar_wait(&bar[j % NS], static_cast<uint32_t>((j / NS) & 1));
+    }
+}
+
 template <class S>
 __global__ void __launch_bounds__(kThreads)
     k_level(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
@@ -460,6 +639,35 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
         FB_CUDA(cudaFuncSetAttribute(k_level_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         k_level_pipe<float><<<grid, kThreads, smem, s>>>(
+            ops, static_cast<const float*>(in.data), in.pitch, in.base,
+            static_cast<float*>(out.data), out.pitch, out.base, ntiles, err);
+    }
+    FB_LAUNCH_CHECK();
+}
+
+void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
+                   unsigned* err, cudaStream_t s) {
+    if (nrows == 0)
+        return;
+    if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
+        out.pitch % 8 != 0 || in.fp16 != out.fp16 || err == nullptr)
+        throw Error(FROST_ERR_INTERNAL, "level2: bad geometry");
+    const int ntiles = ncols / kTimePerCta;
+    const dim3 grid(static_cast<unsigned>(nrows),
+                    static_cast<unsigned>((ntiles + kTilesPerCta - 1) / kTilesPerCta));
+    const size_t es = out.fp16 ? 2 : 4;
+    if (out.fp16) {
+        const size_t smem = kStages2<__half> * (4 * kTimePerCta * es + 48);
+        FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_level2_pipe<__half><<<grid, kThreads, smem, s>>>(
+            ops, static_cast<const __half*>(in.data), in.pitch, in.base,
+            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, err);
+    } else {
+        const size_t smem = kStages2<float> * (4 * kTimePerCta * es + 48);
+        FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_level2_pipe<float><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const float*>(in.data), in.pitch, in.base,
             static_cast<float*>(out.data), out.pitch, out.base, ntiles, err);
     }

@@ -35,6 +35,19 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
                   unsigned* err, cudaStream_t s);
 
+/** A row of level h+1 from four rows of level h-1: the sum of row[j] read at
+ * t - shift[j] (shift[0] = 0), grouped (row0 + row1) + (row2 + row3); a
+ * negative row[j] is absent (pass-through nodes). */
+struct FusedOp {
+    int32_t row[4];
+    int32_t shift[4];
+};
+
+/** Level h+1 straight from level h-1 (TMA-pipelined; *err set if a bounded
+ * wait ran out). */
+void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
+                   unsigned* err, cudaStream_t s);
+
 /** Copies the last `hist` columns ending at column base + n_valid of every
  * row of `view` into hist_buf[rows][hist]. */
 void launch_save_history(LevelView view, int64_t rows, int32_t hist, int32_t n_valid,

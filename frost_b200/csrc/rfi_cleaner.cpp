@@ -288,7 +288,7 @@ SizeType Cleaner::memory_usage() const {
         &m_s_det, &m_s_keep_d, &m_s_keep_f, &m_row_std, &m_kspec_pos, &m_kspec_neg,
         &m_kspec_whole, &m_chunk_min, &m_chunk_max, &m_chunk_zdot, &m_chunk_kpos, &m_chunk_kneg,
         &m_lo, &m_hi, &m_zdot_sum, &m_kpos_best, &m_kneg_best, &m_time_flags_d, &m_zdot_a_d,
-        &m_zdot_b_d, &m_kchan_pos_d, &m_kchan_neg_d, &m_flagged_d, &m_work, &m_out, &m_counters,
+        &m_zdot_b_d, &m_kchan_pos_d, &m_kchan_neg_d, &m_kchan_any_d, &m_flagged_d, &m_work, &m_out, &m_counters,
         &m_first_bad, &m_tail_loc, &m_tail_scale, &m_tail_out_loc, &m_tail_out_scale, &m_recip};
     SizeType total = 0;
     for (const auto* b : all)
@@ -832,20 +832,32 @@ void Cleaner::run_full(const Dims& d, cudaStream_t s) {
     h2d(m_mask_d, m_mask.data(), n, s);
     h2d(m_zdot_a_d, m_zdot_a.data(), n, s);
     h2d(m_zdot_b_d, m_zdot_b.data(), n, s);
+    // channels with a Kadane-along-time segment (the rest skip the test)
+    std::vector<uint8_t> kany(n, 0);
+    bool any_segment = false;
     if (kchan) {
+        for (SizeType ch = 0; ch < n; ++ch) {
+            kany[ch]    = (kcp[ch].start <= kcp[ch].end || kcn[ch].start <= kcn[ch].end) ? 1 : 0;
+            any_segment = any_segment || kany[ch] != 0;
+        }
         h2d(m_kchan_pos_d, kcp.data(), n, s);
         h2d(m_kchan_neg_d, kcn.data(), n, s);
     } else {
         m_kchan_pos_d.reserve(sizeof(Segment));
         m_kchan_neg_d.reserve(sizeof(Segment));
     }
+    h2d(m_kchan_any_d, kany.data(), n, s);
     h2d(m_flagged_d, flagged.data(), flagged.size(), s);
     FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, kCountSlots * sizeof(unsigned long long), s));
     const ApplyParams p = apply_params();
-    launch_apply_unflagged(d, p, raw, m_loc.as<float>(), m_scale.as<float>(), m_inv.as<float>(),
+    ApplyParams pu      = p;
+    if (!any_segment)
+        pu.kchan = 0; // no segment anywhere: no cell can be a Kadane-channel cell
+    launch_apply_unflagged(d, pu, raw, m_loc.as<float>(), m_scale.as<float>(), m_inv.as<float>(),
                            m_mask_d.as<uint8_t>(), m_time_flags_d.as<uint8_t>(),
                            m_kspec_pos.as<Span32>(), m_kspec_neg.as<Span32>(),
                            m_kchan_pos_d.as<Segment>(), m_kchan_neg_d.as<Segment>(),
+                           m_kchan_any_d.as<uint8_t>(),
                            m_s_keep_f.as<float>(), m_zdot_a_d.as<float>(), m_zdot_b_d.as<float>(),
                            m_work.as<float>(), m_counters.as<unsigned long long>(), s);
     launch_apply_flagged(d, p, m_flagged_d.as<uint64_t>(), flagged.size(), m_loc.as<float>(),

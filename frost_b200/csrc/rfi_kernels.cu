@@ -629,10 +629,10 @@ __global__ void __launch_bounds__(kScanRows)
                    kspec_whole);
 }
 
-// The same rows with 256-byte column tiles of all 128 rows bulk-copied
-// into shared memory (cp.async, two tiles deep; rows padded to 272 bytes so
+// The same rows with 128-byte column tiles of all 128 rows bulk-copied
+// into shared memory (cp.async, two tiles deep; rows padded to 144 bytes so
 // that each thread's 16-byte reads of its own row are conflict-free).
-constexpr int kRowTileBytes  = 256;
+constexpr int kRowTileBytes  = 128;
 constexpr int kRowTileStride = kRowTileBytes + 16;
 
 template <int D>
@@ -910,6 +910,7 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
                                   const Span32* __restrict__ kspec_neg,
                                   const Segment* __restrict__ kchan_pos,
                                   const Segment* __restrict__ kchan_neg,
+                                  const uint8_t* __restrict__ kchan_any,
                                   const float* __restrict__ s_keep_f,
                                   const float* __restrict__ zdot_a,
                                   const float* __restrict__ zdot_b, float* __restrict__ work,
@@ -946,7 +947,7 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
     // per-window constants and stores of the row, when nchans % 4 == 0)
     for (uint64_t cb = threadIdx.x * V; cb < n; cb += blockDim.x * V) {
         float xs[V], ls[V], ss[V], is[V], outv[V];
-        uint8_t ms[V];
+        uint8_t ms[V], ka[V];
         if constexpr (V == 4) {
             const float4 l4 = *reinterpret_cast<const float4*>(lw + cb);
             const float4 s4 = *reinterpret_cast<const float4*>(sw + cb);
@@ -956,6 +957,12 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
             ss[0] = s4.x; ss[1] = s4.y; ss[2] = s4.z; ss[3] = s4.w;
             is[0] = i4.x; is[1] = i4.y; is[2] = i4.z; is[3] = i4.w;
             ms[0] = m4.x; ms[1] = m4.y; ms[2] = m4.z; ms[3] = m4.w;
+            if (p.kchan) {
+                const uchar4 k4 = *reinterpret_cast<const uchar4*>(kchan_any + cb);
+                ka[0] = k4.x; ka[1] = k4.y; ka[2] = k4.z; ka[3] = k4.w;
+            } else {
+                ka[0] = ka[1] = ka[2] = ka[3] = 0;
+            }
             if constexpr (D == FROST_UINT8) {
                 const uchar4 x4 = *reinterpret_cast<const uchar4*>(in + cb);
                 xs[0] = static_cast<float>(x4.x); xs[1] = static_cast<float>(x4.y);
@@ -970,6 +977,7 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
             ss[0] = sw[cb];
             is[0] = iw[cb];
             ms[0] = mask[cb];
+            ka[0] = p.kchan ? kchan_any[cb] : 0;
             xs[0] = rd<D>(in, cb);
         }
 #pragma unroll
@@ -990,7 +998,7 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
                     st = kNarrow;
                 } else if (p.kspec && (span_has(ksp, c) || span_has(ksn, c))) {
                     st = kKadaneSpectrum;
-                } else if (p.kchan && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
+                } else if (ka[e] != 0 && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
                     st = kKadaneChannel;
                 } else {
                     st = kClean;
@@ -1170,9 +1178,13 @@ __global__ void k_unpack(Dims d, const uint8_t* __restrict__ raw, float* __restr
 // n < 2^40 from a rounding midpoint (a/n is never exactly a midpoint), so
 // it rounds as a/n does. Zero and tiny |a| (where r could lose bits) take
 // the plain division.
+// The plain division as a call, so the compiler keeps it off the common
+// path instead of computing it alongside (if-converting the branch).
+__device__ __noinline__ double div_plain(double a, double n) { return a / n; }
+
 __device__ __forceinline__ double div_by_count(double a, double n, double y) {
     if (!(fabs(a) > 0x1p-900))
-        return a / n;
+        return div_plain(a, n);
     const double q0 = a * y;
     const double r  = fma(-q0, n, a);
     return fma(r, y, q0);
@@ -1195,7 +1207,7 @@ struct WelfordAcc {
     __device__ __forceinline__ void step_by(float xf, double n, double y) {
         const double x     = xf;
         const double delta = x - mean;
-        mean += y != 0.0 ? div_by_count(delta, n, y) : delta / n;
+        mean += y != 0.0 ? div_by_count(delta, n, y) : div_plain(delta, n);
         var += delta * (x - mean);
     }
 };
@@ -1319,6 +1331,74 @@ __global__ void k_normalize(Dims d, const float* __restrict__ work, const float*
                 if (cc < n) {
                     const uint64_t dst      = flip ? n - 1 - cc : cc;
                     out[dst * capacity + t] = tile[threadIdx.x][k];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// The same with 64 x 64 tiles and 16-byte loads and stores (nchans and the
+// output capacity multiples of 4): a thread reads 4 channels of a row and
+// writes 4 samples of a channel.
+constexpr int kNT = 64;
+
+__global__ void __launch_bounds__(256)
+    k_normalize4(Dims d, const float* __restrict__ work, const float* __restrict__ loc,
+                 const float* __restrict__ scale, const uint8_t* __restrict__ mask, int flip,
+                 uint64_t capacity, float* __restrict__ out) {
+    __shared__ float tile[kNT][kNT + 1]; // [channel][time]
+    const uint64_t n  = d.nchans;
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.y) * kNT;
+    const int q       = threadIdx.x % 16; // channel quad (load) / sample quad (store)
+    const int r       = threadIdx.x / 16; // row (load) / channel (store) offset, 0..15
+    const uint64_t c  = c0 + 4 * q;
+    bool on[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+        on[e] = c + e < n && mask[c + e] != 0;
+    uint64_t wend = 0;
+    float l[4] = {0, 0, 0, 0}, is[4] = {1, 1, 1, 1};
+    const uint64_t span0 = static_cast<uint64_t>(blockIdx.x) * kNormSpan;
+    for (uint64_t t0 = span0; t0 < span0 + kNormSpan && t0 < capacity; t0 += kNT) {
+#pragma unroll
+        for (int pass = 0; pass < kNT / 16; ++pass) {
+            const int tl     = r + 16 * pass;
+            const uint64_t t = t0 + tl;
+            float v[4]       = {0, 0, 0, 0};
+            if (t < d.nsamps && c < n) {
+                if (t >= wend) {
+                    const uint64_t w = window_of(t, d.window, d.nwin);
+                    wend             = window_end(w, d);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        l[e]           = loc[w * n + c + e];
+                        const float sc = scale[w * n + c + e];
+                        is[e]          = sc > 0.0F ? 1.0F / sc : 1.0F;
+                    }
+                }
+                const float4 x = *reinterpret_cast<const float4*>(work + t * n + c);
+                const float xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    v[e] = on[e] ? (xs[e] - l[e]) * is[e] : 0.0F;
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                tile[4 * q + e][tl] = v[e];
+        }
+        __syncthreads();
+        const uint64_t t = t0 + 4 * q;
+        if (t < capacity) {
+#pragma unroll
+            for (int pass = 0; pass < kNT / 16; ++pass) {
+                const int cl      = r + 16 * pass;
+                const uint64_t cc = c0 + cl;
+                if (cc < n) {
+                    const uint64_t dst = flip ? n - 1 - cc : cc;
+                    const float4 o = make_float4(tile[cl][4 * q], tile[cl][4 * q + 1], tile[cl][4 * q + 2],
+                                                 tile[cl][4 * q + 3]);
+                    *reinterpret_cast<float4*>(out + dst * capacity + t) = o;
                 }
             }
         }
@@ -1515,7 +1595,8 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
                             const float* loc, const float* scale, const float* inv,
                             const uint8_t* mask, const uint8_t* time_flags, const Span32* kspec_pos,
                             const Span32* kspec_neg, const Segment* kchan_pos,
-                            const Segment* kchan_neg, const float* s_keep_f, const float* zdot_a,
+                            const Segment* kchan_neg, const uint8_t* kchan_any,
+                            const float* s_keep_f, const float* zdot_a,
                             const float* zdot_b, float* work, unsigned long long* counters,
                             cudaStream_t s) {
     const size_t smem = d.nchans * (sizeof(float) + 1);
@@ -1529,12 +1610,12 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
             set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 4>), smem);
             k_apply_unflagged<D, 4><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
                 d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
-                kchan_neg, s_keep_f, zdot_a, zdot_b, work, counters);
+                kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, work, counters);
         } else {
             set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 1>), smem);
             k_apply_unflagged<D, 1><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
                 d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
-                kchan_neg, s_keep_f, zdot_a, zdot_b, work, counters);
+                kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, work, counters);
         }
     });
     FB_COUNT_LAUNCH();
@@ -1580,8 +1661,13 @@ void launch_welford(const Dims& d, const float* work, const double* recip, float
 
 void launch_normalize(const Dims& d, const float* work, const float* loc, const float* scale,
                       const uint8_t* mask, int flip, uint64_t capacity, float* out, cudaStream_t s) {
-    const dim3 grid(grid1(capacity, kNormSpan), grid1(d.nchans, kTile));
-    k_normalize<<<grid, dim3(kTile, 8), 0, s>>>(d, work, loc, scale, mask, flip, capacity, out);
+    if (d.nchans % 4 == 0 && capacity % 4 == 0) {
+        const dim3 grid(grid1(capacity, kNormSpan), grid1(d.nchans, kNT));
+        k_normalize4<<<grid, 256, 0, s>>>(d, work, loc, scale, mask, flip, capacity, out);
+    } else {
+        const dim3 grid(grid1(capacity, kNormSpan), grid1(d.nchans, kTile));
+        k_normalize<<<grid, dim3(kTile, 8), 0, s>>>(d, work, loc, scale, mask, flip, capacity, out);
+    }
     FB_COUNT_LAUNCH();
 }
 

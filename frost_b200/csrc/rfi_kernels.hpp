@@ -92,12 +92,15 @@ void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const
                       KadaneState* chunk_kneg, float* lo, float* hi, ZdotSums* zdot_sum,
                       Run* kpos_best, Run* kneg_best, cudaStream_t s);
 
-// Cleans unflagged rows into work[nsamps][nchans] (float).
+// Cleans unflagged rows into work[nsamps][nchans] (float). kchan_any[c]
+// marks the channels with a Kadane-along-time segment (only those read
+// their segments).
 void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* raw,
                             const float* loc, const float* scale, const float* inv,
                             const uint8_t* mask, const uint8_t* time_flags, const Span32* kspec_pos,
                             const Span32* kspec_neg, const Segment* kchan_pos,
-                            const Segment* kchan_neg, const float* s_keep_f, const float* zdot_a,
+                            const Segment* kchan_neg, const uint8_t* kchan_any,
+                            const float* s_keep_f, const float* zdot_a,
                             const float* zdot_b, float* work, unsigned long long* counters,
                             cudaStream_t s);
 

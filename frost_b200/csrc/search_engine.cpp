@@ -97,6 +97,57 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     }
     upload(m_row_ops, all_ops, s);
 
+    // FDMT schedule. Levels holding searched planes, level 1 and the top are
+    // stored; between them, a level whose successor is not stored is
+    // computed straight from the one below its predecessor (two levels in
+    // one pass, halving that pair's HBM traffic).
+    const auto& plan_planes = m_plan.planes();
+    std::vector<char> keep(L + 1, 0);
+    keep[1] = 1;
+    keep[L] = 1;
+    for (const auto& p : plan_planes)
+        keep[p.height] = 1;
+    m_buf_of.assign(L + 1, -1);
+    m_hist_len.assign(L + 1, 0);
+    m_hist_len[0] = m_plan.level_history(0);
+    m_steps.push_back({1, 0, false, 0});
+    m_buf_of[1] = 0;
+    std::vector<FusedOp> fused_all;
+    for (int h = 1; h < L;) {
+        Step st{};
+        if (h + 2 <= L && !keep[h + 1]) {
+            st = {h + 2, h, true, static_cast<int64_t>(fused_all.size())};
+            const auto& mid = m_plan.row_ops(h + 1);
+            for (const RowOp& op : m_plan.row_ops(h + 2)) {
+                const RowOp& a = mid[op.lo_row];
+                FusedOp f{{a.lo_row, a.hi_row, -1, -1}, {0, a.hi_row >= 0 ? a.shift : 0, 0, 0}};
+                if (op.hi_row >= 0) {
+                    const RowOp& b = mid[op.hi_row];
+                    f.row[2]       = b.lo_row;
+                    f.shift[2]     = op.shift;
+                    f.row[3]       = b.hi_row;
+                    f.shift[3]     = b.hi_row >= 0 ? op.shift + b.shift : 0;
+                }
+                for (int j = 1; j < 4; ++j)
+                    if (f.row[j] >= 0)
+                        m_hist_len[h] = std::max(m_hist_len[h], f.shift[j]);
+                fused_all.push_back(f);
+            }
+            h += 2;
+        } else {
+            st = {h + 1, h, false, m_row_op_offset[h + 1]};
+            for (const RowOp& op : m_plan.row_ops(h + 1))
+                if (op.hi_row >= 0)
+                    m_hist_len[h] = std::max(m_hist_len[h], op.shift);
+            h += 1;
+        }
+        m_buf_of[st.out] = static_cast<int>(m_steps.size() % 2);
+        m_steps.push_back(st);
+    }
+    for (const auto& p : plan_planes)
+        m_hist_len[p.height] = std::max(m_hist_len[p.height], m_plan.widths().back() - 1);
+    upload(m_fused_ops, fused_all, s);
+
     // Searched rows, grouped by height.
     const auto& planes = m_plan.planes();
     std::vector<int32_t> order(planes.size());
@@ -243,12 +294,12 @@ SizeType Engine::plan_bytes(int64_t tile) const {
     const int L          = m_plan.levels();
     int32_t maxh         = 0;
     for (int h = 1; h <= L; ++h)
-        maxh = std::max(maxh, m_plan.level_history(h));
+        maxh = std::max(maxh, m_hist_len[h]);
     const int64_t base   = round_up(std::max<int64_t>(maxh, search_halo(m_plan.widths().back())), 8);
     const int64_t pitch  = base + round_up(tile, kTileQuantum);
     SizeType bytes       = 2 * static_cast<SizeType>(m_plan.max_level_rows()) * pitch * es;
     for (int h = 1; h <= L; ++h)
-        bytes += static_cast<SizeType>(m_plan.level_rows(h)) * m_plan.level_history(h) * es;
+        bytes += static_cast<SizeType>(m_plan.level_rows(h)) * m_hist_len[h] * es;
     bytes += 2 * static_cast<SizeType>(m_plan.nchans()) * m_plan.level_history(0) * sizeof(float);
     bytes += m_leaf_len.bytes() + m_rows.bytes() + m_var.bytes() + m_inv.bytes() * 2 +
              m_carry.bytes() + m_cands.bytes() + m_row_ops.bytes() + m_leaf_ops.bytes();
@@ -260,7 +311,7 @@ void Engine::allocate(int64_t tile) {
     const int L       = m_plan.levels();
     int32_t maxh      = 0;
     for (int h = 1; h <= L; ++h)
-        maxh = std::max(maxh, m_plan.level_history(h));
+        maxh = std::max(maxh, m_hist_len[h]);
     m_tile  = tile;
     m_ncols = round_up(tile, kTileQuantum);
     m_base  = static_cast<int32_t>(round_up(std::max<int64_t>(maxh, search_halo(m_plan.widths().back())), 8));
@@ -273,7 +324,7 @@ void Engine::allocate(int64_t tile) {
     m_hist.clear();
     m_hist.resize(L + 1);
     for (int h = 1; h <= L; ++h) {
-        const SizeType bytes = static_cast<SizeType>(m_plan.level_rows(h)) * m_plan.level_history(h) * es;
+        const SizeType bytes = static_cast<SizeType>(m_plan.level_rows(h)) * m_hist_len[h] * es;
         m_hist[h].reserve(std::max<SizeType>(bytes, 16));
         FB_CUDA(cudaMemsetAsync(m_hist[h].get(), 0, std::max<SizeType>(bytes, 16), m_stream));
     }
@@ -300,7 +351,7 @@ SizeType Engine::device_bytes() const {
 }
 
 LevelView Engine::view(int h) const {
-    return LevelView{m_buf[h % 2].get(), m_pitch, m_base, m_fp16 ? 1 : 0};
+    return LevelView{m_buf[m_buf_of[h]].get(), m_pitch, m_base, m_fp16 ? 1 : 0};
 }
 
 SearchParams Engine::params(int64_t tile_t0, int64_t gulp_t0, int32_t n_valid, bool or_active) const {
@@ -401,9 +452,12 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
     for (int64_t t_off = 0; t_off < static_cast<int64_t>(nsamps); t_off += m_tile) {
         const int32_t n_valid = static_cast<int32_t>(std::min<int64_t>(m_tile, nsamps - t_off));
         const SearchParams sp = params(gulp0 + t_off, gulp0, n_valid, or_active);
-        for (int h = 1; h <= L; ++h) {
+        for (size_t si = 0; si < m_steps.size(); ++si) {
+            const Step& st      = m_steps[si];
+            const int h         = st.out;
             const LevelView out = view(h);
-            if (h == 1) {
+            unsigned* err       = reinterpret_cast<unsigned*>(m_counters.as<unsigned long long>() + 3);
+            if (si == 0) {
                 timed(kLevel1, s, [&] {
                     launch_level1(m_leaf_ops.as<LeafOp>(), m_node_first_op_d.as<int32_t>(),
                                   static_cast<int32_t>(m_node_first_op.size() - 1),
@@ -422,19 +476,20 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
                     static_cast<uint64_t>(m_plan.level_rows(1)) * m_ncols * es;
             } else {
                 timed(kLevel, s, [&] {
-                    launch_level(m_row_ops.as<RowOp>() + m_row_op_offset[h], m_plan.level_rows(h),
-                                 view(h - 1), out, static_cast<int32_t>(m_ncols),
-                                 reinterpret_cast<unsigned*>(m_counters.as<unsigned long long>() + 3),
-                                 s);
+                    if (st.fused)
+                        launch_level2(m_fused_ops.as<FusedOp>() + st.op_offset, m_plan.level_rows(h),
+                                      view(st.in), out, static_cast<int32_t>(m_ncols), err, s);
+                    else
+                        launch_level(m_row_ops.as<RowOp>() + st.op_offset, m_plan.level_rows(h),
+                                     view(st.in), out, static_cast<int32_t>(m_ncols), err, s);
                 });
                 m_launches += 1;
                 m_timing.level_launches += 1;
                 m_timing.algorithmic_level_bytes +=
-                    static_cast<uint64_t>(m_plan.level_rows(h - 1) + m_plan.level_rows(h)) * m_ncols * es;
+                    static_cast<uint64_t>(m_plan.level_rows(st.in) + m_plan.level_rows(h)) * m_ncols * es;
             }
             timed(kHistory, s, [&] {
-                launch_load_history(out, m_plan.level_rows(h), m_plan.level_history(h),
-                                    m_hist[h].get(), s);
+                launch_load_history(out, m_plan.level_rows(h), m_hist_len[h], m_hist[h].get(), s);
             });
             if (m_height_g1[h] > m_height_g0[h]) {
                 timed(kSearch, s, [&] { launch_search(sp, out, m_height_g0[h], m_height_g1[h], s); });
@@ -456,15 +511,14 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
                     }
                 }
             }
-            if (h >= 2)
+            if (si > 0)
                 timed(kHistory, s, [&] {
-                    launch_save_history(view(h - 1), m_plan.level_rows(h - 1),
-                                        m_plan.level_history(h - 1), n_valid, m_hist[h - 1].get(), s);
+                    launch_save_history(view(st.in), m_plan.level_rows(st.in), m_hist_len[st.in],
+                                        n_valid, m_hist[st.in].get(), s);
                 });
         }
         timed(kHistory, s, [&] {
-            launch_save_history(view(L), m_plan.level_rows(L), m_plan.level_history(L), n_valid,
-                                m_hist[L].get(), s);
+            launch_save_history(view(L), m_plan.level_rows(L), m_hist_len[L], n_valid, m_hist[L].get(), s);
         });
     }
     m_samples += nsamps;

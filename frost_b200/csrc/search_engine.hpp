@@ -78,6 +78,18 @@ private:
         m_leaf_offset, m_gtab, m_var, m_inv, m_inv_or, m_mask_d, m_mask_or_d, m_carry,
         m_row_counts, m_cands, m_counters, m_frontier, m_capture_rows;
     std::vector<int64_t> m_row_op_offset;
+    /** One FDMT step: level `out` from level `in` = out - 1 (single) or
+     * out - 2 (fused: the level between is never stored). Step 0 is level 1
+     * from the input. */
+    struct Step {
+        int out, in;
+        bool fused;
+        int64_t op_offset; // into m_row_ops (single) or m_fused_ops (fused)
+    };
+    std::vector<Step> m_steps;
+    std::vector<int> m_buf_of;         // level -> level buffer (-1: not stored)
+    std::vector<int32_t> m_hist_len;   // level -> history columns kept
+    DeviceBuffer m_fused_ops;
     std::vector<DeviceBuffer> m_capture;
     bool m_capture_on = false;
     int64_t m_capture_cols = 0;

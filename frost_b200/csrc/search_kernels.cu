@@ -14,10 +14,10 @@
 // exact test, which also writes the per-width bit masks of the samples that
 // fired. A chunk where nothing fires costs one block vote. The first
 // chunks of a stream or after a mask change (cold prefix, OR-mask
-// variance) build the bit masks from the general S/N. One lane walks the
-// set bits of the widths that fired in time order, extending or closing
-// the run carried from the previous chunk (and tile, and gulp) and
-// emitting each closed run's peak. The DM-time rows are never re-read and
+// variance) build the bit masks from the general S/N. For every width that
+// fired, one lane (widths spread over the warps) walks its set bits in time
+// order, extending or closing the run carried from the previous chunk (and
+// tile, and gulp) and emitting each closed run's peak. The DM-time rows are never re-read and
 // the run state is the only thing carried between calls.
 
 #include <cuda_fp16.h>
@@ -259,17 +259,6 @@ __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float
     }
 }
 
-// Closes the runs still open at the end of a chunk in which nothing fired
-// (what walk_runs does for an all-zero mask).
-__device__ void close_open_runs(const SearchParams& p, RunState* runs, int nruns,
-                                const SearchRow& row, uint32_t* count) {
-    for (int i = 0; i < nruns; ++i)
-        if (runs[i].open) {
-            emit(p, row, runs[i], count);
-            runs[i].open = 0;
-        }
-}
-
 // Words of the per-width bit masks [nw][kWords].
 __host__ __device__ constexpr int search_bits_words(int nw) { return nw * kWords; }
 
@@ -480,8 +469,10 @@ __global__ void __launch_bounds__(kThreads, 4)
             }
             if (!__syncthreads_or(up)) {
                 // nothing fired: runs open at the chunk start close here
-                if (!all && threadIdx.x == 0)
-                    close_open_runs(p, runs, nruns, row, &local_count);
+                if (!all && threadIdx.x < nruns && runs[threadIdx.x].open) {
+                    emit(p, row, runs[threadIdx.x], &local_count);
+                    runs[threadIdx.x].open = 0;
+                }
                 continue; // Ps is rewritten only after every thread passed the barrier
             }
         } else {
@@ -513,35 +504,35 @@ __global__ void __launch_bounds__(kThreads, 4)
             }
             __syncthreads();
         }
-        if (threadIdx.x == 0) {
-            if (all) {
-                // every above-threshold sample and width is a candidate
-                for (int wi = 0; wi < nw; ++wi) {
-                    if (((fw >> wi) & 1U) == 0U)
-                        continue;
-                    for (int wd = 0; wd < kWords; ++wd) {
-                        uint32_t m = bits[wi * kWords + wd];
-                        while (m) {
-                            const int k = wd * 32 + __ffs(m) - 1;
-                            m &= m - 1;
-                            RunState r{};
-                            r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
-                            r.best_w = wi;
-                            r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
-                            emit(p, row, r, &local_count);
-                        }
+        // Widths are independent (each has its own run state): lane 0 of
+        // warp w walks widths w, w + 8, ... Candidates of different widths
+        // may therefore reach the output in any order (results are sorted
+        // afterwards; only which ones a per-DM cap drops can vary).
+        if (all && lane == 0) {
+            for (int wi = warp; wi < nw; wi += kThreads / 32) {
+                if (((fw >> wi) & 1U) == 0U)
+                    continue;
+                for (int wd = 0; wd < kWords; ++wd) {
+                    uint32_t m = bits[wi * kWords + wd];
+                    while (m) {
+                        const int k = wd * 32 + __ffs(m) - 1;
+                        m &= m - 1;
+                        RunState r{};
+                        r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
+                        r.best_w = wi;
+                        r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
+                        emit(p, row, r, &local_count);
                     }
                 }
-            } else if (across) {
-                if (fw != 0U || runs[0].open)
-                    walk_runs(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
-            } else {
-                for (int wi = 0; wi < nw; ++wi)
-                    if (((fw >> wi) & 1U) != 0U || runs[wi].open)
-                        walk_runs(p, rc, Q, c0, row.delay, bits + wi * kWords, wi, runs[wi], row,
-                                  &local_count);
             }
+        } else if (!all && !across && lane == 0) {
+            for (int wi = warp; wi < nw; wi += kThreads / 32)
+                if (((fw >> wi) & 1U) != 0U || runs[wi].open)
+                    walk_runs(p, rc, Q, c0, row.delay, bits + wi * kWords, wi, runs[wi], row,
+                              &local_count);
         }
+        if (across && threadIdx.x == 0 && (fw != 0U || runs[0].open))
+            walk_runs(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
         __syncthreads();
     }
     if (abort_flag) {
