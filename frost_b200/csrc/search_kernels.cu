@@ -422,49 +422,61 @@ __global__ void __launch_bounds__(kThreads, 4)
             // expression as wsum) and set the bits of the samples that fire.
             // Trapezoids take the exact test throughout.
             bool up = false;
-#pragma unroll
-            for (int q = 0; q < kPerThread / 4; ++q) {
-                const int gi   = threadIdx.x + q * kThreads; // group in the chunk
+            // the exact test of group gi at width wi (sets the fired bits)
+            auto exact = [&](int gi, int wi, int W, int E, float T) {
                 const int k    = 4 * gi;
-                const float hi = gmax[gi + halo / 4];
-                for (int wi = 0; wi < nw; ++wi) {
-                    const int W   = rc.W[wi];
-                    const int E   = rc.E[wi];
-                    const float T = rc.thr[wi];
-                    bool maybe    = true;
-                    if (E == 0) {
-                        const int lo_g = (halo + k - W) >> 2; // group of Q[k - W]
-                        float lo       = gmin[lo_g];
-                        if ((W & 3) != 0)
-                            lo = fminf(lo, gmin[lo_g + 1]);
-                        maybe = hi - lo > T;
+                const float4 a = *reinterpret_cast<const float4*>(Q + k);
+                const float4 b = ld4(Q, k - W);
+                float s0, s1, s2, s3;
+                if (E > 0) {
+                    const float4 c = ld4(Q, k - E);
+                    const float4 d = ld4(Q, k - W + E);
+                    s0 = trap_sum(a.x, b.x, c.x, d.x);
+                    s1 = trap_sum(a.y, b.y, c.y, d.y);
+                    s2 = trap_sum(a.z, b.z, c.z, d.z);
+                    s3 = trap_sum(a.w, b.w, c.w, d.w);
+                } else {
+                    s0 = a.x - b.x;
+                    s1 = a.y - b.y;
+                    s2 = a.z - b.z;
+                    s3 = a.w - b.w;
+                }
+                const uint32_t nib = (s0 > T ? 1U : 0U) | (s1 > T ? 2U : 0U) | (s2 > T ? 4U : 0U) |
+                                     (s3 > T ? 8U : 0U);
+                if (nib != 0U) {
+                    // samples 4 gi .. 4 gi + 3: word gi / 8, nibble gi % 8
+                    atomicOr(&bits[wi * kWords + (gi >> 3)], nib << ((gi & 7) * 4));
+                    atomicOr(&fired_w, 1U << wi);
+                    up = true;
+                }
+            };
+            constexpr int NG = kPerThread / 4; // groups per thread
+            float hi[NG];
+#pragma unroll
+            for (int q = 0; q < NG; ++q)
+                hi[q] = gmax[threadIdx.x + q * kThreads + halo / 4];
+            for (int wi = 0; wi < nw; ++wi) {
+                const int W   = rc.W[wi];
+                const int E   = rc.E[wi];
+                const float T = rc.thr[wi];
+                const int sh  = (halo - W) >> 2; // group of Q[4 gi - W] is gi + sh
+                if (E == 0 && (W & 3) == 0) {
+#pragma unroll
+                    for (int q = 0; q < NG; ++q) {
+                        const int gi = threadIdx.x + q * kThreads;
+                        if (hi[q] - gmin[gi + sh] > T)
+                            exact(gi, wi, W, E, T);
                     }
-                    if (maybe) {
-                        const float4 a = *reinterpret_cast<const float4*>(Q + k);
-                        const float4 b = ld4(Q, k - W);
-                        float s0, s1, s2, s3;
-                        if (E > 0) {
-                            const float4 c = ld4(Q, k - E);
-                            const float4 d = ld4(Q, k - W + E);
-                            s0 = trap_sum(a.x, b.x, c.x, d.x);
-                            s1 = trap_sum(a.y, b.y, c.y, d.y);
-                            s2 = trap_sum(a.z, b.z, c.z, d.z);
-                            s3 = trap_sum(a.w, b.w, c.w, d.w);
-                        } else {
-                            s0 = a.x - b.x;
-                            s1 = a.y - b.y;
-                            s2 = a.z - b.z;
-                            s3 = a.w - b.w;
-                        }
-                        const uint32_t nib = (s0 > T ? 1U : 0U) | (s1 > T ? 2U : 0U) |
-                                             (s2 > T ? 4U : 0U) | (s3 > T ? 8U : 0U);
-                        if (nib != 0U) {
-                            // samples 4 gi .. 4 gi + 3: word gi / 8, nibble gi % 8
-                            atomicOr(&bits[wi * kWords + (gi >> 3)], nib << ((gi & 7) * 4));
-                            atomicOr(&fired_w, 1U << wi);
-                            up = true;
-                        }
+                } else if (E == 0) {
+#pragma unroll
+                    for (int q = 0; q < NG; ++q) {
+                        const int gi = threadIdx.x + q * kThreads;
+                        if (hi[q] - fminf(gmin[gi + sh], gmin[gi + sh + 1]) > T)
+                            exact(gi, wi, W, E, T);
                     }
+                } else {
+                    for (int q = 0; q < NG; ++q)
+                        exact(threadIdx.x + q * kThreads, wi, W, E, T);
                 }
             }
             if (!__syncthreads_or(up)) {

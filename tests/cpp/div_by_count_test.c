@@ -16,6 +16,8 @@ static uint64_t next(void) {
 }
 
 static double div_by_count(double a, double n, double y) {
+    if (a == 0.0)
+        return a;
     if (!(fabs(a) > 0x1p-900))
         return a / n;
     const double q0 = a * y;
@@ -36,7 +38,9 @@ int main(void) {
             if (!isfinite(a) || fabs(a) > 1e300)
                 continue;
         } else {
-            a = ((double)(next() % 1000000) - 500000.0) * 0.125; // dyadic values
+            a = ((double)(next() % 1000000) - 500000.0) * 0.125; // dyadic values, zeros included
+            if (i % 7 == 0)
+                a = (i % 2) ? 0.0 : -0.0;
         }
         const double y = 1.0 / (double)n;
         const double q = div_by_count(a, (double)n, y), t = a / (double)n;
