@@ -64,6 +64,7 @@ SIGNATURES = {
     "frost_search_variance_grid": (C.c_int, [_vp, _sz, C.c_uint32, _u8p, C.POINTER(C.c_double), _sz]),
     "frost_search_capture_planes": (C.c_int, [_vp, C.c_int]),
     "frost_search_plane_data": (C.c_int, [_vp, _sz, _f32p, _sz]),
+    "frost_search_use_graphs": (C.c_int, [_vp, C.c_int]),
     "frost_search_enable_timing": (C.c_int, [_vp, C.c_int]),
     "frost_search_get_timing": (C.c_int, [_vp, C.POINTER(_abi.SearchTimingC)]),
     "frost_server_create": (C.c_int, [C.c_int, _sz, C.c_uint32, C.POINTER(_vp)]),

@@ -232,3 +232,4 @@ class BoxcarConfig:
     max_cands_per_dm: int = 4096
     skip_cold_prefix: bool = True
     storage: Storage = Storage.FP32
+    tile_nsamps: int = 0  # FDMT tile in samples (multiple of 4096); 0 = the whole gulp

@@ -506,6 +506,14 @@ int frost_server_get_stats(frost_server* s, frost_server_stats* out) {
     });
 }
 
+int frost_search_use_graphs(frost_search* s, int enable) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_use_graphs: null handle");
+        s->impl.use_graphs(enable != 0);
+    });
+}
+
 int frost_search_enable_timing(frost_search* s, int enable) {
     return guarded([&] {
         if (s == nullptr)

@@ -211,6 +211,8 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     const SizeType maxc = std::max<uint64_t>(bc.max_candidates, 1);
     m_cands.reserve(maxc * sizeof(frost_candidate));
     m_counters.reserve(4 * sizeof(unsigned long long));
+    m_clock.reserve(sizeof(GulpClock));
+    m_clock_h.reserve(sizeof(GulpClock));
     m_frontier.reserve(sizeof(unsigned long long));
     m_mask_d.reserve(C);
     m_mask_or_d.reserve(C);
@@ -239,6 +241,8 @@ Engine::~Engine() {
     if (m_stream != nullptr) {
         cudaSetDevice(m_device);
         cudaStreamSynchronize(m_stream);
+        if (m_graph != nullptr)
+            cudaGraphExecDestroy(m_graph);
         for (auto e : m_event_pool)
             cudaEventDestroy(e);
         cudaStreamDestroy(m_stream);
@@ -354,7 +358,7 @@ LevelView Engine::view(int h) const {
     return LevelView{m_buf[m_buf_of[h]].get(), m_pitch, m_base, m_fp16 ? 1 : 0};
 }
 
-SearchParams Engine::params(int64_t tile_t0, int64_t gulp_t0, int32_t n_valid, bool or_active) const {
+SearchParams Engine::params(int64_t tile_off, int32_t n_valid) const {
     SearchParams p{};
     p.rows         = m_rows.as<SearchRow>();
     p.planes       = m_planes.as<PlaneInfo>();
@@ -367,9 +371,8 @@ SearchParams Engine::params(int64_t tile_t0, int64_t gulp_t0, int32_t n_valid, b
     p.peak_mode    = m_cfg.peak_mode;
     p.trapezoid    = m_cfg.use_trapezoid ? 1 : 0;
     p.skip_cold    = m_cfg.skip_cold_prefix ? 1 : 0;
-    p.or_active    = or_active ? 1 : 0;
-    p.tile_t0      = tile_t0;
-    p.gulp_t0      = gulp_t0;
+    p.clock        = m_clock.as<GulpClock>();
+    p.tile_off     = tile_off;
     p.n_valid      = n_valid;
     p.inv_sigma    = m_inv.as<float>();
     p.inv_sigma_or = m_inv_or.as<float>();
@@ -435,8 +438,6 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
         FB_CUDA(cudaMemcpyAsync(m_wf_stage.get(), waterfall, bytes, cudaMemcpyHostToDevice, s));
         wf = m_wf_stage.as<float>();
     }
-    FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, 4 * sizeof(unsigned long long), s));
-    FB_CUDA(cudaMemsetAsync(m_row_counts.get(), 0, m_nsearch * sizeof(uint32_t), s));
     if (m_capture_on) {
         const auto& planes = m_plan.planes();
         m_capture.resize(planes.size());
@@ -444,14 +445,63 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
         for (size_t p = 0; p < planes.size(); ++p)
             m_capture[p].reserve(std::max<SizeType>(planes[p].delay.size() * nsamps * sizeof(float), 16));
     }
+    // The gulp's start and mask change, read by the search from device memory.
+    {
+        auto* ck      = m_clock_h.as<GulpClock>();
+        ck->gulp_t0   = static_cast<int64_t>(m_samples);
+        ck->or_active = or_active ? 1 : 0;
+        ck->pad       = 0;
+        FB_CUDA(cudaMemcpyAsync(m_clock.get(), ck, sizeof(GulpClock), cudaMemcpyHostToDevice, s));
+    }
+    const uint64_t before = m_launches; // the variance update's
+    if (m_graphs_on && !m_timing_on && !m_capture_on) {
+        if (m_graph == nullptr || m_graph_wf != wf || m_graph_nsamps != nsamps) {
+            if (m_graph != nullptr) {
+                FB_CUDA(cudaGraphExecDestroy(m_graph));
+                m_graph = nullptr;
+            }
+            cudaGraph_t graph = nullptr;
+            FB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                run_tiles(wf, nsamps, s);
+            } catch (...) {
+                cudaStreamEndCapture(s, &graph);
+                if (graph != nullptr)
+                    cudaGraphDestroy(graph);
+                throw;
+            }
+            FB_CUDA(cudaStreamEndCapture(s, &graph));
+            const cudaError_t e = cudaGraphInstantiate(&m_graph, graph, 0);
+            cudaGraphDestroy(graph);
+            FB_CUDA(e);
+            m_graph_wf       = wf;
+            m_graph_nsamps   = nsamps;
+            m_graph_launches = m_launches - before;
+        }
+        FB_CUDA(cudaGraphLaunch(m_graph, s));
+        m_launches = before + m_graph_launches;
+    } else {
+        run_tiles(wf, nsamps, s);
+    }
+    m_samples += nsamps;
+    m_mask = cur;
+    collect(s);
+    m_timing.total_launches += m_launches;
+    m_timing.executes += 1;
+    harvest();
+}
+
+void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
+    FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, 4 * sizeof(unsigned long long), s));
+    FB_CUDA(cudaMemsetAsync(m_row_counts.get(), 0, m_nsearch * sizeof(uint32_t), s));
 
     const int L          = m_plan.levels();
-    const int64_t gulp0  = static_cast<int64_t>(m_samples);
+    const int32_t C      = m_plan.nchans();
     const auto& planes   = m_plan.planes();
     const uint64_t es    = m_fp16 ? 2 : 4;
     for (int64_t t_off = 0; t_off < static_cast<int64_t>(nsamps); t_off += m_tile) {
         const int32_t n_valid = static_cast<int32_t>(std::min<int64_t>(m_tile, nsamps - t_off));
-        const SearchParams sp = params(gulp0 + t_off, gulp0, n_valid, or_active);
+        const SearchParams sp = params(t_off, n_valid);
         for (size_t si = 0; si < m_steps.size(); ++si) {
             const Step& st      = m_steps[si];
             const int h         = st.out;
@@ -521,12 +571,6 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
             launch_save_history(view(L), m_plan.level_rows(L), m_hist_len[L], n_valid, m_hist[L].get(), s);
         });
     }
-    m_samples += nsamps;
-    m_mask = cur;
-    collect(s);
-    m_timing.total_launches += m_launches;
-    m_timing.executes += 1;
-    harvest();
 }
 
 void Engine::collect(cudaStream_t s) {
@@ -561,7 +605,7 @@ void Engine::drain() {
     cudaStream_t s = m_stream;
     FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, 4 * sizeof(unsigned long long), s));
     FB_CUDA(cudaMemsetAsync(m_row_counts.get(), 0, m_nsearch * sizeof(uint32_t), s));
-    const SearchParams sp = params(static_cast<int64_t>(m_samples), static_cast<int64_t>(m_samples), 0, false);
+    const SearchParams sp = params(0, 0); // k_flush only emits the carried runs
     launch_flush_runs(sp, static_cast<int64_t>(m_nsearch), s);
     collect(s);
 }

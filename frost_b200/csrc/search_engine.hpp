@@ -105,7 +105,24 @@ private:
 
     SizeType plan_bytes(int64_t tile) const;
     void allocate(int64_t tile);
-    SearchParams params(int64_t tile_t0, int64_t gulp_t0, int32_t n_valid, bool or_active) const;
+    SearchParams params(int64_t tile_off, int32_t n_valid) const;
+    /** The per-gulp launch sequence (memsets, every tile's FDMT steps,
+     * history copies and searches) for a waterfall at `wf`. */
+    void run_tiles(const float* wf, SizeType nsamps, cudaStream_t s);
+    // The sequence captured as a CUDA graph, replayed while the waterfall
+    // address and length stay the same (timing and plane capture launch
+    // directly).
+    cudaGraphExec_t m_graph     = nullptr;
+    const float* m_graph_wf     = nullptr;
+    SizeType m_graph_nsamps     = 0;
+    uint64_t m_graph_launches   = 0;
+    bool m_graphs_on            = true;
+    DeviceBuffer m_clock;       // GulpClock read by the search
+    PinnedBuffer m_clock_h;
+  public:
+    /** Enables (default) or disables graph capture of the launch sequence. */
+    void use_graphs(bool on) { m_graphs_on = on; }
+  private:
     LevelView view(int h) const;
     void update_variance(const std::vector<uint8_t>& cur, const std::vector<uint8_t>& orm);
     void collect(cudaStream_t s);

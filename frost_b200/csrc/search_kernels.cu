@@ -82,6 +82,9 @@ __device__ void scan_inplace(float* a, int n) {
 
 /** Per-row constants, in shared memory. */
 struct RowConst {
+    int64_t tile_t0;  // absolute sample of tile column 0
+    int64_t gulp_t0;  // absolute sample of the gulp's first column
+    int32_t or_active;
     int W[kMaxWidths];
     int E[kMaxWidths];      // trapezoid half-weight edge, 0 for a boxcar
     float inv[kMaxWidths];  // 1/sigma
@@ -112,10 +115,10 @@ __device__ __forceinline__ float snr_general(const SearchParams& p, const RowCon
     if (col >= p.n_valid)
         return FB_NEG_INF;
     const int W     = rc.W[wi];
-    const int64_t t = p.tile_t0 + col;
+    const int64_t t = rc.tile_t0 + col;
     if (p.skip_cold && t < static_cast<int64_t>(delay) + W - 1)
         return FB_NEG_INF;
-    const bool use_or = p.or_active && (t - p.gulp_t0) < static_cast<int64_t>(delay) + W - 1;
+    const bool use_or = rc.or_active && (t - rc.gulp_t0) < static_cast<int64_t>(delay) + W - 1;
     const float inv   = use_or ? rc.inv_or[wi] : rc.inv[wi];
     if (inv == 0.0F)
         return FB_NEG_INF;
@@ -230,7 +233,7 @@ __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float
                     }
                 }
             }
-            const int64_t t = p.tile_t0 + col;
+            const int64_t t = rc.tile_t0 + col;
             if (run.open && col == last + 1) {
                 if (best > run.best) {
                     run.best   = best;
@@ -288,8 +291,13 @@ __global__ void __launch_bounds__(kThreads, 4)
     const int halo      = p.halo;
     const bool across   = p.peak_mode == FROST_PEAK_ACROSS_WIDTHS;
     const bool all      = p.peak_mode == FROST_PEAK_ALL;
-    if (threadIdx.x == 0)
-        local_count = p.row_counts[g];
+    if (threadIdx.x == 0) {
+        local_count  = p.row_counts[g];
+        const GulpClock ck = *p.clock;
+        rc.gulp_t0   = ck.gulp_t0;
+        rc.tile_t0   = ck.gulp_t0 + p.tile_off;
+        rc.or_active = ck.or_active;
+    }
     if (threadIdx.x < nw) {
         const int w    = threadIdx.x;
         const int W    = p.widths[w];
@@ -411,8 +419,8 @@ __global__ void __launch_bounds__(kThreads, 4)
         }
         __syncthreads();
 
-        const bool fast = c0 + kChunk <= p.n_valid && (!p.skip_cold || p.tile_t0 + c0 >= warm) &&
-                          (!p.or_active || p.tile_t0 + c0 - p.gulp_t0 >= warm);
+        const bool fast = c0 + kChunk <= p.n_valid && (!p.skip_cold || rc.tile_t0 + c0 >= warm) &&
+                          (!rc.or_active || rc.tile_t0 + c0 - rc.gulp_t0 >= warm);
         if (fast) {
             // ---- steady state. Group gi = samples 4 gi .. 4 gi + 3. A window
             // sum Q[k] - Q[k - W] of the group is at most gmax(group) minus
@@ -532,7 +540,7 @@ __global__ void __launch_bounds__(kThreads, 4)
                         RunState r{};
                         r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
                         r.best_w = wi;
-                        r.start = r.best_t = r.last_t = p.tile_t0 + c0 + k;
+                        r.start = r.best_t = r.last_t = rc.tile_t0 + c0 + k;
                         emit(p, row, r, &local_count);
                     }
                 }

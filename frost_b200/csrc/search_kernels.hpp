@@ -48,6 +48,14 @@ struct RunState {
     int64_t last_t;
 };
 
+/** The per-gulp times the search reads from device memory, so that one
+ * captured launch sequence (a CUDA graph) serves every gulp. */
+struct GulpClock {
+    int64_t gulp_t0;   // absolute sample of the gulp's first column
+    int32_t or_active; // this gulp's mask differs from the previous one
+    int32_t pad;
+};
+
 struct SearchParams {
     const SearchRow* rows;   // indexed by global searched-row g
     const PlaneInfo* planes;
@@ -59,9 +67,8 @@ struct SearchParams {
     int32_t peak_mode;       // enum frost_peak_mode
     int32_t trapezoid;
     int32_t skip_cold;
-    int32_t or_active;       // this gulp's mask differs from the previous one
-    int64_t tile_t0;         // absolute sample of tile column 0
-    int64_t gulp_t0;         // absolute sample of the gulp's first column
+    const GulpClock* clock;  // gulp start and mask change (device)
+    int64_t tile_off;        // tile column 0 relative to the gulp start
     int32_t n_valid;         // valid columns in this tile
     const float* inv_sigma;  // [g][nwidths]
     const float* inv_sigma_or;

@@ -63,7 +63,7 @@ def _boxcar_c(bc: BoxcarConfig, tile_nsamps: int = 0) -> _abi.BoxcarConfigC:
     c.input_nbits = 32
     c.input_mean = 0.0
     c.storage = int(bc.storage)
-    c.tile_nsamps = int(tile_nsamps)
+    c.tile_nsamps = int(tile_nsamps or bc.tile_nsamps)
     return c
 
 
@@ -180,6 +180,10 @@ class FDMTBoxcar:
         check(lib().frost_search_variance_grid(self._h, plane, width, mp,
                                                out.ctypes.data_as(C.POINTER(C.c_double)), ndm))
         return out
+
+    def use_graphs(self, enable: bool = True):
+        """CUDA-graph replay of the per-gulp launch sequence (default on)."""
+        check(lib().frost_search_use_graphs(self._h, 1 if enable else 0))
 
     def enable_timing(self, enable: bool = True):
         check(lib().frost_search_enable_timing(self._h, int(enable)))

@@ -480,6 +480,14 @@ typedef struct {
     uint64_t executes;
 } frost_search_timing;
 
+/* No counterpart in the reference (dmt launches per call). With `enable`
+ * (the default) the engine captures its per-gulp launch sequence (FDMT
+ * steps, history copies, searches) as a CUDA graph on the first gulp and
+ * replays it while the waterfall's address and length stay the same; the
+ * gulp start and mask-change flag are read from device memory. Timing and
+ * plane capture launch directly. Results are the same either way. */
+int frost_search_use_graphs(frost_search* s, int enable);
+
 /* Enables (and zeroes) or disables per-phase timing. */
 int frost_search_enable_timing(frost_search* s, int enable);
 int frost_search_get_timing(const frost_search* s, frost_search_timing* out);

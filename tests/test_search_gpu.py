@@ -178,3 +178,86 @@ def test_variance_grid_matches_oracle_and_errors():
         eng.execute(np.zeros((pc.nchans, pc.block_nsamps + 1), np.float32))
     info = eng.info()
     assert info["nplanes"] == 11 and info["dt_max"] > 0
+
+
+def test_precision_variant_trapezoid_fifty_pulses_near_threshold():
+    """The precision variant at test scale: trapezoid filters, fp16 planes
+    with float accumulation, FP64 variances, 50 pulses at S/N 6-12. Every
+    DM-time plane's error against the FP64 oracle is reported (fp32 and
+    fp16), and the fp16 candidate list above S/N 7 equals the fp32 one
+    (up to detections within the stated fp16 S/N error of 7)."""
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(nchans=128, gulp=8192, depth=2, dm_max=80.0)
+    rng = np.random.default_rng(404)
+    C = pc.nchans
+    pulses = []
+    for _ in range(50):
+        w = float(rng.uniform(1.0, 16.0))
+        snr = float(rng.uniform(6.0, 12.0))
+        pulses.append((float(rng.uniform(2500, 3 * pc.block_nsamps - 200)), float(rng.uniform(2.0, 80.0)),
+                       w, snr / np.sqrt(C * max(1.0, 1.064 * w))))
+    stream = make_stream(pc, 3, seed=404, pulses=pulses)
+    kw = dict(max_boxcar=32, detect_thresh=6.0, use_trapezoid=True)
+    e32 = FDMTBoxcar(pc, BoxcarConfig(**kw))
+    e16 = FDMTBoxcar(pc, BoxcarConfig(storage=Storage.FP16, **kw))
+    e32.capture_planes(True)
+    e16.capture_planes(True)
+    c32 = run_engine(e32, stream, pc.block_nsamps)
+    c16 = run_engine(e16, stream, pc.block_nsamps)
+    orc = oracle_for(pc, BoxcarConfig(**kw))
+    print("\nplane  fp32 max|err|/rms  fp16 max|err|/rms  fp16 rms(err)/rms")
+    w32 = w16 = 0.0
+    for p, band in enumerate(orc.bands):
+        rows = orc.dedisperse(stream, band)[:, -pc.block_nsamps:]
+        rms = np.sqrt(np.mean(rows ** 2, axis=1, keepdims=True)) + 1e-12
+        d32 = np.abs(e32.plane_data(p, pc.block_nsamps) - rows) / rms
+        d16 = np.abs(e16.plane_data(p, pc.block_nsamps) - rows) / rms
+        print(f"{p:5d}  {d32.max():17.2e}  {d16.max():17.2e}  {np.sqrt(np.mean(d16 ** 2)):17.2e}")
+        w32, w16 = max(w32, float(d32.max())), max(w16, float(d16.max()))
+    assert w32 < 1e-5 and w16 < 1e-2, (w32, w16)
+    ref = orc.search(stream, pc.block_nsamps, [np.ones(C, np.uint8)] * 3)
+    n, missing, extra, bad = compare(c32, ref, 6.0)
+    assert n > 20 and not missing and not extra and not bad, (missing[:3], extra[:3], bad[:3])
+
+    def above7(cs):
+        return {(int(c["subband_level"]), int(c["subband_idx"]), int(c["dm_idx"]), int(c["filter_idx"]),
+                 int(c["peak_sample"])): float(c["snr"]) for c in cs if c["snr"] >= 7.0}
+    a32, a16 = above7(c32), above7(c16)
+    errs = [abs(a16[k] - v) / v for k, v in a32.items() if k in a16]
+    tol = max(errs) if errs else 0.0
+    only32 = [(k, v) for k, v in a32.items() if k not in a16 and abs(v - 7.0) > 7.0 * max(tol, 1e-3) * 2]
+    only16 = [(k, v) for k, v in a16.items() if k not in a32 and abs(v - 7.0) > 7.0 * max(tol, 1e-3) * 2]
+    print(f"above S/N 7: fp32 {len(a32)}, fp16 {len(a16)}, shared {len(errs)}, max S/N error {tol:.2e}")
+    assert tol < 1e-2
+    # a peak may move by a sample inside its run (a near tie); such pairs
+    # share their run and are not counted as missing
+    def moved(k, other):
+        return any(k2[:4] == k[:4] and abs(k2[4] - k[4]) <= 2 for k2 in other)
+    assert not [x for x in only32 if not moved(x[0], a16)], only32[:5]
+    assert not [x for x in only16 if not moved(x[0], a32)], only16[:5]
+
+
+def test_graph_replay_matches_direct_launches():
+    """The per-gulp launch sequence captured once as a CUDA graph and
+    replayed gives the candidates of direct launches, across mask changes
+    (the OR-mask window), a short last gulp (a new capture) and drain."""
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=2, gulp=8192)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0, storage=Storage.FP16)
+    stream = make_stream(pc, 4, seed=77, pulses=PULSES)
+    rng = np.random.default_rng(8)
+    masks = [np.ones(pc.nchans, np.uint8)] + [(rng.random(pc.nchans) > 0.1).astype(np.uint8) for _ in range(3)]
+    outs = []
+    for graphs in (True, False):
+        eng = FDMTBoxcar(pc, bc)
+        eng.use_graphs(graphs)
+        got = []
+        for g in range(4):
+            n = pc.block_nsamps if g < 3 else pc.block_nsamps - 1000
+            wf = np.ascontiguousarray(stream[:, g * pc.block_nsamps:g * pc.block_nsamps + n] *
+                                      masks[g][:, None].astype(np.float32))
+            got.append(eng.execute(wf, masks[g]).candidates.copy())
+        got.append(eng.drain().candidates.copy())
+        outs.append(np.concatenate(got))
+    assert outs[0].size > 0
+    assert np.array_equal(outs[0], outs[1])

@@ -106,3 +106,52 @@ def test_admission_by_device_memory():
     second = srv.add_beam(rfi, layout, 1.0, plan, bc)
     assert srv.stats().beams == 1 and second != first
     srv.close()
+
+
+UNEVEN = [  # channels, dtype, gulp, DM max, sub-band depth (1 / 4 / 11 planes)
+    (1024, "uint8", 32768, 500.0, 0),
+    (2048, "float32", 32768, 800.0, 1),
+    (4096, "uint8", 32768, 500.0, 2),
+    (1024, "float32", 65536, 2500.0, 2),
+]
+
+
+def _uneven(i):
+    from frost_b200.config import BlockLayout, DataType
+    from frost_b200.pipeline import plan_for
+    C, dt, gulp, dm_max, depth = UNEVEN[i]
+    foff = -336.0 / C
+    fb = make_filterbank(C, gulp * 2, 1536.0 + foff / 2, foff, 64e-6, 500 + i, dtype=dt, n_pulses=2,
+                         dm_range=(50.0, dm_max * 0.8), snr_range=(15.0, 30.0),
+                         rfi_channel_fraction=0.02, n_bursts=1)
+    layout = BlockLayout(C, gulp, DataType.UINT8 if dt == "uint8" else DataType.FLOAT32, 64e-6,
+                         1536.0 + foff / 2, foff)
+    plan = plan_for(layout, 0.0, dm_max, subband_depth=depth)
+    return fb.data, layout, plan
+
+
+def test_uneven_beams_served_together_match_each_alone():
+    """Beams of different channel counts, sample types, gulp lengths, DM
+    ranges and plane counts (1, 4, 11) served together on one GPU give the
+    candidates each gives alone."""
+    from frost_b200.pipeline import GulpPipeline
+    from frost_b200.serve import BeamServer
+    bc = BoxcarConfig(max_boxcar=64, detect_thresh=7.0)
+    beams = [_uneven(i) for i in range(len(UNEVEN))]
+    alone = []
+    for data, layout, plan in beams:
+        p = GulpPipeline(RfiConfig(), layout, 1.0, plan, bc)
+        g = layout.max_nsamps
+        alone.append([p.execute(data[k * g:(k + 1) * g], g).candidates for k in range(2)] +
+                     [p.flush().candidates])
+    srv = BeamServer(slots=3)
+    ids = [srv.add_beam(RfiConfig(), layout, 1.0, plan, bc) for _, layout, plan in beams]
+    tickets = [[srv.submit(b, data[k * layout.max_nsamps:(k + 1) * layout.max_nsamps], layout.max_nsamps)
+                for k in range(2)] for b, (data, layout, _) in zip(ids, beams)]
+    for i, b in enumerate(ids):
+        for k, t in enumerate(tickets[i]):
+            cands, _ = srv.wait(t)
+            assert np.array_equal(cands, alone[i][k]), (i, k)
+        assert np.array_equal(srv.drain(b), alone[i][2]), i
+    assert sum(len(c) for per in alone for c in per) > 0
+    srv.close()
