@@ -506,6 +506,22 @@ int frost_server_get_stats(frost_server* s, frost_server_stats* out) {
     });
 }
 
+int frost_search_autotune(frost_search* s, int* fused, int* tiles_per_cta, double* ms, int* cached) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_autotune: null handle");
+        const auto t = s->impl.autotune();
+        if (fused != nullptr)
+            *fused = t.fuse ? 1 : 0;
+        if (tiles_per_cta != nullptr)
+            *tiles_per_cta = t.tiles_per_cta;
+        if (ms != nullptr)
+            *ms = t.ms;
+        if (cached != nullptr)
+            *cached = t.cached ? 1 : 0;
+    });
+}
+
 int frost_search_use_graphs(frost_search* s, int enable) {
     return guarded([&] {
         if (s == nullptr)

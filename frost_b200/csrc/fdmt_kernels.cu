@@ -189,7 +189,7 @@ __device__ __forceinline__ void merge8(const S* lo, const S* stage, int e, int o
 
 // ---- TMA-pipelined level kernel ------------------------------------------
 //
-// One CTA per (output row, run of kTilesPerCta time tiles). Thread 0 keeps
+// One CTA per (output row, run of `tpc` time tiles). Thread 0 keeps
 // kStages tiles in flight with 1-D bulk async copies (cp.async.bulk, local
 // global memory only, no multicast) of the unshifted child segment and the
 // 16-byte-aligned superset of the shifted one, each stage completing on its
@@ -198,14 +198,14 @@ __device__ __forceinline__ void merge8(const S* lo, const S* stage, int e, int o
 // *err and the CTA drains its copies (again bounded) and returns.
 
 constexpr int kStages      = 4;
-constexpr int kTilesPerCta = 16;
+constexpr int kTilesPerCta = 16; // default run of tiles per CTA (tunable per launch)
 using bulk::mbar_wait;
 
 template <class S>
 __global__ void __launch_bounds__(kThreads)
     k_level_pipe(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
                  int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                 int32_t ntiles, unsigned* __restrict__ err) {
+                 int32_t ntiles, int32_t tpc, unsigned* __restrict__ err) {
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -215,8 +215,8 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ int abort_flag;
 
     const RowOp op  = ops[blockIdx.x];
-    const int tile0 = blockIdx.y * kTilesPerCta;
-    const int nt    = min(kTilesPerCta, ntiles - tile0);
+    const int tile0 = blockIdx.y * tpc;
+    const int nt    = min(tpc, ntiles - tile0);
     if (nt <= 0)
         return;
     const bool has_hi = op.hi_row >= 0;
@@ -346,7 +346,7 @@ template <class S>
 __global__ void __launch_bounds__(kThreads)
     k_level2_pipe(const FusedOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
                   int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                  int32_t ntiles, unsigned* __restrict__ err) {
+                  int32_t ntiles, int32_t tpc, unsigned* __restrict__ err) {
     constexpr int NS        = kStages2<S>;
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
@@ -357,8 +357,8 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ int abort_flag;
 
     const FusedOp op = ops[blockIdx.x];
-    const int tile0  = blockIdx.y * kTilesPerCta;
-    const int nt     = min(kTilesPerCta, ntiles - tile0);
+    const int tile0  = blockIdx.y * tpc;
+    const int nt     = min(tpc, ntiles - tile0);
     if (nt <= 0)
         return;
     const S* rows[4];
@@ -604,13 +604,15 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
 }
 
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  unsigned* err, cudaStream_t s) {
+                  unsigned* err, cudaStream_t s, int32_t tpc) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
         out.pitch % 8 != 0 || in.fp16 != out.fp16)
         throw Error(FROST_ERR_INTERNAL, "level: bad geometry");
     const int ntiles = ncols / kTimePerCta;
+    if (tpc < 1 || tpc > 64)
+        throw Error(FROST_ERR_INTERNAL, "level: tiles per CTA must be in [1, 64]");
     if (err == nullptr) {
         // direct form (no bulk copies): one CTA per (row, tile)
         const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>(ntiles));
@@ -626,7 +628,7 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
         return;
     }
     const dim3 grid(static_cast<unsigned>(nrows),
-                    static_cast<unsigned>((ntiles + kTilesPerCta - 1) / kTilesPerCta));
+                    static_cast<unsigned>((ntiles + tpc - 1) / tpc));
     const size_t es   = out.fp16 ? 2 : 4;
     const size_t smem = kStages * (2 * kTimePerCta * es + 16);
     if (out.fp16) {
@@ -634,27 +636,29 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
                                      static_cast<int>(smem)));
         k_level_pipe<__half><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const __half*>(in.data), in.pitch, in.base,
-            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, err);
+            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, err);
     } else {
         FB_CUDA(cudaFuncSetAttribute(k_level_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         k_level_pipe<float><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const float*>(in.data), in.pitch, in.base,
-            static_cast<float*>(out.data), out.pitch, out.base, ntiles, err);
+            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, err);
     }
     FB_LAUNCH_CHECK();
 }
 
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                   unsigned* err, cudaStream_t s) {
+                   unsigned* err, cudaStream_t s, int32_t tpc) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
         out.pitch % 8 != 0 || in.fp16 != out.fp16 || err == nullptr)
         throw Error(FROST_ERR_INTERNAL, "level2: bad geometry");
+    if (tpc < 1 || tpc > 64)
+        throw Error(FROST_ERR_INTERNAL, "level2: tiles per CTA must be in [1, 64]");
     const int ntiles = ncols / kTimePerCta;
     const dim3 grid(static_cast<unsigned>(nrows),
-                    static_cast<unsigned>((ntiles + kTilesPerCta - 1) / kTilesPerCta));
+                    static_cast<unsigned>((ntiles + tpc - 1) / tpc));
     const size_t es = out.fp16 ? 2 : 4;
     if (out.fp16) {
         const size_t smem = kStages2<__half> * (4 * kTimePerCta * es + 48);
@@ -662,14 +666,14 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
                                      static_cast<int>(smem)));
         k_level2_pipe<__half><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const __half*>(in.data), in.pitch, in.base,
-            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, err);
+            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, err);
     } else {
         const size_t smem = kStages2<float> * (4 * kTimePerCta * es + 48);
         FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         k_level2_pipe<float><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const float*>(in.data), in.pitch, in.base,
-            static_cast<float*>(out.data), out.pitch, out.base, ntiles, err);
+            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, err);
     }
     FB_LAUNCH_CHECK();
 }

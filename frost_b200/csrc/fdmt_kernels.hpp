@@ -30,10 +30,11 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
                    LevelView out, int32_t ncols, cudaStream_t s);
 
 /** Level h >= 2: out[row] = in[lo] + in[hi] shifted. With `err` non-null
- * the TMA-pipelined kernel runs and sets *err if a bounded wait ran out;
- * with `err` null the direct (one CTA per row and tile) kernel runs. */
+ * the TMA-pipelined kernel runs (each CTA takes `tiles_per_cta` tiles of
+ * 2048 columns) and sets *err if a bounded wait ran out; with `err` null
+ * the direct (one CTA per row and tile) kernel runs. */
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  unsigned* err, cudaStream_t s);
+                  unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16);
 
 /** A row of level h+1 from four rows of level h-1: the sum of row[j] read at
  * t - shift[j] (shift[0] = 0), grouped (row0 + row1) + (row2 + row3); a
@@ -46,7 +47,7 @@ struct FusedOp {
 /** Level h+1 straight from level h-1 (TMA-pipelined; *err set if a bounded
  * wait ran out). */
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                   unsigned* err, cudaStream_t s);
+                   unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16);
 
 /** Copies the last `hist` columns ending at column base + n_valid of every
  * row of `view` into hist_buf[rows][hist]. */

@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "dedisp.hpp"
@@ -97,56 +99,7 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     }
     upload(m_row_ops, all_ops, s);
 
-    // FDMT schedule. Levels holding searched planes, level 1 and the top are
-    // stored; between them, a level whose successor is not stored is
-    // computed straight from the one below its predecessor (two levels in
-    // one pass, halving that pair's HBM traffic).
-    const auto& plan_planes = m_plan.planes();
-    std::vector<char> keep(L + 1, 0);
-    keep[1] = 1;
-    keep[L] = 1;
-    for (const auto& p : plan_planes)
-        keep[p.height] = 1;
-    m_buf_of.assign(L + 1, -1);
-    m_hist_len.assign(L + 1, 0);
-    m_hist_len[0] = m_plan.level_history(0);
-    m_steps.push_back({1, 0, false, 0});
-    m_buf_of[1] = 0;
-    std::vector<FusedOp> fused_all;
-    for (int h = 1; h < L;) {
-        Step st{};
-        if (h + 2 <= L && !keep[h + 1]) {
-            st = {h + 2, h, true, static_cast<int64_t>(fused_all.size())};
-            const auto& mid = m_plan.row_ops(h + 1);
-            for (const RowOp& op : m_plan.row_ops(h + 2)) {
-                const RowOp& a = mid[op.lo_row];
-                FusedOp f{{a.lo_row, a.hi_row, -1, -1}, {0, a.hi_row >= 0 ? a.shift : 0, 0, 0}};
-                if (op.hi_row >= 0) {
-                    const RowOp& b = mid[op.hi_row];
-                    f.row[2]       = b.lo_row;
-                    f.shift[2]     = op.shift;
-                    f.row[3]       = b.hi_row;
-                    f.shift[3]     = b.hi_row >= 0 ? op.shift + b.shift : 0;
-                }
-                for (int j = 1; j < 4; ++j)
-                    if (f.row[j] >= 0)
-                        m_hist_len[h] = std::max(m_hist_len[h], f.shift[j]);
-                fused_all.push_back(f);
-            }
-            h += 2;
-        } else {
-            st = {h + 1, h, false, m_row_op_offset[h + 1]};
-            for (const RowOp& op : m_plan.row_ops(h + 1))
-                if (op.hi_row >= 0)
-                    m_hist_len[h] = std::max(m_hist_len[h], op.shift);
-            h += 1;
-        }
-        m_buf_of[st.out] = static_cast<int>(m_steps.size() % 2);
-        m_steps.push_back(st);
-    }
-    for (const auto& p : plan_planes)
-        m_hist_len[p.height] = std::max(m_hist_len[p.height], m_plan.widths().back() - 1);
-    upload(m_fused_ops, fused_all, s);
+    build_schedule(true);
 
     // Searched rows, grouped by height.
     const auto& planes = m_plan.planes();
@@ -225,7 +178,7 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     tile = round_up(std::min<int64_t>(tile, static_cast<int64_t>(dd.block_nsamps)), kTileQuantum);
     size_t free_b = 0, total_b = 0;
     FB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const SizeType limit = memory_budget != 0 ? memory_budget
+    const SizeType limit = m_budget = memory_budget != 0 ? memory_budget
                                               : static_cast<SizeType>(0.85 * static_cast<double>(free_b));
     while (plan_bytes(tile) > limit && tile > kTileQuantum)
         tile = round_up(tile / 2, kTileQuantum);
@@ -235,6 +188,155 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
                         " device bytes at the smallest tile; budget " + std::to_string(limit));
     allocate(tile);
     FB_CUDA(cudaStreamSynchronize(s));
+}
+
+// FDMT schedule. Levels holding searched planes, level 1 and the top are
+// stored; with `fuse`, a level whose successor is not stored is computed
+// straight from the one below its predecessor (two levels in one pass,
+// halving that pair's HBM traffic).
+void Engine::build_schedule(bool fuse) {
+    const int L             = m_plan.levels();
+    const auto& plan_planes = m_plan.planes();
+    std::vector<char> keep(L + 1, 0);
+    keep[1] = 1;
+    keep[L] = 1;
+    for (const auto& p : plan_planes)
+        keep[p.height] = 1;
+    m_steps.clear();
+    m_buf_of.assign(L + 1, -1);
+    m_hist_len.assign(L + 1, 0);
+    m_hist_len[0] = m_plan.level_history(0);
+    m_steps.push_back({1, 0, false, 0});
+    m_buf_of[1] = 0;
+    std::vector<FusedOp> fused_all;
+    for (int h = 1; h < L;) {
+        Step st{};
+        if (fuse && h + 2 <= L && !keep[h + 1]) {
+            st = {h + 2, h, true, static_cast<int64_t>(fused_all.size())};
+            const auto& mid = m_plan.row_ops(h + 1);
+            for (const RowOp& op : m_plan.row_ops(h + 2)) {
+                const RowOp& a = mid[op.lo_row];
+                FusedOp f{{a.lo_row, a.hi_row, -1, -1}, {0, a.hi_row >= 0 ? a.shift : 0, 0, 0}};
+                if (op.hi_row >= 0) {
+                    const RowOp& b = mid[op.hi_row];
+                    f.row[2]       = b.lo_row;
+                    f.shift[2]     = op.shift;
+                    f.row[3]       = b.hi_row;
+                    f.shift[3]     = b.hi_row >= 0 ? op.shift + b.shift : 0;
+                }
+                for (int j = 1; j < 4; ++j)
+                    if (f.row[j] >= 0)
+                        m_hist_len[h] = std::max(m_hist_len[h], f.shift[j]);
+                fused_all.push_back(f);
+            }
+            h += 2;
+        } else {
+            st = {h + 1, h, false, m_row_op_offset[h + 1]};
+            for (const RowOp& op : m_plan.row_ops(h + 1))
+                if (op.hi_row >= 0)
+                    m_hist_len[h] = std::max(m_hist_len[h], op.shift);
+            h += 1;
+        }
+        m_buf_of[st.out] = static_cast<int>(m_steps.size() % 2);
+        m_steps.push_back(st);
+    }
+    for (const auto& p : plan_planes)
+        m_hist_len[p.height] = std::max(m_hist_len[p.height], m_plan.widths().back() - 1);
+    upload(m_fused_ops, fused_all, m_stream);
+    m_fuse = fuse;
+    if (m_graph != nullptr) {
+        cudaGraphExecDestroy(m_graph);
+        m_graph = nullptr;
+    }
+}
+
+// ---- autotuning -----------------------------------------------------------
+//
+// The FDMT launch shape is measured, not assumed: for this plan's geometry
+// the engine times one tile pass for every candidate (fused two-level steps
+// or single levels; 4, 8, 16 or 32 tiles of 2048 columns per level-kernel
+// CTA) on a zero waterfall, keeps the fastest and caches it for the
+// process by geometry, then restores a fresh stream state.
+namespace {
+struct TuneChoice {
+    bool fuse;
+    int32_t tpc;
+    double ms;
+};
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice> g_tune_cache;
+} // namespace
+
+Engine::Tuned Engine::autotune() {
+    DeviceGuard g(m_device);
+    const bool timing_was = m_timing_on;
+    m_timing_on           = false;
+    cudaStream_t s = m_stream;
+    std::string key = std::to_string(m_plan.nchans()) + "|" + std::to_string(m_ncols) + "|" +
+                      std::to_string(m_fp16) + "|" + std::to_string(m_plan.widths().back());
+    for (int h = 1; h <= m_plan.levels(); ++h)
+        key += "|" + std::to_string(m_plan.level_rows(h));
+    for (const auto& p : m_plan.planes())
+        key += "|p" + std::to_string(p.height);
+    TuneChoice best{true, 16, 0.0};
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            best   = it->second;
+            cached = true;
+        }
+    }
+    if (!cached) {
+        const int32_t C      = m_plan.nchans();
+        const SizeType ncols = std::min<SizeType>(m_plan.config().block_nsamps, 4096);
+        DeviceBuffer wf;
+        wf.reserve(static_cast<SizeType>(C) * ncols * sizeof(float));
+        FB_CUDA(cudaMemsetAsync(wf.get(), 0, static_cast<SizeType>(C) * ncols * sizeof(float), s));
+        FB_CUDA(cudaMemsetAsync(m_inv.get(), 0, m_inv.bytes(), s));
+        FB_CUDA(cudaMemsetAsync(m_inv_or.get(), 0, m_inv_or.bytes(), s));
+        auto* ck = m_clock_h.as<GulpClock>();
+        *ck      = GulpClock{0, 0, 0};
+        FB_CUDA(cudaMemcpyAsync(m_clock.get(), ck, sizeof(GulpClock), cudaMemcpyHostToDevice, s));
+        cudaEvent_t a, b;
+        FB_CUDA(cudaEventCreate(&a));
+        FB_CUDA(cudaEventCreate(&b));
+        best.ms = -1.0;
+        for (const bool fuse : {true, false}) {
+            build_schedule(fuse);
+            if (plan_bytes(m_tile) > m_budget)
+                continue;
+            allocate(m_tile);
+            for (const int32_t tpc : {4, 8, 16, 32}) {
+                m_level_tpc = tpc;
+                run_tiles(wf.as<float>(), ncols, s); // warm-up
+                FB_CUDA(cudaEventRecord(a, s));
+                run_tiles(wf.as<float>(), ncols, s);
+                FB_CUDA(cudaEventRecord(b, s));
+                FB_CUDA(cudaEventSynchronize(b));
+                float ms = 0.0F;
+                FB_CUDA(cudaEventElapsedTime(&ms, a, b));
+                if (best.ms < 0.0 || ms < best.ms)
+                    best = {fuse, tpc, ms};
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    // apply the choice and start the stream afresh
+    build_schedule(best.fuse);
+    allocate(m_tile);
+    m_level_tpc = best.tpc;
+    m_samples   = 0;
+    m_var_ready = false;
+    const SizeType nruns = m_cfg.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : m_plan.widths().size();
+    FB_CUDA(cudaMemsetAsync(m_carry.get(), 0, m_nsearch * nruns * sizeof(RunState), s));
+    FB_CUDA(cudaStreamSynchronize(s));
+    m_timing_on = timing_was;
+    return Tuned{best.fuse, best.tpc, best.ms, cached};
 }
 
 Engine::~Engine() {
@@ -293,15 +395,23 @@ void Engine::harvest() {
     m_events_used = 0;
 }
 
+int32_t Engine::level_base(int h) const {
+    int64_t need = m_hist_len[h];
+    if (m_height_g1[h] > m_height_g0[h])
+        need = std::max<int64_t>(need, search_halo(m_plan.widths().back()));
+    return static_cast<int32_t>(round_up(need, 8));
+}
+
 SizeType Engine::plan_bytes(int64_t tile) const {
-    const SizeType es    = m_fp16 ? 2 : 4;
-    const int L          = m_plan.levels();
-    int32_t maxh         = 0;
+    const SizeType es   = m_fp16 ? 2 : 4;
+    const int L         = m_plan.levels();
+    const int64_t ncols = round_up(tile, kTileQuantum);
+    SizeType buf[2]     = {0, 0};
     for (int h = 1; h <= L; ++h)
-        maxh = std::max(maxh, m_hist_len[h]);
-    const int64_t base   = round_up(std::max<int64_t>(maxh, search_halo(m_plan.widths().back())), 8);
-    const int64_t pitch  = base + round_up(tile, kTileQuantum);
-    SizeType bytes       = 2 * static_cast<SizeType>(m_plan.max_level_rows()) * pitch * es;
+        if (m_buf_of[h] >= 0)
+            buf[m_buf_of[h]] = std::max<SizeType>(
+                buf[m_buf_of[h]], static_cast<SizeType>(m_plan.level_rows(h)) * (level_base(h) + ncols) * es);
+    SizeType bytes = buf[0] + buf[1];
     for (int h = 1; h <= L; ++h)
         bytes += static_cast<SizeType>(m_plan.level_rows(h)) * m_hist_len[h] * es;
     bytes += 2 * static_cast<SizeType>(m_plan.nchans()) * m_plan.level_history(0) * sizeof(float);
@@ -313,17 +423,22 @@ SizeType Engine::plan_bytes(int64_t tile) const {
 void Engine::allocate(int64_t tile) {
     const SizeType es = m_fp16 ? 2 : 4;
     const int L       = m_plan.levels();
-    int32_t maxh      = 0;
-    for (int h = 1; h <= L; ++h)
-        maxh = std::max(maxh, m_hist_len[h]);
-    m_tile  = tile;
-    m_ncols = round_up(tile, kTileQuantum);
-    m_base  = static_cast<int32_t>(round_up(std::max<int64_t>(maxh, search_halo(m_plan.widths().back())), 8));
-    m_pitch = m_base + m_ncols;
-    const SizeType buf = static_cast<SizeType>(m_plan.max_level_rows()) * m_pitch * es;
-    for (auto& b : m_buf) {
-        b.reserve(buf);
-        FB_CUDA(cudaMemsetAsync(b.get(), 0, buf, m_stream));
+    m_tile            = tile;
+    m_ncols           = round_up(tile, kTileQuantum);
+    m_base_of.assign(L + 1, 0);
+    m_pitch_of.assign(L + 1, 0);
+    SizeType buf[2] = {16, 16};
+    for (int h = 1; h <= L; ++h) {
+        if (m_buf_of[h] < 0)
+            continue;
+        m_base_of[h]  = level_base(h);
+        m_pitch_of[h] = m_base_of[h] + m_ncols;
+        buf[m_buf_of[h]] = std::max<SizeType>(buf[m_buf_of[h]],
+                                              static_cast<SizeType>(m_plan.level_rows(h)) * m_pitch_of[h] * es);
+    }
+    for (int i = 0; i < 2; ++i) {
+        m_buf[i].reserve(buf[i]);
+        FB_CUDA(cudaMemsetAsync(m_buf[i].get(), 0, buf[i], m_stream));
     }
     m_hist.clear();
     m_hist.resize(L + 1);
@@ -355,7 +470,7 @@ SizeType Engine::device_bytes() const {
 }
 
 LevelView Engine::view(int h) const {
-    return LevelView{m_buf[m_buf_of[h]].get(), m_pitch, m_base, m_fp16 ? 1 : 0};
+    return LevelView{m_buf[m_buf_of[h]].get(), m_pitch_of[h], m_base_of[h], m_fp16 ? 1 : 0};
 }
 
 SearchParams Engine::params(int64_t tile_off, int32_t n_valid) const {
@@ -528,10 +643,10 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                 timed(kLevel, s, [&] {
                     if (st.fused)
                         launch_level2(m_fused_ops.as<FusedOp>() + st.op_offset, m_plan.level_rows(h),
-                                      view(st.in), out, static_cast<int32_t>(m_ncols), err, s);
+                                      view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc);
                     else
                         launch_level(m_row_ops.as<RowOp>() + st.op_offset, m_plan.level_rows(h),
-                                     view(st.in), out, static_cast<int32_t>(m_ncols), err, s);
+                                     view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc);
                 });
                 m_launches += 1;
                 m_timing.level_launches += 1;

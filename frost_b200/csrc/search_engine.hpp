@@ -65,8 +65,13 @@ private:
     int m_device;
     cudaStream_t m_stream = nullptr;
     bool m_fp16;
-    int64_t m_tile = 0, m_ncols = 0, m_pitch = 0;
-    int32_t m_base = 0;
+    int64_t m_tile = 0, m_ncols = 0;
+    // Per stored level: history columns before base (the level's own
+    // history, or the search halo for searched levels) and the row pitch.
+    std::vector<int32_t> m_base_of;
+    std::vector<int64_t> m_pitch_of;
+    /** Level h's base column for a tile of ncols columns. */
+    int32_t level_base(int h) const;
     SizeType m_nsearch = 0; // searched rows over all planes
     std::vector<int64_t> m_height_g0, m_height_g1; // searched rows per height
     std::vector<int32_t> m_node_first_op;
@@ -90,6 +95,21 @@ private:
     std::vector<int> m_buf_of;         // level -> level buffer (-1: not stored)
     std::vector<int32_t> m_hist_len;   // level -> history columns kept
     DeviceBuffer m_fused_ops;
+    bool m_fuse        = true; // fused two-level steps in the schedule
+    int32_t m_level_tpc = 16;  // tiles of 2048 columns per level-kernel CTA
+    void build_schedule(bool fuse);
+    SizeType m_budget = 0; // device memory budget of the plan
+  public:
+    struct Tuned {
+        bool fuse;
+        int32_t tiles_per_cta;
+        double ms;   // one tile pass with the choice (0 if taken from the cache)
+        bool cached;
+    };
+    /** Measures the FDMT launch shapes for this geometry, applies the fastest
+     * and restarts the stream (call before the first gulp). */
+    Tuned autotune();
+  private:
     std::vector<DeviceBuffer> m_capture;
     bool m_capture_on = false;
     int64_t m_capture_cols = 0;

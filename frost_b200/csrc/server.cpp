@@ -97,6 +97,7 @@ uint32_t Server::add_beam(const BeamSpec& spec) {
     auto beam = std::make_unique<Beam>(spec, m_device);
     // every steady-state buffer is allocated now, so the charge is the
     // beam's footprint (plus a margin for small per-gulp transfers)
+    beam->autotune();
     beam->preallocate();
     const SizeType need = beam->device_bytes() + (SizeType{16} << 20);
     std::lock_guard<std::mutex> lk(m_mu);

@@ -37,6 +37,9 @@ public:
     Beam(const BeamSpec& spec, int device);
     /** Allocates the beam's steady-state device buffers up front. */
     void preallocate() { m_cleaner->preallocate(); }
+    /** Picks the engine's FDMT launch shape by measurement (cached per
+     * geometry, so only the first beam of a shape pays). */
+    void autotune() { m_engine->autotune(); }
     /** Cleans and searches one gulp (a block of max_nsamps rows, nread
      * valid, on the host or on the beam's device). */
     void process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device);

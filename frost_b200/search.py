@@ -181,6 +181,14 @@ class FDMTBoxcar:
                                                out.ctypes.data_as(C.POINTER(C.c_double)), ndm))
         return out
 
+    def autotune(self) -> dict:
+        """Measures and applies the fastest FDMT launch shape for this
+        geometry (call before the first gulp)."""
+        f, t, c = C.c_int(), C.c_int(), C.c_int()
+        ms = C.c_double()
+        check(lib().frost_search_autotune(self._h, C.byref(f), C.byref(t), C.byref(ms), C.byref(c)))
+        return {"fused": bool(f.value), "tiles_per_cta": t.value, "ms": ms.value, "cached": bool(c.value)}
+
     def use_graphs(self, enable: bool = True):
         """CUDA-graph replay of the per-gulp launch sequence (default on)."""
         check(lib().frost_search_use_graphs(self._h, 1 if enable else 0))

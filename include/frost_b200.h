@@ -488,6 +488,14 @@ typedef struct {
  * plane capture launch directly. Results are the same either way. */
 int frost_search_use_graphs(frost_search* s, int enable);
 
+/* No counterpart in the reference. Measures this geometry's FDMT launch
+ * shapes (fused two-level steps or single levels; 4, 8, 16 or 32 tiles of
+ * 2048 samples per level-kernel CTA) with one tile pass each on a zero
+ * waterfall, applies the fastest and restarts the stream; results are
+ * cached per process by geometry. Call before the first gulp. Any output
+ * pointer may be NULL. */
+int frost_search_autotune(frost_search* s, int* fused, int* tiles_per_cta, double* ms, int* cached);
+
 /* Enables (and zeroes) or disables per-phase timing. */
 int frost_search_enable_timing(frost_search* s, int enable);
 int frost_search_get_timing(const frost_search* s, frost_search_timing* out);
@@ -522,9 +530,10 @@ int frost_server_create(int device, size_t memory_budget, uint32_t slots, frost_
 int frost_server_destroy(frost_server* s);
 
 /* Admits a beam (RFICleaner + search engine, plan.block_nsamps ==
- * layout.max_nsamps): allocates all of its steady-state device buffers and
- * charges their size, or fails with FROST_ERR_OUT_OF_MEMORY when that would
- * exceed the budget. */
+ * layout.max_nsamps): tunes the engine's FDMT launch shape
+ * (frost_search_autotune, cached per geometry), allocates all of its
+ * steady-state device buffers and charges their size, or fails with
+ * FROST_ERR_OUT_OF_MEMORY when that would exceed the budget. */
 int frost_server_add_beam(frost_server* s,
                           const frost_rfi_config* rfi,
                           const frost_block_layout* layout,

@@ -261,3 +261,21 @@ def test_graph_replay_matches_direct_launches():
         outs.append(np.concatenate(got))
     assert outs[0].size > 0
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_autotune_keeps_results_and_caches_choice():
+    """The autotuner measures the launch shapes, applies one, restarts the
+    stream, caches the choice for the geometry, and the tuned engine finds
+    what the default one finds (fused and single-level schedules give the
+    same bits with float planes)."""
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=1, gulp=8192)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0)
+    stream = make_stream(pc, 2, seed=91, pulses=PULSES)
+    ref = run_engine(FDMTBoxcar(pc, bc), stream, pc.block_nsamps)
+    tuned = FDMTBoxcar(pc, bc)
+    t1 = tuned.autotune()
+    assert t1["tiles_per_cta"] in (4, 8, 16, 32) and t1["ms"] > 0 and not t1["cached"]
+    assert np.array_equal(run_engine(tuned, stream, pc.block_nsamps), ref)
+    again = FDMTBoxcar(pc, bc).autotune()
+    assert again["cached"] and again["fused"] == t1["fused"] and again["tiles_per_cta"] == t1["tiles_per_cta"]
