@@ -570,6 +570,120 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def postprocess_config(nrows):
+    from frost_b200.postprocess import SearchConfig
+    return SearchConfig(boxcar_max=MAX_BOXCAR, detect_thresh=6.0, max_candidates=max(nrows, 1))
+
+
+def run_postprocess(args):
+    """Candidate post-processing of the headline workload's own detections:
+    one FP16 gulp of the config-2 beam is searched, and its raw candidates
+    (every plane, DM trial and width above S/N 6) are replayed gulp after
+    gulp with their samples advanced by a gulp each step, so clusters carry
+    across gulps as in a stream. A step is CandidatePostprocessPlan::execute
+    over one gulp's rows (chain clustering per plane, DM wings, carry,
+    sub-band dedup), input resident on the device. The reference arm's CPU
+    plan (its own lib/search sources) runs on the same rows."""
+    import numpy as np
+    import torch
+
+    from frost_b200.config import Storage
+    from frost_b200.pipeline import GulpPipeline, plan_for
+    from frost_b200.postprocess import CandidatePostprocessLayout, CandidatePostprocessPlan
+
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    raw_host = make_gulp(0x46524F5354)
+    raw_dev = torch.from_numpy(raw_host.reshape(-1)).to(dev)
+    del raw_host
+    lay = layout()
+    plan = plan_for(lay, 0.0, DM_MAX, DEPTH)
+    pipe = GulpPipeline(rfi_config(), lay, 2.0, plan, search_config(Storage.FP16), device=local)
+    pipe.execute_device(raw_dev.data_ptr(), GULP, on_device=True)
+    cands = pipe.execute_device(raw_dev.data_ptr(), GULP, on_device=True).candidates.copy()
+    del pipe, raw_dev
+    torch.cuda.empty_cache()
+    n = cands.size
+    nsteps = args.warmup + args.steps
+
+    def shifted(i):
+        c = cands.copy()
+        for f in ("peak_sample", "begin_sample", "end_sample"):
+            c[f] = c[f] + np.uint64(i * GULP)
+        return c
+
+    gulps = [shifted(i) for i in range(nsteps)]
+    dev_rows = [torch.from_numpy(g.view(np.uint8)).to(dev) for g in gulps]
+    cfg = postprocess_config(n)
+    ppl = CandidatePostprocessLayout(NCHANS, TSAMP, FOFF)
+    pp = CandidatePostprocessPlan(cfg, ppl, device=local)
+    frontier_lag = MAX_BOXCAR
+
+    def step(i, rows_ptr=None):
+        sr = (i + 2) * GULP
+        if rows_ptr is None:
+            return pp.execute(gulps[i], sr, GULP, False, sr - frontier_lag)
+        return pp.execute_device(rows_ptr, n, sr, GULP, False, sr - frontier_lag)
+
+    for i in range(args.warmup):
+        step(i, dev_rows[i].data_ptr())
+    torch.cuda.synchronize()
+    times, out_rows, pend, launches, phases = [], 0, 0, 0, [0.0, 0.0]
+    for i in range(args.warmup, nsteps):
+        t0 = time.perf_counter()
+        r = step(i, dev_rows[i].data_ptr())
+        times.append(time.perf_counter() - t0)
+        out_rows += r.candidates.size
+        pend = r.pending_candidates
+        launches += r.launches
+        phases[0] += r.cluster_s
+        phases[1] += r.dedup_s
+    ms = 1e3 * sum(times) / len(times)
+    # end to end: host rows in, giants out (the C ABI's host path)
+    pp_e2e = CandidatePostprocessPlan(cfg, ppl, device=local)
+    e2e_t = []
+    for i in range(nsteps):
+        sr = (i + 2) * GULP
+        t0 = time.perf_counter()
+        pp_e2e.execute(gulps[i], sr, GULP, False, sr - frontier_lag)
+        if i >= args.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_ms = 1e3 * sum(e2e_t) / len(e2e_t)
+    line = {"metric": "candidate rows post-processed/s @4096ch DM2000", "value": round(n / (ms / 1e3), 1),
+            "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64/u64 (coincidence arithmetic)", "data": "the search's own detections of a synthetic "
+            "config-2 gulp, replayed with samples advanced a gulp per step",
+            "config": {"workload": f"CandidatePostprocessPlan over {n} raw rows per gulp (11 planes, "
+                                   "chain + DM wings + carry + transitive sub-band dedup, frost defaults)",
+                       "rows_per_gulp": n, "giants_out_per_gulp": round(out_rows / args.steps, 1),
+                       "pending_after_last": pend},
+            "phase_ms_per_step": {"cluster": round(1e3 * phases[0] / args.steps, 3),
+                                  "dedup": round(1e3 * phases[1] / args.steps, 3)},
+            "e2e": {"value": round(n / (e2e_ms / 1e3), 1), "unit": "rows/s",
+                    "h2d_bytes_per_step": int(gulps[0].nbytes), "d2h_bytes_per_step": None,
+                    "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": launches}
+    if not args.no_cpu_baseline:
+        from oracle import postprocess as op
+        if op.ref_available():
+            rp = op.backend("reference").plan(cfg, ppl)
+            t = []
+            for i in range(min(nsteps, 2)):
+                sr = (i + 2) * GULP
+                t0 = time.perf_counter()
+                rp.execute(gulps[i], sr, GULP, False, sr - frontier_lag)
+                t.append(time.perf_counter() - t0)
+            line["cpu_baseline"] = {"value": round(n / t[-1], 1), "unit": "rows/s", "cores": 1,
+                                    "kind": "reference", "ms_per_gulp": round(1e3 * t[-1], 1),
+                                    "sample": "the reference's own CandidatePostprocessPlan (lib/search "
+                                              "sources, strict build) on the second replayed gulp"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -577,15 +691,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["frost", "reference"], default="frost")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving"], default="config2",
-                    help="config2 (headline), config1 (1024-channel profiling case) or serving "
-                         "(64 beams at real-time cadence)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "postprocess"], default="config2",
+                    help="config2 (headline), config1 (1024-channel profiling case), serving "
+                         "(64 beams at real-time cadence) or postprocess (candidate clustering and "
+                         "dedup of the headline gulp's detections)")
     ap.add_argument("--beams", type=int, default=3, help="served beams per GPU (admitted by memory)")
     ap.add_argument("--served-tile", type=int, default=0,
                     help="FDMT tile of the served beams in samples (0 = the whole gulp)")
     args = ap.parse_args()
     if args.workload == "serving":
         run_serving(args)
+        return
+    if args.workload == "postprocess":
+        run_postprocess(args)
         return
     select_workload(args.workload)
     if args.warmup < 3 and args.impl == "frost":

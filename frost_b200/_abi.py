@@ -232,3 +232,77 @@ class ServerStatsC(C.Structure):
         ("max_latency_s", C.c_double),
         ("launches", C.c_uint64),
     ]
+
+
+class GiantC(C.Structure):
+    """frost_giant: search::Giant (include/frost/search/candidate.hpp:28-66)."""
+
+    _fields_ = [
+        ("samp_idx", C.c_uint64),
+        ("filter_idx", C.c_uint64),
+        ("filter_width", C.c_uint64),
+        ("dm_idx", C.c_uint64),
+        ("begin", C.c_uint64),
+        ("end", C.c_uint64),
+        ("members", C.c_uint64),
+        ("chan_begin", C.c_uint64),
+        ("chan_end", C.c_uint64),
+        ("plane", C.c_uint64),
+        ("best_chan_begin", C.c_uint64),
+        ("best_chan_end", C.c_uint64),
+        ("n_extents", C.c_uint64),
+        ("loc_samp_idx", C.c_uint64),
+        ("loc_filter_width", C.c_uint64),
+        ("snr", C.c_float),
+        ("dm", C.c_float),
+        ("f_low", C.c_float),
+        ("f_high", C.c_float),
+        ("snr_best", C.c_float),
+        ("loc_dm", C.c_float),
+        ("loc_f_low", C.c_float),
+        ("loc_f_high", C.c_float),
+        ("has_location_best", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class ClusterTolerancesC(C.Structure):
+    _fields_ = [
+        ("time_tol", C.c_uint64),
+        ("filter_tol", C.c_uint64),
+        ("dm_tol", C.c_uint64),
+        ("dm_smear", C.c_double),
+        ("tsamp", C.c_double),
+        ("snr_floor", C.c_double),
+    ]
+
+
+class PostprocessConfigC(C.Structure):
+    _fields_ = [
+        ("boxcar_max", C.c_uint64),
+        ("max_candidates", C.c_uint64),
+        ("max_pending_candidates", C.c_uint64),
+        ("cand_sep_time", C.c_uint64),
+        ("cand_sep_filter", C.c_uint64),
+        ("cand_sep_dm", C.c_uint64),
+        ("detect_thresh", C.c_float),
+        ("cand_sep_dm_smear", C.c_float),
+        ("max_giant_rate", C.c_float),
+        ("cluster", C.c_int32),
+        ("subband_dedup", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class PostprocessLayoutC(C.Structure):
+    _fields_ = [("nchans", C.c_uint64), ("tsamp", C.c_double), ("frequency_step", C.c_double)]
+
+
+class PostprocessResultC(C.Structure):
+    _fields_ = [
+        ("count", C.c_size_t),
+        ("pending_candidates", C.c_uint64),
+        ("cluster_s", C.c_double),
+        ("dedup_s", C.c_double),
+        ("launches", C.c_uint64),
+    ]

@@ -82,6 +82,24 @@ SIGNATURES = {
                                      C.POINTER(_sz)]),
     "frost_server_get_stats": (C.c_int, [_vp, C.POINTER(_abi.ServerStatsC)]),
     "frost_server_reset_stats": (C.c_int, [_vp]),
+    "frost_postprocess_create": (C.c_int, [C.POINTER(_abi.PostprocessConfigC), C.POINTER(_abi.PostprocessLayoutC),
+                                           C.c_int, C.POINTER(_vp)]),
+    "frost_postprocess_destroy": (C.c_int, [_vp]),
+    "frost_postprocess_execute": (C.c_int, [_vp, _vp, _sz, C.c_int, _u64, _u64, C.c_int, _u64,
+                                            C.POINTER(_abi.PostprocessResultC)]),
+    "frost_postprocess_execute_search": (C.c_int, [_vp, _vp, _u64, _u64, C.c_int, _u64,
+                                                   C.POINTER(_abi.PostprocessResultC)]),
+    "frost_postprocess_results": (C.c_int, [_vp, _vp, _sz, C.POINTER(_sz)]),
+    "frost_postprocess_memory_usage": (C.c_int, [_vp, C.POINTER(_u64)]),
+    "frost_postprocess_estimate_memory": (C.c_int, [C.POINTER(_abi.PostprocessConfigC), C.POINTER(_u64)]),
+    "frost_cluster_labels": (C.c_int, [_vp, _sz, C.POINTER(_abi.ClusterTolerancesC), C.c_int, _vp, C.c_int]),
+    "frost_merge_candidates": (C.c_int, [_vp, _vp, _sz, _vp, C.POINTER(_sz), C.c_int]),
+    "frost_subband_dedup": (C.c_int, [_vp, _sz, C.POINTER(_abi.ClusterTolerancesC), C.c_float, C.c_int, _vp,
+                                      C.POINTER(_sz), C.c_int]),
+    "frost_are_coincident": (C.c_int, [C.POINTER(_abi.GiantC), C.POINTER(_abi.GiantC),
+                                       C.POINTER(_abi.ClusterTolerancesC), C.c_int]),
+    "frost_subband_time_shift_samples": (C.c_double, [C.c_float, C.c_float, C.c_float, C.c_float]),
+    "frost_subband_dm_step": (C.c_double, [C.c_float, C.c_float, C.c_float]),
 }
 
 

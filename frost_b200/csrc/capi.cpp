@@ -11,6 +11,8 @@
 #include "common.hpp"
 #include "dedisp.hpp"
 #include "host_stats.hpp"
+#include "postprocess.hpp"
+#include "pp_math.cuh"
 #include "rfi_cleaner.hpp"
 #include "search_engine.hpp"
 #include "server.hpp"
@@ -71,7 +73,38 @@ struct frost_server {
     template <class... A> explicit frost_server(A&&... a) : impl(std::forward<A>(a)...) {}
 };
 
+struct frost_postprocess {
+    fb::pp::PostprocessPlan impl;
+    template <class... A> explicit frost_postprocess(A&&... a) : impl(std::forward<A>(a)...) {}
+};
+
 namespace {
+/** Device copy of host giants for a standalone plan call (one stream). */
+struct PlanCall {
+    fb::DeviceGuard guard;
+    cudaStream_t s = nullptr;
+    fb::pp::Workspace ws;
+    fb::DeviceBuffer rows, out, aux;
+    explicit PlanCall(int device) : guard(device) {
+        FB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    }
+    ~PlanCall() {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+    const frost_giant* upload(const frost_giant* g, size_t n) {
+        rows.reserve(std::max<size_t>(n, 1) * sizeof(frost_giant));
+        if (n)
+            FB_CUDA(cudaMemcpyAsync(rows.get(), g, n * sizeof(frost_giant), cudaMemcpyHostToDevice, s));
+        return rows.as<frost_giant>();
+    }
+};
+
+void check_rows(size_t n, const char* what) {
+    if (n >= (size_t{1} << 31))
+        fb::invalid(std::string(what) + ": at most 2^31 - 1 rows per call");
+}
+
 int copy_candidates(const std::vector<frost_candidate>& c, frost_candidate* out, size_t capacity,
                     size_t* count) {
     if (count != nullptr)
@@ -552,6 +585,165 @@ int frost_search_plane_data(const frost_search* s, size_t plane, float* out, siz
             invalid("frost_search_plane_data: null argument");
         s->impl.plane_data(plane, out, capacity);
     });
+}
+
+// ---- candidate post-processing ------------------------------------------------
+
+int frost_postprocess_create(const frost_postprocess_config* cfg, const frost_postprocess_layout* layout,
+                             int device, frost_postprocess** out) {
+    return guarded([&] {
+        if (cfg == nullptr || layout == nullptr || out == nullptr)
+            invalid("frost_postprocess_create: null argument");
+        *out = nullptr;
+        *out = new frost_postprocess(*cfg, *layout, device);
+    });
+}
+
+int frost_postprocess_destroy(frost_postprocess* p) {
+    return guarded([&] { delete p; });
+}
+
+int frost_postprocess_execute(frost_postprocess* p, const frost_candidate* cands, size_t n, int on_device,
+                              uint64_t samples_read, uint64_t duration_samples, int final_call,
+                              uint64_t candidate_frontier, frost_postprocess_result* out) {
+    return guarded([&] {
+        if (p == nullptr || out == nullptr || (cands == nullptr && n > 0))
+            invalid("frost_postprocess_execute: null argument");
+        fb::DeviceGuard g(p->impl.device());
+        *out = p->impl.execute(cands, n, on_device != 0, samples_read, duration_samples, final_call != 0,
+                               candidate_frontier);
+    });
+}
+
+int frost_postprocess_execute_search(frost_postprocess* p, frost_search* s, uint64_t samples_read,
+                                     uint64_t duration_samples, int final_call, uint64_t candidate_frontier,
+                                     frost_postprocess_result* out) {
+    return guarded([&] {
+        if (p == nullptr || s == nullptr || out == nullptr)
+            invalid("frost_postprocess_execute_search: null argument");
+        if (p->impl.device() != s->impl.device())
+            invalid("frost_postprocess_execute_search: the handles are on different devices");
+        fb::DeviceGuard g(p->impl.device());
+        *out = p->impl.execute(s->impl.device_results(), s->impl.results().size(), true, samples_read,
+                               duration_samples, final_call != 0, candidate_frontier);
+    });
+}
+
+int frost_postprocess_results(const frost_postprocess* p, frost_giant* out, size_t capacity, size_t* count) {
+    return guarded([&] {
+        if (p == nullptr || count == nullptr)
+            invalid("frost_postprocess_results: null argument");
+        const auto& r = p->impl.results();
+        *count        = r.size();
+        if (out != nullptr) {
+            if (capacity < r.size())
+                invalid("frost_postprocess_results: output holds too few giants");
+            std::memcpy(out, r.data(), r.size() * sizeof(frost_giant));
+        }
+    });
+}
+
+int frost_postprocess_memory_usage(const frost_postprocess* p, uint64_t* bytes) {
+    return guarded([&] {
+        if (p == nullptr || bytes == nullptr)
+            invalid("frost_postprocess_memory_usage: null argument");
+        *bytes = p->impl.memory_usage();
+    });
+}
+
+int frost_postprocess_estimate_memory(const frost_postprocess_config* cfg, uint64_t* bytes) {
+    return guarded([&] {
+        if (cfg == nullptr || bytes == nullptr)
+            invalid("frost_postprocess_estimate_memory: null argument");
+        *bytes = fb::pp::PostprocessPlan::estimate_memory(*cfg);
+    });
+}
+
+int frost_cluster_labels(const frost_giant* giants, size_t n, const frost_cluster_tolerances* tol, int mode,
+                         uint64_t* labels, int device) {
+    return guarded([&] {
+        if (tol == nullptr || ((giants == nullptr || labels == nullptr) && n > 0))
+            invalid("frost_cluster_labels: null argument");
+        if (mode != FROST_CLUSTER_CHAIN && mode != FROST_CLUSTER_SEEDED)
+            invalid("frost_cluster_labels: unknown mode");
+        check_rows(n, "frost_cluster_labels");
+        if (n == 0)
+            return;
+        PlanCall c(device);
+        const frost_giant* rows = c.upload(giants, n);
+        c.out.reserve(n * sizeof(uint32_t));
+        fb::pp::cluster_labels(c.ws, rows, n, *tol, mode, c.out.as<uint32_t>(), c.s);
+        std::vector<uint32_t> l(n);
+        FB_CUDA(cudaMemcpyAsync(l.data(), c.out.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+        FB_CUDA(cudaStreamSynchronize(c.s));
+        for (size_t i = 0; i < n; ++i)
+            labels[i] = l[i];
+    });
+}
+
+int frost_merge_candidates(const frost_giant* giants, const uint64_t* labels, size_t n, frost_giant* out,
+                           size_t* count, int device) {
+    return guarded([&] {
+        if (count == nullptr || ((giants == nullptr || labels == nullptr || out == nullptr) && n > 0))
+            invalid("frost_merge_candidates: null argument");
+        check_rows(n, "frost_merge_candidates");
+        *count = 0;
+        if (n == 0)
+            return;
+        PlanCall c(device);
+        const frost_giant* rows = c.upload(giants, n);
+        c.aux.reserve(n * sizeof(uint64_t));
+        FB_CUDA(cudaMemcpyAsync(c.aux.get(), labels, n * sizeof(uint64_t), cudaMemcpyHostToDevice, c.s));
+        c.out.reserve(n * sizeof(frost_giant));
+        const size_t m = fb::pp::merge_candidates(c.ws, rows, c.aux.as<uint64_t>(), n,
+                                                  c.out.as<frost_giant>(), c.s);
+        FB_CUDA(cudaMemcpyAsync(out, c.out.get(), m * sizeof(frost_giant), cudaMemcpyDeviceToHost, c.s));
+        FB_CUDA(cudaStreamSynchronize(c.s));
+        *count = m;
+    });
+}
+
+int frost_subband_dedup(const frost_giant* giants, size_t n, const frost_cluster_tolerances* tol, float tsamp,
+                        int mode, frost_giant* out, size_t* count, int device) {
+    return guarded([&] {
+        if (tol == nullptr || count == nullptr || ((giants == nullptr || out == nullptr) && n > 0))
+            invalid("frost_subband_dedup: null argument");
+        if (mode != FROST_DEDUP_TRANSITIVE && mode != FROST_DEDUP_SEEDED)
+            invalid("frost_subband_dedup: unknown mode");
+        check_rows(n, "frost_subband_dedup");
+        *count = 0;
+        if (n == 0)
+            return;
+        if (!fb::pp::posfin_f(tsamp))
+            invalid("sub-band dedup requires tsamp > 0");
+        PlanCall c(device);
+        const frost_giant* rows = c.upload(giants, n);
+        c.out.reserve(n * sizeof(frost_giant));
+        const size_t m = fb::pp::subband_dedup(c.ws, rows, n, *tol, tsamp, mode, c.out.as<frost_giant>(), c.s);
+        FB_CUDA(cudaMemcpyAsync(out, c.out.get(), m * sizeof(frost_giant), cudaMemcpyDeviceToHost, c.s));
+        FB_CUDA(cudaStreamSynchronize(c.s));
+        *count = m;
+    });
+}
+
+int frost_are_coincident(const frost_giant* a, const frost_giant* b, const frost_cluster_tolerances* tol,
+                         int physical) {
+    if (a == nullptr || b == nullptr || tol == nullptr) {
+        fb::set_last_error("frost_are_coincident: null argument");
+        return 0;
+    }
+    const fb::pp::Pt pa = fb::pp::pt_of(*a), pb = fb::pp::pt_of(*b);
+    if (physical != 0)
+        return fb::pp::coincident(pa, pb, *tol) ? 1 : 0;
+    return fb::pp::coincident_basic(pa, pb, tol->time_tol, tol->filter_tol, tol->dm_tol) ? 1 : 0;
+}
+
+double frost_subband_time_shift_samples(float dm, float f_wide, float f_narrow, float tsamp) {
+    return fb::pp::time_shift(dm, f_wide, f_narrow, tsamp);
+}
+
+double frost_subband_dm_step(float f_low, float f_high, float tsamp) {
+    return fb::pp::dm_step(f_low, f_high, tsamp);
 }
 
 } // extern "C"

@@ -28,6 +28,9 @@ public:
     void drain();
 
     const std::vector<frost_candidate>& results() const { return m_results; }
+    /** The last results on the device (unsorted; results().size() rows),
+     * valid until the next execute or drain. */
+    const frost_candidate* device_results() const { return m_cands.as<frost_candidate>(); }
     uint64_t dropped_global() const { return m_dropped_global; }
     uint64_t dropped_per_dm() const { return m_dropped_per_dm; }
     uint64_t frontier();

@@ -578,6 +578,182 @@ int frost_server_drain(frost_server* s,
 int frost_server_get_stats(frost_server* s, frost_server_stats* out);
 int frost_server_reset_stats(frost_server* s);
 
+/* ---- candidate post-processing (include/frost/search/postprocess.hpp) ---
+ *
+ * Friends-of-friends clustering within each FDMT plane, DM-wing seeding,
+ * sub-band deduplication across planes, the per-plane rate limiter and the
+ * streaming carry of unfinished clusters, run on the device
+ * (lib/search/postprocess.cpp:67-241, clustering.cpp:24-226,
+ * merge.cpp:8-37, subband_dedup.cpp:163-315, rate_limiter.cpp:5-30). */
+
+/* search::Giant (include/frost/search/candidate.hpp:28-66). Its optional
+ * location_best is flattened into loc_* with has_location_best. Sample,
+ * index and channel fields are SizeType (64-bit). */
+typedef struct {
+    uint64_t samp_idx;         /* peak sample */
+    uint64_t filter_idx;
+    uint64_t filter_width;     /* 0 derives 1 << filter_idx */
+    uint64_t dm_idx;
+    uint64_t begin;
+    uint64_t end;
+    uint64_t members;
+    uint64_t chan_begin;       /* inclusive, original channel order */
+    uint64_t chan_end;         /* inclusive */
+    uint64_t plane;            /* subband_level * nchans + subband_idx */
+    uint64_t best_chan_begin;
+    uint64_t best_chan_end;
+    uint64_t n_extents;
+    uint64_t loc_samp_idx;     /* location_best.samp_idx */
+    uint64_t loc_filter_width; /* location_best.filter_width */
+    float snr;
+    float dm;
+    float f_low;               /* MHz */
+    float f_high;              /* MHz */
+    float snr_best;
+    float loc_dm;
+    float loc_f_low;
+    float loc_f_high;
+    int32_t has_location_best;
+    int32_t reserved;
+} frost_giant;
+
+/* ClusterTolerances (include/frost/search/clustering.hpp:22-33). */
+typedef struct {
+    uint64_t time_tol;
+    uint64_t filter_tol;
+    uint64_t dm_tol;
+    double dm_smear;  /* 0 = trial count only */
+    double tsamp;     /* seconds */
+    double snr_floor; /* 0 disables the S/N growth of the DM gate */
+} frost_cluster_tolerances;
+
+/* ClusterMode (clustering.hpp:44) and SubbandDedupMode
+ * (subband_dedup.hpp:42). */
+enum frost_cluster_mode { FROST_CLUSTER_CHAIN = 0, FROST_CLUSTER_SEEDED = 1 };
+enum frost_dedup_mode { FROST_DEDUP_TRANSITIVE = 0, FROST_DEDUP_SEEDED = 1 };
+
+/* The SearchConfig fields the post-processor reads
+ * (include/frost/config/config.hpp:57-97). */
+typedef struct {
+    uint64_t boxcar_max;
+    uint64_t max_candidates;
+    uint64_t max_pending_candidates; /* 0 = max_candidates */
+    uint64_t cand_sep_time;
+    uint64_t cand_sep_filter;
+    uint64_t cand_sep_dm;
+    float detect_thresh;
+    float cand_sep_dm_smear;
+    float max_giant_rate;            /* <= 0 disables the rate limiter */
+    int32_t cluster;
+    int32_t subband_dedup;           /* enum frost_dedup_mode */
+    int32_t reserved;
+} frost_postprocess_config;
+
+/* CandidatePostprocessLayout (postprocess.hpp:12-16). */
+typedef struct {
+    uint64_t nchans;
+    double tsamp;
+    double frequency_step; /* MHz; negative = channels stored high first */
+} frost_postprocess_layout;
+
+/* CandidatePostprocessResult (postprocess.hpp:20-25); the giants are read
+ * with frost_postprocess_results. */
+typedef struct {
+    size_t count;
+    uint64_t pending_candidates;
+    double cluster_s;
+    double dedup_s;
+    uint64_t launches; /* kernels this call launched */
+} frost_postprocess_result;
+
+typedef struct frost_postprocess frost_postprocess;
+
+/* CandidatePostprocessPlan(cfg, layout) (postprocess.cpp:50-66): reserves
+ * device memory for max_candidates incoming and max_pending_candidates
+ * carried rows. */
+int frost_postprocess_create(const frost_postprocess_config* cfg,
+                             const frost_postprocess_layout* layout,
+                             int device,
+                             frost_postprocess** out);
+int frost_postprocess_destroy(frost_postprocess* p);
+
+/* CandidatePostprocessPlan::execute (postprocess.cpp:67-180) over `n` raw
+ * detections, on the device when `on_device` else in host memory. Fails
+ * with FROST_ERR_INVALID_ARGUMENT on an invalid row (nothing changes) and
+ * FROST_ERR_OVERFLOW when the carried rows would exceed
+ * max_pending_candidates (the carry keeps its previous rows). */
+int frost_postprocess_execute(frost_postprocess* p,
+                              const frost_candidate* cands,
+                              size_t n,
+                              int on_device,
+                              uint64_t samples_read,
+                              uint64_t duration_samples,
+                              int final_call,
+                              uint64_t candidate_frontier,
+                              frost_postprocess_result* out);
+
+/* The same over the search handle's last results, read in place on the
+ * device (pipeline.cpp:481-487 hands dmt's view over the same way). Both
+ * handles must be on the same device; `s` is synchronised first. */
+int frost_postprocess_execute_search(frost_postprocess* p,
+                                     frost_search* s,
+                                     uint64_t samples_read,
+                                     uint64_t duration_samples,
+                                     int final_call,
+                                     uint64_t candidate_frontier,
+                                     frost_postprocess_result* out);
+
+/* Copies the last execute's giants (valid until the next execute). */
+int frost_postprocess_results(const frost_postprocess* p,
+                              frost_giant* out,
+                              size_t capacity,
+                              size_t* count);
+
+/* memory_usage() and estimate_memory(cfg) (postprocess.cpp:181-286), in
+ * device bytes of this implementation. */
+int frost_postprocess_memory_usage(const frost_postprocess* p, uint64_t* bytes);
+int frost_postprocess_estimate_memory(const frost_postprocess_config* cfg, uint64_t* bytes);
+
+/* ClusterLabelPlan::execute (clustering.cpp:107-226) on the device: one
+ * label per giant (its cluster's representative index). */
+int frost_cluster_labels(const frost_giant* giants,
+                         size_t n,
+                         const frost_cluster_tolerances* tol,
+                         int mode,
+                         uint64_t* labels,
+                         int device);
+
+/* MergeCandidatesPlan::execute (merge.cpp:8-37) on the device; `out` holds
+ * up to n rows, *count is the number of clusters. */
+int frost_merge_candidates(const frost_giant* giants,
+                           const uint64_t* labels,
+                           size_t n,
+                           frost_giant* out,
+                           size_t* count,
+                           int device);
+
+/* SubbandDedupPlan::execute (subband_dedup.cpp:194-315) on the device;
+ * `out` holds up to n rows. */
+int frost_subband_dedup(const frost_giant* giants,
+                        size_t n,
+                        const frost_cluster_tolerances* tol,
+                        float tsamp,
+                        int mode,
+                        frost_giant* out,
+                        size_t* count,
+                        int device);
+
+/* are_coincident (clustering.cpp:24-67): `physical` selects the overload
+ * with the DM-smearing gate. Host arithmetic identical to the kernels'. */
+int frost_are_coincident(const frost_giant* a,
+                         const frost_giant* b,
+                         const frost_cluster_tolerances* tol,
+                         int physical);
+
+/* subband_time_shift_samples / subband_dm_step (subband_dedup.cpp:163-192). */
+double frost_subband_time_shift_samples(float dm, float f_wide, float f_narrow, float tsamp);
+double frost_subband_dm_step(float f_low, float f_high, float tsamp);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
