@@ -50,13 +50,14 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
-/** Column arrays carved from one buffer (80 bytes a row). */
+/** Column arrays carved from one buffer (100 bytes a row + a flag). */
 Columns columns_in(DeviceBuffer& b, size_t n) {
     const size_t a = (n + 63) / 64 * 64;
-    b.reserve(a * 80);
+    b.reserve(a * 100 + 256);
     auto* base = static_cast<uint8_t*>(b.get());
     Columns c;
-    c.samp   = reinterpret_cast<u64*>(base);
+    c.key    = reinterpret_cast<uint4*>(base);
+    c.samp   = reinterpret_cast<u64*>(c.key + a);
     c.width  = c.samp + a;
     c.dm_idx = c.width + a;
     c.filter = c.dm_idx + a;
@@ -67,12 +68,14 @@ Columns columns_in(DeviceBuffer& b, size_t n) {
     c.snr    = c.dm + a;
     c.flo    = c.snr + a;
     c.fhi    = c.flo + a;
-    c.idx    = reinterpret_cast<u32*>(c.fhi + a);
-    c.seg    = c.idx + a;
+    c.idx     = reinterpret_cast<u32*>(c.fhi + a);
+    c.seg     = c.idx + a;
+    c.minidx  = c.seg + a;
+    c.general = c.minidx + a;
     return c;
 }
 
-size_t columns_bytes(size_t n) { return (n + 63) / 64 * 64 * 80; }
+size_t columns_bytes(size_t n) { return (n + 63) / 64 * 64 * 100 + 256; }
 
 /** First k in [0, n) at which the per-plane limiter reads exceeded, else n
  * (postprocess.cpp:143-152 with rate_limiter.cpp:17-24). */
@@ -107,10 +110,10 @@ void chain_labels(Workspace& ws, const frost_giant* rows, size_t n, const u32* s
         f.push_back({kKeyAux32, 0, static_cast<u64>(nseg - 1)});
     const u32* tperm = ws.sort(rows, n, f, seg_of, nullptr, nullptr, s).first;
     const Columns c  = columns_in(cols, n);
-    launch_columns(rows, tperm, seg_of, n, c, s);
+    launch_columns(rows, tperm, seg_of, seg_lo, n, samp_lo, c, s);
     launch_iota(parent, n, s);
     launch_chain(c, seg_lo, seg_hi, n, tol, parent, s);
-    launch_find_all(parent, n, label, s);
+    launch_rank_labels(parent, c, n, label, s);
 }
 
 /** Seeded clustering labels of rows[0, n) by segment (segment-major rows). */

@@ -408,15 +408,23 @@ __global__ void k_build_work(const frost_giant* __restrict__ inc, const frost_gi
 
 // ---- friends-of-friends -------------------------------------------------------
 
+/** Columns of rows[perm[r]] in time order, plus the packed 16-byte key the
+ * fast sweep reads: (samp - samp_lo, width, dm_idx, filter_idx), all
+ * 32-bit. *c.general is set when some row does not fit that key or its
+ * (plane, chan_begin, chan_end) differs from its segment's first row; the
+ * general sweep then runs instead. */
 __global__ void k_columns(const frost_giant* __restrict__ rows, const u32* __restrict__ perm,
-                          const u32* __restrict__ seg_of, size_t n, Columns c) {
+                          const u32* __restrict__ seg_of, const u32* __restrict__ seg_lo, size_t n, u64 samp_lo,
+                          Columns c) {
     const size_t r = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
     if (r >= n)
         return;
     const u32 i          = perm[r];
     const frost_giant& g = rows[i];
+    const u32 sg         = seg_of != nullptr ? seg_of[i] : 0u;
+    const u64 width      = box_width(g.filter_width, g.filter_idx);
     c.samp[r]            = g.samp_idx;
-    c.width[r]           = box_width(g.filter_width, g.filter_idx);
+    c.width[r]           = width;
     c.dm_idx[r]          = g.dm_idx;
     c.filter[r]          = g.filter_idx;
     c.cb[r]              = g.chan_begin;
@@ -427,7 +435,17 @@ __global__ void k_columns(const frost_giant* __restrict__ rows, const u32* __res
     c.flo[r]             = g.f_low;
     c.fhi[r]             = g.f_high;
     c.idx[r]             = i;
-    c.seg[r]             = seg_of != nullptr ? seg_of[i] : 0u;
+    c.seg[r]             = sg;
+    c.minidx[r]          = 0xFFFFFFFFu;
+    const u64 rel        = g.samp_idx - samp_lo;
+    const frost_giant& f = rows[perm[seg_lo != nullptr ? seg_lo[sg] : 0u]];
+    const bool fits = g.samp_idx >= samp_lo && rel <= 0xFFFFFFFFull && width <= 0xFFFFFFFFull &&
+                      g.dm_idx <= 0xFFFFFFFFull && g.filter_idx <= 0xFFFFFFFFull && g.plane == f.plane &&
+                      g.chan_begin == f.chan_begin && g.chan_end == f.chan_end;
+    if (!fits)
+        atomicOr(c.general, 1u);
+    c.key[r] = make_uint4(static_cast<u32>(rel), static_cast<u32>(width), static_cast<u32>(g.dm_idx),
+                          static_cast<u32>(g.filter_idx));
 }
 
 __device__ __forceinline__ Pt column_pt(const Columns& c, size_t r) {
@@ -435,14 +453,92 @@ __device__ __forceinline__ Pt column_pt(const Columns& c, size_t r) {
               c.dm[r],   c.snr[r],    c.flo[r],   c.fhi[r]};
 }
 
-/** One warp per time rank r: the rows inside r's time reach in r's segment,
- * 32 at a time, forward (widths <= r's) and backward (widths < r's), as
- * the reference's sweep pairs them. */
+__device__ __forceinline__ u32 absdiff32(u32 a, u32 b) { return a > b ? a - b : b - a; }
+
+/** Fast sweep (every row fits the packed key and each segment has one
+ * extent). One warp per time rank r tests the rows inside r's time reach in
+ * r's segment, 32 at a time, forward (widths <= r's) and backward (widths
+ * < r's) -- the pairs and orientation of the reference's sweep
+ * (clustering.cpp:146-183). parent[] is over time ranks; a row already
+ * hanging under r's root (one coalesced read per 32 rows) skips the rest. The
+ * DM gate's bound (dm_smear * width * step) depends only on r, the wider
+ * row, and is computed once. */
+__global__ void k_chain_fast(Columns c, const u32* __restrict__ seg_lo, const u32* __restrict__ seg_hi, size_t n,
+                             frost_cluster_tolerances tol, u32* parent) {
+    const size_t r = (blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= n || *c.general != 0)
+        return;
+    volatile u32* p   = parent;
+    const u32 sg      = c.seg[r];
+    const size_t lo   = seg_lo != nullptr ? seg_lo[sg] : 0;
+    const size_t hi   = seg_hi != nullptr ? seg_hi[sg] : n;
+    const uint4 a     = c.key[r];
+    const u64 reach   = time_reach(a.y, tol.time_tol);
+    const bool gate   = tol.dm_smear > 0.0 && tol.tsamp > 0.0;
+    const double step = gate ? dm_step(c.flo[r], c.fhi[r], static_cast<float>(tol.tsamp)) : 0.0;
+    const bool open   = !gate || !(step > 0.0);
+    const double lim  = tol.dm_smear * static_cast<double>(a.y) * step;
+    const double dma  = static_cast<double>(c.dm[r]);
+    const float snra  = c.snr[r];
+    const u32 rr      = static_cast<u32>(r);
+    u32 ra            = find_root(p, rr);
+    auto test         = [&](size_t q, const uint4& b) {
+        const u32 dd = absdiff32(a.z, b.z);
+        if (dd > tol.dm_tol || absdiff32(a.w, b.w) > tol.filter_tol)
+            return;
+        if (p[q] == ra)
+            return;
+        if (!open && dd > 1) {
+            const double ddm = abs_d(dma - static_cast<double>(c.dm[q]));
+            double growth    = 1.0;
+            if (tol.snr_floor > 0.0) {
+                const double ratio = static_cast<double>(max_f(snra, c.snr[q])) / tol.snr_floor;
+                growth             = max_d(1.0, sqrt(max_d(0.0, (ratio * ratio) - 1.0)));
+            }
+            if (!(ddm <= lim * growth))
+                return;
+        }
+        const u32 qq = static_cast<u32>(q);
+        if (find_root(p, qq) != ra)
+            unite(p, rr, qq);
+    };
+    for (size_t q0 = r + 1; q0 < hi; q0 += 32) {
+        const size_t q = q0 + lane;
+        const bool ok  = q < hi;
+        const uint4 b  = ok ? c.key[q] : make_uint4(0, 0, 0, 0);
+        const bool in  = ok && static_cast<u64>(b.x - a.x) <= reach;
+        const u32 m    = __ballot_sync(0xffffffffu, in);
+        if (in && b.y <= a.y)
+            test(q, b);
+        if (m != 0xffffffffu)
+            break;
+        ra = find_root(p, ra);
+    }
+    ra = find_root(p, ra);
+    for (size_t q0 = r; q0 > lo;) {
+        const bool has = q0 > lo + static_cast<size_t>(lane);
+        const size_t q = has ? q0 - 1 - lane : 0;
+        const uint4 b  = has ? c.key[q] : make_uint4(0, 0, 0, 0);
+        const bool in  = has && static_cast<u64>(a.x - b.x) <= reach;
+        const u32 m    = __ballot_sync(0xffffffffu, in);
+        if (in && b.y < a.y)
+            test(q, b);
+        if (m != 0xffffffffu)
+            break;
+        q0 -= 32;
+        ra = find_root(p, ra);
+    }
+}
+
+/** General sweep: 64-bit columns and the full coincidence test on each
+ * pair; same pairs and orientation as the fast sweep. Runs only when
+ * *c.general is set. */
 __global__ void k_chain(Columns c, const u32* __restrict__ seg_lo, const u32* __restrict__ seg_hi, size_t n,
                         frost_cluster_tolerances tol, u32* parent) {
     const size_t r = (blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (r >= n)
+    if (r >= n || *c.general == 0)
         return;
     volatile u32* p  = parent;
     const u32 sg     = c.seg[r];
@@ -450,17 +546,17 @@ __global__ void k_chain(Columns c, const u32* __restrict__ seg_lo, const u32* __
     const size_t hi  = seg_hi != nullptr ? seg_hi[sg] : n;
     const Pt a       = column_pt(c, r);
     const u64 reach  = time_reach(a.width, tol.time_tol);
-    const u32 ia     = c.idx[r];
-    u32 ra           = find_root(p, ia);
+    const u32 rr     = static_cast<u32>(r);
+    u32 ra           = find_root(p, rr);
     auto test        = [&](size_t q) {
         if (absdiff(a.dm_idx, c.dm_idx[q]) > tol.dm_tol || absdiff(a.filter, c.filter[q]) > tol.filter_tol ||
             a.cb != c.cb[q] || a.ce != c.ce[q] || a.plane != c.plane[q])
             return;
         if (!dm_gate(a, column_pt(c, q), tol))
             return;
-        const u32 ib = c.idx[q];
-        if (find_root(p, ib) != ra)
-            unite(p, ia, ib);
+        const u32 qq = static_cast<u32>(q);
+        if (find_root(p, qq) != ra)
+            unite(p, rr, qq);
     };
     for (size_t q0 = r + 1; q0 < hi; q0 += 32) {
         const size_t q = q0 + lane;
@@ -485,6 +581,23 @@ __global__ void k_chain(Columns c, const u32* __restrict__ seg_lo, const u32* __
         q0 -= 32;
         ra = find_root(p, ra);
     }
+}
+
+/** Rank roots to row labels: each component's label is its smallest row
+ * index (what the reference's union-find over row indices gives). */
+__global__ void k_rank_min(u32* parent, const u32* __restrict__ idx, size_t n, u32* minidx) {
+    const size_t r = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (r >= n)
+        return;
+    const u32 root = find_root(parent, static_cast<u32>(r));
+    atomicMin(minidx + root, idx[r]);
+}
+
+__global__ void k_rank_label(u32* parent, const u32* __restrict__ idx, const u32* __restrict__ minidx, size_t n,
+                             u32* __restrict__ label) {
+    const size_t r = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (r < n)
+        label[idx[r]] = minidx[find_root(parent, static_cast<u32>(r))];
 }
 
 __global__ void k_find_all(u32* parent, size_t n, u32* label) {
@@ -967,11 +1080,12 @@ void launch_build_work(const frost_giant* inc, const frost_giant* pend, const Se
     count();
 }
 
-void launch_columns(const frost_giant* rows, const u32* perm, const u32* seg_of, size_t n, const Columns& c,
-                    cudaStream_t s) {
+void launch_columns(const frost_giant* rows, const u32* perm, const u32* seg_of, const u32* seg_lo, size_t n,
+                    u64 samp_lo, const Columns& c, cudaStream_t s) {
+    FB_CUDA(cudaMemsetAsync(c.general, 0, sizeof(u32), s));
     if (n == 0)
         return;
-    k_columns<<<FB_PP_GRID(n)>>>(rows, perm, seg_of, n, c);
+    k_columns<<<FB_PP_GRID(n)>>>(rows, perm, seg_of, seg_lo, n, samp_lo, c);
     FB_LAUNCH_CHECK();
     count();
 }
@@ -980,8 +1094,22 @@ void launch_chain(const Columns& c, const u32* seg_lo, const u32* seg_hi, size_t
                   const frost_cluster_tolerances& tol, u32* parent, cudaStream_t s) {
     if (n < 2)
         return;
+    k_chain_fast<<<blocks_for(n * 32), kThreads, 0, s>>>(c, seg_lo, seg_hi, n, tol, parent);
+    FB_LAUNCH_CHECK();
     k_chain<<<blocks_for(n * 32), kThreads, 0, s>>>(c, seg_lo, seg_hi, n, tol, parent);
     FB_LAUNCH_CHECK();
+    count();
+    count();
+}
+
+void launch_rank_labels(u32* parent, const Columns& c, size_t n, u32* label, cudaStream_t s) {
+    if (n == 0)
+        return;
+    k_rank_min<<<FB_PP_GRID(n)>>>(parent, c.idx, n, c.minidx);
+    FB_LAUNCH_CHECK();
+    k_rank_label<<<FB_PP_GRID(n)>>>(parent, c.idx, c.minidx, n, label);
+    FB_LAUNCH_CHECK();
+    count();
     count();
 }
 

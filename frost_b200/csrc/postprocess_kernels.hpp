@@ -55,6 +55,7 @@ struct RangeKinds {
 
 /** Per-row columns of the friends-of-friends sweep, in time order. */
 struct Columns {
+    uint4* key; // (samp - samp_lo, width, dm_idx, filter_idx) when they fit 32 bits
     u64* samp;
     u64* width;
     u64* dm_idx;
@@ -66,8 +67,10 @@ struct Columns {
     float* snr;
     float* flo;
     float* fhi;
-    u32* idx; // row index in the clustered array
-    u32* seg; // segment (plane) of the row
+    u32* idx;     // row index in the clustered array
+    u32* seg;     // segment (plane) of the row
+    u32* minidx;  // per rank root: smallest row index of its component
+    u32* general; // one word: set when the general sweep must run
 };
 
 /** One plane of one execute call. */
@@ -128,16 +131,23 @@ void launch_build_work(const frost_giant* inc, const frost_giant* pend, const Se
 
 // ---- friends-of-friends (chain) --------------------------------------------
 
-/** Columns of rows[perm[r]] for r < n; seg from seg_of (or 0 if null). */
-void launch_columns(const frost_giant* rows, const u32* perm, const u32* seg_of, size_t n, const Columns& c,
-                    cudaStream_t s);
+/** Columns of rows[perm[r]] for r < n (time order); seg from seg_of (or 0
+ * if null); segment s starts at rank seg_lo[s] (null: 0). Sets
+ * *c.general when the fast sweep cannot take the rows. */
+void launch_columns(const frost_giant* rows, const u32* perm, const u32* seg_of, const u32* seg_lo, size_t n,
+                    u64 samp_lo, const Columns& c, cudaStream_t s);
 
 /** Unites every coincident pair inside the wider giant's time reach
  * (clustering.cpp:129-183). Segment s occupies ranks
  * [seg_lo[s], seg_hi[s]) (null: one segment [0, n)). parent[] starts as the
- * identity over row indices. */
+ * identity over time ranks. Launches the fast and the general sweep; the
+ * one *c.general does not select returns at once. */
 void launch_chain(const Columns& c, const u32* seg_lo, const u32* seg_hi, size_t n,
                   const frost_cluster_tolerances& tol, u32* parent, cudaStream_t s);
+
+/** label[idx[r]] = the smallest row index in r's component. c.minidx must
+ * hold ~0 (k_columns sets it). */
+void launch_rank_labels(u32* parent, const Columns& c, size_t n, u32* label, cudaStream_t s);
 
 /** label[i] = root of i (the smallest index of its component). */
 void launch_find_all(u32* parent, size_t n, u32* label, cudaStream_t s);
