@@ -82,6 +82,9 @@ SIGNATURES = {
                                      C.POINTER(_sz)]),
     "frost_server_get_stats": (C.c_int, [_vp, C.POINTER(_abi.ServerStatsC)]),
     "frost_server_reset_stats": (C.c_int, [_vp]),
+    "frost_server_set_postprocess": (C.c_int, [_vp, C.c_uint32, C.POINTER(_abi.PostprocessConfigC)]),
+    "frost_server_wait_giants": (C.c_int, [_vp, _u64, _vp, _sz, C.POINTER(_sz), C.POINTER(C.c_double)]),
+    "frost_server_drain_giants": (C.c_int, [_vp, C.c_uint32, _vp, _sz, C.POINTER(_sz)]),
     "frost_postprocess_create": (C.c_int, [C.POINTER(_abi.PostprocessConfigC), C.POINTER(_abi.PostprocessLayoutC),
                                            C.c_int, C.POINTER(_vp)]),
     "frost_postprocess_destroy": (C.c_int, [_vp]),

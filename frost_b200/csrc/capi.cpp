@@ -523,6 +523,50 @@ int frost_server_drain(frost_server* s, uint32_t beam, frost_candidate* out, siz
     return g != FROST_OK ? g : rc;
 }
 
+int frost_server_set_postprocess(frost_server* s, uint32_t beam, const frost_postprocess_config* cfg) {
+    return guarded([&] {
+        if (s == nullptr || cfg == nullptr)
+            invalid("frost_server_set_postprocess: null argument");
+        s->impl.set_postprocess(beam, *cfg);
+    });
+}
+
+namespace {
+int copy_giants(const std::vector<frost_giant>& g, frost_giant* out, size_t capacity, size_t* count) {
+    if (count != nullptr)
+        *count = g.size();
+    const size_t n = std::min(capacity, g.size());
+    if (out != nullptr && n)
+        std::memcpy(out, g.data(), n * sizeof(frost_giant));
+    if (g.size() > capacity) {
+        fb::set_last_error("giant buffer holds " + std::to_string(capacity) + " of " + std::to_string(g.size()));
+        return FROST_ERR_OVERFLOW;
+    }
+    return FROST_OK;
+}
+} // namespace
+
+int frost_server_wait_giants(frost_server* s, uint64_t ticket, frost_giant* out, size_t capacity, size_t* count,
+                             double* latency_s) {
+    int rc      = FROST_OK;
+    const int g = guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_wait_giants: null handle");
+        rc = copy_giants(s->impl.wait_giants(ticket, latency_s), out, capacity, count);
+    });
+    return g != FROST_OK ? g : rc;
+}
+
+int frost_server_drain_giants(frost_server* s, uint32_t beam, frost_giant* out, size_t capacity, size_t* count) {
+    int rc      = FROST_OK;
+    const int g = guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_drain_giants: null handle");
+        rc = copy_giants(s->impl.drain_giants(beam), out, capacity, count);
+    });
+    return g != FROST_OK ? g : rc;
+}
+
 int frost_server_reset_stats(frost_server* s) {
     return guarded([&] {
         if (s == nullptr)

@@ -14,7 +14,7 @@ double now_seconds() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-Beam::Beam(const BeamSpec& spec, int device) : m_spec(spec) {
+Beam::Beam(const BeamSpec& spec, int device) : m_spec(spec), m_device(device) {
     frost_rfi_config c = spec.rfi;
     c.zap_chans        = spec.zap_chans.data();
     c.n_zap_chans      = spec.zap_chans.size();
@@ -38,7 +38,28 @@ SizeType Beam::block_bytes() const {
            static_cast<SizeType>(bits_of(m_spec.layout.dtype)) / 8;
 }
 
-SizeType Beam::device_bytes() const { return m_cleaner->memory_usage() + m_engine->device_bytes(); }
+SizeType Beam::device_bytes() const {
+    return m_cleaner->memory_usage() + m_engine->device_bytes() + (m_post ? m_post->memory_usage() : 0);
+}
+
+void Beam::attach_postprocess(const frost_postprocess_config& cfg) {
+    const frost_postprocess_layout lay{m_spec.layout.nchans, m_spec.layout.tsamp, m_spec.layout.df};
+    m_post = std::make_unique<pp::PostprocessPlan>(cfg, lay, m_device);
+}
+
+const std::vector<frost_giant>& Beam::giants() const {
+    static const std::vector<frost_giant> kNone;
+    return m_post ? m_post->results() : kNone;
+}
+
+void Beam::postprocess(bool final_call) {
+    if (!m_post)
+        return;
+    const uint64_t l0 = pp::launch_counter();
+    m_post->execute(m_engine->device_results(), m_engine->results().size(), true, m_read, m_last_nread,
+                    final_call, m_engine->frontier());
+    m_last_launches += pp::launch_counter() - l0;
+}
 
 void Beam::process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device) {
     if (bytes != block_bytes())
@@ -52,13 +73,16 @@ void Beam::process(const uint8_t* block, SizeType bytes, SizeType nread, bool on
     m_last_launches = (m_cleaner->launches() - l0) + m_engine->last_launches();
     // samples searched: frost's accounting, lib/pipeline/pipeline.cpp:610-614
     m_read += nread;
+    m_last_nread            = nread;
     const uint64_t previous = m_read - nread;
     if (m_read > m_max_delay)
         m_searched += m_read - std::max(previous, m_max_delay);
+    postprocess(false);
 }
 
 std::vector<frost_candidate> Beam::drain() {
     m_engine->drain();
+    postprocess(true);
     return m_engine->results();
 }
 
@@ -189,11 +213,14 @@ void Server::worker() {
         int status = FROST_OK;
         std::string err;
         std::vector<frost_candidate> cands;
+        std::vector<frost_giant> giants;
         uint64_t launches = 0;
         try {
             b->process(req->block, req->bytes, req->nread, req->on_device);
             cands    = b->results();
             launches = b->last_launches();
+            if (b->has_postprocess())
+                giants = b->giants();
         } catch (const Error& e) {
             status = e.code();
             err    = e.what();
@@ -207,6 +234,7 @@ void Server::worker() {
             req->status   = status;
             req->error    = err;
             req->cands    = std::move(cands);
+            req->giants   = std::move(giants);
             req->finished = true;
             m_busy[beam]  = false;
             if (status == FROST_OK) {
@@ -222,7 +250,7 @@ void Server::worker() {
     }
 }
 
-std::vector<frost_candidate> Server::wait(uint64_t ticket, double* latency_s) {
+std::shared_ptr<Request> Server::finish(uint64_t ticket, double* latency_s) {
     std::unique_lock<std::mutex> lk(m_mu);
     auto it = m_requests.find(ticket);
     if (it == m_requests.end())
@@ -234,30 +262,97 @@ std::vector<frost_candidate> Server::wait(uint64_t ticket, double* latency_s) {
         throw Error(req->status, req->error);
     if (latency_s != nullptr)
         *latency_s = req->done - req->arrival;
-    return std::move(req->cands);
+    return req;
 }
 
-std::vector<frost_candidate> Server::drain(uint32_t beam) {
-    std::unique_lock<std::mutex> lk(m_mu);
+std::vector<frost_candidate> Server::wait(uint64_t ticket, double* latency_s) {
+    return std::move(finish(ticket, latency_s)->cands);
+}
+
+std::vector<frost_giant> Server::wait_giants(uint64_t ticket, double* latency_s) {
+    return std::move(finish(ticket, latency_s)->giants);
+}
+
+/** Waits until the beam is idle with nothing queued and marks it busy. */
+Beam* Server::hold(uint32_t beam, std::unique_lock<std::mutex>& lk) {
     auto it = m_beams.find(beam);
     if (it == m_beams.end())
         invalid("serve: unknown beam");
     m_done_cv.wait(lk, [&] { return !m_busy[beam] && m_queue[beam].empty(); });
     m_busy[beam] = true;
-    Beam* b      = it->second.get();
+    return it->second.get();
+}
+
+void Server::release(uint32_t beam) {
+    {
+        std::lock_guard<std::mutex> lk(m_mu);
+        m_busy[beam] = false;
+    }
+    m_work_cv.notify_all();
+}
+
+std::vector<frost_candidate> Server::drain(uint32_t beam) {
+    std::unique_lock<std::mutex> lk(m_mu);
+    Beam* b = hold(beam, lk);
     lk.unlock();
     std::vector<frost_candidate> out;
     try {
         out = b->drain();
     } catch (...) {
-        lk.lock();
-        m_busy[beam] = false;
+        release(beam);
         throw;
     }
-    lk.lock();
-    m_busy[beam] = false;
-    m_work_cv.notify_all();
+    release(beam);
     return out;
+}
+
+std::vector<frost_giant> Server::drain_giants(uint32_t beam) {
+    std::unique_lock<std::mutex> lk(m_mu);
+    Beam* b = hold(beam, lk);
+    lk.unlock();
+    std::vector<frost_giant> out;
+    try {
+        if (!b->has_postprocess())
+            invalid("serve: beam has no post-processor");
+        b->drain();
+        out = b->giants();
+    } catch (...) {
+        release(beam);
+        throw;
+    }
+    release(beam);
+    return out;
+}
+
+void Server::set_postprocess(uint32_t beam, const frost_postprocess_config& cfg) {
+    std::unique_lock<std::mutex> lk(m_mu);
+    Beam* b = hold(beam, lk);
+    lk.unlock();
+    try {
+        DeviceGuard g(m_device);
+        if (b->has_postprocess())
+            invalid("serve: beam already has a post-processor");
+        const SizeType need = pp::PostprocessPlan::estimate_memory(cfg);
+        {
+            std::lock_guard<std::mutex> g2(m_mu);
+            if (m_budget != 0 && m_used + need > m_budget)
+                throw Error(FROST_ERR_OUT_OF_MEMORY, "serve: the post-processor does not fit the memory budget");
+            m_used += need;
+            m_charge[beam] += need;
+        }
+        try {
+            b->attach_postprocess(cfg);
+        } catch (...) {
+            std::lock_guard<std::mutex> g2(m_mu);
+            m_used -= need;
+            m_charge[beam] -= need;
+            throw;
+        }
+    } catch (...) {
+        release(beam);
+        throw;
+    }
+    release(beam);
 }
 
 void Server::reset_stats() {

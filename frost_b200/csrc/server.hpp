@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "postprocess.hpp"
 #include "rfi_cleaner.hpp"
 #include "search_engine.hpp"
 
@@ -45,6 +46,12 @@ public:
     void process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device);
     std::vector<frost_candidate> results() const { return m_engine->results(); }
     std::vector<frost_candidate> drain();
+    /** Adds CandidatePostprocessPlan after the search of every gulp
+     * (Pipeline::publish, lib/pipeline/pipeline.cpp:478-493), on the device
+     * over the engine's candidates. */
+    void attach_postprocess(const frost_postprocess_config& cfg);
+    bool has_postprocess() const { return m_post != nullptr; }
+    const std::vector<frost_giant>& giants() const;
     uint64_t samples_searched() const { return m_searched; }
     /** Kernels launched by the last process() call. */
     uint64_t last_launches() const { return m_last_launches; }
@@ -56,9 +63,12 @@ private:
     BeamSpec m_spec;
     std::unique_ptr<rfi::Cleaner> m_cleaner;
     std::unique_ptr<fdmt::Engine> m_engine;
+    std::unique_ptr<pp::PostprocessPlan> m_post;
+    int m_device;
     bool m_descending;
     std::vector<uint8_t> m_fdmt_mask;
-    uint64_t m_read = 0, m_searched = 0, m_max_delay = 0, m_last_launches = 0;
+    uint64_t m_read = 0, m_searched = 0, m_max_delay = 0, m_last_launches = 0, m_last_nread = 0;
+    void postprocess(bool final_call);
 };
 
 struct Request {
@@ -74,6 +84,7 @@ struct Request {
     int status    = FROST_OK;
     std::string error;
     std::vector<frost_candidate> cands;
+    std::vector<frost_giant> giants;
 };
 
 class Server {
@@ -86,6 +97,13 @@ public:
                     bool on_device);
     /** Blocks until the ticket is done; moves its candidates out. */
     std::vector<frost_candidate> wait(uint64_t ticket, double* latency_s);
+    /** As wait, moving out the gulp's post-processed giants instead. */
+    std::vector<frost_giant> wait_giants(uint64_t ticket, double* latency_s);
+    /** Attaches a post-processor to an idle beam; its device memory is
+     * charged against the server's budget. */
+    void set_postprocess(uint32_t beam, const frost_postprocess_config& cfg);
+    /** drain() of a beam with a post-processor: the final giants. */
+    std::vector<frost_giant> drain_giants(uint32_t beam);
     frost_server_stats stats();
     void reset_stats();
     std::vector<frost_candidate> drain(uint32_t beam);
@@ -110,6 +128,9 @@ private:
 
     void worker();
     bool pick(uint32_t& beam, std::shared_ptr<Request>& req);
+    std::shared_ptr<Request> finish(uint64_t ticket, double* latency_s);
+    Beam* hold(uint32_t beam, std::unique_lock<std::mutex>& lk);
+    void release(uint32_t beam);
 };
 
 double now_seconds();

@@ -27,7 +27,11 @@ def plan_for(layout: BlockLayout, dm_min: float, dm_max: float, subband_depth: i
 class GulpPipeline:
     def __init__(self, rfi_cfg: RfiConfig, layout: BlockLayout, baseline_length: float,
                  plan: DedispPlanConfig, search_cfg: BoxcarConfig, device: int = 0,
-                 tile_nsamps: int = 0, memory_budget: int = 0):
+                 tile_nsamps: int = 0, memory_budget: int = 0, postprocess=None):
+        """`postprocess` (a frost_b200.postprocess.SearchConfig) adds
+        CandidatePostprocessPlan after every gulp's search, as
+        Pipeline::publish does (lib/pipeline/pipeline.cpp:478-493); its
+        result of the last gulp is `self.postprocessed`."""
         self.layout = layout
         self.rfi = RFICleaner(rfi_cfg, layout, baseline_length, device)
         self.descending = layout.df < 0
@@ -40,6 +44,13 @@ class GulpPipeline:
         self.samples_read = 0
         self.samples_searched = 0
         self.block = layout.max_nsamps
+        self.post = None
+        self.postprocessed = None
+        self._last_nread = 0
+        if postprocess is not None:
+            from .postprocess import CandidatePostprocessLayout, CandidatePostprocessPlan
+            self.post = CandidatePostprocessPlan(
+                postprocess, CandidatePostprocessLayout(layout.nchans, layout.tsamp, layout.df), device)
 
     def _fdmt_mask(self):
         m = self.rfi.channel_mask()
@@ -60,6 +71,10 @@ class GulpPipeline:
                                                 stream=stream)
         res = self.search.execute_device(wf, self.block, self._fdmt_mask())
         self._account(nread)
+        self._last_nread = nread
+        if self.post is not None:
+            self.postprocessed = self.post.execute(self.search, self.samples_read, nread, False,
+                                                   self.search.get_candidate_frontier())
         return res
 
     def execute(self, block: np.ndarray, nread: int = 0) -> CandidateResult:
@@ -68,4 +83,8 @@ class GulpPipeline:
         return self.execute_device(buf.ctypes.data, nread, on_device=False)
 
     def flush(self) -> CandidateResult:
-        return self.search.drain()
+        res = self.search.drain()
+        if self.post is not None:
+            self.postprocessed = self.post.execute(self.search, self.samples_read, self._last_nread, True,
+                                                   self.search.get_candidate_frontier())
+        return res

@@ -44,6 +44,7 @@ class BeamServer:
         self._capacity: Dict[int, int] = {}
         self._beam_of: Dict[int, int] = {}
         self._blocks: Dict[int, np.ndarray] = {}
+        self._giant_capacity: Dict[int, int] = {}
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -104,6 +105,36 @@ class BeamServer:
             self._blocks.pop(ticket, None)
             self._beam_of.pop(ticket, None)
         return out[:n.value], lat.value
+
+    def set_postprocess(self, beam: int, cfg) -> None:
+        """Adds CandidatePostprocessPlan (frost_b200.postprocess.SearchConfig)
+        after every gulp's search of `beam`; wait_giants / drain_giants then
+        return its giants."""
+        check(lib().frost_server_set_postprocess(self._h, beam, C.byref(cfg._c())))
+        pend = cfg.max_pending_candidates or cfg.max_candidates
+        self._giant_capacity[beam] = max(1, int(cfg.max_candidates + pend))
+
+    def wait_giants(self, ticket: int):
+        """The gulp's post-processed giants (GIANT_DTYPE) and its latency."""
+        from .postprocess import GIANT_DTYPE
+        cap = self._giant_capacity[self._beam_of[ticket]]
+        out = np.zeros(cap, GIANT_DTYPE)
+        n, lat = C.c_size_t(), C.c_double()
+        try:
+            check(lib().frost_server_wait_giants(self._h, ticket, out.ctypes.data, cap, C.byref(n),
+                                                 C.byref(lat)))
+        finally:
+            self._blocks.pop(ticket, None)
+            self._beam_of.pop(ticket, None)
+        return out[:n.value].copy(), lat.value
+
+    def drain_giants(self, beam: int) -> np.ndarray:
+        from .postprocess import GIANT_DTYPE
+        cap = self._giant_capacity[beam]
+        out = np.zeros(cap, GIANT_DTYPE)
+        n = C.c_size_t()
+        check(lib().frost_server_drain_giants(self._h, beam, out.ctypes.data, cap, C.byref(n)))
+        return out[:n.value].copy()
 
     def drain(self, beam: int) -> np.ndarray:
         cap = self._capacity[beam]

@@ -677,6 +677,28 @@ int frost_postprocess_create(const frost_postprocess_config* cfg,
                              frost_postprocess** out);
 int frost_postprocess_destroy(frost_postprocess* p);
 
+/* Attaches a CandidatePostprocessPlan to a served beam: after the search of
+ * each of its gulps the detections are clustered and deduplicated on the
+ * device, as frost's Pipeline::publish does (lib/pipeline/pipeline.cpp:
+ * 478-493, samples_read = the beam's samples so far, duration = the gulp's
+ * rows, frontier = the engine's). Waits for the beam to be idle; the plan's
+ * device memory is charged to the server budget (FROST_ERR_OUT_OF_MEMORY if
+ * it does not fit). */
+int frost_server_set_postprocess(frost_server* s, uint32_t beam, const frost_postprocess_config* cfg);
+
+/* frost_server_wait for a beam with a post-processor: the gulp's giants
+ * (its raw candidates are dropped). */
+int frost_server_wait_giants(frost_server* s,
+                             uint64_t ticket,
+                             frost_giant* out,
+                             size_t capacity,
+                             size_t* count,
+                             double* latency_s);
+
+/* drain() of a beam with a post-processor: the final call's giants (every
+ * carried cluster released). */
+int frost_server_drain_giants(frost_server* s, uint32_t beam, frost_giant* out, size_t capacity, size_t* count);
+
 /* CandidatePostprocessPlan::execute (postprocess.cpp:67-180) over `n` raw
  * detections, on the device when `on_device` else in host memory. Fails
  * with FROST_ERR_INVALID_ARGUMENT on an invalid row (nothing changes) and

@@ -10,6 +10,11 @@
 //   frost::b200::FDMTBoxcar   ~ the dmt::FDMTBoxcar call shape frost uses
 //                               (lib/pipeline/pipeline.cpp:316-367, 493-517, 598-608)
 //   frost::b200::BeamServer   ~ many beams on one GPU (no frost counterpart)
+//   frost::b200::CandidatePostprocessPlan, ClusterLabelPlan,
+//   MergeCandidatesPlan, SubbandDedupPlan, are_coincident,
+//   subband_time_shift_samples, subband_dm_step
+//                             ~ frost::search (include/frost/search/*.hpp),
+//                               on the device
 //
 // Link with frost_b200/lib/libfrost_b200.so.
 #pragma once
@@ -209,6 +214,9 @@ public:
         return r;
     }
 
+    /** The C handle (for calls that read the engine's results in place). */
+    frost_search* handle() const { return m_h; }
+
 private:
     const uint8_t* mask_ptr(std::span<const uint8_t> mask) const {
         if (mask.empty())
@@ -329,8 +337,171 @@ public:
     }
     void reset_stats() { check(frost_server_reset_stats(m_h)); }
 
+    /** Adds CandidatePostprocessPlan after every gulp of `beam`. */
+    void set_postprocess(uint32_t beam, const frost_postprocess_config& cfg) {
+        check(frost_server_set_postprocess(m_h, beam, &cfg));
+    }
+
+    std::vector<frost_giant> wait_giants(uint64_t ticket, size_t capacity, double* latency_s = nullptr) {
+        std::vector<frost_giant> out(capacity);
+        size_t n = 0;
+        check(frost_server_wait_giants(m_h, ticket, out.data(), out.size(), &n, latency_s));
+        out.resize(n);
+        return out;
+    }
+
+    std::vector<frost_giant> drain_giants(uint32_t beam, size_t capacity) {
+        std::vector<frost_giant> out(capacity);
+        size_t n = 0;
+        check(frost_server_drain_giants(m_h, beam, out.data(), out.size(), &n));
+        out.resize(n);
+        return out;
+    }
+
 private:
     frost_server* m_h = nullptr;
 };
+
+/** config::SearchConfig's post-processing defaults (config.hpp:57-97). */
+inline frost_postprocess_config default_postprocess_config() {
+    frost_postprocess_config c{};
+    c.boxcar_max        = 4096;
+    c.max_candidates    = 131072;
+    c.cand_sep_time     = 3;
+    c.cand_sep_filter   = 3;
+    c.cand_sep_dm       = 200;
+    c.detect_thresh     = 6.0F;
+    c.cand_sep_dm_smear = 8.0F;
+    c.cluster           = 1;
+    c.subband_dedup     = FROST_DEDUP_TRANSITIVE;
+    return c;
+}
+
+struct CandidatePostprocessResult {
+    std::vector<frost_giant> candidates;
+    double cluster_s = 0.0;
+    double dedup_s   = 0.0;
+    uint64_t pending_candidates = 0;
+};
+
+/** search::CandidatePostprocessPlan (postprocess.hpp:28-62) on the device. */
+class CandidatePostprocessPlan {
+public:
+    CandidatePostprocessPlan(const frost_postprocess_config& cfg, const frost_postprocess_layout& layout,
+                             int device = 0) {
+        check(frost_postprocess_create(&cfg, &layout, device, &m_h));
+    }
+    CandidatePostprocessPlan(const CandidatePostprocessPlan&)            = delete;
+    CandidatePostprocessPlan& operator=(const CandidatePostprocessPlan&) = delete;
+    ~CandidatePostprocessPlan() {
+        if (m_h != nullptr)
+            frost_postprocess_destroy(m_h);
+    }
+
+    /** Over raw rows (host memory, or device memory when on_device). */
+    CandidatePostprocessResult execute(std::span<const frost_candidate> rows, uint64_t samples_read,
+                                       uint64_t duration_samples, bool final_call, uint64_t frontier,
+                                       bool on_device = false) {
+        frost_postprocess_result r{};
+        check(frost_postprocess_execute(m_h, rows.data(), rows.size(), on_device ? 1 : 0, samples_read,
+                                        duration_samples, final_call ? 1 : 0, frontier, &r));
+        return collect(r);
+    }
+    /** Over the search engine's last results, in place on the device. */
+    CandidatePostprocessResult execute(FDMTBoxcar& engine, uint64_t samples_read, uint64_t duration_samples,
+                                       bool final_call, uint64_t frontier) {
+        frost_postprocess_result r{};
+        check(frost_postprocess_execute_search(m_h, engine.handle(), samples_read, duration_samples,
+                                               final_call ? 1 : 0, frontier, &r));
+        return collect(r);
+    }
+    uint64_t memory_usage() const {
+        uint64_t b = 0;
+        check(frost_postprocess_memory_usage(m_h, &b));
+        return b;
+    }
+    static uint64_t estimate_memory(const frost_postprocess_config& cfg) {
+        uint64_t b = 0;
+        check(frost_postprocess_estimate_memory(&cfg, &b));
+        return b;
+    }
+
+private:
+    CandidatePostprocessResult collect(const frost_postprocess_result& r) {
+        CandidatePostprocessResult out;
+        out.candidates.resize(r.count);
+        size_t n = 0;
+        check(frost_postprocess_results(m_h, out.candidates.data(), out.candidates.size(), &n));
+        out.cluster_s          = r.cluster_s;
+        out.dedup_s            = r.dedup_s;
+        out.pending_candidates = r.pending_candidates;
+        return out;
+    }
+    frost_postprocess* m_h = nullptr;
+};
+
+/** search::ClusterLabelPlan (clustering.hpp:51-66) on the device. */
+class ClusterLabelPlan {
+public:
+    explicit ClusterLabelPlan(int mode = FROST_CLUSTER_CHAIN, int device = 0) : m_mode(mode), m_device(device) {}
+    std::vector<uint64_t> execute(std::span<const frost_giant> giants, const frost_cluster_tolerances& tol) const {
+        std::vector<uint64_t> labels(giants.size());
+        check(frost_cluster_labels(giants.data(), giants.size(), &tol, m_mode, labels.data(), m_device));
+        return labels;
+    }
+
+private:
+    int m_mode, m_device;
+};
+
+/** search::MergeCandidatesPlan (merge.hpp:16-24) on the device. */
+class MergeCandidatesPlan {
+public:
+    explicit MergeCandidatesPlan(int device = 0) : m_device(device) {}
+    std::vector<frost_giant> execute(std::span<const frost_giant> giants, std::span<const uint64_t> labels) const {
+        if (giants.size() != labels.size())
+            throw std::invalid_argument("candidates/labels size mismatch");
+        std::vector<frost_giant> out(giants.size());
+        size_t n = 0;
+        check(frost_merge_candidates(giants.data(), labels.data(), giants.size(), out.data(), &n, m_device));
+        out.resize(n);
+        return out;
+    }
+
+private:
+    int m_device;
+};
+
+/** search::SubbandDedupPlan (subband_dedup.hpp:62-77) on the device. */
+class SubbandDedupPlan {
+public:
+    explicit SubbandDedupPlan(int mode = FROST_DEDUP_TRANSITIVE, int device = 0) : m_mode(mode), m_device(device) {}
+    std::vector<frost_giant> execute(std::span<const frost_giant> giants, const frost_cluster_tolerances& tol,
+                                     float tsamp) const {
+        std::vector<frost_giant> out(giants.size());
+        size_t n = 0;
+        check(frost_subband_dedup(giants.data(), giants.size(), &tol, tsamp, m_mode, out.data(), &n, m_device));
+        out.resize(n);
+        return out;
+    }
+
+private:
+    int m_mode, m_device;
+};
+
+inline bool are_coincident(const frost_giant& a, const frost_giant& b, uint64_t time_tol, uint64_t filter_tol,
+                           uint64_t dm_tol) {
+    const frost_cluster_tolerances t{time_tol, filter_tol, dm_tol, 0.0, 0.0, 0.0};
+    return frost_are_coincident(&a, &b, &t, 0) != 0;
+}
+inline bool are_coincident(const frost_giant& a, const frost_giant& b, const frost_cluster_tolerances& tol) {
+    return frost_are_coincident(&a, &b, &tol, 1) != 0;
+}
+inline double subband_time_shift_samples(float dm, float f_wide, float f_narrow, float tsamp) {
+    return frost_subband_time_shift_samples(dm, f_wide, f_narrow, tsamp);
+}
+inline double subband_dm_step(float f_low, float f_high, float tsamp) {
+    return frost_subband_dm_step(f_low, f_high, tsamp);
+}
 
 } // namespace frost::b200

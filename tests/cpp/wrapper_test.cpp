@@ -53,6 +53,36 @@ static int cpu_mode() {
         std::cout << "validate accepted a bad config\n";
         return 1;
     }
+    // post-processing host helpers (candidate_test.cpp:14-30)
+    frost_giant a{}, b{};
+    a.samp_idx = 1000, a.filter_idx = 3, a.dm_idx = 10, a.members = b.members = 1;
+    b            = a;
+    b.samp_idx   = 1040;
+    const bool in = fb::are_coincident(a, b, 5, 1, 2);
+    b.samp_idx    = 1048;
+    const bool out = fb::are_coincident(a, b, 5, 1, 2);
+    if (!in || out) {
+        std::cout << "are_coincident wrong\n";
+        return 1;
+    }
+    if (!(fb::subband_dm_step(1000.0F, 1256.0F, 0.001F) > 0.0) ||
+        !(fb::subband_time_shift_samples(100.0F, 1000.0F, 1100.0F, 0.001F) > 13.0)) {
+        std::cout << "dispersion helpers wrong\n";
+        return 1;
+    }
+    const auto ppc = fb::default_postprocess_config();
+    if (fb::CandidatePostprocessPlan::estimate_memory(ppc) == 0) {
+        std::cout << "estimate_memory zero\n";
+        return 1;
+    }
+    try {
+        frost_postprocess_layout bad_layout{8, 0.0, 1.0};
+        fb::CandidatePostprocessPlan plan(ppc, bad_layout);
+        std::cout << "bad layout accepted\n";
+        return 1;
+    } catch (const std::invalid_argument&) {
+        std::cout << "postprocess invalid_argument\n";
+    }
     std::cout << "ok\n";
     return 0;
 }

@@ -155,3 +155,42 @@ def test_uneven_beams_served_together_match_each_alone():
         assert np.array_equal(srv.drain(b), alone[i][2]), i
     assert sum(len(c) for per in alone for c in per) > 0
     srv.close()
+
+
+def test_served_postprocessing_matches_pipeline_and_oracle():
+    """A served beam with a post-processor gives per gulp the giants of the
+    single-beam pipeline with post-processing, and both equal the CPU
+    oracle's plan fed the same raw candidates (samples read, gulp rows and
+    the engine's frontier, as Pipeline::publish passes them)."""
+    from frost_b200.pipeline import GulpPipeline
+    from frost_b200.postprocess import CandidatePostprocessLayout, SearchConfig
+    from frost_b200.serve import BeamServer
+    from oracle import postprocess as op
+    from tests.postprocess_cases import same_giants
+    rfi, layout, plan, bc = _setup()
+    ppcfg = SearchConfig(boxcar_max=bc.max_boxcar, detect_thresh=bc.detect_thresh, max_candidates=bc.max_candidates)
+    streams = [_beam_stream(s) for s in (31, 32)]
+    srv = BeamServer(slots=2)
+    beams = [srv.add_beam(rfi, layout, 1.0, plan, bc) for _ in streams]
+    for b in beams:
+        srv.set_postprocess(b, ppcfg)
+    tickets = [[srv.submit(b, st[g * GULP:(g + 1) * GULP], _nread(g)) for g in range(NGULPS)]
+               for b, st in zip(beams, streams)]
+    total = 0
+    for i, b in enumerate(beams):
+        p = GulpPipeline(rfi, layout, 1.0, plan, bc, postprocess=ppcfg)
+        orc = op.backend("oracle").plan(ppcfg, CandidatePostprocessLayout(layout.nchans, layout.tsamp, layout.df))
+        for g, t in enumerate(tickets[i]):
+            giants, _ = srv.wait_giants(t)
+            res = p.execute(streams[i][g * GULP:(g + 1) * GULP], _nread(g))
+            ref, _ = orc.execute(res.candidates, p.samples_read, _nread(g), False, p.search.get_candidate_frontier())
+            assert same_giants(giants, p.postprocessed.candidates), (i, g)
+            assert same_giants(giants, ref), (i, g)
+            total += giants.size
+        last = srv.drain_giants(b)
+        res = p.flush()
+        ref, pend = orc.execute(res.candidates, p.samples_read, _nread(NGULPS - 1), True,
+                                p.search.get_candidate_frontier())
+        assert same_giants(last, p.postprocessed.candidates) and same_giants(last, ref) and pend == 0
+        total += last.size
+    assert total > 0
