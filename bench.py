@@ -213,6 +213,7 @@ def run_gpu(args):
 
     def measure(storage, e2e=False, sample_clocks=False):
         pipe = GulpPipeline(rfi_config(), lay, 2.0, plan, search_config(storage), device=local)
+        tuned = pipe.search.autotune()  # the same launch-shape choice the server makes per beam
         step = (lambda: pipe.execute_device(pinned.data_ptr(), GULP, on_device=False)) if e2e else \
                (lambda: pipe.execute_device(raw_dev.data_ptr(), GULP, on_device=True))
         for _ in range(args.warmup):
@@ -242,7 +243,7 @@ def run_gpu(args):
         timing = pipe.search.timing()
         launches = timing["total_launches"] + (pipe.rfi.launches() - l0)
         rep = pipe.rfi.report()
-        out = {"total_ms": max_over_ranks(total_ms), "lat": lat, "timing": timing,
+        out = {"total_ms": max_over_ranks(total_ms), "lat": lat, "timing": timing, "tuned": tuned,
                "launches": launches, "ncands": ncands, "d2h": d2h,
                "dropped": [res.dropped_global, res.dropped_per_dm],
                "clocks": sampler.summary() if sampler else None,
@@ -335,7 +336,8 @@ def run_gpu(args):
     traffic = ncu_traffic_per_launch()
     roofline = {
         "bound": "hbm",
-        "kernel": "k_level_pipe<__half> (FDMT levels 2-12, plain FP16 single-beam run)",
+        "kernel": ("FDMT level phase: k_level2_pipe<__half> (two levels per pass) + k_level_pipe<__half> "
+                   "(single levels), plain FP16 single-beam run"),
         "achieved": round(level_gbs, 1),
         "peak": peak,
         "unit": "GB/s",
@@ -374,9 +376,10 @@ def run_gpu(args):
                        "max": round(st.max_latency_s * 1e3, 2), "realtime_gulp_ms": gulp_s * 1e3,
                        "what": "served gulp, submit to candidates ready, one gulp in flight per beam"},
         "plain_fp32": {"value": round(plain32, 3), "ms_per_step": round(single32["total_ms"] / args.steps, 3),
-                       "what": "single beam, FP32 planes, no server"},
+                       "what": "single beam, FP32 planes, no server", "launch_shape": single32["tuned"]},
         "plain_fp16": {"value": round(plain16, 3), "ms_per_step": round(single16["total_ms"] / args.steps, 3),
-                       "p50_ms": round(p(0.5), 2), "p99_ms": round(p(0.99), 2)},
+                       "p50_ms": round(p(0.5), 2), "p99_ms": round(p(0.99), 2),
+                       "launch_shape": single16["tuned"]},
         "served_vs_plain_fp32": round(value / plain32, 3),
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
                 "h2d_bytes_per_step": nbytes * e2e["beams"],

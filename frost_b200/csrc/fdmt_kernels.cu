@@ -342,12 +342,11 @@ __device__ __forceinline__ void load8(const S* stage, int e, int off, float (&x)
 
 template <class S> constexpr int kStages2 = sizeof(S) == 2 ? 4 : 3;
 
-template <class S>
+template <class S, int NS>
 __global__ void __launch_bounds__(kThreads)
     k_level2_pipe(const FusedOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
                   int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
                   int32_t ntiles, int32_t tpc, unsigned* __restrict__ err) {
-    constexpr int NS        = kStages2<S>;
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -647,8 +646,31 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
     FB_LAUNCH_CHECK();
 }
 
+namespace {
+template <class S, int NS>
+void level2_stages(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
+                   unsigned* err, cudaStream_t s) {
+    const size_t smem = NS * (4 * kTimePerCta * sizeof(S) + 48);
+    FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<S, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    k_level2_pipe<S, NS><<<grid, kThreads, smem, s>>>(ops, static_cast<const S*>(in.data), in.pitch, in.base,
+                                                      static_cast<S*>(out.data), out.pitch, out.base, ntiles,
+                                                      tpc, err);
+}
+template <class S>
+void level2_typed(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
+                  int32_t stages, unsigned* err, cudaStream_t s) {
+    switch (stages == 0 ? kStages2<S> : stages) {
+    case 2: level2_stages<S, 2>(ops, grid, in, out, ntiles, tpc, err, s); break;
+    case 3: level2_stages<S, 3>(ops, grid, in, out, ntiles, tpc, err, s); break;
+    case 4: level2_stages<S, 4>(ops, grid, in, out, ntiles, tpc, err, s); break;
+    default: throw Error(FROST_ERR_INTERNAL, "level2: stages must be 2, 3 or 4");
+    }
+}
+} // namespace
+
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                   unsigned* err, cudaStream_t s, int32_t tpc) {
+                   unsigned* err, cudaStream_t s, int32_t tpc, int32_t stages) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
@@ -656,25 +678,14 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
         throw Error(FROST_ERR_INTERNAL, "level2: bad geometry");
     if (tpc < 1 || tpc > 64)
         throw Error(FROST_ERR_INTERNAL, "level2: tiles per CTA must be in [1, 64]");
+    if (stages == 4 && !out.fp16)
+        throw Error(FROST_ERR_INTERNAL, "level2: 4 float stages exceed the shared memory of a CTA");
     const int ntiles = ncols / kTimePerCta;
-    const dim3 grid(static_cast<unsigned>(nrows),
-                    static_cast<unsigned>((ntiles + tpc - 1) / tpc));
-    const size_t es = out.fp16 ? 2 : 4;
-    if (out.fp16) {
-        const size_t smem = kStages2<__half> * (4 * kTimePerCta * es + 48);
-        FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-        k_level2_pipe<__half><<<grid, kThreads, smem, s>>>(
-            ops, static_cast<const __half*>(in.data), in.pitch, in.base,
-            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, err);
-    } else {
-        const size_t smem = kStages2<float> * (4 * kTimePerCta * es + 48);
-        FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-        k_level2_pipe<float><<<grid, kThreads, smem, s>>>(
-            ops, static_cast<const float*>(in.data), in.pitch, in.base,
-            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, err);
-    }
+    const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>((ntiles + tpc - 1) / tpc));
+    if (out.fp16)
+        level2_typed<__half>(ops, grid, in, out, ntiles, tpc, stages, err, s);
+    else
+        level2_typed<float>(ops, grid, in, out, ntiles, tpc, stages, err, s);
     FB_LAUNCH_CHECK();
 }
 

@@ -45,9 +45,11 @@ struct FusedOp {
 };
 
 /** Level h+1 straight from level h-1 (TMA-pipelined; *err set if a bounded
- * wait ran out). */
+ * wait ran out). `stages` tiles in flight per CTA (2, 3 or 4; 4 only with
+ * fp16 storage; 0 = 4 for fp16, 3 for float): fewer stages leave room for
+ * more CTAs per SM. */
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                   unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16);
+                   unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t stages = 0);
 
 /** Copies the last `hist` columns ending at column base + n_valid of every
  * row of `view` into hist_buf[rows][hist]. */

@@ -254,13 +254,15 @@ void Engine::build_schedule(bool fuse) {
 //
 // The FDMT launch shape is measured, not assumed: for this plan's geometry
 // the engine times one tile pass for every candidate (fused two-level steps
-// or single levels; 4, 8, 16 or 32 tiles of 2048 columns per level-kernel
-// CTA) on a zero waterfall, keeps the fastest and caches it for the
-// process by geometry, then restores a fresh stream state.
+// with 2, 3 or 4 bulk-copy stages, or single levels; 4, 8, 16 or 32 tiles
+// of 2048 columns per level-kernel CTA) on a zero waterfall (the level
+// kernels always process the tile's full width), keeps the fastest and
+// caches it for the process by geometry, then restores a fresh stream state.
 namespace {
 struct TuneChoice {
     bool fuse;
     int32_t tpc;
+    int32_t stages;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -278,7 +280,7 @@ Engine::Tuned Engine::autotune() {
         key += "|" + std::to_string(m_plan.level_rows(h));
     for (const auto& p : m_plan.planes())
         key += "|p" + std::to_string(p.height);
-    TuneChoice best{true, 16, 0.0};
+    TuneChoice best{true, 16, 0, 0.0};
     bool cached = false;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -308,17 +310,23 @@ Engine::Tuned Engine::autotune() {
             if (plan_bytes(m_tile) > m_budget)
                 continue;
             allocate(m_tile);
-            for (const int32_t tpc : {4, 8, 16, 32}) {
-                m_level_tpc = tpc;
-                run_tiles(wf.as<float>(), ncols, s); // warm-up
-                FB_CUDA(cudaEventRecord(a, s));
-                run_tiles(wf.as<float>(), ncols, s);
-                FB_CUDA(cudaEventRecord(b, s));
-                FB_CUDA(cudaEventSynchronize(b));
-                float ms = 0.0F;
-                FB_CUDA(cudaEventElapsedTime(&ms, a, b));
-                if (best.ms < 0.0 || ms < best.ms)
-                    best = {fuse, tpc, ms};
+            std::vector<int32_t> stage_options{0};
+            if (fuse)
+                stage_options = m_fp16 ? std::vector<int32_t>{2, 3, 4} : std::vector<int32_t>{2, 3};
+            for (const int32_t stages : stage_options) {
+                for (const int32_t tpc : {4, 8, 16, 32}) {
+                    m_level_tpc     = tpc;
+                    m_level2_stages = stages;
+                    run_tiles(wf.as<float>(), ncols, s); // warm-up
+                    FB_CUDA(cudaEventRecord(a, s));
+                    run_tiles(wf.as<float>(), ncols, s);
+                    FB_CUDA(cudaEventRecord(b, s));
+                    FB_CUDA(cudaEventSynchronize(b));
+                    float ms = 0.0F;
+                    FB_CUDA(cudaEventElapsedTime(&ms, a, b));
+                    if (best.ms < 0.0 || ms < best.ms)
+                        best = {fuse, tpc, stages, ms};
+                }
             }
         }
         cudaEventDestroy(a);
@@ -329,14 +337,15 @@ Engine::Tuned Engine::autotune() {
     // apply the choice and start the stream afresh
     build_schedule(best.fuse);
     allocate(m_tile);
-    m_level_tpc = best.tpc;
-    m_samples   = 0;
+    m_level_tpc     = best.tpc;
+    m_level2_stages = best.stages;
+    m_samples       = 0;
     m_var_ready = false;
     const SizeType nruns = m_cfg.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : m_plan.widths().size();
     FB_CUDA(cudaMemsetAsync(m_carry.get(), 0, m_nsearch * nruns * sizeof(RunState), s));
     FB_CUDA(cudaStreamSynchronize(s));
     m_timing_on = timing_was;
-    return Tuned{best.fuse, best.tpc, best.ms, cached};
+    return Tuned{best.fuse, best.tpc, best.stages, best.ms, cached};
 }
 
 Engine::~Engine() {
@@ -643,7 +652,8 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                 timed(kLevel, s, [&] {
                     if (st.fused)
                         launch_level2(m_fused_ops.as<FusedOp>() + st.op_offset, m_plan.level_rows(h),
-                                      view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc);
+                                      view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc,
+                                      m_level2_stages);
                     else
                         launch_level(m_row_ops.as<RowOp>() + st.op_offset, m_plan.level_rows(h),
                                      view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc);

@@ -100,12 +100,14 @@ private:
     DeviceBuffer m_fused_ops;
     bool m_fuse        = true; // fused two-level steps in the schedule
     int32_t m_level_tpc = 16;  // tiles of 2048 columns per level-kernel CTA
+    int32_t m_level2_stages = 0; // bulk-copy stages of the fused kernel (0: its default)
     void build_schedule(bool fuse);
     SizeType m_budget = 0; // device memory budget of the plan
   public:
     struct Tuned {
         bool fuse;
         int32_t tiles_per_cta;
+        int32_t stages; // fused kernel's stages (0 = default or not fused)
         double ms;   // one tile pass with the choice (0 if taken from the cache)
         bool cached;
     };
