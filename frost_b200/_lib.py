@@ -67,6 +67,9 @@ SIGNATURES = {
     "frost_search_use_graphs": (C.c_int, [_vp, C.c_int]),
     "frost_search_autotune": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
                                         C.POINTER(C.c_int)]),
+    "frost_search_set_launch_shape": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "frost_search_get_launch_shape": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                                C.POINTER(C.c_int)]),
     "frost_search_enable_timing": (C.c_int, [_vp, C.c_int]),
     "frost_search_get_timing": (C.c_int, [_vp, C.POINTER(_abi.SearchTimingC)]),
     "frost_server_create": (C.c_int, [C.c_int, _sz, C.c_uint32, C.POINTER(_vp)]),

@@ -599,6 +599,31 @@ int frost_search_autotune(frost_search* s, int* fused, int* tiles_per_cta, doubl
     });
 }
 
+int frost_search_set_launch_shape(frost_search* s, int fused, int tiles_per_cta, int stages, int search_chunk) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_set_launch_shape: null handle");
+        s->impl.set_launch_shape(fused != 0, tiles_per_cta, stages, search_chunk);
+    });
+}
+
+int frost_search_get_launch_shape(const frost_search* s, int* fused, int* tiles_per_cta, int* stages,
+                                  int* search_chunk) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_get_launch_shape: null handle");
+        const auto t = s->impl.launch_shape();
+        if (fused != nullptr)
+            *fused = t.fuse ? 1 : 0;
+        if (tiles_per_cta != nullptr)
+            *tiles_per_cta = t.tiles_per_cta;
+        if (stages != nullptr)
+            *stages = t.stages;
+        if (search_chunk != nullptr)
+            *search_chunk = t.search_chunk;
+    });
+}
+
 int frost_search_use_graphs(frost_search* s, int enable) {
     return guarded([&] {
         if (s == nullptr)

@@ -258,11 +258,16 @@ void Engine::build_schedule(bool fuse) {
 // of 2048 columns per level-kernel CTA) on a zero waterfall (the level
 // kernels always process the tile's full width), keeps the fastest and
 // caches it for the process by geometry, then restores a fresh stream state.
+// The search chunk stays at 4096 samples: a zero waterfall exercises only
+// the search's no-detection path, where 2048-sample chunks look faster, but
+// on real detections (4096 channels, DM 0-2000) they are slower (38 vs 32 ms
+// per gulp), so it is a manual option (set_launch_shape), not a tuned one.
 namespace {
 struct TuneChoice {
     bool fuse;
     int32_t tpc;
     int32_t stages;
+    int32_t chunk;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -280,7 +285,7 @@ Engine::Tuned Engine::autotune() {
         key += "|" + std::to_string(m_plan.level_rows(h));
     for (const auto& p : m_plan.planes())
         key += "|p" + std::to_string(p.height);
-    TuneChoice best{true, 16, 0, 0.0};
+    TuneChoice best{true, 16, 0, kSearchChunk, 0.0};
     bool cached = false;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -325,7 +330,7 @@ Engine::Tuned Engine::autotune() {
                     float ms = 0.0F;
                     FB_CUDA(cudaEventElapsedTime(&ms, a, b));
                     if (best.ms < 0.0 || ms < best.ms)
-                        best = {fuse, tpc, stages, ms};
+                        best = {fuse, tpc, stages, kSearchChunk, ms};
                 }
             }
         }
@@ -335,17 +340,44 @@ Engine::Tuned Engine::autotune() {
         g_tune_cache[key] = best;
     }
     // apply the choice and start the stream afresh
-    build_schedule(best.fuse);
+    apply_shape(best.fuse, best.tpc, best.stages, best.chunk);
+    m_timing_on = timing_was;
+    return Tuned{best.fuse, best.tpc, best.stages, best.chunk, best.ms, cached};
+}
+
+void Engine::apply_shape(bool fuse, int32_t tpc, int32_t stages, int32_t chunk) {
+    cudaStream_t s = m_stream;
+    build_schedule(fuse);
     allocate(m_tile);
-    m_level_tpc     = best.tpc;
-    m_level2_stages = best.stages;
+    m_level_tpc     = tpc;
+    m_level2_stages = stages;
+    m_search_chunk  = chunk;
     m_samples       = 0;
-    m_var_ready = false;
+    m_var_ready     = false;
     const SizeType nruns = m_cfg.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : m_plan.widths().size();
     FB_CUDA(cudaMemsetAsync(m_carry.get(), 0, m_nsearch * nruns * sizeof(RunState), s));
     FB_CUDA(cudaStreamSynchronize(s));
-    m_timing_on = timing_was;
-    return Tuned{best.fuse, best.tpc, best.stages, best.ms, cached};
+}
+
+void Engine::set_launch_shape(bool fuse, int32_t tpc, int32_t stages, int32_t chunk) {
+    if (tpc < 1 || tpc > 64)
+        invalid("search: tiles per CTA must be in [1, 64]");
+    if (stages != 0 && stages != 2 && stages != 3 && !(stages == 4 && m_fp16))
+        invalid("search: fused stages must be 0, 2, 3 (or 4 with fp16 storage)");
+    if (chunk != 2048 && chunk != 4096)
+        invalid("search: the search chunk must be 2048 or 4096 samples");
+    DeviceGuard g(m_device);
+    const bool was = m_fuse;
+    build_schedule(fuse);
+    if (plan_bytes(m_tile) > m_budget) {
+        build_schedule(was);
+        throw Error(FROST_ERR_OUT_OF_MEMORY, "search: the launch shape does not fit the memory budget");
+    }
+    apply_shape(fuse, tpc, stages, chunk);
+}
+
+Engine::Tuned Engine::launch_shape() const {
+    return Tuned{m_fuse, m_level_tpc, m_level2_stages, m_search_chunk, 0.0, false};
 }
 
 Engine::~Engine() {
@@ -667,7 +699,8 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                 launch_load_history(out, m_plan.level_rows(h), m_hist_len[h], m_hist[h].get(), s);
             });
             if (m_height_g1[h] > m_height_g0[h]) {
-                timed(kSearch, s, [&] { launch_search(sp, out, m_height_g0[h], m_height_g1[h], s); });
+                timed(kSearch, s,
+                      [&] { launch_search(sp, out, m_height_g0[h], m_height_g1[h], s, m_search_chunk); });
                 m_launches += 1;
                 m_timing.search_launches += 1;
                 m_timing.algorithmic_search_bytes +=

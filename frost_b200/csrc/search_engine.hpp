@@ -101,19 +101,26 @@ private:
     bool m_fuse        = true; // fused two-level steps in the schedule
     int32_t m_level_tpc = 16;  // tiles of 2048 columns per level-kernel CTA
     int32_t m_level2_stages = 0; // bulk-copy stages of the fused kernel (0: its default)
+    int32_t m_search_chunk  = kSearchChunk; // samples per search-kernel step
     void build_schedule(bool fuse);
+    void apply_shape(bool fuse, int32_t tpc, int32_t stages, int32_t chunk);
     SizeType m_budget = 0; // device memory budget of the plan
   public:
     struct Tuned {
         bool fuse;
         int32_t tiles_per_cta;
         int32_t stages; // fused kernel's stages (0 = default or not fused)
+        int32_t search_chunk;
         double ms;   // one tile pass with the choice (0 if taken from the cache)
         bool cached;
     };
     /** Measures the FDMT launch shapes for this geometry, applies the fastest
      * and restarts the stream (call before the first gulp). */
     Tuned autotune();
+    /** Pins a launch shape (as autotune would set it) and restarts the
+     * stream (call before the first gulp). */
+    void set_launch_shape(bool fuse, int32_t tiles_per_cta, int32_t stages, int32_t search_chunk);
+    Tuned launch_shape() const;
   private:
     std::vector<DeviceBuffer> m_capture;
     bool m_capture_on = false;

@@ -1,6 +1,7 @@
 // Boxcar/trapezoid matched filter, exact noise and peak finding on sm_100a.
 //
-// One CTA per searched (plane, DM) row walks the tile in 4096-sample chunks.
+// One CTA per searched (plane, DM) row walks the tile in chunks of 2048 or
+// 4096 samples (a launch-shape choice).
 // The chunk plus a halo of the widest boxcar (rounded to 256 columns) is
 // bulk-copied into shared memory one chunk ahead, prefix-summed (warp
 // shuffles, then one offset per warp), and every width's window sum is a
@@ -32,9 +33,6 @@ namespace fb::fdmt {
 namespace {
 
 constexpr int kThreads   = 256;
-constexpr int kChunk     = kSearchChunk;
-constexpr int kPerThread = kChunk / kThreads;
-constexpr int kWords     = kChunk / 32;
 constexpr int kMaxWidths = 32;
 #define FB_NEG_INF (-__int_as_float(0x7f800000))
 #define FB_POS_INF (__int_as_float(0x7f800000))
@@ -208,11 +206,12 @@ __device__ void emit(const SearchParams& p, const SearchRow& row, const RunState
 
 // Walks the set bits of one chunk's mask in time order (one lane). For the
 // across-widths mode `wi` < 0: the peak is the best S/N over widths.
+template <int CH>
 __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float* Q, int64_t c0,
                           int32_t delay, const uint32_t* bits, int wi, RunState& run,
                           const SearchRow& row, uint32_t* count) {
     int64_t last = run.open ? c0 - 1 : -2; // tile column of the last set bit
-    for (int wd = 0; wd < kWords; ++wd) {
+    for (int wd = 0; wd < (CH / 32); ++wd) {
         uint32_t b = bits[wd];
         while (b) {
             const int bit     = __ffs(b) - 1;
@@ -255,29 +254,29 @@ __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float
         }
     }
     // A run that does not reach the chunk's last valid column has closed.
-    const int64_t chunk_end = min(c0 + kChunk, static_cast<int64_t>(p.n_valid));
+    const int64_t chunk_end = min(c0 + CH, static_cast<int64_t>(p.n_valid));
     if (run.open && last != chunk_end - 1) {
         emit(p, row, run, count);
         run.open = 0;
     }
 }
 
-// Words of the per-width bit masks [nw][kWords].
-__host__ __device__ constexpr int search_bits_words(int nw) { return nw * kWords; }
+// Words of the per-width bit masks [nw][chunk / 32].
+__host__ __device__ constexpr int search_bits_words(int nw, int chunk) { return nw * (chunk / 32); }
 
-template <class S>
-__global__ void __launch_bounds__(kThreads, 4)
+template <class S, int CH>
+__global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0) {
     // Dynamic shared memory: Ps, the chunk's prefix sums over columns
-    // [c0 - halo, c0 + kChunk) after 4 floats of padding (Q = Ps + 4 + halo
+    // [c0 - halo, c0 + CH) after 4 floats of padding (Q = Ps + 4 + halo
     // puts sample k of the chunk at Q[k], 16-byte aligned); gmin / gmax, the
     // least and greatest of each aligned group of 4 prefix values; the
-    // per-width bit masks [nw][kWords]; two staging buffers of the raw row
+    // per-width bit masks [nw][(CH / 32)]; two staging buffers of the raw row
     // segment, filled by bulk copies one chunk ahead.
     extern __shared__ __align__(16) float Ps[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int abort_flag;
-    __shared__ uint32_t any_bits[kWords];
+    __shared__ uint32_t any_bits[(CH / 32)];
     __shared__ RunState runs[kMaxWidths];
     __shared__ RowConst rc;
     __shared__ uint32_t local_count;
@@ -316,17 +315,17 @@ __global__ void __launch_bounds__(kThreads, 4)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* Q       = Ps + 4 + halo;
     const S* src   = level + row.level_row * pitch + base;
-    const int seg_cols       = halo + kChunk;
+    const int seg_cols       = halo + CH;
     const uint32_t seg_bytes = static_cast<uint32_t>(seg_cols * sizeof(S));
     const int ngroups        = seg_cols / 4;
     float* const gmin        = Ps + 4 + seg_cols + 4;
     float* const gmax        = gmin + ngroups;
     uint32_t* const bits     = reinterpret_cast<uint32_t*>(gmax + ngroups);
-    S* const stage0 = reinterpret_cast<S*>(bits + search_bits_words(nw)); // buffer b at stage0 + b * seg_cols
-    const int nchunks = (p.n_valid + kChunk - 1) / kChunk;
+    S* const stage0 = reinterpret_cast<S*>(bits + search_bits_words(nw, CH)); // buffer b at stage0 + b * seg_cols
+    const int nchunks = (p.n_valid + CH - 1) / CH;
     auto issue = [&](int ci) {
         bulk::mbar_expect(&bar[ci & 1], seg_bytes);
-        bulk::load(stage0 + (ci & 1) * seg_cols, src + static_cast<int64_t>(ci) * kChunk - halo, seg_bytes,
+        bulk::load(stage0 + (ci & 1) * seg_cols, src + static_cast<int64_t>(ci) * CH - halo, seg_bytes,
                    &bar[ci & 1]);
     };
     if (threadIdx.x == 0) {
@@ -345,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     const int jmin  = halo - wmax + 1; // earlier columns never enter a window
     const int64_t warm = static_cast<int64_t>(row.delay) + wmax - 1;
     int ci = 0;
-    for (int64_t c0 = 0; c0 < p.n_valid; c0 += kChunk, ++ci) {
+    for (int64_t c0 = 0; c0 < p.n_valid; c0 += CH, ++ci) {
         // ---- wait for the chunk's segment (bounded; a timeout ends the row)
         if (!bulk::mbar_wait(&bar[ci & 1], static_cast<uint32_t>((ci >> 1) & 1)))
             atomicExch(&abort_flag, 1);
@@ -392,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, 4)
             issue(ci + 2);
         // clear the bit masks (a steady chunk sets only the words of
         // samples that fired)
-        for (int i = threadIdx.x; i < nw * kWords; i += kThreads)
+        for (int i = threadIdx.x; i < nw * (CH / 32); i += kThreads)
             bits[i] = 0U;
         if (threadIdx.x == 0)
             fired_w = 0U;
@@ -419,7 +418,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         }
         __syncthreads();
 
-        const bool fast = c0 + kChunk <= p.n_valid && (!p.skip_cold || rc.tile_t0 + c0 >= warm) &&
+        const bool fast = c0 + CH <= p.n_valid && (!p.skip_cold || rc.tile_t0 + c0 >= warm) &&
                           (!rc.or_active || rc.tile_t0 + c0 - rc.gulp_t0 >= warm);
         if (fast) {
             // ---- steady state. Group gi = samples 4 gi .. 4 gi + 3. A window
@@ -453,12 +452,12 @@ __global__ void __launch_bounds__(kThreads, 4)
                                      (s3 > T ? 8U : 0U);
                 if (nib != 0U) {
                     // samples 4 gi .. 4 gi + 3: word gi / 8, nibble gi % 8
-                    atomicOr(&bits[wi * kWords + (gi >> 3)], nib << ((gi & 7) * 4));
+                    atomicOr(&bits[wi * (CH / 32) + (gi >> 3)], nib << ((gi & 7) * 4));
                     atomicOr(&fired_w, 1U << wi);
                     up = true;
                 }
             };
-            constexpr int NG = kPerThread / 4; // groups per thread
+            constexpr int NG = (CH / kThreads) / 4; // groups per thread
             float hi[NG];
 #pragma unroll
             for (int q = 0; q < NG; ++q)
@@ -498,13 +497,13 @@ __global__ void __launch_bounds__(kThreads, 4)
         } else {
             // ---- not steady (cold prefix, mask change, partial chunk): the
             // bit masks from the general S/N
-            for (int j = 0; j < kPerThread; ++j) {
+            for (int j = 0; j < (CH / kThreads); ++j) {
                 const int k = threadIdx.x + j * kThreads;
                 for (int wi = 0; wi < nw; ++wi) {
                     const bool hit   = snr_general(p, rc, Q, c0, k, wi, row.delay) > p.thresh;
                     const uint32_t m = __ballot_sync(0xFFFFFFFFU, hit);
                     if (lane == 0) {
-                        bits[wi * kWords + j * (kThreads / 32) + warp] = m;
+                        bits[wi * (CH / 32) + j * (kThreads / 32) + warp] = m;
                         if (m != 0U)
                             atomicOr(&fired_w, 1U << wi);
                     }
@@ -515,11 +514,11 @@ __global__ void __launch_bounds__(kThreads, 4)
         // bits now hold exactly the above-threshold samples of every width
         const uint32_t fw = fired_w;
         if (across) {
-            for (int wd = threadIdx.x; wd < kWords; wd += kThreads) {
+            for (int wd = threadIdx.x; wd < (CH / 32); wd += kThreads) {
                 uint32_t m = 0;
                 for (int wi = 0; wi < nw; ++wi)
                     if ((fw >> wi) & 1U)
-                        m |= bits[wi * kWords + wd];
+                        m |= bits[wi * (CH / 32) + wd];
                 any_bits[wd] = m;
             }
             __syncthreads();
@@ -532,8 +531,8 @@ __global__ void __launch_bounds__(kThreads, 4)
             for (int wi = warp; wi < nw; wi += kThreads / 32) {
                 if (((fw >> wi) & 1U) == 0U)
                     continue;
-                for (int wd = 0; wd < kWords; ++wd) {
-                    uint32_t m = bits[wi * kWords + wd];
+                for (int wd = 0; wd < (CH / 32); ++wd) {
+                    uint32_t m = bits[wi * (CH / 32) + wd];
                     while (m) {
                         const int k = wd * 32 + __ffs(m) - 1;
                         m &= m - 1;
@@ -548,11 +547,11 @@ __global__ void __launch_bounds__(kThreads, 4)
         } else if (!all && !across && lane == 0) {
             for (int wi = warp; wi < nw; wi += kThreads / 32)
                 if (((fw >> wi) & 1U) != 0U || runs[wi].open)
-                    walk_runs(p, rc, Q, c0, row.delay, bits + wi * kWords, wi, runs[wi], row,
+                    walk_runs<CH>(p, rc, Q, c0, row.delay, bits + wi * (CH / 32), wi, runs[wi], row,
                               &local_count);
         }
         if (across && threadIdx.x == 0 && (fw != 0U || runs[0].open))
-            walk_runs(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
+            walk_runs<CH>(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
         __syncthreads();
     }
     if (abort_flag) {
@@ -627,31 +626,41 @@ __global__ void k_variance(const SearchRow* __restrict__ rows, const PlaneInfo* 
 
 } // namespace
 
-void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1, cudaStream_t s) {
+void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1, cudaStream_t s,
+                   int32_t chunk) {
     if (g1 <= g0 || p.n_valid <= 0)
         return;
+    if (chunk != 2048 && chunk != 4096)
+        throw Error(FROST_ERR_INTERNAL, "search: chunk must be 2048 or 4096 samples");
     if (p.nwidths > kMaxWidths)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "search: more than 32 boxcar widths");
     if (p.halo != search_halo(p.wmax) || level.base < p.halo)
         throw Error(FROST_ERR_INTERNAL, "search: level history shorter than the search halo");
-    if (level.pitch - level.base < ((p.n_valid + kChunk - 1) / kChunk) * kChunk)
+    if (level.pitch - level.base < ((p.n_valid + chunk - 1) / chunk) * chunk)
         throw Error(FROST_ERR_INTERNAL, "search: tile columns are not a whole number of chunks");
     if (p.err == nullptr)
         throw Error(FROST_ERR_INTERNAL, "search: no error flag");
     const size_t es   = level.fp16 ? 2 : 4;
-    const size_t seg  = static_cast<size_t>(p.halo) + kChunk;
+    const size_t seg  = static_cast<size_t>(p.halo) + chunk;
     const size_t smem = sizeof(float) * (4 + seg + 4 + 2 * (seg / 4)) +
-                        sizeof(uint32_t) * search_bits_words(p.nwidths) + 2 * es * seg;
+                        sizeof(uint32_t) * search_bits_words(p.nwidths, chunk) + 2 * es * seg;
     const dim3 grid(static_cast<unsigned>(g1 - g0));
     auto go = [&](auto kernel, auto data) {
         FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         kernel<<<grid, kThreads, smem, s>>>(p, data, level.pitch, level.base, g0);
     };
-    if (level.fp16)
-        go(k_search<__half>, static_cast<const __half*>(level.data));
-    else
-        go(k_search<float>, static_cast<const float*>(level.data));
+    if (level.fp16) {
+        if (chunk == 2048)
+            go(k_search<__half, 2048>, static_cast<const __half*>(level.data));
+        else
+            go(k_search<__half, 4096>, static_cast<const __half*>(level.data));
+    } else {
+        if (chunk == 2048)
+            go(k_search<float, 2048>, static_cast<const float*>(level.data));
+        else
+            go(k_search<float, 4096>, static_cast<const float*>(level.data));
+    }
     FB_LAUNCH_CHECK();
 }
 

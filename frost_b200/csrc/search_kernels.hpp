@@ -82,9 +82,12 @@ struct SearchParams {
     unsigned* err;           // set when a bounded wait for staged data ran out
 };
 
-/** Searches rows [g0, g1) (all in `level`) over the tile's valid columns. */
+/** Searches rows [g0, g1) (all in `level`) over the tile's valid columns,
+ * `chunk` (2048 or 4096) samples per step of a CTA: the smaller chunk needs
+ * half the shared memory and fewer registers, so more CTAs fit an SM, at
+ * the cost of a larger halo share. */
 void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1,
-                   cudaStream_t s);
+                   cudaStream_t s, int32_t chunk = kSearchChunk);
 
 /** Exact variance of every searched row and width for `mask` and for
  * `mask_or`: var = sum over active channels of g[L_c][w]; writes

@@ -187,7 +187,21 @@ class FDMTBoxcar:
         f, t, c = C.c_int(), C.c_int(), C.c_int()
         ms = C.c_double()
         check(lib().frost_search_autotune(self._h, C.byref(f), C.byref(t), C.byref(ms), C.byref(c)))
-        return {"fused": bool(f.value), "tiles_per_cta": t.value, "ms": ms.value, "cached": bool(c.value)}
+        out = self.launch_shape()
+        out.update({"ms": ms.value, "cached": bool(c.value)})
+        return out
+
+    def launch_shape(self) -> dict:
+        """The FDMT/search launch shape in use (autotune's choice or the default)."""
+        f, t, st, ch = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().frost_search_get_launch_shape(self._h, C.byref(f), C.byref(t), C.byref(st), C.byref(ch)))
+        return {"fused": bool(f.value), "tiles_per_cta": t.value, "stages": st.value, "search_chunk": ch.value}
+
+    def set_launch_shape(self, fused: bool = True, tiles_per_cta: int = 16, stages: int = 0,
+                         search_chunk: int = 4096):
+        """Pins a launch shape and restarts the stream (call before the first gulp)."""
+        check(lib().frost_search_set_launch_shape(self._h, 1 if fused else 0, int(tiles_per_cta), int(stages),
+                                                  int(search_chunk)))
 
     def use_graphs(self, enable: bool = True):
         """CUDA-graph replay of the per-gulp launch sequence (default on)."""

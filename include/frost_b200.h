@@ -489,12 +489,32 @@ typedef struct {
 int frost_search_use_graphs(frost_search* s, int enable);
 
 /* No counterpart in the reference. Measures this geometry's FDMT launch
- * shapes (fused two-level steps or single levels; 4, 8, 16 or 32 tiles of
- * 2048 samples per level-kernel CTA) with one tile pass each on a zero
- * waterfall, applies the fastest and restarts the stream; results are
- * cached per process by geometry. Call before the first gulp. Any output
- * pointer may be NULL. */
+ * shapes (fused two-level steps with 2, 3 or 4 bulk-copy stages, or single
+ * levels; 4, 8, 16 or 32 tiles of 2048 samples per level-kernel CTA) with
+ * one tile pass each on a zero waterfall, applies the fastest and restarts
+ * the stream; results are cached per process by geometry. The search chunk
+ * keeps its default (4096). Call before the first gulp. Any output pointer
+ * may be NULL. */
 int frost_search_autotune(frost_search* s, int* fused, int* tiles_per_cta, double* ms, int* cached);
+
+/* No counterpart in the reference. The launch shape in use (autotune's
+ * choice or the default): fused two-level steps, tiles of 2048 samples per
+ * level-kernel CTA, the fused kernel's bulk-copy stages (0 = its default:
+ * 4 with fp16 storage, 3 with float) and the search kernel's chunk (2048 or
+ * 4096 samples). */
+int frost_search_get_launch_shape(const frost_search* s,
+                                  int* fused,
+                                  int* tiles_per_cta,
+                                  int* stages,
+                                  int* search_chunk);
+
+/* No counterpart in the reference. Pins a launch shape (for example one
+ * autotune chose in an earlier process) and restarts the stream; call
+ * before the first gulp. The level shape never changes results; the search
+ * chunk changes where window sums are rounded from (relative 1e-7).
+ * FROST_ERR_OUT_OF_MEMORY if the schedule does not fit the engine's memory
+ * budget. */
+int frost_search_set_launch_shape(frost_search* s, int fused, int tiles_per_cta, int stages, int search_chunk);
 
 /* Enables (and zeroes) or disables per-phase timing. */
 int frost_search_enable_timing(frost_search* s, int enable);

@@ -85,3 +85,21 @@ def compare(gpu, oracle_cands, thresh, snr_rtol=1e-3, margin=0.02):
         if float(c["snr"]) >= thresh + margin and k not in o:
             extra.append((k, float(c["snr"])))
     return len(o), missing, extra, bad
+
+
+def same_detections(a, b, thresh, snr_rtol=1e-5, margin=0.02):
+    """Two engines' candidates agree: every peak clear of the threshold in
+    either list is in the other with the same plane, DM index, width and
+    peak sample, S/N within snr_rtol (search steps of different lengths
+    round their window sums from different prefix origins)."""
+    ka = {key((c["subband_level"], c["subband_idx"]), c["dm_idx"], c["filter_idx"], c["peak_sample"]): float(c["snr"])
+          for c in a}
+    kb = {key((c["subband_level"], c["subband_idx"]), c["dm_idx"], c["filter_idx"], c["peak_sample"]): float(c["snr"])
+          for c in b}
+    for x, y in ((ka, kb), (kb, ka)):
+        for k, s in x.items():
+            if s < thresh + margin:
+                continue
+            if k not in y or abs(y[k] - s) > snr_rtol * s:
+                return False
+    return True

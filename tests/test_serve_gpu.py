@@ -42,6 +42,7 @@ def test_served_beams_match_each_beam_alone():
     alone = []
     for st in streams:
         p = GulpPipeline(rfi, layout, 1.0, plan, bc)
+        p.search.autotune()  # the launch shape the server gives each beam (cached per geometry)
         per = [p.execute(st[g * GULP:(g + 1) * GULP], _nread(g)).candidates for g in range(NGULPS)]
         per.append(p.flush().candidates)
         alone.append(per)
@@ -141,6 +142,7 @@ def test_uneven_beams_served_together_match_each_alone():
     alone = []
     for data, layout, plan in beams:
         p = GulpPipeline(RfiConfig(), layout, 1.0, plan, bc)
+        p.search.autotune()  # the launch shape the server gives each beam (cached per geometry)
         g = layout.max_nsamps
         alone.append([p.execute(data[k * g:(k + 1) * g], g).candidates for k in range(2)] +
                      [p.flush().candidates])
@@ -179,6 +181,7 @@ def test_served_postprocessing_matches_pipeline_and_oracle():
     total = 0
     for i, b in enumerate(beams):
         p = GulpPipeline(rfi, layout, 1.0, plan, bc, postprocess=ppcfg)
+        p.search.autotune()
         orc = op.backend("oracle").plan(ppcfg, CandidatePostprocessLayout(layout.nchans, layout.tsamp, layout.df))
         for g, t in enumerate(tickets[i]):
             giants, _ = srv.wait_giants(t)
