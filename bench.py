@@ -319,7 +319,43 @@ def run_gpu(args):
         torch.cuda.empty_cache()
         return out
 
+    def measure_prefetch(storage):
+        """The plain single-beam path fed by the library's input staging: a
+        reader thread copies each gulp from host memory into pinned slots and
+        on to the device, depth 3, while the previous gulp is searched."""
+        import numpy as np
+        from frost_b200.pipeline import GulpPipeline
+        from frost_b200.staging import GulpPrefetch
+        rows = np.tile(pinned.numpy().reshape(GULP, NCHANS), (args.warmup + args.steps, 1))
+        pipe = GulpPipeline(rfi_config(), lay, 2.0, plan, search_config(storage), device=local)
+        pipe.search.autotune()
+        pf = GulpPrefetch.from_memory(rows, GULP, depth=3, device=local)
+        for _ in range(args.warmup):
+            ptr, n = pf.next()
+            pipe.execute_device(ptr, n, on_device=True)
+        torch.cuda.synchronize()
+        barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        st0 = pf.stats()
+        ev[0].record()
+        for _ in range(args.steps):
+            ptr, n = pf.next()
+            pipe.execute_device(ptr, n, on_device=True)
+        ev[1].record()
+        torch.cuda.synchronize()
+        st1 = pf.stats()
+        barrier()
+        out = {"total_ms": max_over_ranks(ev[0].elapsed_time(ev[1])),
+               "read_ms_per_gulp": round(1e3 * (st1.read_s - st0.read_s) / args.steps, 2),
+               "wait_ms_per_gulp": round(1e3 * (st1.wait_s - st0.wait_s) / args.steps, 2)}
+        pf.close()
+        del pipe, rows
+        torch.cuda.empty_cache()
+        return out
+
     single16 = measure(Storage.FP16)
+    single16_host = measure(Storage.FP16, e2e=True)
+    single16_pf = measure_prefetch(Storage.FP16)
     single32 = measure(Storage.FP32)
     served = measure_served(args.beams, on_device=True, sample_clocks=True)
     e2e = measure_served(args.beams, on_device=False)
@@ -380,6 +416,15 @@ def run_gpu(args):
         "plain_fp16": {"value": round(plain16, 3), "ms_per_step": round(single16["total_ms"] / args.steps, 3),
                        "p50_ms": round(p(0.5), 2), "p99_ms": round(p(0.99), 2),
                        "launch_shape": single16["tuned"]},
+        "plain_fp16_host_input": {
+            "value": round(per_beam_steps * gulp_s / (single16_host["total_ms"] / 1e3), 3),
+            "what": "plain FP16 from pinned host gulps, copied inside each gulp's call (no overlap)"},
+        "plain_fp16_prefetch": {
+            "value": round(per_beam_steps * gulp_s / (single16_pf["total_ms"] / 1e3), 3),
+            "read_ms_per_gulp": single16_pf["read_ms_per_gulp"],
+            "caller_wait_ms_per_gulp": single16_pf["wait_ms_per_gulp"],
+            "what": "plain FP16 fed by GulpPrefetch (reader thread: host memory -> pinned slots -> device, "
+                    "depth 3), overlapping the next gulp's read and copy with the current search"},
         "served_vs_plain_fp32": round(value / plain32, 3),
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
                 "h2d_bytes_per_step": nbytes * e2e["beams"],

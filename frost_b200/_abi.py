@@ -306,3 +306,10 @@ class PostprocessResultC(C.Structure):
         ("dedup_s", C.c_double),
         ("launches", C.c_uint64),
     ]
+
+
+class PrefetchStatsC(C.Structure):
+    _fields_ = [("gulps", C.c_uint64), ("bytes", C.c_uint64), ("read_s", C.c_double), ("wait_s", C.c_double)]
+
+
+READ_FN = C.CFUNCTYPE(C.c_long, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)

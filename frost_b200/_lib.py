@@ -88,6 +88,12 @@ SIGNATURES = {
     "frost_server_set_postprocess": (C.c_int, [_vp, C.c_uint32, C.POINTER(_abi.PostprocessConfigC)]),
     "frost_server_wait_giants": (C.c_int, [_vp, _u64, _vp, _sz, C.POINTER(_sz), C.POINTER(C.c_double)]),
     "frost_server_drain_giants": (C.c_int, [_vp, C.c_uint32, _vp, _sz, C.POINTER(_sz)]),
+    "frost_prefetch_create": (C.c_int, [_sz, _sz, C.c_int, C.c_int, _abi.READ_FN, _vp, C.POINTER(_vp)]),
+    "frost_prefetch_create_file": (C.c_int, [C.c_char_p, _u64, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "frost_prefetch_create_memory": (C.c_int, [_vp, _sz, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "frost_prefetch_next": (C.c_int, [_vp, _vp, C.POINTER(_vp), C.POINTER(_sz)]),
+    "frost_prefetch_get_stats": (C.c_int, [_vp, C.POINTER(_abi.PrefetchStatsC)]),
+    "frost_prefetch_destroy": (C.c_int, [_vp]),
     "frost_postprocess_create": (C.c_int, [C.POINTER(_abi.PostprocessConfigC), C.POINTER(_abi.PostprocessLayoutC),
                                            C.c_int, C.POINTER(_vp)]),
     "frost_postprocess_destroy": (C.c_int, [_vp]),

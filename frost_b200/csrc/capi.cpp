@@ -3,6 +3,8 @@
 // message for frost_last_error(); nothing throws across this boundary.
 
 #include <algorithm>
+#include <cstdio>
+#include <memory>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -12,6 +14,7 @@
 #include "dedisp.hpp"
 #include "host_stats.hpp"
 #include "postprocess.hpp"
+#include "prefetch.hpp"
 #include "pp_math.cuh"
 #include "rfi_cleaner.hpp"
 #include "search_engine.hpp"
@@ -71,6 +74,19 @@ struct frost_search {
 struct frost_server {
     fb::serve::Server impl;
     template <class... A> explicit frost_server(A&&... a) : impl(std::forward<A>(a)...) {}
+};
+
+struct frost_prefetch {
+    std::FILE* file = nullptr;        // the built-in file source, when used
+    const uint8_t* memory = nullptr;  // the built-in memory source, when used
+    size_t total_rows = 0, next_row = 0;
+    size_t row_bytes = 0;
+    std::unique_ptr<fb::staging::Prefetch> impl;
+    ~frost_prefetch() {
+        impl.reset(); // joins the reader before the file closes
+        if (file != nullptr)
+            std::fclose(file);
+    }
 };
 
 struct frost_postprocess {
@@ -813,6 +829,97 @@ double frost_subband_time_shift_samples(float dm, float f_wide, float f_narrow, 
 
 double frost_subband_dm_step(float f_low, float f_high, float tsamp) {
     return fb::pp::dm_step(f_low, f_high, tsamp);
+}
+
+// ---- input staging ----------------------------------------------------------------
+
+namespace {
+long read_file_rows(void* ctx, uint8_t* buf, size_t max_rows) {
+    auto* p        = static_cast<frost_prefetch*>(ctx);
+    const size_t n = std::fread(buf, p->row_bytes, max_rows, p->file);
+    if (n < max_rows && std::ferror(p->file))
+        return -1;
+    return static_cast<long>(n);
+}
+long read_memory_rows(void* ctx, uint8_t* buf, size_t max_rows) {
+    auto* p        = static_cast<frost_prefetch*>(ctx);
+    const size_t n = std::min(max_rows, p->total_rows - p->next_row);
+    if (n > 0)
+        std::memcpy(buf, p->memory + p->next_row * p->row_bytes, n * p->row_bytes);
+    p->next_row += n;
+    return static_cast<long>(n);
+}
+} // namespace
+
+int frost_prefetch_create_memory(const uint8_t* rows, size_t total_rows, size_t block_rows, size_t row_bytes,
+                                 int depth, int device, frost_prefetch** out) {
+    return guarded([&] {
+        if ((rows == nullptr && total_rows > 0) || out == nullptr)
+            invalid("frost_prefetch_create_memory: null argument");
+        *out            = nullptr;
+        auto p          = std::make_unique<frost_prefetch>();
+        p->memory       = rows;
+        p->total_rows   = total_rows;
+        p->row_bytes    = row_bytes;
+        p->impl = std::make_unique<fb::staging::Prefetch>(block_rows, row_bytes, depth, device, read_memory_rows,
+                                                          p.get());
+        *out = p.release();
+    });
+}
+
+int frost_prefetch_create(size_t block_rows, size_t row_bytes, int depth, int device, frost_read_fn read,
+                          void* ctx, frost_prefetch** out) {
+    return guarded([&] {
+        if (read == nullptr || out == nullptr)
+            invalid("frost_prefetch_create: null argument");
+        *out      = nullptr;
+        auto p    = std::make_unique<frost_prefetch>();
+        p->impl   = std::make_unique<fb::staging::Prefetch>(block_rows, row_bytes, depth, device, read, ctx);
+        *out      = p.release();
+    });
+}
+
+int frost_prefetch_create_file(const char* path, uint64_t header_bytes, size_t block_rows, size_t row_bytes,
+                               int depth, int device, frost_prefetch** out) {
+    return guarded([&] {
+        if (path == nullptr || out == nullptr)
+            invalid("frost_prefetch_create_file: null argument");
+        *out = nullptr;
+        if (row_bytes == 0)
+            invalid("frost_prefetch_create_file: row bytes must be positive");
+        auto p  = std::make_unique<frost_prefetch>();
+        p->file = std::fopen(path, "rb");
+        if (p->file == nullptr)
+            throw fb::Error(FROST_ERR_IO, std::string("frost_prefetch_create_file: cannot open ") + path);
+        if (std::fseek(p->file, static_cast<long>(header_bytes), SEEK_SET) != 0)
+            throw fb::Error(FROST_ERR_IO, "frost_prefetch_create_file: cannot seek past the header");
+        p->row_bytes = row_bytes;
+        p->impl = std::make_unique<fb::staging::Prefetch>(block_rows, row_bytes, depth, device, read_file_rows,
+                                                          p.get());
+        *out = p.release();
+    });
+}
+
+int frost_prefetch_next(frost_prefetch* p, void* stream, const uint8_t** block_device, size_t* nread) {
+    return guarded([&] {
+        if (p == nullptr || block_device == nullptr || nread == nullptr)
+            invalid("frost_prefetch_next: null argument");
+        fb::SizeType n = 0;
+        *block_device  = p->impl->next(&n, static_cast<cudaStream_t>(stream));
+        *nread         = n;
+    });
+}
+
+int frost_prefetch_get_stats(const frost_prefetch* p, frost_prefetch_stats* out) {
+    return guarded([&] {
+        if (p == nullptr || out == nullptr)
+            invalid("frost_prefetch_get_stats: null argument");
+        *out = p->impl->stats();
+    });
+}
+
+int frost_prefetch_destroy(frost_prefetch* p) {
+    return guarded([&] { delete p; });
 }
 
 } // extern "C"

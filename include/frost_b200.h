@@ -598,6 +598,72 @@ int frost_server_drain(frost_server* s,
 int frost_server_get_stats(frost_server* s, frost_server_stats* out);
 int frost_server_reset_stats(frost_server* s);
 
+/* ---- input staging (GulpPrefetch, lib/pipeline/pipeline.cpp:105-262) -----
+ *
+ * frost's GulpPrefetch reads the next block on a thread while the caller
+ * searches the current one. Here a reader thread fills pinned host slots
+ * from a block source and copies each to a device slot on its own stream,
+ * so reading and the host-to-device copy of gulp k+1 overlap the kernels of
+ * gulp k; gulps come out in order, already on the device. */
+
+/* A block source: writes up to `max_rows` packed rows into `buf` and
+ * returns how many (fewer than max_rows at the end, 0 once exhausted) or a
+ * negative value on error. Called on the prefetch thread. */
+typedef long (*frost_read_fn)(void* ctx, uint8_t* buf, size_t max_rows);
+
+typedef struct {
+    uint64_t gulps;
+    uint64_t bytes;
+    double read_s; /* reader thread: source reads and copy issue */
+    double wait_s; /* caller blocked in frost_prefetch_next */
+} frost_prefetch_stats;
+
+typedef struct frost_prefetch frost_prefetch;
+
+/* `depth` slots (2-8) of block_rows x row_bytes, pinned on the host and
+ * resident on `device`; the reader starts at once. */
+int frost_prefetch_create(size_t block_rows,
+                          size_t row_bytes,
+                          int depth,
+                          int device,
+                          frost_read_fn read,
+                          void* ctx,
+                          frost_prefetch** out);
+
+/* The same over a file of packed rows after `header_bytes` of header (a
+ * SIGPROC filterbank's data section, for instance). */
+int frost_prefetch_create_file(const char* path,
+                               uint64_t header_bytes,
+                               size_t block_rows,
+                               size_t row_bytes,
+                               int depth,
+                               int device,
+                               frost_prefetch** out);
+
+/* The same over `total_rows` packed rows in caller host memory (kept valid
+ * until destroy): the reader thread copies them into the pinned slots, as a
+ * socket or ring-buffer reader would. */
+int frost_prefetch_create_memory(const uint8_t* rows,
+                                 size_t total_rows,
+                                 size_t block_rows,
+                                 size_t row_bytes,
+                                 int depth,
+                                 int device,
+                                 frost_prefetch** out);
+
+/* GulpPrefetch::next (pipeline.cpp:131-152): the next gulp on the device
+ * (*block_device valid until the next call) and its row count (0 = end of
+ * source). With a `stream`, that stream waits for the gulp's copy and the
+ * slot is refilled only after the work the caller enqueues on it before its
+ * next call; with NULL the call waits for the copy on the host and the
+ * caller must have finished with the previous gulp (as a pipeline that reads
+ * its candidates back has). A source error is returned here
+ * (FROST_ERR_IO). */
+int frost_prefetch_next(frost_prefetch* p, void* stream, const uint8_t** block_device, size_t* nread);
+
+int frost_prefetch_get_stats(const frost_prefetch* p, frost_prefetch_stats* out);
+int frost_prefetch_destroy(frost_prefetch* p);
+
 /* ---- candidate post-processing (include/frost/search/postprocess.hpp) ---
  *
  * Friends-of-friends clustering within each FDMT plane, DM-wing seeding,

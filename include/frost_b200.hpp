@@ -10,6 +10,8 @@
 //   frost::b200::FDMTBoxcar   ~ the dmt::FDMTBoxcar call shape frost uses
 //                               (lib/pipeline/pipeline.cpp:316-367, 493-517, 598-608)
 //   frost::b200::BeamServer   ~ many beams on one GPU (no frost counterpart)
+//   frost::b200::GulpPrefetch ~ GulpPrefetch (lib/pipeline/pipeline.cpp:105-262),
+//                               delivering gulps on the device
 //   frost::b200::CandidatePostprocessPlan, ClusterLabelPlan,
 //   MergeCandidatesPlan, SubbandDedupPlan, are_coincident,
 //   subband_time_shift_samples, subband_dm_step
@@ -360,6 +362,46 @@ public:
 
 private:
     frost_server* m_h = nullptr;
+};
+
+/** frost's GulpPrefetch (lib/pipeline/pipeline.cpp:105-262) on the device:
+ * the next gulp is read and copied to the GPU while the current one is
+ * searched. */
+class GulpPrefetch {
+public:
+    /** A file of packed rows after `header_bytes`. */
+    GulpPrefetch(const std::string& path, uint64_t header_bytes, size_t block_rows, size_t row_bytes,
+                 int depth = 2, int device = 0) {
+        check(frost_prefetch_create_file(path.c_str(), header_bytes, block_rows, row_bytes, depth, device, &m_h));
+    }
+    /** A caller block source (runs on the prefetch thread). */
+    GulpPrefetch(frost_read_fn read, void* ctx, size_t block_rows, size_t row_bytes, int depth = 2,
+                 int device = 0) {
+        check(frost_prefetch_create(block_rows, row_bytes, depth, device, read, ctx, &m_h));
+    }
+    GulpPrefetch(const GulpPrefetch&)            = delete;
+    GulpPrefetch& operator=(const GulpPrefetch&) = delete;
+    ~GulpPrefetch() {
+        if (m_h != nullptr)
+            frost_prefetch_destroy(m_h);
+    }
+    struct Gulp {
+        const uint8_t* device = nullptr;
+        size_t nread          = 0; // 0 at the end of the source
+    };
+    Gulp next(void* stream = nullptr) {
+        Gulp g;
+        check(frost_prefetch_next(m_h, stream, &g.device, &g.nread));
+        return g;
+    }
+    frost_prefetch_stats stats() const {
+        frost_prefetch_stats s{};
+        check(frost_prefetch_get_stats(m_h, &s));
+        return s;
+    }
+
+private:
+    frost_prefetch* m_h = nullptr;
 };
 
 /** config::SearchConfig's post-processing defaults (config.hpp:57-97). */
