@@ -88,6 +88,10 @@ SIGNATURES = {
     "frost_server_set_postprocess": (C.c_int, [_vp, C.c_uint32, C.POINTER(_abi.PostprocessConfigC)]),
     "frost_server_wait_giants": (C.c_int, [_vp, _u64, _vp, _sz, C.POINTER(_sz), C.POINTER(C.c_double)]),
     "frost_server_drain_giants": (C.c_int, [_vp, C.c_uint32, _vp, _sz, C.POINTER(_sz)]),
+    "frost_cand_writer_open": (C.c_int, [C.c_char_p, C.c_double, C.c_int, C.POINTER(_vp)]),
+    "frost_cand_writer_write": (C.c_int, [_vp, _vp, _sz, _u64]),
+    "frost_cand_writer_close": (C.c_int, [_vp]),
+    "frost_cand_filename": (C.c_int, [C.c_int64, _u64, C.c_char_p, _sz]),
     "frost_prefetch_create": (C.c_int, [_sz, _sz, C.c_int, C.c_int, _abi.READ_FN, _vp, C.POINTER(_vp)]),
     "frost_prefetch_create_file": (C.c_int, [C.c_char_p, _u64, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]),
     "frost_prefetch_create_memory": (C.c_int, [_vp, _sz, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]),

@@ -13,6 +13,7 @@
 #include "common.hpp"
 #include "dedisp.hpp"
 #include "host_stats.hpp"
+#include "cand_writer.hpp"
 #include "postprocess.hpp"
 #include "prefetch.hpp"
 #include "pp_math.cuh"
@@ -74,6 +75,11 @@ struct frost_search {
 struct frost_server {
     fb::serve::Server impl;
     template <class... A> explicit frost_server(A&&... a) : impl(std::forward<A>(a)...) {}
+};
+
+struct frost_cand_writer {
+    fb::output::CandWriter impl;
+    template <class... A> explicit frost_cand_writer(A&&... a) : impl(std::forward<A>(a)...) {}
 };
 
 struct frost_prefetch {
@@ -920,6 +926,40 @@ int frost_prefetch_get_stats(const frost_prefetch* p, frost_prefetch_stats* out)
 
 int frost_prefetch_destroy(frost_prefetch* p) {
     return guarded([&] { delete p; });
+}
+
+// ---- candidate file -------------------------------------------------------------
+
+int frost_cand_writer_open(const char* path, double dt, int append, frost_cand_writer** out) {
+    return guarded([&] {
+        if (path == nullptr || out == nullptr)
+            invalid("frost_cand_writer_open: null argument");
+        *out = nullptr;
+        *out = new frost_cand_writer(std::string(path), dt, append != 0);
+    });
+}
+
+int frost_cand_writer_write(frost_cand_writer* w, const frost_giant* giants, size_t n, uint64_t first_samp_idx) {
+    return guarded([&] {
+        if (w == nullptr || (giants == nullptr && n > 0))
+            invalid("frost_cand_writer_write: null argument");
+        w->impl.write(giants, n, first_samp_idx);
+    });
+}
+
+int frost_cand_writer_close(frost_cand_writer* w) {
+    return guarded([&] { delete w; });
+}
+
+int frost_cand_filename(int64_t utc, uint64_t beam, char* out, size_t capacity) {
+    return guarded([&] {
+        if (out == nullptr)
+            invalid("frost_cand_filename: null argument");
+        const std::string s = fb::output::cand_filename(static_cast<std::time_t>(utc), beam);
+        if (s.size() + 1 > capacity)
+            invalid("frost_cand_filename: output holds too few characters");
+        std::memcpy(out, s.c_str(), s.size() + 1);
+    });
 }
 
 } // extern "C"

@@ -862,6 +862,33 @@ int frost_are_coincident(const frost_giant* a,
 double frost_subband_time_shift_samples(float dm, float f_wide, float f_narrow, float tsamp);
 double frost_subband_dm_step(float f_low, float f_high, float tsamp);
 
+/* ---- candidate file (include/frost/output/cand_writer.hpp) --------------
+ *
+ * frost's `.cand` layout: 23 tab-separated columns per giant (snr,
+ * samp_idx, time, filter_idx, dm_idx, dm, members, begin, end, f_low,
+ * f_high, chan_begin, chan_end, snr_best, chan_begin_best, chan_end_best,
+ * n_extents, samp_idx_best, time_best, dm_best, width_best, f_low_best,
+ * f_high_best), printed as frost prints them. Host code: the giants come
+ * from frost_postprocess_results or frost_server_wait_giants. */
+
+typedef struct frost_cand_writer frost_cand_writer;
+
+/* CandWriter(path, dt, mode) (cand_writer.hpp:38-45,
+ * lib/output/cand_writer.cpp:26-38): creates missing parent directories;
+ * `append` 0 truncates. FROST_ERR_IO if the file cannot be opened. */
+int frost_cand_writer_open(const char* path, double dt, int append, frost_cand_writer** out);
+
+/* CandWriter::write (cand_writer.cpp:40-71): one row per giant, sample
+ * columns offset by `first_samp_idx`; flushes; FROST_ERR_IO on a failed
+ * write. */
+int frost_cand_writer_write(frost_cand_writer* w, const frost_giant* giants, size_t n, uint64_t first_samp_idx);
+
+int frost_cand_writer_close(frost_cand_writer* w);
+
+/* cand_filename (cand_writer.cpp:73-87): "YYYY-MM-DD-HH:MM:SS_BB.cand" of
+ * `utc` (seconds since the epoch) and 1-based `beam`, into out[capacity]. */
+int frost_cand_filename(int64_t utc, uint64_t beam, char* out, size_t capacity);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

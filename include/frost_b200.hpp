@@ -10,6 +10,7 @@
 //   frost::b200::FDMTBoxcar   ~ the dmt::FDMTBoxcar call shape frost uses
 //                               (lib/pipeline/pipeline.cpp:316-367, 493-517, 598-608)
 //   frost::b200::BeamServer   ~ many beams on one GPU (no frost counterpart)
+//   frost::b200::CandWriter, cand_filename ~ frost::output (cand_writer.hpp)
 //   frost::b200::GulpPrefetch ~ GulpPrefetch (lib/pipeline/pipeline.cpp:105-262),
 //                               delivering gulps on the device
 //   frost::b200::CandidatePostprocessPlan, ClusterLabelPlan,
@@ -403,6 +404,32 @@ public:
 private:
     frost_prefetch* m_h = nullptr;
 };
+
+/** output::CandWriter (include/frost/output/cand_writer.hpp:38-55). */
+class CandWriter {
+public:
+    CandWriter(const std::string& path, double dt, bool append = false) {
+        check(frost_cand_writer_open(path.c_str(), dt, append ? 1 : 0, &m_h));
+    }
+    CandWriter(const CandWriter&)            = delete;
+    CandWriter& operator=(const CandWriter&) = delete;
+    ~CandWriter() {
+        if (m_h != nullptr)
+            frost_cand_writer_close(m_h);
+    }
+    void write(std::span<const frost_giant> giants, uint64_t first_samp_idx = 0) {
+        check(frost_cand_writer_write(m_h, giants.data(), giants.size(), first_samp_idx));
+    }
+
+private:
+    frost_cand_writer* m_h = nullptr;
+};
+
+inline std::string cand_filename(int64_t utc, uint64_t beam) {
+    char buf[64];
+    check(frost_cand_filename(utc, beam, buf, sizeof(buf)));
+    return buf;
+}
 
 /** config::SearchConfig's post-processing defaults (config.hpp:57-97). */
 inline frost_postprocess_config default_postprocess_config() {

@@ -97,6 +97,10 @@ class Backend:
             L.refs_pp_execute.argtypes = [_vp, _vp, _sz, _u64, _u64, C.c_int, _u64, C.POINTER(_u64)]
             L.refs_pp_results.restype = _sz
             L.refs_pp_results.argtypes = [_vp, _vp, _sz]
+            L.refs_cand_write.restype = C.c_int
+            L.refs_cand_write.argtypes = [C.c_char_p, C.c_double, C.c_int, _vp, _sz, _u64]
+            L.refs_cand_filename.restype = C.c_int
+            L.refs_cand_filename.argtypes = [C.c_int64, _u64, C.c_char_p, _sz]
             L.refs_pp_memory_usage.restype = _u64
             L.refs_pp_memory_usage.argtypes = [_vp]
             self._merge, self._dedup, self._labels = L.refs_merge, L.refs_subband_dedup, L.refs_cluster_labels
@@ -146,6 +150,20 @@ class Backend:
         if m < 0:
             raise PlanError("invalid_argument", self.error())
         return out[:m].copy()
+
+    def cand_write(self, path: str, dt: float, append: bool, giants, first_samp_idx: int = 0):
+        """The reference's own CandWriter (reference back end only)."""
+        g = np.ascontiguousarray(giants, GIANT_DTYPE).reshape(-1)
+        rc = self.L.refs_cand_write(path.encode(), dt, 1 if append else 0, g.ctypes.data if g.size else None,
+                                    g.size, int(first_samp_idx))
+        if rc != 0:
+            raise PlanError("runtime_error", self.error())
+
+    def cand_filename(self, utc: int, beam: int) -> str:
+        buf = C.create_string_buffer(64)
+        if self.L.refs_cand_filename(int(utc), int(beam), buf, len(buf)) != 0:
+            raise PlanError("invalid_argument", self.error())
+        return buf.value.decode()
 
     def plan(self, cfg: SearchConfig, layout: CandidatePostprocessLayout) -> "Plan":
         return Plan(self, cfg, layout)

@@ -5,6 +5,7 @@
 // plain C records of include/frost_b200.h and frost::search::Giant /
 // dmt::RawCandidate (the stand-in of oracle/stubs/dmt/common/candidate.hpp).
 
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <stdexcept>
@@ -12,6 +13,7 @@
 #include <vector>
 
 #include <frost/config/config.hpp>
+#include <frost/output/cand_writer.hpp>
 #include <frost/search/candidate.hpp>
 #include <frost/search/clustering.hpp>
 #include <frost/search/merge.hpp>
@@ -229,6 +231,32 @@ double refs_time_shift(float dm, float f_wide, float f_narrow, float tsamp) {
 
 double refs_dm_step(float f_low, float f_high, float tsamp) {
     return fs::subband_dm_step(f_low, f_high, tsamp);
+}
+
+// CandWriter (lib/output/cand_writer.cpp): 0 ok, -2 on an exception.
+int refs_cand_write(const char* path, double dt, int append, const frost_giant* g, size_t n,
+                    uint64_t first_samp_idx) {
+    try {
+        frost::output::CandWriter w(path, dt,
+                                    append != 0 ? frost::output::CandWriter::OpenMode::kAppend
+                                                : frost::output::CandWriter::OpenMode::kTruncate);
+        w.write(giants(g, n), first_samp_idx);
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -2;
+    }
+}
+
+int refs_cand_filename(int64_t utc, uint64_t beam, char* out, size_t cap) {
+    try {
+        const std::string s = frost::output::cand_filename(static_cast<std::time_t>(utc), beam);
+        std::snprintf(out, cap, "%s", s.c_str());
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
 }
 
 } // extern "C"
