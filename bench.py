@@ -256,7 +256,7 @@ def run_gpu(args):
         torch.cuda.empty_cache()
         return out
 
-    def measure_served(nbeams, on_device, sample_clocks=False):
+    def measure_served(nbeams, on_device, sample_clocks=False, postprocess=False):
         """Beams of the workload on one GPU through the server: each beam has
         one gulp in flight (the next is submitted when the previous one's
         candidates are ready), so every beam is busy and its latency is
@@ -275,13 +275,18 @@ def run_gpu(args):
                 if e.code != -2:  # ERR_OUT_OF_MEMORY: admission refused
                     raise
                 break
+        if postprocess:
+            # frost's per-gulp publish: clustering, DM wings, carry and
+            # sub-band dedup of every gulp's detections, on the device
+            for b in beams:
+                srv.set_postprocess(b, postprocess_config(int(bc.max_candidates)))
         src = raw_dev.data_ptr() if on_device else pinned.data_ptr()
-        counts = {b: [0, 0] for b in beams}  # candidates, bytes
+        counts = {b: [0, 0] for b in beams}  # candidates (or giants), bytes
 
         def run_beam(b, n, keep):
             for _ in range(n):
                 t = srv.submit_ptr(b, src, nbytes, GULP, on_device)
-                cands, _ = srv.wait(t)
+                cands, _ = srv.wait_giants(t) if postprocess else srv.wait(t)
                 if keep:
                     counts[b][0] += cands.size
                     counts[b][1] += cands.nbytes
@@ -359,6 +364,7 @@ def run_gpu(args):
     single32 = measure(Storage.FP32)
     served = measure_served(args.beams, on_device=True, sample_clocks=True)
     e2e = measure_served(args.beams, on_device=False)
+    served_pp = measure_served(args.beams, on_device=True, postprocess=True)
 
     gulp_s = GULP * TSAMP
     per_beam_steps = args.steps * world
@@ -425,6 +431,12 @@ def run_gpu(args):
             "caller_wait_ms_per_gulp": single16_pf["wait_ms_per_gulp"],
             "what": "plain FP16 fed by GulpPrefetch (reader thread: host memory -> pinned slots -> device, "
                     "depth 3), overlapping the next gulp's read and copy with the current search"},
+        "served_with_postprocess": {
+            "value": round(served_pp["beams"] * per_beam_steps * gulp_s / (served_pp["total_ms"] / 1e3), 3),
+            "p99_ms": round(served_pp["stats"].p99_latency_s * 1e3, 2),
+            "giants_per_beam_gulp": round(served_pp["ncands"] / max(served_pp["beams"] * args.steps, 1), 1),
+            "what": "the same served beams with frost's per-gulp post-processing (clustering, DM wings, carry, "
+                    "sub-band dedup) on the device after each search"},
         "served_vs_plain_fp32": round(value / plain32, 3),
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
                 "h2d_bytes_per_step": nbytes * e2e["beams"],
