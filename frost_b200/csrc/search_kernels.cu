@@ -1,25 +1,30 @@
 // Boxcar/trapezoid matched filter, exact noise and peak finding on sm_100a.
 //
 // One CTA per searched (plane, DM) row walks the tile in chunks of 2048 or
-// 4096 samples (a launch-shape choice).
-// The chunk plus a halo of the widest boxcar (rounded to 256 columns) is
-// bulk-copied into shared memory one chunk ahead, prefix-summed (warp
-// shuffles, then one offset per warp), and every width's window sum is a
+// 4096 samples (a launch-shape choice), the raw row segment bulk-copied into
+// shared memory one chunk ahead. Each thread owns P = chunk / 256
+// consecutive samples and keeps their prefix sums in registers (serial sum,
+// warp shuffles, one offset per warp); the prefix origin is the chunk's
+// first column, and the halo before it (the widest boxcar, rounded to 256
+// columns) is the previous chunk's last columns rebased to that origin, so
+// only a tile's first chunk scans its halo. Every width's window sum is a
 // difference of two (four for the trapezoid) prefix values. In the steady
 // state (no cold prefix, no mask change in the chunk) a sample is above
 // threshold when its window sum exceeds thresh * sigma, precomputed per
-// width. Each thread covers groups of 4 consecutive samples: the group's
-// largest prefix value minus the least prefix value the group's windows
-// start from bounds all 4 window sums, so almost every (group, width) is
-// cleared by one shared load, a subtract and a compare; the rest take the
-// exact test, which also writes the per-width bit masks of the samples that
-// fired. A chunk where nothing fires costs one block vote. The first
-// chunks of a stream or after a mask change (cold prefix, OR-mask
-// variance) build the bit masks from the general S/N. For every width that
-// fired, one lane (widths spread over the warps) walks its set bits in time
-// order, extending or closing the run carried from the previous chunk (and
-// tile, and gulp) and emitting each closed run's peak. The DM-time rows are never re-read and
-// the run state is the only thing carried between calls.
+// width, and nothing is written to shared memory but the least prefix value
+// of each 4-sample group and of each thread's samples: widths 1 and 2 take
+// the exact sums in registers, wider boxcars a bound (the greatest prefix
+// value of a set of samples minus the least one their windows start from),
+// per thread first for wide boxcars, then per group. A chunk where nothing
+// may fire costs one block vote. Only otherwise are the prefix sums stored
+// and the exact test run on the groups a bound did not clear, writing the
+// per-width bit masks of the samples that fired. The first chunks of a
+// stream or after a mask change (cold prefix, OR-mask variance) build the
+// bit masks from the general S/N. For every width that fired, one lane
+// (widths spread over the warps) walks its set bits in time order,
+// extending or closing the run carried from the previous chunk (and tile,
+// and gulp) and emitting each closed run's peak. The DM-time rows are never
+// re-read and the run state is the only thing carried between calls.
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -139,19 +144,6 @@ __device__ __forceinline__ float4 ld4(const float* Q, int idx) {
     return make_float4(a.w, b.x, b.y, b.z);
 }
 
-// Four consecutive staged level samples as float (8-byte fp16 / 16-byte
-// fp32 shared-memory load).
-template <class S> __device__ __forceinline__ float4 ld4s(const S* p);
-template <> __device__ __forceinline__ float4 ld4s<float>(const float* p) {
-    return *reinterpret_cast<const float4*>(p);
-}
-template <> __device__ __forceinline__ float4 ld4s<__half>(const __half* p) {
-    const uint2 u  = *reinterpret_cast<const uint2*>(p);
-    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
-    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
-    return make_float4(a.x, a.y, b.x, b.y);
-}
-
 // Eight consecutive staged samples (16-byte aligned) as float.
 template <class S> __device__ __forceinline__ void ld8s(const S* p, float (&x)[8]) {
     if constexpr (sizeof(S) == 4) {
@@ -264,24 +256,135 @@ __device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float
 // Words of the per-width bit masks [nw][chunk / 32].
 __host__ __device__ constexpr int search_bits_words(int nw, int chunk) { return nw * (chunk / 32); }
 
+// How the steady-state pass clears a width before any exact test.
+enum : int {
+    kTestExact = 0, // boxcar of 1 or 2 samples: the exact window sums, in registers
+    kTestGroup = 1, // per 4-sample group: group max minus the least prefix a window starts from
+    kTestBlock = 2, // per thread's columns first (wide boxcars), then per group
+    kTestAll   = 3, // trapezoid: the exact test on every group
+};
+
+/** Per-width constants of the steady-state pass, built once per CTA. For a
+ * thread t owning chunk columns [P t, P t + P): gmin index of its first
+ * group's first window start = NG t + gconst, tmin index of its first
+ * window start = t + bconst; `two` / `btwo`: the starts straddle two
+ * groups / blocks. */
+struct WidthTest {
+    int kind;
+    int W;
+    int gconst;
+    int two;
+    int bconst;
+    int btwo;
+    float T;
+    int pad;
+};
+
+// Loads P staged samples (16-byte aligned) as float.
+template <class S, int P> __device__ __forceinline__ void ld_cols(const S* p, float (&x)[P]) {
+#pragma unroll
+    for (int i = 0; i < P / 8; ++i) {
+        float y[8];
+        ld8s<S>(p + 8 * i, y);
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+            x[8 * i + e] = y[e];
+    }
+}
+
+template <int R, int NG, int N>
+__device__ __forceinline__ void pick_lows(const float (&e)[N], bool two, float (&lo)[NG]) {
+#pragma unroll
+    for (int g = 0; g < NG; ++g)
+        lo[g] = two ? fminf(e[R + g], e[R + g + 1]) : e[R + g];
+}
+
+// lo[g] = gmin[i0 + g], or the lesser of gmin[i0 + g] and gmin[i0 + g + 1]
+// when the window starts straddle two groups: the least prefix value a
+// window of the thread's group g starts from. i0 mod NG is the same for
+// every thread of the block, so the values come from aligned vector loads
+// (gmin is padded by 4 floats for the second one).
+template <int NG>
+__device__ __forceinline__ void group_lows(const float* gmin, int i0, bool two, float (&lo)[NG]) {
+    if constexpr (NG == 4) {
+        const int r     = i0 & 3;
+        const float4* v = reinterpret_cast<const float4*>(gmin + (i0 - r));
+        const float4 a  = v[0];
+        const float4 b  = (r != 0 || two) ? v[1] : a;
+        const float e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        switch (r) {
+        case 0: pick_lows<0, 4, 8>(e, two, lo); break;
+        case 1: pick_lows<1, 4, 8>(e, two, lo); break;
+        case 2: pick_lows<2, 4, 8>(e, two, lo); break;
+        default: pick_lows<3, 4, 8>(e, two, lo); break;
+        }
+    } else {
+        const int r     = i0 & 1;
+        const float2* v = reinterpret_cast<const float2*>(gmin + (i0 - r));
+        const float2 a  = v[0];
+        const float2 b  = (r != 0 || two) ? v[1] : a;
+        const float e[4] = {a.x, a.y, b.x, b.y};
+        if (r == 0)
+            pick_lows<0, 2, 4>(e, two, lo);
+        else
+            pick_lows<1, 2, 4>(e, two, lo);
+    }
+}
+
+// Q[-halo .. -1] straight from the staged halo columns: a prefix sum from
+// the first column a window can reach (earlier columns count 0), rebased so
+// that Q[-1] = 0, and the halo's entries of gmin (per 4 columns) and tmin
+// (per P columns). Rounding is monotonic, so the least rebased value of a
+// group is its least prefix value, rebased.
+template <class S, int P>
+__device__ void scan_halo(const S* seg, int halo, int jmin, float* Q, float* gmin, float* tmin) {
+    float* H = Q - halo;
+    for (int i = threadIdx.x; i < halo; i += kThreads)
+        H[i] = i < jmin ? 0.0F : ldf<S>(seg + i);
+    __syncthreads();
+    scan_inplace(H, halo);
+    const float last = H[halo - 1];
+    for (int j = threadIdx.x; j < halo / 4; j += kThreads)
+        gmin[j] = fminf(fminf(H[4 * j], H[4 * j + 1]), fminf(H[4 * j + 2], H[4 * j + 3])) - last;
+    for (int j = threadIdx.x; j < halo / P; j += kThreads) {
+        float m = H[P * j];
+        for (int e = 1; e < P; ++e)
+            m = fminf(m, H[P * j + e]);
+        tmin[j] = m - last;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < halo; i += kThreads)
+        H[i] -= last;
+}
+
 template <class S, int CH>
 __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0) {
-    // Dynamic shared memory: Ps, the chunk's prefix sums over columns
-    // [c0 - halo, c0 + CH) after 4 floats of padding (Q = Ps + 4 + halo
-    // puts sample k of the chunk at Q[k], 16-byte aligned); gmin / gmax, the
-    // least and greatest of each aligned group of 4 prefix values; the
-    // per-width bit masks [nw][(CH / 32)]; two staging buffers of the raw row
-    // segment, filled by bulk copies one chunk ahead.
+    constexpr int P  = CH / kThreads; // chunk columns per thread
+    constexpr int NG = P / 4;         // 4-column groups per thread
+    // Dynamic shared memory (floats unless noted):
+    //   Ps     4 pad + halo + CH + 4 pad: Q = Ps + 4 + halo holds the chunk's
+    //          prefix sums from its first column (Q[-1] = 0) and, before it,
+    //          the halo's, rebased to the same origin; Q is written only in
+    //          chunks where some test may fire
+    //   gmin   (halo + CH) / 4 + 4 pad: least Q of each aligned 4-column group
+    //   tmin   (halo + CH) / P: least Q of each thread's P columns
+    //   nh     2 x nh_len: the next chunk's halo (Q, gmin, tmin and this
+    //          chunk's last Q, not yet rebased), by chunk parity
+    //   bits   uint32 [nw][CH / 32]: per-width masks of the samples that fired
+    //   stage  S [2][halo + CH]: the raw row segment, bulk-copied one chunk
+    //          ahead (the halo columns only for the first chunk)
     extern __shared__ __align__(16) float Ps[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int abort_flag;
     __shared__ uint32_t any_bits[(CH / 32)];
     __shared__ RunState runs[kMaxWidths];
     __shared__ RowConst rc;
+    __shared__ WidthTest wt[kMaxWidths];
     __shared__ uint32_t local_count;
     __shared__ uint32_t fired_w; // widths with a set bit in this chunk
     __shared__ float warp_tot[kThreads / 32];
+    __shared__ float wtail[kThreads / 32][2]; // each warp's last two prefix values
 
     const int64_t g     = g0 + blockIdx.x;
     const SearchRow row = p.rows[g];
@@ -300,12 +403,24 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     if (threadIdx.x < nw) {
         const int w    = threadIdx.x;
         const int W    = p.widths[w];
+        const int E    = (p.trapezoid && W >= 3) ? (W + 1) / 4 : 0;
         rc.W[w]        = W;
-        rc.E[w]        = (p.trapezoid && W >= 3) ? (W + 1) / 4 : 0;
+        rc.E[w]        = E;
         const float iv = p.inv_sigma[g * nw + w];
         rc.inv[w]      = iv;
         rc.inv_or[w]   = p.inv_sigma_or[g * nw + w];
-        rc.thr[w]      = iv > 0.0F ? p.thresh / iv : FB_POS_INF;
+        const float T  = iv > 0.0F ? p.thresh / iv : FB_POS_INF;
+        rc.thr[w]      = T;
+        WidthTest t;
+        t.kind   = E > 0 ? kTestAll : W <= 2 ? kTestExact : W < 4 * P ? kTestGroup : kTestBlock;
+        t.W      = W;
+        t.gconst = (halo - W) >> 2;
+        t.two    = ((halo - W) & 3) != 0 ? 1 : 0;
+        t.bconst = (halo - W) / P;
+        t.btwo   = ((halo - W) % P) != 0 ? 1 : 0;
+        t.T      = T;
+        t.pad    = 0;
+        wt[w]    = t;
     }
     const int nruns = across ? 1 : nw;
     if (threadIdx.x < nruns && !all)
@@ -313,19 +428,25 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float* Q       = Ps + 4 + halo;
-    const S* src   = level + row.level_row * pitch + base;
-    const int seg_cols       = halo + CH;
-    const uint32_t seg_bytes = static_cast<uint32_t>(seg_cols * sizeof(S));
-    const int ngroups        = seg_cols / 4;
-    float* const gmin        = Ps + 4 + seg_cols + 4;
-    float* const gmax        = gmin + ngroups;
-    uint32_t* const bits     = reinterpret_cast<uint32_t*>(gmax + ngroups);
-    S* const stage0 = reinterpret_cast<S*>(bits + search_bits_words(nw, CH)); // buffer b at stage0 + b * seg_cols
-    const int nchunks = (p.n_valid + CH - 1) / CH;
+    const int seg_cols   = halo + CH;
+    float* const Q       = Ps + 4 + halo;
+    float* const gmin    = Ps + 4 + seg_cols + 4;
+    float* const tmin    = gmin + seg_cols / 4 + 4;
+    const int nh_len     = halo + halo / 4 + halo / P + 4;
+    float* const nh0     = tmin + seg_cols / P;
+    uint32_t* const bits = reinterpret_cast<uint32_t*>(nh0 + 2 * nh_len);
+    S* const stage0      = reinterpret_cast<S*>(bits + search_bits_words(nw, CH)); // buffer b at stage0 + b * seg_cols
+    const S* src         = level + row.level_row * pitch + base;
+    // A chunk's halo is the previous chunk's last `halo` columns, whose prefix
+    // sums that chunk has: only the first chunk (or every chunk, for a halo
+    // wider than a chunk) stages and scans its halo.
+    const bool carry_halo = halo <= CH;
+    const int nchunks     = (p.n_valid + CH - 1) / CH;
     auto issue = [&](int ci) {
-        bulk::mbar_expect(&bar[ci & 1], seg_bytes);
-        bulk::load(stage0 + (ci & 1) * seg_cols, src + static_cast<int64_t>(ci) * CH - halo, seg_bytes,
+        const int off        = (ci == 0 || !carry_halo) ? 0 : halo;
+        const uint32_t bytes = static_cast<uint32_t>((seg_cols - off) * sizeof(S));
+        bulk::mbar_expect(&bar[ci & 1], bytes);
+        bulk::load(stage0 + (ci & 1) * seg_cols + off, src + static_cast<int64_t>(ci) * CH - halo + off, bytes,
                    &bar[ci & 1]);
     };
     if (threadIdx.x == 0) {
@@ -337,12 +458,15 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     if (threadIdx.x == 0)
         for (int ci = 0; ci < min(2, nchunks); ++ci)
             issue(ci);
-    // 256-column segments (8 per lane): warp w scans a contiguous run of them
-    const int nseg  = seg_cols / 256;
-    const int spw   = (nseg + kThreads / 32 - 1) / (kThreads / 32);
-    const int s_beg = warp * spw, s_end = min(s_beg + spw, nseg);
-    const int jmin  = halo - wmax + 1; // earlier columns never enter a window
+    const int jmin     = halo - wmax + 1; // earlier columns never enter a window
     const int64_t warm = static_cast<int64_t>(row.delay) + wmax - 1;
+    auto close_runs = [&]() {
+        // nothing fired: runs open at the chunk start close here
+        if (!all && threadIdx.x < nruns && runs[threadIdx.x].open) {
+            emit(p, row, runs[threadIdx.x], &local_count);
+            runs[threadIdx.x].open = 0;
+        }
+    };
     int ci = 0;
     for (int64_t c0 = 0; c0 < p.n_valid; c0 += CH, ++ci) {
         // ---- wait for the chunk's segment (bounded; a timeout ends the row)
@@ -351,83 +475,167 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
         __syncthreads();
         if (abort_flag)
             break;
-        // ---- prefix sum: warp-local scans, then warp offsets
-        const S* seg = stage0 + (ci & 1) * seg_cols;
-        float carry  = 0.0F;
-        for (int sg = s_beg; sg < s_end; ++sg) {
-            const int j = sg * 256 + 8 * lane;
-            float x[8];
-            ld8s<S>(seg + j, x);
-            if (j < jmin) {
+        const S* seg           = stage0 + (ci & 1) * seg_cols;
+        const bool direct_halo = ci == 0 || !carry_halo;
+        if (direct_halo)
+            scan_halo<S, P>(seg, halo, jmin, Q, gmin, tmin);
+        // ---- prefix sums of the thread's P columns: serial, then across the
+        // warp (shuffles), then across warps (one offset per warp)
+        float q[P];
+        ld_cols<S, P>(seg + halo + P * threadIdx.x, q);
 #pragma unroll
-                for (int e = 0; e < 8; ++e)
-                    x[e] = j + e < jmin ? 0.0F : x[e];
-            }
+        for (int e = 1; e < P; ++e)
+            q[e] += q[e - 1];
+        float incl = q[P - 1];
 #pragma unroll
-            for (int e = 1; e < 8; ++e)
-                x[e] += x[e - 1];
-            float t = x[7];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const float u = __shfl_up_sync(0xFFFFFFFFU, t, o);
-                if (lane >= o)
-                    t += u;
-            }
-            const float before = __shfl_up_sync(0xFFFFFFFFU, t, 1);
-            const float off    = carry + (lane > 0 ? before : 0.0F);
-#pragma unroll
-            for (int e = 0; e < 8; ++e)
-                x[e] += off;
-            float4* dst = reinterpret_cast<float4*>(Ps + 4 + j);
-            dst[0]      = make_float4(x[0], x[1], x[2], x[3]);
-            dst[1]      = make_float4(x[4], x[5], x[6], x[7]);
-            carry += __shfl_sync(0xFFFFFFFFU, t, 31);
+        for (int o = 1; o < 32; o <<= 1) {
+            const float u = __shfl_up_sync(0xFFFFFFFFU, incl, o);
+            if (lane >= o)
+                incl += u;
         }
+        float excl = __shfl_up_sync(0xFFFFFFFFU, incl, 1);
         if (lane == 0)
-            warp_tot[warp] = carry;
+            excl = 0.0F;
+        if (lane == 31)
+            warp_tot[warp] = incl;
         __syncthreads();
         // every thread has read this chunk's staging buffer: refill it
         if (threadIdx.x == 0 && ci + 2 < nchunks)
             issue(ci + 2);
-        // clear the bit masks (a steady chunk sets only the words of
-        // samples that fired)
-        for (int i = threadIdx.x; i < nw * (CH / 32); i += kThreads)
-            bits[i] = 0U;
-        if (threadIdx.x == 0)
-            fired_w = 0U;
-        {
-            // add the preceding warps' totals; record each 4-group's range
-            float woff = 0.0F;
-            for (int w = 0; w < warp; ++w)
-                woff += warp_tot[w];
-            for (int sg = s_beg; sg < s_end; ++sg) {
-                const int j = sg * 256 + 8 * lane;
-                float4* v   = reinterpret_cast<float4*>(Ps + 4 + j);
-                float4 a = v[0], b = v[1];
-                if (warp > 0) {
-                    a.x += woff; a.y += woff; a.z += woff; a.w += woff;
-                    b.x += woff; b.y += woff; b.z += woff; b.w += woff;
-                    v[0] = a;
-                    v[1] = b;
+        float woff = 0.0F;
+        for (int w = 0; w < warp; ++w)
+            woff += warp_tot[w];
+        const float off = excl + woff;
+#pragma unroll
+        for (int e = 0; e < P; ++e)
+            q[e] += off;
+        // ---- group and block extremes (registers; the minima to shared memory)
+        float gmx[NG], gmn[NG];
+#pragma unroll
+        for (int gq = 0; gq < NG; ++gq) {
+            gmx[gq] = fmaxf(fmaxf(q[4 * gq], q[4 * gq + 1]), fmaxf(q[4 * gq + 2], q[4 * gq + 3]));
+            gmn[gq] = fminf(fminf(q[4 * gq], q[4 * gq + 1]), fminf(q[4 * gq + 2], q[4 * gq + 3]));
+        }
+        float bmax = gmx[0], bmin = gmn[0];
+#pragma unroll
+        for (int gq = 1; gq < NG; ++gq) {
+            bmax = fmaxf(bmax, gmx[gq]);
+            bmin = fminf(bmin, gmn[gq]);
+        }
+        if constexpr (NG == 4)
+            reinterpret_cast<float4*>(gmin + halo / 4)[threadIdx.x] = make_float4(gmn[0], gmn[1], gmn[2], gmn[3]);
+        else
+            reinterpret_cast<float2*>(gmin + halo / 4)[threadIdx.x] = make_float2(gmn[0], gmn[1]);
+        tmin[halo / P + threadIdx.x] = bmin;
+        if (lane == 31) {
+            wtail[warp][0] = q[P - 2];
+            wtail[warp][1] = q[P - 1];
+        }
+        if (carry_halo) {
+            // the next chunk's halo: this chunk's last `halo` columns
+            float* nh    = nh0 + (ci & 1) * nh_len;
+            const int tt = static_cast<int>(threadIdx.x) - (kThreads - halo / P);
+            if (tt >= 0) {
+                float4* d = reinterpret_cast<float4*>(nh + P * tt);
+#pragma unroll
+                for (int i = 0; i < P / 4; ++i)
+                    d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+#pragma unroll
+                for (int gq = 0; gq < NG; ++gq)
+                    nh[halo + NG * tt + gq] = gmn[gq];
+                nh[halo + halo / 4 + tt] = bmin;
+                if (threadIdx.x == kThreads - 1)
+                    nh[halo + halo / 4 + halo / P] = q[P - 1];
+            }
+            if (!direct_halo) {
+                // this chunk's halo from the previous chunk's, rebased so that Q[-1] = 0
+                const float* ph  = nh0 + ((ci - 1) & 1) * nh_len;
+                const int n      = halo + halo / 4 + halo / P;
+                const float last = ph[n];
+                for (int i = threadIdx.x; i < n; i += kThreads) {
+                    const float v = ph[i] - last;
+                    if (i < halo)
+                        Q[i - halo] = v;
+                    else if (i < halo + halo / 4)
+                        gmin[i - halo] = v;
+                    else
+                        tmin[i - halo - halo / 4] = v;
                 }
-                reinterpret_cast<float2*>(gmin)[j / 8] = make_float2(
-                    fminf(fminf(a.x, a.y), fminf(a.z, a.w)), fminf(fminf(b.x, b.y), fminf(b.z, b.w)));
-                reinterpret_cast<float2*>(gmax)[j / 8] = make_float2(
-                    fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)), fmaxf(fmaxf(b.x, b.y), fmaxf(b.z, b.w)));
             }
         }
         __syncthreads();
 
+        auto store_q = [&]() {
+            float4* d = reinterpret_cast<float4*>(Q + P * threadIdx.x);
+#pragma unroll
+            for (int i = 0; i < P / 4; ++i)
+                d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+            for (int i = threadIdx.x; i < nw * (CH / 32); i += kThreads)
+                bits[i] = 0U;
+            if (threadIdx.x == 0)
+                fired_w = 0U;
+        };
         const bool fast = c0 + CH <= p.n_valid && (!p.skip_cold || rc.tile_t0 + c0 >= warm) &&
                           (!rc.or_active || rc.tile_t0 + c0 - rc.gulp_t0 >= warm);
         if (fast) {
-            // ---- steady state. Group gi = samples 4 gi .. 4 gi + 3. A window
-            // sum Q[k] - Q[k - W] of the group is at most gmax(group) minus
-            // gmin over the groups holding Q[4 gi - W .. 4 gi + 3 - W]
-            // (rounding is monotonic), so a (group, width) the bound clears
-            // cannot fire. The others take the exact test (the same float
-            // expression as wsum) and set the bits of the samples that fire.
-            // Trapezoids take the exact test throughout.
+            // ---- steady state. A window sum Q[k] - Q[k - W] of a set of
+            // samples is at most their greatest Q minus the least Q their
+            // windows start from (rounding is monotonic), so a set the bound
+            // clears cannot fire. Widths 1 and 2 take the exact sums in
+            // registers, the others a bound per 4-sample group (wide boxcars
+            // first one per thread); only a chunk where some test may fire
+            // stores Q and runs the exact tests.
+            float pm1 = __shfl_up_sync(0xFFFFFFFFU, q[P - 1], 1); // Q[P t - 1]
+            float pm2 = __shfl_up_sync(0xFFFFFFFFU, q[P - 2], 1); // Q[P t - 2]
+            if (lane == 0) {
+                pm1 = warp == 0 ? Q[-1] : wtail[warp - 1][1];
+                pm2 = warp == 0 ? Q[-2] : wtail[warp - 1][0];
+            }
+            uint32_t cand = 0U;
+            for (int wi = 0; wi < nw; ++wi) {
+                const WidthTest t = wt[wi];
+                bool maybe        = true;
+                if (t.kind == kTestExact) {
+                    float m;
+                    if (t.W == 1) {
+                        m = q[0] - pm1;
+#pragma unroll
+                        for (int e = 1; e < P; ++e)
+                            m = fmaxf(m, q[e] - q[e - 1]);
+                    } else {
+                        m = fmaxf(q[0] - pm2, q[1] - pm1);
+#pragma unroll
+                        for (int e = 2; e < P; ++e)
+                            m = fmaxf(m, q[e] - q[e - 2]);
+                    }
+                    maybe = m > t.T;
+                } else if (t.kind != kTestAll) {
+                    if (t.kind == kTestBlock) {
+                        const int b = static_cast<int>(threadIdx.x) + t.bconst;
+                        float lo    = tmin[b];
+                        if (t.btwo)
+                            lo = fminf(lo, tmin[b + 1]);
+                        maybe = bmax - lo > t.T;
+                    }
+                    if (maybe) {
+                        float lo[NG];
+                        group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
+                        float m = gmx[0] - lo[0];
+#pragma unroll
+                        for (int gq = 1; gq < NG; ++gq)
+                            m = fmaxf(m, gmx[gq] - lo[gq]);
+                        maybe = m > t.T;
+                    }
+                }
+                if (maybe)
+                    cand |= 1U << wi;
+            }
+            if (!__syncthreads_or(cand != 0U)) {
+                close_runs();
+                continue; // shared memory is rewritten only after every thread passed the barrier
+            }
+            store_q();
+            __syncthreads();
             bool up = false;
             // the exact test of group gi at width wi (sets the fired bits)
             auto exact = [&](int gi, int wi, int W, int E, float T) {
@@ -457,46 +665,32 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                     up = true;
                 }
             };
-            constexpr int NG = (CH / kThreads) / 4; // groups per thread
-            float hi[NG];
+            for (uint32_t c = cand; c != 0U; c &= c - 1U) {
+                const int wi      = __ffs(static_cast<int>(c)) - 1;
+                const WidthTest t = wt[wi];
+                const int E       = rc.E[wi];
+                if (t.kind == kTestGroup || t.kind == kTestBlock) {
+                    float lo[NG];
+                    group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
 #pragma unroll
-            for (int q = 0; q < NG; ++q)
-                hi[q] = gmax[threadIdx.x + q * kThreads + halo / 4];
-            for (int wi = 0; wi < nw; ++wi) {
-                const int W   = rc.W[wi];
-                const int E   = rc.E[wi];
-                const float T = rc.thr[wi];
-                const int sh  = (halo - W) >> 2; // group of Q[4 gi - W] is gi + sh
-                if (E == 0 && (W & 3) == 0) {
-#pragma unroll
-                    for (int q = 0; q < NG; ++q) {
-                        const int gi = threadIdx.x + q * kThreads;
-                        if (hi[q] - gmin[gi + sh] > T)
-                            exact(gi, wi, W, E, T);
-                    }
-                } else if (E == 0) {
-#pragma unroll
-                    for (int q = 0; q < NG; ++q) {
-                        const int gi = threadIdx.x + q * kThreads;
-                        if (hi[q] - fminf(gmin[gi + sh], gmin[gi + sh + 1]) > T)
-                            exact(gi, wi, W, E, T);
-                    }
+                    for (int gq = 0; gq < NG; ++gq)
+                        if (gmx[gq] - lo[gq] > t.T)
+                            exact(NG * static_cast<int>(threadIdx.x) + gq, wi, t.W, E, t.T);
                 } else {
-                    for (int q = 0; q < NG; ++q)
-                        exact(threadIdx.x + q * kThreads, wi, W, E, T);
+#pragma unroll
+                    for (int gq = 0; gq < NG; ++gq)
+                        exact(NG * static_cast<int>(threadIdx.x) + gq, wi, t.W, E, t.T);
                 }
             }
             if (!__syncthreads_or(up)) {
-                // nothing fired: runs open at the chunk start close here
-                if (!all && threadIdx.x < nruns && runs[threadIdx.x].open) {
-                    emit(p, row, runs[threadIdx.x], &local_count);
-                    runs[threadIdx.x].open = 0;
-                }
-                continue; // Ps is rewritten only after every thread passed the barrier
+                close_runs();
+                continue;
             }
         } else {
             // ---- not steady (cold prefix, mask change, partial chunk): the
             // bit masks from the general S/N
+            store_q();
+            __syncthreads();
             for (int j = 0; j < (CH / kThreads); ++j) {
                 const int k = threadIdx.x + j * kThreads;
                 for (int wi = 0; wi < nw; ++wi) {
@@ -642,7 +836,11 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
         throw Error(FROST_ERR_INTERNAL, "search: no error flag");
     const size_t es   = level.fp16 ? 2 : 4;
     const size_t seg  = static_cast<size_t>(p.halo) + chunk;
-    const size_t smem = sizeof(float) * (4 + seg + 4 + 2 * (seg / 4)) +
+    // Ps, gmin (+4 padding), tmin, the next chunk's halo by parity, the bit
+    // masks and the staging buffers (the kernel's layout)
+    const size_t per  = static_cast<size_t>(chunk) / kThreads; // columns per thread
+    const size_t nh   = static_cast<size_t>(p.halo) + p.halo / 4 + p.halo / per + 4;
+    const size_t smem = sizeof(float) * ((4 + seg + 4) + (seg / 4 + 4) + seg / per + 2 * nh) +
                         sizeof(uint32_t) * search_bits_words(p.nwidths, chunk) + 2 * es * seg;
     const dim3 grid(static_cast<unsigned>(g1 - g0));
     auto go = [&](auto kernel, auto data) {
