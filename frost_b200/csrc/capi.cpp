@@ -545,6 +545,14 @@ int frost_server_drain(frost_server* s, uint32_t beam, frost_candidate* out, siz
     return g != FROST_OK ? g : rc;
 }
 
+int frost_server_set_residency(frost_server* s, uint32_t beam, int ctas_per_sm) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_set_residency: null handle");
+        s->impl.set_residency(beam, ctas_per_sm);
+    });
+}
+
 int frost_server_set_postprocess(frost_server* s, uint32_t beam, const frost_postprocess_config* cfg) {
     return guarded([&] {
         if (s == nullptr || cfg == nullptr)
@@ -643,6 +651,22 @@ int frost_search_get_launch_shape(const frost_search* s, int* fused, int* tiles_
             *stages = t.stages;
         if (search_chunk != nullptr)
             *search_chunk = t.search_chunk;
+    });
+}
+
+int frost_search_set_residency(frost_search* s, int ctas_per_sm) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_set_residency: null handle");
+        s->impl.set_residency(ctas_per_sm);
+    });
+}
+
+int frost_search_get_residency(const frost_search* s, int* ctas_per_sm) {
+    return guarded([&] {
+        if (s == nullptr || ctas_per_sm == nullptr)
+            invalid("frost_search_get_residency: null argument");
+        *ctas_per_sm = s->impl.residency();
     });
 }
 

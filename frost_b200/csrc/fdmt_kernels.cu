@@ -79,52 +79,58 @@ __device__ void block_scan(float* a, int n) {
 
 template <class S>
 __global__ void __launch_bounds__(kThreads)
-    k_level1(const LeafOp* __restrict__ ops, const int32_t* __restrict__ node_first_op,
-             int32_t H, const float* __restrict__ wf, int64_t wpitch, int64_t t0, int32_t n_valid,
-             const float* __restrict__ hist, int32_t hist_len, S* __restrict__ out,
+    k_level1(const LeafOp* __restrict__ ops, const int32_t* __restrict__ node_first_op, int32_t nnodes,
+             int32_t ntiles, int32_t H, const float* __restrict__ wf, int64_t wpitch, int64_t t0,
+             int32_t n_valid, const float* __restrict__ hist, int32_t hist_len, S* __restrict__ out,
              int64_t pitch, int32_t base) {
     extern __shared__ float smem[];
-    const int32_t node = blockIdx.x;
-    const int32_t op0 = node_first_op[node], op1 = node_first_op[node + 1];
-    const int32_t ca  = ops[op0].chan_lo;
-    const int32_t cb  = ops[op0].chan_hi;
-    const int32_t k0  = blockIdx.y * kTimePerCta;
-    const int32_t N   = kTimePerCta + H + 1;
-    float* Pa         = smem;
-    float* Pb         = smem + N;
-    // x(i) for tile-relative time t = k0 + i - H - 1; x(0) is the scan base.
-    for (int i = threadIdx.x; i < N; i += kThreads) {
-        const int64_t t = static_cast<int64_t>(k0) + i - H - 1;
-        float a = 0.0F, b = 0.0F;
-        if (i > 0) {
-            if (t < 0) {
-                a = hist[static_cast<int64_t>(ca) * hist_len + hist_len + t];
+    const int32_t N = kTimePerCta + H + 1;
+    float* Pa       = smem;
+    float* Pb       = smem + N;
+    // Work items (node, tile), nodes fastest; a CTA takes items blockIdx.x,
+    // blockIdx.x + gridDim.x, ...
+    const int64_t nitems = static_cast<int64_t>(nnodes) * ntiles;
+    for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int32_t node = static_cast<int32_t>(item % nnodes);
+        const int32_t op0 = node_first_op[node], op1 = node_first_op[node + 1];
+        const int32_t ca  = ops[op0].chan_lo;
+        const int32_t cb  = ops[op0].chan_hi;
+        const int32_t k0  = static_cast<int32_t>(item / nnodes) * kTimePerCta;
+        // x(i) for tile-relative time t = k0 + i - H - 1; x(0) is the scan base.
+        for (int i = threadIdx.x; i < N; i += kThreads) {
+            const int64_t t = static_cast<int64_t>(k0) + i - H - 1;
+            float a = 0.0F, b = 0.0F;
+            if (i > 0) {
+                if (t < 0) {
+                    a = hist[static_cast<int64_t>(ca) * hist_len + hist_len + t];
+                    if (cb >= 0)
+                        b = hist[static_cast<int64_t>(cb) * hist_len + hist_len + t];
+                } else if (t < n_valid) {
+                    a = wf[static_cast<int64_t>(ca) * wpitch + t0 + t];
+                    if (cb >= 0)
+                        b = wf[static_cast<int64_t>(cb) * wpitch + t0 + t];
+                }
+            }
+            Pa[i] = a;
+            Pb[i] = b;
+        }
+        __syncthreads();
+        block_scan(Pa, N);
+        if (cb >= 0)
+            block_scan(Pb, N);
+        for (int32_t r = op0; r < op1; ++r) {
+            const LeafOp op = ops[r];
+            S* row          = out + static_cast<int64_t>(r) * pitch + base + k0;
+            for (int j = 0; j < kPer; ++j) {
+                const int k = threadIdx.x + j * kThreads;
+                const int i = k + H + 1;
+                float v     = Pa[i] - Pa[i - op.d_lo - 1];
                 if (cb >= 0)
-                    b = hist[static_cast<int64_t>(cb) * hist_len + hist_len + t];
-            } else if (t < n_valid) {
-                a = wf[static_cast<int64_t>(ca) * wpitch + t0 + t];
-                if (cb >= 0)
-                    b = wf[static_cast<int64_t>(cb) * wpitch + t0 + t];
+                    v += Pb[i - op.d_lo] - Pb[i - op.d_lo - op.d_hi - 1];
+                st<S>(row + k, v);
             }
         }
-        Pa[i] = a;
-        Pb[i] = b;
-    }
-    __syncthreads();
-    block_scan(Pa, N);
-    if (cb >= 0)
-        block_scan(Pb, N);
-    for (int32_t r = op0; r < op1; ++r) {
-        const LeafOp op = ops[r];
-        S* row          = out + static_cast<int64_t>(r) * pitch + base + k0;
-        for (int j = 0; j < kPer; ++j) {
-            const int k = threadIdx.x + j * kThreads;
-            const int i = k + H + 1;
-            float v     = Pa[i] - Pa[i - op.d_lo - 1];
-            if (cb >= 0)
-                v += Pb[i - op.d_lo] - Pb[i - op.d_lo - op.d_hi - 1];
-            st<S>(row + k, v);
-        }
+        __syncthreads(); // every thread is done with Pa / Pb
     }
 }
 
@@ -205,7 +211,7 @@ template <class S>
 __global__ void __launch_bounds__(kThreads)
     k_level_pipe(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
                  int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                 int32_t ntiles, int32_t tpc, unsigned* __restrict__ err) {
+                 int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err) {
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -214,73 +220,83 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ __align__(8) uint64_t bar[kStages];
     __shared__ int abort_flag;
 
-    const RowOp op  = ops[blockIdx.x];
-    const int tile0 = blockIdx.y * tpc;
-    const int nt    = min(tpc, ntiles - tile0);
-    if (nt <= 0)
-        return;
-    const bool has_hi = op.hi_row >= 0;
-    const S* lo_row   = in + static_cast<int64_t>(op.lo_row) * in_pitch + in_base;
-    const S* hi_base  = in + static_cast<int64_t>(has_hi ? op.hi_row : op.lo_row) * in_pitch;
-    S* dst_row        = out + static_cast<int64_t>(blockIdx.x) * out_pitch + out_base;
-    // the shifted segment's offset inside its aligned superset is the same
-    // for every tile (tiles start at multiples of kTimePerCta)
-    const int64_t e_first = static_cast<int64_t>(in_base) - op.shift;
-    const int off         = static_cast<int>(((e_first % VEC) + VEC) % VEC);
-    const uint32_t hi_bytes = has_hi ? static_cast<uint32_t>((kTimePerCta / VEC + (off > 0 ? 1 : 0)) * 16) : 0U;
-
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < kStages; ++s)
             bulk::mbar_init(&bar[s]);
     }
     __syncthreads();
+    // Work items (row, run of tpc tiles), rows fastest; a CTA takes items
+    // blockIdx.x, blockIdx.x + gridDim.x, ... and its tiles use the stages
+    // in turn across items (tile n of the CTA: stage n % kStages).
+    const int nruns      = (ntiles + tpc - 1) / tpc;
+    const int64_t nitems = nrows * nruns;
+    const int e          = 8 * threadIdx.x;
+    int64_t done         = 0; // tiles this CTA has consumed
+    for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int64_t r = item % nrows;
+        const RowOp op  = ops[r];
+        const int tile0 = static_cast<int>(item / nrows) * tpc;
+        const int nt    = min(tpc, ntiles - tile0);
+        const bool has_hi = op.hi_row >= 0;
+        const S* lo_row   = in + static_cast<int64_t>(op.lo_row) * in_pitch + in_base;
+        const S* hi_base  = in + static_cast<int64_t>(has_hi ? op.hi_row : op.lo_row) * in_pitch;
+        S* dst_row        = out + r * out_pitch + out_base;
+        // the shifted segment's offset inside its aligned superset is the same
+        // for every tile (tiles start at multiples of kTimePerCta)
+        const int64_t e_first = static_cast<int64_t>(in_base) - op.shift;
+        const int off         = static_cast<int>(((e_first % VEC) + VEC) % VEC);
+        const uint32_t hi_bytes = has_hi ? static_cast<uint32_t>((kTimePerCta / VEC + (off > 0 ? 1 : 0)) * 16) : 0U;
 
-    auto issue = [&](int i) {
-        const int s       = i % kStages;
-        const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
-        unsigned char* st = pipe_smem + s * kStageBytes;
-        bulk::mbar_expect(&bar[s], static_cast<uint32_t>(kLoBytes) + hi_bytes);
-        bulk::load(st, lo_row + k0, static_cast<uint32_t>(kLoBytes), &bar[s]);
-        if (has_hi) {
-            const int64_t v0 = (e_first + k0 - off) / VEC; // aligned start, in vectors
-            bulk::load(st + kLoBytes, hi_base + v0 * VEC, hi_bytes, &bar[s]);
-        }
-    };
+        auto issue = [&](int i) {
+            const int s       = static_cast<int>((done + i) % kStages);
+            const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
+            unsigned char* st = pipe_smem + s * kStageBytes;
+            bulk::mbar_expect(&bar[s], static_cast<uint32_t>(kLoBytes) + hi_bytes);
+            bulk::load(st, lo_row + k0, static_cast<uint32_t>(kLoBytes), &bar[s]);
+            if (has_hi) {
+                const int64_t v0 = (e_first + k0 - off) / VEC; // aligned start, in vectors
+                bulk::load(st + kLoBytes, hi_base + v0 * VEC, hi_bytes, &bar[s]);
+            }
+        };
 
-    if (threadIdx.x == 0)
-        for (int i = 0; i < min(kStages, nt); ++i)
-            issue(i);
-    const int e = 8 * threadIdx.x;
-    int i       = 0;
-    for (; i < nt; ++i) {
-        const int s           = i % kStages;
-        const uint32_t phase  = static_cast<uint32_t>((i / kStages) & 1);
-        if (!mbar_wait(&bar[s], phase))
-            atomicExch(&abort_flag, 1);
-        __syncthreads();
-        if (abort_flag)
-            break;
-        const S* lo_s = reinterpret_cast<const S*>(pipe_smem + s * kStageBytes);
-        const S* hi_s = reinterpret_cast<const S*>(pipe_smem + s * kStageBytes + kLoBytes);
-        S* dst        = dst_row + static_cast<int64_t>(tile0 + i) * kTimePerCta + e;
-        if (has_hi) {
-            merge8<S>(lo_s + e, hi_s, e, off, dst);
-        } else {
-            const uint4* s4 = reinterpret_cast<const uint4*>(lo_s + e);
-            uint4* d4       = reinterpret_cast<uint4*>(dst);
-            for (int v = 0; v < 8 / VEC; ++v)
-                d4[v] = s4[v];
+        if (threadIdx.x == 0)
+            for (int i = 0; i < min(kStages, nt); ++i)
+                issue(i);
+        int i = 0;
+        for (; i < nt; ++i) {
+            const int s           = static_cast<int>((done + i) % kStages);
+            const uint32_t phase  = static_cast<uint32_t>(((done + i) / kStages) & 1);
+            if (!mbar_wait(&bar[s], phase))
+                atomicExch(&abort_flag, 1);
+            __syncthreads();
+            if (abort_flag)
+                break;
+            const S* lo_s = reinterpret_cast<const S*>(pipe_smem + s * kStageBytes);
+            const S* hi_s = reinterpret_cast<const S*>(pipe_smem + s * kStageBytes + kLoBytes);
+            S* dst        = dst_row + static_cast<int64_t>(tile0 + i) * kTimePerCta + e;
+            if (has_hi) {
+                merge8<S>(lo_s + e, hi_s, e, off, dst);
+            } else {
+                const uint4* s4 = reinterpret_cast<const uint4*>(lo_s + e);
+                uint4* d4       = reinterpret_cast<uint4*>(dst);
+                for (int v = 0; v < 8 / VEC; ++v)
+                    d4[v] = s4[v];
+            }
+            __syncthreads(); // every thread is done with stage s
+            if (threadIdx.x == 0 && i + kStages < nt)
+                issue(i + kStages);
         }
-        __syncthreads(); // every thread is done with stage s
-        if (threadIdx.x == 0 && i + kStages < nt)
-            issue(i + kStages);
-    }
-    if (i < nt && threadIdx.x == 0) {
-        // a wait ran out: report it, then let the copies still in flight land
-        atomicOr(err, 1U);
-        for (int j = i; j < min(nt, i + kStages); ++j)
-            (void)mbar_wait(&bar[j % kStages], static_cast<uint32_t>((j / kStages) & 1));
+        if (i < nt) {
+            if (threadIdx.x == 0) {
+                // a wait ran out: report it, then let the copies still in flight land
+                atomicOr(err, 1U);
+                for (int j = i; j < min(nt, i + kStages); ++j)
+                    (void)mbar_wait(&bar[(done + j) % kStages], static_cast<uint32_t>(((done + j) / kStages) & 1));
+            }
+            return;
+        }
+        done += nt;
     }
 }
 
@@ -346,7 +362,7 @@ template <class S, int NS>
 __global__ void __launch_bounds__(kThreads)
     k_level2_pipe(const FusedOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
                   int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                  int32_t ntiles, int32_t tpc, unsigned* __restrict__ err) {
+                  int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err) {
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -355,110 +371,118 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ __align__(8) uint64_t bar[NS];
     __shared__ int abort_flag;
 
-    const FusedOp op = ops[blockIdx.x];
-    const int tile0  = blockIdx.y * tpc;
-    const int nt     = min(tpc, ntiles - tile0);
-    if (nt <= 0)
-        return;
-    const S* rows[4];
-    int off[4];
-    uint32_t bytes[4];
-    int64_t first[4];
-    uint32_t total = 0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const bool has = op.row[j] >= 0;
-        rows[j]        = in + static_cast<int64_t>(has ? op.row[j] : op.row[0]) * in_pitch;
-        first[j]       = static_cast<int64_t>(in_base) - op.shift[j];
-        off[j]         = static_cast<int>(((first[j] % VEC) + VEC) % VEC);
-        bytes[j]       = !has ? 0U
-                         : j == 0 ? static_cast<uint32_t>(kLoBytes)
-                                  : static_cast<uint32_t>((kTimePerCta / VEC + (off[j] > 0 ? 1 : 0)) * 16);
-        total += bytes[j];
-    }
-    S* dst_row = out + static_cast<int64_t>(blockIdx.x) * out_pitch + out_base;
-
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int st = 0; st < NS; ++st)
             bulk::mbar_init(&bar[st]);
     }
     __syncthreads();
-
-    auto issue = [&](int i) {
-        const int st      = i % NS;
-        const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
-        unsigned char* sb = pipe2_smem + st * kStageBytes;
-        bulk::mbar_expect(&bar[st], total);
+    // Work items (row, run of tpc tiles) as in k_level_pipe.
+    const int nruns      = (ntiles + tpc - 1) / tpc;
+    const int64_t nitems = nrows * nruns;
+    const int e          = 8 * threadIdx.x;
+    int64_t done         = 0; // tiles this CTA has consumed
+    for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int64_t r  = item % nrows;
+        const FusedOp op = ops[r];
+        const int tile0  = static_cast<int>(item / nrows) * tpc;
+        const int nt     = min(tpc, ntiles - tile0);
+        const S* rows[4];
+        int off[4];
+        uint32_t bytes[4];
+        int64_t first[4];
+        uint32_t total = 0;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            if (bytes[j] == 0U)
-                continue;
-            const int64_t v0 = (first[j] + k0 - off[j]) / VEC; // aligned start, in vectors
-            bulk::load(sb + (j == 0 ? 0 : kLoBytes + (j - 1) * kHiBytes), rows[j] + v0 * VEC, bytes[j],
-                       &bar[st]);
+            const bool has = op.row[j] >= 0;
+            rows[j]        = in + static_cast<int64_t>(has ? op.row[j] : op.row[0]) * in_pitch;
+            first[j]       = static_cast<int64_t>(in_base) - op.shift[j];
+            off[j]         = static_cast<int>(((first[j] % VEC) + VEC) % VEC);
+            bytes[j]       = !has ? 0U
+                             : j == 0 ? static_cast<uint32_t>(kLoBytes)
+                                      : static_cast<uint32_t>((kTimePerCta / VEC + (off[j] > 0 ? 1 : 0)) * 16);
+            total += bytes[j];
         }
-    };
+        S* dst_row = out + r * out_pitch + out_base;
 
-    if (threadIdx.x == 0)
-        for (int i = 0; i < min(NS, nt); ++i)
-            issue(i);
-    const int e = 8 * threadIdx.x;
-    int i       = 0;
-    for (; i < nt; ++i) {
-        const int st         = i % NS;
-        const uint32_t phase = static_cast<uint32_t>((i / NS) & 1);
-        if (!mbar_wait(&bar[st], phase))
-            atomicExch(&abort_flag, 1);
-        __syncthreads();
-        if (abort_flag)
-            break;
-        const unsigned char* sb = pipe2_smem + st * kStageBytes;
-        float a[8], x[8];
-        load8<S>(reinterpret_cast<const S*>(sb), e, 0, a);
-        if (bytes[1] != 0U) {
-            load8<S>(reinterpret_cast<const S*>(sb + kLoBytes), e, off[1], x);
+        auto issue = [&](int i) {
+            const int st      = static_cast<int>((done + i) % NS);
+            const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
+            unsigned char* sb = pipe2_smem + st * kStageBytes;
+            bulk::mbar_expect(&bar[st], total);
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                a[q] = a[q] + x[q];
-        }
-        if (bytes[2] != 0U) {
-            float b[8];
-            load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + kHiBytes), e, off[2], b);
-            if (bytes[3] != 0U) {
-                load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], x);
+            for (int j = 0; j < 4; ++j) {
+                if (bytes[j] == 0U)
+                    continue;
+                const int64_t v0 = (first[j] + k0 - off[j]) / VEC; // aligned start, in vectors
+                bulk::load(sb + (j == 0 ? 0 : kLoBytes + (j - 1) * kHiBytes), rows[j] + v0 * VEC, bytes[j],
+                           &bar[st]);
+            }
+        };
+
+        if (threadIdx.x == 0)
+            for (int i = 0; i < min(NS, nt); ++i)
+                issue(i);
+        int i = 0;
+        for (; i < nt; ++i) {
+            const int st         = static_cast<int>((done + i) % NS);
+            const uint32_t phase = static_cast<uint32_t>(((done + i) / NS) & 1);
+            if (!mbar_wait(&bar[st], phase))
+                atomicExch(&abort_flag, 1);
+            __syncthreads();
+            if (abort_flag)
+                break;
+            const unsigned char* sb = pipe2_smem + st * kStageBytes;
+            float a[8], x[8];
+            load8<S>(reinterpret_cast<const S*>(sb), e, 0, a);
+            if (bytes[1] != 0U) {
+                load8<S>(reinterpret_cast<const S*>(sb + kLoBytes), e, off[1], x);
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
-                    b[q] = b[q] + x[q];
+                    a[q] = a[q] + x[q];
             }
+            if (bytes[2] != 0U) {
+                float b[8];
+                load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + kHiBytes), e, off[2], b);
+                if (bytes[3] != 0U) {
+                    load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], x);
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                a[q] = a[q] + b[q];
-        }
-        S* dst = dst_row + static_cast<int64_t>(tile0 + i) * kTimePerCta + e;
-        if constexpr (sizeof(S) == 4) {
-            float4* d4 = reinterpret_cast<float4*>(dst);
-            d4[0]      = make_float4(a[0], a[1], a[2], a[3]);
-            d4[1]      = make_float4(a[4], a[5], a[6], a[7]);
-        } else {
-            uint32_t r[4];
+                    for (int q = 0; q < 8; ++q)
+                        b[q] = b[q] + x[q];
+                }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const __half2 h = __floats2half2_rn(fminf(fmaxf(a[2 * q], -65504.0F), 65504.0F),
-                                                    fminf(fmaxf(a[2 * q + 1], -65504.0F), 65504.0F));
-                r[q] = *reinterpret_cast<const uint32_t*>(&h);
+                for (int q = 0; q < 8; ++q)
+                    a[q] = a[q] + b[q];
             }
-            *reinterpret_cast<uint4*>(dst) = make_uint4(r[0], r[1], r[2], r[3]);
+            S* dst = dst_row + static_cast<int64_t>(tile0 + i) * kTimePerCta + e;
+            if constexpr (sizeof(S) == 4) {
+                float4* d4 = reinterpret_cast<float4*>(dst);
+                d4[0]      = make_float4(a[0], a[1], a[2], a[3]);
+                d4[1]      = make_float4(a[4], a[5], a[6], a[7]);
+            } else {
+                uint32_t r[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const __half2 h = __floats2half2_rn(fminf(fmaxf(a[2 * q], -65504.0F), 65504.0F),
+                                                        fminf(fmaxf(a[2 * q + 1], -65504.0F), 65504.0F));
+                    r[q] = *reinterpret_cast<const uint32_t*>(&h);
+                }
+                *reinterpret_cast<uint4*>(dst) = make_uint4(r[0], r[1], r[2], r[3]);
+            }
+            __syncthreads(); // every thread is done with stage st
+            if (threadIdx.x == 0 && i + NS < nt)
+                issue(i + NS);
         }
-        __syncthreads(); // every thread is done with stage st
-        if (threadIdx.x == 0 && i + NS < nt)
-            issue(i + NS);
-    }
-    if (i < nt && threadIdx.x == 0) {
-        // a wait ran out: report it, then let the copies still in flight land
-        atomicOr(err, 1U);
-        for (int j = i; j < min(nt, i + NS); ++j)
-            (void)mbar_wait(&bar[j % NS], static_cast<uint32_t>((j / NS) & 1));
+        if (i < nt) {
+            if (threadIdx.x == 0) {
+                // a wait ran out: report it, then let the copies still in flight land
+                atomicOr(err, 1U);
+                for (int j = i; j < min(nt, i + NS); ++j)
+                    (void)mbar_wait(&bar[(done + j) % NS], static_cast<uint32_t>(((done + j) / NS) & 1));
+            }
+            return;
+        }
+        done += nt;
     }
 }
 
@@ -576,13 +600,24 @@ void launch_capture_rows(LevelView v, const int64_t* rows, int64_t nrows, float*
     FB_LAUNCH_CHECK();
 }
 
+namespace {
+// One CTA per work item, or at most `ctas` CTAs looping over the items.
+unsigned grid_for(int64_t items, int32_t ctas) {
+    const int64_t g = ctas > 0 ? std::min<int64_t>(items, ctas) : items;
+    if (g > 0x7FFFFFFF)
+        throw Error(FROST_ERR_INTERNAL, "level: too many work items for one launch");
+    return static_cast<unsigned>(g);
+}
+} // namespace
+
 void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnodes,
                    int32_t max_node_delay, const float* waterfall, int64_t waterfall_pitch,
                    int64_t t0, int32_t n_valid, const float* input_hist, int32_t hist_len,
-                   LevelView out, int32_t ncols, cudaStream_t s) {
+                   LevelView out, int32_t ncols, cudaStream_t s, int32_t ctas) {
     if (ncols % kTimePerCta != 0 || max_node_delay > hist_len)
         throw Error(FROST_ERR_INTERNAL, "level1: bad geometry");
-    const dim3 grid(static_cast<unsigned>(nnodes), static_cast<unsigned>(ncols / kTimePerCta));
+    const int32_t ntiles = ncols / kTimePerCta;
+    const dim3 grid(grid_for(static_cast<int64_t>(nnodes) * ntiles, ctas));
     const size_t smem = 2 * sizeof(float) * (kTimePerCta + max_node_delay + 1);
     if (smem > 200 * 1024)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "level1: leaf windows too long for shared memory");
@@ -590,20 +625,20 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
         FB_CUDA(cudaFuncSetAttribute(k_level1<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         k_level1<__half><<<grid, kThreads, smem, s>>>(
-            ops, node_first_op, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
+            ops, node_first_op, nnodes, ntiles, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
             input_hist, hist_len, static_cast<__half*>(out.data), out.pitch, out.base);
     } else {
         FB_CUDA(cudaFuncSetAttribute(k_level1<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         k_level1<float><<<grid, kThreads, smem, s>>>(
-            ops, node_first_op, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
+            ops, node_first_op, nnodes, ntiles, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
             input_hist, hist_len, static_cast<float*>(out.data), out.pitch, out.base);
     }
     FB_LAUNCH_CHECK();
 }
 
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  unsigned* err, cudaStream_t s, int32_t tpc) {
+                  unsigned* err, cudaStream_t s, int32_t tpc, int32_t ctas) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
@@ -626,8 +661,7 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
         FB_LAUNCH_CHECK();
         return;
     }
-    const dim3 grid(static_cast<unsigned>(nrows),
-                    static_cast<unsigned>((ntiles + tpc - 1) / tpc));
+    const dim3 grid(grid_for(nrows * ((ntiles + tpc - 1) / tpc), ctas));
     const size_t es   = out.fp16 ? 2 : 4;
     const size_t smem = kStages * (2 * kTimePerCta * es + 16);
     if (out.fp16) {
@@ -635,13 +669,13 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
                                      static_cast<int>(smem)));
         k_level_pipe<__half><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const __half*>(in.data), in.pitch, in.base,
-            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, err);
+            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err);
     } else {
         FB_CUDA(cudaFuncSetAttribute(k_level_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         k_level_pipe<float><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const float*>(in.data), in.pitch, in.base,
-            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, err);
+            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err);
     }
     FB_LAUNCH_CHECK();
 }
@@ -649,28 +683,28 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
 namespace {
 template <class S, int NS>
 void level2_stages(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
-                   unsigned* err, cudaStream_t s) {
+                   int64_t nrows, unsigned* err, cudaStream_t s) {
     const size_t smem = NS * (4 * kTimePerCta * sizeof(S) + 48);
     FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<S, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     k_level2_pipe<S, NS><<<grid, kThreads, smem, s>>>(ops, static_cast<const S*>(in.data), in.pitch, in.base,
                                                       static_cast<S*>(out.data), out.pitch, out.base, ntiles,
-                                                      tpc, err);
+                                                      tpc, nrows, err);
 }
 template <class S>
 void level2_typed(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
-                  int32_t stages, unsigned* err, cudaStream_t s) {
+                  int64_t nrows, int32_t stages, unsigned* err, cudaStream_t s) {
     switch (stages == 0 ? kStages2<S> : stages) {
-    case 2: level2_stages<S, 2>(ops, grid, in, out, ntiles, tpc, err, s); break;
-    case 3: level2_stages<S, 3>(ops, grid, in, out, ntiles, tpc, err, s); break;
-    case 4: level2_stages<S, 4>(ops, grid, in, out, ntiles, tpc, err, s); break;
+    case 2: level2_stages<S, 2>(ops, grid, in, out, ntiles, tpc, nrows, err, s); break;
+    case 3: level2_stages<S, 3>(ops, grid, in, out, ntiles, tpc, nrows, err, s); break;
+    case 4: level2_stages<S, 4>(ops, grid, in, out, ntiles, tpc, nrows, err, s); break;
     default: throw Error(FROST_ERR_INTERNAL, "level2: stages must be 2, 3 or 4");
     }
 }
 } // namespace
 
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                   unsigned* err, cudaStream_t s, int32_t tpc, int32_t stages) {
+                   unsigned* err, cudaStream_t s, int32_t tpc, int32_t stages, int32_t ctas) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
@@ -681,11 +715,11 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
     if (stages == 4 && !out.fp16)
         throw Error(FROST_ERR_INTERNAL, "level2: 4 float stages exceed the shared memory of a CTA");
     const int ntiles = ncols / kTimePerCta;
-    const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>((ntiles + tpc - 1) / tpc));
+    const dim3 grid(grid_for(nrows * ((ntiles + tpc - 1) / tpc), ctas));
     if (out.fp16)
-        level2_typed<__half>(ops, grid, in, out, ntiles, tpc, stages, err, s);
+        level2_typed<__half>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, s);
     else
-        level2_typed<float>(ops, grid, in, out, ntiles, tpc, stages, err, s);
+        level2_typed<float>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, s);
     FB_LAUNCH_CHECK();
 }
 

@@ -21,20 +21,25 @@ struct LevelView {
 
 constexpr int kTimePerCta = 2048; // samples per CTA in the level kernels
 
+/* Residency: every level launcher takes `ctas`, the most CTAs of the launch
+ * (0: one CTA per work item). With a cap each CTA loops over work items, so
+ * a launch holds at most `ctas` CTAs' resources and leaves the rest of the
+ * GPU to other streams' kernels; results do not depend on it. */
+
 /** Level 1 straight from the input channels: each row is the sum of two
  * leaf windows read from the waterfall (columns t0 .. t0 + n_valid) and,
  * for times before the tile, the input history [C][hist_len]. */
 void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnodes,
                    int32_t max_node_delay, const float* waterfall, int64_t waterfall_pitch,
                    int64_t t0, int32_t n_valid, const float* input_hist, int32_t hist_len,
-                   LevelView out, int32_t ncols, cudaStream_t s);
+                   LevelView out, int32_t ncols, cudaStream_t s, int32_t ctas = 0);
 
 /** Level h >= 2: out[row] = in[lo] + in[hi] shifted. With `err` non-null
  * the TMA-pipelined kernel runs (each CTA takes `tiles_per_cta` tiles of
  * 2048 columns) and sets *err if a bounded wait ran out; with `err` null
  * the direct (one CTA per row and tile) kernel runs. */
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16);
+                  unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t ctas = 0);
 
 /** A row of level h+1 from four rows of level h-1: the sum of row[j] read at
  * t - shift[j] (shift[0] = 0), grouped (row0 + row1) + (row2 + row3); a
@@ -49,7 +54,8 @@ struct FusedOp {
  * fp16 storage; 0 = 4 for fp16, 3 for float): fewer stages leave room for
  * more CTAs per SM. */
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                   unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t stages = 0);
+                   unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t stages = 0,
+                   int32_t ctas = 0);
 
 /** Copies the last `hist` columns ending at column base + n_valid of every
  * row of `view` into hist_buf[rows][hist]. */

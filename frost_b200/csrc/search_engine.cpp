@@ -66,6 +66,7 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     if (device < 0 || device >= ndev)
         invalid("search: device " + std::to_string(device) + " does not exist");
     DeviceGuard g(device);
+    FB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, device));
     FB_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
     cudaStream_t s = m_stream;
 
@@ -376,6 +377,19 @@ void Engine::set_launch_shape(bool fuse, int32_t tpc, int32_t stages, int32_t ch
     apply_shape(fuse, tpc, stages, chunk);
 }
 
+void Engine::set_residency(int32_t ctas_per_sm) {
+    if (ctas_per_sm < 0 || ctas_per_sm > 64)
+        invalid("search: CTAs per SM must be in [0, 64]");
+    DeviceGuard g(m_device);
+    FB_CUDA(cudaStreamSynchronize(m_stream));
+    if (m_graph != nullptr) {
+        // the captured launches carry the old grids
+        FB_CUDA(cudaGraphExecDestroy(m_graph));
+        m_graph = nullptr;
+    }
+    m_ctas_per_sm = ctas_per_sm;
+}
+
 Engine::Tuned Engine::launch_shape() const {
     return Tuned{m_fuse, m_level_tpc, m_level2_stages, m_search_chunk, 0.0, false};
 }
@@ -669,7 +683,7 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                                   static_cast<int32_t>(m_node_first_op.size() - 1),
                                   m_plan.level_history(0), wf, static_cast<int64_t>(nsamps), t_off,
                                   n_valid, m_in_hist.as<float>(), m_plan.level_history(0), out,
-                                  static_cast<int32_t>(m_ncols), s);
+                                  static_cast<int32_t>(m_ncols), s, cta_cap());
                 });
                 timed(kHistory, s, [&] {
                     launch_save_input_history(wf, static_cast<int64_t>(nsamps), t_off, n_valid, C,
@@ -685,10 +699,11 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                     if (st.fused)
                         launch_level2(m_fused_ops.as<FusedOp>() + st.op_offset, m_plan.level_rows(h),
                                       view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc,
-                                      m_level2_stages);
+                                      m_level2_stages, cta_cap());
                     else
                         launch_level(m_row_ops.as<RowOp>() + st.op_offset, m_plan.level_rows(h),
-                                     view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc);
+                                     view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc,
+                                     cta_cap());
                 });
                 m_launches += 1;
                 m_timing.level_launches += 1;
@@ -700,7 +715,7 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
             });
             if (m_height_g1[h] > m_height_g0[h]) {
                 timed(kSearch, s,
-                      [&] { launch_search(sp, out, m_height_g0[h], m_height_g1[h], s, m_search_chunk); });
+                      [&] { launch_search(sp, out, m_height_g0[h], m_height_g1[h], s, m_search_chunk, cta_cap()); });
                 m_launches += 1;
                 m_timing.search_launches += 1;
                 m_timing.algorithmic_search_bytes +=

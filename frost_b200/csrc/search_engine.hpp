@@ -121,7 +121,17 @@ private:
      * stream (call before the first gulp). */
     void set_launch_shape(bool fuse, int32_t tiles_per_cta, int32_t stages, int32_t search_chunk);
     Tuned launch_shape() const;
+    /** Caps the level and search kernels at `ctas_per_sm` resident CTAs per
+     * SM, each CTA looping over work items (0: one CTA per work item). The
+     * rest of every SM stays free for other streams' kernels (the served
+     * beams' kernels overlap); results do not depend on it. */
+    void set_residency(int32_t ctas_per_sm);
+    int32_t residency() const { return m_ctas_per_sm; }
   private:
+    int32_t m_ctas_per_sm = 0;
+    int32_t m_sms         = 0;
+    /** CTA cap of a launch (0: none). */
+    int32_t cta_cap() const { return m_ctas_per_sm > 0 ? m_sms * m_ctas_per_sm : 0; }
     std::vector<DeviceBuffer> m_capture;
     bool m_capture_on = false;
     int64_t m_capture_cols = 0;

@@ -26,6 +26,8 @@
 // and gulp) and emitting each closed run's peak. The DM-time rows are never
 // re-read and the run state is the only thing carried between calls.
 
+#include <algorithm>
+
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -359,7 +361,8 @@ __device__ void scan_halo(const S* seg, int halo, int jmin, float* Q, float* gmi
 
 template <class S, int CH>
 __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
-    k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0) {
+    k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0,
+             int64_t nrows) {
     constexpr int P  = CH / kThreads; // chunk columns per thread
     constexpr int NG = P / 4;         // 4-column groups per thread
     // Dynamic shared memory (floats unless noted):
@@ -386,47 +389,12 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     __shared__ float warp_tot[kThreads / 32];
     __shared__ float wtail[kThreads / 32][2]; // each warp's last two prefix values
 
-    const int64_t g     = g0 + blockIdx.x;
-    const SearchRow row = p.rows[g];
     const int nw        = p.nwidths;
     const int wmax      = p.wmax;
     const int halo      = p.halo;
     const bool across   = p.peak_mode == FROST_PEAK_ACROSS_WIDTHS;
     const bool all      = p.peak_mode == FROST_PEAK_ALL;
-    if (threadIdx.x == 0) {
-        local_count  = p.row_counts[g];
-        const GulpClock ck = *p.clock;
-        rc.gulp_t0   = ck.gulp_t0;
-        rc.tile_t0   = ck.gulp_t0 + p.tile_off;
-        rc.or_active = ck.or_active;
-    }
-    if (threadIdx.x < nw) {
-        const int w    = threadIdx.x;
-        const int W    = p.widths[w];
-        const int E    = (p.trapezoid && W >= 3) ? (W + 1) / 4 : 0;
-        rc.W[w]        = W;
-        rc.E[w]        = E;
-        const float iv = p.inv_sigma[g * nw + w];
-        rc.inv[w]      = iv;
-        rc.inv_or[w]   = p.inv_sigma_or[g * nw + w];
-        const float T  = iv > 0.0F ? p.thresh / iv : FB_POS_INF;
-        rc.thr[w]      = T;
-        WidthTest t;
-        t.kind   = E > 0 ? kTestAll : W <= 2 ? kTestExact : W < 4 * P ? kTestGroup : kTestBlock;
-        t.W      = W;
-        t.gconst = (halo - W) >> 2;
-        t.two    = ((halo - W) & 3) != 0 ? 1 : 0;
-        t.bconst = (halo - W) / P;
-        t.btwo   = ((halo - W) % P) != 0 ? 1 : 0;
-        t.T      = T;
-        t.pad    = 0;
-        wt[w]    = t;
-    }
-    const int nruns = across ? 1 : nw;
-    if (threadIdx.x < nruns && !all)
-        runs[threadIdx.x] = p.carry[g * nruns + threadIdx.x];
-    __syncthreads();
-
+    const int nruns     = across ? 1 : nw;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg_cols   = halo + CH;
     float* const Q       = Ps + 4 + halo;
@@ -436,331 +404,373 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     float* const nh0     = tmin + seg_cols / P;
     uint32_t* const bits = reinterpret_cast<uint32_t*>(nh0 + 2 * nh_len);
     S* const stage0      = reinterpret_cast<S*>(bits + search_bits_words(nw, CH)); // buffer b at stage0 + b * seg_cols
-    const S* src         = level + row.level_row * pitch + base;
     // A chunk's halo is the previous chunk's last `halo` columns, whose prefix
     // sums that chunk has: only the first chunk (or every chunk, for a halo
     // wider than a chunk) stages and scans its halo.
     const bool carry_halo = halo <= CH;
     const int nchunks     = (p.n_valid + CH - 1) / CH;
-    auto issue = [&](int ci) {
-        const int off        = (ci == 0 || !carry_halo) ? 0 : halo;
-        const uint32_t bytes = static_cast<uint32_t>((seg_cols - off) * sizeof(S));
-        bulk::mbar_expect(&bar[ci & 1], bytes);
-        bulk::load(stage0 + (ci & 1) * seg_cols + off, src + static_cast<int64_t>(ci) * CH - halo + off, bytes,
-                   &bar[ci & 1]);
-    };
     if (threadIdx.x == 0) {
         abort_flag = 0;
         bulk::mbar_init(&bar[0]);
         bulk::mbar_init(&bar[1]);
     }
     __syncthreads();
-    if (threadIdx.x == 0)
-        for (int ci = 0; ci < min(2, nchunks); ++ci)
-            issue(ci);
-    const int jmin     = halo - wmax + 1; // earlier columns never enter a window
-    const int64_t warm = static_cast<int64_t>(row.delay) + wmax - 1;
-    auto close_runs = [&]() {
-        // nothing fired: runs open at the chunk start close here
-        if (!all && threadIdx.x < nruns && runs[threadIdx.x].open) {
-            emit(p, row, runs[threadIdx.x], &local_count);
-            runs[threadIdx.x].open = 0;
+    // Rows blockIdx.x, blockIdx.x + gridDim.x, ...; the staging buffers and
+    // barriers alternate over the CTA's chunks across rows.
+    int64_t cc = 0; // chunks this CTA has consumed
+    for (int64_t gi = blockIdx.x; gi < nrows; gi += gridDim.x) {
+        const int64_t g = g0 + gi;
+        const SearchRow row = p.rows[g];
+        if (threadIdx.x == 0) {
+            local_count  = p.row_counts[g];
+            const GulpClock ck = *p.clock;
+            rc.gulp_t0   = ck.gulp_t0;
+            rc.tile_t0   = ck.gulp_t0 + p.tile_off;
+            rc.or_active = ck.or_active;
         }
-    };
-    int ci = 0;
-    for (int64_t c0 = 0; c0 < p.n_valid; c0 += CH, ++ci) {
-        // ---- wait for the chunk's segment (bounded; a timeout ends the row)
-        if (!bulk::mbar_wait(&bar[ci & 1], static_cast<uint32_t>((ci >> 1) & 1)))
-            atomicExch(&abort_flag, 1);
-        __syncthreads();
-        if (abort_flag)
-            break;
-        const S* seg           = stage0 + (ci & 1) * seg_cols;
-        const bool direct_halo = ci == 0 || !carry_halo;
-        if (direct_halo)
-            scan_halo<S, P>(seg, halo, jmin, Q, gmin, tmin);
-        // ---- prefix sums of the thread's P columns: serial, then across the
-        // warp (shuffles), then across warps (one offset per warp)
-        float q[P];
-        ld_cols<S, P>(seg + halo + P * threadIdx.x, q);
-#pragma unroll
-        for (int e = 1; e < P; ++e)
-            q[e] += q[e - 1];
-        float incl = q[P - 1];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const float u = __shfl_up_sync(0xFFFFFFFFU, incl, o);
-            if (lane >= o)
-                incl += u;
+        if (threadIdx.x < nw) {
+            const int w    = threadIdx.x;
+            const int W    = p.widths[w];
+            const int E    = (p.trapezoid && W >= 3) ? (W + 1) / 4 : 0;
+            rc.W[w]        = W;
+            rc.E[w]        = E;
+            const float iv = p.inv_sigma[g * nw + w];
+            rc.inv[w]      = iv;
+            rc.inv_or[w]   = p.inv_sigma_or[g * nw + w];
+            const float T  = iv > 0.0F ? p.thresh / iv : FB_POS_INF;
+            rc.thr[w]      = T;
+            WidthTest t;
+            t.kind   = E > 0 ? kTestAll : W <= 2 ? kTestExact : W < 4 * P ? kTestGroup : kTestBlock;
+            t.W      = W;
+            t.gconst = (halo - W) >> 2;
+            t.two    = ((halo - W) & 3) != 0 ? 1 : 0;
+            t.bconst = (halo - W) / P;
+            t.btwo   = ((halo - W) % P) != 0 ? 1 : 0;
+            t.T      = T;
+            t.pad    = 0;
+            wt[w]    = t;
         }
-        float excl = __shfl_up_sync(0xFFFFFFFFU, incl, 1);
-        if (lane == 0)
-            excl = 0.0F;
-        if (lane == 31)
-            warp_tot[warp] = incl;
-        __syncthreads();
-        // every thread has read this chunk's staging buffer: refill it
-        if (threadIdx.x == 0 && ci + 2 < nchunks)
-            issue(ci + 2);
-        float woff = 0.0F;
-        for (int w = 0; w < warp; ++w)
-            woff += warp_tot[w];
-        const float off = excl + woff;
-#pragma unroll
-        for (int e = 0; e < P; ++e)
-            q[e] += off;
-        // ---- group and block extremes (registers; the minima to shared memory)
-        float gmx[NG], gmn[NG];
-#pragma unroll
-        for (int gq = 0; gq < NG; ++gq) {
-            gmx[gq] = fmaxf(fmaxf(q[4 * gq], q[4 * gq + 1]), fmaxf(q[4 * gq + 2], q[4 * gq + 3]));
-            gmn[gq] = fminf(fminf(q[4 * gq], q[4 * gq + 1]), fminf(q[4 * gq + 2], q[4 * gq + 3]));
-        }
-        float bmax = gmx[0], bmin = gmn[0];
-#pragma unroll
-        for (int gq = 1; gq < NG; ++gq) {
-            bmax = fmaxf(bmax, gmx[gq]);
-            bmin = fminf(bmin, gmn[gq]);
-        }
-        if constexpr (NG == 4)
-            reinterpret_cast<float4*>(gmin + halo / 4)[threadIdx.x] = make_float4(gmn[0], gmn[1], gmn[2], gmn[3]);
-        else
-            reinterpret_cast<float2*>(gmin + halo / 4)[threadIdx.x] = make_float2(gmn[0], gmn[1]);
-        tmin[halo / P + threadIdx.x] = bmin;
-        if (lane == 31) {
-            wtail[warp][0] = q[P - 2];
-            wtail[warp][1] = q[P - 1];
-        }
-        if (carry_halo) {
-            // the next chunk's halo: this chunk's last `halo` columns
-            float* nh    = nh0 + (ci & 1) * nh_len;
-            const int tt = static_cast<int>(threadIdx.x) - (kThreads - halo / P);
-            if (tt >= 0) {
-                float4* d = reinterpret_cast<float4*>(nh + P * tt);
-#pragma unroll
-                for (int i = 0; i < P / 4; ++i)
-                    d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
-#pragma unroll
-                for (int gq = 0; gq < NG; ++gq)
-                    nh[halo + NG * tt + gq] = gmn[gq];
-                nh[halo + halo / 4 + tt] = bmin;
-                if (threadIdx.x == kThreads - 1)
-                    nh[halo + halo / 4 + halo / P] = q[P - 1];
-            }
-            if (!direct_halo) {
-                // this chunk's halo from the previous chunk's, rebased so that Q[-1] = 0
-                const float* ph  = nh0 + ((ci - 1) & 1) * nh_len;
-                const int n      = halo + halo / 4 + halo / P;
-                const float last = ph[n];
-                for (int i = threadIdx.x; i < n; i += kThreads) {
-                    const float v = ph[i] - last;
-                    if (i < halo)
-                        Q[i - halo] = v;
-                    else if (i < halo + halo / 4)
-                        gmin[i - halo] = v;
-                    else
-                        tmin[i - halo - halo / 4] = v;
-                }
-            }
-        }
+        if (threadIdx.x < nruns && !all)
+            runs[threadIdx.x] = p.carry[g * nruns + threadIdx.x];
         __syncthreads();
 
-        auto store_q = [&]() {
-            float4* d = reinterpret_cast<float4*>(Q + P * threadIdx.x);
-#pragma unroll
-            for (int i = 0; i < P / 4; ++i)
-                d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
-            for (int i = threadIdx.x; i < nw * (CH / 32); i += kThreads)
-                bits[i] = 0U;
-            if (threadIdx.x == 0)
-                fired_w = 0U;
+        const S* src = level + row.level_row * pitch + base;
+        auto issue = [&](int ci) {
+            const int b          = static_cast<int>((cc + ci) & 1);
+            const int off        = (ci == 0 || !carry_halo) ? 0 : halo;
+            const uint32_t bytes = static_cast<uint32_t>((seg_cols - off) * sizeof(S));
+            bulk::mbar_expect(&bar[b], bytes);
+            bulk::load(stage0 + b * seg_cols + off, src + static_cast<int64_t>(ci) * CH - halo + off, bytes, &bar[b]);
         };
-        const bool fast = c0 + CH <= p.n_valid && (!p.skip_cold || rc.tile_t0 + c0 >= warm) &&
-                          (!rc.or_active || rc.tile_t0 + c0 - rc.gulp_t0 >= warm);
-        if (fast) {
-            // ---- steady state. A window sum Q[k] - Q[k - W] of a set of
-            // samples is at most their greatest Q minus the least Q their
-            // windows start from (rounding is monotonic), so a set the bound
-            // clears cannot fire. Widths 1 and 2 take the exact sums in
-            // registers, the others a bound per 4-sample group (wide boxcars
-            // first one per thread); only a chunk where some test may fire
-            // stores Q and runs the exact tests.
-            float pm1 = __shfl_up_sync(0xFFFFFFFFU, q[P - 1], 1); // Q[P t - 1]
-            float pm2 = __shfl_up_sync(0xFFFFFFFFU, q[P - 2], 1); // Q[P t - 2]
-            if (lane == 0) {
-                pm1 = warp == 0 ? Q[-1] : wtail[warp - 1][1];
-                pm2 = warp == 0 ? Q[-2] : wtail[warp - 1][0];
+        if (threadIdx.x == 0)
+            for (int ci = 0; ci < min(2, nchunks); ++ci)
+                issue(ci);
+        const int jmin     = halo - wmax + 1; // earlier columns never enter a window
+        const int64_t warm = static_cast<int64_t>(row.delay) + wmax - 1;
+        auto close_runs = [&]() {
+            // nothing fired: runs open at the chunk start close here
+            if (!all && threadIdx.x < nruns && runs[threadIdx.x].open) {
+                emit(p, row, runs[threadIdx.x], &local_count);
+                runs[threadIdx.x].open = 0;
             }
-            uint32_t cand = 0U;
-            for (int wi = 0; wi < nw; ++wi) {
-                const WidthTest t = wt[wi];
-                bool maybe        = true;
-                if (t.kind == kTestExact) {
-                    float m;
-                    if (t.W == 1) {
-                        m = q[0] - pm1;
-#pragma unroll
-                        for (int e = 1; e < P; ++e)
-                            m = fmaxf(m, q[e] - q[e - 1]);
+        };
+        int ci = 0;
+        for (int64_t c0 = 0; c0 < p.n_valid; c0 += CH, ++ci) {
+            // ---- wait for the chunk's segment (bounded; a timeout ends the row)
+            if (!bulk::mbar_wait(&bar[(cc + ci) & 1], static_cast<uint32_t>(((cc + ci) >> 1) & 1)))
+                atomicExch(&abort_flag, 1);
+            __syncthreads();
+            if (abort_flag)
+                break;
+            const S* seg           = stage0 + ((cc + ci) & 1) * seg_cols;
+            const bool direct_halo = ci == 0 || !carry_halo;
+            if (direct_halo)
+                scan_halo<S, P>(seg, halo, jmin, Q, gmin, tmin);
+            // ---- prefix sums of the thread's P columns: serial, then across the
+            // warp (shuffles), then across warps (one offset per warp)
+            float q[P];
+            ld_cols<S, P>(seg + halo + P * threadIdx.x, q);
+    #pragma unroll
+            for (int e = 1; e < P; ++e)
+                q[e] += q[e - 1];
+            float incl = q[P - 1];
+    #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float u = __shfl_up_sync(0xFFFFFFFFU, incl, o);
+                if (lane >= o)
+                    incl += u;
+            }
+            float excl = __shfl_up_sync(0xFFFFFFFFU, incl, 1);
+            if (lane == 0)
+                excl = 0.0F;
+            if (lane == 31)
+                warp_tot[warp] = incl;
+            __syncthreads();
+            // every thread has read this chunk's staging buffer: refill it
+            if (threadIdx.x == 0 && ci + 2 < nchunks)
+                issue(ci + 2);
+            float woff = 0.0F;
+            for (int w = 0; w < warp; ++w)
+                woff += warp_tot[w];
+            const float off = excl + woff;
+    #pragma unroll
+            for (int e = 0; e < P; ++e)
+                q[e] += off;
+            // ---- group and block extremes (registers; the minima to shared memory)
+            float gmx[NG], gmn[NG];
+    #pragma unroll
+            for (int gq = 0; gq < NG; ++gq) {
+                gmx[gq] = fmaxf(fmaxf(q[4 * gq], q[4 * gq + 1]), fmaxf(q[4 * gq + 2], q[4 * gq + 3]));
+                gmn[gq] = fminf(fminf(q[4 * gq], q[4 * gq + 1]), fminf(q[4 * gq + 2], q[4 * gq + 3]));
+            }
+            float bmax = gmx[0], bmin = gmn[0];
+    #pragma unroll
+            for (int gq = 1; gq < NG; ++gq) {
+                bmax = fmaxf(bmax, gmx[gq]);
+                bmin = fminf(bmin, gmn[gq]);
+            }
+            if constexpr (NG == 4)
+                reinterpret_cast<float4*>(gmin + halo / 4)[threadIdx.x] = make_float4(gmn[0], gmn[1], gmn[2], gmn[3]);
+            else
+                reinterpret_cast<float2*>(gmin + halo / 4)[threadIdx.x] = make_float2(gmn[0], gmn[1]);
+            tmin[halo / P + threadIdx.x] = bmin;
+            if (lane == 31) {
+                wtail[warp][0] = q[P - 2];
+                wtail[warp][1] = q[P - 1];
+            }
+            if (carry_halo) {
+                // the next chunk's halo: this chunk's last `halo` columns
+                float* nh    = nh0 + (ci & 1) * nh_len;
+                const int tt = static_cast<int>(threadIdx.x) - (kThreads - halo / P);
+                if (tt >= 0) {
+                    float4* d = reinterpret_cast<float4*>(nh + P * tt);
+    #pragma unroll
+                    for (int i = 0; i < P / 4; ++i)
+                        d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+    #pragma unroll
+                    for (int gq = 0; gq < NG; ++gq)
+                        nh[halo + NG * tt + gq] = gmn[gq];
+                    nh[halo + halo / 4 + tt] = bmin;
+                    if (threadIdx.x == kThreads - 1)
+                        nh[halo + halo / 4 + halo / P] = q[P - 1];
+                }
+                if (!direct_halo) {
+                    // this chunk's halo from the previous chunk's, rebased so that Q[-1] = 0
+                    const float* ph  = nh0 + ((ci - 1) & 1) * nh_len;
+                    const int n      = halo + halo / 4 + halo / P;
+                    const float last = ph[n];
+                    for (int i = threadIdx.x; i < n; i += kThreads) {
+                        const float v = ph[i] - last;
+                        if (i < halo)
+                            Q[i - halo] = v;
+                        else if (i < halo + halo / 4)
+                            gmin[i - halo] = v;
+                        else
+                            tmin[i - halo - halo / 4] = v;
+                    }
+                }
+            }
+            __syncthreads();
+
+            auto store_q = [&]() {
+                float4* d = reinterpret_cast<float4*>(Q + P * threadIdx.x);
+    #pragma unroll
+                for (int i = 0; i < P / 4; ++i)
+                    d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+                for (int i = threadIdx.x; i < nw * (CH / 32); i += kThreads)
+                    bits[i] = 0U;
+                if (threadIdx.x == 0)
+                    fired_w = 0U;
+            };
+            const bool fast = c0 + CH <= p.n_valid && (!p.skip_cold || rc.tile_t0 + c0 >= warm) &&
+                              (!rc.or_active || rc.tile_t0 + c0 - rc.gulp_t0 >= warm);
+            if (fast) {
+                // ---- steady state. A window sum Q[k] - Q[k - W] of a set of
+                // samples is at most their greatest Q minus the least Q their
+                // windows start from (rounding is monotonic), so a set the bound
+                // clears cannot fire. Widths 1 and 2 take the exact sums in
+                // registers, the others a bound per 4-sample group (wide boxcars
+                // first one per thread); only a chunk where some test may fire
+                // stores Q and runs the exact tests.
+                float pm1 = __shfl_up_sync(0xFFFFFFFFU, q[P - 1], 1); // Q[P t - 1]
+                float pm2 = __shfl_up_sync(0xFFFFFFFFU, q[P - 2], 1); // Q[P t - 2]
+                if (lane == 0) {
+                    pm1 = warp == 0 ? Q[-1] : wtail[warp - 1][1];
+                    pm2 = warp == 0 ? Q[-2] : wtail[warp - 1][0];
+                }
+                uint32_t cand = 0U;
+                for (int wi = 0; wi < nw; ++wi) {
+                    const WidthTest t = wt[wi];
+                    bool maybe        = true;
+                    if (t.kind == kTestExact) {
+                        float m;
+                        if (t.W == 1) {
+                            m = q[0] - pm1;
+    #pragma unroll
+                            for (int e = 1; e < P; ++e)
+                                m = fmaxf(m, q[e] - q[e - 1]);
+                        } else {
+                            m = fmaxf(q[0] - pm2, q[1] - pm1);
+    #pragma unroll
+                            for (int e = 2; e < P; ++e)
+                                m = fmaxf(m, q[e] - q[e - 2]);
+                        }
+                        maybe = m > t.T;
+                    } else if (t.kind != kTestAll) {
+                        if (t.kind == kTestBlock) {
+                            const int b = static_cast<int>(threadIdx.x) + t.bconst;
+                            float lo    = tmin[b];
+                            if (t.btwo)
+                                lo = fminf(lo, tmin[b + 1]);
+                            maybe = bmax - lo > t.T;
+                        }
+                        if (maybe) {
+                            float lo[NG];
+                            group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
+                            float m = gmx[0] - lo[0];
+    #pragma unroll
+                            for (int gq = 1; gq < NG; ++gq)
+                                m = fmaxf(m, gmx[gq] - lo[gq]);
+                            maybe = m > t.T;
+                        }
+                    }
+                    if (maybe)
+                        cand |= 1U << wi;
+                }
+                if (!__syncthreads_or(cand != 0U)) {
+                    close_runs();
+                    continue; // shared memory is rewritten only after every thread passed the barrier
+                }
+                store_q();
+                __syncthreads();
+                bool up = false;
+                // the exact test of group gi at width wi (sets the fired bits)
+                auto exact = [&](int gi, int wi, int W, int E, float T) {
+                    const int k    = 4 * gi;
+                    const float4 a = *reinterpret_cast<const float4*>(Q + k);
+                    const float4 b = ld4(Q, k - W);
+                    float s0, s1, s2, s3;
+                    if (E > 0) {
+                        const float4 c = ld4(Q, k - E);
+                        const float4 d = ld4(Q, k - W + E);
+                        s0 = trap_sum(a.x, b.x, c.x, d.x);
+                        s1 = trap_sum(a.y, b.y, c.y, d.y);
+                        s2 = trap_sum(a.z, b.z, c.z, d.z);
+                        s3 = trap_sum(a.w, b.w, c.w, d.w);
                     } else {
-                        m = fmaxf(q[0] - pm2, q[1] - pm1);
-#pragma unroll
-                        for (int e = 2; e < P; ++e)
-                            m = fmaxf(m, q[e] - q[e - 2]);
+                        s0 = a.x - b.x;
+                        s1 = a.y - b.y;
+                        s2 = a.z - b.z;
+                        s3 = a.w - b.w;
                     }
-                    maybe = m > t.T;
-                } else if (t.kind != kTestAll) {
-                    if (t.kind == kTestBlock) {
-                        const int b = static_cast<int>(threadIdx.x) + t.bconst;
-                        float lo    = tmin[b];
-                        if (t.btwo)
-                            lo = fminf(lo, tmin[b + 1]);
-                        maybe = bmax - lo > t.T;
+                    const uint32_t nib = (s0 > T ? 1U : 0U) | (s1 > T ? 2U : 0U) | (s2 > T ? 4U : 0U) |
+                                         (s3 > T ? 8U : 0U);
+                    if (nib != 0U) {
+                        // samples 4 gi .. 4 gi + 3: word gi / 8, nibble gi % 8
+                        atomicOr(&bits[wi * (CH / 32) + (gi >> 3)], nib << ((gi & 7) * 4));
+                        atomicOr(&fired_w, 1U << wi);
+                        up = true;
                     }
-                    if (maybe) {
+                };
+                for (uint32_t c = cand; c != 0U; c &= c - 1U) {
+                    const int wi      = __ffs(static_cast<int>(c)) - 1;
+                    const WidthTest t = wt[wi];
+                    const int E       = rc.E[wi];
+                    if (t.kind == kTestGroup || t.kind == kTestBlock) {
                         float lo[NG];
                         group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
-                        float m = gmx[0] - lo[0];
-#pragma unroll
-                        for (int gq = 1; gq < NG; ++gq)
-                            m = fmaxf(m, gmx[gq] - lo[gq]);
-                        maybe = m > t.T;
-                    }
-                }
-                if (maybe)
-                    cand |= 1U << wi;
-            }
-            if (!__syncthreads_or(cand != 0U)) {
-                close_runs();
-                continue; // shared memory is rewritten only after every thread passed the barrier
-            }
-            store_q();
-            __syncthreads();
-            bool up = false;
-            // the exact test of group gi at width wi (sets the fired bits)
-            auto exact = [&](int gi, int wi, int W, int E, float T) {
-                const int k    = 4 * gi;
-                const float4 a = *reinterpret_cast<const float4*>(Q + k);
-                const float4 b = ld4(Q, k - W);
-                float s0, s1, s2, s3;
-                if (E > 0) {
-                    const float4 c = ld4(Q, k - E);
-                    const float4 d = ld4(Q, k - W + E);
-                    s0 = trap_sum(a.x, b.x, c.x, d.x);
-                    s1 = trap_sum(a.y, b.y, c.y, d.y);
-                    s2 = trap_sum(a.z, b.z, c.z, d.z);
-                    s3 = trap_sum(a.w, b.w, c.w, d.w);
-                } else {
-                    s0 = a.x - b.x;
-                    s1 = a.y - b.y;
-                    s2 = a.z - b.z;
-                    s3 = a.w - b.w;
-                }
-                const uint32_t nib = (s0 > T ? 1U : 0U) | (s1 > T ? 2U : 0U) | (s2 > T ? 4U : 0U) |
-                                     (s3 > T ? 8U : 0U);
-                if (nib != 0U) {
-                    // samples 4 gi .. 4 gi + 3: word gi / 8, nibble gi % 8
-                    atomicOr(&bits[wi * (CH / 32) + (gi >> 3)], nib << ((gi & 7) * 4));
-                    atomicOr(&fired_w, 1U << wi);
-                    up = true;
-                }
-            };
-            for (uint32_t c = cand; c != 0U; c &= c - 1U) {
-                const int wi      = __ffs(static_cast<int>(c)) - 1;
-                const WidthTest t = wt[wi];
-                const int E       = rc.E[wi];
-                if (t.kind == kTestGroup || t.kind == kTestBlock) {
-                    float lo[NG];
-                    group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
-#pragma unroll
-                    for (int gq = 0; gq < NG; ++gq)
-                        if (gmx[gq] - lo[gq] > t.T)
+    #pragma unroll
+                        for (int gq = 0; gq < NG; ++gq)
+                            if (gmx[gq] - lo[gq] > t.T)
+                                exact(NG * static_cast<int>(threadIdx.x) + gq, wi, t.W, E, t.T);
+                    } else {
+    #pragma unroll
+                        for (int gq = 0; gq < NG; ++gq)
                             exact(NG * static_cast<int>(threadIdx.x) + gq, wi, t.W, E, t.T);
-                } else {
-#pragma unroll
-                    for (int gq = 0; gq < NG; ++gq)
-                        exact(NG * static_cast<int>(threadIdx.x) + gq, wi, t.W, E, t.T);
-                }
-            }
-            if (!__syncthreads_or(up)) {
-                close_runs();
-                continue;
-            }
-        } else {
-            // ---- not steady (cold prefix, mask change, partial chunk): the
-            // bit masks from the general S/N
-            store_q();
-            __syncthreads();
-            for (int j = 0; j < (CH / kThreads); ++j) {
-                const int k = threadIdx.x + j * kThreads;
-                for (int wi = 0; wi < nw; ++wi) {
-                    const bool hit   = snr_general(p, rc, Q, c0, k, wi, row.delay) > p.thresh;
-                    const uint32_t m = __ballot_sync(0xFFFFFFFFU, hit);
-                    if (lane == 0) {
-                        bits[wi * (CH / 32) + j * (kThreads / 32) + warp] = m;
-                        if (m != 0U)
-                            atomicOr(&fired_w, 1U << wi);
                     }
                 }
-            }
-            __syncthreads();
-        }
-        // bits now hold exactly the above-threshold samples of every width
-        const uint32_t fw = fired_w;
-        if (across) {
-            for (int wd = threadIdx.x; wd < (CH / 32); wd += kThreads) {
-                uint32_t m = 0;
-                for (int wi = 0; wi < nw; ++wi)
-                    if ((fw >> wi) & 1U)
-                        m |= bits[wi * (CH / 32) + wd];
-                any_bits[wd] = m;
-            }
-            __syncthreads();
-        }
-        // Widths are independent (each has its own run state): lane 0 of
-        // warp w walks widths w, w + 8, ... Candidates of different widths
-        // may therefore reach the output in any order (results are sorted
-        // afterwards; only which ones a per-DM cap drops can vary).
-        if (all && lane == 0) {
-            for (int wi = warp; wi < nw; wi += kThreads / 32) {
-                if (((fw >> wi) & 1U) == 0U)
+                if (!__syncthreads_or(up)) {
+                    close_runs();
                     continue;
-                for (int wd = 0; wd < (CH / 32); ++wd) {
-                    uint32_t m = bits[wi * (CH / 32) + wd];
-                    while (m) {
-                        const int k = wd * 32 + __ffs(m) - 1;
-                        m &= m - 1;
-                        RunState r{};
-                        r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
-                        r.best_w = wi;
-                        r.start = r.best_t = r.last_t = rc.tile_t0 + c0 + k;
-                        emit(p, row, r, &local_count);
+                }
+            } else {
+                // ---- not steady (cold prefix, mask change, partial chunk): the
+                // bit masks from the general S/N
+                store_q();
+                __syncthreads();
+                for (int j = 0; j < (CH / kThreads); ++j) {
+                    const int k = threadIdx.x + j * kThreads;
+                    for (int wi = 0; wi < nw; ++wi) {
+                        const bool hit   = snr_general(p, rc, Q, c0, k, wi, row.delay) > p.thresh;
+                        const uint32_t m = __ballot_sync(0xFFFFFFFFU, hit);
+                        if (lane == 0) {
+                            bits[wi * (CH / 32) + j * (kThreads / 32) + warp] = m;
+                            if (m != 0U)
+                                atomicOr(&fired_w, 1U << wi);
+                        }
                     }
                 }
+                __syncthreads();
             }
-        } else if (!all && !across && lane == 0) {
-            for (int wi = warp; wi < nw; wi += kThreads / 32)
-                if (((fw >> wi) & 1U) != 0U || runs[wi].open)
-                    walk_runs<CH>(p, rc, Q, c0, row.delay, bits + wi * (CH / 32), wi, runs[wi], row,
-                              &local_count);
+            // bits now hold exactly the above-threshold samples of every width
+            const uint32_t fw = fired_w;
+            if (across) {
+                for (int wd = threadIdx.x; wd < (CH / 32); wd += kThreads) {
+                    uint32_t m = 0;
+                    for (int wi = 0; wi < nw; ++wi)
+                        if ((fw >> wi) & 1U)
+                            m |= bits[wi * (CH / 32) + wd];
+                    any_bits[wd] = m;
+                }
+                __syncthreads();
+            }
+            // Widths are independent (each has its own run state): lane 0 of
+            // warp w walks widths w, w + 8, ... Candidates of different widths
+            // may therefore reach the output in any order (results are sorted
+            // afterwards; only which ones a per-DM cap drops can vary).
+            if (all && lane == 0) {
+                for (int wi = warp; wi < nw; wi += kThreads / 32) {
+                    if (((fw >> wi) & 1U) == 0U)
+                        continue;
+                    for (int wd = 0; wd < (CH / 32); ++wd) {
+                        uint32_t m = bits[wi * (CH / 32) + wd];
+                        while (m) {
+                            const int k = wd * 32 + __ffs(m) - 1;
+                            m &= m - 1;
+                            RunState r{};
+                            r.best   = snr_general(p, rc, Q, c0, k, wi, row.delay);
+                            r.best_w = wi;
+                            r.start = r.best_t = r.last_t = rc.tile_t0 + c0 + k;
+                            emit(p, row, r, &local_count);
+                        }
+                    }
+                }
+            } else if (!all && !across && lane == 0) {
+                for (int wi = warp; wi < nw; wi += kThreads / 32)
+                    if (((fw >> wi) & 1U) != 0U || runs[wi].open)
+                        walk_runs<CH>(p, rc, Q, c0, row.delay, bits + wi * (CH / 32), wi, runs[wi], row,
+                                  &local_count);
+            }
+            if (across && threadIdx.x == 0 && (fw != 0U || runs[0].open))
+                walk_runs<CH>(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
+            __syncthreads();
         }
-        if (across && threadIdx.x == 0 && (fw != 0U || runs[0].open))
-            walk_runs<CH>(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
-        __syncthreads();
-    }
-    if (abort_flag) {
-        // a segment never landed: report it and let the copies in flight end
-        if (threadIdx.x == 0) {
-            atomicOr(p.err, 1U);
-            for (int j = ci; j < min(ci + 2, nchunks); ++j)
-                (void)bulk::mbar_wait(&bar[j & 1], static_cast<uint32_t>((j >> 1) & 1));
+        if (abort_flag) {
+            // a segment never landed: report it and let the copies in flight end
+            if (threadIdx.x == 0) {
+                atomicOr(p.err, 1U);
+                for (int j = ci; j < min(ci + 2, nchunks); ++j)
+                    (void)bulk::mbar_wait(&bar[(cc + j) & 1], static_cast<uint32_t>(((cc + j) >> 1) & 1));
+            }
+            return;
         }
-        return;
+        if (threadIdx.x < nruns && !all)
+            p.carry[g * nruns + threadIdx.x] = runs[threadIdx.x];
+        if (threadIdx.x == 0)
+            p.row_counts[g] = local_count;
+        cc += nchunks;
+        __syncthreads(); // the next row rewrites the row constants and run states
     }
-    if (threadIdx.x < nruns && !all)
-        p.carry[g * nruns + threadIdx.x] = runs[threadIdx.x];
-    if (threadIdx.x == 0)
-        p.row_counts[g] = local_count;
 }
 
 __global__ void k_flush(SearchParams p, int64_t nrows) {
@@ -821,7 +831,7 @@ __global__ void k_variance(const SearchRow* __restrict__ rows, const PlaneInfo* 
 } // namespace
 
 void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1, cudaStream_t s,
-                   int32_t chunk) {
+                   int32_t chunk, int32_t ctas) {
     if (g1 <= g0 || p.n_valid <= 0)
         return;
     if (chunk != 2048 && chunk != 4096)
@@ -842,11 +852,12 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
     const size_t nh   = static_cast<size_t>(p.halo) + p.halo / 4 + p.halo / per + 4;
     const size_t smem = sizeof(float) * ((4 + seg + 4) + (seg / 4 + 4) + seg / per + 2 * nh) +
                         sizeof(uint32_t) * search_bits_words(p.nwidths, chunk) + 2 * es * seg;
-    const dim3 grid(static_cast<unsigned>(g1 - g0));
+    const int64_t nrows = g1 - g0;
+    const dim3 grid(static_cast<unsigned>(ctas > 0 ? std::min<int64_t>(nrows, ctas) : nrows));
     auto go = [&](auto kernel, auto data) {
         FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-        kernel<<<grid, kThreads, smem, s>>>(p, data, level.pitch, level.base, g0);
+        kernel<<<grid, kThreads, smem, s>>>(p, data, level.pitch, level.base, g0, nrows);
     };
     if (level.fp16) {
         if (chunk == 2048)

@@ -85,9 +85,10 @@ struct SearchParams {
 /** Searches rows [g0, g1) (all in `level`) over the tile's valid columns,
  * `chunk` (2048 or 4096) samples per step of a CTA: the smaller chunk needs
  * half the shared memory and fewer registers, so more CTAs fit an SM, at
- * the cost of a larger halo share. */
+ * the cost of a larger halo share. `ctas` caps the launch's CTAs, each then
+ * looping over rows (0: one CTA per row). */
 void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1,
-                   cudaStream_t s, int32_t chunk = kSearchChunk);
+                   cudaStream_t s, int32_t chunk = kSearchChunk, int32_t ctas = 0);
 
 /** Exact variance of every searched row and width for `mask` and for
  * `mask_or`: var = sum over active channels of g[L_c][w]; writes

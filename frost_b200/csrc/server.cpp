@@ -324,6 +324,20 @@ std::vector<frost_giant> Server::drain_giants(uint32_t beam) {
     return out;
 }
 
+void Server::set_residency(uint32_t beam, int32_t ctas_per_sm) {
+    std::unique_lock<std::mutex> lk(m_mu);
+    Beam* b = hold(beam, lk);
+    lk.unlock();
+    try {
+        DeviceGuard g(m_device);
+        b->set_residency(ctas_per_sm);
+    } catch (...) {
+        release(beam);
+        throw;
+    }
+    release(beam);
+}
+
 void Server::set_postprocess(uint32_t beam, const frost_postprocess_config& cfg) {
     std::unique_lock<std::mutex> lk(m_mu);
     Beam* b = hold(beam, lk);

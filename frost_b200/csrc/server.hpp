@@ -41,6 +41,7 @@ public:
     /** Picks the engine's FDMT launch shape by measurement (cached per
      * geometry, so only the first beam of a shape pays). */
     void autotune() { m_engine->autotune(); }
+    void set_residency(int32_t ctas_per_sm) { m_engine->set_residency(ctas_per_sm); }
     /** Cleans and searches one gulp (a block of max_nsamps rows, nread
      * valid, on the host or on the beam's device). */
     void process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device);
@@ -101,6 +102,9 @@ public:
     std::vector<frost_giant> wait_giants(uint64_t ticket, double* latency_s);
     /** Attaches a post-processor to an idle beam; its device memory is
      * charged against the server's budget. */
+    /** Caps the beam's level and search kernels at `ctas_per_sm` resident
+     * CTAs per SM (fdmt::Engine::set_residency). */
+    void set_residency(uint32_t beam, int32_t ctas_per_sm);
     void set_postprocess(uint32_t beam, const frost_postprocess_config& cfg);
     /** drain() of a beam with a post-processor: the final giants. */
     std::vector<frost_giant> drain_giants(uint32_t beam);

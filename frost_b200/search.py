@@ -203,6 +203,17 @@ class FDMTBoxcar:
         check(lib().frost_search_set_launch_shape(self._h, 1 if fused else 0, int(tiles_per_cta), int(stages),
                                                   int(search_chunk)))
 
+    def set_residency(self, ctas_per_sm: int):
+        """Caps the level and search kernels at `ctas_per_sm` resident CTAs per
+        SM (0: one CTA per work item); leaves room on every SM for other
+        streams' kernels. Results do not depend on it."""
+        check(lib().frost_search_set_residency(self._h, int(ctas_per_sm)))
+
+    def residency(self) -> int:
+        v = C.c_int()
+        check(lib().frost_search_get_residency(self._h, C.byref(v)))
+        return v.value
+
     def use_graphs(self, enable: bool = True):
         """CUDA-graph replay of the per-gulp launch sequence (default on)."""
         check(lib().frost_search_use_graphs(self._h, 1 if enable else 0))

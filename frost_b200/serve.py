@@ -106,6 +106,12 @@ class BeamServer:
             self._beam_of.pop(ticket, None)
         return out[:n.value], lat.value
 
+    def set_residency(self, beam: int, ctas_per_sm: int) -> None:
+        """Caps the beam's level and search kernels at `ctas_per_sm` resident
+        CTAs per SM (0: one CTA per work item), so that the served beams'
+        kernels share the SMs instead of queueing behind each other."""
+        check(lib().frost_server_set_residency(self._h, beam, int(ctas_per_sm)))
+
     def set_postprocess(self, beam: int, cfg) -> None:
         """Adds CandidatePostprocessPlan (frost_b200.postprocess.SearchConfig)
         after every gulp's search of `beam`; wait_giants / drain_giants then

@@ -516,6 +516,16 @@ int frost_search_get_launch_shape(const frost_search* s,
  * budget. */
 int frost_search_set_launch_shape(frost_search* s, int fused, int tiles_per_cta, int stages, int search_chunk);
 
+/* No counterpart in the reference. Caps the engine's FDMT level and search
+ * kernels at `ctas_per_sm` resident CTAs per SM (0, the default: one CTA
+ * per work item, each launch filling the GPU). A capped launch loops over
+ * its work items and leaves the rest of every SM to kernels on other
+ * streams, which is what lets several beams' HBM-bound level passes and
+ * instruction-bound searches run side by side. Results do not depend on
+ * it. Waits for the engine's stream. */
+int frost_search_set_residency(frost_search* s, int ctas_per_sm);
+int frost_search_get_residency(const frost_search* s, int* ctas_per_sm);
+
 /* Enables (and zeroes) or disables per-phase timing. */
 int frost_search_enable_timing(frost_search* s, int enable);
 int frost_search_get_timing(const frost_search* s, frost_search_timing* out);
@@ -771,6 +781,10 @@ int frost_postprocess_destroy(frost_postprocess* p);
  * device memory is charged to the server budget (FROST_ERR_OUT_OF_MEMORY if
  * it does not fit). */
 int frost_server_set_postprocess(frost_server* s, uint32_t beam, const frost_postprocess_config* cfg);
+
+/* No counterpart in the reference. frost_search_set_residency for one
+ * served beam (between its gulps). */
+int frost_server_set_residency(frost_server* s, uint32_t beam, int ctas_per_sm);
 
 /* frost_server_wait for a beam with a post-processor: the gulp's giants
  * (its raw candidates are dropped). */

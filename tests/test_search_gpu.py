@@ -318,3 +318,31 @@ def test_every_launch_shape_gives_the_same_candidates(peak_mode):
         assert same_detections(ref[2048], ref[4096], bc.detect_thresh), storage
     with pytest.raises(ValueError):
         FDMTBoxcar(pc, BoxcarConfig(max_boxcar=16)).set_launch_shape(True, 16, 4, 1024)
+
+
+@pytest.mark.parametrize("storage", [Storage.FP32, Storage.FP16])
+def test_residency_caps_keep_the_candidates(storage):
+    """A residency cap (level and search kernels at a few CTAs per SM, each
+    looping over work items) changes which CTA does a row, not the
+    arithmetic: the candidates and the last gulp's planes are bit-identical
+    to the uncapped launches, for single and fused level steps."""
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=1, gulp=8192)
+    stream = make_stream(pc, 3, seed=95, pulses=PULSES)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0, storage=storage)
+    for fused in (True, False):
+        outs, planes = [], []
+        for cap in (0, 1, 3):
+            eng = FDMTBoxcar(pc, bc)
+            eng.set_launch_shape(fused, 4, 2 if fused else 0, 4096)
+            eng.set_residency(cap)
+            assert eng.residency() == cap
+            eng.capture_planes(True)
+            outs.append(run_engine(eng, stream, pc.block_nsamps, drain=False))
+            planes.append([eng.plane_data(p, pc.block_nsamps) for p in range(len(eng.get_search_plans()))])
+        assert outs[0].size > 0
+        for k in (1, 2):
+            assert np.array_equal(outs[k], outs[0]), (fused, k)
+            assert all(np.array_equal(a, b) for a, b in zip(planes[k], planes[0])), (fused, k)
+    with pytest.raises(ValueError):
+        FDMTBoxcar(pc, bc).set_residency(-1)
