@@ -723,14 +723,45 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
     FB_LAUNCH_CHECK();
 }
 
+namespace {
+// dst[r][0 .. w) = src[r][0 .. w) in 16-byte vectors, w vectors a row.
+__global__ void __launch_bounds__(256)
+    k_copy_rows16(uint4* __restrict__ dst, int64_t dpitch, const uint4* __restrict__ src, int64_t spitch,
+                  uint32_t w, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t r = i / w, c = i - r * w;
+        dst[r * dpitch + c] = src[r * spitch + c];
+    }
+}
+} // namespace
+
+void copy_rows(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t rows,
+               cudaStream_t s) {
+    if (rows == 0 || width == 0)
+        return;
+    const uintptr_t bits = reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src) | dpitch | spitch | width;
+    const size_t n = rows * (width / 16);
+    if (bits % 16 != 0 || n > 0x7FFFFFFFU) {
+        FB_CUDA(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    int dev = 0, sms = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    FB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t blocks = std::min<size_t>((n + 255) / 256, static_cast<size_t>(sms) * 8);
+    k_copy_rows16<<<static_cast<unsigned>(blocks), 256, 0, s>>>(
+        static_cast<uint4*>(dst), static_cast<int64_t>(dpitch / 16), static_cast<const uint4*>(src),
+        static_cast<int64_t>(spitch / 16), static_cast<uint32_t>(width / 16), static_cast<uint32_t>(n));
+    FB_LAUNCH_CHECK();
+}
+
 void launch_save_history(LevelView v, int64_t rows, int32_t hist, int32_t n_valid, void* hist_buf,
                          cudaStream_t s) {
     if (rows == 0 || hist == 0)
         return;
     const size_t es  = v.fp16 ? 2 : 4;
     const char* src  = static_cast<const char*>(v.data) + (v.base + n_valid - hist) * es;
-    FB_CUDA(cudaMemcpy2DAsync(hist_buf, hist * es, src, v.pitch * es, hist * es,
-                              static_cast<size_t>(rows), cudaMemcpyDeviceToDevice, s));
+    copy_rows(hist_buf, hist * es, src, v.pitch * es, hist * es, static_cast<size_t>(rows), s);
 }
 
 void launch_load_history(LevelView v, int64_t rows, int32_t hist, const void* hist_buf,
@@ -739,8 +770,7 @@ void launch_load_history(LevelView v, int64_t rows, int32_t hist, const void* hi
         return;
     const size_t es = v.fp16 ? 2 : 4;
     char* dst       = static_cast<char*>(v.data) + (v.base - hist) * es;
-    FB_CUDA(cudaMemcpy2DAsync(dst, v.pitch * es, hist_buf, hist * es, hist * es,
-                              static_cast<size_t>(rows), cudaMemcpyDeviceToDevice, s));
+    copy_rows(dst, v.pitch * es, hist_buf, hist * es, hist * es, static_cast<size_t>(rows), s);
 }
 
 void launch_save_input_history(const float* wf, int64_t pitch, int64_t t0, int32_t n_valid,

@@ -57,6 +57,12 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
                    unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t stages = 0,
                    int32_t ctas = 0);
 
+/** dst[r][0 .. width) = src[r][0 .. width) for `rows` rows of pitches
+ * dpitch / spitch bytes (device memory): 16-byte vectors when pointers,
+ * pitches and width allow, cudaMemcpy2DAsync otherwise. */
+void copy_rows(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t rows,
+               cudaStream_t s);
+
 /** Copies the last `hist` columns ending at column base + n_valid of every
  * row of `view` into hist_buf[rows][hist]. */
 void launch_save_history(LevelView view, int64_t rows, int32_t hist, int32_t n_valid,

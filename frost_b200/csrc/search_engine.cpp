@@ -243,6 +243,10 @@ void Engine::build_schedule(bool fuse) {
     }
     for (const auto& p : plan_planes)
         m_hist_len[p.height] = std::max(m_hist_len[p.height], m_plan.widths().back() - 1);
+    // whole 16-byte vectors of fp16 (and fp32) columns, so that the history
+    // copies move aligned vectors (a longer history is a superset)
+    for (int h = 1; h <= L; ++h)
+        m_hist_len[h] = static_cast<int32_t>(round_up(m_hist_len[h], 8));
     upload(m_fused_ops, fused_all, m_stream);
     m_fuse = fuse;
     if (m_graph != nullptr) {
@@ -541,6 +545,10 @@ SearchParams Engine::params(int64_t tile_off, int32_t n_valid) const {
     p.peak_mode    = m_cfg.peak_mode;
     p.trapezoid    = m_cfg.use_trapezoid ? 1 : 0;
     p.skip_cold    = m_cfg.skip_cold_prefix ? 1 : 0;
+    p.pow2_widths  = 1;
+    for (size_t w = 0; w < m_plan.widths().size(); ++w)
+        if (m_plan.widths()[w] != (int32_t{1} << std::min<size_t>(w, 30)))
+            p.pow2_widths = 0;
     p.clock        = m_clock.as<GulpClock>();
     p.tile_off     = tile_off;
     p.n_valid      = n_valid;

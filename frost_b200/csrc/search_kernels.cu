@@ -41,6 +41,8 @@ namespace {
 
 constexpr int kThreads   = 256;
 constexpr int kMaxWidths = 32;
+// widths 1, 2, ..., 2^15 take the unrolled steady-state tests
+constexpr int kMaxPow2Widths = 16;
 #define FB_NEG_INF (-__int_as_float(0x7f800000))
 #define FB_POS_INF (__int_as_float(0x7f800000))
 
@@ -333,6 +335,71 @@ __device__ __forceinline__ void group_lows(const float* gmin, int i0, bool two, 
     }
 }
 
+// The steady-state test of width 2^WI for the widths 1, 2, 4, ... (no
+// trapezoid): the same tests as the per-width table, with every offset and
+// alignment a compile-time constant (the halo is a multiple of 256, so the
+// window starts' group and block offsets depend on W alone).
+template <int P, int NG, int WI>
+__device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float pm2, const float (&gmx)[NG],
+                                           float bmax, const float* gmin, const float* tmin, int halo, float T) {
+    constexpr int W = 1 << WI;
+    if constexpr (W == 1) {
+        float m = q[0] - pm1;
+#pragma unroll
+        for (int e = 1; e < P; ++e)
+            m = fmaxf(m, q[e] - q[e - 1]);
+        return m > T;
+    } else if constexpr (W == 2) {
+        float m = fmaxf(q[0] - pm2, q[1] - pm1);
+#pragma unroll
+        for (int e = 2; e < P; ++e)
+            m = fmaxf(m, q[e] - q[e - 2]);
+        return m > T;
+    } else {
+        if constexpr (W >= 4 * P) {
+            // the thread's window starts are exactly block t - W / P
+            if (!(bmax - tmin[static_cast<int>(threadIdx.x) + halo / P - W / P] > T))
+                return false;
+        }
+        // own group g starts in group NG t + g + halo / 4 - W / 4, whose
+        // vector alignment R is fixed by W
+        constexpr int R = (NG - (W / 4) % NG) % NG;
+        const int i0    = NG * static_cast<int>(threadIdx.x) + halo / 4 - W / 4;
+        float lo[NG];
+        if constexpr (NG == 4) {
+            const float4* v = reinterpret_cast<const float4*>(gmin + (i0 - R));
+            const float4 a  = v[0];
+            const float4 b  = R != 0 ? v[1] : a;
+            const float e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            pick_lows<R, 4, 8>(e, false, lo);
+        } else {
+            const float2* v = reinterpret_cast<const float2*>(gmin + (i0 - R));
+            const float2 a  = v[0];
+            const float2 b  = R != 0 ? v[1] : a;
+            const float e[4] = {a.x, a.y, b.x, b.y};
+            pick_lows<R, 2, 4>(e, false, lo);
+        }
+        float m = gmx[0] - lo[0];
+#pragma unroll
+        for (int g = 1; g < NG; ++g)
+            m = fmaxf(m, gmx[g] - lo[g]);
+        return m > T;
+    }
+}
+
+template <int P, int NG, int WI>
+__device__ __forceinline__ void pow2_all(uint32_t& cand, int nw, const float (&q)[P], float pm1, float pm2,
+                                         const float (&gmx)[NG], float bmax, const float* gmin,
+                                         const float* tmin, int halo, const WidthTest* wt) {
+    if constexpr (WI < kMaxPow2Widths) {
+        if (WI < nw) {
+            if (pow2_maybe<P, NG, WI>(q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt[WI].T))
+                cand |= 1U << WI;
+            pow2_all<P, NG, WI + 1>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt);
+        }
+    }
+}
+
 // Q[-halo .. -1] straight from the staged halo columns: a prefix sum from
 // the first column a window can reach (earlier columns count 0), rebased so
 // that Q[-1] = 0, and the halo's entries of gmin (per 4 columns) and tmin
@@ -359,7 +426,7 @@ __device__ void scan_halo(const S* seg, int halo, int jmin, float* Q, float* gmi
         H[i] -= last;
 }
 
-template <class S, int CH>
+template <class S, int CH, bool POW2>
 __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0,
              int64_t nrows) {
@@ -490,11 +557,11 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             // warp (shuffles), then across warps (one offset per warp)
             float q[P];
             ld_cols<S, P>(seg + halo + P * threadIdx.x, q);
-    #pragma unroll
+#pragma unroll
             for (int e = 1; e < P; ++e)
                 q[e] += q[e - 1];
             float incl = q[P - 1];
-    #pragma unroll
+#pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const float u = __shfl_up_sync(0xFFFFFFFFU, incl, o);
                 if (lane >= o)
@@ -513,18 +580,18 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             for (int w = 0; w < warp; ++w)
                 woff += warp_tot[w];
             const float off = excl + woff;
-    #pragma unroll
+#pragma unroll
             for (int e = 0; e < P; ++e)
                 q[e] += off;
             // ---- group and block extremes (registers; the minima to shared memory)
             float gmx[NG], gmn[NG];
-    #pragma unroll
+#pragma unroll
             for (int gq = 0; gq < NG; ++gq) {
                 gmx[gq] = fmaxf(fmaxf(q[4 * gq], q[4 * gq + 1]), fmaxf(q[4 * gq + 2], q[4 * gq + 3]));
                 gmn[gq] = fminf(fminf(q[4 * gq], q[4 * gq + 1]), fminf(q[4 * gq + 2], q[4 * gq + 3]));
             }
             float bmax = gmx[0], bmin = gmn[0];
-    #pragma unroll
+#pragma unroll
             for (int gq = 1; gq < NG; ++gq) {
                 bmax = fmaxf(bmax, gmx[gq]);
                 bmin = fminf(bmin, gmn[gq]);
@@ -544,10 +611,10 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                 const int tt = static_cast<int>(threadIdx.x) - (kThreads - halo / P);
                 if (tt >= 0) {
                     float4* d = reinterpret_cast<float4*>(nh + P * tt);
-    #pragma unroll
+#pragma unroll
                     for (int i = 0; i < P / 4; ++i)
                         d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
-    #pragma unroll
+#pragma unroll
                     for (int gq = 0; gq < NG; ++gq)
                         nh[halo + NG * tt + gq] = gmn[gq];
                     nh[halo + halo / 4 + tt] = bmin;
@@ -574,7 +641,7 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
 
             auto store_q = [&]() {
                 float4* d = reinterpret_cast<float4*>(Q + P * threadIdx.x);
-    #pragma unroll
+#pragma unroll
                 for (int i = 0; i < P / 4; ++i)
                     d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
                 for (int i = threadIdx.x; i < nw * (CH / 32); i += kThreads)
@@ -599,43 +666,47 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                     pm2 = warp == 0 ? Q[-2] : wtail[warp - 1][0];
                 }
                 uint32_t cand = 0U;
-                for (int wi = 0; wi < nw; ++wi) {
-                    const WidthTest t = wt[wi];
-                    bool maybe        = true;
-                    if (t.kind == kTestExact) {
-                        float m;
-                        if (t.W == 1) {
-                            m = q[0] - pm1;
-    #pragma unroll
-                            for (int e = 1; e < P; ++e)
-                                m = fmaxf(m, q[e] - q[e - 1]);
-                        } else {
-                            m = fmaxf(q[0] - pm2, q[1] - pm1);
-    #pragma unroll
-                            for (int e = 2; e < P; ++e)
-                                m = fmaxf(m, q[e] - q[e - 2]);
-                        }
-                        maybe = m > t.T;
-                    } else if (t.kind != kTestAll) {
-                        if (t.kind == kTestBlock) {
-                            const int b = static_cast<int>(threadIdx.x) + t.bconst;
-                            float lo    = tmin[b];
-                            if (t.btwo)
-                                lo = fminf(lo, tmin[b + 1]);
-                            maybe = bmax - lo > t.T;
-                        }
-                        if (maybe) {
-                            float lo[NG];
-                            group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
-                            float m = gmx[0] - lo[0];
-    #pragma unroll
-                            for (int gq = 1; gq < NG; ++gq)
-                                m = fmaxf(m, gmx[gq] - lo[gq]);
+                if constexpr (POW2)
+                    pow2_all<P, NG, 0>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt);
+                else {
+                    for (int wi = 0; wi < nw; ++wi) {
+                        const WidthTest t = wt[wi];
+                        bool maybe        = true;
+                        if (t.kind == kTestExact) {
+                            float m;
+                            if (t.W == 1) {
+                                m = q[0] - pm1;
+#pragma unroll
+                                for (int e = 1; e < P; ++e)
+                                    m = fmaxf(m, q[e] - q[e - 1]);
+                            } else {
+                                m = fmaxf(q[0] - pm2, q[1] - pm1);
+#pragma unroll
+                                for (int e = 2; e < P; ++e)
+                                    m = fmaxf(m, q[e] - q[e - 2]);
+                            }
                             maybe = m > t.T;
+                        } else if (t.kind != kTestAll) {
+                            if (t.kind == kTestBlock) {
+                                const int b = static_cast<int>(threadIdx.x) + t.bconst;
+                                float lo    = tmin[b];
+                                if (t.btwo)
+                                    lo = fminf(lo, tmin[b + 1]);
+                                maybe = bmax - lo > t.T;
+                            }
+                            if (maybe) {
+                                float lo[NG];
+                                group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
+                                float m = gmx[0] - lo[0];
+#pragma unroll
+                                for (int gq = 1; gq < NG; ++gq)
+                                    m = fmaxf(m, gmx[gq] - lo[gq]);
+                                maybe = m > t.T;
+                            }
                         }
+                        if (maybe)
+                            cand |= 1U << wi;
                     }
-                    if (maybe)
-                        cand |= 1U << wi;
                 }
                 if (!__syncthreads_or(cand != 0U)) {
                     close_runs();
@@ -679,12 +750,12 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                     if (t.kind == kTestGroup || t.kind == kTestBlock) {
                         float lo[NG];
                         group_lows<NG>(gmin, NG * static_cast<int>(threadIdx.x) + t.gconst, t.two != 0, lo);
-    #pragma unroll
+#pragma unroll
                         for (int gq = 0; gq < NG; ++gq)
                             if (gmx[gq] - lo[gq] > t.T)
                                 exact(NG * static_cast<int>(threadIdx.x) + gq, wi, t.W, E, t.T);
                     } else {
-    #pragma unroll
+#pragma unroll
                         for (int gq = 0; gq < NG; ++gq)
                             exact(NG * static_cast<int>(threadIdx.x) + gq, wi, t.W, E, t.T);
                     }
@@ -859,17 +930,19 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
                                      static_cast<int>(smem)));
         kernel<<<grid, kThreads, smem, s>>>(p, data, level.pitch, level.base, g0, nrows);
     };
-    if (level.fp16) {
+    // widths 1, 2, 4, ... (no trapezoid): the unrolled steady-state tests
+    const bool pow2 = p.pow2_widths != 0 && !p.trapezoid && p.nwidths <= kMaxPow2Widths;
+    auto typed = [&](auto tag, const auto* data) {
+        using S = decltype(tag);
         if (chunk == 2048)
-            go(k_search<__half, 2048>, static_cast<const __half*>(level.data));
+            pow2 ? go(k_search<S, 2048, true>, data) : go(k_search<S, 2048, false>, data);
         else
-            go(k_search<__half, 4096>, static_cast<const __half*>(level.data));
-    } else {
-        if (chunk == 2048)
-            go(k_search<float, 2048>, static_cast<const float*>(level.data));
-        else
-            go(k_search<float, 4096>, static_cast<const float*>(level.data));
-    }
+            pow2 ? go(k_search<S, 4096, true>, data) : go(k_search<S, 4096, false>, data);
+    };
+    if (level.fp16)
+        typed(__half{}, static_cast<const __half*>(level.data));
+    else
+        typed(float{}, static_cast<const float*>(level.data));
     FB_LAUNCH_CHECK();
 }
 

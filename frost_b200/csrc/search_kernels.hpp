@@ -67,6 +67,7 @@ struct SearchParams {
     int32_t peak_mode;       // enum frost_peak_mode
     int32_t trapezoid;
     int32_t skip_cold;
+    int32_t pow2_widths;     // the widths are 1, 2, 4, ... (read by the launcher)
     const GulpClock* clock;  // gulp start and mask change (device)
     int64_t tile_off;        // tile column 0 relative to the gulp start
     int32_t n_valid;         // valid columns in this tile

@@ -346,3 +346,22 @@ def test_residency_caps_keep_the_candidates(storage):
             assert all(np.array_equal(a, b) for a, b in zip(planes[k], planes[0])), (fused, k)
     with pytest.raises(ValueError):
         FDMTBoxcar(pc, bc).set_residency(-1)
+
+
+def test_uneven_widths_match_oracle():
+    """Widths that are not powers of two (wtsp 1.5: 1, 2, 3, 5, ..., 93)
+    take the table-driven steady-state tests (window starts straddling two
+    4-sample groups, per-thread bounds for the widest): identical candidate
+    indices and S/N within 1e-3 of the oracle."""
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=1, gulp=8192)
+    bc = BoxcarConfig(max_boxcar=100, wtsp=1.5, detect_thresh=6.0)
+    stream = make_stream(pc, 3, seed=97, pulses=PULSES)
+    eng = FDMTBoxcar(pc, bc)
+    cands = run_engine(eng, stream, pc.block_nsamps)
+    widths = sorted(set(int(w) for w in cands["width"]))
+    assert any(w % 2 == 1 and w > 2 for w in widths), widths
+    ref = oracle_for(pc, bc).search(stream, pc.block_nsamps, [np.ones(pc.nchans, np.uint8)] * 3)
+    n, missing, extra, bad = compare(cands, ref, bc.detect_thresh)
+    assert n > 10
+    assert not missing and not extra and not bad, (missing[:5], extra[:5], bad[:5])
