@@ -313,3 +313,15 @@ class PrefetchStatsC(C.Structure):
 
 
 READ_FN = C.CFUNCTYPE(C.c_long, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
+
+
+class MemoryEstimateC(C.Structure):
+    _fields_ = [("rfi_bytes", C.c_uint64), ("fdmt_bytes", C.c_uint64), ("search_bytes", C.c_uint64),
+                ("postprocess_bytes", C.c_uint64), ("transient_bytes", C.c_uint64), ("total_bytes", C.c_uint64),
+                ("max_delay", C.c_uint64)]
+
+
+class MemoryCheckC(C.Structure):
+    _fields_ = [("estimate", MemoryEstimateC), ("requested_bytes", C.c_uint64), ("available_bytes", C.c_uint64),
+                ("gulp_requested", C.c_uint64), ("gulp_used", C.c_uint64), ("lowered", C.c_int32),
+                ("device_memory", C.c_int32)]

@@ -100,6 +100,13 @@ SIGNATURES = {
     "frost_prefetch_create_memory": (C.c_int, [_vp, _sz, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]),
     "frost_prefetch_next": (C.c_int, [_vp, _vp, C.POINTER(_vp), C.POINTER(_sz)]),
     "frost_prefetch_get_stats": (C.c_int, [_vp, C.POINTER(_abi.PrefetchStatsC)]),
+    "frost_estimate_memory": (C.c_int, [C.POINTER(_abi.RfiConfigC), C.POINTER(_abi.BlockLayoutC), C.c_float,
+                                        C.POINTER(_abi.DedispPlanConfigC), C.POINTER(_abi.BoxcarConfigC),
+                                        C.POINTER(_abi.PostprocessConfigC), C.POINTER(_abi.MemoryEstimateC)]),
+    "frost_check_memory": (C.c_int, [C.POINTER(_abi.RfiConfigC), C.POINTER(_abi.BlockLayoutC), C.c_float,
+                                     C.POINTER(_abi.DedispPlanConfigC), C.POINTER(_abi.BoxcarConfigC),
+                                     C.POINTER(_abi.PostprocessConfigC), C.c_int, C.c_uint64, C.c_uint64, C.c_int,
+                                     C.POINTER(_abi.MemoryCheckC)]),
     "frost_prefetch_destroy": (C.c_int, [_vp]),
     "frost_postprocess_create": (C.c_int, [C.POINTER(_abi.PostprocessConfigC), C.POINTER(_abi.PostprocessLayoutC),
                                            C.c_int, C.POINTER(_vp)]),

@@ -14,6 +14,7 @@
 #include "dedisp.hpp"
 #include "host_stats.hpp"
 #include "cand_writer.hpp"
+#include "memory_plan.hpp"
 #include "postprocess.hpp"
 #include "prefetch.hpp"
 #include "pp_math.cuh"
@@ -983,6 +984,28 @@ int frost_cand_filename(int64_t utc, uint64_t beam, char* out, size_t capacity) 
         if (s.size() + 1 > capacity)
             invalid("frost_cand_filename: output holds too few characters");
         std::memcpy(out, s.c_str(), s.size() + 1);
+    });
+}
+
+int frost_estimate_memory(const frost_rfi_config* rfi, const frost_block_layout* layout, float baseline_length,
+                          const frost_dedisp_plan_config* plan, const frost_boxcar_config* search,
+                          const frost_postprocess_config* post, frost_memory_estimate* out) {
+    return guarded([&] {
+        if (rfi == nullptr || layout == nullptr || plan == nullptr || search == nullptr || out == nullptr)
+            invalid("frost_estimate_memory: null argument");
+        *out = fb::memplan::estimate(*rfi, *layout, baseline_length, *plan, *search, post);
+    });
+}
+
+int frost_check_memory(const frost_rfi_config* rfi, frost_block_layout* layout, float baseline_length,
+                       frost_dedisp_plan_config* plan, const frost_boxcar_config* search,
+                       const frost_postprocess_config* post, int gulp_is_default, uint64_t available_bytes,
+                       uint64_t memory_limit_bytes, int device, frost_memory_check* out) {
+    return guarded([&] {
+        if (rfi == nullptr || layout == nullptr || plan == nullptr || search == nullptr || out == nullptr)
+            invalid("frost_check_memory: null argument");
+        *out = fb::memplan::check(*rfi, *layout, baseline_length, *plan, *search, post, gulp_is_default != 0,
+                                  available_bytes, memory_limit_bytes, device);
     });
 }
 

@@ -296,6 +296,44 @@ SizeType Cleaner::memory_usage() const {
     return total;
 }
 
+SizeType Cleaner::estimate_memory(const frost_rfi_config& cfg, const frost_block_layout& layout,
+                                  float baseline_length) {
+    Config conf = Config::from(cfg);
+    conf.validate();
+    validate_layout(layout, baseline_length);
+    const auto& c         = conf.c;
+    const SizeType n      = layout.nchans;
+    const SizeType T      = layout.max_nsamps;
+    const SizeType row    = n * static_cast<SizeType>(bits_of(layout.dtype)) / 8;
+    const SizeType window = std::max(static_cast<SizeType>(static_cast<double>(baseline_length) / layout.tsamp),
+                                     SizeType{kMinWindow});
+    const SizeType nwin   = std::max<SizeType>(T / window, 1);
+    const SizeType nck    = std::clamp<SizeType>((T + kMinChunkRows - 1) / kMinChunkRows, 1, kMaxChunks) * n;
+    const bool moments    = c.moments_enabled || c.iqrm_enabled || c.kadane_channel_enabled;
+    const bool zdot       = c.zero_dm == FROST_ZERO_DM_ZDOT;
+    const bool kchan      = c.kadane_channel_enabled != 0;
+    const SizeType T1     = std::max<SizeType>(T, 1);
+    const SizeType f      = sizeof(float);
+    SizeType total        = 0;
+    // ensure_capacity(T, T): raw block, float work and output, per-window
+    // statistics, tails, counters
+    total += std::max<SizeType>(T * row, 16) + 2 * std::max<SizeType>(T * n * f, 16);
+    total += 5 * nwin * n * f + 4 * n * f + kCountSlots * sizeof(unsigned long long) + sizeof(unsigned long long);
+    // reserve_phase_buffers
+    total += nwin * kMaxBandpassRows * n * f + n * sizeof(uint32_t);
+    total += (moments ? nwin * n * sizeof(MomentSums) : 0) + 2 * std::max<SizeType>(moments ? nwin * n * f : 0, f);
+    total += T * (f + sizeof(double) + f + f) + 2 * T1 * sizeof(Span32) + 2 * T1;
+    total += 2 * nck * f + std::max<SizeType>(zdot ? nck : 1, 1) * sizeof(ZdotSums) +
+             2 * std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState);
+    total += 2 * n * f + n * sizeof(ZdotSums) + 2 * n * sizeof(Run);
+    // tables uploaded per gulp: masks, good-channel prefix, zero-DM fit,
+    // Kadane segments, flagged samples (at most every sample), Welford
+    // reciprocals
+    total += 2 * n + (n + 1) * sizeof(uint64_t) + 2 * n * f + 2 * (kchan ? n : 1) * sizeof(Segment) + n;
+    total += T1 * sizeof(uint64_t) + (T + 1) * sizeof(double);
+    return total;
+}
+
 Dims Cleaner::dims(SizeType nsamps, int dtype) const {
     Dims d{};
     d.dtype     = dtype;

@@ -58,6 +58,13 @@ public:
     int device() const { return m_device; }
     cudaStream_t stream() const { return m_stream; }
     SizeType memory_usage() const;
+    /** Device bytes a cleaner for (cfg, layout) holds once its whole-block
+     * buffers are in place (preallocate, then any gulp), computed on the
+     * host without allocating: the buffers sized by data (flagged samples,
+     * Kadane segments) at their largest. RFICleaner::estimate_memory
+     * (include/frost/prepare/rfi.hpp) for the device path. */
+    static SizeType estimate_memory(const frost_rfi_config& cfg, const frost_block_layout& layout,
+                                    float baseline_length);
     /** Allocates every device buffer a full block of max_nsamps rows needs,
      * so memory_usage() is the cleaner's steady-state footprint. */
     void preallocate();

@@ -46,21 +46,7 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
                const uint8_t* kill_mask, SizeType memory_budget, int device)
     : m_plan(plan_config(dd, bc)), m_cfg(bc), m_device(device),
       m_fp16(bc.storage == FROST_STORAGE_FP16) {
-    if (bc.storage != FROST_STORAGE_FP32 && bc.storage != FROST_STORAGE_FP16)
-        invalid("search: storage must be fp32 or fp16");
-    if (bc.peak_mode < FROST_PEAK_PER_WIDTH || bc.peak_mode > FROST_PEAK_ALL)
-        invalid("search: invalid peak_mode");
-    if (!is_finite(bc.detect_thresh))
-        invalid("search: detect_thresh must be finite");
-    if (!(bc.noise_sigma == 1.0F) || bc.input_nbits != 32 || !(bc.input_mean == 0.0F))
-        invalid("search: the engine takes calibrated float32 input (noise_sigma 1, "
-                "input_nbits 32, input_mean 0)");
-    if (m_plan.widths().size() > 32)
-        invalid("search: more than 32 boxcar widths (raise wtsp)");
-    if (dd.block_nsamps <= static_cast<uint64_t>(m_plan.dt_max()) + bc.max_boxcar)
-        invalid("nsamps_gulp must exceed the dedispersion max_delay (" +
-                std::to_string(m_plan.dt_max()) + ") plus boxcar_max (" +
-                std::to_string(bc.max_boxcar) + ")");
+    validate(dd, bc, m_plan);
     int ndev = 0;
     FB_CUDA(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev)
@@ -174,8 +160,6 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     // Tile length: the whole gulp unless the budget (or the device) is short.
     int64_t tile = bc.tile_nsamps != 0 ? static_cast<int64_t>(bc.tile_nsamps)
                                        : static_cast<int64_t>(dd.block_nsamps);
-    if (bc.tile_nsamps != 0 && bc.tile_nsamps % kTileQuantum != 0)
-        invalid("search: tile_nsamps must be a multiple of 4096");
     tile = round_up(std::min<int64_t>(tile, static_cast<int64_t>(dd.block_nsamps)), kTileQuantum);
     size_t free_b = 0, total_b = 0;
     FB_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -195,27 +179,117 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
 // stored; with `fuse`, a level whose successor is not stored is computed
 // straight from the one below its predecessor (two levels in one pass,
 // halving that pair's HBM traffic).
-void Engine::build_schedule(bool fuse) {
-    const int L             = m_plan.levels();
-    const auto& plan_planes = m_plan.planes();
+void Engine::validate(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc, const Plan& plan) {
+    if (bc.storage != FROST_STORAGE_FP32 && bc.storage != FROST_STORAGE_FP16)
+        invalid("search: storage must be fp32 or fp16");
+    if (bc.peak_mode < FROST_PEAK_PER_WIDTH || bc.peak_mode > FROST_PEAK_ALL)
+        invalid("search: invalid peak_mode");
+    if (!is_finite(bc.detect_thresh))
+        invalid("search: detect_thresh must be finite");
+    if (!(bc.noise_sigma == 1.0F) || bc.input_nbits != 32 || !(bc.input_mean == 0.0F))
+        invalid("search: the engine takes calibrated float32 input (noise_sigma 1, "
+                "input_nbits 32, input_mean 0)");
+    if (plan.widths().size() > 32)
+        invalid("search: more than 32 boxcar widths (raise wtsp)");
+    if (dd.block_nsamps <= static_cast<uint64_t>(plan.dt_max()) + bc.max_boxcar)
+        invalid("nsamps_gulp must exceed the dedispersion max_delay (" + std::to_string(plan.dt_max()) +
+                ") plus boxcar_max (" + std::to_string(bc.max_boxcar) + ")");
+    if (bc.tile_nsamps != 0 && bc.tile_nsamps % kTileQuantum != 0)
+        invalid("search: tile_nsamps must be a multiple of 4096");
+}
+
+Engine::Footprint Engine::estimate(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc) {
+    const Plan plan(plan_config(dd, bc));
+    validate(dd, bc, plan);
+    // The allocations of the constructor, allocate() for the configured tile
+    // under both schedules autotune may try (buffers only grow), and
+    // autotune's zero waterfall; every buffer at least 16 bytes.
+    auto b16 = [](SizeType bytes) { return std::max<SizeType>(bytes, 16); };
+    const SizeType es   = bc.storage == FROST_STORAGE_FP16 ? 2 : 4;
+    const int L         = plan.levels();
+    const int32_t C     = plan.nchans();
+    const auto& widths  = plan.widths();
+    const SizeType nw   = widths.size();
+    Footprint f;
+    // tables
+    const auto& leaf = plan.leaf_ops();
+    SizeType nodes   = leaf.empty() ? 0 : 1;
+    for (size_t i = 1; i < leaf.size(); ++i)
+        if (leaf[i].chan_lo != leaf[i - 1].chan_lo || leaf[i].chan_hi != leaf[i - 1].chan_hi)
+            ++nodes;
+    SizeType nrow_ops = 0;
+    std::vector<int64_t> row_op_offset(L + 2, 0);
+    for (int h = 2; h <= L; ++h) {
+        row_op_offset[h] = static_cast<int64_t>(nrow_ops);
+        nrow_ops += plan.row_ops(h).size();
+    }
+    SizeType nsearch = 0, nleaf = 0;
+    std::vector<char> searched(L + 1, 0);
+    for (const auto& p : plan.planes()) {
+        nsearch += p.delay.size();
+        nleaf += p.delay.size() * static_cast<SizeType>(p.chan_end - p.chan_begin);
+        searched[p.height] = 1;
+    }
+    const SizeType nruns = bc.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : nw;
+    f.table_bytes = b16(leaf.size() * sizeof(LeafOp)) + b16((nodes + 1) * sizeof(int32_t)) +
+                    b16(nrow_ops * sizeof(RowOp)) + b16(nsearch * sizeof(SearchRow)) +
+                    b16(plan.planes().size() * sizeof(PlaneInfo)) + b16(nleaf * sizeof(uint16_t)) +
+                    b16(nsearch * sizeof(int64_t)) + b16(nw * sizeof(int32_t)) +
+                    b16((static_cast<SizeType>(plan.max_leaf_length()) + 1) * nw * sizeof(double)) +
+                    nsearch * nw * (sizeof(double) + 2 * sizeof(float)) + b16(nsearch * nruns * sizeof(RunState)) +
+                    b16(nsearch * sizeof(uint32_t)) + 4 * sizeof(unsigned long long) + sizeof(GulpClock) +
+                    sizeof(unsigned long long) + 2 * static_cast<SizeType>(C);
+    f.candidate_bytes = std::max<SizeType>(bc.max_candidates, 1) * sizeof(frost_candidate);
+    // level buffers and histories of the fused and single-level schedules
+    int64_t tile = bc.tile_nsamps != 0 ? static_cast<int64_t>(bc.tile_nsamps) : static_cast<int64_t>(dd.block_nsamps);
+    tile                = round_up(std::min<int64_t>(tile, static_cast<int64_t>(dd.block_nsamps)), kTileQuantum);
+    const int64_t ncols = round_up(tile, kTileQuantum);
+    const int32_t halo  = search_halo(widths.back());
+    SizeType buf[2] = {16, 16}, hist = 0, fused = 16;
+    for (const bool fuse : {true, false}) {
+        const Schedule sc = make_schedule(plan, row_op_offset, fuse);
+        SizeType h_bytes  = 0;
+        for (int h = 1; h <= L; ++h) {
+            h_bytes += b16(static_cast<SizeType>(plan.level_rows(h)) * sc.hist_len[h] * es);
+            if (sc.buf_of[h] < 0)
+                continue;
+            const int64_t need = searched[h] ? std::max<int64_t>(sc.hist_len[h], halo) : sc.hist_len[h];
+            const SizeType base = static_cast<SizeType>(round_up(need, 8));
+            buf[sc.buf_of[h]] = std::max<SizeType>(buf[sc.buf_of[h]],
+                                                   static_cast<SizeType>(plan.level_rows(h)) * (base + ncols) * es);
+        }
+        hist  = std::max(hist, h_bytes);
+        fused = std::max<SizeType>(fused, sc.fused.size() * sizeof(FusedOp));
+    }
+    const SizeType in_hist = b16(static_cast<SizeType>(C) * plan.level_history(0) * sizeof(float));
+    f.table_bytes += fused;
+    f.level_bytes     = buf[0] + buf[1];
+    f.history_bytes   = hist + 2 * in_hist;
+    f.transient_bytes = static_cast<SizeType>(C) * std::min<SizeType>(dd.block_nsamps, 4096) * sizeof(float);
+    f.dt_max          = plan.dt_max();
+    return f;
+}
+
+Engine::Schedule Engine::make_schedule(const Plan& plan, const std::vector<int64_t>& row_op_offset, bool fuse) {
+    const int L             = plan.levels();
+    const auto& plan_planes = plan.planes();
     std::vector<char> keep(L + 1, 0);
     keep[1] = 1;
     keep[L] = 1;
     for (const auto& p : plan_planes)
         keep[p.height] = 1;
-    m_steps.clear();
-    m_buf_of.assign(L + 1, -1);
-    m_hist_len.assign(L + 1, 0);
-    m_hist_len[0] = m_plan.level_history(0);
-    m_steps.push_back({1, 0, false, 0});
-    m_buf_of[1] = 0;
-    std::vector<FusedOp> fused_all;
+    Schedule sc;
+    sc.buf_of.assign(L + 1, -1);
+    sc.hist_len.assign(L + 1, 0);
+    sc.hist_len[0] = plan.level_history(0);
+    sc.steps.push_back({1, 0, false, 0});
+    sc.buf_of[1] = 0;
     for (int h = 1; h < L;) {
         Step st{};
         if (fuse && h + 2 <= L && !keep[h + 1]) {
-            st = {h + 2, h, true, static_cast<int64_t>(fused_all.size())};
-            const auto& mid = m_plan.row_ops(h + 1);
-            for (const RowOp& op : m_plan.row_ops(h + 2)) {
+            st = {h + 2, h, true, static_cast<int64_t>(sc.fused.size())};
+            const auto& mid = plan.row_ops(h + 1);
+            for (const RowOp& op : plan.row_ops(h + 2)) {
                 const RowOp& a = mid[op.lo_row];
                 FusedOp f{{a.lo_row, a.hi_row, -1, -1}, {0, a.hi_row >= 0 ? a.shift : 0, 0, 0}};
                 if (op.hi_row >= 0) {
@@ -227,27 +301,35 @@ void Engine::build_schedule(bool fuse) {
                 }
                 for (int j = 1; j < 4; ++j)
                     if (f.row[j] >= 0)
-                        m_hist_len[h] = std::max(m_hist_len[h], f.shift[j]);
-                fused_all.push_back(f);
+                        sc.hist_len[h] = std::max(sc.hist_len[h], f.shift[j]);
+                sc.fused.push_back(f);
             }
             h += 2;
         } else {
-            st = {h + 1, h, false, m_row_op_offset[h + 1]};
-            for (const RowOp& op : m_plan.row_ops(h + 1))
+            st = {h + 1, h, false, row_op_offset[h + 1]};
+            for (const RowOp& op : plan.row_ops(h + 1))
                 if (op.hi_row >= 0)
-                    m_hist_len[h] = std::max(m_hist_len[h], op.shift);
+                    sc.hist_len[h] = std::max(sc.hist_len[h], op.shift);
             h += 1;
         }
-        m_buf_of[st.out] = static_cast<int>(m_steps.size() % 2);
-        m_steps.push_back(st);
+        sc.buf_of[st.out] = static_cast<int>(sc.steps.size() % 2);
+        sc.steps.push_back(st);
     }
     for (const auto& p : plan_planes)
-        m_hist_len[p.height] = std::max(m_hist_len[p.height], m_plan.widths().back() - 1);
+        sc.hist_len[p.height] = std::max(sc.hist_len[p.height], plan.widths().back() - 1);
     // whole 16-byte vectors of fp16 (and fp32) columns, so that the history
     // copies move aligned vectors (a longer history is a superset)
     for (int h = 1; h <= L; ++h)
-        m_hist_len[h] = static_cast<int32_t>(round_up(m_hist_len[h], 8));
-    upload(m_fused_ops, fused_all, m_stream);
+        sc.hist_len[h] = static_cast<int32_t>(round_up(sc.hist_len[h], 8));
+    return sc;
+}
+
+void Engine::build_schedule(bool fuse) {
+    Schedule sc = make_schedule(m_plan, m_row_op_offset, fuse);
+    m_steps     = std::move(sc.steps);
+    m_buf_of    = std::move(sc.buf_of);
+    m_hist_len  = std::move(sc.hist_len);
+    upload(m_fused_ops, sc.fused, m_stream);
     m_fuse = fuse;
     if (m_graph != nullptr) {
         cudaGraphExecDestroy(m_graph);
@@ -517,10 +599,10 @@ SizeType Engine::device_bytes() const {
     for (const auto& b : m_hist)
         total += b.bytes();
     const DeviceBuffer* rest[] = {&m_in_hist, &m_in_scratch, &m_wf_stage, &m_leaf_ops,
-                                  &m_node_first_op_d, &m_row_ops, &m_rows, &m_planes, &m_widths,
-                                  &m_leaf_len, &m_leaf_offset, &m_gtab, &m_var, &m_inv, &m_inv_or,
-                                  &m_mask_d, &m_mask_or_d, &m_carry, &m_row_counts, &m_cands,
-                                  &m_counters, &m_frontier, &m_capture_rows};
+                                  &m_node_first_op_d, &m_row_ops, &m_fused_ops, &m_rows, &m_planes,
+                                  &m_widths, &m_leaf_len, &m_leaf_offset, &m_gtab, &m_var, &m_inv,
+                                  &m_inv_or, &m_mask_d, &m_mask_or_d, &m_carry, &m_row_counts, &m_cands,
+                                  &m_counters, &m_clock, &m_frontier, &m_capture_rows};
     for (const auto* b : rest)
         total += b->bytes();
     for (const auto& b : m_capture)

@@ -97,6 +97,16 @@ private:
     std::vector<Step> m_steps;
     std::vector<int> m_buf_of;         // level -> level buffer (-1: not stored)
     std::vector<int32_t> m_hist_len;   // level -> history columns kept
+    struct Schedule {
+        std::vector<Step> steps;
+        std::vector<int> buf_of;
+        std::vector<int32_t> hist_len;
+        std::vector<FusedOp> fused;
+    };
+    /** The FDMT schedule of `plan` (host only): steps, the buffer of every
+     * stored level, history lengths and the fused ops. */
+    static Schedule make_schedule(const Plan& plan, const std::vector<int64_t>& row_op_offset, bool fuse);
+    static void validate(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc, const Plan& plan);
     DeviceBuffer m_fused_ops;
     bool m_fuse        = true; // fused two-level steps in the schedule
     int32_t m_level_tpc = 16;  // tiles of 2048 columns per level-kernel CTA
@@ -127,6 +137,19 @@ private:
      * beams' kernels overlap); results do not depend on it. */
     void set_residency(int32_t ctas_per_sm);
     int32_t residency() const { return m_ctas_per_sm; }
+
+    /** Device bytes an engine for (dd, bc) allocates, computed on the host
+     * from its plan without allocating anything: level buffers (under
+     * either schedule autotune may try), histories, tables, candidates, and
+     * autotune's transient zero waterfall. Throws what the constructor
+     * throws for an invalid configuration. */
+    struct Footprint {
+        SizeType level_bytes = 0, history_bytes = 0, table_bytes = 0, candidate_bytes = 0;
+        SizeType transient_bytes = 0;
+        int32_t dt_max           = 0;
+        SizeType total() const { return level_bytes + history_bytes + table_bytes + candidate_bytes; }
+    };
+    static Footprint estimate(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc);
   private:
     int32_t m_ctas_per_sm = 0;
     int32_t m_sms         = 0;

@@ -903,6 +903,58 @@ int frost_cand_writer_close(frost_cand_writer* w);
  * `utc` (seconds since the epoch) and 1-based `beam`, into out[capacity]. */
 int frost_cand_filename(int64_t utc, uint64_t beam, char* out, size_t capacity);
 
+/* ---- memory planning (include/frost/pipeline/memory.hpp) ------------------
+ *
+ * The device counterpart of frost's planner (lib/pipeline/memory.cpp:294-508):
+ * the device bytes of one beam's RFI cleaner, FDMT/search engine and
+ * (optionally) post-processor, computed on the host from the plans without
+ * allocating anything, and the gulp check frost runs before building them. */
+
+typedef struct {
+    uint64_t rfi_bytes;         /* RFI cleaner: raw block, float work and output, window / chunk tables */
+    uint64_t fdmt_bytes;        /* FDMT level buffers and histories */
+    uint64_t search_bytes;      /* plan and search tables, run state, candidate buffer */
+    uint64_t postprocess_bytes; /* device post-processing (0 without a config) */
+    uint64_t transient_bytes;   /* autotune's zero waterfall, freed before the first gulp */
+    uint64_t total_bytes;       /* the sum of the above */
+    uint64_t max_delay;         /* the plan's dispersion delay in samples */
+} frost_memory_estimate;
+
+/* The footprint of a beam of `layout` (max_nsamps is the gulp), `plan`
+ * (block_nsamps must equal it), `search` and, if not NULL, `post`, as this
+ * implementation allocates it (level buffers under either schedule the
+ * autotuner may try; buffers sized by data at their largest). The same
+ * errors as building them for an invalid configuration. */
+int frost_estimate_memory(const frost_rfi_config* rfi, const frost_block_layout* layout, float baseline_length,
+                          const frost_dedisp_plan_config* plan, const frost_boxcar_config* search,
+                          const frost_postprocess_config* post, frost_memory_estimate* out);
+
+/* MemoryCheck (include/frost/pipeline/memory.hpp). */
+typedef struct {
+    frost_memory_estimate estimate; /* at gulp_used */
+    uint64_t requested_bytes;       /* total_bytes at gulp_requested */
+    uint64_t available_bytes;       /* 0: unknown, nothing was enforced */
+    uint64_t gulp_requested;
+    uint64_t gulp_used;
+    int32_t lowered;
+    int32_t device_memory;          /* always 1: the budget is device memory */
+} frost_memory_check;
+
+/* check_memory (lib/pipeline/memory.cpp:294-508) for the device: compares
+ * the estimate at the configured gulp with 90 % of `available_bytes` (0:
+ * the free memory of `device`, further capped by `memory_limit_bytes` when
+ * that is not 0; if neither is known, nothing is enforced). When it does not
+ * fit and `gulp_is_default` is set, the gulp (layout->max_nsamps and
+ * plan->block_nsamps) is lowered to the largest multiple of 1024 samples
+ * that fits and `lowered` is set; otherwise, or when even the smallest
+ * valid gulp (max_delay + boxcar_max + 1, rounded up to 1024) does not fit,
+ * FROST_ERR_OUT_OF_MEMORY with a message naming the estimate, the budget
+ * and the largest gulp that fits. */
+int frost_check_memory(const frost_rfi_config* rfi, frost_block_layout* layout, float baseline_length,
+                       frost_dedisp_plan_config* plan, const frost_boxcar_config* search,
+                       const frost_postprocess_config* post, int gulp_is_default, uint64_t available_bytes,
+                       uint64_t memory_limit_bytes, int device, frost_memory_check* out);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

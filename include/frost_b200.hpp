@@ -431,6 +431,31 @@ inline std::string cand_filename(int64_t utc, uint64_t beam) {
     return buf;
 }
 
+/** frost::pipeline::MemoryEstimate for this implementation's device
+ * buffers (frost_estimate_memory); `post` may be null. */
+inline frost_memory_estimate estimate_memory(const frost_rfi_config& rfi, const frost_block_layout& layout,
+                                             float baseline_length, const frost_dedisp_plan_config& plan,
+                                             const frost_boxcar_config& search,
+                                             const frost_postprocess_config* post = nullptr) {
+    frost_memory_estimate e{};
+    check(frost_estimate_memory(&rfi, &layout, baseline_length, &plan, &search, post, &e));
+    return e;
+}
+
+/** frost::pipeline::check_memory on the device (frost_check_memory): may
+ * lower the gulp in `layout` and `plan`; throws frost::b200::Error with
+ * FROST_ERR_OUT_OF_MEMORY when it cannot. */
+inline frost_memory_check check_memory(const frost_rfi_config& rfi, frost_block_layout& layout, float baseline_length,
+                                       frost_dedisp_plan_config& plan, const frost_boxcar_config& search,
+                                       bool gulp_is_default, uint64_t available_bytes = 0,
+                                       const frost_postprocess_config* post = nullptr,
+                                       uint64_t memory_limit_bytes = 0, int device = 0) {
+    frost_memory_check c{};
+    check(frost_check_memory(&rfi, &layout, baseline_length, &plan, &search, post, gulp_is_default ? 1 : 0,
+                             available_bytes, memory_limit_bytes, device, &c));
+    return c;
+}
+
 /** config::SearchConfig's post-processing defaults (config.hpp:57-97). */
 inline frost_postprocess_config default_postprocess_config() {
     frost_postprocess_config c{};

@@ -83,6 +83,25 @@ static int cpu_mode() {
     } catch (const std::invalid_argument&) {
         std::cout << "postprocess invalid_argument\n";
     }
+    // memory planning: a beam that needs more than 90 % of the budget has
+    // its default gulp lowered to a multiple of 1024 samples that fits
+    {
+        frost_block_layout lay{1024, 65536, FROST_UINT8, 64e-6, 1500.0, -0.29296875};
+        auto dd = plan_for(1024, 65536, 64e-6, 1500.0, -0.29296875, 500.0F, 1);
+        frost_boxcar_config sc{};
+        sc.max_boxcar = 64, sc.wtsp = 2.0F, sc.detect_thresh = 6.0F, sc.noise_sigma = 1.0F;
+        sc.peak_mode = FROST_PEAK_PER_WIDTH, sc.max_candidates = 1 << 16, sc.skip_cold_prefix = 1;
+        sc.input_nbits = 32, sc.storage = FROST_STORAGE_FP16;
+        const auto rc = fb::default_rfi_config();
+        const auto e  = fb::estimate_memory(rc, lay, 1.0F, dd, sc);
+        const auto c  = fb::check_memory(rc, lay, 1.0F, dd, sc, true, e.total_bytes / 2);
+        if (!c.lowered || c.gulp_used % 1024 != 0 || lay.max_nsamps != c.gulp_used || dd.block_nsamps != c.gulp_used ||
+            c.estimate.total_bytes > e.total_bytes / 2 - e.total_bytes / 20) {
+            std::cout << "check_memory wrong\n";
+            return 1;
+        }
+        std::cout << "memory lowered " << c.gulp_used << "\n";
+    }
     std::cout << "ok\n";
     return 0;
 }
