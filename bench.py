@@ -744,6 +744,48 @@ def run_postprocess(args):
     print(json.dumps(line), flush=True)
 
 
+def run_rfi(args):
+    """The RFI stage of the headline gulp alone (4096 channels, uint8, the
+    config-2 RFI recipe and strategies: bandpass, moments, IQRM, Kadane in
+    time and frequency, zero-DM) on its first `--rfi-nsamps` samples: one
+    step cleans and normalises one block on the device. A profiling case for
+    the order-exact statistics kernels, small enough for multi-pass ncu
+    captures; not the headline metric."""
+    import numpy as np
+    import torch
+
+    from frost_b200.rfi import RFICleaner
+
+    select_workload("config2")
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    n = int(args.rfi_nsamps)
+    raw = np.ascontiguousarray(make_gulp(0x46524F5354)[:n])
+    dev = torch.from_numpy(raw.reshape(-1)).to("cuda")
+    cl = RFICleaner(rfi_config(), layout(n), 2.0, device=local)
+    for _ in range(args.warmup):
+        cl.execute_normalized_device(dev.data_ptr(), raw.size, n, on_device=True)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(args.steps):
+        cl.execute_normalized_device(dev.data_ptr(), raw.size, n, on_device=True)
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    rep = cl.report()
+    print(json.dumps({"metric": "RFI stage, samples cleaned per second", "value": round(n / (ms / 1e3), 1),
+                      "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f64 statistics, f32 output", "data": "synthetic",
+                      "config": {"workload": f"4096ch uint8, config-2 RFI recipe, first {n} samples of the gulp"},
+                      "rfi_stage_ms": {k: round(rep[k] * 1e3, 2) for k in
+                                       ("t_bandpass", "t_moments", "t_scan", "t_flags", "t_apply")}}),
+          flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -751,14 +793,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["frost", "reference"], default="frost")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "postprocess"], default="config2",
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "postprocess", "rfi"], default="config2",
                     help="config2 (headline), config1 (1024-channel profiling case), serving "
-                         "(64 beams at real-time cadence) or postprocess (candidate clustering and "
-                         "dedup of the headline gulp's detections)")
+                         "(64 beams at real-time cadence), postprocess (candidate clustering and "
+                         "dedup of the headline gulp's detections) or rfi (the RFI stage alone, a "
+                         "profiling case)")
     ap.add_argument("--beams", type=int, default=3, help="served beams per GPU (admitted by memory)")
     ap.add_argument("--served-tile", type=int, default=0,
                     help="FDMT tile of the served beams in samples (0 = the whole gulp)")
+    ap.add_argument("--rfi-nsamps", type=int, default=131072,
+                    help="samples of the headline gulp the rfi workload cleans per step")
     args = ap.parse_args()
+    if args.workload == "rfi":
+        run_rfi(args)
+        return
     if args.workload == "serving":
         run_serving(args)
         return

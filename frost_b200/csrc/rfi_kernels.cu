@@ -1213,6 +1213,19 @@ struct WelfordAcc {
         mean += y != 0.0 ? div_by_count(delta, n, y) : div_plain(delta, n);
         var += delta * (x - mean);
     }
+    /** step_by for y = RN(1/n) > 0, with div_by_count's cases folded into
+     * one rarely taken branch and a select (the same bits): a zero
+     * numerator is returned as is, a tiny or NaN one takes the division. */
+    __device__ __forceinline__ void step_recip(float xf, double n, double y) {
+        const double x     = xf;
+        const double delta = x - mean;
+        const double q0    = delta * y;
+        double q           = fma(fma(-q0, n, delta), y, q0);
+        if (!(fabs(delta) > 0x1p-900) && delta != 0.0)
+            q = div_plain(delta, n);
+        mean += delta == 0.0 ? delta : q;
+        var += delta * (x - mean);
+    }
 };
 
 __global__ void k_welford(Dims d, const float* __restrict__ work, const double* __restrict__ recip,
@@ -1273,10 +1286,17 @@ __global__ void __launch_bounds__(kStageChans)
         const int nr      = st.rows_of(k);
         double nd         = static_cast<double>(st.t0(k) - b); // exact below 2^53
         if (in) {
+            if (recip != nullptr) {
 #pragma unroll 8
-            for (int r = 0; r < nr; ++r) {
-                nd += 1.0;
-                acc.step_by(buf[r * stride + threadIdx.x], nd, ys[k & 1][r]);
+                for (int r = 0; r < nr; ++r) {
+                    nd += 1.0;
+                    acc.step_recip(buf[r * stride + threadIdx.x], nd, ys[k & 1][r]);
+                }
+            } else {
+                for (int r = 0; r < nr; ++r) {
+                    nd += 1.0;
+                    acc.step_by(buf[r * stride + threadIdx.x], nd, 0.0);
+                }
             }
         }
         st.release(k);
