@@ -38,6 +38,16 @@ template <> __device__ __forceinline__ void st<__half>(__half* p, float v) {
     *p = __float2half_rn(fminf(fmaxf(v, -65504.0F), 65504.0F));
 }
 
+// Two sums of finite fp16 level values (at most four of them, so finite
+// floats) rounded to an fp16 pair, lo in the low half: the saturating
+// convert gives st<__half>'s clamp-then-round bit for bit for finite
+// inputs (a magnitude past 65504 becomes 65504), in one instruction.
+__device__ __forceinline__ uint32_t pack_sat(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
 // Inclusive block scan of smem[0..n) in place (float), n <= kThreads * 64.
 __device__ void block_scan(float* a, int n) {
     __shared__ float warp_tot[kThreads / 32];
@@ -184,10 +194,7 @@ __device__ __forceinline__ void merge8(const S* lo, const S* stage, int e, int o
         for (int i = 0; i < 4; ++i) {
             const float2 x = __half22float2(*reinterpret_cast<const __half2*>(&av[i]));
             const float2 y = __half22float2(*reinterpret_cast<const __half2*>(&g[i]));
-            const float lo_sum = fminf(fmaxf(x.x + y.x, -65504.0F), 65504.0F);
-            const float hi_sum = fminf(fmaxf(x.y + y.y, -65504.0F), 65504.0F);
-            const __half2 s    = __floats2half2_rn(lo_sum, hi_sum);
-            r[i]               = *reinterpret_cast<const uint32_t*>(&s);
+            r[i]           = pack_sat(x.x + y.x, x.y + y.y);
         }
         *reinterpret_cast<uint4*>(dst) = make_uint4(r[0], r[1], r[2], r[3]);
     }
@@ -463,9 +470,7 @@ __global__ void __launch_bounds__(kThreads)
                 uint32_t r[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const __half2 h = __floats2half2_rn(fminf(fmaxf(a[2 * q], -65504.0F), 65504.0F),
-                                                        fminf(fmaxf(a[2 * q + 1], -65504.0F), 65504.0F));
-                    r[q] = *reinterpret_cast<const uint32_t*>(&h);
+                    r[q] = pack_sat(a[2 * q], a[2 * q + 1]);
                 }
                 *reinterpret_cast<uint4*>(dst) = make_uint4(r[0], r[1], r[2], r[3]);
             }
@@ -563,10 +568,7 @@ __global__ void __launch_bounds__(kThreads)
         for (int i = 0; i < 4; ++i) {
             const float2 x = __half22float2(*reinterpret_cast<const __half2*>(&av[i]));
             const float2 y = __half22float2(*reinterpret_cast<const __half2*>(&g[i]));
-            const float lo_sum = fminf(fmaxf(x.x + y.x, -65504.0F), 65504.0F);
-            const float hi_sum = fminf(fmaxf(x.y + y.y, -65504.0F), 65504.0F);
-            const __half2 s    = __floats2half2_rn(lo_sum, hi_sum);
-            r[i]               = *reinterpret_cast<const uint32_t*>(&s);
+            r[i]           = pack_sat(x.x + y.x, x.y + y.y);
         }
         *reinterpret_cast<uint4*>(dst + e) = make_uint4(r[0], r[1], r[2], r[3]);
     }
