@@ -235,11 +235,13 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     // Work items (row, run of tpc tiles), rows fastest; a CTA takes items
     // blockIdx.x, blockIdx.x + gridDim.x, ... and its tiles use the stages
-    // in turn across items (tile n of the CTA: stage n % kStages).
+    // in turn across items (the CTA's tile n: stage n % kStages, barrier
+    // phase (n / kStages) % 2, kept as running counters).
     const int nruns      = (ntiles + tpc - 1) / tpc;
     const int64_t nitems = nrows * nruns;
     const int e          = 8 * threadIdx.x;
-    int64_t done         = 0; // tiles this CTA has consumed
+    int cs      = 0;  // stage of the CTA's next tile
+    uint32_t cp = 0U; // and its barrier's phase parity
     for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int64_t r = item % nrows;
         const RowOp op  = ops[r];
@@ -255,8 +257,7 @@ __global__ void __launch_bounds__(kThreads)
         const int off         = static_cast<int>(((e_first % VEC) + VEC) % VEC);
         const uint32_t hi_bytes = has_hi ? static_cast<uint32_t>((kTimePerCta / VEC + (off > 0 ? 1 : 0)) * 16) : 0U;
 
-        auto issue = [&](int i) {
-            const int s       = static_cast<int>((done + i) % kStages);
+        auto issue = [&](int i, int s) {
             const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
             unsigned char* st = pipe_smem + s * kStageBytes;
             bulk::mbar_expect(&bar[s], static_cast<uint32_t>(kLoBytes) + hi_bytes);
@@ -268,13 +269,12 @@ __global__ void __launch_bounds__(kThreads)
         };
 
         if (threadIdx.x == 0)
-            for (int i = 0; i < min(kStages, nt); ++i)
-                issue(i);
+            for (int i = 0, s = cs; i < min(kStages, nt); ++i, s = s + 1 == kStages ? 0 : s + 1)
+                issue(i, s);
         int i = 0;
         for (; i < nt; ++i) {
-            const int s           = static_cast<int>((done + i) % kStages);
-            const uint32_t phase  = static_cast<uint32_t>(((done + i) / kStages) & 1);
-            if (!mbar_wait(&bar[s], phase))
+            const int s = cs;
+            if (!mbar_wait(&bar[s], cp))
                 atomicExch(&abort_flag, 1);
             __syncthreads();
             if (abort_flag)
@@ -292,18 +292,26 @@ __global__ void __launch_bounds__(kThreads)
             }
             __syncthreads(); // every thread is done with stage s
             if (threadIdx.x == 0 && i + kStages < nt)
-                issue(i + kStages);
+                issue(i + kStages, s);
+            if (++cs == kStages) {
+                cs = 0;
+                cp ^= 1U;
+            }
         }
         if (i < nt) {
             if (threadIdx.x == 0) {
                 // a wait ran out: report it, then let the copies still in flight land
                 atomicOr(err, 1U);
-                for (int j = i; j < min(nt, i + kStages); ++j)
-                    (void)mbar_wait(&bar[(done + j) % kStages], static_cast<uint32_t>(((done + j) / kStages) & 1));
+                for (int j = i, s = cs, p = static_cast<int>(cp); j < min(nt, i + kStages); ++j) {
+                    (void)mbar_wait(&bar[s], static_cast<uint32_t>(p));
+                    if (++s == kStages) {
+                        s = 0;
+                        p ^= 1;
+                    }
+                }
             }
             return;
         }
-        done += nt;
     }
 }
 
@@ -388,7 +396,8 @@ __global__ void __launch_bounds__(kThreads)
     const int nruns      = (ntiles + tpc - 1) / tpc;
     const int64_t nitems = nrows * nruns;
     const int e          = 8 * threadIdx.x;
-    int64_t done         = 0; // tiles this CTA has consumed
+    int cs      = 0;  // stage of the CTA's next tile
+    uint32_t cp = 0U; // and its barrier's phase parity
     for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int64_t r  = item % nrows;
         const FusedOp op = ops[r];
@@ -412,8 +421,7 @@ __global__ void __launch_bounds__(kThreads)
         }
         S* dst_row = out + r * out_pitch + out_base;
 
-        auto issue = [&](int i) {
-            const int st      = static_cast<int>((done + i) % NS);
+        auto issue = [&](int i, int st) {
             const int64_t k0  = static_cast<int64_t>(tile0 + i) * kTimePerCta;
             unsigned char* sb = pipe2_smem + st * kStageBytes;
             bulk::mbar_expect(&bar[st], total);
@@ -428,13 +436,12 @@ __global__ void __launch_bounds__(kThreads)
         };
 
         if (threadIdx.x == 0)
-            for (int i = 0; i < min(NS, nt); ++i)
-                issue(i);
+            for (int i = 0, st = cs; i < min(NS, nt); ++i, st = st + 1 == NS ? 0 : st + 1)
+                issue(i, st);
         int i = 0;
         for (; i < nt; ++i) {
-            const int st         = static_cast<int>((done + i) % NS);
-            const uint32_t phase = static_cast<uint32_t>(((done + i) / NS) & 1);
-            if (!mbar_wait(&bar[st], phase))
+            const int st = cs;
+            if (!mbar_wait(&bar[st], cp))
                 atomicExch(&abort_flag, 1);
             __syncthreads();
             if (abort_flag)
@@ -476,18 +483,26 @@ __global__ void __launch_bounds__(kThreads)
             }
             __syncthreads(); // every thread is done with stage st
             if (threadIdx.x == 0 && i + NS < nt)
-                issue(i + NS);
+                issue(i + NS, st);
+            if (++cs == NS) {
+                cs = 0;
+                cp ^= 1U;
+            }
         }
         if (i < nt) {
             if (threadIdx.x == 0) {
                 // a wait ran out: report it, then let the copies still in flight land
                 atomicOr(err, 1U);
-                for (int j = i; j < min(nt, i + NS); ++j)
-                    (void)mbar_wait(&bar[(done + j) % NS], static_cast<uint32_t>(((done + j) / NS) & 1));
+                for (int j = i, st = cs, p = static_cast<int>(cp); j < min(nt, i + NS); ++j) {
+                    (void)mbar_wait(&bar[st], static_cast<uint32_t>(p));
+                    if (++st == NS) {
+                        st = 0;
+                        p ^= 1;
+                    }
+                }
             }
             return;
         }
-        done += nt;
     }
 }
 
