@@ -528,16 +528,17 @@ constexpr int kScanChans = 64;  // channel tile staged in shared memory
 // channels in ascending order: the detection series sums and the Kadane
 // states across frequency.
 struct ScanRowAcc {
-    double sum_det = 0.0, sum_keep = 0.0, n_keep = 0.0, sx = 0.0, sxx = 0.0, n_meas = 0.0;
+    double sum_det = 0.0, sum_keep = 0.0, sx = 0.0, sxx = 0.0;
+    uint32_t n_keep = 0, n_meas = 0; // counts (exact as doubles when used)
     KadaneState sp = KadaneState::make(), sn = KadaneState::make();
     __device__ __forceinline__ void step(uint64_t c, float x, float l, float ic, float clip, int kspec) {
-        n_meas += 1.0;
+        ++n_meas;
         const float zc = (x - l) * ic;
         const float cl = clampf(zc, -clip, clip);
         sum_det += cl;
         if (fabsf(zc) <= clip) {
             sum_keep += zc;
-            n_keep += 1.0;
+            ++n_keep;
         }
         sx += x;
         sxx += static_cast<double>(x) * x;
@@ -551,8 +552,8 @@ struct ScanRowAcc {
                            double* __restrict__ s_keep_d, float* __restrict__ s_keep_f,
                            float* __restrict__ row_std, Span32* __restrict__ kspec_pos,
                            Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole) const {
-        const double dn     = n_meas > 1.0 ? n_meas : 1.0;
-        const double s_keep = n_keep > 0.0 ? sum_keep / n_keep : 0.0;
+        const double dn     = n_meas > 1 ? static_cast<double>(n_meas) : 1.0;
+        const double s_keep = n_keep > 0 ? sum_keep / static_cast<double>(n_keep) : 0.0;
         s_det[t]            = static_cast<float>(sum_det / dn);
         s_keep_f[t]         = static_cast<float>(s_keep);
         s_keep_d[t]         = s_keep;
@@ -678,9 +679,9 @@ __global__ void __launch_bounds__(kScanRows)
         __syncthreads();
         if (active) {
             const uint8_t* row = tiles + (j & 1) * kScanRows * kRowTileStride + threadIdx.x * kRowTileStride;
-            const uint64_t cb  = static_cast<uint64_t>(j) * kTileCh;
-            const uint64_t ce  = cb + kTileCh < n ? cb + kTileCh : n;
-            for (uint64_t q = cb; q < ce; q += kPerChunk) {
+            const uint32_t cb  = static_cast<uint32_t>(j) * kTileCh; // channel indices fit 32 bits
+            const uint32_t ce  = cb + kTileCh < n ? cb + kTileCh : static_cast<uint32_t>(n);
+            for (uint32_t q = cb; q < ce; q += kPerChunk) {
                 union {
                     uint4 v;
                     uint8_t b[16];
@@ -688,7 +689,7 @@ __global__ void __launch_bounds__(kScanRows)
                 u.v = *reinterpret_cast<const uint4*>(row + (q - cb) * kBitsOf<D> / 8);
 #pragma unroll
                 for (int e = 0; e < kPerChunk; ++e) {
-                    const uint64_t c = q + e;
+                    const uint32_t c = q + e;
                     if (c >= ce)
                         break;
                     if (mask[c] == 0)
@@ -944,8 +945,11 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
     };
 
     // V consecutive channels per thread (V = 4: 16-byte loads of the
-    // per-window constants and stores of the row, when nchans % 4 == 0)
-    for (uint64_t cb = threadIdx.x * V; cb < n; cb += blockDim.x * V) {
+    // per-window constants and stores of the row, when nchans % 4 == 0);
+    // channel indices fit 32 bits (the launcher checks)
+    const uint32_t n32 = static_cast<uint32_t>(n);
+    bool dirty         = false; // a cell of this thread's needs a fill
+    for (uint32_t cb = threadIdx.x * V; cb < n32; cb += blockDim.x * V) {
         float xs[V], ls[V], ss[V], is[V], outv[V];
         uint8_t ms[V], ka[V];
         if constexpr (V == 4) {
@@ -982,7 +986,7 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
         }
 #pragma unroll
         for (int e = 0; e < V; ++e) {
-            const uint64_t c = cb + e;
+            const uint32_t c = cb + e;
             const float x    = xs[e];
             uint8_t st;
             float v = 0.0F;
@@ -1013,6 +1017,7 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
             }
             state[c] = st;
             sv[c]    = v;
+            dirty    = dirty || st == kNarrow || st == kKadaneSpectrum || st == kKadaneChannel;
         }
         // masked and flagged cells are (re)written below or never read
         if constexpr (V == 4)
@@ -1020,10 +1025,12 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
         else
             out[cb] = outv[0];
     }
-    __syncthreads();
+    // a row with no cell to fill (almost every row) is done
+    if (!__syncthreads_or(dirty))
+        return;
 
     unsigned long long narrow = 0, nks = 0, nkc = 0, fallbacks = 0;
-    for (uint64_t c = threadIdx.x; c < n; c += blockDim.x) {
+    for (uint32_t c = threadIdx.x; c < n32; c += blockDim.x) {
         const uint8_t st = state[c];
         if (st == kClean || st == kUnmeasured || st == kMasked)
             continue;
@@ -1569,6 +1576,8 @@ void launch_scan_rows(const Dims& d, const uint8_t* raw, const float* loc, const
                       const uint64_t* good_prefix, float* s_det, double* s_keep_d, float* s_keep_f,
                       float* row_std, Span32* kspec_pos, Span32* kspec_neg, uint8_t* kspec_whole,
                       cudaStream_t s) {
+    if (d.nchans >= (uint64_t{1} << 31))
+        throw Error(FROST_ERR_INVALID_ARGUMENT, "scan: too many channels for 32-bit channel indices");
     const unsigned grid = grid1(d.nsamps, kScanRows);
     if (d.row_bytes % 16 != 0 || reinterpret_cast<uintptr_t>(raw) % 16 != 0) {
         FB_DISPATCH(d.dtype, k_scan_rows<D><<<grid, kScanRows, 0, s>>>(
@@ -1625,6 +1634,8 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
     const size_t smem = d.nchans * (sizeof(float) + 1);
     if (d.nsamps == 0)
         return;
+    if (d.nchans >= (uint64_t{1} << 31))
+        throw Error(FROST_ERR_INVALID_ARGUMENT, "apply: too many channels for one row's block");
     // 4-channel vectors need nchans % 4 == 0 and, for the byte loads of the
     // raw row, a 4-byte aligned block
     const bool vec = d.nchans % 4 == 0 && reinterpret_cast<uintptr_t>(raw) % 4 == 0;
