@@ -326,6 +326,37 @@ __global__ void __launch_bounds__(kThreads)
 // k_level_pipe: one unshifted segment and up to three 16-byte-aligned
 // supersets of the shifted ones per tile, kStages2 tiles in flight.
 
+// The 8 fp16 values starting at element off + e of a staged aligned
+// segment (off < 8), as packed pairs (value 2i in the low half of g[i]).
+__device__ __forceinline__ void pick8h(const __half* stage, int e, int off, uint32_t (&g)[4]) {
+    const uint4* sv = reinterpret_cast<const uint4*>(stage) + e / 8;
+    const uint4 b0 = sv[0], b1 = sv[1]; // b1 unused when off == 0
+    const uint32_t w[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+    switch (off) {
+#define FB_PICK_EVEN(O)                                                                           \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] = w[O / 2 + i];                         \
+        break;
+#define FB_PICK_ODD(O)                                                                            \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] =                                      \
+            __byte_perm(w[O / 2 + i], w[O / 2 + i + 1], 0x5432);                                  \
+        break;
+        FB_PICK_EVEN(0) FB_PICK_ODD(1) FB_PICK_EVEN(2) FB_PICK_ODD(3)
+        FB_PICK_EVEN(4) FB_PICK_ODD(5) FB_PICK_EVEN(6) FB_PICK_ODD(7)
+#undef FB_PICK_EVEN
+#undef FB_PICK_ODD
+    }
+}
+
+// f + h in float, h an fp16 value: the widening is exact, so this is
+// float(h) + f rounded to nearest, in one mixed-precision add.
+__device__ __forceinline__ float add_h(uint16_t h, float f) {
+    float r;
+    asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(h), "f"(f));
+    return r;
+}
+
 // 8 consecutive values starting at element off + e of a staged aligned
 // segment (off < 16 / sizeof(S)), as float.
 template <class S>
@@ -343,30 +374,34 @@ __device__ __forceinline__ void load8(const S* stage, int e, int off, float (&x)
 #undef FB_PICK
         }
     } else {
-        const uint4* sv = reinterpret_cast<const uint4*>(stage) + e / 8;
-        const uint4 b0 = sv[0], b1 = sv[1]; // b1 unused when off == 0
-        const uint32_t w[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
         uint32_t g[4];
-        switch (off) {
-#define FB_PICK_EVEN(O)                                                                           \
-    case O:                                                                                       \
-        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] = w[O / 2 + i];                         \
-        break;
-#define FB_PICK_ODD(O)                                                                            \
-    case O:                                                                                       \
-        _Pragma("unroll") for (int i = 0; i < 4; ++i) g[i] =                                      \
-            __byte_perm(w[O / 2 + i], w[O / 2 + i + 1], 0x5432);                                  \
-        break;
-            FB_PICK_EVEN(0) FB_PICK_ODD(1) FB_PICK_EVEN(2) FB_PICK_ODD(3)
-            FB_PICK_EVEN(4) FB_PICK_ODD(5) FB_PICK_EVEN(6) FB_PICK_ODD(7)
-#undef FB_PICK_EVEN
-#undef FB_PICK_ODD
-        }
+        pick8h(stage, e, off, g);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&g[i]));
             x[2 * i]       = f.x;
             x[2 * i + 1]   = f.y;
+        }
+    }
+}
+
+// acc[q] = acc[q] + (value q of load8), the same float sums; fp16 values are
+// added with mixed-precision adds instead of being widened first.
+template <class S>
+__device__ __forceinline__ void add8(const S* stage, int e, int off, float (&acc)[8]) {
+    if constexpr (sizeof(S) == 4) {
+        float x[8];
+        load8<S>(stage, e, off, x);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            acc[q] = acc[q] + x[q];
+    } else {
+        uint32_t g[4];
+        pick8h(stage, e, off, g);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            acc[2 * i]     = add_h(static_cast<uint16_t>(g[i] & 0xFFFFU), acc[2 * i]);
+            acc[2 * i + 1] = add_h(static_cast<uint16_t>(g[i] >> 16), acc[2 * i + 1]);
         }
     }
 }
@@ -447,23 +482,15 @@ __global__ void __launch_bounds__(kThreads)
             if (abort_flag)
                 break;
             const unsigned char* sb = pipe2_smem + st * kStageBytes;
-            float a[8], x[8];
+            float a[8];
             load8<S>(reinterpret_cast<const S*>(sb), e, 0, a);
-            if (bytes[1] != 0U) {
-                load8<S>(reinterpret_cast<const S*>(sb + kLoBytes), e, off[1], x);
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    a[q] = a[q] + x[q];
-            }
+            if (bytes[1] != 0U)
+                add8<S>(reinterpret_cast<const S*>(sb + kLoBytes), e, off[1], a);
             if (bytes[2] != 0U) {
                 float b[8];
                 load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + kHiBytes), e, off[2], b);
-                if (bytes[3] != 0U) {
-                    load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], x);
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        b[q] = b[q] + x[q];
-                }
+                if (bytes[3] != 0U)
+                    add8<S>(reinterpret_cast<const S*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], b);
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
                     a[q] = a[q] + b[q];
