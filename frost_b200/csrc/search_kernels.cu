@@ -296,6 +296,32 @@ template <class S, int P> __device__ __forceinline__ void ld_cols(const S* p, fl
     }
 }
 
+// q[e] = x[0] + ... + x[e] (left to right, float) of the P staged samples
+// at `p` (16-byte aligned); fp16 samples are added with mixed-precision
+// adds (`add.rn.f32.f16`: the widening is exact, so the same bits as
+// widening first).
+template <class S, int P> __device__ __forceinline__ void scan_cols(const S* p, float (&q)[P]) {
+    if constexpr (sizeof(S) == 4) {
+        ld_cols<S, P>(p, q);
+#pragma unroll
+        for (int e = 1; e < P; ++e)
+            q[e] += q[e - 1];
+    } else {
+        uint32_t w[P / 2];
+#pragma unroll
+        for (int i = 0; i < P / 8; ++i) {
+            const uint4 u = reinterpret_cast<const uint4*>(p)[i];
+            w[4 * i] = u.x, w[4 * i + 1] = u.y, w[4 * i + 2] = u.z, w[4 * i + 3] = u.w;
+        }
+        q[0] = __half2float(__ushort_as_half(static_cast<unsigned short>(w[0] & 0xFFFFU)));
+#pragma unroll
+        for (int e = 1; e < P; ++e) {
+            const uint16_t h = static_cast<uint16_t>((e & 1) ? (w[e / 2] >> 16) : (w[e / 2] & 0xFFFFU));
+            asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(q[e]) : "h"(h), "f"(q[e - 1]));
+        }
+    }
+}
+
 template <int R, int NG, int N>
 __device__ __forceinline__ void pick_lows(const float (&e)[N], bool two, float (&lo)[NG]) {
 #pragma unroll
@@ -556,10 +582,7 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             // ---- prefix sums of the thread's P columns: serial, then across the
             // warp (shuffles), then across warps (one offset per warp)
             float q[P];
-            ld_cols<S, P>(seg + halo + P * threadIdx.x, q);
-#pragma unroll
-            for (int e = 1; e < P; ++e)
-                q[e] += q[e - 1];
+            scan_cols<S, P>(seg + halo + P * threadIdx.x, q);
             float incl = q[P - 1];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
