@@ -370,16 +370,18 @@ __global__ void __launch_bounds__(kBandChans)
         if (!__syncthreads_or(live))
             break;
         const double cut = kClipSigma * sd;
-        double count = 0.0, sum = 0.0;
+        uint32_t kept    = 0; // the count of kept samples (exact as a double)
+        double sum       = 0.0;
         sweep([&](float x, uint64_t) {
             if (live) {
                 const double dv = x - centre;
                 if (fabs(dv) <= cut) {
-                    count += 1.0;
+                    ++kept;
                     sum += dv;
                 }
             }
         });
+        const double count = static_cast<double>(kept);
         if (live && count < 2.0)
             live = false;
         const double shift = live ? sum / count : 0.0;
@@ -418,6 +420,7 @@ __global__ void __launch_bounds__(kBandChans)
 // (lib/cpu/rfi_cpu_measure.cpp:91-138).
 struct MomentsAcc {
     MomentSums s{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t n = 0, nc = 0; // the counts s.n and s.nc, kept as integers (exact)
     double prev = 0.0;
     float l, iv;
     double clip;
@@ -425,7 +428,7 @@ struct MomentsAcc {
     __device__ __forceinline__ void step(float x, uint64_t t) {
         const double z  = (x - l) * iv;
         const double z2 = z * z;
-        s.n += 1.0;
+        ++n;
         s.s1 += z;
         s.s2 += z2;
         s.s3 += z2 * z;
@@ -434,10 +437,16 @@ struct MomentsAcc {
             s.lag += z * prev;
         prev = z;
         if (fabs(z) <= clip) {
-            s.nc += 1.0;
+            ++nc;
             s.c1 += z;
             s.c2 += z2;
         }
+    }
+    __device__ __forceinline__ MomentSums sums() const {
+        MomentSums r = s;
+        r.n          = static_cast<double>(n);
+        r.nc         = static_cast<double>(nc);
+        return r;
     }
 };
 
@@ -472,7 +481,7 @@ __global__ void k_moments(Dims d, const uint8_t* __restrict__ raw, const float* 
             }
         }
     }
-    out[o] = acc.s;
+    out[o] = acc.sums();
 }
 
 // The same sequences with the block's channel columns streamed through
@@ -516,7 +525,7 @@ __global__ void __launch_bounds__(kStageChans)
         st.release(k);
     }
     if (in)
-        out[o] = acc.s;
+        out[o] = acc.sums();
 }
 
 // ---- row scan ---------------------------------------------------------------
