@@ -367,15 +367,27 @@ __device__ __forceinline__ void group_lows(const float* gmin, int i0, bool two, 
 // window starts' group and block offsets depend on W alone).
 template <int P, int NG, int WI>
 __device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float pm2, const float (&gmx)[NG],
-                                           float bmax, const float* gmin, const float* tmin, int halo, float T) {
+                                           float bmax, const float* gmin, const float* tmin, int halo, float T,
+                                           float& m1) {
     constexpr int W = 1 << WI;
     if constexpr (W == 1) {
         float m = q[0] - pm1;
 #pragma unroll
         for (int e = 1; e < P; ++e)
             m = fmaxf(m, q[e] - q[e - 1]);
+        m1 = m; // the largest width-1 sum of the thread's samples
         return m > T;
     } else if constexpr (W == 2) {
+        // Every width-2 window sum is, before rounding, the sum of two of the
+        // thread's width-1 sums (or of its first one and the one ending just
+        // before it). With M the largest of them as rounded, each is at most
+        // M (1 + 2^-23) when M > 0 and at most 0 otherwise (a rounded
+        // difference is 0 only when exact), so no width-2 sum rounds above
+        // 2 M (1 + 2^-22): skip the exact test when that cannot exceed T
+        // (NaN M or T <= 0: test).
+        const float d = fmaxf(m1, pm1 - pm2);
+        if (T > 0.0F && 2.0F * d * (1.0F + 0x1p-20F) <= T)
+            return false;
         float m = fmaxf(q[0] - pm2, q[1] - pm1);
 #pragma unroll
         for (int e = 2; e < P; ++e)
@@ -416,12 +428,12 @@ __device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float
 template <int P, int NG, int WI>
 __device__ __forceinline__ void pow2_all(uint32_t& cand, int nw, const float (&q)[P], float pm1, float pm2,
                                          const float (&gmx)[NG], float bmax, const float* gmin,
-                                         const float* tmin, int halo, const WidthTest* wt) {
+                                         const float* tmin, int halo, const WidthTest* wt, float& m1) {
     if constexpr (WI < kMaxPow2Widths) {
         if (WI < nw) {
-            if (pow2_maybe<P, NG, WI>(q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt[WI].T))
+            if (pow2_maybe<P, NG, WI>(q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt[WI].T, m1))
                 cand |= 1U << WI;
-            pow2_all<P, NG, WI + 1>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt);
+            pow2_all<P, NG, WI + 1>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt, m1);
         }
     }
 }
@@ -689,8 +701,10 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                     pm2 = warp == 0 ? Q[-2] : wtail[warp - 1][0];
                 }
                 uint32_t cand = 0U;
-                if constexpr (POW2)
-                    pow2_all<P, NG, 0>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt);
+                if constexpr (POW2) {
+                    float m1 = FB_POS_INF; // set by the width-1 test
+                    pow2_all<P, NG, 0>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt, m1);
+                }
                 else {
                     for (int wi = 0; wi < nw; ++wi) {
                         const WidthTest t = wt[wi];
