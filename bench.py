@@ -95,6 +95,24 @@ def dist_env():
     return rank, world, local
 
 
+def ranks_barrier(world):
+    """All ranks of the job meet here (one process per GPU; gloo)."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def ranks_max(x, world):
+    """The largest of every rank's `x` (timings are the slowest rank's)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
 
@@ -198,18 +216,8 @@ def run_gpu(args):
     lay = layout()
     plan = plan_for(lay, 0.0, DM_MAX, DEPTH)
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = lambda: ranks_barrier(world)
+    max_over_ranks = lambda x: ranks_max(x, world)
 
     def measure(storage, e2e=False, sample_clocks=False):
         pipe = GulpPipeline(rfi_config(), lay, 2.0, plan, search_config(storage), device=local)
