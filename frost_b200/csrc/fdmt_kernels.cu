@@ -689,8 +689,8 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
         out.pitch % 8 != 0 || in.fp16 != out.fp16)
         throw Error(FROST_ERR_INTERNAL, "level: bad geometry");
     const int ntiles = ncols / kTimePerCta;
-    if (tpc < 1 || tpc > 64)
-        throw Error(FROST_ERR_INTERNAL, "level: tiles per CTA must be in [1, 64]");
+    if (tpc < 1 || tpc > 128)
+        throw Error(FROST_ERR_INTERNAL, "level: tiles per CTA must be in [1, 128]");
     if (err == nullptr) {
         // direct form (no bulk copies): one CTA per (row, tile)
         const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>(ntiles));
@@ -754,8 +754,8 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
         out.pitch % 8 != 0 || in.fp16 != out.fp16 || err == nullptr)
         throw Error(FROST_ERR_INTERNAL, "level2: bad geometry");
-    if (tpc < 1 || tpc > 64)
-        throw Error(FROST_ERR_INTERNAL, "level2: tiles per CTA must be in [1, 64]");
+    if (tpc < 1 || tpc > 128)
+        throw Error(FROST_ERR_INTERNAL, "level2: tiles per CTA must be in [1, 128]");
     if (stages == 4 && !out.fp16)
         throw Error(FROST_ERR_INTERNAL, "level2: 4 float stages exceed the shared memory of a CTA");
     const int ntiles = ncols / kTimePerCta;

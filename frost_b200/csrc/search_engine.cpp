@@ -341,7 +341,7 @@ void Engine::build_schedule(bool fuse) {
 //
 // The FDMT launch shape is measured, not assumed: for this plan's geometry
 // the engine times one tile pass for every candidate (fused two-level steps
-// with 2, 3 or 4 bulk-copy stages, or single levels; 4, 8, 16 or 32 tiles
+// with 2, 3 or 4 bulk-copy stages, or single levels; 4 to 128 tiles
 // of 2048 columns per level-kernel CTA) on a zero waterfall (the level
 // kernels always process the tile's full width), keeps the fastest and
 // caches it for the process by geometry, then restores a fresh stream state.
@@ -406,7 +406,7 @@ Engine::Tuned Engine::autotune() {
             if (fuse)
                 stage_options = m_fp16 ? std::vector<int32_t>{2, 3, 4} : std::vector<int32_t>{2, 3};
             for (const int32_t stages : stage_options) {
-                for (const int32_t tpc : {4, 8, 16, 32}) {
+                for (const int32_t tpc : {4, 8, 16, 32, 64, 128}) {
                     m_level_tpc     = tpc;
                     m_level2_stages = stages;
                     run_tiles(wf.as<float>(), ncols, s); // warm-up
@@ -447,8 +447,8 @@ void Engine::apply_shape(bool fuse, int32_t tpc, int32_t stages, int32_t chunk) 
 }
 
 void Engine::set_launch_shape(bool fuse, int32_t tpc, int32_t stages, int32_t chunk) {
-    if (tpc < 1 || tpc > 64)
-        invalid("search: tiles per CTA must be in [1, 64]");
+    if (tpc < 1 || tpc > 128)
+        invalid("search: tiles per CTA must be in [1, 128]");
     if (stages != 0 && stages != 2 && stages != 3 && !(stages == 4 && m_fp16))
         invalid("search: fused stages must be 0, 2, 3 (or 4 with fp16 storage)");
     if (chunk != 2048 && chunk != 4096)

@@ -490,7 +490,7 @@ int frost_search_use_graphs(frost_search* s, int enable);
 
 /* No counterpart in the reference. Measures this geometry's FDMT launch
  * shapes (fused two-level steps with 2, 3 or 4 bulk-copy stages, or single
- * levels; 4, 8, 16 or 32 tiles of 2048 samples per level-kernel CTA) with
+ * levels; 4, 8, 16, 32, 64 or 128 tiles of 2048 samples per level-kernel CTA) with
  * one tile pass each on a zero waterfall, applies the fastest and restarts
  * the stream; results are cached per process by geometry. The search chunk
  * keeps its default (4096). Call before the first gulp. Any output pointer

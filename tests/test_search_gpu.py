@@ -275,7 +275,7 @@ def test_autotune_keeps_results_and_caches_choice():
     ref = run_engine(FDMTBoxcar(pc, bc), stream, pc.block_nsamps)
     tuned = FDMTBoxcar(pc, bc)
     t1 = tuned.autotune()
-    assert t1["tiles_per_cta"] in (4, 8, 16, 32) and t1["ms"] > 0 and not t1["cached"]
+    assert t1["tiles_per_cta"] in (4, 8, 16, 32, 64, 128) and t1["ms"] > 0 and not t1["cached"]
     assert t1 == {**tuned.launch_shape(), "ms": t1["ms"], "cached": False}
     got = run_engine(tuned, stream, pc.block_nsamps)
     if t1["search_chunk"] == 4096:
