@@ -8,7 +8,6 @@
 
 #include <condition_variable>
 #include <cstdint>
-#include <exception>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -52,10 +51,9 @@ private:
     void* m_ctx;
     cudaStream_t m_copy = nullptr;
     std::vector<Slot> m_slots;
-    int m_next_fill = 0, m_next_out = 0, m_out_count = 0, m_handed = -1;
+    int m_next_fill = 0, m_next_out = 0, m_handed = -1;
     int m_free;              // slots the reader may fill
     bool m_stop = false, m_eof = false;
-    std::exception_ptr m_error;
     std::string m_error_msg;
     int m_error_code = FROST_OK;
     mutable std::mutex m_mu;
