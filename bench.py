@@ -3,7 +3,9 @@
 workload: beam-seconds searched per second (whole job) of several beams
 served together on one GPU with FP16 plane storage, their p50/p99 gulp
 latency, the plain single-beam FP32 and FP16 paths beside them, the same
-served run fed from pinned host memory (e2e), the FDMT level kernel's HBM
+served run fed from pinned host memory (e2e; --staging N keeps N gulps in
+flight per beam, each uploaded into a staging block at submit), the FDMT
+level kernel's HBM
 roofline, and the CPU baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl frost|reference]
@@ -290,14 +292,26 @@ def run_gpu(args):
                 srv.set_postprocess(b, postprocess_config(int(bc.max_candidates)))
         src = raw_dev.data_ptr() if on_device else pinned.data_ptr()
         counts = {b: [0, 0] for b in beams}  # candidates (or giants), bytes
+        # Host gulps with --staging N: N in flight per beam, the next ones
+        # uploaded into staging blocks while the beam works on the one before.
+        depth = 1 if on_device else max(1, args.staging)
+        if not on_device and args.staging > 0:
+            for b in beams:
+                srv.set_staging(b, depth)
 
         def run_beam(b, n, keep):
-            for _ in range(n):
-                t = srv.submit_ptr(b, src, nbytes, GULP, on_device)
+            def collect(t):
                 cands, _ = srv.wait_giants(t) if postprocess else srv.wait(t)
                 if keep:
                     counts[b][0] += cands.size
                     counts[b][1] += cands.nbytes
+            pending = []
+            for _ in range(n):
+                pending.append(srv.submit_ptr(b, src, nbytes, GULP, on_device))
+                if len(pending) == depth:
+                    collect(pending.pop(0))
+            for t in pending:
+                collect(t)
 
         def run_all(n, keep):
             ths = [threading.Thread(target=run_beam, args=(b, n, keep)) for b in beams]
@@ -449,7 +463,8 @@ def run_gpu(args):
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
                 "h2d_bytes_per_step": nbytes * e2e["beams"],
                 "d2h_bytes_per_step": int(e2e["d2h"] / args.steps),
-                "what": "served beams fed from pinned host gulps through frost_server_submit"},
+                "what": "served beams fed from pinned host gulps through frost_server_submit",
+                "gulps_in_flight_per_beam": max(1, args.staging), "staging_blocks_per_beam": max(0, args.staging)},
         "gpu_launches": int(st.launches),
         "roofline": roofline,
         "clocks": served["clocks"],
@@ -807,6 +822,9 @@ def main():
                          "dedup of the headline gulp's detections) or rfi (the RFI stage alone, a "
                          "profiling case)")
     ap.add_argument("--beams", type=int, default=3, help="served beams per GPU (admitted by memory)")
+    ap.add_argument("--staging", type=int, default=0,
+                    help="e2e leg: staging blocks (and gulps in flight) per beam; 0 = one gulp in flight, "
+                         "uploaded when it is processed")
     ap.add_argument("--served-tile", type=int, default=0,
                     help="FDMT tile of the served beams in samples (0 = the whole gulp)")
     ap.add_argument("--rfi-nsamps", type=int, default=131072,

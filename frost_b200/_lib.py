@@ -89,6 +89,7 @@ SIGNATURES = {
     "frost_server_reset_stats": (C.c_int, [_vp]),
     "frost_server_set_postprocess": (C.c_int, [_vp, C.c_uint32, C.POINTER(_abi.PostprocessConfigC)]),
     "frost_server_set_residency": (C.c_int, [_vp, C.c_uint32, C.c_int]),
+    "frost_server_set_staging": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
     "frost_server_wait_giants": (C.c_int, [_vp, _u64, _vp, _sz, C.POINTER(_sz), C.POINTER(C.c_double)]),
     "frost_server_drain_giants": (C.c_int, [_vp, C.c_uint32, _vp, _sz, C.POINTER(_sz)]),
     "frost_cand_writer_open": (C.c_int, [C.c_char_p, C.c_double, C.c_int, C.POINTER(_vp)]),

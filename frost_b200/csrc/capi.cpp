@@ -554,6 +554,14 @@ int frost_server_set_residency(frost_server* s, uint32_t beam, int ctas_per_sm) 
     });
 }
 
+int frost_server_set_staging(frost_server* s, uint32_t beam, uint32_t slots) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_server_set_staging: null handle");
+        s->impl.set_staging(beam, slots);
+    });
+}
+
 int frost_server_set_postprocess(frost_server* s, uint32_t beam, const frost_postprocess_config* cfg) {
     return guarded([&] {
         if (s == nullptr || cfg == nullptr)

@@ -211,7 +211,6 @@ __device__ __forceinline__ void merge8(const S* lo, const S* stage, int e, int o
 // *err and the CTA drains its copies (again bounded) and returns.
 
 constexpr int kStages      = 4;
-constexpr int kTilesPerCta = 16; // default run of tiles per CTA (tunable per launch)
 using bulk::mbar_wait;
 
 template <class S>

@@ -39,7 +39,91 @@ SizeType Beam::block_bytes() const {
 }
 
 SizeType Beam::device_bytes() const {
-    return m_cleaner->memory_usage() + m_engine->device_bytes() + (m_post ? m_post->memory_usage() : 0);
+    return m_cleaner->memory_usage() + m_engine->device_bytes() + (m_post ? m_post->memory_usage() : 0) +
+           staging_bytes();
+}
+
+Beam::~Beam() { release_staging(); }
+
+void Beam::release_staging() {
+    DeviceGuard g(m_device);
+    if (m_copy != nullptr)
+        cudaStreamSynchronize(m_copy);
+    for (auto& st : m_stage) {
+        if (st.consumed != nullptr) {
+            cudaEventSynchronize(st.consumed);
+            cudaEventDestroy(st.consumed);
+        }
+        if (st.copied != nullptr)
+            cudaEventDestroy(st.copied);
+    }
+    m_stage.clear();
+    if (m_copy != nullptr)
+        cudaStreamDestroy(m_copy);
+    m_copy = nullptr;
+}
+
+void Beam::set_staging(uint32_t slots) {
+    if (slots > 4)
+        invalid("serve: staging slots must be in [0, 4]");
+    release_staging();
+    if (slots == 0)
+        return;
+    DeviceGuard g(m_device);
+    try {
+        FB_CUDA(cudaStreamCreateWithFlags(&m_copy, cudaStreamNonBlocking));
+        m_stage.resize(slots);
+        for (auto& st : m_stage) {
+            st.block.reserve(block_bytes());
+            FB_CUDA(cudaEventCreateWithFlags(&st.copied, cudaEventDisableTiming));
+            FB_CUDA(cudaEventCreateWithFlags(&st.consumed, cudaEventDisableTiming));
+        }
+    } catch (...) {
+        release_staging();
+        throw;
+    }
+}
+
+int Beam::stage(const uint8_t* block, SizeType bytes) {
+    if (m_stage.empty() || bytes != block_bytes())
+        return -1;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, block) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    if (a.type != cudaMemoryTypeHost)
+        return -1; // pageable: a copy from it would hold the caller
+    for (size_t i = 0; i < m_stage.size(); ++i) {
+        Stage& st = m_stage[i];
+        if (st.busy)
+            continue;
+        DeviceGuard g(m_device);
+        // the slot's last reader was queued before the slot was freed
+        if (st.used)
+            FB_CUDA(cudaStreamWaitEvent(m_copy, st.consumed, 0));
+        FB_CUDA(cudaMemcpyAsync(st.block.get(), block, bytes, cudaMemcpyHostToDevice, m_copy));
+        FB_CUDA(cudaEventRecord(st.copied, m_copy));
+        st.busy = true;
+        return static_cast<int>(i);
+    }
+    return -1;
+}
+
+void Beam::process_staged(int slot, SizeType bytes, SizeType nread) {
+    Stage& st = m_stage[static_cast<size_t>(slot)];
+    FB_CUDA(cudaStreamWaitEvent(m_cleaner->stream(), st.copied, 0));
+    auto done = [&] {
+        cudaEventRecord(st.consumed, m_cleaner->stream());
+        st.used = true;
+    };
+    try {
+        process(st.block.as<uint8_t>(), bytes, nread, true);
+    } catch (...) {
+        done();
+        throw;
+    }
+    done();
 }
 
 void Beam::attach_postprocess(const frost_postprocess_config& cfg) {
@@ -165,6 +249,8 @@ uint64_t Server::submit(uint32_t beam, const uint8_t* block, SizeType bytes, Siz
     req->bytes   = bytes;
     req->nread     = nread;
     req->on_device = on_device;
+    if (!on_device)
+        req->slot = m_beams[beam]->stage(block, bytes);
     req->arrival = now_seconds();
     if (m_first_arrival < 0)
         m_first_arrival = req->arrival;
@@ -216,7 +302,10 @@ void Server::worker() {
         std::vector<frost_giant> giants;
         uint64_t launches = 0;
         try {
-            b->process(req->block, req->bytes, req->nread, req->on_device);
+            if (req->slot >= 0)
+                b->process_staged(req->slot, req->bytes, req->nread);
+            else
+                b->process(req->block, req->bytes, req->nread, req->on_device);
             cands    = b->results();
             launches = b->last_launches();
             if (b->has_postprocess())
@@ -237,6 +326,8 @@ void Server::worker() {
             req->giants   = std::move(giants);
             req->finished = true;
             m_busy[beam]  = false;
+            if (req->slot >= 0)
+                b->unstage(req->slot);
             if (status == FROST_OK) {
                 m_latencies.push_back(req->done - req->arrival);
                 m_beam_seconds += static_cast<double>(req->nread) * b->tsamp();
@@ -360,6 +451,37 @@ void Server::set_postprocess(uint32_t beam, const frost_postprocess_config& cfg)
             std::lock_guard<std::mutex> g2(m_mu);
             m_used -= need;
             m_charge[beam] -= need;
+            throw;
+        }
+    } catch (...) {
+        release(beam);
+        throw;
+    }
+    release(beam);
+}
+
+void Server::set_staging(uint32_t beam, uint32_t slots) {
+    std::unique_lock<std::mutex> lk(m_mu);
+    Beam* b = hold(beam, lk);
+    lk.unlock();
+    try {
+        if (slots > 4)
+            invalid("serve: staging slots must be in [0, 4]");
+        const SizeType had  = b->staging_bytes();
+        const SizeType need = static_cast<SizeType>(slots) * b->block_bytes();
+        {
+            std::lock_guard<std::mutex> g2(m_mu);
+            if (need > had && m_budget != 0 && m_used + (need - had) > m_budget)
+                throw Error(FROST_ERR_OUT_OF_MEMORY, "serve: the staging blocks do not fit the memory budget");
+            m_used = m_used - had + need;
+            m_charge[beam] = m_charge[beam] - had + need;
+        }
+        try {
+            b->set_staging(slots);
+        } catch (...) {
+            std::lock_guard<std::mutex> g2(m_mu);
+            m_used = m_used - need + b->staging_bytes();
+            m_charge[beam] = m_charge[beam] - need + b->staging_bytes();
             throw;
         }
     } catch (...) {

@@ -60,7 +60,32 @@ public:
     SizeType device_bytes() const;
     SizeType block_bytes() const;
 
+    /** Input staging (Server::set_staging): `slots` device blocks that host
+     * gulps in pinned memory are copied into when they are submitted, on a
+     * copy stream of their own, so that the copy of a queued gulp overlaps
+     * the work on the gulp before it (0 releases them). */
+    void set_staging(uint32_t slots);
+    SizeType staging_bytes() const { return static_cast<SizeType>(m_stage.size()) * block_bytes(); }
+    /** Starts the copy of a host gulp into a free slot; -1 when none is free
+     * or the block is not in pinned memory (it is then copied when it is
+     * processed). Called with the server's lock held. */
+    int stage(const uint8_t* block, SizeType bytes);
+    /** process() of a staged gulp: the beam's stream waits for its copy. */
+    void process_staged(int slot, SizeType bytes, SizeType nread);
+    /** Frees a slot after process_staged (server's lock held). */
+    void unstage(int slot) { m_stage[static_cast<size_t>(slot)].busy = false; }
+    ~Beam();
+
 private:
+    struct Stage {
+        DeviceBuffer block;
+        cudaEvent_t copied   = nullptr; // the host block is on the device
+        cudaEvent_t consumed = nullptr; // the gulp that read it has run
+        bool busy = false, used = false;
+    };
+    void release_staging();
+    std::vector<Stage> m_stage;
+    cudaStream_t m_copy = nullptr;
     BeamSpec m_spec;
     std::unique_ptr<rfi::Cleaner> m_cleaner;
     std::unique_ptr<fdmt::Engine> m_engine;
@@ -79,6 +104,7 @@ struct Request {
     SizeType bytes;
     SizeType nread;
     bool on_device;
+    int slot = -1;   // staging slot holding the block, or -1
     double arrival;  // steady seconds
     double done = 0;
     bool finished = false;
@@ -100,12 +126,15 @@ public:
     std::vector<frost_candidate> wait(uint64_t ticket, double* latency_s);
     /** As wait, moving out the gulp's post-processed giants instead. */
     std::vector<frost_giant> wait_giants(uint64_t ticket, double* latency_s);
-    /** Attaches a post-processor to an idle beam; its device memory is
-     * charged against the server's budget. */
     /** Caps the beam's level and search kernels at `ctas_per_sm` resident
      * CTAs per SM (fdmt::Engine::set_residency). */
     void set_residency(uint32_t beam, int32_t ctas_per_sm);
+    /** Attaches a post-processor to an idle beam; its device memory is
+     * charged against the server's budget. */
     void set_postprocess(uint32_t beam, const frost_postprocess_config& cfg);
+    /** Gives an idle beam `slots` (0-4) input staging blocks
+     * (Beam::set_staging), charged against the server's budget. */
+    void set_staging(uint32_t beam, uint32_t slots);
     /** drain() of a beam with a post-processor: the final giants. */
     std::vector<frost_giant> drain_giants(uint32_t beam);
     frost_server_stats stats();

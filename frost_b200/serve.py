@@ -112,6 +112,14 @@ class BeamServer:
         kernels share the SMs instead of queueing behind each other."""
         check(lib().frost_server_set_residency(self._h, beam, int(ctas_per_sm)))
 
+    def set_staging(self, beam: int, slots: int) -> None:
+        """Gives `beam` `slots` (0-4) device blocks that pinned host gulps
+        are copied into when they are submitted, so that with more than one
+        gulp in flight a gulp's upload overlaps the work on the one before
+        it (GulpPrefetch's overlap, lib/pipeline/pipeline.cpp:105-262).
+        Charged to the server's memory budget."""
+        check(lib().frost_server_set_staging(self._h, beam, int(slots)))
+
     def set_postprocess(self, beam: int, cfg) -> None:
         """Adds CandidatePostprocessPlan (frost_b200.postprocess.SearchConfig)
         after every gulp's search of `beam`; wait_giants / drain_giants then

@@ -786,6 +786,16 @@ int frost_server_set_postprocess(frost_server* s, uint32_t beam, const frost_pos
  * served beam (between its gulps). */
 int frost_server_set_residency(frost_server* s, uint32_t beam, int ctas_per_sm);
 
+/* GulpPrefetch's overlap of a gulp's upload with the work on the gulp
+ * before it (lib/pipeline/pipeline.cpp:105-262), for served beams: gives the
+ * idle beam `slots` (0-4) device blocks. A host gulp in pinned memory that
+ * is submitted while a slot is free is copied into it at once, on a copy
+ * stream of the beam's own; the beam's gulps still run in submission order.
+ * Other host gulps are copied when they are processed. The blocks are charged
+ * to the server budget (FROST_ERR_OUT_OF_MEMORY if they do not fit); 0
+ * releases them. */
+int frost_server_set_staging(frost_server* s, uint32_t beam, uint32_t slots);
+
 /* frost_server_wait for a beam with a post-processor: the gulp's giants
  * (its raw candidates are dropped). */
 int frost_server_wait_giants(frost_server* s,

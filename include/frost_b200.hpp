@@ -340,6 +340,11 @@ public:
     }
     void reset_stats() { check(frost_server_reset_stats(m_h)); }
 
+    /** Device blocks that pinned host gulps are uploaded into at submit. */
+    void set_staging(uint32_t beam, uint32_t slots) { check(frost_server_set_staging(m_h, beam, slots)); }
+    /** Caps the beam's level and search kernels at `ctas_per_sm` CTAs per SM. */
+    void set_residency(uint32_t beam, int ctas_per_sm) { check(frost_server_set_residency(m_h, beam, ctas_per_sm)); }
+
     /** Adds CandidatePostprocessPlan after every gulp of `beam`. */
     void set_postprocess(uint32_t beam, const frost_postprocess_config& cfg) {
         check(frost_server_set_postprocess(m_h, beam, &cfg));

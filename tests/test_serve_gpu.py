@@ -88,6 +88,41 @@ def test_device_resident_gulps_match_host_gulps():
     srv.close()
 
 
+def test_staged_host_gulps_match_unstaged():
+    """Pinned host gulps uploaded into staging blocks when they are
+    submitted, with every gulp queued at once (more gulps than blocks, so
+    some are copied when processed), give the candidates of the same gulps
+    uploaded when they are processed; the blocks are charged to the budget
+    and given back."""
+    import torch
+
+    from frost_b200.serve import BeamServer
+    rfi, layout, plan, bc = _setup()
+    st = _beam_stream(41)
+    pinned = torch.from_numpy(st.reshape(-1)).pin_memory()
+    gulp_bytes = GULP * NCHANS
+    srv = BeamServer(slots=2)
+    plain, staged = srv.add_beam(rfi, layout, 1.0, plan, bc), srv.add_beam(rfi, layout, 1.0, plan, bc)
+    before = srv.stats().device_bytes
+    srv.set_staging(staged, 2)
+    assert srv.stats().device_bytes == before + 2 * gulp_bytes
+    order = [(g, GULP) for g in range(NGULPS)] + [(g, _nread(g)) for g in range(NGULPS)]
+    tp = [srv.submit(plain, st[g * GULP:(g + 1) * GULP], n) for g, n in order]
+    ts = [srv.submit_ptr(staged, pinned.data_ptr() + g * gulp_bytes, gulp_bytes, n, on_device=False)
+          for g, n in order]
+    total = 0
+    for k in range(len(order)):
+        a, _ = srv.wait(tp[k])
+        b, _ = srv.wait(ts[k])
+        assert np.array_equal(a, b), k
+        total += len(a)
+    assert total > 0
+    assert np.array_equal(srv.drain(plain), srv.drain(staged))
+    srv.set_staging(staged, 0)
+    assert srv.stats().device_bytes == before
+    srv.close()
+
+
 def test_admission_by_device_memory():
     from frost_b200._abi import ERR_OUT_OF_MEMORY
     from frost_b200._lib import FrostError
