@@ -188,6 +188,11 @@ def ncu_traffic_per_launch():
         return None
 
 
+def beam_seed(rank, beam):
+    """Seed of one beam's synthetic gulp (beam 0 of rank 0: 0x46524F5354)."""
+    return 0x46524F5354 ^ (rank << 20) ^ (beam << 8)
+
+
 def make_gulp(seed):
     from frost_b200.synth import config1_gulp, config2_gulp
     if NCHANS == 1024:
@@ -209,12 +214,18 @@ def run_gpu(args):
         import torch.distributed as dist
         dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
 
-    raw_host = make_gulp(0x46524F5354 ^ rank)
-    nbytes = raw_host.size
-    raw_dev = torch.from_numpy(raw_host.reshape(-1)).to(dev)
-    pinned = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-    pinned.copy_(torch.from_numpy(raw_host.reshape(-1)))
-    del raw_host
+    # Every served beam has its own seeded gulp; beam 0's is the one the
+    # plain single-beam paths run, so their candidate lists can be compared.
+    gulps_dev, gulps_pin = [], []
+    for b in range(max(args.beams, 1)):
+        raw_host = make_gulp(beam_seed(rank, b))
+        nbytes = raw_host.size
+        gulps_dev.append(torch.from_numpy(raw_host.reshape(-1)).to(dev))
+        pin = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        pin.copy_(torch.from_numpy(raw_host.reshape(-1)))
+        gulps_pin.append(pin)
+        del raw_host
+    raw_dev, pinned = gulps_dev[0], gulps_pin[0]
     lay = layout()
     plan = plan_for(lay, 0.0, DM_MAX, DEPTH)
 
@@ -244,6 +255,7 @@ def run_gpu(args):
             ncands += res.candidates.size
             d2h += res.candidates.nbytes
             starts[i + 1].record()
+        last = res.candidates.copy()
         torch.cuda.synchronize()
         if sampler:
             sampler.__exit__(None, None, None)
@@ -253,7 +265,7 @@ def run_gpu(args):
         timing = pipe.search.timing()
         launches = timing["total_launches"] + (pipe.rfi.launches() - l0)
         rep = pipe.rfi.report()
-        out = {"total_ms": max_over_ranks(total_ms), "lat": lat, "timing": timing, "tuned": tuned,
+        out = {"total_ms": max_over_ranks(total_ms), "lat": lat, "timing": timing, "tuned": tuned, "last": last,
                "launches": launches, "ncands": ncands, "d2h": d2h,
                "dropped": [res.dropped_global, res.dropped_per_dm],
                "clocks": sampler.summary() if sampler else None,
@@ -290,8 +302,9 @@ def run_gpu(args):
             # sub-band dedup of every gulp's detections, on the device
             for b in beams:
                 srv.set_postprocess(b, postprocess_config(int(bc.max_candidates)))
-        src = raw_dev.data_ptr() if on_device else pinned.data_ptr()
+        src = {b: (gulps_dev[i] if on_device else gulps_pin[i]).data_ptr() for i, b in enumerate(beams)}
         counts = {b: [0, 0] for b in beams}  # candidates (or giants), bytes
+        last = {}
         # Host gulps with --staging N: N in flight per beam, the next ones
         # uploaded into staging blocks while the beam works on the one before.
         depth = 1 if on_device else max(1, args.staging)
@@ -305,9 +318,10 @@ def run_gpu(args):
                 if keep:
                     counts[b][0] += cands.size
                     counts[b][1] += cands.nbytes
+                    last[b] = cands
             pending = []
             for _ in range(n):
-                pending.append(srv.submit_ptr(b, src, nbytes, GULP, on_device))
+                pending.append(srv.submit_ptr(b, src[b], nbytes, GULP, on_device))
                 if len(pending) == depth:
                     collect(pending.pop(0))
             for t in pending:
@@ -339,6 +353,7 @@ def run_gpu(args):
         barrier()
         st = srv.stats()
         out = {"total_ms": max_over_ranks(ev[0].elapsed_time(ev[1])), "beams": len(beams),
+               "last0": last.get(beams[0]) if beams else None,
                "stats": st, "ncands": sum(c[0] for c in counts.values()),
                "d2h": sum(c[1] for c in counts.values()),
                "clocks": sampler.summary() if sampler else None}
@@ -413,6 +428,10 @@ def run_gpu(args):
         "phase_ms_per_step": {k: round(t[k] / args.steps, 3) for k in
                               ("level1_ms", "level_ms", "search_ms", "history_ms", "variance_ms")},
     }
+    from frost_b200.search import candidate_list_diff
+    fp16_vs_fp32 = candidate_list_diff(single32["last"], served["last0"], 7.0)
+    fp16_vs_fp32["what"] = ("served FP16 beam 0 against the plain FP32 path on the same gulp after the same "
+                            "number of gulps, detections above S/N 7 (same plane, DM, width and peak sample)")
     st = served["stats"]
     lat1 = sorted(single16["lat"])
     p = lambda q: lat1[min(len(lat1) - 1, int(round(q * (len(lat1) - 1))))]
@@ -429,7 +448,8 @@ def run_gpu(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 (fp16 plane storage)",
-        "data": "synthetic (seeded filterbank, config-2 noise/RFI/pulse recipe); every beam replays its gulp",
+        "data": ("synthetic (seeded filterbank, 4096-channel noise/RFI/pulse recipe); each served beam has its "
+                 "own seeded gulp, replayed every step (beam 0's is the plain paths' gulp)"),
         "config": {"workload": WORKLOAD, "storage": "fp16", "served_beams_per_gpu": served["beams"],
                    "step": f"one gulp of each of the {served['beams']} served beams",
                    "served_tile_nsamps": args.served_tile or GULP,
@@ -460,6 +480,7 @@ def run_gpu(args):
             "what": "the same served beams with frost's per-gulp post-processing (clustering, DM wings, carry, "
                     "sub-band dedup) on the device after each search"},
         "served_vs_plain_fp32": round(value / plain32, 3),
+        "fp16_vs_fp32": fp16_vs_fp32,
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
                 "h2d_bytes_per_step": nbytes * e2e["beams"],
                 "d2h_bytes_per_step": int(e2e["d2h"] / args.steps),
@@ -486,22 +507,39 @@ def run_gpu(args):
 CPU_SAMPLE = 16384  # rows of the gulp timed on the host cores
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_baseline(sample=CPU_SAMPLE, steps=1):
     """The reference's CPU RFI cleaner (oracle/_ref, shipped -O3 -ffast-math
     build) plus this project's CPU port of the FDMT + boxcar search
     (oracle/cpu_fdmt.c; the reference's own engine, dmt, is not available)
     on a `sample`-row block of the same recipe; beam-s/s of that work."""
-    from frost_b200.dedisp import band_edges, generate_dm_list
-    from frost_b200.pipeline import plan_for
+    from frost_b200.config import DedispPlanConfig
     from frost_b200.synth import config2_gulp
     from oracle import ref
     from oracle.fdmt import cpu_search, widths
 
     raw = config2_gulp(seed=0x46524F5354, nsamps=sample, n_pulses=2).data
     lay = layout(sample)
-    plan = plan_for(layout(), 0.0, DM_MAX, DEPTH)
-    f_min, f_max = band_edges(plan)
-    dms = generate_dm_list(plan)
+    full = layout()
+    # frost's plan arguments (make_dedisp_plan_config, lib/pipeline/pipeline.cpp:290-304);
+    # the DM list and band edges come from the reference's own lib/dedisp
+    # compiled into oracle/_ref, so this leg maps none of this repo's libraries
+    plan = DedispPlanConfig(nchans=full.nchans, dt=float(full.tsamp), f0=float(full.f0), df=float(full.df),
+                            dm_min=0.0, dm_max=DM_MAX, dm_pulse_width=40.0, dm_tol=1.25,
+                            block_nsamps=full.max_nsamps, subband_depth=DEPTH)
+    f_min, f_max = ref.fdmt_band_edges(plan)
+    dms = ref.generate_dm_list(plan)
     ws = widths(MAX_BOXCAR, 2.0)
     fast = ref.available(fast=True)
     cleaner = ref.RefRFICleaner(rfi_config(), lay, 2.0, fast=fast)
@@ -516,7 +554,7 @@ def cpu_baseline(sample=CPU_SAMPLE, steps=1):
         t_fdmt += t2 - t1
     beam_s = steps * sample * TSAMP
     return {"value": round(beam_s / (t_rfi + t_fdmt), 4), "unit": UNIT,
-            "cores": os.cpu_count(), "kind": "port",
+            "cores": os.cpu_count(), "cpu_model": cpu_model(), "kind": "port",
             "sample": (f"{steps} x {sample} rows x 4096 ch: reference RFICleaner "
                        f"({'shipped -ffast-math' if fast else 'strict'} build of its own sources) "
                        f"{t_rfi:.2f} s + CPU port of FDMT+boxcar (11 planes, widths 1-256, zero "
@@ -539,7 +577,7 @@ def run_reference(args):
             "config": {"workload": WORKLOAD + f"; each step a {CPU_SAMPLE}-row sample",
                        "parallelism": "host cores"},
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": os.cpu_count(),
-                             "kind": "port", "sample": cb["sample"] if cb else ""},
+                             "cpu_model": cb["cpu_model"], "kind": "port", "sample": cb["sample"] if cb else ""},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -186,6 +186,11 @@ int frost_rfi_execute_normalized(frost_rfi* rfi, const uint8_t* block, size_t bl
     return guarded([&] {
         if (rfi == nullptr)
             invalid("frost_rfi_execute_normalized: null handle");
+        // frost's device RFI path takes the pipeline's stream and refuses the
+        // null stream (lib/cuda/device_rfi_detail.cuh:77-83): a device block
+        // is read only after the work queued on the caller's stream.
+        if (block_on_device != 0 && stream == nullptr)
+            invalid("RFICleaner: a device block requires the pipeline stream, not the null stream");
         const float* out = rfi->impl.execute_normalized(block, block_bytes, nsamps,
                                                         block_on_device != 0,
                                                         static_cast<cudaStream_t>(stream));
@@ -252,6 +257,8 @@ int frost_rfi_normalize_static(const frost_block_layout* layout, float baseline_
     return guarded([&] {
         if (layout == nullptr)
             invalid("frost_rfi_normalize_static: null layout");
+        if (stream == nullptr)
+            invalid("normalize_static: requires the caller's stream, not the null stream");
         fb::rfi::normalize_static(*layout, baseline_length, block, block_bytes, nsamps, out,
                                   out_count, static_cast<cudaStream_t>(stream));
     });
@@ -262,6 +269,14 @@ int frost_rfi_launch_count(const frost_rfi* rfi, uint64_t* launches) {
         if (rfi == nullptr || launches == nullptr)
             invalid("frost_rfi_launch_count: null argument");
         *launches = rfi->impl.launches();
+    });
+}
+
+int frost_rfi_get_stream(const frost_rfi* rfi, void** stream) {
+    return guarded([&] {
+        if (rfi == nullptr || stream == nullptr)
+            invalid("frost_rfi_get_stream: null argument");
+        *stream = static_cast<void*>(rfi->impl.stream());
     });
 }
 
@@ -350,6 +365,8 @@ int frost_search_execute(frost_search* s, const float* waterfall, size_t nsamps,
     return guarded([&] {
         if (s == nullptr)
             invalid("frost_search_execute: null handle");
+        if (on_device != 0 && stream == nullptr)
+            invalid("search: a device waterfall requires the pipeline stream, not the null stream");
         s->impl.execute(waterfall, nsamps, on_device != 0, mask, static_cast<cudaStream_t>(stream));
     });
 }
@@ -676,6 +693,14 @@ int frost_search_get_residency(const frost_search* s, int* ctas_per_sm) {
         if (s == nullptr || ctas_per_sm == nullptr)
             invalid("frost_search_get_residency: null argument");
         *ctas_per_sm = s->impl.residency();
+    });
+}
+
+int frost_search_get_stream(const frost_search* s, void** stream) {
+    return guarded([&] {
+        if (s == nullptr || stream == nullptr)
+            invalid("frost_search_get_stream: null argument");
+        *stream = static_cast<void*>(s->impl.stream());
     });
 }
 

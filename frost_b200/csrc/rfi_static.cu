@@ -14,8 +14,10 @@
 // The scratch is a file-scope static __device__ array of kScratchFloats
 // floats (32 MiB + 256 KiB): every GPU that loads this module holds it until
 // the process exits. Its device address is looked up once per device, on the
-// first call made with that device current; that first call should come
-// before any stream capture. Every call shares the one array, so calls whose
+// first call made with that device current; under lazy module loading that
+// lookup is also when the driver loads this module onto the device and sets
+// the array up, so callers make that first call at start-up, before any
+// stream capture. Every call shares the one array, so calls whose
 // work overlaps on the GPU (different streams, or other threads) race and
 // must be serialised by the caller; the array keeps the last call's contents
 // and the call clears what must start at zero. No cudaMalloc, cudaFree or

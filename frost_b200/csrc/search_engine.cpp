@@ -54,6 +54,7 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     DeviceGuard g(device);
     FB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, device));
     FB_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
+    FB_CUDA(cudaEventCreateWithFlags(&m_order, cudaEventDisableTiming));
     cudaStream_t s = m_stream;
 
     const int32_t C = m_plan.nchans();
@@ -488,6 +489,8 @@ Engine::~Engine() {
             cudaGraphExecDestroy(m_graph);
         for (auto e : m_event_pool)
             cudaEventDestroy(e);
+        if (m_order != nullptr)
+            cudaEventDestroy(m_order);
         cudaStreamDestroy(m_stream);
     }
 }
@@ -683,11 +686,8 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
         orm[c] = (cur[c] | m_mask[c]) ? 1 : 0;
     // Order the caller's stream before the engine's.
     if (stream != nullptr && stream != s) {
-        cudaEvent_t ev;
-        FB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        FB_CUDA(cudaEventRecord(ev, stream));
-        FB_CUDA(cudaStreamWaitEvent(s, ev, 0));
-        FB_CUDA(cudaEventDestroy(ev));
+        FB_CUDA(cudaEventRecord(m_order, stream));
+        FB_CUDA(cudaStreamWaitEvent(s, m_order, 0));
     }
     timed(kVariance, s, [&] { update_variance(cur, orm); });
 

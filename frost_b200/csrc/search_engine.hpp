@@ -67,6 +67,7 @@ private:
     frost_boxcar_config m_cfg;
     int m_device;
     cudaStream_t m_stream = nullptr;
+    cudaEvent_t m_order   = nullptr; // orders the caller's stream before the engine's
     bool m_fp16;
     int64_t m_tile = 0, m_ncols = 0;
     // Per stored level: history columns before base (the level's own

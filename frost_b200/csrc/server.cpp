@@ -218,6 +218,7 @@ uint32_t Server::add_beam(const BeamSpec& spec) {
     m_beams[id]       = std::move(beam);
     m_queue[id];
     m_busy[id]   = false;
+    m_held[id]   = false;
     m_charge[id] = need;
     return id;
 }
@@ -233,6 +234,7 @@ void Server::remove_beam(uint32_t beam) {
     m_charge.erase(beam);
     m_queue.erase(beam);
     m_busy.erase(beam);
+    m_held.erase(beam);
 }
 
 uint64_t Server::submit(uint32_t beam, const uint8_t* block, SizeType bytes, SizeType nread,
@@ -249,7 +251,10 @@ uint64_t Server::submit(uint32_t beam, const uint8_t* block, SizeType bytes, Siz
     req->bytes   = bytes;
     req->nread     = nread;
     req->on_device = on_device;
-    if (!on_device)
+    // Staging touches the beam's slots and copy stream, which a setter
+    // holding the beam may be replacing; such a gulp is uploaded when it is
+    // processed instead.
+    if (!on_device && !m_held[beam])
         req->slot = m_beams[beam]->stage(block, bytes);
     req->arrival = now_seconds();
     if (m_first_arrival < 0)
@@ -371,6 +376,7 @@ Beam* Server::hold(uint32_t beam, std::unique_lock<std::mutex>& lk) {
         invalid("serve: unknown beam");
     m_done_cv.wait(lk, [&] { return !m_busy[beam] && m_queue[beam].empty(); });
     m_busy[beam] = true;
+    m_held[beam] = true;
     return it->second.get();
 }
 
@@ -378,6 +384,7 @@ void Server::release(uint32_t beam) {
     {
         std::lock_guard<std::mutex> lk(m_mu);
         m_busy[beam] = false;
+        m_held[beam] = false;
     }
     m_work_cv.notify_all();
 }

@@ -152,6 +152,7 @@ private:
     std::map<uint32_t, std::unique_ptr<Beam>> m_beams;
     std::map<uint32_t, std::deque<uint64_t>> m_queue; // per-beam FIFO of tickets
     std::map<uint32_t, bool> m_busy;
+    std::map<uint32_t, bool> m_held; // a setter is reconfiguring the beam: submits do not stage
     std::map<uint32_t, SizeType> m_charge; // device bytes charged at admission
     std::map<uint64_t, std::shared_ptr<Request>> m_requests;
     std::vector<double> m_latencies;

@@ -65,11 +65,14 @@ class GulpPipeline:
     def execute_device(self, raw_ptr: int, nread: int, on_device: bool = True,
                        stream: Optional[int] = None) -> CandidateResult:
         """One gulp whose packed block (block rows, `nread` valid) is at
-        raw_ptr (device, or pinned host when on_device is False)."""
+        raw_ptr (device, or pinned host when on_device is False). A device
+        block is read after the work queued on `stream` (default: the
+        cleaner's own stream, so the block must be complete)."""
         nbytes = self.block * self.layout.row_bytes
-        wf = self.rfi.execute_normalized_device(raw_ptr, nbytes, nread, on_device=on_device,
-                                                stream=stream)
-        res = self.search.execute_device(wf, self.block, self._fdmt_mask())
+        s = stream or self.rfi.stream()
+        wf = self.rfi.execute_normalized_device(raw_ptr, nbytes, nread, on_device=on_device, stream=s)
+        # the engine reads the waterfall after the cleaner's work on `s`
+        res = self.search.execute_device(wf, self.block, self._fdmt_mask(), stream=s)
         self._account(nread)
         self._last_nread = nread
         if self.post is not None:

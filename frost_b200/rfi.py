@@ -51,10 +51,21 @@ class RFICleaner:
         except Exception:
             pass
 
+    def stream(self) -> int:
+        """The cleaner's own CUDA stream handle."""
+        s = C.c_void_p()
+        check(lib().frost_rfi_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def execute_normalized_device(self, block_ptr: int, block_bytes: int, nsamps: int = 0,
                                   on_device: bool = True, stream: Optional[int] = None) -> int:
         """Runs on a block at `block_ptr` (device pointer when on_device, else a
-        host address); returns the device pointer of the normalized waterfall."""
+        host address); returns the device pointer of the normalized waterfall
+        (complete on return). A device block is read after the work queued
+        on `stream`; without one it is read on the cleaner's own stream, so
+        its writes must already be complete."""
+        if on_device and not stream:
+            stream = self.stream()
         out = C.c_void_p()
         check(lib().frost_rfi_execute_normalized(self._h, C.c_void_p(block_ptr), block_bytes, nsamps,
                                                  1 if on_device else 0,

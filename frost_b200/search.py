@@ -120,7 +120,18 @@ class FDMTBoxcar:
                                          wf.shape[1], 0, mp, None))
         return self.result()
 
+    def stream(self) -> int:
+        """The engine's own CUDA stream handle."""
+        s = C.c_void_p()
+        check(lib().frost_search_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def execute_device(self, ptr: int, nsamps: int, mask=None, stream: Optional[int] = None):
+        """A device waterfall, read after the work queued on `stream`;
+        without one it is read on the engine's own stream, so its writes
+        must already be complete."""
+        if not stream:
+            stream = self.stream()
         keep, mp = self._mask_ptr(mask)
         check(lib().frost_search_execute(self._h, C.cast(C.c_void_p(ptr), C.POINTER(C.c_float)),
                                          nsamps, 1, mp, C.c_void_p(stream) if stream else None))
@@ -235,3 +246,50 @@ class FDMTBoxcar:
         check(lib().frost_search_plane_data(self._h, plane, out.ctypes.data_as(C.POINTER(C.c_float)),
                                             out.size))
         return out
+
+
+def candidate_list_diff(ref: np.ndarray, other: np.ndarray, snr_min: float = 7.0) -> dict:
+    """Compares two candidate lists of the same stream (for example FP16
+    plane storage against FP32) above `snr_min`.
+
+    A detection is keyed by (subband_level, subband_idx, dm_idx, filter_idx).
+    A detection of either list at S/N >= snr_min is `matched` when the other
+    list (at any S/N it reports, down to its detection threshold) has the
+    same key and the same peak sample, `moved` when the other list's
+    detection of that key covers the same run with a different peak (a near
+    tie inside the run), and `only_ref` / `only_other` otherwise.
+    `max_snr_rel_err` is the largest relative S/N difference over matched
+    and moved pairs; `edge` counts matched pairs with one side below
+    snr_min (a threshold crossing, not a missing detection)."""
+    def index(cs):
+        out = {}
+        for c in cs:
+            k = (int(c["subband_level"]), int(c["subband_idx"]), int(c["dm_idx"]), int(c["filter_idx"]))
+            out.setdefault(k, []).append((int(c["begin_sample"]), int(c["end_sample"]),
+                                          int(c["peak_sample"]), float(c["snr"])))
+        return out
+    a, b = index(ref), index(other)
+    res = {"snr_min": snr_min, "n_ref": 0, "n_other": 0, "matched": 0, "moved": 0, "only_ref": 0,
+           "only_other": 0, "edge": 0, "max_snr_rel_err": 0.0}
+
+    def walk(x, y, count_key, only_key, pairs):
+        for k, lst in x.items():
+            for beg, end, pk, snr in lst:
+                if snr < snr_min:
+                    continue
+                res[count_key] += 1
+                same = [d for d in y.get(k, []) if d[2] == pk]
+                hit = same or [d for d in y.get(k, []) if d[0] <= pk <= d[1] or beg <= d[2] <= end]
+                if not hit:
+                    res[only_key] += 1
+                    continue
+                # the second walk counts only pairs the first one skipped
+                # (the reference side below snr_min)
+                if pairs or hit[0][3] < snr_min:
+                    res["matched" if same else "moved"] += 1
+                    res["max_snr_rel_err"] = max(res["max_snr_rel_err"], abs(hit[0][3] - snr) / abs(snr))
+                    res["edge"] += int(hit[0][3] < snr_min)
+    walk(a, b, "n_ref", "only_ref", True)
+    walk(b, a, "n_other", "only_other", False)
+    res["identical"] = res["only_ref"] == 0 and res["only_other"] == 0 and res["moved"] == 0
+    return res

@@ -58,6 +58,27 @@ def dispersion_delay(dm, f, f_ref, tsamp):
     return KDM * dm * (1.0 / np.square(f) - 1.0 / (f_ref * f_ref)) / tsamp
 
 
+_CHUNK_ROWS = 8192
+
+
+def _chunks(nsamps):
+    return [(a, min(a + _CHUNK_ROWS, nsamps)) for a in range(0, nsamps, _CHUNK_ROWS)]
+
+
+def _parallel(fn, items):
+    """Runs fn over items on host threads (numpy's random fills and ufuncs
+    release the GIL); the result does not depend on the thread count."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    workers = max(1, min(len(items), os.cpu_count() or 1))
+    if workers == 1:
+        for it in items:
+            fn(it)
+        return
+    with ThreadPoolExecutor(workers) as ex:
+        list(ex.map(fn, items))
+
+
 def make_filterbank(nchans: int, nsamps: int, fch1: float, foff: float, tsamp: float,
                     seed: int, dtype: str = "uint8", mean: float = 128.0, sd: float = 16.0,
                     pulses: Optional[List[Pulse]] = None, n_pulses: int = 0,
@@ -67,19 +88,31 @@ def make_filterbank(nchans: int, nsamps: int, fch1: float, foff: float, tsamp: f
                     n_dropouts: int = 0, dropout_len: int = 512,
                     first_sample: int = 0) -> Filterbank:
     """A seeded filterbank. `first_sample` offsets pulse times so successive
-    gulps of one stream can be generated independently."""
+    gulps of one stream can be generated independently. The noise of each
+    8192-row chunk comes from its own generator spawned from `seed`, so the
+    output is the same however many threads fill it."""
     rng = np.random.default_rng(seed)
-    noise = rng.standard_normal((nsamps, nchans), dtype=np.float32)
-    noise *= sd
-    noise += mean
+    chunks = _chunks(nsamps)
+    streams = np.random.SeedSequence(seed).spawn(len(chunks))
+    noise = np.empty((nsamps, nchans), np.float32)
     freqs = fch1 + foff * np.arange(nchans)
     f_top = freqs.max()
     rfi_channels = np.zeros(0, np.int64)
     if rfi_channel_fraction > 0:
         k = int(round(rfi_channel_fraction * nchans))
         rfi_channels = np.sort(rng.choice(nchans, size=k, replace=False))
-        extra = np.sqrt(rfi_var_factor - 1.0) * sd
-        noise[:, rfi_channels] += extra * rng.standard_normal((nsamps, k), dtype=np.float32)
+    extra = np.sqrt(rfi_var_factor - 1.0) * sd if rfi_channels.size else 0.0
+
+    def fill(i):
+        a, b = chunks[i]
+        g = np.random.default_rng(streams[i])
+        part = noise[a:b]
+        g.standard_normal(out=part, dtype=np.float32)
+        part *= sd
+        part += mean
+        if rfi_channels.size:
+            part[:, rfi_channels] += extra * g.standard_normal((b - a, rfi_channels.size), dtype=np.float32)
+    _parallel(fill, range(len(chunks)))
     if pulses is None:
         pulses = []
         delay_max = dispersion_delay(dm_range[1], freqs.min(), f_top, tsamp)
@@ -120,12 +153,20 @@ def make_filterbank(nchans: int, nsamps: int, fch1: float, foff: float, tsamp: f
     dropouts = []
     for _ in range(n_dropouts):
         start = int(rng.integers(0, max(nsamps - dropout_len, 1)))
-        noise[start:start + dropout_len, :] = 0.0 if dtype == "uint8" else 0.0
+        noise[start:start + dropout_len, :] = 0.0
         dropouts.append((start, dropout_len))
     if dtype == "uint8":
-        data = np.clip(np.rint(noise), 0, 255).astype(np.uint8)
+        data = np.empty((nsamps, nchans), np.uint8)
+
+        def quantise(i):
+            a, b = chunks[i]
+            part = noise[a:b]
+            np.rint(part, out=part)
+            np.clip(part, 0, 255, out=part)
+            data[a:b] = part
+        _parallel(quantise, range(len(chunks)))
     elif dtype == "float32":
-        data = noise.astype(np.float32, copy=False)
+        data = noise
     else:
         raise ValueError(dtype)
     return Filterbank(data, fch1, foff, tsamp, pulses, rfi_channels, bursts, dropouts)

@@ -8,7 +8,10 @@
  * throws; frost_last_error() gives the calling thread's last message.
  * Arguments are validated before any state changes. Handles own their device
  * buffers; device pointers they return stay valid until the next call on the
- * same handle. A NULL stream argument selects the handle's own stream.
+ * same handle. Device inputs are read in the order of the caller's stream,
+ * which must not be NULL (frost refuses the null stream for device input,
+ * lib/cuda/device_rfi_detail.cuh:77-83); with host inputs a NULL stream
+ * selects the handle's own stream.
  *
  * Reference interfaces each entry point replaces are cited as
  * file:line within pravirkr/frost.
@@ -179,10 +182,10 @@ int frost_rfi_destroy(frost_rfi* rfi);
  * order, low frequency first, `capacity = block_bytes / row_bytes` samples
  * per channel, masked channels and padding zero. `block` is host memory
  * (copied to the device inside the call) when `block_on_device` is 0, else a
- * device pointer. `nsamps` = 0 uses every row. The device result is returned
- * in `*out_device` (valid until the next call); the call does not
- * synchronise the stream except to read back the small per-gulp statistics
- * the flag logic needs. */
+ * device pointer, read after the work already queued on `stream` (which
+ * must then not be NULL: FROST_ERR_INVALID_ARGUMENT). `nsamps` = 0 uses
+ * every row. The device result is returned in `*out_device` (valid until the
+ * next call) and is complete when the call returns. */
 int frost_rfi_execute_normalized(frost_rfi* rfi,
                                  const uint8_t* block,
                                  size_t block_bytes,
@@ -211,6 +214,11 @@ int frost_rfi_memory_usage(const frost_rfi* rfi, size_t* bytes);
 /* Kernels this cleaner has launched since it was created. */
 int frost_rfi_launch_count(const frost_rfi* rfi, uint64_t* launches);
 
+/* No counterpart in the reference. The cleaner's own stream (a
+ * cudaStream_t): a caller that writes a device block on it, or that hands
+ * the normalised waterfall to frost_search_execute, passes it as `stream`. */
+int frost_rfi_get_stream(const frost_rfi* rfi, void** stream);
+
 /* No counterpart in the reference. An allocation-free form of
  * frost_rfi_execute_normalized for callers that cannot call cudaMalloc once
  * they are processing (a real-time consumer that sizes all device memory at
@@ -226,9 +234,13 @@ int frost_rfi_launch_count(const frost_rfi* rfi, uint64_t* launches);
  * array in the library (held by every GPU that loads it until exit), limiting
  * windows x channels to 2684; larger blocks are rejected with
  * FROST_ERR_INVALID_ARGUMENT. The first call on a device looks up the
- * array's address and should come before any stream capture. All calls
- * share the array: calls that overlap on the GPU race. Synchronises
- * `stream` (NULL = the default stream) before returning. */
+ * array's address, which also makes the driver load this library's device
+ * code onto that device and set the array up (under CUDA's default lazy
+ * module loading that is driver-side memory too), so make one call at
+ * start-up, before processing begins, and before any stream capture; later
+ * calls allocate nothing. All calls share the array: calls that overlap on
+ * the GPU race. The block is read after the work queued on `stream`, which
+ * must not be NULL; the call synchronises `stream` before returning. */
 int frost_rfi_normalize_static(const frost_block_layout* layout,
                                float baseline_length,
                                const uint8_t* block,
@@ -395,8 +407,9 @@ int frost_search_destroy(frost_search* s);
 /* FDMTBoxcar::execute (host span: lib/pipeline/pipeline.cpp:608; device
  * span + copy_result: :603-605). `waterfall` is [nchans][nsamps] float32,
  * low frequency first, nsamps <= block_nsamps, on the device when
- * `on_device` else host memory. `mask` (nchans bytes, FDMT order) replaces
- * the constructor mask for this and later calls; NULL keeps the current one.
+ * `on_device` (read after the work queued on `stream`, which must then not
+ * be NULL) else host memory. `mask` (nchans bytes, FDMT order) replaces the
+ * constructor mask for this and later calls; NULL keeps the current one.
  * Results are complete when the call returns. */
 int frost_search_execute(frost_search* s,
                          const float* waterfall,
@@ -488,6 +501,10 @@ typedef struct {
  * plane capture launch directly. Results are the same either way. */
 int frost_search_use_graphs(frost_search* s, int enable);
 
+/* No counterpart in the reference. The engine's own stream (a
+ * cudaStream_t), on which it runs every launch of a gulp. */
+int frost_search_get_stream(const frost_search* s, void** stream);
+
 /* No counterpart in the reference. Measures this geometry's FDMT launch
  * shapes (fused two-level steps with 2, 3 or 4 bulk-copy stages, or single
  * levels; 4, 8, 16, 32, 64 or 128 tiles of 2048 samples per level-kernel CTA) with
@@ -577,7 +594,9 @@ int frost_server_remove_beam(frost_server* s, uint32_t beam);
 
 /* Queues one gulp (a block of max_nsamps rows, `nread` valid) that is in
  * host memory, or in the server device's memory when on_device is non-zero;
- * the block must stay valid until frost_server_wait returns for the ticket. */
+ * the block must stay valid until frost_server_wait returns for the ticket.
+ * The server reads it on its own streams, so a device block must be
+ * complete when it is submitted (its writes synchronised). */
 int frost_server_submit(frost_server* s,
                         uint32_t beam,
                         const uint8_t* block,

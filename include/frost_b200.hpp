@@ -116,6 +116,13 @@ public:
         return out;
     }
 
+    /** The cleaner's own stream (a cudaStream_t). */
+    void* stream() const {
+        void* s = nullptr;
+        check(frost_rfi_get_stream(m_h, &s));
+        return s;
+    }
+
     /** 1 = good, 0 = masked, in the cleaner's (data) channel order. */
     std::span<const uint8_t> channel_mask() {
         m_mask.resize(m_nchans);
@@ -183,10 +190,19 @@ public:
         return result();
     }
 
-    /** Device waterfall [nchans][nsamps] on `stream`. */
+    /** The engine's own stream (a cudaStream_t). */
+    void* stream() const {
+        void* s = nullptr;
+        check(frost_search_get_stream(m_h, &s));
+        return s;
+    }
+
+    /** Device waterfall [nchans][nsamps], read after the work queued on
+     * `stream` (default: the engine's own stream; the waterfall must then
+     * be complete). */
     CandidateResult execute_device(const float* waterfall, size_t nsamps,
                                    std::span<const uint8_t> mask = {}, void* stream = nullptr) {
-        check(frost_search_execute(m_h, waterfall, nsamps, 1, mask_ptr(mask), stream));
+        check(frost_search_execute(m_h, waterfall, nsamps, 1, mask_ptr(mask), stream ? stream : this->stream()));
         return result();
     }
 
@@ -255,9 +271,12 @@ public:
     /** One gulp at a host or device pointer. */
     CandidateResult execute_ptr(const uint8_t* block, size_t bytes, size_t nread, bool on_device,
                                 void* stream) {
-        const float* wf = m_rfi.execute_normalized_device(block, bytes, nread, on_device, stream);
+        // a device block without a stream is read on the cleaner's stream;
+        // the engine reads the waterfall after the cleaner's work
+        void* s         = stream != nullptr ? stream : m_rfi.stream();
+        const float* wf = m_rfi.execute_normalized_device(block, bytes, nread, on_device, s);
         const auto mask = fdmt_order(m_rfi.channel_mask());
-        auto res        = m_search.execute_device(wf, m_layout.max_nsamps, mask, stream);
+        auto res        = m_search.execute_device(wf, m_layout.max_nsamps, mask, s);
         m_read += nread;
         const uint64_t previous = m_read - nread;
         if (m_read > m_max_delay)

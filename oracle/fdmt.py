@@ -44,6 +44,8 @@ def lib():
         L.oracle_dedisperse.argtypes = [f64p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, i64p, i64p,
                                         C.c_int64, f64p]
         L.oracle_variance.argtypes = [i64p, C.c_int64, C.c_int64, u8p, C.c_int64, C.c_int, f64p]
+        L.oracle_dedisperse_rows.argtypes = [C.POINTER(C.c_float), C.c_int64, C.c_int64, C.c_int64,
+                                             C.c_int64, i64p, i64p, C.c_int64, f64p]
         L.cpu_fdmt_search.restype = C.c_int64
         L.cpu_fdmt_search.argtypes = [C.POINTER(C.c_float), C.c_int64, C.c_int64, C.c_double,
                                       C.c_double, C.c_double, C.POINTER(C.c_float), C.c_int64,
@@ -134,16 +136,34 @@ class Oracle:
         bw = (self.f_max - self.f_min) / self.nchans
         return self.f_min + c * bw
 
-    def geometry(self, band: Band):
+    def geometry(self, band: Band, rows=None):
+        """Per-channel shifts and window lengths of the band's rows (all, or
+        the selected row indices), each [rows][b - a]."""
         n = band.b - band.a
-        rows = band.delays.size
-        shifts = np.zeros(rows * n, np.int64)
-        lens = np.zeros(rows * n, np.int64)
+        delays = np.ascontiguousarray(band.delays if rows is None else band.delays[np.asarray(rows)], np.int64)
+        nr = delays.size
+        shifts = np.zeros(nr * n, np.int64)
+        lens = np.zeros(nr * n, np.int64)
         rc = lib().oracle_row_geometry(self.nchans, self.f_min, self.f_max, band.a, band.m, band.b,
-                                       _p(band.delays, C.c_int64), rows, _p(shifts, C.c_int64),
+                                       _p(delays, C.c_int64), nr, _p(shifts, C.c_int64),
                                        _p(lens, C.c_int64))
         assert rc == 0
-        return shifts.reshape(rows, n), lens.reshape(rows, n)
+        return shifts.reshape(nr, n), lens.reshape(nr, n)
+
+    def dedisperse_rows(self, stream: np.ndarray, band: Band, rows) -> np.ndarray:
+        """Selected rows of a band from a float32 [nchans][T] stream (masked
+        channels already zero) -> [len(rows)][T] FP64, without an FP64 copy
+        of the stream (sliding FP64 windows)."""
+        x = np.ascontiguousarray(stream, np.float32)
+        T = x.shape[1]
+        shifts, lens = self.geometry(band, rows)
+        out = np.zeros((shifts.shape[0], T), np.float64)
+        shifts, lens = np.ascontiguousarray(shifts), np.ascontiguousarray(lens)
+        rc = lib().oracle_dedisperse_rows(_p(x, C.c_float), self.nchans, T, band.a, band.b,
+                                          _p(shifts, C.c_int64), _p(lens, C.c_int64), shifts.shape[0],
+                                          _p(out, C.c_double))
+        assert rc == 0
+        return out
 
     def dedisperse(self, stream: np.ndarray, band: Band) -> np.ndarray:
         """stream: [nchans][T] (masked channels already zero) -> [rows][T] FP64."""
@@ -157,20 +177,24 @@ class Oracle:
         assert rc == 0
         return out
 
-    def variance(self, band: Band, mask: np.ndarray, W: int) -> np.ndarray:
-        _, lens = self.geometry(band)
+    def variance(self, band: Band, mask: np.ndarray, W: int, rows=None) -> np.ndarray:
+        _, lens = self.geometry(band, rows)
         m = np.ascontiguousarray(mask[band.a:band.b], np.uint8)
-        out = np.zeros(band.delays.size, np.float64)
+        out = np.zeros(lens.shape[0], np.float64)
         lens = np.ascontiguousarray(lens)
         rc = lib().oracle_variance(_p(lens, C.c_int64), lens.shape[0], lens.shape[1], _p(m, C.c_uint8),
                                    W, int(self.trapezoid), _p(out, C.c_double))
         assert rc == 0
         return out
 
-    def search(self, stream: np.ndarray, gulp: int, masks: List[np.ndarray]):
+    def search(self, stream: np.ndarray, gulp: int, masks: List[np.ndarray], rows=None, data=None):
         """Searches the whole stream ([nchans][T], T a multiple of `gulp`,
         gulp g under masks[g] with its masked channels already zero).
-        Returns a list of dicts sorted like the engine's results."""
+        `rows` (optional) maps a band index to the row indices to search;
+        other bands are skipped. `data` (optional) maps a band index to
+        those rows' FP64 values already computed by dedisperse_rows.
+        Returns a list of dicts sorted like the engine's results, with
+        dm_idx the row index within the band."""
         T = stream.shape[1]
         ngulps = T // gulp
         assert ngulps * gulp == T and len(masks) == ngulps
@@ -179,27 +203,44 @@ class Oracle:
             or_gulp[g] = np.any(masks[g] != masks[g - 1])
         ws = np.array(self.widths, np.int64)
         out = []
-        for band in self.bands:
-            rows = self.dedisperse(stream, band)
-            nr = rows.shape[0]
+        for bi, band in enumerate(self.bands):
+            sel = None
+            if rows is not None:
+                if bi not in rows:
+                    continue
+                sel = np.asarray(sorted(set(int(r) for r in rows[bi])), np.int64)
+                band = Band(band.a, band.m, band.b, band.level, band.idx, band.staggered,
+                            band.delays[sel], band.dm[sel], band.dm_index[sel])
+                if data is not None and bi in data:
+                    rows_data = np.ascontiguousarray(data[bi], np.float64)
+                    assert rows_data.shape == (sel.size, T)
+                else:
+                    rows_data = self.dedisperse_rows(stream, self.bands[bi], sel)
+            else:
+                rows_data = self.dedisperse(stream, band)
             # variance per gulp mask: the search uses one table per gulp, so
             # run gulp by gulp when masks differ
             var_by_mask = {}
 
-            def var_of(mask):
+            def var_of(mask, band=band, bi=bi, sel=sel):
                 key = mask.tobytes()
                 if key not in var_by_mask:
-                    var_by_mask[key] = np.stack([self.variance(band, mask, W) for W in self.widths], 1)
+                    var_by_mask[key] = np.stack([self.variance(self.bands[bi], mask, W, sel)
+                                                 for W in self.widths], 1)
                 return var_by_mask[key]
             if all(np.array_equal(m, masks[0]) for m in masks):
                 v = np.ascontiguousarray(var_of(masks[0]))
-                out += self._search_rows(rows, band, ws, v, v, T, or_gulp, ngulps * gulp)
+                found = self._search_rows(rows_data, band, ws, v, v, T, or_gulp, ngulps * gulp)
             else:
                 # gulp-wise: S/N in gulp g uses masks[g] (OR with masks[g-1]
                 # at the start); runs are carried by searching the stream once
                 # per gulp-mask with the other gulps' S/N suppressed is not
                 # equivalent, so assemble per-gulp S/N tables instead.
-                out += self._search_mixed(rows, band, ws, masks, gulp, or_gulp, var_of)
+                found = self._search_mixed(rows_data, band, ws, masks, gulp, or_gulp, var_of)
+            if sel is not None:
+                for c in found:
+                    c["dm_idx"] = int(sel[c["dm_idx"]])
+            out += found
         return out
 
     def _search_rows(self, rows, band, ws, var, var_or, T, or_gulp, gulp):

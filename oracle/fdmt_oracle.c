@@ -127,32 +127,110 @@ static void weights(int64_t W, int trap, double* w) {
     }
 }
 
+/* Sum over k of m(k)^2, m = the width-W weights convolved with an L-sample
+ * box: m(k) = sum of w[i] over max(0, k-L+1) <= i <= min(W-1, k), for
+ * k = 0 .. W+L-2. For L >= W the middle L-W+1 values all equal sum(w), so
+ * only the two ramps are summed term by term. Every term is a multiple of
+ * 1/4 and every partial sum stays far below 2^51, so the result is exact and
+ * independent of the summation order. */
+static double box_sq(int64_t L, int64_t W, const double* wpre) {
+    double v = 0.0;
+#define MULT(k) (wpre[((k) < W - 1 ? (k) : W - 1) + 1] - wpre[((k) - L + 1 > 0 ? (k) - L + 1 : 0)])
+    if (L >= W) {
+        const double s = wpre[W];
+        for (int64_t k = 0; k < W - 1; ++k) {
+            const double m = MULT(k);
+            v += m * m;
+        }
+        v += (double)(L - W + 1) * s * s;
+        for (int64_t k = L; k < W + L - 1; ++k) {
+            const double m = MULT(k);
+            v += m * m;
+        }
+    } else {
+        for (int64_t k = 0; k < W + L - 1; ++k) {
+            const double m = MULT(k);
+            v += m * m;
+        }
+    }
+#undef MULT
+    return v;
+}
+
 /* Noise variance of the width-W window for unit-variance input: per active
  * channel, the sum of squared multiplicities of the window convolved with
- * the channel's L-sample box, by direct convolution. */
+ * the channel's L-sample box (box_sq, memoised per distinct L). */
 int oracle_variance(const int64_t* lens, int64_t nrows, int64_t n, const uint8_t* mask,
                     int64_t W, int trap, double* out) {
-    double* w = (double*)malloc(sizeof(double) * (size_t)W);
-    if (w == NULL)
+    double* w    = (double*)malloc(sizeof(double) * (size_t)W);
+    double* wpre = (double*)malloc(sizeof(double) * (size_t)(W + 1));
+    int64_t lmax = 1;
+    for (int64_t i = 0; i < nrows * n; ++i)
+        if (lens[i] > lmax)
+            lmax = lens[i];
+    double* memo = (double*)malloc(sizeof(double) * (size_t)(lmax + 1));
+    if (w == NULL || wpre == NULL || memo == NULL) {
+        free(w);
+        free(wpre);
+        free(memo);
         return -1;
+    }
     weights(W, trap, w);
+    wpre[0] = 0.0;
+    for (int64_t i = 0; i < W; ++i)
+        wpre[i + 1] = wpre[i] + w[i];
+    for (int64_t l = 0; l <= lmax; ++l)
+        memo[l] = -1.0;
     for (int64_t r = 0; r < nrows; ++r) {
         double v = 0.0;
         for (int64_t c = 0; c < n; ++c) {
             if (!mask[c])
                 continue;
             const int64_t L = lens[r * n + c];
-            for (int64_t k = 0; k < W + L - 1; ++k) {
-                double m = 0.0;
-                for (int64_t i = 0; i < W; ++i)
-                    if (k - i >= 0 && k - i < L)
-                        m += w[i];
-                v += m * m;
-            }
+            if (memo[L] < 0.0)
+                memo[L] = box_sq(L, W, wpre);
+            v += memo[L];
         }
         out[r] = v;
     }
     free(w);
+    free(wpre);
+    free(memo);
+    return 0;
+}
+
+/* Selected rows of one band straight from a float32 [C][T] input:
+ * out[i][t] = sum over channels [a, b) of the FP64 window sum
+ * in[c][t - s - L + 1 .. t - s] (samples before 0 are zero), with (s, L)
+ * the row's per-channel shift and length ([nrows][b - a] each). The window
+ * slides along t in FP64 (one add and one subtract per sample), so no
+ * prefix array of the whole input is held. */
+int oracle_dedisperse_rows(const float* in, int64_t C, int64_t T, int64_t a, int64_t b,
+                           const int64_t* shifts, const int64_t* lens, int64_t nrows, double* out) {
+    const int64_t n = b - a;
+    if (a < 0 || b > C || n <= 0)
+        return -1;
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t r = 0; r < nrows; ++r) {
+        double* o = out + r * T;
+        for (int64_t t = 0; t < T; ++t)
+            o[t] = 0.0;
+        for (int64_t c = 0; c < n; ++c) {
+            const int64_t s = shifts[r * n + c], L = lens[r * n + c];
+            const float* x  = in + (a + c) * T;
+            double acc      = 0.0;
+            /* window of output t covers input [t - s - L + 1, t - s] */
+            for (int64_t t = 0; t < T; ++t) {
+                const int64_t hi = t - s;
+                const int64_t lo = t - s - L;
+                if (hi >= 0)
+                    acc += (double)x[hi];
+                if (lo >= 0)
+                    acc -= (double)x[lo];
+                o[t] += acc;
+            }
+        }
+    }
     return 0;
 }
 

@@ -119,3 +119,38 @@ def test_rfi_unaligned_device_block_matches_aligned(name):
         outs.append((gpu.download().copy(), gpu.channel_mask().copy()))
     assert np.array_equal(outs[0][0].view(np.uint32), outs[1][0].view(np.uint32))
     assert np.array_equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.gpu
+def test_rfi_device_block_needs_a_stream_and_orders_after_it():
+    """A device block is read after the work queued on the caller's stream
+    (an async copy written behind other work on that stream gives the
+    host-input result), and the null stream is refused for a device block."""
+    import ctypes as C
+
+    import torch
+
+    from frost_b200._lib import lib
+    from frost_b200.rfi import RFICleaner
+    cfg, layout, baseline, blocks = make_case("default_u8")
+    block, nsamps = blocks[0]
+    ref = RFICleaner(cfg, layout, baseline)
+    want = ref.execute_normalized(block, nsamps)
+    gpu = RFICleaner(cfg, layout, baseline)
+    s = torch.cuda.Stream()
+    dev = torch.zeros(block.size, dtype=torch.uint8, device="cuda")
+    host = torch.from_numpy(np.ascontiguousarray(block)).pin_memory()
+    junk = torch.empty((4096, 4096), device="cuda")
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        for _ in range(8):
+            junk.normal_()
+            junk = junk @ junk
+        dev.copy_(host, non_blocking=True)
+    gpu.execute_normalized_device(dev.data_ptr(), block.size, nsamps, on_device=True, stream=s.cuda_stream)
+    got = gpu.download()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    out = C.c_void_p()
+    rc = lib().frost_rfi_execute_normalized(gpu._h, C.c_void_p(dev.data_ptr()), block.size, nsamps, 1, None,
+                                            C.byref(out))
+    assert rc == -1 and "null stream" in lib().frost_last_error().decode()

@@ -365,3 +365,41 @@ def test_uneven_widths_match_oracle():
     n, missing, extra, bad = compare(cands, ref, bc.detect_thresh)
     assert n > 10
     assert not missing and not extra and not bad, (missing[:5], extra[:5], bad[:5])
+
+
+def test_device_waterfall_written_on_a_caller_stream():
+    """A waterfall written on the caller's stream (an async copy from pinned
+    memory behind other work on that stream) and passed with that stream is
+    read after the writes: the candidates equal the host-input run. The
+    null stream is refused for device input, as frost refuses it
+    (lib/cuda/device_rfi_detail.cuh:77-83)."""
+    import ctypes as C
+
+    import torch
+
+    from frost_b200._lib import lib
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=1, gulp=8192)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0)
+    stream = make_stream(pc, 2, seed=31, pulses=PULSES)
+    gulp = pc.block_nsamps
+    ref = run_engine(FDMTBoxcar(pc, bc), stream, gulp)
+    eng = FDMTBoxcar(pc, bc)
+    s = torch.cuda.Stream()
+    wf = torch.zeros((pc.nchans, gulp), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    junk = torch.empty((4096, 4096), device="cuda")
+    out = []
+    for g in range(2):
+        host = torch.from_numpy(np.ascontiguousarray(stream[:, g * gulp:(g + 1) * gulp])).pin_memory()
+        with torch.cuda.stream(s):
+            for _ in range(8):           # other work queued ahead of the copy
+                junk.normal_()
+                junk = junk @ junk
+            wf.copy_(host, non_blocking=True)
+        out.append(eng.execute_device(wf.data_ptr(), gulp, None, stream=s.cuda_stream).candidates.copy())
+    out.append(eng.drain().candidates.copy())
+    assert np.array_equal(np.concatenate(out), ref)
+    rc = lib().frost_search_execute(eng._h, C.cast(C.c_void_p(wf.data_ptr()), C.POINTER(C.c_float)),
+                                    gulp, 1, None, None)
+    assert rc == -1 and "null stream" in lib().frost_last_error().decode()

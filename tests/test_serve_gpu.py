@@ -123,6 +123,55 @@ def test_staged_host_gulps_match_unstaged():
     srv.close()
 
 
+def test_set_staging_while_another_thread_submits():
+    """A thread that changes a beam's staging blocks (1, 2, 0, ...) while
+    another thread keeps submitting pinned gulps to that beam: gulps that
+    arrive while the beam is being reconfigured are uploaded when they are
+    processed, and every gulp gives the candidates of an unstaged beam fed
+    the same gulps."""
+    import threading
+
+    import torch
+
+    from frost_b200.serve import BeamServer
+    rfi, layout, plan, bc = _setup()
+    st = _beam_stream(43)
+    pinned = torch.from_numpy(st.reshape(-1)).pin_memory()
+    gulp_bytes = GULP * NCHANS
+    srv = BeamServer(slots=2)
+    plain, staged = srv.add_beam(rfi, layout, 1.0, plan, bc), srv.add_beam(rfi, layout, 1.0, plan, bc)
+    order = [g % NGULPS for g in range(12)]
+    ref = [srv.wait(srv.submit(plain, st[g * GULP:(g + 1) * GULP], GULP))[0] for g in order]
+    stop, errors, toggles = threading.Event(), [], [0]
+
+    def toggler():
+        while not stop.is_set():
+            try:
+                srv.set_staging(staged, (1, 2, 0)[toggles[0] % 3])
+            except Exception as e:  # reported below
+                errors.append(e)
+                return
+            toggles[0] += 1
+    th = threading.Thread(target=toggler)
+    th.start()
+    got = []
+    try:
+        for i in range(0, len(order), 2):
+            ts = [srv.submit_ptr(staged, pinned.data_ptr() + g * gulp_bytes, gulp_bytes, GULP, on_device=False)
+                  for g in order[i:i + 2]]
+            got += [srv.wait(t)[0] for t in ts]
+    finally:
+        stop.set()
+        th.join()
+    assert not errors, errors
+    assert toggles[0] > 0
+    assert sum(len(a) for a in ref) > 0
+    for k, (a, b) in enumerate(zip(ref, got)):
+        assert np.array_equal(a, b), k
+    srv.set_staging(staged, 0)
+    srv.close()
+
+
 def test_admission_by_device_memory():
     from frost_b200._abi import ERR_OUT_OF_MEMORY
     from frost_b200._lib import FrostError

@@ -3,8 +3,9 @@ that cannot call cudaMalloc while processing (a real-time consumer whose
 device memory is all sized at start-up, or a program whose device memory
 belongs to another framework's pool): through the C ABI, two calls in a row
 must give exactly what the allocating frost_rfi_execute_normalized gives for
-the same blocks with every excision strategy off, and requests larger than
-its fixed static scratch must be refused with a clear error.
+the same blocks with every excision strategy off, later calls must leave the
+device's free memory unchanged, and requests larger than its fixed static
+scratch (or without a stream) must be refused with a clear error.
 
 Named to be collected last, so a run that stops at the first failure has
 already run every other test."""
@@ -29,6 +30,14 @@ def _blocks(nchans, nsamps, seed, dtype):
     return x
 
 
+def _static(layout, raw, nsamps, out, stream):
+    from frost_b200 import _lib
+    lay = layout.to_c()
+    return _lib.lib().frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr()),
+                                                 raw.numel(), nsamps, C.c_void_p(out.data_ptr()),
+                                                 out.numel(), C.c_void_p(stream) if stream else None)
+
+
 def _run_both(layout, block_np, nsamps=0):
     import torch
 
@@ -36,14 +45,12 @@ def _run_both(layout, block_np, nsamps=0):
     from frost_b200.config import RfiConfig
     from frost_b200.rfi import RFICleaner
 
-    L = _lib.lib()
     raw = torch.from_numpy(np.ascontiguousarray(block_np).view(np.uint8).reshape(-1)).cuda()
     capacity = raw.numel() // layout.row_bytes
     out = torch.empty(layout.nchans * capacity, dtype=torch.float32, device="cuda")
-    lay = layout.to_c()
-    _lib.check(L.frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr()),
-                                            raw.numel(), nsamps, C.c_void_p(out.data_ptr()),
-                                            out.numel(), None))
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    _lib.check(_static(layout, raw, nsamps, out, s.cuda_stream))
     static_out = out.cpu().numpy().reshape(layout.nchans, capacity)
 
     cleaner = RFICleaner(RfiConfig.quiet(), layout, 2.0)
@@ -62,6 +69,31 @@ def test_static_scratch_matches_allocating_cleaner_twice():
         assert not mine[1024 - 1 - 5].any()  # dead channel (flipped order) zeroed
 
 
+def test_static_scratch_calls_after_the_first_allocate_nothing():
+    """After the first call on the device, repeated calls leave the device's
+    free memory (cudaMemGetInfo) exactly as it was."""
+    import torch
+
+    from frost_b200 import _lib
+    from frost_b200.config import BlockLayout, DataType
+    lay = BlockLayout(512, 32768, DataType.UINT8, 64e-6, 1500.0, -0.5)
+    raw = torch.from_numpy(_blocks(512, 32768, 7, "uint8").reshape(-1)).cuda()
+    out = torch.empty(512 * 32768, dtype=torch.float32, device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    _lib.check(_static(lay, raw, 0, out, s.cuda_stream))  # start-up call
+    torch.cuda.synchronize()
+    first = out.clone()  # torch allocates here, before the free-memory reading
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(4):
+        _lib.check(_static(lay, raw, 0, out, s.cuda_stream))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert torch.equal(out.view(torch.int32), first.view(torch.int32))
+
+
 def test_static_scratch_float_partial_block():
     from frost_b200.config import BlockLayout, DataType
     lay = BlockLayout(256, 8192, DataType.FLOAT32, 1e-3, 800.0, 1.0)
@@ -76,20 +108,28 @@ def test_static_scratch_refuses_oversize_and_short_blocks():
     from frost_b200 import _lib
     from frost_b200.config import BlockLayout, DataType
     L = _lib.lib()
+    s = torch.cuda.Stream()
     big = BlockLayout(4096, 65536, DataType.UINT8, 64e-6, 1500.0, -0.1)  # 2 windows x 4096 > 2684
     raw = torch.zeros(4096 * 65536, dtype=torch.uint8, device="cuda")
     out = torch.empty(4096 * 65536, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
     lay = big.to_c()
     rc = L.frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr()),
-                                      raw.numel(), 0, C.c_void_p(out.data_ptr()), out.numel(), None)
+                                      raw.numel(), 0, C.c_void_p(out.data_ptr()), out.numel(),
+                                      C.c_void_p(s.cuda_stream))
     assert rc == -1 and "static scratch" in L.frost_last_error().decode()
     small = BlockLayout(64, 4096, DataType.UINT8, 1e-3, 1500.0, -1.0)
     lay = small.to_c()
     rc = L.frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr()),
-                                      64 * 4096, 40, C.c_void_p(out.data_ptr()), out.numel(), None)
+                                      64 * 4096, 40, C.c_void_p(out.data_ptr()), out.numel(),
+                                      C.c_void_p(s.cuda_stream))
     assert rc == -1 and "at least 64" in L.frost_last_error().decode()
+    rc = L.frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr()),
+                                      64 * 4096, 0, C.c_void_p(out.data_ptr()), out.numel(), None)
+    assert rc == -1 and "null stream" in L.frost_last_error().decode()
     f32 = BlockLayout(64, 4096, DataType.FLOAT32, 1e-3, 1500.0, -1.0)
     lay = f32.to_c()
     rc = L.frost_rfi_normalize_static(C.byref(lay), C.c_float(2.0), C.c_void_p(raw.data_ptr() + 2),
-                                      64 * 4096 * 4, 0, C.c_void_p(out.data_ptr()), out.numel(), None)
+                                      64 * 4096 * 4, 0, C.c_void_p(out.data_ptr()), out.numel(),
+                                      C.c_void_p(s.cuda_stream))
     assert rc == -1 and "aligned" in L.frost_last_error().decode()
