@@ -54,6 +54,8 @@ SIGNATURES = {
     "frost_search_destroy": (C.c_int, [_vp]),
     "frost_search_execute": (C.c_int, [_vp, _f32p, _sz, C.c_int, _u8p, _vp]),
     "frost_search_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "frost_search_set_wait_limit": (C.c_int, [_vp, C.c_int64]),
+    "frost_search_restart": (C.c_int, [_vp]),
     "frost_rfi_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "frost_search_drain": (C.c_int, [_vp]),
     "frost_search_result_count": (C.c_int, [_vp, C.POINTER(_sz), C.POINTER(_u64), C.POINTER(_u64)]),

@@ -39,10 +39,10 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t phase) {
 }
 
 /** Waits for phase `phase` of `bar` to complete; false if it did not within
- * kSpinLimit tries. */
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+ * `limit` tries (kSpinLimit by default). */
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit = kSpinLimit) {
     const uint32_t b = smem_addr(bar);
-    for (long it = 0; it < kSpinLimit; ++it)
+    for (long long it = 0; it < limit; ++it)
         if (mbar_try(b, phase))
             return true;
     return false;

@@ -12,7 +12,7 @@
 
 #include "common.hpp"
 #include "dedisp.hpp"
-#include "host_stats.hpp"
+#include "rfi_decide.hpp"
 #include "cand_writer.hpp"
 #include "memory_plan.hpp"
 #include "postprocess.hpp"
@@ -285,12 +285,7 @@ int frost_iqrm_mask(const float* x, size_t n, uint64_t radius, float threshold,
     return guarded([&] {
         if ((x == nullptr || out == nullptr) && n != 0)
             invalid("frost_iqrm_mask: null argument");
-        std::span<const uint8_t> ig;
-        if (ignore != nullptr)
-            ig = {ignore, n};
-        const auto m = fb::stats::iqrm_mask({x, n}, radius, threshold, ig);
-        if (n)
-            std::memcpy(out, m.data(), n);
+        fb::rfi::iqrm_mask_host(x, n, radius, threshold, ignore, out);
     });
 }
 
@@ -693,6 +688,22 @@ int frost_search_get_residency(const frost_search* s, int* ctas_per_sm) {
         if (s == nullptr || ctas_per_sm == nullptr)
             invalid("frost_search_get_residency: null argument");
         *ctas_per_sm = s->impl.residency();
+    });
+}
+
+int frost_search_set_wait_limit(frost_search* s, int64_t tries) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_set_wait_limit: null handle");
+        s->impl.set_wait_limit(tries);
+    });
+}
+
+int frost_search_restart(frost_search* s) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_restart: null handle");
+        s->impl.restart();
     });
 }
 

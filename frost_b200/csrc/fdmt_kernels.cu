@@ -49,21 +49,25 @@ __device__ __forceinline__ uint32_t pack_sat(float lo, float hi) {
 }
 
 // Inclusive block scan of smem[0..n) in place (float), n <= kThreads * 64.
-__device__ void block_scan(float* a, int n) {
-    __shared__ float warp_tot[kThreads / 32];
+// Inclusive prefix sum of a[0..n) in place, in FP64: leaf windows are
+// differences of these sums, and a double prefix keeps each window sum
+// within one rounding of its exact value however long the tile is (a float
+// prefix would carry an error proportional to the running sum).
+__device__ void block_scan(double* a, int n) {
+    __shared__ double warp_tot[kThreads / 32];
     const int per  = (n + kThreads - 1) / kThreads;
     const int beg  = threadIdx.x * per;
     const int end  = min(beg + per, n);
-    float run      = 0.0F;
+    double run     = 0.0;
     for (int i = beg; i < end; ++i) {
         run += a[i];
         a[i] = run;
     }
     // exclusive scan of the per-thread totals
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float v        = run;
+    double v       = run;
     for (int o = 1; o < 32; o <<= 1) {
-        const float u = __shfl_up_sync(0xFFFFFFFFU, v, o);
+        const double u = __shfl_up_sync(0xFFFFFFFFU, v, o);
         if (lane >= o)
             v += u;
     }
@@ -71,9 +75,9 @@ __device__ void block_scan(float* a, int n) {
         warp_tot[warp] = v;
     __syncthreads();
     if (warp == 0) {
-        float w = lane < kThreads / 32 ? warp_tot[lane] : 0.0F;
+        double w = lane < kThreads / 32 ? warp_tot[lane] : 0.0;
         for (int o = 1; o < 32; o <<= 1) {
-            const float u = __shfl_up_sync(0xFFFFFFFFU, w, o);
+            const double u = __shfl_up_sync(0xFFFFFFFFU, w, o);
             if (lane >= o)
                 w += u;
         }
@@ -81,7 +85,7 @@ __device__ void block_scan(float* a, int n) {
             warp_tot[lane] = w;
     }
     __syncthreads();
-    const float offset = (v - run) + (warp > 0 ? warp_tot[warp - 1] : 0.0F);
+    const double offset = (v - run) + (warp > 0 ? warp_tot[warp - 1] : 0.0);
     for (int i = beg; i < end; ++i)
         a[i] += offset;
     __syncthreads();
@@ -93,10 +97,10 @@ __global__ void __launch_bounds__(kThreads)
              int32_t ntiles, int32_t H, const float* __restrict__ wf, int64_t wpitch, int64_t t0,
              int32_t n_valid, const float* __restrict__ hist, int32_t hist_len, S* __restrict__ out,
              int64_t pitch, int32_t base) {
-    extern __shared__ float smem[];
+    extern __shared__ double smem_d[];
     const int32_t N = kTimePerCta + H + 1;
-    float* Pa       = smem;
-    float* Pb       = smem + N;
+    double* Pa      = smem_d;
+    double* Pb      = smem_d + N;
     // Work items (node, tile), nodes fastest; a CTA takes items blockIdx.x,
     // blockIdx.x + gridDim.x, ...
     const int64_t nitems = static_cast<int64_t>(nnodes) * ntiles;
@@ -134,10 +138,10 @@ __global__ void __launch_bounds__(kThreads)
             for (int j = 0; j < kPer; ++j) {
                 const int k = threadIdx.x + j * kThreads;
                 const int i = k + H + 1;
-                float v     = Pa[i] - Pa[i - op.d_lo - 1];
+                double v    = Pa[i] - Pa[i - op.d_lo - 1];
                 if (cb >= 0)
                     v += Pb[i - op.d_lo] - Pb[i - op.d_lo - op.d_hi - 1];
-                st<S>(row + k, v);
+                st<S>(row + k, static_cast<float>(v));
             }
         }
         __syncthreads(); // every thread is done with Pa / Pb
@@ -217,7 +221,7 @@ template <class S>
 __global__ void __launch_bounds__(kThreads)
     k_level_pipe(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
                  int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                 int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err) {
+                 int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err, long long wait_limit) {
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -273,7 +277,7 @@ __global__ void __launch_bounds__(kThreads)
         int i = 0;
         for (; i < nt; ++i) {
             const int s = cs;
-            if (!mbar_wait(&bar[s], cp))
+            if (!mbar_wait(&bar[s], cp, wait_limit))
                 atomicExch(&abort_flag, 1);
             __syncthreads();
             if (abort_flag)
@@ -411,7 +415,7 @@ template <class S, int NS>
 __global__ void __launch_bounds__(kThreads)
     k_level2_pipe(const FusedOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
                   int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                  int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err) {
+                  int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err, long long wait_limit) {
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -475,7 +479,7 @@ __global__ void __launch_bounds__(kThreads)
         int i = 0;
         for (; i < nt; ++i) {
             const int st = cs;
-            if (!mbar_wait(&bar[st], cp))
+            if (!mbar_wait(&bar[st], cp, wait_limit))
                 atomicExch(&abort_flag, 1);
             __syncthreads();
             if (abort_flag)
@@ -661,7 +665,7 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
         throw Error(FROST_ERR_INTERNAL, "level1: bad geometry");
     const int32_t ntiles = ncols / kTimePerCta;
     const dim3 grid(grid_for(static_cast<int64_t>(nnodes) * ntiles, ctas));
-    const size_t smem = 2 * sizeof(float) * (kTimePerCta + max_node_delay + 1);
+    const size_t smem = 2 * sizeof(double) * (kTimePerCta + max_node_delay + 1);
     if (smem > 200 * 1024)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "level1: leaf windows too long for shared memory");
     if (out.fp16) {
@@ -681,7 +685,7 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
 }
 
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  unsigned* err, cudaStream_t s, int32_t tpc, int32_t ctas) {
+                  unsigned* err, cudaStream_t s, int32_t tpc, int32_t ctas, long long wait_limit) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
@@ -712,13 +716,13 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
                                      static_cast<int>(smem)));
         k_level_pipe<__half><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const __half*>(in.data), in.pitch, in.base,
-            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err);
+            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err, wait_limit);
     } else {
         FB_CUDA(cudaFuncSetAttribute(k_level_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
         k_level_pipe<float><<<grid, kThreads, smem, s>>>(
             ops, static_cast<const float*>(in.data), in.pitch, in.base,
-            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err);
+            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err, wait_limit);
     }
     FB_LAUNCH_CHECK();
 }
@@ -726,28 +730,29 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
 namespace {
 template <class S, int NS>
 void level2_stages(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
-                   int64_t nrows, unsigned* err, cudaStream_t s) {
+                   int64_t nrows, unsigned* err, long long wait_limit, cudaStream_t s) {
     const size_t smem = NS * (4 * kTimePerCta * sizeof(S) + 48);
     FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<S, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     k_level2_pipe<S, NS><<<grid, kThreads, smem, s>>>(ops, static_cast<const S*>(in.data), in.pitch, in.base,
                                                       static_cast<S*>(out.data), out.pitch, out.base, ntiles,
-                                                      tpc, nrows, err);
+                                                      tpc, nrows, err, wait_limit);
 }
 template <class S>
 void level2_typed(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
-                  int64_t nrows, int32_t stages, unsigned* err, cudaStream_t s) {
+                  int64_t nrows, int32_t stages, unsigned* err, long long wait_limit, cudaStream_t s) {
     switch (stages == 0 ? kStages2<S> : stages) {
-    case 2: level2_stages<S, 2>(ops, grid, in, out, ntiles, tpc, nrows, err, s); break;
-    case 3: level2_stages<S, 3>(ops, grid, in, out, ntiles, tpc, nrows, err, s); break;
-    case 4: level2_stages<S, 4>(ops, grid, in, out, ntiles, tpc, nrows, err, s); break;
+    case 2: level2_stages<S, 2>(ops, grid, in, out, ntiles, tpc, nrows, err, wait_limit, s); break;
+    case 3: level2_stages<S, 3>(ops, grid, in, out, ntiles, tpc, nrows, err, wait_limit, s); break;
+    case 4: level2_stages<S, 4>(ops, grid, in, out, ntiles, tpc, nrows, err, wait_limit, s); break;
     default: throw Error(FROST_ERR_INTERNAL, "level2: stages must be 2, 3 or 4");
     }
 }
 } // namespace
 
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                   unsigned* err, cudaStream_t s, int32_t tpc, int32_t stages, int32_t ctas) {
+                   unsigned* err, cudaStream_t s, int32_t tpc, int32_t stages, int32_t ctas,
+                   long long wait_limit) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
@@ -759,10 +764,12 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
         throw Error(FROST_ERR_INTERNAL, "level2: 4 float stages exceed the shared memory of a CTA");
     const int ntiles = ncols / kTimePerCta;
     const dim3 grid(grid_for(nrows * ((ntiles + tpc - 1) / tpc), ctas));
+    if (wait_limit < 0)
+        throw Error(FROST_ERR_INTERNAL, "level2: wait limit must be >= 0");
     if (out.fp16)
-        level2_typed<__half>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, s);
+        level2_typed<__half>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, wait_limit, s);
     else
-        level2_typed<float>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, s);
+        level2_typed<float>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, wait_limit, s);
     FB_LAUNCH_CHECK();
 }
 

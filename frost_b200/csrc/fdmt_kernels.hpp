@@ -20,6 +20,9 @@ struct LevelView {
 };
 
 constexpr int kTimePerCta = 2048; // samples per CTA in the level kernels
+/** Tries a pipelined kernel's first wait on a bulk copy makes before it
+ * gives up (bulk::kSpinLimit); a drain after a give-up always uses it. */
+constexpr long long kDefaultWaitLimit = 1LL << 22;
 
 /* Residency: every level launcher takes `ctas`, the most CTAs of the launch
  * (0: one CTA per work item). With a cap each CTA loops over work items, so
@@ -39,7 +42,8 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
  * 2048 columns) and sets *err if a bounded wait ran out; with `err` null
  * the direct (one CTA per row and tile) kernel runs. */
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t ctas = 0);
+                  unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t ctas = 0,
+                  long long wait_limit = kDefaultWaitLimit);
 
 /** A row of level h+1 from four rows of level h-1: the sum of row[j] read at
  * t - shift[j] (shift[0] = 0), grouped (row0 + row1) + (row2 + row3); a
@@ -55,7 +59,7 @@ struct FusedOp {
  * more CTAs per SM. */
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
                    unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t stages = 0,
-                   int32_t ctas = 0);
+                   int32_t ctas = 0, long long wait_limit = kDefaultWaitLimit);
 
 /** dst[r][0 .. width) = src[r][0 .. width) for `rows` rows of pitches
  * dpitch / spitch bytes (device memory): 16-byte vectors when pointers,

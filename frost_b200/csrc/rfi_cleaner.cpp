@@ -3,10 +3,11 @@
 //   moments -> channel mask (moments IQR outliers, IQRM, growth) ->
 //   row scan + column scan -> flags -> apply (fills, transforms) ->
 //   optional Welford re-measure -> normalise + transpose to [channel][time].
-// Every T x C pass is a kernel (rfi_kernels.cu); the per-gulp decisions use
-// the O(T) / O(C) series the kernels reduce the block to, as frost's own
-// device cleaner does (lib/cuda/device_rfi_cuda.cu:187-262). Semantics follow
-// RFICleaner::Impl (lib/cpu/rfi_cpu.cpp, lib/cpu/rfi_cpu_measure.cpp).
+// Every T x C pass is a kernel (rfi_kernels.cu) and every per-gulp decision
+// on the O(T) / O(C) series those passes reduce the block to is a kernel
+// too (rfi_decide.cu): the whole gulp is queued on one stream and the host
+// reads back only the mask and the report counters at the end. Semantics
+// follow RFICleaner::Impl (lib/cpu/rfi_cpu.cpp, lib/cpu/rfi_cpu_measure.cpp).
 
 #include "rfi_cleaner.hpp"
 
@@ -18,27 +19,14 @@
 #include <limits>
 #include <string_view>
 
-#include "host_stats.hpp"
-
 namespace fb::rfi {
 
 namespace {
-
-using Clock = std::chrono::steady_clock;
-double since(Clock::time_point t) {
-    return std::chrono::duration<double>(Clock::now() - t).count();
-}
 
 template <class T> void h2d(DeviceBuffer& dst, const T* src, SizeType count, cudaStream_t s) {
     dst.reserve(std::max<SizeType>(count * sizeof(T), 1));
     if (count)
         FB_CUDA(cudaMemcpyAsync(dst.get(), src, count * sizeof(T), cudaMemcpyHostToDevice, s));
-}
-
-template <class T> void d2h(std::vector<T>& dst, const DeviceBuffer& src, SizeType count, cudaStream_t s) {
-    dst.resize(count);
-    if (count)
-        FB_CUDA(cudaMemcpyAsync(dst.data(), src.get(), count * sizeof(T), cudaMemcpyDeviceToHost, s));
 }
 
 SizeType count_zeros(const std::vector<uint8_t>& v) {
@@ -250,10 +238,25 @@ Cleaner::Cleaner(const frost_rfi_config& cfg, const frost_block_layout& layout,
     m_report              = frost_rfi_report{};
     m_report.chans_zapped = count_zeros(m_static_mask);
     m_report.chans_masked = m_report.chans_zapped;
-    m_zdot_a.assign(m_n, 0.0F);
-    m_zdot_b.assign(m_n, 0.0F);
     FB_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
+    for (auto& e : m_ev)
+        FB_CUDA(cudaEventCreate(&e));
     h2d(m_static_mask_d, m_static_mask.data(), m_n, m_stream);
+    // zero-DM fit of the last full block (read by short tails); zero until one
+    m_zdot_a_d.reserve(m_n * sizeof(float));
+    m_zdot_b_d.reserve(m_n * sizeof(float));
+    FB_CUDA(cudaMemsetAsync(m_zdot_a_d.get(), 0, m_n * sizeof(float), m_stream));
+    FB_CUDA(cudaMemsetAsync(m_zdot_b_d.get(), 0, m_n * sizeof(float), m_stream));
+    m_counters.reserve(kRepSlots * sizeof(unsigned long long));
+    m_pinned.reserve(kRepSlots * sizeof(unsigned long long) + m_n);
+    // channel-decision scratch; IQRM lags of this band
+    if (c.iqrm_enabled)
+        m_lags = iqrm_lags(m_n, c.iqrm_radius > 0 ? c.iqrm_radius : std::max<SizeType>(m_n / 10, 1));
+    m_chan_scratch.reserve(ChannelScratch::size_for(m_n, m_lags.size()));
+    m_cw.carve(m_chan_scratch.get(), m_n, m_lags.size());
+    if (!m_lags.empty())
+        FB_CUDA(cudaMemcpyAsync(m_cw.lags, m_lags.data(), m_lags.size() * sizeof(uint64_t),
+                                cudaMemcpyHostToDevice, m_stream));
     // Reciprocals of the Welford counts (correctly rounded host divisions).
     std::vector<double> recip(layout.max_nsamps + 1, 0.0);
     for (SizeType n = 1; n < recip.size(); ++n)
@@ -266,8 +269,25 @@ Cleaner::~Cleaner() {
     if (m_stream != nullptr) {
         cudaSetDevice(m_device);
         cudaStreamSynchronize(m_stream);
+        for (auto e : m_ev)
+            if (e != nullptr)
+                cudaEventDestroy(e);
         cudaStreamDestroy(m_stream);
     }
+}
+
+const std::vector<uint8_t>& Cleaner::time_flags() const {
+    if (!m_flags_fresh) {
+        m_time_flags.assign(m_flags_len, 0U);
+        if (m_flags_on_device && m_flags_len > 0) {
+            DeviceGuard g(m_device);
+            FB_CUDA(cudaMemcpyAsync(m_time_flags.data(), m_time_flags_d.get(), m_flags_len,
+                                    cudaMemcpyDeviceToHost, m_stream));
+            FB_CUDA(cudaStreamSynchronize(m_stream));
+        }
+        m_flags_fresh = true;
+    }
+    return m_time_flags;
 }
 
 void Cleaner::build_static_mask() {
@@ -289,7 +309,8 @@ SizeType Cleaner::memory_usage() const {
         &m_kspec_whole, &m_chunk_min, &m_chunk_max, &m_chunk_zdot, &m_chunk_kpos, &m_chunk_kneg,
         &m_lo, &m_hi, &m_zdot_sum, &m_kpos_best, &m_kneg_best, &m_time_flags_d, &m_zdot_a_d,
         &m_zdot_b_d, &m_kchan_pos_d, &m_kchan_neg_d, &m_kchan_any_d, &m_flagged_d, &m_work, &m_out, &m_counters,
-        &m_first_bad, &m_tail_loc, &m_tail_scale, &m_tail_out_loc, &m_tail_out_scale, &m_recip};
+        &m_first_bad, &m_tail_loc, &m_tail_scale, &m_tail_out_loc, &m_tail_out_scale, &m_recip,
+        &m_chan_scratch, &m_flag_scratch};
     SizeType total = 0;
     for (const auto* b : all)
         total += b->bytes();
@@ -318,7 +339,12 @@ SizeType Cleaner::estimate_memory(const frost_rfi_config& cfg, const frost_block
     // ensure_capacity(T, T): raw block, float work and output, per-window
     // statistics, tails, counters
     total += std::max<SizeType>(T * row, 16) + 2 * std::max<SizeType>(T * n * f, 16);
-    total += 5 * nwin * n * f + 4 * n * f + kCountSlots * sizeof(unsigned long long) + sizeof(unsigned long long);
+    total += 5 * nwin * n * f + 4 * n * f + kRepSlots * sizeof(unsigned long long) + sizeof(unsigned long long);
+    // decision scratch (channel mask, time flags)
+    const SizeType nlags = c.iqrm_enabled
+                               ? iqrm_lags(n, c.iqrm_radius > 0 ? c.iqrm_radius : std::max<SizeType>(n / 10, 1)).size()
+                               : 0;
+    total += ChannelScratch::size_for(n, nlags) + FlagScratch::size_for(T, c.broad_boxcar_max);
     // reserve_phase_buffers
     total += nwin * kMaxBandpassRows * n * f + n * sizeof(uint32_t);
     total += (moments ? nwin * n * sizeof(MomentSums) : 0) + 2 * std::max<SizeType>(moments ? nwin * n * f : 0, f);
@@ -384,7 +410,7 @@ void Cleaner::ensure_capacity(SizeType capacity, SizeType valid) {
     m_tail_scale.reserve(n * sizeof(float));
     m_tail_out_loc.reserve(n * sizeof(float));
     m_tail_out_scale.reserve(n * sizeof(float));
-    m_counters.reserve(kCountSlots * sizeof(unsigned long long));
+    m_counters.reserve(kRepSlots * sizeof(unsigned long long));
     m_first_bad.reserve(sizeof(unsigned long long));
 }
 
@@ -444,6 +470,9 @@ const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, S
         launch_unpack(d, raw, m_work.as<float>(), s);
         normalize_short(capacity, valid, s);
         FB_CUDA(cudaStreamSynchronize(s));
+        m_flags_len       = valid;
+        m_flags_on_device = false;
+        m_flags_fresh     = false;
         return m_out.as<float>();
     }
 
@@ -467,7 +496,6 @@ const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, S
         launch_welford(d, m_work.as<float>(), m_recip.as<double>(), m_loc2.as<float>(), m_scale2.as<float>(), s);
         loc   = m_loc2.as<float>();
         scale = m_scale2.as<float>();
-        m_time_flags.assign(valid, 0);
     } else {
         run_full(d, s);
         ++m_block_index;
@@ -488,9 +516,48 @@ const float* Cleaner::execute_normalized(const uint8_t* block, SizeType bytes, S
     }
     launch_normalize(d, m_work.as<float>(), loc, scale, m_mask_d.as<uint8_t>(), flip, capacity,
                      m_out.as<float>(), s);
-    FB_CUDA(cudaStreamSynchronize(s));
-    m_tail_ready = !short_block;
+    if (short_block)
+        FB_CUDA(cudaStreamSynchronize(s));
+    else
+        read_back(s);
+    m_flags_len       = valid;
+    m_flags_on_device = !short_block;
+    m_flags_fresh     = false;
+    m_tail_ready      = !short_block;
     return m_out.as<float>();
+}
+
+// The gulp's channel mask and report counters, copied back once the whole
+// gulp (normalisation included) is queued; the stage times are the device
+// intervals between the phase events.
+void Cleaner::read_back(cudaStream_t s) {
+    auto* counts = m_pinned.as<unsigned long long>();
+    auto* mask   = reinterpret_cast<uint8_t*>(counts + kRepSlots);
+    FB_CUDA(cudaMemcpyAsync(counts, m_counters.get(), kRepSlots * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaMemcpyAsync(mask, m_mask_d.get(), m_n, cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
+    m_mask.assign(mask, mask + m_n);
+    m_report.chans_moments         = counts[kRepMoments];
+    m_report.chans_iqrm            = counts[kRepIqrm];
+    m_report.chans_grown           = counts[kRepGrown];
+    m_report.chans_masked          = counts[kRepMasked];
+    m_report.chans_dead            = counts[kRepDead];
+    m_report.samps_broad           = counts[kRepBroad];
+    m_report.samps_dropout         = counts[kRepDropout];
+    m_report.samps_kadane          = counts[kRepKadane];
+    m_report.samps_flagged         = counts[kRepFlagged];
+    m_report.cells_narrow          = counts[kCountNarrow];
+    m_report.cells_kadane_spectrum = counts[kCountKspec];
+    m_report.cells_kadane_channel  = counts[kCountKchan];
+    m_report.fill_fallbacks        = counts[kCountFallback];
+    double* t[] = {&m_report.t_bandpass, &m_report.t_moments, &m_report.t_scan, &m_report.t_flags,
+                   &m_report.t_apply};
+    for (int i = 0; i < 5; ++i) {
+        float ms = 0.0F;
+        FB_CUDA(cudaEventElapsedTime(&ms, m_ev[i], m_ev[i + 1]));
+        *t[i] = 1e-3 * static_cast<double>(ms);
+    }
 }
 
 void Cleaner::normalize_short(SizeType capacity, SizeType valid, cudaStream_t s) {
@@ -501,126 +568,12 @@ void Cleaner::normalize_short(SizeType capacity, SizeType valid, cudaStream_t s)
     m_report.calibration_reused = 1;
     Dims d                      = dims(valid, m_layout.dtype);
     h2d(m_mask_d, m_mask.data(), m_n, s);
-    h2d(m_zdot_a_d, m_zdot_a.data(), m_n, s);
-    h2d(m_zdot_b_d, m_zdot_b.data(), m_n, s);
     launch_normalize_short(d, apply_params(), m_work.as<float>(), m_tail_loc.as<float>(),
                            m_tail_scale.as<float>(), m_tail_out_loc.as<float>(),
                            m_tail_out_scale.as<float>(), m_mask_d.as<uint8_t>(),
                            m_zdot_a_d.as<float>(), m_zdot_b_d.as<float>(),
                            m_layout.df < 0.0 ? 1 : 0, capacity, m_out.as<float>(), s);
-    m_time_flags.assign(valid, 0);
     ++m_block_index;
-}
-
-// Channel mask from the static zaps, moments outliers, IQRM and growth
-// (lib/cpu/rfi_cpu_measure.cpp:140-300).
-void Cleaner::build_channel_mask(const Dims& d, const std::vector<uint32_t>& unmeasured,
-                                 const std::vector<float>& scale,
-                                 const std::vector<MomentSums>& mom) {
-    const SizeType n    = m_n;
-    const SizeType nwin = d.nwin;
-    const auto& c       = m_cfg.c;
-    std::vector<uint8_t> dynamic(n, 0U);
-    if (c.moments_enabled) {
-        std::vector<double> mean(n, 0.0), stdev(n, 0.0), skew(n, 0.0), kurt(n, 0.0), acf(n, 0.0);
-        std::vector<uint8_t> good(n, 0U);
-        for (SizeType ch = 0; ch < n; ++ch) {
-            if (m_mask[ch] == 0)
-                continue;
-            MomentSums s{};
-            double lag_pairs = 0.0;
-            for (SizeType w = 0; w < nwin; ++w) {
-                const auto& sw = mom[w * n + ch];
-                s.n += sw.n;
-                s.s1 += sw.s1;
-                s.s2 += sw.s2;
-                s.s3 += sw.s3;
-                s.s4 += sw.s4;
-                s.lag += sw.lag;
-                lag_pairs += std::max(sw.n - 1.0, 0.0);
-            }
-            if (s.n < 2.0)
-                continue;
-            const double m1  = s.s1 / s.n;
-            const double m2  = s.s2 / s.n;
-            const double m3  = s.s3 / s.n;
-            const double m4  = s.s4 / s.n;
-            const double var = m2 - (m1 * m1);
-            if (!(var > 0.0))
-                continue;
-            good[ch]  = 1;
-            mean[ch]  = m1;
-            stdev[ch] = std::sqrt(var);
-            skew[ch]  = (m3 - (3.0 * m1 * m2) + (2.0 * m1 * m1 * m1)) / (var * stdev[ch]);
-            kurt[ch]  = ((m4 - (4.0 * m1 * m3) + (6.0 * m1 * m1 * m2) - (3.0 * m1 * m1 * m1 * m1)) /
-                        (var * var)) -
-                       3.0;
-            acf[ch] = lag_pairs > 0.0 ? ((s.lag / lag_pairs) - (m1 * m1)) / var : 0.0;
-        }
-        const double k = c.moments_threshold;
-        if (c.moments_mean)
-            stats::flag_iqr_outliers(mean, good, k, dynamic);
-        if (c.moments_std)
-            stats::flag_iqr_outliers(stdev, good, k, dynamic);
-        if (c.moments_skewness)
-            stats::flag_iqr_outliers(skew, good, k, dynamic);
-        if (c.moments_kurtosis)
-            stats::flag_iqr_outliers(kurt, good, k, dynamic);
-        if (c.moments_autocorr)
-            stats::flag_iqr_outliers(acf, good, k, dynamic);
-        if (c.moments_kurtosis_max > 0.0F)
-            for (SizeType ch = 0; ch < n; ++ch)
-                if (good[ch] && std::abs(kurt[ch]) > c.moments_kurtosis_max)
-                    dynamic[ch] = 1;
-        m_report.chans_moments = static_cast<SizeType>(std::count(dynamic.begin(), dynamic.end(), 1U));
-    }
-    if (c.iqrm_enabled) {
-        std::vector<float> std_data(n, 0.0F);
-        std::vector<uint8_t> ignore(n, 0U);
-        for (SizeType ch = 0; ch < n; ++ch) {
-            ignore[ch]    = (m_mask[ch] == 0 || unmeasured[ch] > 0) ? 1 : 0;
-            double weight = 0.0, acc = 0.0;
-            for (SizeType w = 0; w < nwin; ++w) {
-                const auto& s = mom[w * n + ch];
-                if (s.n > 1.0) {
-                    const double mean = s.s1 / s.n;
-                    const double var  = (s.s2 / s.n) - (mean * mean);
-                    const double sc   = scale[w * n + ch];
-                    acc += s.n * std::max(var, 0.0) * sc * sc;
-                    weight += s.n;
-                }
-            }
-            std_data[ch] = weight > 0.0 ? static_cast<float>(std::sqrt(acc / weight)) : 0.0F;
-        }
-        const SizeType radius = c.iqrm_radius > 0 ? c.iqrm_radius : std::max<SizeType>(n / 10, 1);
-        const auto flags      = stats::iqrm_mask(std_data, radius, c.iqrm_threshold, ignore);
-        for (SizeType ch = 0; ch < n; ++ch) {
-            if (flags[ch] != 0 && ignore[ch] == 0 && dynamic[ch] == 0) {
-                dynamic[ch] = 1;
-                ++m_report.chans_iqrm;
-            }
-        }
-    }
-    if (c.mask_grow > 0) {
-        std::vector<uint8_t> grown = dynamic;
-        const SizeType g           = c.mask_grow;
-        for (SizeType ch = 0; ch < n; ++ch) {
-            if (dynamic[ch] == 0)
-                continue;
-            const SizeType first = ch > g ? ch - g : 0;
-            const SizeType last  = ch + std::min(g, n - 1 - ch);
-            for (SizeType k = first; k <= last; ++k)
-                grown[k] = 1;
-        }
-        for (SizeType ch = 0; ch < n; ++ch)
-            if (grown[ch] != 0 && dynamic[ch] == 0 && m_mask[ch] != 0)
-                ++m_report.chans_grown;
-        dynamic = std::move(grown);
-    }
-    for (SizeType ch = 0; ch < n; ++ch)
-        if (dynamic[ch] != 0)
-            m_mask[ch] = 0;
-    m_report.chans_masked = count_zeros(m_mask);
 }
 
 // Device buffers of the full cleaning path for a block of d.nsamps rows.
@@ -657,6 +610,57 @@ void Cleaner::reserve_phase_buffers(const Dims& d) {
     m_zdot_sum.reserve(n * sizeof(ZdotSums));
     m_kpos_best.reserve(n * sizeof(Run));
     m_kneg_best.reserve(n * sizeof(Run));
+    m_clip_mean.reserve(sizeof(float));
+    m_clip_inv.reserve(sizeof(float));
+    // decision outputs
+    m_mask_d.reserve(n);
+    m_good_prefix.reserve((n + 1) * sizeof(uint64_t));
+    m_flagged_d.reserve(std::max<SizeType>(T, 1) * sizeof(uint64_t));
+    m_kchan_pos_d.reserve((kchan ? n : 1) * sizeof(Segment));
+    m_kchan_neg_d.reserve((kchan ? n : 1) * sizeof(Segment));
+    m_kchan_any_d.reserve(n);
+    m_flag_scratch.reserve(FlagScratch::size_for(T, c.broad_boxcar_max));
+    m_fw.carve(m_flag_scratch.get(), T, c.broad_boxcar_max);
+}
+
+ChannelMaskParams Cleaner::channel_params(const Dims& d) const {
+    const auto& c = m_cfg.c;
+    ChannelMaskParams p{};
+    p.n              = m_n;
+    p.nwin           = d.nwin;
+    p.moments        = c.moments_enabled ? 1 : 0;
+    p.need_clip      = m_need_moments ? 1 : 0;
+    p.stat_on[0]     = c.moments_mean ? 1 : 0;
+    p.stat_on[1]     = c.moments_std ? 1 : 0;
+    p.stat_on[2]     = c.moments_skewness ? 1 : 0;
+    p.stat_on[3]     = c.moments_kurtosis ? 1 : 0;
+    p.stat_on[4]     = c.moments_autocorr ? 1 : 0;
+    p.k              = c.moments_threshold;
+    p.kurt_max       = c.moments_kurtosis_max;
+    p.iqrm           = c.iqrm_enabled ? 1 : 0;
+    p.iqrm_threshold = c.iqrm_threshold;
+    p.grow           = c.mask_grow;
+    return p;
+}
+
+FlagParams Cleaner::flag_params(const Dims& d) const {
+    const auto& c = m_cfg.c;
+    FlagParams p{};
+    p.nsamps           = d.nsamps;
+    p.nchans           = m_n;
+    p.nwin             = d.nwin;
+    p.broad            = c.broad_enabled ? 1 : 0;
+    p.smooth_radius    = m_smooth_radius;
+    p.broad_threshold  = c.broad_threshold;
+    p.boxcar_max       = c.broad_boxcar_max;
+    p.dropout          = c.dropout_enabled ? 1 : 0;
+    p.dropout_fraction = c.dropout_min_std_fraction;
+    p.kspec            = c.kadane_spectrum_enabled ? 1 : 0;
+    p.zdot             = c.zero_dm == FROST_ZERO_DM_ZDOT ? 1 : 0;
+    p.kchan            = c.kadane_channel_enabled ? 1 : 0;
+    p.kchan_min_len    = static_cast<double>(c.kadane_channel_min_duration) / m_layout.tsamp;
+    p.kchan_threshold  = c.kadane_channel_threshold;
+    return p;
 }
 
 void Cleaner::preallocate() {
@@ -668,248 +672,73 @@ void Cleaner::preallocate() {
 
 void Cleaner::run_full(const Dims& d, cudaStream_t s) {
     reserve_phase_buffers(d);
-    const SizeType n     = m_n;
-    const SizeType nwin  = d.nwin;
-    const SizeType T     = d.nsamps;
-    const auto& c        = m_cfg.c;
-    const uint8_t* raw   = m_raw_ptr;
-    const bool zdot      = c.zero_dm == FROST_ZERO_DM_ZDOT;
-    const bool kchan     = c.kadane_channel_enabled != 0;
-    const bool kspec     = c.kadane_spectrum_enabled != 0;
+    const SizeType n   = m_n;
+    const auto& c      = m_cfg.c;
+    const uint8_t* raw = m_raw_ptr;
+    const bool zdot    = c.zero_dm == FROST_ZERO_DM_ZDOT;
+    const bool kchan   = c.kadane_channel_enabled != 0;
+    const bool kspec   = c.kadane_spectrum_enabled != 0;
+    auto* counters     = m_counters.as<unsigned long long>();
+    FB_CUDA(cudaMemsetAsync(counters, 0, kRepSlots * sizeof(unsigned long long), s));
 
     // ---- bandpass ----
-    auto t = Clock::now();
+    FB_CUDA(cudaEventRecord(m_ev[0], s));
     FB_CUDA(cudaMemsetAsync(m_unmeasured.get(), 0, n * sizeof(uint32_t), s));
     launch_sample_rows(d, raw, m_samples.as<float>(), s);
     launch_bandpass(d, m_samples.as<float>(), m_loc.as<float>(), m_scale.as<float>(),
                     m_inv.as<float>(), m_unmeasured.as<uint32_t>(), s);
-    std::vector<uint32_t> unmeasured;
-    std::vector<float> scale_h;
-    d2h(unmeasured, m_unmeasured, n, s);
-    if (c.iqrm_enabled)
-        d2h(scale_h, m_scale, nwin * n, s);
-    FB_CUDA(cudaStreamSynchronize(s));
-    m_report.t_bandpass = since(t);
+    FB_CUDA(cudaEventRecord(m_ev[1], s));
 
-    // ---- moments and channel mask ----
-    t = Clock::now();
-    std::vector<MomentSums> mom;
-    if (m_need_moments) {
+    // ---- moments and channel mask (lib/cpu/rfi_cpu_measure.cpp:140-300) ----
+    if (m_need_moments)
         launch_moments(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_static_mask_d.as<uint8_t>(),
                        m_clip, m_moments.as<MomentSums>(), s);
-        d2h(mom, m_moments, nwin * n, s);
-        FB_CUDA(cudaStreamSynchronize(s));
-        std::vector<float> cmean(nwin * n, 0.0F), cinv(nwin * n, 0.0F);
-        for (SizeType i = 0; i < nwin * n; ++i) {
-            const auto& sm = mom[i];
-            if (sm.nc > 1.0) {
-                const double mean = sm.c1 / sm.nc;
-                const double var  = (sm.c2 / sm.nc) - (mean * mean);
-                cmean[i]          = static_cast<float>(mean);
-                cinv[i]           = var > 0.0 ? static_cast<float>(1.0 / std::sqrt(var)) : 0.0F;
-            }
-        }
-        h2d(m_clip_mean, cmean.data(), nwin * n, s);
-        h2d(m_clip_inv, cinv.data(), nwin * n, s);
-    }
-    build_channel_mask(d, unmeasured, scale_h, mom);
-    std::vector<uint64_t> good_prefix(n + 1, 0);
-    for (SizeType ch = 0; ch < n; ++ch)
-        good_prefix[ch + 1] = good_prefix[ch] + (m_mask[ch] != 0 ? 1 : 0);
-    h2d(m_mask_d, m_mask.data(), n, s);
-    h2d(m_good_prefix, good_prefix.data(), n + 1, s);
-    m_report.t_moments = since(t);
+    decide_channel_mask(channel_params(d), m_cw, m_need_moments ? m_moments.as<MomentSums>() : nullptr,
+                        m_scale.as<float>(), m_unmeasured.as<uint32_t>(), m_static_mask_d.as<uint8_t>(),
+                        m_clip_mean.as<float>(), m_clip_inv.as<float>(), m_mask_d.as<uint8_t>(),
+                        m_good_prefix.as<uint64_t>(), counters, s);
+    FB_CUDA(cudaEventRecord(m_ev[2], s));
 
-    // ---- scan ----
-    t = Clock::now();
-    m_clip_mean.reserve(sizeof(float));
-    m_clip_inv.reserve(sizeof(float));
-
-    std::vector<float> s_det, row_std, lo, hi;
-    std::vector<uint8_t> kwhole;
-    std::vector<ZdotSums> zsum;
-    std::vector<Run> kpb, knb;
-    const bool any_good = good_prefix[n] != 0;
-    if (any_good) {
-        KspecParams kp{};
-        kp.enabled      = kspec ? 1 : 0;
-        kp.min_bw_chans = kspec ? static_cast<double>(c.kadane_spectrum_min_bandwidth) /
-                                      std::abs(m_layout.df)
-                                : 0.0;
-        kp.whole_chans = static_cast<double>(c.kadane_spectrum_whole_band_fraction) *
-                         static_cast<double>(n);
-        kp.threshold = c.kadane_spectrum_threshold;
-        launch_scan_rows(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(),
-                         m_clip, kp, m_good_prefix.as<uint64_t>(), m_s_det.as<float>(),
-                         m_s_keep_d.as<double>(), m_s_keep_f.as<float>(), m_row_std.as<float>(),
-                         m_kspec_pos.as<Span32>(), m_kspec_neg.as<Span32>(),
-                         m_kspec_whole.as<uint8_t>(), s);
-        launch_scan_cols(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(),
-                         m_clip, m_s_keep_d.as<double>(), zdot ? 1 : 0, kchan ? 1 : 0,
-                         m_clip_mean.as<float>(), m_clip_inv.as<float>(), m_chunk_min.as<float>(),
-                         m_chunk_max.as<float>(), m_chunk_zdot.as<ZdotSums>(),
-                         m_chunk_kpos.as<KadaneState>(), m_chunk_kneg.as<KadaneState>(),
-                         m_lo.as<float>(), m_hi.as<float>(), m_zdot_sum.as<ZdotSums>(),
-                         m_kpos_best.as<Run>(), m_kneg_best.as<Run>(), s);
-        d2h(s_det, m_s_det, T, s);
-        if (c.dropout_enabled)
-            d2h(row_std, m_row_std, T, s);
-        if (kspec)
-            d2h(kwhole, m_kspec_whole, T, s);
-        d2h(lo, m_lo, n, s);
-        d2h(hi, m_hi, n, s);
-        if (zdot)
-            d2h(zsum, m_zdot_sum, n, s);
-        if (kchan) {
-            d2h(kpb, m_kpos_best, n, s);
-            d2h(knb, m_kneg_best, n, s);
-        }
-    } else {
-        FB_CUDA(cudaMemsetAsync(m_s_keep_f.get(), 0, T * sizeof(float), s));
-        if (kspec) {
-            FB_CUDA(cudaMemsetAsync(m_kspec_pos.get(), 0xFF, T * sizeof(Span32), s));
-            FB_CUDA(cudaMemsetAsync(m_kspec_neg.get(), 0xFF, T * sizeof(Span32), s));
-        }
-    }
-    FB_CUDA(cudaStreamSynchronize(s));
-    m_report.t_scan = since(t);
+    // ---- scan (masked channels are skipped; with no good channel the
+    // series come out as frost's empty ones) ----
+    KspecParams kp{};
+    kp.enabled      = kspec ? 1 : 0;
+    kp.min_bw_chans = kspec ? static_cast<double>(c.kadane_spectrum_min_bandwidth) / std::abs(m_layout.df) : 0.0;
+    kp.whole_chans  = static_cast<double>(c.kadane_spectrum_whole_band_fraction) * static_cast<double>(n);
+    kp.threshold    = c.kadane_spectrum_threshold;
+    launch_scan_rows(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(), m_clip, kp,
+                     m_good_prefix.as<uint64_t>(), m_s_det.as<float>(), m_s_keep_d.as<double>(),
+                     m_s_keep_f.as<float>(), m_row_std.as<float>(), m_kspec_pos.as<Span32>(),
+                     m_kspec_neg.as<Span32>(), m_kspec_whole.as<uint8_t>(), s);
+    launch_scan_cols(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(), m_clip,
+                     m_s_keep_d.as<double>(), zdot ? 1 : 0, kchan ? 1 : 0, m_clip_mean.as<float>(),
+                     m_clip_inv.as<float>(), m_chunk_min.as<float>(), m_chunk_max.as<float>(),
+                     m_chunk_zdot.as<ZdotSums>(), m_chunk_kpos.as<KadaneState>(), m_chunk_kneg.as<KadaneState>(),
+                     m_lo.as<float>(), m_hi.as<float>(), m_zdot_sum.as<ZdotSums>(), m_kpos_best.as<Run>(),
+                     m_kneg_best.as<Run>(), s);
+    FB_CUDA(cudaEventRecord(m_ev[3], s));
 
     // ---- flags (lib/cpu/rfi_cpu.cpp:347-468) ----
-    t = Clock::now();
-    if (any_good) {
-        for (SizeType ch = 0; ch < n; ++ch) {
-            if (m_mask[ch] == 0 || unmeasured[ch] < nwin)
-                continue;
-            if (!(hi[ch] > lo[ch])) {
-                m_mask[ch] = 0;
-                ++m_report.chans_dead;
-            }
-        }
-    }
-    m_report.chans_masked = count_zeros(m_mask);
-    m_time_flags.assign(T, 0U);
-    std::vector<Segment> kcp, kcn;
-    if (any_good) {
-        if (c.broad_enabled)
-            m_report.samps_broad = stats::broadband_time_flags(
-                s_det, m_smooth_radius, c.broad_threshold, c.broad_boxcar_max, m_time_flags);
-        if (c.dropout_enabled) {
-            std::vector<float> spread = row_std;
-            const auto mid = spread.begin() + static_cast<IndexType>(T / 2);
-            std::nth_element(spread.begin(), mid, spread.end());
-            const float cut = c.dropout_min_std_fraction * *mid;
-            std::vector<uint8_t> drop(T, 0U);
-            for (SizeType i = 0; i < T; ++i) {
-                if (row_std[i] < cut) {
-                    drop[i] = 1;
-                    if (i > 0)
-                        drop[i - 1] = 1;
-                    if (i + 1 < T)
-                        drop[i + 1] = 1;
-                }
-            }
-            for (SizeType i = 0; i < T; ++i) {
-                if (drop[i] != 0 && m_time_flags[i] == 0) {
-                    m_time_flags[i] = 1;
-                    ++m_report.samps_dropout;
-                }
-            }
-        }
-        if (kspec) {
-            for (SizeType i = 0; i < T; ++i) {
-                if (kwhole[i] != 0 && m_time_flags[i] == 0) {
-                    m_time_flags[i] = 1;
-                    ++m_report.samps_kadane;
-                }
-            }
-        }
-        m_report.samps_flagged =
-            static_cast<SizeType>(std::count(m_time_flags.begin(), m_time_flags.end(), 1U));
-        if (zdot) {
-            m_zdot_a.assign(n, 0.0F);
-            m_zdot_b.assign(n, 0.0F);
-            for (SizeType ch = 0; ch < n; ++ch) {
-                const ZdotSums& sm = zsum[ch];
-                if (sm.n < 2.0)
-                    continue;
-                const double mz    = sm.sz / sm.n;
-                const double ms    = sm.ss / sm.n;
-                const double var_s = (sm.sss / sm.n) - (ms * ms);
-                const double cov   = (sm.szs / sm.n) - (mz * ms);
-                const double a     = var_s > 0.0 ? cov / var_s : 0.0;
-                m_zdot_a[ch]       = static_cast<float>(a);
-                m_zdot_b[ch]       = static_cast<float>(mz - (a * ms));
-            }
-        }
-        if (kchan) {
-            const double min_len = static_cast<double>(c.kadane_channel_min_duration) / m_layout.tsamp;
-            kcp.assign(n, Segment{0, -1});
-            kcn.assign(n, Segment{0, -1});
-            auto accept = [&](const Run& r, Segment& out) {
-                const auto len = static_cast<double>(r.length());
-                if (len > 0.0 && len >= min_len && r.sum / std::sqrt(len) > c.kadane_channel_threshold)
-                    out = {r.start, r.end};
-            };
-            for (SizeType ch = 0; ch < n; ++ch) {
-                if (m_mask[ch] == 0)
-                    continue;
-                accept(kpb[ch], kcp[ch]);
-                accept(knb[ch], kcn[ch]);
-            }
-        }
-    }
-    m_report.t_flags = since(t);
+    decide_flags(flag_params(d), m_fw, m_good_prefix.as<uint64_t>(), m_unmeasured.as<uint32_t>(),
+                 m_lo.as<float>(), m_hi.as<float>(), m_s_det.as<float>(), m_row_std.as<float>(),
+                 m_kspec_whole.as<uint8_t>(), m_zdot_sum.as<ZdotSums>(), m_kpos_best.as<Run>(),
+                 m_kneg_best.as<Run>(), m_mask_d.as<uint8_t>(), m_time_flags_d.as<uint8_t>(),
+                 m_zdot_a_d.as<float>(), m_zdot_b_d.as<float>(), m_kchan_pos_d.as<Segment>(),
+                 m_kchan_neg_d.as<Segment>(), m_kchan_any_d.as<uint8_t>(), m_flagged_d.as<uint64_t>(), counters,
+                 s);
+    FB_CUDA(cudaEventRecord(m_ev[4], s));
 
     // ---- apply (lib/cpu/rfi_cpu.cpp:526-720) ----
-    t = Clock::now();
-    std::vector<uint64_t> flagged;
-    for (SizeType i = 0; i < T; ++i)
-        if (m_time_flags[i] != 0)
-            flagged.push_back(i);
-    h2d(m_time_flags_d, m_time_flags.data(), T, s);
-    h2d(m_mask_d, m_mask.data(), n, s);
-    h2d(m_zdot_a_d, m_zdot_a.data(), n, s);
-    h2d(m_zdot_b_d, m_zdot_b.data(), n, s);
-    // channels with a Kadane-along-time segment (the rest skip the test)
-    std::vector<uint8_t> kany(n, 0);
-    bool any_segment = false;
-    if (kchan) {
-        for (SizeType ch = 0; ch < n; ++ch) {
-            kany[ch]    = (kcp[ch].start <= kcp[ch].end || kcn[ch].start <= kcn[ch].end) ? 1 : 0;
-            any_segment = any_segment || kany[ch] != 0;
-        }
-        h2d(m_kchan_pos_d, kcp.data(), n, s);
-        h2d(m_kchan_neg_d, kcn.data(), n, s);
-    } else {
-        m_kchan_pos_d.reserve(sizeof(Segment));
-        m_kchan_neg_d.reserve(sizeof(Segment));
-    }
-    h2d(m_kchan_any_d, kany.data(), n, s);
-    h2d(m_flagged_d, flagged.data(), flagged.size(), s);
-    FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, kCountSlots * sizeof(unsigned long long), s));
     const ApplyParams p = apply_params();
-    ApplyParams pu      = p;
-    if (!any_segment)
-        pu.kchan = 0; // no segment anywhere: no cell can be a Kadane-channel cell
-    launch_apply_unflagged(d, pu, raw, m_loc.as<float>(), m_scale.as<float>(), m_inv.as<float>(),
-                           m_mask_d.as<uint8_t>(), m_time_flags_d.as<uint8_t>(),
-                           m_kspec_pos.as<Span32>(), m_kspec_neg.as<Span32>(),
-                           m_kchan_pos_d.as<Segment>(), m_kchan_neg_d.as<Segment>(),
-                           m_kchan_any_d.as<uint8_t>(),
-                           m_s_keep_f.as<float>(), m_zdot_a_d.as<float>(), m_zdot_b_d.as<float>(),
-                           m_work.as<float>(), m_counters.as<unsigned long long>(), s);
-    launch_apply_flagged(d, p, m_flagged_d.as<uint64_t>(), flagged.size(), m_loc.as<float>(),
+    launch_apply_unflagged(d, p, raw, m_loc.as<float>(), m_scale.as<float>(), m_inv.as<float>(),
+                           m_mask_d.as<uint8_t>(), m_time_flags_d.as<uint8_t>(), m_kspec_pos.as<Span32>(),
+                           m_kspec_neg.as<Span32>(), m_kchan_pos_d.as<Segment>(), m_kchan_neg_d.as<Segment>(),
+                           m_kchan_any_d.as<uint8_t>(), m_s_keep_f.as<float>(), m_zdot_a_d.as<float>(),
+                           m_zdot_b_d.as<float>(), m_work.as<float>(), counters, s);
+    launch_apply_flagged(d, p, m_flagged_d.as<uint64_t>(), counters + kRepFlagged, m_loc.as<float>(),
                          m_scale.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(),
-                         m_time_flags_d.as<uint8_t>(), m_work.as<float>(),
-                         m_counters.as<unsigned long long>(), s);
-    unsigned long long counts[kCountSlots];
-    FB_CUDA(cudaMemcpyAsync(counts, m_counters.get(), sizeof(counts), cudaMemcpyDeviceToHost, s));
-    FB_CUDA(cudaStreamSynchronize(s));
-    m_report.cells_narrow          = counts[kCountNarrow];
-    m_report.cells_kadane_spectrum = counts[kCountKspec];
-    m_report.cells_kadane_channel  = counts[kCountKchan];
-    m_report.fill_fallbacks        = counts[kCountFallback];
-    m_report.t_apply               = since(t);
+                         m_time_flags_d.as<uint8_t>(), m_work.as<float>(), counters, s);
+    FB_CUDA(cudaEventRecord(m_ev[5], s));
 }
 
 } // namespace fb::rfi

@@ -1,7 +1,8 @@
 // RFICleaner on the GPU: frost's per-gulp RFI excision and normalisation
 // (include/frost/prepare/rfi.hpp:243-297, lib/cpu/rfi_cpu.cpp) with every
-// T x C pass as a CUDA kernel and the per-gulp decisions on the short series
-// those passes reduce the block to.
+// T x C pass as a CUDA kernel and the per-gulp decisions as device kernels
+// on the short series those passes reduce the block to (rfi_decide.cu), so
+// a gulp runs without host round trips until its results are read back.
 #pragma once
 
 #include <cstdint>
@@ -12,6 +13,7 @@
 #include <cuda_runtime_api.h>
 
 #include "common.hpp"
+#include "rfi_decide.hpp"
 #include "rfi_kernels.hpp"
 
 namespace fb::rfi {
@@ -51,7 +53,9 @@ public:
 
     const std::vector<uint8_t>& channel_mask() const { return m_mask; }
     const frost_rfi_report& report() const { return m_report; }
-    const std::vector<uint8_t>& time_flags() const { return m_time_flags; }
+    /** Per-sample flags of the last call (1 = flagged), read back from the
+     * device on first use after the call. */
+    const std::vector<uint8_t>& time_flags() const;
     const float* output() const { return m_out.as<float>(); }
     SizeType capacity() const { return m_capacity; }
     SizeType nchans() const { return m_n; }
@@ -84,13 +88,26 @@ private:
     float m_eq_loc = 0.0F, m_eq_scale = 1.0F;
     uint64_t m_block_index = 0;
 
-    std::vector<uint8_t> m_static_mask, m_mask, m_time_flags;
+    std::vector<uint8_t> m_static_mask, m_mask;
     frost_rfi_report m_report{};
     SizeType m_capacity = 0;
+    // time flags of the last call: m_flags_len samples, on the device unless
+    // the call flagged nothing by construction (short blocks)
+    mutable std::vector<uint8_t> m_time_flags;
+    mutable bool m_flags_fresh = true;
+    SizeType m_flags_len       = 0;
+    bool m_flags_on_device     = false;
 
-    // Retained calibration for short tails (lib/cpu/rfi_cpu.cpp:209-244).
+    // Retained calibration for short tails (lib/cpu/rfi_cpu.cpp:209-244);
+    // the zero-DM fit stays in m_zdot_a_d / m_zdot_b_d.
     bool m_tail_ready = false;
-    std::vector<float> m_zdot_a, m_zdot_b;
+
+    // Decision scratch (rfi_decide.hpp) and the IQRM lags of this band.
+    std::vector<uint64_t> m_lags;
+    DeviceBuffer m_chan_scratch, m_flag_scratch;
+    ChannelScratch m_cw{};
+    FlagScratch m_fw{};
+    cudaEvent_t m_ev[6] = {};
 
     // Device workspace.
     DeviceBuffer m_raw, m_samples, m_loc, m_scale, m_inv, m_loc2, m_scale2, m_unmeasured,
@@ -112,8 +129,9 @@ private:
 
     void run_full(const Dims& d, cudaStream_t s);
     void normalize_short(SizeType capacity, SizeType valid, cudaStream_t s);
-    void build_channel_mask(const Dims& d, const std::vector<uint32_t>& unmeasured,
-                            const std::vector<float>& scale, const std::vector<MomentSums>& mom);
+    ChannelMaskParams channel_params(const Dims& d) const;
+    FlagParams flag_params(const Dims& d) const;
+    void read_back(cudaStream_t s);
 };
 
 } // namespace fb::rfi

@@ -1084,21 +1084,15 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
 // from a random unflagged row within the time-fill radius (already final),
 // or rebuilds the spectrum in noise units and removes its band mean when a
 // zero-DM transform is on. The band-mean sum keeps channel order.
-__global__ void k_apply_flagged(Dims d, ApplyParams p, const uint64_t* __restrict__ flagged,
-                                const float* __restrict__ loc, const float* __restrict__ scale,
-                                const float* __restrict__ inv, const uint8_t* __restrict__ mask,
-                                const uint8_t* __restrict__ time_flags, float* __restrict__ work,
-                                unsigned long long* __restrict__ counters) {
-    extern __shared__ unsigned char smem[];
-    const uint64_t n  = d.nchans;
-    float* sv         = reinterpret_cast<float*>(smem);
-    uint8_t* contrib  = reinterpret_cast<uint8_t*>(sv + n);
-    __shared__ float s_mean;
-    __shared__ unsigned long long s_fallbacks;
+__device__ void apply_flagged_row(const Dims& d, const ApplyParams& p, uint64_t t, const float* __restrict__ loc,
+                                  const float* __restrict__ scale, const float* __restrict__ inv,
+                                  const uint8_t* __restrict__ mask, const uint8_t* __restrict__ time_flags,
+                                  float* __restrict__ work, unsigned long long* __restrict__ counters,
+                                  float* sv, uint8_t* contrib, float& s_mean, unsigned long long& s_fallbacks) {
+    const uint64_t n = d.nchans;
     if (threadIdx.x == 0)
         s_fallbacks = 0;
     __syncthreads();
-    const uint64_t t  = flagged[blockIdx.x];
     const uint64_t w  = window_of(t, d.window, d.nwin);
     const uint64_t r  = p.time_fill_radius;
     const uint64_t lo = t > r ? t - r : 0;
@@ -1168,6 +1162,25 @@ __global__ void k_apply_flagged(Dims d, ApplyParams p, const uint64_t* __restric
     }
     if (threadIdx.x == 0 && s_fallbacks)
         atomicAdd(&counters[kCountFallback], s_fallbacks);
+    __syncthreads();
+}
+
+// The flagged rows listed in flagged[0 .. *count), a row per CTA at a time
+// (the count is known only on the device).
+__global__ void k_apply_flagged(Dims d, ApplyParams p, const uint64_t* __restrict__ flagged,
+                                const unsigned long long* __restrict__ count, const float* __restrict__ loc,
+                                const float* __restrict__ scale, const float* __restrict__ inv,
+                                const uint8_t* __restrict__ mask, const uint8_t* __restrict__ time_flags,
+                                float* __restrict__ work, unsigned long long* __restrict__ counters) {
+    extern __shared__ unsigned char smem[];
+    float* sv        = reinterpret_cast<float*>(smem);
+    uint8_t* contrib = reinterpret_cast<uint8_t*>(sv + d.nchans);
+    __shared__ float s_mean;
+    __shared__ unsigned long long s_fallbacks;
+    const unsigned long long rows = *count;
+    for (unsigned long long i = blockIdx.x; i < rows; i += gridDim.x)
+        apply_flagged_row(d, p, flagged[i], loc, scale, inv, mask, time_flags, work, counters, sv, contrib, s_mean,
+                          s_fallbacks);
 }
 
 // ---- re-measure and normalise ---------------------------------------------
@@ -1665,15 +1678,16 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
 }
 
 void launch_apply_flagged(const Dims& d, const ApplyParams& p, const uint64_t* flagged,
-                          uint64_t nflagged, const float* loc, const float* scale,
+                          const unsigned long long* nflagged, const float* loc, const float* scale,
                           const float* inv, const uint8_t* mask, const uint8_t* time_flags,
                           float* work, unsigned long long* counters, cudaStream_t s) {
-    if (nflagged == 0)
+    if (d.nsamps == 0)
         return;
-    const size_t smem = d.nchans * (sizeof(float) + 1);
+    const size_t smem     = d.nchans * (sizeof(float) + 1);
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(d.nsamps, 148 * 8));
     set_smem(reinterpret_cast<const void*>(&k_apply_flagged), smem);
-    k_apply_flagged<<<static_cast<unsigned>(nflagged), 256, smem, s>>>(
-        d, p, flagged, loc, scale, inv, mask, time_flags, work, counters);
+    k_apply_flagged<<<blocks, 256, smem, s>>>(d, p, flagged, nflagged, loc, scale, inv, mask, time_flags, work,
+                                              counters);
     FB_COUNT_LAUNCH();
 }
 

@@ -104,9 +104,10 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
                             const float* zdot_b, float* work, unsigned long long* counters,
                             cudaStream_t s);
 
-// Refills the listed flagged rows of work from unflagged rows.
+// Refills the flagged rows flagged[0 .. *nflagged) of work from unflagged
+// rows (the count is read on the device).
 void launch_apply_flagged(const Dims& d, const ApplyParams& p, const uint64_t* flagged,
-                          uint64_t nflagged, const float* loc, const float* scale,
+                          const unsigned long long* nflagged, const float* loc, const float* scale,
                           const float* inv, const uint8_t* mask, const uint8_t* time_flags,
                           float* work, unsigned long long* counters, cudaStream_t s);
 

@@ -62,6 +62,7 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     if (kill_mask != nullptr)
         for (int32_t c = 0; c < C; ++c)
             m_mask[c] = kill_mask[c] != 0 ? 1 : 0;
+    m_kill = m_mask;
 
     // Level ops.
     const int L = m_plan.levels();
@@ -477,6 +478,27 @@ void Engine::set_residency(int32_t ctas_per_sm) {
     m_ctas_per_sm = ctas_per_sm;
 }
 
+void Engine::set_wait_limit(long long tries) {
+    DeviceGuard g(m_device);
+    FB_CUDA(cudaStreamSynchronize(m_stream));
+    if (m_graph != nullptr) {
+        // the captured launches carry the old limit
+        FB_CUDA(cudaGraphExecDestroy(m_graph));
+        m_graph = nullptr;
+    }
+    m_wait_limit = tries < 0 ? kDefaultWaitLimit : tries;
+}
+
+void Engine::restart() {
+    DeviceGuard g(m_device);
+    FB_CUDA(cudaStreamSynchronize(m_stream));
+    apply_shape(m_fuse, m_level_tpc, m_level2_stages, m_search_chunk);
+    m_mask = m_kill;
+    m_results.clear();
+    m_dropped_global = 0;
+    m_dropped_per_dm = 0;
+}
+
 Engine::Tuned Engine::launch_shape() const {
     return Tuned{m_fuse, m_level_tpc, m_level2_stages, m_search_chunk, 0.0, false};
 }
@@ -626,6 +648,7 @@ SearchParams Engine::params(int64_t tile_off, int32_t n_valid) const {
     p.wmax         = m_plan.widths().back();
     p.halo         = search_halo(p.wmax);
     p.err          = reinterpret_cast<unsigned*>(m_counters.as<unsigned long long>() + 3);
+    p.wait_limit   = m_wait_limit;
     p.thresh       = m_cfg.detect_thresh;
     p.peak_mode    = m_cfg.peak_mode;
     p.trapezoid    = m_cfg.use_trapezoid ? 1 : 0;
@@ -789,11 +812,11 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                     if (st.fused)
                         launch_level2(m_fused_ops.as<FusedOp>() + st.op_offset, m_plan.level_rows(h),
                                       view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc,
-                                      m_level2_stages, cta_cap());
+                                      m_level2_stages, cta_cap(), m_wait_limit);
                     else
                         launch_level(m_row_ops.as<RowOp>() + st.op_offset, m_plan.level_rows(h),
                                      view(st.in), out, static_cast<int32_t>(m_ncols), err, s, m_level_tpc,
-                                     cta_cap());
+                                     cta_cap(), m_wait_limit);
                 });
                 m_launches += 1;
                 m_timing.level_launches += 1;

@@ -47,6 +47,13 @@ public:
     uint64_t last_launches() const { return m_launches; }
     void enable_timing(bool on);
     const frost_search_timing& timing() const { return m_timing; }
+    /** Tries of the level and search kernels' first wait on each bulk copy
+     * (negative: the default; 0: give up at once); a drain after a give-up
+     * always uses the default. */
+    void set_wait_limit(long long tries);
+    /** Starts the stream afresh: histories and run states cleared, sample
+     * count zero, the constructor's mask current (after a failed gulp). */
+    void restart();
 
 private:
     enum Phase { kLevel1, kLevel, kSearch, kHistory, kVariance, kPhases };
@@ -68,6 +75,8 @@ private:
     int m_device;
     cudaStream_t m_stream = nullptr;
     cudaEvent_t m_order   = nullptr; // orders the caller's stream before the engine's
+    long long m_wait_limit = kDefaultWaitLimit;
+    std::vector<uint8_t> m_kill; // the constructor's mask
     bool m_fp16;
     int64_t m_tile = 0, m_ncols = 0;
     // Per stored level: history columns before base (the level's own

@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
         int ci = 0;
         for (int64_t c0 = 0; c0 < p.n_valid; c0 += CH, ++ci) {
             // ---- wait for the chunk's segment (bounded; a timeout ends the row)
-            if (!bulk::mbar_wait(&bar[(cc + ci) & 1], static_cast<uint32_t>(((cc + ci) >> 1) & 1)))
+            if (!bulk::mbar_wait(&bar[(cc + ci) & 1], static_cast<uint32_t>(((cc + ci) >> 1) & 1), p.wait_limit))
                 atomicExch(&abort_flag, 1);
             __syncthreads();
             if (abort_flag)
@@ -952,6 +952,8 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
         throw Error(FROST_ERR_INTERNAL, "search: tile columns are not a whole number of chunks");
     if (p.err == nullptr)
         throw Error(FROST_ERR_INTERNAL, "search: no error flag");
+    if (p.wait_limit < 0)
+        throw Error(FROST_ERR_INTERNAL, "search: wait limit must be >= 0");
     const size_t es   = level.fp16 ? 2 : 4;
     const size_t seg  = static_cast<size_t>(p.halo) + chunk;
     // Ps, gmin (+4 padding), tmin, the next chunk's halo by parity, the bit

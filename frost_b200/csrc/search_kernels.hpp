@@ -81,6 +81,7 @@ struct SearchParams {
     uint32_t max_per_dm;     // 0 = unlimited
     unsigned long long* dropped; // [0] global, [1] per DM
     unsigned* err;           // set when a bounded wait for staged data ran out
+    long long wait_limit;    // tries of a chunk's first wait (a drain uses kSpinLimit)
 };
 
 /** Searches rows [g0, g1) (all in `level`) over the tile's valid columns,

@@ -225,6 +225,16 @@ class FDMTBoxcar:
         check(lib().frost_search_get_residency(self._h, C.byref(v)))
         return v.value
 
+    def set_wait_limit(self, tries: int = -1):
+        """Bound (mbarrier tries) of the kernels' first wait on each bulk
+        copy; negative restores the default, 0 gives up at once. A
+        diagnostic of the timeout path."""
+        check(lib().frost_search_set_wait_limit(self._h, int(tries)))
+
+    def restart(self):
+        """Starts the stream afresh (after a gulp that failed)."""
+        check(lib().frost_search_restart(self._h))
+
     def use_graphs(self, enable: bool = True):
         """CUDA-graph replay of the per-gulp launch sequence (default on)."""
         check(lib().frost_search_use_graphs(self._h, 1 if enable else 0))
@@ -248,19 +258,23 @@ class FDMTBoxcar:
         return out
 
 
-def candidate_list_diff(ref: np.ndarray, other: np.ndarray, snr_min: float = 7.0) -> dict:
+def candidate_list_diff(ref: np.ndarray, other: np.ndarray, snr_min: float = 7.0,
+                        tie_rtol: float = 1e-2) -> dict:
     """Compares two candidate lists of the same stream (for example FP16
     plane storage against FP32) above `snr_min`.
 
     A detection is keyed by (subband_level, subband_idx, dm_idx, filter_idx).
     A detection of either list at S/N >= snr_min is `matched` when the other
     list (at any S/N it reports, down to its detection threshold) has the
-    same key and the same peak sample, `moved` when the other list's
-    detection of that key covers the same run with a different peak (a near
-    tie inside the run), and `only_ref` / `only_other` otherwise.
-    `max_snr_rel_err` is the largest relative S/N difference over matched
-    and moved pairs; `edge` counts matched pairs with one side below
-    snr_min (a threshold crossing, not a missing detection)."""
+    same key and the same peak sample; `moved` when the other list's
+    detection of that key covers the same run with a different peak whose
+    S/N is within tie_rtol (a near tie inside the run); otherwise it counts
+    in `only_ref` / `only_other` (no detection of that key covers it, or the
+    covering run peaks elsewhere with a different S/N: runs split or merged
+    at the detection threshold). `max_snr_rel_err` is the largest relative
+    S/N difference over matched pairs, `moved_max_snr_rel_err` over moved
+    ones; `edge` counts matched pairs with one side below snr_min (a
+    threshold crossing, not a missing detection)."""
     def index(cs):
         out = {}
         for c in cs:
@@ -270,7 +284,7 @@ def candidate_list_diff(ref: np.ndarray, other: np.ndarray, snr_min: float = 7.0
         return out
     a, b = index(ref), index(other)
     res = {"snr_min": snr_min, "n_ref": 0, "n_other": 0, "matched": 0, "moved": 0, "only_ref": 0,
-           "only_other": 0, "edge": 0, "max_snr_rel_err": 0.0}
+           "only_other": 0, "edge": 0, "max_snr_rel_err": 0.0, "moved_max_snr_rel_err": 0.0}
 
     def walk(x, y, count_key, only_key, pairs):
         for k, lst in x.items():
@@ -278,17 +292,25 @@ def candidate_list_diff(ref: np.ndarray, other: np.ndarray, snr_min: float = 7.0
                 if snr < snr_min:
                     continue
                 res[count_key] += 1
-                same = [d for d in y.get(k, []) if d[2] == pk]
-                hit = same or [d for d in y.get(k, []) if d[0] <= pk <= d[1] or beg <= d[2] <= end]
-                if not hit:
-                    res[only_key] += 1
+                cand = y.get(k, [])
+                same = [d for d in cand if d[2] == pk]
+                if same:
+                    # the second walk counts only pairs the first one skipped
+                    # (the reference side below snr_min)
+                    if pairs or same[0][3] < snr_min:
+                        res["matched"] += 1
+                        res["max_snr_rel_err"] = max(res["max_snr_rel_err"], abs(same[0][3] - snr) / abs(snr))
+                        res["edge"] += int(same[0][3] < snr_min)
                     continue
-                # the second walk counts only pairs the first one skipped
-                # (the reference side below snr_min)
-                if pairs or hit[0][3] < snr_min:
-                    res["matched" if same else "moved"] += 1
-                    res["max_snr_rel_err"] = max(res["max_snr_rel_err"], abs(hit[0][3] - snr) / abs(snr))
-                    res["edge"] += int(hit[0][3] < snr_min)
+                near = [d for d in cand if (d[0] <= pk <= d[1] or beg <= d[2] <= end)
+                        and abs(d[3] - snr) <= tie_rtol * abs(snr)]
+                if near:
+                    if pairs or near[0][3] < snr_min:
+                        res["moved"] += 1
+                        res["moved_max_snr_rel_err"] = max(res["moved_max_snr_rel_err"],
+                                                           abs(near[0][3] - snr) / abs(snr))
+                    continue
+                res[only_key] += 1
     walk(a, b, "n_ref", "only_ref", True)
     walk(b, a, "n_other", "only_other", False)
     res["identical"] = res["only_ref"] == 0 and res["only_other"] == 0 and res["moved"] == 0

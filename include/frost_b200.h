@@ -505,6 +505,21 @@ int frost_search_use_graphs(frost_search* s, int enable);
  * cudaStream_t), on which it runs every launch of a gulp. */
 int frost_search_get_stream(const frost_search* s, void** stream);
 
+/* No counterpart in the reference; a diagnostic of the error path. The
+ * pipelined level and search kernels wait for each bulk copy a bounded
+ * number of tries (mbarrier.try_wait); a wait that runs out makes the call
+ * fail with FROST_ERR_TIMEOUT instead of hanging. `tries` sets that bound
+ * for the first wait on each copy (a negative value restores the default,
+ * 2^22; 0 gives up at once, which forces the timeout path); a kernel that
+ * gave up still waits for every copy it has in flight, with the default
+ * bound, before it exits. */
+int frost_search_set_wait_limit(frost_search* s, int64_t tries);
+
+/* No counterpart in the reference. Starts the stream afresh (histories and
+ * open runs cleared, sample count zero, the constructor's mask current), as
+ * after a gulp that failed with FROST_ERR_TIMEOUT. */
+int frost_search_restart(frost_search* s);
+
 /* No counterpart in the reference. Measures this geometry's FDMT launch
  * shapes (fused two-level steps with 2, 3 or 4 bulk-copy stages, or single
  * levels; 4, 8, 16, 32, 64 or 128 tiles of 2048 samples per level-kernel CTA) with

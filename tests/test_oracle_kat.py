@@ -1,6 +1,7 @@
 """Known-answer tests that pin the oracle (the reference's own CPU code built
-into oracle/_ref) and this library's host-side logic to the reference's own
-golden vectors. CPU only."""
+into oracle/_ref) and this library to the reference's own golden vectors.
+The library's IQRM runs on the GPU, so its cases are marked gpu; the rest
+is CPU only."""
 
 import json
 import os
@@ -30,7 +31,10 @@ def iqrm_cases():
         yield x, case, ig
 
 
-@pytest.mark.parametrize("impl", ["reference", "frost_b200"])
+GPU_IMPL = pytest.param("frost_b200", marks=pytest.mark.gpu)
+
+
+@pytest.mark.parametrize("impl", ["reference", GPU_IMPL])
 def test_iqrm_golden_vectors(ref, impl):
     """rfi_test.cpp:213-257: Morello et al. (2022) synthetic channels."""
     fn = ref.iqrm_mask if impl == "reference" else frfi.iqrm_mask
@@ -38,7 +42,7 @@ def test_iqrm_golden_vectors(ref, impl):
         assert flagged(fn(x, case["radius"], case["threshold"], ig)) == case["expected"], case
 
 
-@pytest.mark.parametrize("impl", ["reference", "frost_b200"])
+@pytest.mark.parametrize("impl", ["reference", GPU_IMPL])
 def test_iqrm_noise_tophat_and_limits(ref, impl):
     fn = ref.iqrm_mask if impl == "reference" else frfi.iqrm_mask
     rng = np.random.default_rng(3)
@@ -55,6 +59,7 @@ def test_iqrm_noise_tophat_and_limits(ref, impl):
         fn(x, 3, 0.0)
 
 
+@pytest.mark.gpu
 def test_iqrm_matches_reference_on_random_inputs(ref):
     """Lag saturation and ignore handling (iqrm_limits_test.cpp:8-28) plus
     random statistics with ignored channels: identical flags."""

@@ -403,3 +403,31 @@ def test_device_waterfall_written_on_a_caller_stream():
     rc = lib().frost_search_execute(eng._h, C.cast(C.c_void_p(wf.data_ptr()), C.POINTER(C.c_float)),
                                     gulp, 1, None, None)
     assert rc == -1 and "null stream" in lib().frost_last_error().decode()
+
+
+def test_bounded_wait_timeout_is_reported_and_the_stream_restarts():
+    """The level and search kernels' bounded waits on their bulk copies:
+    with the first-wait bound at zero every kernel gives up at once, lets
+    its copies in flight land (waiting with the default bound) and sets the
+    error flag, so execute fails with FROST_ERR_TIMEOUT instead of hanging
+    (frost maps device failures to exceptions, lib/cuda/gpu_utils.cuh:13-20).
+    After the default bound is restored and the stream restarted, the engine
+    gives a fresh engine's candidates, graphs on or off."""
+    from frost_b200._lib import FrostError
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=1, gulp=8192)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0)
+    stream = make_stream(pc, 2, seed=33, pulses=PULSES)
+    gulp = pc.block_nsamps
+    ref = run_engine(FDMTBoxcar(pc, bc), stream, gulp)
+    assert ref.size > 0
+    for graphs in (True, False):
+        eng = FDMTBoxcar(pc, bc)
+        eng.use_graphs(graphs)
+        eng.set_wait_limit(0)
+        with pytest.raises(FrostError) as e:
+            eng.execute(np.ascontiguousarray(stream[:, :gulp]))
+        assert e.value.code == -4 and "bounded wait" in str(e.value)
+        eng.set_wait_limit(-1)
+        eng.restart()
+        assert np.array_equal(run_engine(eng, stream, gulp), ref), graphs
