@@ -586,13 +586,25 @@ def run_reference(args):
 SERVING = dict(beams=64, gulp=65536, gulps=4, tile=16384, slots=8, jitter_s=0.05)
 
 
+def serving_gulp(beam, C, is_float, dm_max):
+    """One beam's seeded 65536-sample gulp of the 4096-channel recipe scaled
+    to its band: 4 dispersed pulses (DM 100 to dm_max - 100, widths 1-128,
+    S/N 7-50), 5 % noisy channels, 5 zero-DM bursts and a dropout."""
+    from frost_b200.synth import make_filterbank
+    foff = -336.0 / C
+    return make_filterbank(C, SERVING["gulp"], 1536.0 + foff / 2, foff, TSAMP, beam_seed(0, 1000 + beam),
+                           dtype="float32" if is_float else "uint8", n_pulses=4,
+                           dm_range=(100.0, dm_max - 100.0), width_range=(1.0, 128.0), snr_range=(7.0, 50.0),
+                           rfi_channel_fraction=0.05, n_bursts=5, n_dropouts=1).data
+
+
 def run_serving(args):
     """Beams at real-time cadence: 64 simulated beams (1024 or 4096 channels,
-    uint8 or float32, DM max 1000-3000, 4 sub-band planes) each emit 65536-
-    sample gulps every 65536 x 64 us = 4.19 s with exponential arrival
-    jitter; the server admits beams by device memory and reports the gulp
-    latency (arrival to candidates ready) of every gulp after each beam's
-    first. Each (channels, sample type) class replays one seeded gulp."""
+    uint8 or float32, DM max 1000-3000, 4 sub-band planes) each emit their
+    own seeded 65536-sample gulps (the noise, RFI and pulse recipe) every
+    65536 x 64 us = 4.19 s with exponential arrival jitter; the server
+    admits beams by device memory and reports the gulp latency (arrival to
+    candidates ready) of every gulp after each beam's first."""
     import numpy as np
     import torch
 
@@ -610,53 +622,56 @@ def run_serving(args):
     rng = np.random.default_rng(0x46524F5354)
     classes = [(1024, DataType.UINT8), (1024, DataType.FLOAT32), (4096, DataType.UINT8),
                (4096, DataType.FLOAT32)]
-    host = {}
-    gen = torch.Generator(device="cuda").manual_seed(5)
-    for C, dt in classes:
-        x = torch.randn((gulp, C), generator=gen, device="cuda") * 16.0 + 128.0
-        x = x.clamp(0, 255).round().to(torch.uint8) if dt == DataType.UINT8 else x.float()
-        buf = torch.empty(x.numel() * x.element_size(), dtype=torch.uint8, pin_memory=True)
-        buf.copy_(x.reshape(-1).view(torch.uint8).cpu())
-        host[(C, dt)] = buf
     srv = BeamServer(device=local, slots=S["slots"])
     from frost_b200.config import BoxcarConfig, Storage as St
     bc = BoxcarConfig(max_boxcar=256, wtsp=2.0, detect_thresh=6.0, storage=St.FP16,
                       max_candidates=1 << 18, max_cands_per_dm=4096, tile_nsamps=S["tile"])
     admitted, refused = [], 0
+    t_gen = time.perf_counter()
     for b in range(S["beams"]):
         C, dt = classes[b % 4]
         foff = -336.0 / C
+        dm_max = float(rng.uniform(1000.0, 3000.0))
         lay = BlockLayout(C, gulp, dt, TSAMP, 1536.0 + foff / 2, foff)
-        plan = plan_for(lay, 0.0, float(rng.uniform(1000.0, 3000.0)), 1)
+        plan = plan_for(lay, 0.0, dm_max, 1)
         try:
-            admitted.append((srv.add_beam(rfi_config(), lay, 2.0, plan, bc), (C, dt)))
+            bid = srv.add_beam(rfi_config(), lay, 2.0, plan, bc)
         except FrostError as e:
             if e.code != -2:
                 raise
             refused += 1
+            continue
+        data = serving_gulp(b, C, dt == DataType.FLOAT32, dm_max)
+        buf = torch.empty(data.nbytes, dtype=torch.uint8, pin_memory=True)
+        buf.copy_(torch.from_numpy(np.ascontiguousarray(data).reshape(-1).view(np.uint8)))
+        admitted.append((bid, buf, (C, dt)))
+        del data
+    t_gen = time.perf_counter() - t_gen
     events = []
-    for bid, cls in admitted:
+    for bid, _, _ in admitted:
         off = float(rng.uniform(0.0, cadence))
         for g in range(S["gulps"]):
-            events.append((off + g * cadence + float(rng.exponential(S["jitter_s"])), bid, cls, g))
+            events.append((off + g * cadence + float(rng.exponential(S["jitter_s"])), bid, g))
     events.sort()
+    bufs = {bid: buf for bid, buf, _ in admitted}
     lat, lock = [], threading.Lock()
-    pending = []
+    pending, ncands = [], [0]
 
     def waiter(ticket, g):
-        _, l = srv.wait(ticket)
-        if g > 0:
-            with lock:
+        cands, l = srv.wait(ticket)
+        with lock:
+            ncands[0] += cands.size
+            if g > 0:
                 lat.append(l)
 
     sampler = ClockSampler(local)
     sampler.__enter__()
     t0 = time.perf_counter()
-    for at, bid, cls, g in events:
+    for at, bid, g in events:
         now = time.perf_counter() - t0
         if at > now:
             time.sleep(at - now)
-        buf = host[cls]
+        buf = bufs[bid]
         t = srv.submit_ptr(bid, buf.data_ptr(), buf.numel(), gulp, on_device=False)
         th = threading.Thread(target=waiter, args=(t, g))
         th.start()
@@ -669,22 +684,28 @@ def run_serving(args):
     lat.sort()
     q = lambda f: lat[min(len(lat) - 1, int(round(f * (len(lat) - 1))))] if lat else None
     beam_s = len(admitted) * S["gulps"] * cadence
+    mix = {}
+    for _, _, (C, dt) in admitted:
+        k = f"{C}ch_{'f32' if dt == DataType.FLOAT32 else 'u8'}"
+        mix[k] = mix.get(k, 0) + 1
     line = {
         "metric": "served beams at real-time cadence; p50/p99 gulp latency",
         "value": round(beam_s / wall, 3), "unit": UNIT, "n_gpus": 1, "steps": S["gulps"], "warmup": 1,
         "ms_per_step": round(wall * 1e3 / S["gulps"], 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (fp16 plane storage)",
-        "data": "synthetic (seeded noise gulps, one per channels x sample-type class, replayed)",
+        "data": ("synthetic: every admitted beam its own seeded gulp (noise, 5 % noisy channels, bursts, a "
+                 "dropout, 4 dispersed pulses), replayed at each of its arrivals"),
         "config": {"workload": "64 beams: 1024/4096 ch, uint8/float32, DM max U[1000,3000], 4 planes, "
                                "65536-sample gulps at 64 us cadence with exponential jitter "
                                f"(mean {S['jitter_s']} s)",
                    "beams_offered": S["beams"], "beams_admitted": len(admitted), "beams_refused": refused,
-                   "device_bytes_admitted": int(st.device_bytes), "slots": S["slots"],
-                   "tile_nsamps": S["tile"]},
+                   "admitted_mix": mix, "device_bytes_admitted": int(st.device_bytes), "slots": S["slots"],
+                   "tile_nsamps": S["tile"], "gulp_generation_s": round(t_gen, 1)},
         "latency_ms": {"p50": round(q(0.5) * 1e3, 1), "p99": round(q(0.99) * 1e3, 1),
                        "max": round(lat[-1] * 1e3, 1), "realtime_gulp_ms": round(cadence * 1e3, 1),
                        "gulps_timed": len(lat)},
         "p99_below_realtime": bool(lat and q(0.99) < cadence),
+        "candidates_per_gulp": round(ncands[0] / max(len(events), 1), 1),
         "clocks": sampler.summary(),
     }
     srv.close()

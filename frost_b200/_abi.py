@@ -79,6 +79,37 @@ class RfiConfigC(C.Structure):
     ]
 
 
+class SigprocHeaderC(C.Structure):
+    _fields_ = [
+        ("header_bytes", C.c_uint64),
+        ("nchans", C.c_uint64),
+        ("row_bytes", C.c_uint64),
+        ("data_rows", C.c_uint64),
+        ("nsamples", C.c_uint64),
+        ("nbits", C.c_int32),
+        ("nifs", C.c_int32),
+        ("data_type", C.c_int32),
+        ("telescope_id", C.c_int32),
+        ("machine_id", C.c_int32),
+        ("ibeam", C.c_int32),
+        ("nbeams", C.c_int32),
+        ("signed_samples", C.c_int32),
+        ("fch1", C.c_double),
+        ("foff", C.c_double),
+        ("tsamp", C.c_double),
+        ("tstart", C.c_double),
+        ("src_raj", C.c_double),
+        ("src_dej", C.c_double),
+        ("refdm", C.c_double),
+        ("source_name", C.c_char * 80),
+    ]
+
+    def as_dict(self) -> dict:
+        out = {k: getattr(self, k) for k, _ in self._fields_}
+        out["source_name"] = self.source_name.decode(errors="replace")
+        return out
+
+
 class BlockLayoutC(C.Structure):
     _fields_ = [
         ("nchans", C.c_uint64),

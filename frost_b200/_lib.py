@@ -104,6 +104,10 @@ SIGNATURES = {
     "frost_prefetch_create_file": (C.c_int, [C.c_char_p, _u64, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]),
     "frost_prefetch_create_memory": (C.c_int, [_vp, _sz, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]),
     "frost_prefetch_next": (C.c_int, [_vp, _vp, C.POINTER(_vp), C.POINTER(_sz)]),
+    "frost_sigproc_read_header": (C.c_int, [C.c_char_p, C.POINTER(_abi.SigprocHeaderC)]),
+    "frost_sigproc_layout": (C.c_int, [C.POINTER(_abi.SigprocHeaderC), _u64, C.POINTER(_abi.BlockLayoutC)]),
+    "frost_prefetch_create_sigproc": (C.c_int, [C.c_char_p, _sz, C.c_int, C.c_int,
+                                                C.POINTER(_abi.SigprocHeaderC), C.POINTER(_vp)]),
     "frost_prefetch_get_stats": (C.c_int, [_vp, C.POINTER(_abi.PrefetchStatsC)]),
     "frost_estimate_memory": (C.c_int, [C.POINTER(_abi.RfiConfigC), C.POINTER(_abi.BlockLayoutC), C.c_float,
                                         C.POINTER(_abi.DedispPlanConfigC), C.POINTER(_abi.BoxcarConfigC),

@@ -13,6 +13,7 @@
 #include "common.hpp"
 #include "dedisp.hpp"
 #include "rfi_decide.hpp"
+#include "sigproc.hpp"
 #include "cand_writer.hpp"
 #include "memory_plan.hpp"
 #include "postprocess.hpp"
@@ -972,6 +973,38 @@ int frost_prefetch_create_file(const char* path, uint64_t header_bytes, size_t b
         p->impl = std::make_unique<fb::staging::Prefetch>(block_rows, row_bytes, depth, device, read_file_rows,
                                                           p.get());
         *out = p.release();
+    });
+}
+
+int frost_sigproc_read_header(const char* path, frost_sigproc_header* out) {
+    return guarded([&] {
+        if (path == nullptr || out == nullptr)
+            invalid("frost_sigproc_read_header: null argument");
+        *out = fb::io::read_sigproc_header(path);
+    });
+}
+
+int frost_sigproc_layout(const frost_sigproc_header* header, uint64_t block_rows, frost_block_layout* out) {
+    return guarded([&] {
+        if (header == nullptr || out == nullptr)
+            invalid("frost_sigproc_layout: null argument");
+        *out = fb::io::sigproc_layout(*header, block_rows);
+    });
+}
+
+int frost_prefetch_create_sigproc(const char* path, size_t block_rows, int depth, int device,
+                                  frost_sigproc_header* header, frost_prefetch** out) {
+    return guarded([&] {
+        if (path == nullptr || out == nullptr)
+            invalid("frost_prefetch_create_sigproc: null argument");
+        *out                         = nullptr;
+        const frost_sigproc_header h = fb::io::read_sigproc_header(path);
+        (void)fb::io::sigproc_layout(h, block_rows); // a supported sample type
+        const int rc = frost_prefetch_create_file(path, h.header_bytes, block_rows, h.row_bytes, depth, device, out);
+        if (rc != FROST_OK)
+            throw fb::Error(rc, frost_last_error());
+        if (header != nullptr)
+            *header = h;
     });
 }
 

@@ -2,8 +2,12 @@
 (lib/pipeline/pipeline.cpp:105-262): a reader thread in the library fills
 pinned host slots from a block source and copies them to device slots, so
 the next gulp is read and transferred while the current one is searched.
+SIGPROC filterbanks (frost's file input, lib/pipeline/input.cpp:32-69) are
+opened by their header:
 
-    with GulpPrefetch.from_file(path, header_bytes, block_rows, row_bytes) as pf:
+    pf = GulpPrefetch.from_sigproc(path, block_rows)
+    layout = sigproc_layout(pf.header, block_rows)
+    with pf:
         for ptr, nread in pf:
             pipe.execute_device(ptr, nread, on_device=True)
 """
@@ -18,6 +22,27 @@ import numpy as np
 
 from . import _abi
 from ._lib import check, lib
+
+
+def read_sigproc_header(path: str) -> dict:
+    """The SIGPROC header of the filterbank at `path` (header_bytes, nchans,
+    nbits, row_bytes, data_rows, fch1, foff, tsamp, tstart, ...)."""
+    h = _abi.SigprocHeaderC()
+    check(lib().frost_sigproc_read_header(str(path).encode(), C.byref(h)))
+    return h.as_dict()
+
+
+def sigproc_layout(header: dict, block_rows: int):
+    """frost_b200.config.BlockLayout of a SIGPROC file's rows for gulps of
+    `block_rows` samples."""
+    from .config import BlockLayout, DataType
+    h = _abi.SigprocHeaderC()
+    for k, _ in h._fields_:
+        v = header[k]
+        setattr(h, k, v.encode() if k == "source_name" else v)
+    out = _abi.BlockLayoutC()
+    check(lib().frost_sigproc_layout(C.byref(h), int(block_rows), C.byref(out)))
+    return BlockLayout(out.nchans, out.max_nsamps, DataType(out.dtype), out.tsamp, out.f0, out.df)
 
 
 @dataclass
@@ -43,6 +68,18 @@ class GulpPrefetch:
         check(lib().frost_prefetch_create_file(path.encode(), int(header_bytes), int(block_rows), int(row_bytes),
                                                int(depth), int(device), C.byref(h)))
         return cls(h)
+
+    @classmethod
+    def from_sigproc(cls, path: str, block_rows: int, depth: int = 2, device: int = 0) -> "GulpPrefetch":
+        """The rows of a SIGPROC filterbank after its parsed header; the
+        header is `self.header`."""
+        h = C.c_void_p()
+        hdr = _abi.SigprocHeaderC()
+        check(lib().frost_prefetch_create_sigproc(str(path).encode(), int(block_rows), int(depth), int(device),
+                                                  C.byref(hdr), C.byref(h)))
+        pf = cls(h)
+        pf.header = hdr.as_dict()
+        return pf
 
     @classmethod
     def from_memory(cls, rows: np.ndarray, block_rows: int, depth: int = 2, device: int = 0) -> "GulpPrefetch":

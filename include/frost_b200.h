@@ -684,6 +684,55 @@ int frost_prefetch_create_file(const char* path,
                                int device,
                                frost_prefetch** out);
 
+/* The SIGPROC filterbank header (the sigproc file input of frost's
+ * open_input, lib/pipeline/input.cpp:32-69, read there through psrio):
+ * the fields the search needs, where the data start and how many whole
+ * rows follow. */
+typedef struct {
+    uint64_t header_bytes;   /* data start */
+    uint64_t nchans;
+    uint64_t row_bytes;      /* nchans * nbits / 8 */
+    uint64_t data_rows;      /* whole rows after the header */
+    uint64_t nsamples;       /* the header's nsamples keyword, 0 if absent */
+    int32_t nbits;
+    int32_t nifs;
+    int32_t data_type;
+    int32_t telescope_id;
+    int32_t machine_id;
+    int32_t ibeam;
+    int32_t nbeams;
+    int32_t signed_samples;  /* the `signed` keyword */
+    double fch1;             /* MHz, channel 0 */
+    double foff;             /* MHz */
+    double tsamp;            /* seconds */
+    double tstart;           /* MJD */
+    double src_raj;
+    double src_dej;
+    double refdm;
+    char source_name[80];
+} frost_sigproc_header;
+
+/* Reads the header of the SIGPROC filterbank at `path`. FROST_ERR_IO if it
+ * cannot be opened; FROST_ERR_INVALID_ARGUMENT if the header is malformed,
+ * names an unknown keyword, lacks nchans, nbits, tsamp, fch1 or foff, or
+ * has more than one IF. */
+int frost_sigproc_read_header(const char* path, frost_sigproc_header* out);
+
+/* The BlockLayout of a SIGPROC file's rows for gulps of `block_rows`
+ * samples: nbits 1/2/4/8/16 unsigned or 32 float, channel 0 at fch1,
+ * spacing foff. */
+int frost_sigproc_layout(const frost_sigproc_header* header, uint64_t block_rows, frost_block_layout* out);
+
+/* frost_prefetch_create_file over a SIGPROC filterbank: its header is
+ * parsed (written to `header` when not NULL) and the rows after it are
+ * staged in gulps of `block_rows`. */
+int frost_prefetch_create_sigproc(const char* path,
+                                  size_t block_rows,
+                                  int depth,
+                                  int device,
+                                  frost_sigproc_header* header,
+                                  frost_prefetch** out);
+
 /* The same over `total_rows` packed rows in caller host memory (kept valid
  * until destroy): the reader thread copies them into the pinned slots, as a
  * socket or ring-buffer reader would. */

@@ -404,6 +404,11 @@ public:
                  int device = 0) {
         check(frost_prefetch_create(block_rows, row_bytes, depth, device, read, ctx, &m_h));
     }
+    /** The rows of a SIGPROC filterbank after its header (header()). */
+    GulpPrefetch(const std::string& sigproc_path, size_t block_rows, int depth = 2, int device = 0) {
+        check(frost_prefetch_create_sigproc(sigproc_path.c_str(), block_rows, depth, device, &m_header, &m_h));
+    }
+    const frost_sigproc_header& header() const { return m_header; }
     GulpPrefetch(const GulpPrefetch&)            = delete;
     GulpPrefetch& operator=(const GulpPrefetch&) = delete;
     ~GulpPrefetch() {
@@ -427,7 +432,23 @@ public:
 
 private:
     frost_prefetch* m_h = nullptr;
+    frost_sigproc_header m_header{};
 };
+
+/** The header of a SIGPROC filterbank (frost's file input,
+ * lib/pipeline/input.cpp:32-69). */
+inline frost_sigproc_header read_sigproc_header(const std::string& path) {
+    frost_sigproc_header h{};
+    check(frost_sigproc_read_header(path.c_str(), &h));
+    return h;
+}
+
+/** BlockLayout of a SIGPROC file's rows for gulps of `block_rows`. */
+inline frost_block_layout sigproc_layout(const frost_sigproc_header& h, uint64_t block_rows) {
+    frost_block_layout l{};
+    check(frost_sigproc_layout(&h, block_rows, &l));
+    return l;
+}
 
 /** output::CandWriter (include/frost/output/cand_writer.hpp:38-55). */
 class CandWriter {

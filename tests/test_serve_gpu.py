@@ -193,6 +193,40 @@ def test_admission_by_device_memory():
     srv.close()
 
 
+def test_gulp_arriving_while_slots_are_busy_waits_for_a_slot_and_gives_its_solo_result():
+    """Continuous batching: with both worker slots busy on two beams' gulps,
+    a third beam's gulp that arrives meanwhile is queued, starts when a slot
+    frees (its latency includes the wait) and gives exactly the candidates
+    of that beam run alone; so do the first two."""
+    import time
+
+    from frost_b200.pipeline import GulpPipeline
+    from frost_b200.serve import BeamServer
+    rfi, layout, plan, bc = _setup()
+    streams = [_beam_stream(s) for s in (61, 62, 63)]
+    alone = []
+    for st in streams:
+        p = GulpPipeline(rfi, layout, 1.0, plan, bc)
+        p.search.autotune()
+        alone.append(p.execute(st[:GULP], GULP).candidates)
+    srv = BeamServer(slots=2)
+    ids = [srv.add_beam(rfi, layout, 1.0, plan, bc) for _ in streams]
+    t_busy = [srv.submit(ids[k], streams[k][:GULP], GULP) for k in range(2)]
+    time.sleep(0.002)  # the two gulps are on the device
+    t_late = srv.submit(ids[2], streams[2][:GULP], GULP)
+    lat = []
+    for k, t in enumerate(t_busy + [t_late]):
+        cands, l = srv.wait(t)
+        lat.append(l)
+        assert np.array_equal(cands, alone[k]), k
+    assert sum(len(a) for a in alone) > 0
+    # the late gulp waited for a slot: its latency exceeds the faster busy
+    # gulp's service time less the head start it was given
+    assert lat[2] > min(lat[0], lat[1]) - 0.002
+    assert srv.stats().completed == 3
+    srv.close()
+
+
 UNEVEN = [  # channels, dtype, gulp, DM max, sub-band depth (1 / 4 / 11 planes)
     (1024, "uint8", 32768, 500.0, 0),
     (2048, "float32", 32768, 800.0, 1),

@@ -91,6 +91,23 @@ def test_file_source_and_caller_stream(tmp_path):
         _same(_through(pf, layout, plan, bc, stream=s), ref)
 
 
+def test_sigproc_filterbank_source(tmp_path):
+    """A SIGPROC filterbank written as frost's fake filterbank writes one:
+    the prefetch parses its header, and the layout taken from the header
+    gives the pipeline the candidates of the same rows fed directly."""
+    from frost_b200.staging import GulpPrefetch, sigproc_layout
+    from tests.test_sigproc import write_filterbank
+    data, layout, plan, bc = _setup(3, 300)
+    ref = _direct(data, layout, plan, bc)
+    path = os.path.join(tmp_path, "beam.fil")
+    write_filterbank(path, nchans=NCHANS, nbits=8, fch1=1500.0, foff=-1.0, tsamp=TSAMP, data=data)
+    pf = GulpPrefetch.from_sigproc(path, GULP, depth=2)
+    assert pf.header["data_rows"] == data.shape[0] and pf.header["nchans"] == NCHANS
+    assert sigproc_layout(pf.header, GULP) == layout
+    with pf:
+        _same(_through(pf, layout, plan, bc), ref)
+
+
 def test_callback_source_and_its_failure():
     from frost_b200._lib import FrostError
     from frost_b200.staging import GulpPrefetch
