@@ -826,6 +826,140 @@ def run_postprocess(args):
     print(json.dumps(line), flush=True)
 
 
+BATCH = dict(beams=32, tile=32768)
+
+
+def batch_beams(n):
+    """The multi-beam workload's beams, seeded: channels 1024 / 2048 / 4096,
+    uint8 or float32, gulps of 2^15 - 2^18 samples, DM max 500 - 3000, 1, 4
+    or 11 sub-band planes."""
+    import numpy as np
+    rng = np.random.default_rng(0x46524F5354 ^ 3)
+    out = []
+    for b in range(n):
+        C = int(rng.choice([1024, 2048, 4096]))
+        out.append(dict(C=C, f32=bool(rng.integers(0, 2)), T=int(2 ** rng.integers(15, 19)),
+                        dm_max=float(round(rng.uniform(500.0, 3000.0), 1)), depth=int(rng.choice([0, 1, 2]))))
+    return out
+
+
+def batch_gulp(b, spec):
+    """A beam's seeded gulp of the 4096-channel recipe scaled to its shape:
+    pulses at DM 100 to dm_max - 100 (one per 2^15 samples), 5 % noisy
+    channels, bursts and a dropout."""
+    from frost_b200.synth import make_filterbank
+    C, T = spec["C"], spec["T"]
+    foff = -336.0 / C
+    return make_filterbank(C, T, 1536.0 + foff / 2, foff, TSAMP, beam_seed(0, 2000 + b),
+                           dtype="float32" if spec["f32"] else "uint8", n_pulses=max(1, T // 32768),
+                           dm_range=(100.0, spec["dm_max"] - 100.0), width_range=(1.0, 128.0),
+                           snr_range=(7.0, 50.0), rfi_channel_fraction=0.05, n_bursts=max(1, T // 16384),
+                           n_dropouts=1).data
+
+
+def run_config3(args):
+    """Batched multi-beam search: 32 seeded beams of uneven shapes (channels,
+    sample type, gulp length, DM range, plane count) searched together, one
+    gulp of every beam per step, their level steps and searches run as
+    single launches over all beams and replayed from a CUDA graph; beside it
+    the same beams served concurrently by the server (one stream and worker
+    per beam). Gulps resident on the device; beams admitted by memory."""
+    import numpy as np
+    import torch
+
+    from frost_b200._lib import FrostError
+    from frost_b200.batch import BeamBatch
+    from frost_b200.config import BlockLayout, DataType, Storage
+    from frost_b200.pipeline import plan_for
+    from frost_b200.serve import BeamServer
+
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    specs = batch_beams(BATCH["beams"])
+    bc = search_config(Storage.FP16)
+    bc.tile_nsamps = BATCH["tile"]
+
+    def layout_of(sp):
+        foff = -336.0 / sp["C"]
+        return BlockLayout(sp["C"], sp["T"], DataType.FLOAT32 if sp["f32"] else DataType.UINT8, TSAMP,
+                           1536.0 + foff / 2, foff)
+
+    def admit(add):
+        ids = []
+        for sp in specs:
+            lay = layout_of(sp)
+            try:
+                ids.append(add(rfi_config(), lay, 2.0, plan_for(lay, 0.0, sp["dm_max"], sp["depth"]), bc))
+            except FrostError as e:
+                if e.code != -2:
+                    raise
+                ids.append(None)
+        return ids
+
+    batch = BeamBatch(device=local)
+    ids = admit(batch.add_beam)
+    keep = [i for i, b in enumerate(ids) if b is not None]
+    dev = {}
+    t_gen = time.perf_counter()
+    for i in keep:
+        data = batch_gulp(i, specs[i])
+        dev[i] = torch.from_numpy(np.ascontiguousarray(data).reshape(-1).view(np.uint8)).to("cuda")
+        del data
+    t_gen = time.perf_counter() - t_gen
+    ptrs = [dev[i].data_ptr() for i in keep]
+    nread = [specs[i]["T"] for i in keep]
+    beam_s = sum(specs[i]["T"] for i in keep) * TSAMP
+
+    def timed(step):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(args.steps):
+            step()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / args.steps
+
+    ms_batch = timed(lambda: batch.execute_ptrs(ptrs, nread, on_device=True))
+    st = batch.stats()
+    batch.close()
+    torch.cuda.empty_cache()
+    srv = BeamServer(device=local, slots=len(keep))
+    sid = admit(srv.add_beam)
+    served = [i for i in keep if sid[i] is not None]
+
+    def serve_step():
+        tickets = [srv.submit_ptr(sid[i], dev[i].data_ptr(), dev[i].numel(), specs[i]["T"], True) for i in served]
+        for t in tickets:
+            srv.wait(t)
+    ms_served = timed(serve_step)
+    srv.close()
+    mix = {}
+    for i in keep:
+        sp = specs[i]
+        k = f"{sp['C']}ch_{'f32' if sp['f32'] else 'u8'}_{ {0: 1, 1: 4, 2: 11}[sp['depth']]}p"
+        mix[k] = mix.get(k, 0) + 1
+    line = {
+        "metric": "beam-s searched/s, batched uneven beams", "value": round(beam_s / (ms_batch / 1e3), 3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_batch, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp16 plane storage)",
+        "data": "synthetic: every beam its own seeded gulp (noise, RFI, pulses), resident on the device",
+        "config": {"workload": f"{BATCH['beams']} beams: 1024/2048/4096 ch, uint8/float32, gulps 2^15-2^18, "
+                               "DM max U[500,3000], 1/4/11 planes, boxcar 1-256; one gulp of every beam a step",
+                   "beams_offered": len(specs), "beams_admitted": len(keep), "mix": mix,
+                   "fdmt_tile_nsamps": BATCH["tile"], "gulp_generation_s": round(t_gen, 1)},
+        "batch_stats": st,
+        "served": {"value": round(sum(specs[i]["T"] for i in served) * TSAMP / (ms_served / 1e3), 3),
+                   "ms_per_step": round(ms_served, 3), "beams": len(served),
+                   "what": "the same beams through the server, one worker and stream per beam"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_rfi(args):
     """The RFI stage of the headline gulp alone (4096 channels, uint8, the
     config-2 RFI recipe and strategies: bandpass, moments, IQRM, Kadane in
@@ -875,11 +1009,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["frost", "reference"], default="frost")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "postprocess", "rfi"], default="config2",
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "postprocess", "rfi", "config3"],
+                    default="config2",
                     help="config2 (headline), config1 (1024-channel profiling case), serving "
                          "(64 beams at real-time cadence), postprocess (candidate clustering and "
-                         "dedup of the headline gulp's detections) or rfi (the RFI stage alone, a "
-                         "profiling case)")
+                         "dedup of the headline gulp's detections), rfi (the RFI stage alone, a "
+                         "profiling case) or config3 (32 uneven beams searched as one batch)")
     ap.add_argument("--beams", type=int, default=3, help="served beams per GPU (admitted by memory)")
     ap.add_argument("--staging", type=int, default=0,
                     help="e2e leg: staging blocks (and gulps in flight) per beam; 0 = one gulp in flight, "
@@ -889,6 +1024,9 @@ def main():
     ap.add_argument("--rfi-nsamps", type=int, default=131072,
                     help="samples of the headline gulp the rfi workload cleans per step")
     args = ap.parse_args()
+    if args.workload == "config3":
+        run_config3(args)
+        return
     if args.workload == "rfi":
         run_rfi(args)
         return

@@ -265,6 +265,19 @@ class ServerStatsC(C.Structure):
     ]
 
 
+class BatchStatsC(C.Structure):
+    _fields_ = [
+        ("executes", C.c_uint64),
+        ("beams", C.c_uint64),
+        ("rounds", C.c_uint64),
+        ("merged_level_launches", C.c_uint64),
+        ("merged_search_launches", C.c_uint64),
+        ("beam_launches", C.c_uint64),
+        ("graph_replays", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+    ]
+
+
 class GiantC(C.Structure):
     """frost_giant: search::Giant (include/frost/search/candidate.hpp:28-66)."""
 

@@ -56,6 +56,16 @@ SIGNATURES = {
     "frost_search_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "frost_search_set_wait_limit": (C.c_int, [_vp, C.c_int64]),
     "frost_search_restart": (C.c_int, [_vp]),
+    "frost_batch_create": (C.c_int, [C.c_int, _sz, C.POINTER(_vp)]),
+    "frost_batch_destroy": (C.c_int, [_vp]),
+    "frost_batch_add_beam": (C.c_int, [_vp, C.POINTER(_abi.RfiConfigC), C.POINTER(_abi.BlockLayoutC), C.c_float,
+                                       C.POINTER(_abi.DedispPlanConfigC), C.POINTER(_abi.BoxcarConfigC),
+                                       C.POINTER(C.c_uint32)]),
+    "frost_batch_execute": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_sz), C.c_int]),
+    "frost_batch_results": (C.c_int, [_vp, C.c_uint32, _vp, _sz, C.POINTER(_sz)]),
+    "frost_batch_drain": (C.c_int, [_vp, C.c_uint32, _vp, _sz, C.POINTER(_sz)]),
+    "frost_batch_use_graph": (C.c_int, [_vp, C.c_int]),
+    "frost_batch_get_stats": (C.c_int, [_vp, C.POINTER(_abi.BatchStatsC)]),
     "frost_rfi_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "frost_search_drain": (C.c_int, [_vp]),
     "frost_search_result_count": (C.c_int, [_vp, C.POINTER(_sz), C.POINTER(_u64), C.POINTER(_u64)]),

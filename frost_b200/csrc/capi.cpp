@@ -12,6 +12,7 @@
 
 #include "common.hpp"
 #include "dedisp.hpp"
+#include "batch.hpp"
 #include "rfi_decide.hpp"
 #include "sigproc.hpp"
 #include "cand_writer.hpp"
@@ -77,6 +78,11 @@ struct frost_search {
 struct frost_server {
     fb::serve::Server impl;
     template <class... A> explicit frost_server(A&&... a) : impl(std::forward<A>(a)...) {}
+};
+
+struct frost_batch {
+    fb::serve::Batch impl;
+    template <class... A> explicit frost_batch(A&&... a) : impl(std::forward<A>(a)...) {}
 };
 
 struct frost_cand_writer {
@@ -516,6 +522,84 @@ int frost_server_add_beam(frost_server* s, const frost_rfi_config* rfi,
         spec.plan            = *plan;
         spec.search          = *search;
         *beam                = s->impl.add_beam(spec);
+    });
+}
+
+int frost_batch_create(int device, size_t memory_budget, frost_batch** out) {
+    return guarded([&] {
+        if (out == nullptr)
+            invalid("frost_batch_create: null output");
+        *out = nullptr;
+        *out = new frost_batch(device, memory_budget);
+    });
+}
+
+int frost_batch_destroy(frost_batch* b) {
+    return guarded([&] { delete b; });
+}
+
+int frost_batch_add_beam(frost_batch* b, const frost_rfi_config* rfi, const frost_block_layout* layout,
+                         float baseline_length, const frost_dedisp_plan_config* plan,
+                         const frost_boxcar_config* search, uint32_t* beam) {
+    return guarded([&] {
+        if (b == nullptr || rfi == nullptr || layout == nullptr || plan == nullptr || search == nullptr ||
+            beam == nullptr)
+            invalid("frost_batch_add_beam: null argument");
+        fb::serve::BeamSpec spec;
+        spec.rfi = *rfi;
+        if (rfi->n_zap_chans)
+            spec.zap_chans.assign(rfi->zap_chans, rfi->zap_chans + rfi->n_zap_chans);
+        if (rfi->n_zap_freqs)
+            spec.zap_freqs.assign(rfi->zap_freqs, rfi->zap_freqs + rfi->n_zap_freqs);
+        spec.layout          = *layout;
+        spec.baseline_length = baseline_length;
+        spec.plan            = *plan;
+        spec.search          = *search;
+        *beam                = b->impl.add_beam(spec);
+    });
+}
+
+int frost_batch_execute(frost_batch* b, const uint8_t* const* blocks, const size_t* nread, int on_device) {
+    return guarded([&] {
+        if (b == nullptr)
+            invalid("frost_batch_execute: null handle");
+        b->impl.execute(blocks, nread, on_device != 0);
+    });
+}
+
+int frost_batch_results(const frost_batch* b, uint32_t beam, frost_candidate* out, size_t capacity, size_t* count) {
+    int rc      = FROST_OK;
+    const int g = guarded([&] {
+        if (b == nullptr)
+            invalid("frost_batch_results: null handle");
+        rc = copy_candidates(b->impl.results(beam), out, capacity, count);
+    });
+    return g != FROST_OK ? g : rc;
+}
+
+int frost_batch_drain(frost_batch* b, uint32_t beam, frost_candidate* out, size_t capacity, size_t* count) {
+    int rc      = FROST_OK;
+    const int g = guarded([&] {
+        if (b == nullptr)
+            invalid("frost_batch_drain: null handle");
+        rc = copy_candidates(b->impl.drain(beam), out, capacity, count);
+    });
+    return g != FROST_OK ? g : rc;
+}
+
+int frost_batch_use_graph(frost_batch* b, int enable) {
+    return guarded([&] {
+        if (b == nullptr)
+            invalid("frost_batch_use_graph: null handle");
+        b->impl.use_graph(enable != 0);
+    });
+}
+
+int frost_batch_get_stats(const frost_batch* b, frost_batch_stats* out) {
+    return guarded([&] {
+        if (b == nullptr || out == nullptr)
+            invalid("frost_batch_get_stats: null argument");
+        *out = b->impl.stats();
     });
 }
 

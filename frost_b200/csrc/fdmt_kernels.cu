@@ -217,11 +217,9 @@ __device__ __forceinline__ void merge8(const S* lo, const S* stage, int e, int o
 constexpr int kStages      = 4;
 using bulk::mbar_wait;
 
-template <class S>
+template <class S, int K>
 __global__ void __launch_bounds__(kThreads)
-    k_level_pipe(const RowOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
-                 int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                 int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err, long long wait_limit) {
+    k_level_pipe(const __grid_constant__ LevelSegTable<K> tab, long long wait_limit) {
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -236,20 +234,34 @@ __global__ void __launch_bounds__(kThreads)
             bulk::mbar_init(&bar[s]);
     }
     __syncthreads();
-    // Work items (row, run of tpc tiles), rows fastest; a CTA takes items
-    // blockIdx.x, blockIdx.x + gridDim.x, ... and its tiles use the stages
-    // in turn across items (the CTA's tile n: stage n % kStages, barrier
-    // phase (n / kStages) % 2, kept as running counters).
-    const int nruns      = (ntiles + tpc - 1) / tpc;
-    const int64_t nitems = nrows * nruns;
+    // Work items (segment, row, run of tpc tiles), rows fastest within a
+    // segment; a CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ... and
+    // its tiles use the stages in turn across items and segments (the CTA's
+    // tile n: stage n % kStages, barrier phase (n / kStages) % 2, kept as
+    // running counters).
+    const int64_t nitems = tab.s[tab.n - 1].item_end;
     const int e          = 8 * threadIdx.x;
     int cs      = 0;  // stage of the CTA's next tile
     uint32_t cp = 0U; // and its barrier's phase parity
+    int sg       = 0;  // the segment of the CTA's current item
+    int64_t sbeg = 0;  // and its first item
     for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
-        const int64_t r = item % nrows;
-        const RowOp op  = ops[r];
-        const int tile0 = static_cast<int>(item / nrows) * tpc;
-        const int nt    = min(tpc, ntiles - tile0);
+        while (item >= tab.s[sg].item_end) {
+            sbeg = tab.s[sg].item_end;
+            ++sg;
+        }
+        const LevelSeg& G      = tab.s[sg];
+        const RowOp* ops       = static_cast<const RowOp*>(G.ops);
+        const S* in            = static_cast<const S*>(G.in);
+        S* out                 = static_cast<S*>(G.out);
+        const int64_t in_pitch = G.in_pitch, out_pitch = G.out_pitch;
+        const int32_t in_base = G.in_base, out_base = G.out_base;
+        unsigned* err          = G.err;
+        const int64_t local    = item - sbeg;
+        const int64_t r        = local % G.nrows;
+        const RowOp op         = ops[r];
+        const int tile0        = static_cast<int>(local / G.nrows) * G.tpc;
+        const int nt           = min(G.tpc, G.ntiles - tile0);
         const bool has_hi = op.hi_row >= 0;
         const S* lo_row   = in + static_cast<int64_t>(op.lo_row) * in_pitch + in_base;
         const S* hi_base  = in + static_cast<int64_t>(has_hi ? op.hi_row : op.lo_row) * in_pitch;
@@ -411,11 +423,9 @@ __device__ __forceinline__ void add8(const S* stage, int e, int off, float (&acc
 
 template <class S> constexpr int kStages2 = sizeof(S) == 2 ? 4 : 3;
 
-template <class S, int NS>
+template <class S, int NS, int K>
 __global__ void __launch_bounds__(kThreads)
-    k_level2_pipe(const FusedOp* __restrict__ ops, const S* __restrict__ in, int64_t in_pitch,
-                  int32_t in_base, S* __restrict__ out, int64_t out_pitch, int32_t out_base,
-                  int32_t ntiles, int32_t tpc, int64_t nrows, unsigned* __restrict__ err, long long wait_limit) {
+    k_level2_pipe(const __grid_constant__ LevelSegTable<K> tab, long long wait_limit) {
     constexpr int VEC       = 16 / static_cast<int>(sizeof(S));
     constexpr int kLoBytes  = kTimePerCta * static_cast<int>(sizeof(S));
     constexpr int kHiBytes  = kLoBytes + 16;
@@ -430,17 +440,30 @@ __global__ void __launch_bounds__(kThreads)
             bulk::mbar_init(&bar[st]);
     }
     __syncthreads();
-    // Work items (row, run of tpc tiles) as in k_level_pipe.
-    const int nruns      = (ntiles + tpc - 1) / tpc;
-    const int64_t nitems = nrows * nruns;
+    // Work items (segment, row, run of tpc tiles) as in k_level_pipe.
+    const int64_t nitems = tab.s[tab.n - 1].item_end;
     const int e          = 8 * threadIdx.x;
     int cs      = 0;  // stage of the CTA's next tile
     uint32_t cp = 0U; // and its barrier's phase parity
+    int sg       = 0;
+    int64_t sbeg = 0;
     for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
-        const int64_t r  = item % nrows;
-        const FusedOp op = ops[r];
-        const int tile0  = static_cast<int>(item / nrows) * tpc;
-        const int nt     = min(tpc, ntiles - tile0);
+        while (item >= tab.s[sg].item_end) {
+            sbeg = tab.s[sg].item_end;
+            ++sg;
+        }
+        const LevelSeg& G      = tab.s[sg];
+        const FusedOp* ops     = static_cast<const FusedOp*>(G.ops);
+        const S* in            = static_cast<const S*>(G.in);
+        S* out                 = static_cast<S*>(G.out);
+        const int64_t in_pitch = G.in_pitch, out_pitch = G.out_pitch;
+        const int32_t in_base = G.in_base, out_base = G.out_base;
+        unsigned* err          = G.err;
+        const int64_t local    = item - sbeg;
+        const int64_t r        = local % G.nrows;
+        const FusedOp op       = ops[r];
+        const int tile0        = static_cast<int>(local / G.nrows) * G.tpc;
+        const int nt           = min(G.tpc, G.ntiles - tile0);
         const S* rows[4];
         int off[4];
         uint32_t bytes[4];
@@ -708,47 +731,87 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
         FB_LAUNCH_CHECK();
         return;
     }
-    const dim3 grid(grid_for(nrows * ((ntiles + tpc - 1) / tpc), ctas));
-    const size_t es   = out.fp16 ? 2 : 4;
-    const size_t smem = kStages * (2 * kTimePerCta * es + 16);
-    if (out.fp16) {
-        FB_CUDA(cudaFuncSetAttribute(k_level_pipe<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-        k_level_pipe<__half><<<grid, kThreads, smem, s>>>(
-            ops, static_cast<const __half*>(in.data), in.pitch, in.base,
-            static_cast<__half*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err, wait_limit);
-    } else {
-        FB_CUDA(cudaFuncSetAttribute(k_level_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-        k_level_pipe<float><<<grid, kThreads, smem, s>>>(
-            ops, static_cast<const float*>(in.data), in.pitch, in.base,
-            static_cast<float*>(out.data), out.pitch, out.base, ntiles, tpc, nrows, err, wait_limit);
-    }
-    FB_LAUNCH_CHECK();
+    LevelSeg g{ops, in.data, out.data, in.pitch, out.pitch, in.base, out.base, ntiles, tpc, nrows, 0, err};
+    launch_level_segs(&g, 1, false, out.fp16 != 0, 0, s, ctas, wait_limit);
 }
 
 namespace {
-template <class S, int NS>
-void level2_stages(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
-                   int64_t nrows, unsigned* err, long long wait_limit, cudaStream_t s) {
-    const size_t smem = NS * (4 * kTimePerCta * sizeof(S) + 48);
-    FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<S, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
-    k_level2_pipe<S, NS><<<grid, kThreads, smem, s>>>(ops, static_cast<const S*>(in.data), in.pitch, in.base,
-                                                      static_cast<S*>(out.data), out.pitch, out.base, ntiles,
-                                                      tpc, nrows, err, wait_limit);
+
+template <int K>
+LevelSegTable<K> seg_table(LevelSeg* segs, int n, int64_t* total) {
+    LevelSegTable<K> t{};
+    t.n       = n;
+    int64_t e = 0;
+    for (int i = 0; i < n; ++i) {
+        LevelSeg& g = segs[i];
+        if (g.tpc < 1 || g.tpc > 128 || g.ntiles < 1 || g.nrows < 1 || g.err == nullptr ||
+            g.in_base % 8 != 0 || g.in_pitch % 8 != 0 || g.out_base % 8 != 0 || g.out_pitch % 8 != 0)
+            throw Error(FROST_ERR_INTERNAL, "level: bad segment geometry");
+        e += g.nrows * ((g.ntiles + g.tpc - 1) / g.tpc);
+        g.item_end = e;
+        t.s[i]     = g;
+    }
+    *total = e;
+    return t;
 }
-template <class S>
-void level2_typed(const FusedOp* ops, dim3 grid, LevelView in, LevelView out, int32_t ntiles, int32_t tpc,
-                  int64_t nrows, int32_t stages, unsigned* err, long long wait_limit, cudaStream_t s) {
+
+template <class S, int NS, int K>
+void level2_go(const LevelSegTable<K>& t, int64_t total, cudaStream_t s, int32_t ctas, long long wait_limit) {
+    const size_t smem = NS * (4 * kTimePerCta * sizeof(S) + 48);
+    FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<S, NS, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    k_level2_pipe<S, NS, K><<<grid_for(total, ctas), kThreads, smem, s>>>(t, wait_limit);
+}
+
+template <class S, int K>
+void level_go(const LevelSegTable<K>& t, int64_t total, bool fused, int32_t stages, cudaStream_t s, int32_t ctas,
+              long long wait_limit) {
+    if (!fused) {
+        const size_t smem = kStages * (2 * kTimePerCta * sizeof(S) + 16);
+        FB_CUDA(cudaFuncSetAttribute(k_level_pipe<S, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        k_level_pipe<S, K><<<grid_for(total, ctas), kThreads, smem, s>>>(t, wait_limit);
+        return;
+    }
     switch (stages == 0 ? kStages2<S> : stages) {
-    case 2: level2_stages<S, 2>(ops, grid, in, out, ntiles, tpc, nrows, err, wait_limit, s); break;
-    case 3: level2_stages<S, 3>(ops, grid, in, out, ntiles, tpc, nrows, err, wait_limit, s); break;
-    case 4: level2_stages<S, 4>(ops, grid, in, out, ntiles, tpc, nrows, err, wait_limit, s); break;
+    case 2: level2_go<S, 2, K>(t, total, s, ctas, wait_limit); break;
+    case 3: level2_go<S, 3, K>(t, total, s, ctas, wait_limit); break;
+    case 4:
+        if constexpr (sizeof(S) == 2)
+            level2_go<S, 4, K>(t, total, s, ctas, wait_limit);
+        else
+            throw Error(FROST_ERR_INTERNAL, "level2: 4 float stages exceed the shared memory of a CTA");
+        break;
     default: throw Error(FROST_ERR_INTERNAL, "level2: stages must be 2, 3 or 4");
     }
 }
+
+template <int K>
+void launch_table(LevelSeg* segs, int n, bool fused, bool fp16, int32_t stages, cudaStream_t s, int32_t ctas,
+                  long long wait_limit) {
+    int64_t total = 0;
+    const LevelSegTable<K> t = seg_table<K>(segs, n, &total);
+    if (fp16)
+        level_go<__half, K>(t, total, fused, stages, s, ctas, wait_limit);
+    else
+        level_go<float, K>(t, total, fused, stages, s, ctas, wait_limit);
+    FB_LAUNCH_CHECK();
+}
+
 } // namespace
+
+void launch_level_segs(LevelSeg* segs, int n, bool fused, bool fp16, int32_t stages, cudaStream_t s, int32_t ctas,
+                       long long wait_limit) {
+    if (wait_limit < 0)
+        throw Error(FROST_ERR_INTERNAL, "level: wait limit must be >= 0");
+    if (n == 1) {
+        launch_table<1>(segs, 1, fused, fp16, stages, s, ctas, wait_limit);
+        return;
+    }
+    for (int i = 0; i < n; i += kMaxLevelSegs)
+        launch_table<kMaxLevelSegs>(segs + i, std::min(kMaxLevelSegs, n - i), fused, fp16, stages, s, ctas,
+                                    wait_limit);
+}
 
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
                    unsigned* err, cudaStream_t s, int32_t tpc, int32_t stages, int32_t ctas,
@@ -763,14 +826,8 @@ void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView ou
     if (stages == 4 && !out.fp16)
         throw Error(FROST_ERR_INTERNAL, "level2: 4 float stages exceed the shared memory of a CTA");
     const int ntiles = ncols / kTimePerCta;
-    const dim3 grid(grid_for(nrows * ((ntiles + tpc - 1) / tpc), ctas));
-    if (wait_limit < 0)
-        throw Error(FROST_ERR_INTERNAL, "level2: wait limit must be >= 0");
-    if (out.fp16)
-        level2_typed<__half>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, wait_limit, s);
-    else
-        level2_typed<float>(ops, grid, in, out, ntiles, tpc, nrows, stages, err, wait_limit, s);
-    FB_LAUNCH_CHECK();
+    LevelSeg g{ops, in.data, out.data, in.pitch, out.pitch, in.base, out.base, ntiles, tpc, nrows, 0, err};
+    launch_level_segs(&g, 1, true, out.fp16 != 0, stages, s, ctas, wait_limit);
 }
 
 namespace {

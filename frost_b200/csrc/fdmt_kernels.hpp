@@ -20,6 +20,32 @@ struct LevelView {
 };
 
 constexpr int kTimePerCta = 2048; // samples per CTA in the level kernels
+
+/** One level step of one engine as a segment of a pipelined level launch:
+ * output rows [0, nrows) of `out` from `in` by its ops (RowOp for single
+ * levels, FusedOp for fused steps), each row cut into runs of `tpc` of
+ * `ntiles` time tiles. A launch covers several segments (the same step of
+ * several beams) in one grid; item_end is filled by the launcher. */
+struct LevelSeg {
+    const void* ops;
+    const void* in;
+    void* out;
+    int64_t in_pitch;
+    int64_t out_pitch;
+    int32_t in_base;
+    int32_t out_base;
+    int32_t ntiles;
+    int32_t tpc;
+    int64_t nrows;
+    int64_t item_end;
+    unsigned* err;
+};
+constexpr int kMaxLevelSegs = 48;
+template <int K> struct LevelSegTable {
+    int32_t n;
+    int32_t pad;
+    LevelSeg s[K];
+};
 /** Tries a pipelined kernel's first wait on a bulk copy makes before it
  * gives up (bulk::kSpinLimit); a drain after a give-up always uses it. */
 constexpr long long kDefaultWaitLimit = 1LL << 22;
@@ -60,6 +86,12 @@ struct FusedOp {
 void launch_level2(const FusedOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
                    unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t stages = 0,
                    int32_t ctas = 0, long long wait_limit = kDefaultWaitLimit);
+
+/** One pipelined launch over `n` level segments of the same kind (fused
+ * or single), element type and stage count; more than kMaxLevelSegs
+ * segments take several launches. `ctas` caps each launch's CTAs. */
+void launch_level_segs(LevelSeg* segs, int n, bool fused, bool fp16, int32_t stages, cudaStream_t s,
+                       int32_t ctas = 0, long long wait_limit = kDefaultWaitLimit);
 
 /** dst[r][0 .. width) = src[r][0 .. width) for `rows` rows of pitches
  * dpitch / spitch bytes (device memory): 16-byte vectors when pointers,

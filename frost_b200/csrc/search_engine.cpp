@@ -489,6 +489,146 @@ void Engine::set_wait_limit(long long tries) {
     m_wait_limit = tries < 0 ? kDefaultWaitLimit : tries;
 }
 
+// ---- batch members ----------------------------------------------------------
+
+void Engine::batch_begin(const float* waterfall, SizeType nsamps, const uint8_t* mask, cudaStream_t caller) {
+    if (waterfall == nullptr)
+        invalid("search: null waterfall");
+    if (nsamps == 0 || nsamps > m_plan.config().block_nsamps)
+        invalid("search: nsamps must be in [1, block_nsamps]");
+    if (m_capture_on || m_timing_on)
+        fail_state("search: plane capture and timing are off in a batch");
+    DeviceGuard g(m_device);
+    cudaStream_t s  = m_stream;
+    m_launches      = 0;
+    const int32_t C = m_plan.nchans();
+    std::vector<uint8_t> cur = m_mask;
+    if (mask != nullptr)
+        for (int32_t c = 0; c < C; ++c)
+            cur[c] = mask[c] != 0 ? 1 : 0;
+    const bool or_active = cur != m_mask;
+    std::vector<uint8_t> orm(C);
+    for (int32_t c = 0; c < C; ++c)
+        orm[c] = (cur[c] | m_mask[c]) ? 1 : 0;
+    if (caller != nullptr && caller != s) {
+        FB_CUDA(cudaEventRecord(m_order, caller));
+        FB_CUDA(cudaStreamWaitEvent(s, m_order, 0));
+    }
+    update_variance(cur, orm);
+    auto* ck      = m_clock_h.as<GulpClock>();
+    ck->gulp_t0   = static_cast<int64_t>(m_samples);
+    ck->or_active = or_active ? 1 : 0;
+    ck->pad       = 0;
+    FB_CUDA(cudaMemcpyAsync(m_clock.get(), ck, sizeof(GulpClock), cudaMemcpyHostToDevice, s));
+    FB_CUDA(cudaMemsetAsync(m_counters.get(), 0, 4 * sizeof(unsigned long long), s));
+    FB_CUDA(cudaMemsetAsync(m_row_counts.get(), 0, m_nsearch * sizeof(uint32_t), s));
+    m_batch_wf     = waterfall;
+    m_batch_nsamps = nsamps;
+    m_batch_mask   = std::move(cur);
+}
+
+int64_t Engine::batch_rounds() const {
+    const int64_t tiles = (static_cast<int64_t>(m_batch_nsamps) + m_tile - 1) / m_tile;
+    return tiles * static_cast<int64_t>(m_steps.size());
+}
+
+int Engine::batch_pre(int64_t round, cudaStream_t s, RoundWork& w) {
+    const int64_t nsteps  = static_cast<int64_t>(m_steps.size());
+    const int64_t t_off   = (round / nsteps) * m_tile;
+    const size_t si       = static_cast<size_t>(round % nsteps);
+    const int32_t n_valid = static_cast<int32_t>(std::min<int64_t>(m_tile, static_cast<int64_t>(m_batch_nsamps) - t_off));
+    const Step& st        = m_steps[si];
+    const LevelView out   = view(st.out);
+    unsigned* err         = reinterpret_cast<unsigned*>(m_counters.as<unsigned long long>() + 3);
+    w                     = RoundWork{};
+    if (si == 0) {
+        const int32_t C = m_plan.nchans();
+        launch_level1(m_leaf_ops.as<LeafOp>(), m_node_first_op_d.as<int32_t>(),
+                      static_cast<int32_t>(m_node_first_op.size() - 1), m_plan.level_history(0), m_batch_wf,
+                      static_cast<int64_t>(m_batch_nsamps), t_off, n_valid, m_in_hist.as<float>(),
+                      m_plan.level_history(0), out, static_cast<int32_t>(m_ncols), s, 0);
+        launch_save_input_history(m_batch_wf, static_cast<int64_t>(m_batch_nsamps), t_off, n_valid, C,
+                                  m_in_hist.as<float>(), m_in_scratch.as<float>(), m_plan.level_history(0), s);
+        m_launches += 1;
+        return 2;
+    }
+    const LevelView in = view(st.in);
+    w.has_level        = true;
+    w.fused            = st.fused;
+    w.fp16             = m_fp16;
+    w.stages           = m_level2_stages;
+    w.level            = LevelSeg{st.fused ? static_cast<const void*>(m_fused_ops.as<FusedOp>() + st.op_offset)
+                                           : static_cast<const void*>(m_row_ops.as<RowOp>() + st.op_offset),
+                                  in.data,
+                                  out.data,
+                                  in.pitch,
+                                  out.pitch,
+                                  in.base,
+                                  out.base,
+                                  static_cast<int32_t>(m_ncols / kTimePerCta),
+                                  m_level_tpc,
+                                  static_cast<int64_t>(m_plan.level_rows(st.out)),
+                                  0,
+                                  err};
+    m_launches += 1;
+    return 0;
+}
+
+int Engine::batch_mid(int64_t round, cudaStream_t s, RoundWork& w) {
+    const int64_t nsteps  = static_cast<int64_t>(m_steps.size());
+    const int64_t t_off   = (round / nsteps) * m_tile;
+    const Step& st        = m_steps[static_cast<size_t>(round % nsteps)];
+    const int h           = st.out;
+    const int32_t n_valid = static_cast<int32_t>(std::min<int64_t>(m_tile, static_cast<int64_t>(m_batch_nsamps) - t_off));
+    const LevelView out   = view(h);
+    launch_load_history(out, m_plan.level_rows(h), m_hist_len[h], m_hist[h].get(), s);
+    if (m_height_g1[h] > m_height_g0[h]) {
+        w.has_search   = true;
+        w.chunk        = m_search_chunk;
+        w.search       = SearchSeg{};
+        w.search.p     = params(t_off, n_valid);
+        w.search.level = out.data;
+        w.search.pitch = out.pitch;
+        w.search.base  = out.base;
+        w.search.fp16  = out.fp16;
+        w.search.g0    = m_height_g0[h];
+        w.search.nrows = m_height_g1[h] - m_height_g0[h];
+        m_launches += 1;
+    }
+    return 1;
+}
+
+int Engine::batch_post(int64_t round, cudaStream_t s) {
+    const int64_t nsteps  = static_cast<int64_t>(m_steps.size());
+    const int64_t t_off   = (round / nsteps) * m_tile;
+    const size_t si       = static_cast<size_t>(round % nsteps);
+    const int32_t n_valid = static_cast<int32_t>(std::min<int64_t>(m_tile, static_cast<int64_t>(m_batch_nsamps) - t_off));
+    const Step& st        = m_steps[si];
+    int n                 = 0;
+    if (si > 0) {
+        launch_save_history(view(st.in), m_plan.level_rows(st.in), m_hist_len[st.in], n_valid,
+                            m_hist[st.in].get(), s);
+        ++n;
+    }
+    if (static_cast<int64_t>(si) == nsteps - 1) {
+        const int L = m_plan.levels();
+        launch_save_history(view(L), m_plan.level_rows(L), m_hist_len[L], n_valid, m_hist[L].get(), s);
+        ++n;
+    }
+    return n;
+}
+
+void Engine::batch_finish() {
+    DeviceGuard g(m_device);
+    m_samples += m_batch_nsamps;
+    m_mask = m_batch_mask;
+    collect(m_stream);
+    m_timing.total_launches += m_launches;
+    m_timing.executes += 1;
+    m_batch_wf     = nullptr;
+    m_batch_nsamps = 0;
+}
+
 void Engine::restart() {
     DeviceGuard g(m_device);
     FB_CUDA(cudaStreamSynchronize(m_stream));

@@ -51,6 +51,35 @@ public:
      * (negative: the default; 0: give up at once); a drain after a give-up
      * always uses the default. */
     void set_wait_limit(long long tries);
+
+    /** The engine as one member of a multi-beam batch (serve::Batch): the
+     * gulp is taken on the engine's own stream (batch_begin: mask, noise
+     * tables, gulp clock, counters; ordered after `caller`), then run as
+     * batch_rounds() rounds, one (tile, level step) each, whose level and
+     * search launches the batch merges with the other members' into single
+     * launches on its stream: batch_pre enqueues the round's own launches
+     * that come before the level step (the leaf level) and describes its
+     * level segment, batch_mid loads the level's history and describes its
+     * search segment, batch_post saves the histories. batch_finish collects
+     * the results once the engine's stream waits for the batch's. Device
+     * waterfalls only; no plane capture or per-phase timing. */
+    struct RoundWork {
+        bool has_level  = false;
+        bool fused      = false;
+        bool fp16       = false;
+        int32_t stages  = 0;
+        LevelSeg level{};
+        bool has_search = false;
+        int32_t chunk   = 0;
+        SearchSeg search{};
+    };
+    void batch_begin(const float* waterfall, SizeType nsamps, const uint8_t* mask, cudaStream_t caller);
+    int64_t batch_rounds() const;
+    /** Each returns the launches it enqueued itself (segments not counted). */
+    int batch_pre(int64_t round, cudaStream_t s, RoundWork& w);
+    int batch_mid(int64_t round, cudaStream_t s, RoundWork& w);
+    int batch_post(int64_t round, cudaStream_t s);
+    void batch_finish();
     /** Starts the stream afresh: histories and run states cleared, sample
      * count zero, the constructor's mask current (after a failed gulp). */
     void restart();
@@ -76,6 +105,10 @@ private:
     cudaStream_t m_stream = nullptr;
     cudaEvent_t m_order   = nullptr; // orders the caller's stream before the engine's
     long long m_wait_limit = kDefaultWaitLimit;
+    // the batch gulp in progress
+    const float* m_batch_wf = nullptr;
+    SizeType m_batch_nsamps = 0;
+    std::vector<uint8_t> m_batch_mask;
     std::vector<uint8_t> m_kill; // the constructor's mask
     bool m_fp16;
     int64_t m_tile = 0, m_ncols = 0;

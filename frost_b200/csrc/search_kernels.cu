@@ -464,10 +464,12 @@ __device__ void scan_halo(const S* seg, int halo, int jmin, float* Q, float* gmi
         H[i] -= last;
 }
 
-template <class S, int CH, bool POW2>
+template <class S, int CH, bool POW2, int K>
 __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
-    k_search(SearchParams p, const S* __restrict__ level, int64_t pitch, int32_t base, int64_t g0,
-             int64_t nrows) {
+    k_search(const __grid_constant__ SearchSegTable<K> tab) {
+    // The search shape (widths, halo, peak mode, valid columns) is the same
+    // in every segment; the rows, tables and outputs are each segment's.
+    const SearchParams& p = tab.s[0].p;
     constexpr int P  = CH / kThreads; // chunk columns per thread
     constexpr int NG = P / 4;         // 4-column groups per thread
     // Dynamic shared memory (floats unless noted):
@@ -523,8 +525,20 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     // Rows blockIdx.x, blockIdx.x + gridDim.x, ...; the staging buffers and
     // barriers alternate over the CTA's chunks across rows.
     int64_t cc = 0; // chunks this CTA has consumed
-    for (int64_t gi = blockIdx.x; gi < nrows; gi += gridDim.x) {
-        const int64_t g = g0 + gi;
+    const int64_t nrows_all = tab.s[tab.n - 1].row_end;
+    int sg       = 0; // the segment of the CTA's current row
+    int64_t sbeg = 0; // and its first row
+    for (int64_t gi = blockIdx.x; gi < nrows_all; gi += gridDim.x) {
+        while (gi >= tab.s[sg].row_end) {
+            sbeg = tab.s[sg].row_end;
+            ++sg;
+        }
+        const SearchSeg& SG   = tab.s[sg];
+        const SearchParams& p = SG.p;
+        const S* level        = static_cast<const S*>(SG.level);
+        const int64_t pitch   = SG.pitch;
+        const int32_t base    = SG.base;
+        const int64_t g       = SG.g0 + (gi - sbeg);
         const SearchRow row = p.rows[g];
         if (threadIdx.x == 0) {
             local_count  = p.row_counts[g];
@@ -938,51 +952,105 @@ __global__ void k_variance(const SearchRow* __restrict__ rows, const PlaneInfo* 
 
 } // namespace
 
-void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1, cudaStream_t s,
-                   int32_t chunk, int32_t ctas) {
-    if (g1 <= g0 || p.n_valid <= 0)
-        return;
-    if (chunk != 2048 && chunk != 4096)
-        throw Error(FROST_ERR_INTERNAL, "search: chunk must be 2048 or 4096 samples");
+namespace {
+
+void check_search(const SearchParams& p, int64_t pitch, int32_t base, int32_t chunk) {
     if (p.nwidths > kMaxWidths)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "search: more than 32 boxcar widths");
-    if (p.halo != search_halo(p.wmax) || level.base < p.halo)
+    if (p.halo != search_halo(p.wmax) || base < p.halo)
         throw Error(FROST_ERR_INTERNAL, "search: level history shorter than the search halo");
-    if (level.pitch - level.base < ((p.n_valid + chunk - 1) / chunk) * chunk)
+    if (pitch - base < ((p.n_valid + chunk - 1) / chunk) * chunk)
         throw Error(FROST_ERR_INTERNAL, "search: tile columns are not a whole number of chunks");
     if (p.err == nullptr)
         throw Error(FROST_ERR_INTERNAL, "search: no error flag");
     if (p.wait_limit < 0)
         throw Error(FROST_ERR_INTERNAL, "search: wait limit must be >= 0");
-    const size_t es   = level.fp16 ? 2 : 4;
-    const size_t seg  = static_cast<size_t>(p.halo) + chunk;
+}
+
+bool same_shape(const SearchParams& a, const SearchParams& b) {
+    return a.nwidths == b.nwidths && a.wmax == b.wmax && a.halo == b.halo && a.peak_mode == b.peak_mode &&
+           a.trapezoid == b.trapezoid && a.skip_cold == b.skip_cold && a.pow2_widths == b.pow2_widths &&
+           a.n_valid == b.n_valid;
+}
+
+template <int K>
+void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t ctas) {
+    SearchSegTable<K> t{};
+    t.n            = n;
+    int64_t rows   = 0;
+    const auto& p0 = segs[0].p;
+    for (int i = 0; i < n; ++i) {
+        SearchSeg& g = segs[i];
+        check_search(g.p, g.pitch, g.base, chunk);
+        if (!same_shape(g.p, p0) || g.fp16 != segs[0].fp16)
+            throw Error(FROST_ERR_INTERNAL, "search: segments of one launch differ in shape");
+        rows += g.nrows;
+        g.row_end = rows;
+        t.s[i]    = g;
+    }
+    const size_t es   = segs[0].fp16 ? 2 : 4;
+    const size_t seg  = static_cast<size_t>(p0.halo) + chunk;
     // Ps, gmin (+4 padding), tmin, the next chunk's halo by parity, the bit
     // masks and the staging buffers (the kernel's layout)
     const size_t per  = static_cast<size_t>(chunk) / kThreads; // columns per thread
-    const size_t nh   = static_cast<size_t>(p.halo) + p.halo / 4 + p.halo / per + 4;
+    const size_t nh   = static_cast<size_t>(p0.halo) + p0.halo / 4 + p0.halo / per + 4;
     const size_t smem = sizeof(float) * ((4 + seg + 4) + (seg / 4 + 4) + seg / per + 2 * nh) +
-                        sizeof(uint32_t) * search_bits_words(p.nwidths, chunk) + 2 * es * seg;
-    const int64_t nrows = g1 - g0;
-    const dim3 grid(static_cast<unsigned>(ctas > 0 ? std::min<int64_t>(nrows, ctas) : nrows));
-    auto go = [&](auto kernel, auto data) {
+                        sizeof(uint32_t) * search_bits_words(p0.nwidths, chunk) + 2 * es * seg;
+    const dim3 grid(static_cast<unsigned>(ctas > 0 ? std::min<int64_t>(rows, ctas) : rows));
+    auto go = [&](auto kernel) {
         FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-        kernel<<<grid, kThreads, smem, s>>>(p, data, level.pitch, level.base, g0, nrows);
+        kernel<<<grid, kThreads, smem, s>>>(t);
     };
     // widths 1, 2, 4, ... (no trapezoid): the unrolled steady-state tests
-    const bool pow2 = p.pow2_widths != 0 && !p.trapezoid && p.nwidths <= kMaxPow2Widths;
-    auto typed = [&](auto tag, const auto* data) {
+    const bool pow2 = p0.pow2_widths != 0 && !p0.trapezoid && p0.nwidths <= kMaxPow2Widths;
+    auto typed = [&](auto tag) {
         using S = decltype(tag);
         if (chunk == 2048)
-            pow2 ? go(k_search<S, 2048, true>, data) : go(k_search<S, 2048, false>, data);
+            pow2 ? go(k_search<S, 2048, true, K>) : go(k_search<S, 2048, false, K>);
         else
-            pow2 ? go(k_search<S, 4096, true>, data) : go(k_search<S, 4096, false>, data);
+            pow2 ? go(k_search<S, 4096, true, K>) : go(k_search<S, 4096, false, K>);
     };
-    if (level.fp16)
-        typed(__half{}, static_cast<const __half*>(level.data));
+    if (segs[0].fp16)
+        typed(__half{});
     else
-        typed(float{}, static_cast<const float*>(level.data));
+        typed(float{});
     FB_LAUNCH_CHECK();
+}
+
+} // namespace
+
+void launch_search_segs(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t ctas) {
+    if (chunk != 2048 && chunk != 4096)
+        throw Error(FROST_ERR_INTERNAL, "search: chunk must be 2048 or 4096 samples");
+    // segments without rows or valid columns launch nothing
+    int m = 0;
+    for (int i = 0; i < n; ++i)
+        if (segs[i].nrows > 0 && segs[i].p.n_valid > 0)
+            segs[m++] = segs[i];
+    if (m == 0)
+        return;
+    if (m == 1) {
+        search_table<1>(segs, 1, s, chunk, ctas);
+        return;
+    }
+    for (int i = 0; i < m; i += kMaxSearchSegs)
+        search_table<kMaxSearchSegs>(segs + i, std::min(kMaxSearchSegs, m - i), s, chunk, ctas);
+}
+
+void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1, cudaStream_t s,
+                   int32_t chunk, int32_t ctas) {
+    if (g1 <= g0 || p.n_valid <= 0)
+        return;
+    SearchSeg g{};
+    g.p     = p;
+    g.level = level.data;
+    g.pitch = level.pitch;
+    g.base  = level.base;
+    g.fp16  = level.fp16;
+    g.g0    = g0;
+    g.nrows = g1 - g0;
+    launch_search_segs(&g, 1, s, chunk, ctas);
 }
 
 void launch_variance(const SearchRow* rows, const PlaneInfo* planes, const int64_t* leaf_offset,

@@ -84,6 +84,31 @@ struct SearchParams {
     long long wait_limit;    // tries of a chunk's first wait (a drain uses kSpinLimit)
 };
 
+/** One engine's search of rows [g0, g0 + nrows) of one level as a segment
+ * of a search launch; a launch covers the segments of several beams whose
+ * search shape (widths, halo, peak mode, trapezoid, cold prefix, valid
+ * columns) is the same. row_end is filled by the launcher. */
+struct SearchSeg {
+    SearchParams p;
+    const void* level;
+    int64_t pitch;
+    int32_t base;
+    int32_t fp16;
+    int64_t g0;
+    int64_t nrows;
+    int64_t row_end;
+};
+constexpr int kMaxSearchSegs = 32;
+template <int K> struct SearchSegTable {
+    int32_t n;
+    int32_t pad;
+    SearchSeg s[K];
+};
+
+/** One launch (or one per kMaxSearchSegs) over `n` search segments of the
+ * same shape and element type. */
+void launch_search_segs(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk = kSearchChunk, int32_t ctas = 0);
+
 /** Searches rows [g0, g1) (all in `level`) over the tile's valid columns,
  * `chunk` (2048 or 4096) samples per step of a CTA: the smaller chunk needs
  * half the shared memory and fewer registers, so more CTAs fit an SM, at

@@ -145,16 +145,17 @@ void Beam::postprocess(bool final_call) {
     m_last_launches += pp::launch_counter() - l0;
 }
 
-void Beam::process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device) {
+const float* Beam::clean(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device) {
     if (bytes != block_bytes())
         invalid("serve: a gulp must be a whole block of max_nsamps rows");
-    const uint64_t l0 = m_cleaner->launches();
-    const float* wf   = m_cleaner->execute_normalized(block, bytes, nread, on_device, nullptr);
+    const float* wf = m_cleaner->execute_normalized(block, bytes, nread, on_device, nullptr);
     m_fdmt_mask     = m_cleaner->channel_mask();
     if (m_descending)
         std::reverse(m_fdmt_mask.begin(), m_fdmt_mask.end());
-    m_engine->execute(wf, m_spec.layout.max_nsamps, true, m_fdmt_mask.data(), m_cleaner->stream());
-    m_last_launches = (m_cleaner->launches() - l0) + m_engine->last_launches();
+    return wf;
+}
+
+void Beam::account(SizeType nread) {
     // samples searched: frost's accounting, lib/pipeline/pipeline.cpp:610-614
     m_read += nread;
     m_last_nread            = nread;
@@ -162,6 +163,14 @@ void Beam::process(const uint8_t* block, SizeType bytes, SizeType nread, bool on
     if (m_read > m_max_delay)
         m_searched += m_read - std::max(previous, m_max_delay);
     postprocess(false);
+}
+
+void Beam::process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device) {
+    const uint64_t l0 = m_cleaner->launches();
+    const float* wf   = clean(block, bytes, nread, on_device);
+    m_engine->execute(wf, m_spec.layout.max_nsamps, true, m_fdmt_mask.data(), m_cleaner->stream());
+    m_last_launches = (m_cleaner->launches() - l0) + m_engine->last_launches();
+    account(nread);
 }
 
 std::vector<frost_candidate> Beam::drain() {

@@ -45,6 +45,17 @@ public:
     /** Cleans and searches one gulp (a block of max_nsamps rows, nread
      * valid, on the host or on the beam's device). */
     void process(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device);
+    /** The RFI half of process(): cleans and normalises the gulp on the
+     * cleaner's stream and takes its channel mask into FDMT order; returns
+     * the device waterfall. */
+    const float* clean(const uint8_t* block, SizeType bytes, SizeType nread, bool on_device);
+    /** The bookkeeping after a gulp's search: frost's searched-samples
+     * accounting and the post-processing, if any. */
+    void account(SizeType nread);
+    fdmt::Engine& engine() { return *m_engine; }
+    rfi::Cleaner& cleaner() { return *m_cleaner; }
+    const std::vector<uint8_t>& fdmt_mask() const { return m_fdmt_mask; }
+    SizeType gulp_nsamps() const { return m_spec.layout.max_nsamps; }
     std::vector<frost_candidate> results() const { return m_engine->results(); }
     std::vector<frost_candidate> drain();
     /** Adds CandidatePostprocessPlan after the search of every gulp

@@ -642,6 +642,64 @@ int frost_server_drain(frost_server* s,
 int frost_server_get_stats(frost_server* s, frost_server_stats* out);
 int frost_server_reset_stats(frost_server* s);
 
+/* ---- batched multi-beam search -------------------------------------------
+ *
+ * No counterpart in the reference: frost runs one engine per pipeline and
+ * one beam per process (lib/pipeline/pipeline.cpp:346-367). A batch runs one
+ * gulp of each of its beams per call: the beams' RFI stages concurrently,
+ * then their searches as rounds in which the level steps of all beams are
+ * one launch and their searches one launch (segment tables over the beams'
+ * buffers), captured once as a CUDA graph and replayed while the beams'
+ * waterfalls stay in place. Beams may differ in channel count, sample type,
+ * gulp length, DM range and plane count; each beam's candidates equal those
+ * of the same beam run alone. */
+
+typedef struct {
+    uint64_t executes;
+    uint64_t beams;
+    uint64_t rounds;                  /* (tile, level step) rounds run */
+    uint64_t merged_level_launches;   /* level launches covering many beams */
+    uint64_t merged_search_launches;  /* search launches covering many beams */
+    uint64_t beam_launches;           /* per-beam launches of the rounds */
+    uint64_t graph_replays;
+    uint64_t device_bytes;            /* charged to admitted beams */
+} frost_batch_stats;
+
+typedef struct frost_batch frost_batch;
+
+/* memory_budget 0 = 90 % of the device's free memory. */
+int frost_batch_create(int device, size_t memory_budget, frost_batch** out);
+int frost_batch_destroy(frost_batch* b);
+
+/* Admits a beam (as frost_server_add_beam: launch shape tuned, buffers
+ * allocated, FROST_ERR_OUT_OF_MEMORY beyond the budget); beams are numbered
+ * 0, 1, ... in the order they are added. */
+int frost_batch_add_beam(frost_batch* b,
+                         const frost_rfi_config* rfi,
+                         const frost_block_layout* layout,
+                         float baseline_length,
+                         const frost_dedisp_plan_config* plan,
+                         const frost_boxcar_config* search,
+                         uint32_t* beam);
+
+/* One gulp of every beam: blocks[i] is beam i's block of max_nsamps rows,
+ * nread[i] of them valid, in host memory or (on_device) complete in device
+ * memory. The candidates are read with frost_batch_results. */
+int frost_batch_execute(frost_batch* b, const uint8_t* const* blocks, const size_t* nread, int on_device);
+
+/* Copies up to `capacity` of beam's last candidates (sorted as
+ * frost_search_results); *count is their number; FROST_ERR_OVERFLOW if some
+ * did not fit. */
+int frost_batch_results(const frost_batch* b, uint32_t beam, frost_candidate* out, size_t capacity, size_t* count);
+
+/* drain() of one beam's engine (end of its stream). */
+int frost_batch_drain(frost_batch* b, uint32_t beam, frost_candidate* out, size_t capacity, size_t* count);
+
+/* CUDA-graph replay of the batched rounds (default on). */
+int frost_batch_use_graph(frost_batch* b, int enable);
+
+int frost_batch_get_stats(const frost_batch* b, frost_batch_stats* out);
+
 /* ---- input staging (GulpPrefetch, lib/pipeline/pipeline.cpp:105-262) -----
  *
  * frost's GulpPrefetch reads the next block on a thread while the caller
