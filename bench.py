@@ -178,8 +178,8 @@ def measured_peaks():
 
 
 def ncu_traffic_per_launch():
-    """Level-kernel DRAM bytes per launch from the committed ncu summary,
-    scaled to the full gulp (profiles/fdmt_level_config2.md), or None."""
+    """Level-kernel DRAM bytes per launch from the committed ncu summary
+    (profiles/fdmt_level_config2.json), scaled to the full gulp, or None."""
     path = os.path.join(ROOT, "profiles", "fdmt_level_config2.json")
     try:
         with open(path) as f:
