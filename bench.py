@@ -428,6 +428,17 @@ def run_gpu(args):
         "phase_ms_per_step": {k: round(t[k] / args.steps, 3) for k in
                               ("level1_ms", "level_ms", "search_ms", "history_ms", "variance_ms")},
     }
+    # the unfused per-beam-gulp model: two raw passes and the normalised
+    # waterfall's write and read, plus every FDMT level read and written once
+    # with its history and every searched plane read once
+    rfi_model = 2 * NCHANS * GULP * 1 + 2 * NCHANS * GULP * 4  # uint8 samples
+    fdmt_model = t["unfused_model_bytes"] / max(t["executes"], 1)
+    model = rfi_model + fdmt_model
+    step_s = single16["total_ms"] / args.steps / 1e3
+    roofline["unfused_model"] = {
+        "bytes_per_beam_gulp": int(model), "rfi_bytes": int(rfi_model), "fdmt_search_bytes": int(fdmt_model),
+        "achieved_gbs": round(model / step_s / 1e9, 1), "frac": round(model / step_s / 1e9 / peak, 4),
+        "what": "unfused model bytes of one beam-gulp over the plain FP16 step time (fusion moves fewer bytes)"}
     from frost_b200.search import candidate_list_diff
     fp16_vs_fp32 = candidate_list_diff(single32["last"], served["last0"], 7.0)
     fp16_vs_fp32["what"] = ("served FP16 beam 0 against the plain FP32 path on the same gulp after the same "
@@ -832,14 +843,21 @@ BATCH = dict(beams=32, tile=32768)
 def batch_beams(n):
     """The multi-beam workload's beams, seeded: channels 1024 / 2048 / 4096,
     uint8 or float32, gulps of 2^15 - 2^18 samples, DM max 500 - 3000, 1, 4
-    or 11 sub-band planes."""
+    or 11 sub-band planes. A gulp must exceed the beam's largest dispersion
+    delay plus the widest boxcar (frost's rule), so a drawn length is doubled
+    until it does (1200-1536 MHz at 64 us: 17.54 samples per unit DM)."""
     import numpy as np
     rng = np.random.default_rng(0x46524F5354 ^ 3)
     out = []
     for b in range(n):
         C = int(rng.choice([1024, 2048, 4096]))
-        out.append(dict(C=C, f32=bool(rng.integers(0, 2)), T=int(2 ** rng.integers(15, 19)),
-                        dm_max=float(round(rng.uniform(500.0, 3000.0), 1)), depth=int(rng.choice([0, 1, 2]))))
+        f32 = bool(rng.integers(0, 2))
+        T = int(2 ** rng.integers(15, 19))
+        dm_max = float(round(rng.uniform(500.0, 3000.0), 1))
+        depth = int(rng.choice([0, 1, 2]))
+        while T <= 17.6 * dm_max + 2 * MAX_BOXCAR:
+            T *= 2
+        out.append(dict(C=C, f32=f32, T=T, dm_max=dm_max, depth=depth))
     return out
 
 
@@ -898,7 +916,12 @@ def run_config3(args):
                 ids.append(None)
         return ids
 
-    batch = BeamBatch(device=local)
+    # the beams' device-resident gulps are allocated after admission: keep
+    # their bytes (and 2 GiB) out of the batch's and the server's budgets
+    gulp_bytes = sum(sp["T"] * sp["C"] * (4 if sp["f32"] else 1) for sp in specs)
+    free, _ = torch.cuda.mem_get_info(local)
+    budget = max(int(0.9 * (free - gulp_bytes - (2 << 30))), 1)
+    batch = BeamBatch(device=local, memory_budget=budget)
     ids = admit(batch.add_beam)
     keep = [i for i, b in enumerate(ids) if b is not None]
     dev = {}
@@ -928,7 +951,7 @@ def run_config3(args):
     st = batch.stats()
     batch.close()
     torch.cuda.empty_cache()
-    srv = BeamServer(device=local, slots=len(keep))
+    srv = BeamServer(device=local, memory_budget=budget, slots=len(keep))
     sid = admit(srv.add_beam)
     served = [i for i in keep if sid[i] is not None]
 

@@ -232,6 +232,7 @@ class SearchTimingC(C.Structure):
         ("algorithmic_level1_bytes", C.c_uint64),
         ("algorithmic_search_bytes", C.c_uint64),
         ("executes", C.c_uint64),
+        ("unfused_model_bytes", C.c_uint64),
     ]
 
 

@@ -1,9 +1,9 @@
 // FDMT level kernels for sm_100a.
 //
 // Every level is one streaming pass: read two child rows, write one parent
-// row, HBM-bound. Level 1 is fused with the leaf initialisation (the
-// per-channel window sums are prefix-sum differences in shared memory), so
-// the ~C * (1 + d) leaf rows are never materialised. Rows live in level
+// row, HBM-bound. Level 1 is fused with the leaf initialisation (each
+// thread slides the per-channel window sums over the node's rows in
+// shared memory), so the ~C * (1 + d) leaf rows are never materialised. Rows live in level
 // buffers with a per-level history prefix (see LevelView), so a shifted read
 // t - d_lo before the tile start lands in the history columns without a
 // branch. The shifted (high-child) row segment of each CTA is staged in
@@ -48,59 +48,25 @@ __device__ __forceinline__ uint32_t pack_sat(float lo, float hi) {
     return r;
 }
 
-// Inclusive block scan of smem[0..n) in place (float), n <= kThreads * 64.
-// Inclusive prefix sum of a[0..n) in place, in FP64: leaf windows are
-// differences of these sums, and a double prefix keeps each window sum
-// within one rounding of its exact value however long the tile is (a float
-// prefix would carry an error proportional to the running sum).
-__device__ void block_scan(double* a, int n) {
-    __shared__ double warp_tot[kThreads / 32];
-    const int per  = (n + kThreads - 1) / kThreads;
-    const int beg  = threadIdx.x * per;
-    const int end  = min(beg + per, n);
-    double run     = 0.0;
-    for (int i = beg; i < end; ++i) {
-        run += a[i];
-        a[i] = run;
-    }
-    // exclusive scan of the per-thread totals
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double v       = run;
-    for (int o = 1; o < 32; o <<= 1) {
-        const double u = __shfl_up_sync(0xFFFFFFFFU, v, o);
-        if (lane >= o)
-            v += u;
-    }
-    if (lane == 31)
-        warp_tot[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        double w = lane < kThreads / 32 ? warp_tot[lane] : 0.0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const double u = __shfl_up_sync(0xFFFFFFFFU, w, o);
-            if (lane >= o)
-                w += u;
-        }
-        if (lane < kThreads / 32)
-            warp_tot[lane] = w;
-    }
-    __syncthreads();
-    const double offset = (v - run) + (warp > 0 ? warp_tot[warp - 1] : 0.0);
-    for (int i = beg; i < end; ++i)
-        a[i] += offset;
-    __syncthreads();
-}
-
+// Level 1 with the leaf initialisation: row (d_lo, d_hi) of a two-channel
+// node at time t is sum_{s=0..d_lo} a[t - s] + sum_{s=0..d_hi} b[t - d_lo - s]
+// (one channel: the first term). The node's rows have non-decreasing d_lo
+// and d_hi (ascending delays), so each thread walks them in order and moves
+// its two windows by the samples that enter or leave them, accumulating in
+// double (every window sum is then its exact value to ~1e-16 relative,
+// however long the tile, and rounds once to float). The two channels' tile
+// segments, with the H samples before the tile, sit in shared memory as
+// floats; thread t owns samples t, t + 256, ... of the tile.
 template <class S>
 __global__ void __launch_bounds__(kThreads)
     k_level1(const LeafOp* __restrict__ ops, const int32_t* __restrict__ node_first_op, int32_t nnodes,
              int32_t ntiles, int32_t H, const float* __restrict__ wf, int64_t wpitch, int64_t t0,
              int32_t n_valid, const float* __restrict__ hist, int32_t hist_len, S* __restrict__ out,
              int64_t pitch, int32_t base) {
-    extern __shared__ double smem_d[];
+    extern __shared__ float smem_x[];
     const int32_t N = kTimePerCta + H + 1;
-    double* Pa      = smem_d;
-    double* Pb      = smem_d + N;
+    float* Xa       = smem_x;
+    float* Xb       = smem_x + N;
     // Work items (node, tile), nodes fastest; a CTA takes items blockIdx.x,
     // blockIdx.x + gridDim.x, ...
     const int64_t nitems = static_cast<int64_t>(nnodes) * ntiles;
@@ -110,7 +76,7 @@ __global__ void __launch_bounds__(kThreads)
         const int32_t ca  = ops[op0].chan_lo;
         const int32_t cb  = ops[op0].chan_hi;
         const int32_t k0  = static_cast<int32_t>(item / nnodes) * kTimePerCta;
-        // x(i) for tile-relative time t = k0 + i - H - 1; x(0) is the scan base.
+        // x(i) for tile-relative time t = k0 + i - H - 1 (index 0 unused)
         for (int i = threadIdx.x; i < N; i += kThreads) {
             const int64_t t = static_cast<int64_t>(k0) + i - H - 1;
             float a = 0.0F, b = 0.0F;
@@ -125,26 +91,67 @@ __global__ void __launch_bounds__(kThreads)
                         b = wf[static_cast<int64_t>(cb) * wpitch + t0 + t];
                 }
             }
-            Pa[i] = a;
-            Pb[i] = b;
+            Xa[i] = a;
+            Xb[i] = b;
         }
         __syncthreads();
-        block_scan(Pa, N);
-        if (cb >= 0)
-            block_scan(Pb, N);
+        // window state per owned sample: A = sum a[t - dl .. t],
+        // B = sum b[t - dl - dh .. t - dl]; (dl, dh) = (-1, -1): both empty
+        double A[kPer], B[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            A[j] = 0.0;
+            B[j] = 0.0;
+        }
+        int32_t dl = -1, dh = -1;
+        const int i0 = threadIdx.x + H + 1; // index of the thread's first sample
         for (int32_t r = op0; r < op1; ++r) {
             const LeafOp op = ops[r];
-            S* row          = out + static_cast<int64_t>(r) * pitch + base + k0;
-            for (int j = 0; j < kPer; ++j) {
-                const int k = threadIdx.x + j * kThreads;
-                const int i = k + H + 1;
-                double v    = Pa[i] - Pa[i - op.d_lo - 1];
-                if (cb >= 0)
-                    v += Pb[i - op.d_lo] - Pb[i - op.d_lo - op.d_hi - 1];
-                st<S>(row + k, static_cast<float>(v));
+            S* row          = out + static_cast<int64_t>(r) * pitch + base + k0 + threadIdx.x;
+            // A's window grows from dl to op.d_lo samples back (restarts if
+            // the rows ever went backwards)
+            int32_t from = dl + 1;
+            if (op.d_lo < dl) {
+#pragma unroll
+                for (int j = 0; j < kPer; ++j)
+                    A[j] = 0.0;
+                from = 0;
             }
+            for (int32_t q = from; q <= op.d_lo; ++q)
+#pragma unroll
+                for (int j = 0; j < kPer; ++j)
+                    A[j] += static_cast<double>(Xa[i0 + j * kThreads - q]);
+            if (cb >= 0) {
+                // B's window moves from back offsets [dl, dl + dh] to
+                // [op.d_lo, op.d_lo + op.d_hi]: drop the top, add the bottom,
+                // or start afresh when the two do not overlap
+                const int32_t ob = dl + dh, nb = op.d_lo + op.d_hi;
+                if (dh < 0 || op.d_lo > ob || nb < ob || op.d_lo < dl) {
+#pragma unroll
+                    for (int j = 0; j < kPer; ++j)
+                        B[j] = 0.0;
+                    for (int32_t q = op.d_lo; q <= nb; ++q)
+#pragma unroll
+                        for (int j = 0; j < kPer; ++j)
+                            B[j] += static_cast<double>(Xb[i0 + j * kThreads - q]);
+                } else {
+                    for (int32_t q = dl; q < op.d_lo; ++q)
+#pragma unroll
+                        for (int j = 0; j < kPer; ++j)
+                            B[j] -= static_cast<double>(Xb[i0 + j * kThreads - q]);
+                    for (int32_t q = ob + 1; q <= nb; ++q)
+#pragma unroll
+                        for (int j = 0; j < kPer; ++j)
+                            B[j] += static_cast<double>(Xb[i0 + j * kThreads - q]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kPer; ++j)
+                st<S>(row + j * kThreads, static_cast<float>(A[j] + B[j]));
+            dl = op.d_lo;
+            dh = op.d_hi;
         }
-        __syncthreads(); // every thread is done with Pa / Pb
+        __syncthreads(); // every thread is done with Xa / Xb
     }
 }
 
@@ -688,7 +695,7 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
         throw Error(FROST_ERR_INTERNAL, "level1: bad geometry");
     const int32_t ntiles = ncols / kTimePerCta;
     const dim3 grid(grid_for(static_cast<int64_t>(nnodes) * ntiles, ctas));
-    const size_t smem = 2 * sizeof(double) * (kTimePerCta + max_node_delay + 1);
+    const size_t smem = 2 * sizeof(float) * (kTimePerCta + max_node_delay + 1);
     if (smem > 200 * 1024)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "level1: leaf windows too long for shared memory");
     if (out.fp16) {

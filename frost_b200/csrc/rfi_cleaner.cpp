@@ -257,10 +257,15 @@ Cleaner::Cleaner(const frost_rfi_config& cfg, const frost_block_layout& layout,
     if (!m_lags.empty())
         FB_CUDA(cudaMemcpyAsync(m_cw.lags, m_lags.data(), m_lags.size() * sizeof(uint64_t),
                                 cudaMemcpyHostToDevice, m_stream));
-    // Reciprocals of the Welford counts (correctly rounded host divisions).
-    std::vector<double> recip(layout.max_nsamps + 1, 0.0);
-    for (SizeType n = 1; n < recip.size(); ++n)
-        recip[n] = 1.0 / static_cast<double>(n);
+    // Two-term reciprocals of the Welford counts: y_hi = RN(1/n) and
+    // y_lo = RN((1 - n y_hi) / n), the residual exact by a fused multiply-add.
+    std::vector<double> recip(2 * (layout.max_nsamps + 1), 0.0);
+    for (SizeType n = 1; n <= layout.max_nsamps; ++n) {
+        const double dn = static_cast<double>(n);
+        const double yh = 1.0 / dn;
+        recip[2 * n]     = yh;
+        recip[2 * n + 1] = std::fma(-dn, yh, 1.0) / dn;
+    }
     h2d(m_recip, recip.data(), recip.size(), m_stream);
     FB_CUDA(cudaStreamSynchronize(m_stream));
 }
@@ -354,9 +359,9 @@ SizeType Cleaner::estimate_memory(const frost_rfi_config& cfg, const frost_block
     total += 2 * n * f + n * sizeof(ZdotSums) + 2 * n * sizeof(Run);
     // tables uploaded per gulp: masks, good-channel prefix, zero-DM fit,
     // Kadane segments, flagged samples (at most every sample), Welford
-    // reciprocals
+    // two-term reciprocals
     total += 2 * n + (n + 1) * sizeof(uint64_t) + 2 * n * f + 2 * (kchan ? n : 1) * sizeof(Segment) + n;
-    total += T1 * sizeof(uint64_t) + (T + 1) * sizeof(double);
+    total += T1 * sizeof(uint64_t) + 2 * (T + 1) * sizeof(double);
     return total;
 }
 

@@ -117,7 +117,7 @@ private:
         m_kneg_best, m_time_flags_d, m_zdot_a_d, m_zdot_b_d, m_kchan_pos_d, m_kchan_neg_d, m_kchan_any_d,
         m_flagged_d, m_work, m_out, m_counters, m_first_bad, m_tail_loc, m_tail_scale,
         m_tail_out_loc, m_tail_out_scale;
-    DeviceBuffer m_recip; // [max_nsamps + 1] doubles, recip[n] = RN(1/n)
+    DeviceBuffer m_recip; // [max_nsamps + 1] pairs: RN(1/n) and RN((1 - n RN(1/n)) / n)
     PinnedBuffer m_pinned;
     const uint8_t* m_raw_ptr = nullptr; // raw block of the current call (device)
 

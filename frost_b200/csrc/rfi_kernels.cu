@@ -77,6 +77,10 @@ constexpr uint64_t kBitsOf = D == FROST_UINT1 ? 1 : D == FROST_UINT2 ? 2 : D == 
 // channel) loops: the loads are independent, only the sums are sequential.
 constexpr int kBlock = 16;
 
+// Buffers of the per-window sequence kernels' staging: with one or two CTAs
+// per SM, three stages in flight keep enough bytes moving for the chains.
+constexpr int kDeepStages = 4;
+
 // ---- order-exact helpers ------------------------------------------------
 
 // std::min / std::max semantics (first argument kept on ties), which the
@@ -271,13 +275,161 @@ __global__ void k_bandpass(Dims d, const float* __restrict__ samples, float* __r
     inv_out[o]     = 1.0F / fs;
 }
 
-// The same per-(window, channel) bandpass with the sampled rows streamed
-// through shared memory (rfi_stage.cuh), one thread per channel of a
-// 128-channel segment. Every pass over the rows is one staged sweep; the
-// block runs the optional passes (mean fallback, clip iterations) when any
-// of its channels needs them, and each channel updates only while its own
-// sequence of steps is still running, so every channel takes exactly the
-// steps of the direct kernel above.
+// The remedian is a fixed tree (medians of five consecutive values, level by
+// level), so its groups are independent: k_remedian evaluates it in
+// parallel. One CTA covers 32 channels (a lane each) of one window; each
+// warp reduces 125-row blocks (three tree levels in registers) to one value
+// per channel, and warp 0 finishes the tree over the <= 25 block values.
+// Pass 1 (ABS false) writes the level to loc and a flat flag (every sampled
+// value of the channel compares equal) to inv; pass 2 (ABS true) the scale,
+// remedian(|x - level|) x 1.4826, to scale (lib/cpu/spectra_cpu.cpp:73-130).
+constexpr int kRemedianWarps = 8;
+
+// The remedian of 25 values p[0], p[stride], ... (medians of five
+// consecutive values, then their median): the 25 loads are issued together
+// before any is used, then lo / hi track the range of the raw values.
+template <bool ABS>
+__device__ __forceinline__ float remedian25(const float* __restrict__ p, uint64_t stride, float level, float& lo,
+                                            float& hi) {
+    float x[25];
+#pragma unroll
+    for (int i = 0; i < 25; ++i)
+        x[i] = p[i * stride];
+    float v[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        float y[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            const float r = x[5 * j + i];
+            if constexpr (ABS) {
+                y[i] = fabsf(r - level);
+            } else {
+                lo   = fminf(lo, r);
+                hi   = fmaxf(hi, r);
+                y[i] = r;
+            }
+        }
+        v[j] = median5(y[0], y[1], y[2], y[3], y[4]);
+    }
+    return median5(v[0], v[1], v[2], v[3], v[4]);
+}
+
+template <bool ABS>
+__device__ __forceinline__ float remedian5(const float* __restrict__ p, uint64_t stride, float level, float& lo,
+                                           float& hi) {
+    float y[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const float r = p[i * stride];
+        if constexpr (ABS) {
+            y[i] = fabsf(r - level);
+        } else {
+            lo   = fminf(lo, r);
+            hi   = fmaxf(hi, r);
+            y[i] = r;
+        }
+    }
+    return median5(y[0], y[1], y[2], y[3], y[4]);
+}
+
+// 125 values: five 25-value subtrees in turn (25 loads in flight per lane),
+// their results shifted through registers in order.
+template <bool ABS>
+__device__ __forceinline__ float remedian125(const float* __restrict__ p, uint64_t stride, float level, float& lo,
+                                             float& hi) {
+    float a = 0.0F, b = 0.0F, c = 0.0F, d = 0.0F, e = 0.0F;
+#pragma unroll 1
+    for (int j = 0; j < 5; ++j) {
+        const float t = remedian25<ABS>(p + 25 * j * stride, stride, level, lo, hi);
+        a = b;
+        b = c;
+        c = d;
+        d = e;
+        e = t;
+    }
+    return median5(a, b, c, d, e);
+}
+
+template <bool ABS>
+__global__ void __launch_bounds__(32 * kRemedianWarps)
+    k_remedian(Dims d, const float* __restrict__ samples, float* __restrict__ loc, float* __restrict__ scale,
+               float* __restrict__ flat_out) {
+    __shared__ float part[25][32];
+    __shared__ float plo[kRemedianWarps][32], phi[kRemedianWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t n = d.nchans;
+    const uint64_t c = static_cast<uint64_t>(blockIdx.x) * 32 + lane;
+    const uint64_t w = blockIdx.y;
+    const bool in    = c < n;
+    const uint64_t len = window_end(w, d) - window_begin(w, d.window);
+    const uint64_t m   = largest_power_of_five_leq(len < kMaxBandpassRows ? len : kMaxBandpassRows);
+    int levels = 0;
+    for (uint64_t q = m; q > 1; q /= 5)
+        ++levels;
+    const int kb       = levels < 3 ? levels : 3; // tree levels inside a block
+    const int up       = levels - kb;             // levels over the blocks (0..2)
+    const int nblk     = up == 0 ? 1 : up == 1 ? 5 : 25;
+    const uint64_t blk = kb == 1 ? 5 : kb == 2 ? 25 : 125;
+    const uint64_t o   = w * n + c;
+    const float level  = (ABS && in) ? loc[o] : 0.0F;
+    const float* src   = samples + w * kMaxBandpassRows * n + (in ? c : 0);
+    float lo = FLT_MAX, hi = -FLT_MAX;
+    for (int b = warp; b < nblk; b += kRemedianWarps) {
+        const float* p = src + static_cast<uint64_t>(b) * blk * n;
+        float v        = 0.0F;
+        if (in) {
+            switch (kb) {
+            case 1: v = remedian5<ABS>(p, n, level, lo, hi); break;
+            case 2: v = remedian25<ABS>(p, n, level, lo, hi); break;
+            default: v = remedian125<ABS>(p, n, level, lo, hi); break;
+            }
+        }
+        part[b][lane] = v;
+    }
+    if constexpr (!ABS) {
+        plo[warp][lane] = lo;
+        phi[warp][lane] = hi;
+    }
+    __syncthreads();
+    if (warp != 0 || !in)
+        return;
+    float r;
+    if (up == 0) {
+        r = part[0][lane];
+    } else if (up == 1) {
+        r = median5(part[0][lane], part[1][lane], part[2][lane], part[3][lane], part[4][lane]);
+    } else {
+        float v[5];
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+            v[j] = median5(part[5 * j][lane], part[5 * j + 1][lane], part[5 * j + 2][lane],
+                           part[5 * j + 3][lane], part[5 * j + 4][lane]);
+        r = median5(v[0], v[1], v[2], v[3], v[4]);
+    }
+    if constexpr (ABS) {
+        scale[o] = r * kMadToStd;
+    } else {
+        float a = plo[0][lane], z = phi[0][lane];
+#pragma unroll
+        for (int k = 1; k < kRemedianWarps; ++k) {
+            a = fminf(a, plo[k][lane]);
+            z = fmaxf(z, phi[k][lane]);
+        }
+        loc[o]      = r;
+        flat_out[o] = z > a ? 0.0F : 1.0F;
+    }
+}
+
+// The clipped refinement of the bandpass (lib/cpu/bandpass_kernels.hpp:17-76)
+// after the two remedian passes, with the sampled rows streamed through
+// shared memory (rfi_stage.cuh), one thread per channel of a 128-channel
+// segment. Every pass over the rows is one staged sweep; the block runs the
+// optional passes (mean fallback, clip iterations) when any of its channels
+// needs them, and each channel updates only while its own sequence of steps
+// is still running, so every channel takes exactly the steps of the direct
+// kernel above. A flat channel (every sampled value equal) keeps its first
+// sampled value as its level, as the sequential minimum does.
 constexpr int kBandChans = 128;
 
 __global__ void __launch_bounds__(kBandChans)
@@ -292,9 +444,6 @@ __global__ void __launch_bounds__(kBandChans)
     const uint64_t b   = window_begin(w, d.window);
     const uint64_t len = window_end(w, d) - b;
     const uint64_t m   = largest_power_of_five_leq(len < kMaxBandpassRows ? len : kMaxBandpassRows);
-    int levels         = 0;
-    for (uint64_t p = m; p > 1; p /= 5)
-        ++levels;
     const uint64_t n     = d.nchans;
     const uint64_t pitch = n * sizeof(float);
     const uint64_t left  = pitch - c0 * sizeof(float);
@@ -303,7 +452,7 @@ __global__ void __launch_bounds__(kBandChans)
     const uint8_t* src   = reinterpret_cast<const uint8_t*>(samples + w * kMaxBandpassRows * n + c0);
     // one sweep over rows 0 .. m-1: f(x, i) per row, in order
     auto sweep = [&](auto&& f) {
-        stage::Stager st(stage_buf, src, pitch, seg_bytes, copy, rows, 0, m);
+        stage::StagerN<kDeepStages> st(stage_buf, src, pitch, seg_bytes, copy, rows, 0, m);
         st.start();
         for (int k = 0; k < st.nblk; ++k) {
             st.wait(k);
@@ -317,31 +466,12 @@ __global__ void __launch_bounds__(kBandChans)
         }
     };
 
-    // Level (remedian) and the sample range; then the scale (remedian of
-    // |x - level| times 1.4826) (lib/cpu/spectra_cpu.cpp:73-130).
-    Remedian r;
-    r.init(levels);
-    float lo = 0.0F, hi = 0.0F;
-    sweep([&](float x, uint64_t i) {
-        r.push(x);
-        if (i == 0) {
-            lo = x;
-            hi = x;
-        } else {
-            lo = smin(lo, x);
-            hi = smax(hi, x);
-        }
-    });
-    const float level = r.result;
-    r.init(levels);
-    sweep([&](float x, uint64_t) { r.push(fabsf(x - level)); });
-    const float rms = r.result * kMadToStd;
-
-    // Clipped refinement in double (lib/cpu/bandpass_kernels.hpp:17-76).
-    const uint64_t o = w * n + c;
-    const bool flat  = !(hi > lo);
+    const uint64_t o   = w * n + c;
+    const float level  = in ? loc_out[o] : 0.0F;
+    const float rms    = in ? scale_out[o] : 0.0F;
+    const bool flat    = in && inv_out[o] != 0.0F;
     if (in && flat) {
-        loc_out[o]   = lo;
+        loc_out[o]   = samples[w * kMaxBandpassRows * n + c];
         scale_out[o] = 0.0F;
         inv_out[o]   = 0.0F;
         atomicAdd(&unmeasured[c], 1U);
@@ -510,7 +640,7 @@ __global__ void __launch_bounds__(kStageChans)
     const uint64_t off  = c0 * kBitsOf<D> / 8;
     const uint64_t left = d.row_bytes - off;
     const int copy      = static_cast<int>(left < static_cast<uint64_t>(seg_bytes) ? left : seg_bytes);
-    stage::Stager st(stage_buf, raw + off, d.row_bytes, seg_bytes, copy, rows, b, e);
+    stage::StagerN<kDeepStages> st(stage_buf, raw + off, d.row_bytes, seg_bytes, copy, rows, b, e);
     st.start();
     for (int k = 0; k < st.nblk; ++k) {
         st.wait(k);
@@ -1196,63 +1326,62 @@ __global__ void k_unpack(Dims d, const uint8_t* __restrict__ raw, float* __restr
     }
 }
 
-// a / n for a count n >= 1 with y = RN(1/n) precomputed, correctly
-// rounded (round to nearest even) with one fused multiply-add correction
-// (Markstein's theorem: P. Markstein, "Computation of elementary functions
-// on the IBM RISC System/6000 processor", IBM J. Res. Develop. 34, 1990;
-// Muller et al., Handbook of Floating-Point Arithmetic, ch. 4). q0 = a*y is
-// within 1.5 ulp of a/n, so r = a - q0*n is exact (a multiple of ulp(q0)
-// below 2n ulps); q0 + r*y then differs from a/n by at most ~2^-52 ulp, far
-// less than the distance ulp/(2n) that separates a quotient by an integer
-// n < 2^40 from a rounding midpoint (a/n is never exactly a midpoint), so
-// it rounds as a/n does. Zero is returned as is; tiny |a| (where r could
-// lose bits) takes the plain division (a dependent double division costs
-// ~400 cycles on sm_100, the correction step ~40).
-// The plain division as a call, so the compiler keeps it off the common
-// path instead of computing it alongside (if-converting the branch).
+// Division in the Welford re-measure. The reference updates
+// mean += (x - mean) / n in double. A dependent double division costs
+// ~400 cycles on sm_100; the division by the count is instead
+// q = RN(delta * y_hi + RN(delta * y_lo)) (one multiply, one fused
+// multiply-add), with y_hi = RN(1/n) and y_lo = RN((1 - n y_hi) / n) from
+// the host (1 - n y_hi is exact in double). y_hi + y_lo is within 2^-105 / n
+// of 1/n and the product's rounding adds at most 2^-105 |delta| / n, so the
+// value rounded is within 2^-104 relative of delta / n; delta / n is never a
+// rounding midpoint (n delta-midpoint products need more than 53 bits) and
+// lies at least 2^-54 / n relative from every midpoint, far more than
+// 2^-104 for n < 2^40, so q is the correctly rounded quotient, as
+// Markstein-style corrections argue (P. Markstein, IBM J. Res. Develop. 34,
+// 1990; Muller et al., Handbook of Floating-Point Arithmetic, ch. 4). Tiny
+// nonzero |delta| (where delta * y_lo could lose bits) takes the plain
+// division. The plain division as a call, so the compiler keeps it off the
+// common path instead of computing it alongside (if-converting the branch).
 __device__ __noinline__ double div_plain(double a, double n) { return a / n; }
 
-__device__ __forceinline__ double div_by_count(double a, double n, double y) {
-    if (a == 0.0)
-        return a; // exactly 0 / n, sign included (constant and masked channels)
-    if (!(fabs(a) > 0x1p-900))
-        return div_plain(a, n);
-    const double q0 = a * y;
-    const double r  = fma(-q0, n, a);
-    return fma(r, y, q0);
-}
-
 // One (window, channel) Welford sequence of the re-measure after a
-// transform (lib/cpu/rfi_cpu.cpp:219-238).
+// transform (lib/cpu/rfi_cpu.cpp:219-238). The mean never becomes -0 (it
+// starts at +0 and a rounded sum is -0 only when both terms are), so a zero
+// quotient (delta = +-0) leaves it unchanged without a select.
 struct WelfordAcc {
     double mean = 0.0, var = 0.0;
     uint64_t b;
-    const double* recip; // recip[n] = RN(1/n), or null for the plain division
+    const double* recip; // recip[2n], recip[2n + 1] = y_hi, y_lo of 1/n, or null for the plain division
     __device__ __forceinline__ void step(float xf, uint64_t t) {
         const uint64_t n = t - b + 1;
         if (recip != nullptr)
-            step_by(xf, static_cast<double>(n), recip[n]);
+            step_recip(xf, static_cast<double>(n), recip[2 * n], recip[2 * n + 1]);
         else
-            step_by(xf, static_cast<double>(n), 0.0);
+            step_plain(xf, static_cast<double>(n));
     }
-    /** The update for the n-th sample given y = RN(1/n) (y = 0: divide). */
-    __device__ __forceinline__ void step_by(float xf, double n, double y) {
+    __device__ __forceinline__ void step_plain(float xf, double n) {
         const double x     = xf;
         const double delta = x - mean;
-        mean += y != 0.0 ? div_by_count(delta, n, y) : div_plain(delta, n);
+        mean += div_plain(delta, n);
         var += delta * (x - mean);
     }
-    /** step_by for y = RN(1/n) > 0, with div_by_count's cases folded into
-     * one rarely taken branch and a select (the same bits): a zero
-     * numerator is returned as is, a tiny or NaN one takes the division. */
-    __device__ __forceinline__ void step_recip(float xf, double n, double y) {
+    /** step_recip without the tiny-numerator branch: `bad` records that
+     * the step needed it (the caller then redoes the steps with it). */
+    __device__ __forceinline__ void step_fast(float xf, double yh, double yl, bool& bad) {
         const double x     = xf;
         const double delta = x - mean;
-        const double q0    = delta * y;
-        double q           = fma(fma(-q0, n, delta), y, q0);
+        bad |= !(fabs(delta) > 0x1p-900) && delta != 0.0;
+        mean += fma(delta, yh, delta * yl);
+        var += delta * (x - mean);
+    }
+    /** The update for the n-th sample given the two-term reciprocal of n. */
+    __device__ __forceinline__ void step_recip(float xf, double n, double yh, double yl) {
+        const double x     = xf;
+        const double delta = x - mean;
+        double q           = fma(delta, yh, delta * yl);
         if (!(fabs(delta) > 0x1p-900) && delta != 0.0)
             q = div_plain(delta, n);
-        mean += delta == 0.0 ? delta : q;
+        mean += q;
         var += delta * (x - mean);
     }
 };
@@ -1285,7 +1414,7 @@ __global__ void __launch_bounds__(kStageChans)
     k_welford_staged(Dims d, const float* __restrict__ work, const double* __restrict__ recip,
                      float* __restrict__ loc, float* __restrict__ scale, int seg_bytes, int rows) {
     extern __shared__ __align__(16) uint8_t stage_buf[];
-    __shared__ double ys[2][256]; // reciprocal counts of each stage's rows (rows <= 256)
+    __shared__ double2 ys[kDeepStages][kStageChans]; // two-term reciprocals of each stage's rows
     const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kStageChans;
     const uint64_t c  = c0 + threadIdx.x;
     const uint64_t w  = blockIdx.y;
@@ -1296,18 +1425,19 @@ __global__ void __launch_bounds__(kStageChans)
     const uint64_t left  = pitch - c0 * sizeof(float);
     const int copy       = static_cast<int>(left < static_cast<uint64_t>(seg_bytes) ? left : seg_bytes);
     const int stride     = seg_bytes / static_cast<int>(sizeof(float));
-    stage::Stager st(stage_buf, reinterpret_cast<const uint8_t*>(work + c0), pitch, seg_bytes, copy,
-                     rows, b, e);
+    stage::StagerN<kDeepStages> st(stage_buf, reinterpret_cast<const uint8_t*>(work + c0), pitch, seg_bytes,
+                                   copy, rows, b, e);
     // The reciprocals of a stage's counts are read into shared memory with
     // the stage, so no load sits on the sequential update chain.
     auto load_recip = [&](int k) {
         if (k < st.nblk && static_cast<int>(threadIdx.x) < st.rows_of(k)) {
             const uint64_t n = st.t0(k) - b + 1 + threadIdx.x;
-            ys[k & 1][threadIdx.x] = recip != nullptr ? recip[n] : 0.0;
+            ys[k % kDeepStages][threadIdx.x] = recip != nullptr ? make_double2(recip[2 * n], recip[2 * n + 1])
+                                                                : make_double2(0.0, 0.0);
         }
     };
-    load_recip(0);
-    load_recip(1);
+    for (int k = 0; k < kDeepStages; ++k)
+        load_recip(k);
     st.start();
     for (int k = 0; k < st.nblk; ++k) {
         st.wait(k);
@@ -1316,20 +1446,37 @@ __global__ void __launch_bounds__(kStageChans)
         double nd         = static_cast<double>(st.t0(k) - b); // exact below 2^53
         if (in) {
             if (recip != nullptr) {
-#pragma unroll 8
-                for (int r = 0; r < nr; ++r) {
-                    nd += 1.0;
-                    acc.step_recip(buf[r * stride + threadIdx.x], nd, ys[k & 1][r]);
+                // Eight steps at a time without a branch on the update chain;
+                // the rare eight with a tiny nonzero numerator are redone with
+                // the plain division where it is needed.
+                const double2* yk = ys[k % kDeepStages];
+                for (int r0 = 0; r0 < nr; r0 += 8) {
+                    const double m0 = acc.mean, v0 = acc.var;
+                    bool bad        = false;
+                    if (r0 + 8 <= nr) {
+#pragma unroll
+                        for (int r = r0; r < r0 + 8; ++r)
+                            acc.step_fast(buf[r * stride + threadIdx.x], yk[r].x, yk[r].y, bad);
+                    } else {
+                        for (int r = r0; r < nr; ++r)
+                            acc.step_fast(buf[r * stride + threadIdx.x], yk[r].x, yk[r].y, bad);
+                    }
+                    if (bad) {
+                        acc.mean = m0;
+                        acc.var  = v0;
+                        for (int r = r0; r < min(r0 + 8, nr); ++r)
+                            acc.step_recip(buf[r * stride + threadIdx.x], nd + (r + 1), yk[r].x, yk[r].y);
+                    }
                 }
             } else {
                 for (int r = 0; r < nr; ++r) {
                     nd += 1.0;
-                    acc.step_by(buf[r * stride + threadIdx.x], nd, 0.0);
+                    acc.step_plain(buf[r * stride + threadIdx.x], nd);
                 }
             }
         }
         st.release(k);
-        load_recip(k + 2);
+        load_recip(k + kDeepStages);
     }
     if (in) {
         loc[w * d.nchans + c] = static_cast<float>(acc.mean);
@@ -1547,11 +1694,18 @@ void launch_bandpass(const Dims& d, const float* samples, float* loc, float* sca
         const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nwin));
         k_bandpass<<<grid, 64, 0, s>>>(d, samples, loc, scale, inv, unmeasured);
     } else {
-        const int seg  = static_cast<int>(std::min<uint64_t>(kBandChans * sizeof(float), pitch));
-        const int rows = std::max(8, 16384 / seg);
+        // level and flat flag, then the scale, then the clipped refinement
+        const dim3 rgrid(grid1(d.nchans, 32), static_cast<unsigned>(d.nwin));
+        k_remedian<false><<<rgrid, 32 * kRemedianWarps, 0, s>>>(d, samples, loc, scale, inv);
+        FB_COUNT_LAUNCH();
+        k_remedian<true><<<rgrid, 32 * kRemedianWarps, 0, s>>>(d, samples, loc, scale, inv);
+        FB_COUNT_LAUNCH();
+        const int seg     = static_cast<int>(std::min<uint64_t>(kBandChans * sizeof(float), pitch));
+        const int rows    = std::max(8, 16384 / seg);
+        const size_t smem = kDeepStages * static_cast<size_t>(seg) * rows;
         const dim3 grid(grid1(d.nchans, kBandChans), static_cast<unsigned>(d.nwin));
-        k_bandpass_staged<<<grid, kBandChans, 2 * static_cast<size_t>(seg) * rows, s>>>(
-            d, samples, loc, scale, inv, unmeasured, seg, rows);
+        set_smem(reinterpret_cast<const void*>(&k_bandpass_staged), smem);
+        k_bandpass_staged<<<grid, kBandChans, smem, s>>>(d, samples, loc, scale, inv, unmeasured, seg, rows);
     }
     FB_COUNT_LAUNCH();
 }
@@ -1564,6 +1718,7 @@ constexpr int kStageBytes = 16 * 1024;
 struct StageGeom {
     int seg_bytes = 0, rows = 0;
     size_t smem() const { return 2 * static_cast<size_t>(seg_bytes) * rows; }
+    size_t smem_deep() const { return kDeepStages * static_cast<size_t>(seg_bytes) * rows; }
 };
 
 bool aligned16(const void* p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; }
@@ -1587,8 +1742,11 @@ void launch_moments(const Dims& d, const uint8_t* raw, const float* loc, const f
         FB_DISPATCH(d.dtype, k_moments<D><<<grid, 64, 0, s>>>(d, raw, loc, inv, static_mask, clip, out));
     } else {
         const dim3 grid(grid1(d.nchans, kStageChans), static_cast<unsigned>(d.nwin));
-        FB_DISPATCH(d.dtype, k_moments_staged<D><<<grid, kStageChans, g.smem(), s>>>(
-                                 d, raw, loc, inv, static_mask, clip, out, g.seg_bytes, g.rows));
+        FB_DISPATCH(d.dtype, {
+            set_smem(reinterpret_cast<const void*>(&k_moments_staged<D>), g.smem_deep());
+            k_moments_staged<D><<<grid, kStageChans, g.smem_deep(), s>>>(d, raw, loc, inv, static_mask, clip, out,
+                                                                        g.seg_bytes, g.rows);
+        });
     }
     FB_COUNT_LAUNCH();
 }
@@ -1709,9 +1867,10 @@ void launch_welford(const Dims& d, const float* work, const double* recip, float
     } else {
         const dim3 grid(grid1(d.nchans, kStageChans), static_cast<unsigned>(d.nwin));
         // a stage's reciprocals are loaded one per thread
-        const int rows = std::min(g.rows, kStageChans);
-        k_welford_staged<<<grid, kStageChans, 2 * static_cast<size_t>(g.seg_bytes) * rows, s>>>(
-            d, work, recip, loc, scale, g.seg_bytes, rows);
+        const int rows    = std::min(g.rows, kStageChans);
+        const size_t smem = kDeepStages * static_cast<size_t>(g.seg_bytes) * rows;
+        set_smem(reinterpret_cast<const void*>(&k_welford_staged), smem);
+        k_welford_staged<<<grid, kStageChans, smem, s>>>(d, work, recip, loc, scale, g.seg_bytes, rows);
     }
     FB_COUNT_LAUNCH();
 }

@@ -116,9 +116,10 @@ void launch_unpack(const Dims& d, const uint8_t* raw, float* work, cudaStream_t 
 
 // Per (window, channel) Welford mean/rms of work rows in that window.
 /** Per (window, channel) Welford mean / std of the cleaned float rows.
- * `recip[n]` = RN(1/n) for n up to the longest window lets the update
- * divide with one correction step instead of a full division (same bits);
- * null uses the plain division. */
+ * `recip[2n]`, `recip[2n + 1]` = RN(1/n), RN((1 - n RN(1/n)) / n) for n up
+ * to the longest window let the update divide with one multiply and one
+ * fused multiply-add instead of a full division (same bits); null uses the
+ * plain division. */
 void launch_welford(const Dims& d, const float* work, const double* recip, float* loc, float* scale,
                     cudaStream_t s);
 

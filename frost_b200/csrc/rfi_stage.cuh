@@ -6,8 +6,8 @@
 // a row stride between steps: few bytes in flight and latency-bound. Here
 // the block's threads instead copy whole row segments (the block's
 // channels, 16-byte cp.async copies, coalesced) a stage of rows at a time,
-// two stages deep, and then every thread walks its column in shared
-// memory.
+// two to eight stages deep, and then every thread walks its column in
+// shared memory.
 //
 // Requirements (the launchers check them and otherwise use the direct
 // kernels): the row pitch and the segment's byte offset are multiples of
@@ -46,13 +46,14 @@ __device__ __forceinline__ void stage_rows(uint8_t* dst, const uint8_t* src, uin
     commit();
 }
 
-/** Double-buffered staging of rows [b, e) of one column segment. Every
- * thread of the block calls start(), then for k = 0 .. nblk-1: wait(k),
- * reads rows_of(k) rows at buf(k) (row r is time t0(k) + r), release(k).
- * `smem` holds 2 * rows * seg_bytes bytes; `copy_bytes` (<= seg_bytes, a
- * multiple of 16) of each row are fetched (a row's last segment can be
- * short). */
-struct Stager {
+/** Staging of rows [b, e) of one column segment through S buffers (S - 1
+ * stages in flight while one is read). Every thread of the block calls
+ * start(), then for k = 0 .. nblk-1: wait(k), reads rows_of(k) rows at
+ * buf(k) (row r is time t0(k) + r), release(k). `smem` holds
+ * S * rows * seg_bytes bytes; `copy_bytes` (<= seg_bytes, a multiple of 16)
+ * of each row are fetched (a row's last segment can be short). */
+template <int S> struct StagerN {
+    static_assert(S >= 2 && S <= 8, "2 to 8 stages");
     uint8_t* smem;
     const uint8_t* src;
     uint64_t pitch;
@@ -60,8 +61,8 @@ struct Stager {
     uint64_t b, n;
     int nblk;
 
-    __device__ Stager(uint8_t* smem_, const uint8_t* src_, uint64_t pitch_, int seg_bytes_,
-                      int copy_bytes_, int rows_, uint64_t b_, uint64_t e_)
+    __device__ StagerN(uint8_t* smem_, const uint8_t* src_, uint64_t pitch_, int seg_bytes_,
+                       int copy_bytes_, int rows_, uint64_t b_, uint64_t e_)
         : smem(smem_), src(src_), pitch(pitch_), seg_bytes(seg_bytes_), copy_bytes(copy_bytes_),
           rows(rows_), b(b_), n(e_ > b_ ? e_ - b_ : 0) {
         nblk = static_cast<int>((n + rows - 1) / rows);
@@ -71,33 +72,45 @@ struct Stager {
         return static_cast<int>(left < static_cast<uint64_t>(rows) ? left : rows);
     }
     __device__ __forceinline__ uint64_t t0(int k) const { return b + static_cast<uint64_t>(k) * rows; }
+    __device__ __forceinline__ int slot(int k) const { return k % S; }
     __device__ __forceinline__ const uint8_t* buf(int k) const {
-        return smem + (k & 1) * rows * seg_bytes;
+        return smem + slot(k) * rows * seg_bytes;
     }
     __device__ __forceinline__ void issue(int k) {
-        stage_rows(smem + (k & 1) * rows * seg_bytes, src, pitch, t0(k), rows_of(k), seg_bytes,
-                   copy_bytes);
+        stage_rows(smem + slot(k) * rows * seg_bytes, src, pitch, t0(k), rows_of(k), seg_bytes, copy_bytes);
     }
     __device__ __forceinline__ void start() {
-        if (nblk > 0)
-            issue(0);
-        if (nblk > 1)
-            issue(1);
+        for (int k = 0; k < S && k < nblk; ++k)
+            issue(k);
     }
-    /** Waits for stage k's copies (this thread's, then the block's). */
+    /** Waits for stage k's copies (this thread's, then the block's): the
+     * groups committed after stage k's may stay pending. */
     __device__ __forceinline__ void wait(int k) {
-        if (k + 1 < nblk)
-            wait_pending<1>();
-        else
-            wait_pending<0>();
+        const int later = nblk - 1 - k; // stages issued after k (at most S - 1)
+        if (later >= S - 1) {
+            wait_pending<S - 1>();
+        } else {
+            switch (later) {
+            case 0: wait_pending<0>(); break;
+            case 1: wait_pending<1>(); break;
+            case 2: wait_pending<2>(); break;
+            case 3: wait_pending<3>(); break;
+            case 4: wait_pending<4>(); break;
+            case 5: wait_pending<5>(); break;
+            default: wait_pending<6>(); break;
+            }
+        }
         __syncthreads();
     }
-    /** Every thread is done with stage k's buffer: refill it with k + 2. */
+    /** Every thread is done with stage k's buffer: refill it with k + S. */
     __device__ __forceinline__ void release(int k) {
         __syncthreads();
-        if (k + 2 < nblk)
-            issue(k + 2);
+        if (k + S < nblk)
+            issue(k + S);
     }
 };
+
+/** The double-buffered form. */
+using Stager = StagerN<2>;
 
 } // namespace fb::rfi::stage

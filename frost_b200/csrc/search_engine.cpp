@@ -625,6 +625,7 @@ void Engine::batch_finish() {
     collect(m_stream);
     m_timing.total_launches += m_launches;
     m_timing.executes += 1;
+    m_timing.unfused_model_bytes += unfused_model_bytes(m_batch_nsamps);
     m_batch_wf     = nullptr;
     m_batch_nsamps = 0;
 }
@@ -655,6 +656,21 @@ Engine::~Engine() {
             cudaEventDestroy(m_order);
         cudaStreamDestroy(m_stream);
     }
+}
+
+uint64_t Engine::unfused_model_bytes(SizeType nsamps) const {
+    const uint64_t s = m_fp16 ? 2 : 4;
+    const uint64_t T = nsamps;
+    uint64_t b      = 0;
+    for (int l = 1; l <= m_plan.levels(); ++l) {
+        const uint64_t below = l == 1 ? static_cast<uint64_t>(m_plan.nchans())
+                                      : static_cast<uint64_t>(m_plan.level_rows(l - 1));
+        const uint64_t rows  = static_cast<uint64_t>(m_plan.level_rows(l));
+        b += (below + rows) * (T + static_cast<uint64_t>(m_plan.level_history(l))) * s;
+    }
+    for (const auto& p : m_plan.planes())
+        b += static_cast<uint64_t>(p.level_row.size()) * T * s;
+    return b;
 }
 
 void Engine::enable_timing(bool on) {
@@ -911,6 +927,7 @@ void Engine::execute(const float* waterfall, SizeType nsamps, bool on_device, co
     collect(s);
     m_timing.total_launches += m_launches;
     m_timing.executes += 1;
+    m_timing.unfused_model_bytes += unfused_model_bytes(nsamps);
     harvest();
 }
 

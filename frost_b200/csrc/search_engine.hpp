@@ -51,6 +51,9 @@ public:
      * (negative: the default; 0: give up at once); a drain after a give-up
      * always uses the default. */
     void set_wait_limit(long long tries);
+    /** Bytes of the unfused FDMT + search model for a gulp of `nsamps`
+     * samples (frost_search_timing.unfused_model_bytes). */
+    uint64_t unfused_model_bytes(SizeType nsamps) const;
 
     /** The engine as one member of a multi-beam batch (serve::Batch): the
      * gulp is taken on the engine's own stream (batch_begin: mask, noise

@@ -50,6 +50,33 @@ template <class S> __device__ __forceinline__ float ldf(const S* p);
 template <> __device__ __forceinline__ float ldf<float>(const float* p) { return *p; }
 template <> __device__ __forceinline__ float ldf<__half>(const __half* p) { return __half2float(*p); }
 
+// Three-operand max / min (one sm_100 instruction; the same values as two
+// fmaxf / fminf: no rounding, NaN operands ignored).
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// max over e of q[e] - q[e - S] (S = 1 or 2) for e = S .. P - 1, folded into
+// `m`, two differences per instruction.
+template <int P, int S>
+__device__ __forceinline__ float max_diffs(const float (&q)[P], float m) {
+#pragma unroll
+    for (int e = S; e < P; e += 2) {
+        if (e + 1 < P)
+            m = fmax3(m, q[e] - q[e - S], q[e + 1] - q[e + 1 - S]);
+        else
+            m = fmaxf(m, q[e] - q[e - S]);
+    }
+    return m;
+}
+
 __device__ void scan_inplace(float* a, int n) {
     __shared__ float warp_tot[kThreads / 32];
     const int per = (n + kThreads - 1) / kThreads;
@@ -200,60 +227,170 @@ __device__ void emit(const SearchParams& p, const SearchRow& row, const RunState
     p.cands[idx]    = c;
 }
 
-// Walks the set bits of one chunk's mask in time order (one lane). For the
-// across-widths mode `wi` < 0: the peak is the best S/N over widths.
-template <int CH>
-__device__ void walk_runs(const SearchParams& p, const RowConst& rc, const float* Q, int64_t c0,
-                          int32_t delay, const uint32_t* bits, int wi, RunState& run,
-                          const SearchRow& row, uint32_t* count) {
-    int64_t last = run.open ? c0 - 1 : -2; // tile column of the last set bit
-    for (int wd = 0; wd < (CH / 32); ++wd) {
-        uint32_t b = bits[wd];
-        while (b) {
-            const int bit     = __ffs(b) - 1;
-            b &= b - 1;
-            const int k       = wd * 32 + bit;
-            const int64_t col = c0 + k;
-            float best        = FB_NEG_INF;
-            int bw            = 0;
-            if (wi >= 0) {
-                best = snr_general(p, rc, Q, c0, k, wi, delay);
-                bw   = wi;
-            } else {
-                for (int w = 0; w < p.nwidths; ++w) {
-                    const float s = snr_general(p, rc, Q, c0, k, w, delay);
-                    if (s > best) {
-                        best = s;
-                        bw   = w;
-                    }
-                }
-            }
-            const int64_t t = rc.tile_t0 + col;
-            if (run.open && col == last + 1) {
-                if (best > run.best) {
-                    run.best   = best;
-                    run.best_t = t;
-                    run.best_w = bw;
-                }
-                run.last_t = t;
-            } else {
-                if (run.open)
-                    emit(p, row, run, count);
-                run.open   = 1;
-                run.start  = t;
-                run.best   = best;
-                run.best_t = t;
-                run.best_w = bw;
-                run.last_t = t;
-            }
-            last = col;
+// A maximal run of set bits inside one lane's share of a chunk's mask: its
+// first and last chunk sample and its first maximum.
+struct Seg {
+    int32_t first_k, last_k, best_k, best_w;
+    float best;
+};
+
+// S/N of set bit k for width wi, or the best over widths (first maximum)
+// for wi < 0.
+__device__ __forceinline__ float bit_snr(const SearchParams& p, const RowConst& rc, const float* Q, int64_t c0,
+                                         int k, int wi, int32_t delay, int& bw) {
+    if (wi >= 0) {
+        bw = wi;
+        return snr_general(p, rc, Q, c0, k, wi, delay);
+    }
+    float best = FB_NEG_INF;
+    bw         = 0;
+    for (int w = 0; w < p.nwidths; ++w) {
+        const float s = snr_general(p, rc, Q, c0, k, w, delay);
+        if (s > best) {
+            best = s;
+            bw   = w;
         }
     }
-    // A run that does not reach the chunk's last valid column has closed.
-    const int64_t chunk_end = min(c0 + CH, static_cast<int64_t>(p.n_valid));
-    if (run.open && last != chunk_end - 1) {
-        emit(p, row, run, count);
-        run.open = 0;
+    return best;
+}
+
+__device__ __forceinline__ RunState run_of(const RowConst& rc, int64_t c0, const Seg& g) {
+    RunState r{};
+    r.open   = 1;
+    r.start  = rc.tile_t0 + c0 + g.first_k;
+    r.best   = g.best;
+    r.best_t = rc.tile_t0 + c0 + g.best_k;
+    r.best_w = g.best_w;
+    r.last_t = rc.tile_t0 + c0 + g.last_k;
+    return r;
+}
+
+__device__ __forceinline__ Seg shfl_seg(const Seg& g, int src) {
+    Seg r;
+    r.first_k = __shfl_sync(0xFFFFFFFFU, g.first_k, src);
+    r.last_k  = __shfl_sync(0xFFFFFFFFU, g.last_k, src);
+    r.best_k  = __shfl_sync(0xFFFFFFFFU, g.best_k, src);
+    r.best_w  = __shfl_sync(0xFFFFFFFFU, g.best_w, src);
+    r.best    = __shfl_sync(0xFFFFFFFFU, g.best, src);
+    return r;
+}
+
+// The runs of one chunk's mask for one width (or across widths, wi < 0), by
+// a whole warp: lane L takes the chunk's samples [L CH / 32, (L + 1) CH / 32)
+// (cut at the last valid sample) and finds its maximal runs in time order
+// (S/N of each set bit, first maximum); runs that touch neither end of the
+// lane's share are complete and emitted at once. Lane 0 then joins, in time order, the runs that do
+// touch a share's end with each other and with the run carried from the
+// previous chunk, exactly as a sequential walk over the bits would (the
+// strict comparison keeps the earliest maximum), emits the closed ones and
+// leaves `run` open when it reaches the chunk's last valid sample.
+template <int CH>
+__device__ __noinline__ void walk_runs_warp(const SearchParams& p, const RowConst& rc, const float* Q, int64_t c0,
+                               int32_t delay, const uint32_t* bits, int wi, RunState& run,
+                               const SearchRow& row, uint32_t* count) {
+    constexpr int kPerLane = CH / 32 / 32; // mask words per lane
+    const int lane = threadIdx.x & 31;
+    // the lane's share ends at its last sample or at the chunk's last valid one
+    const int64_t valid = static_cast<int64_t>(p.n_valid) - c0;
+    const int kbeg = lane * kPerLane * 32;
+    const int kend = static_cast<int>(min(static_cast<int64_t>(kbeg + kPerLane * 32), valid));
+    Seg left{}, right{}, cur{};
+    bool has_left = false, has_right = false, whole = false, open = false;
+    int prev = -2;
+    auto finish = [&](const Seg& g) {
+        if (g.first_k == kbeg) {
+            left     = g;
+            has_left = true;
+        } else {
+            emit(p, row, run_of(rc, c0, g), count);
+        }
+    };
+#pragma unroll
+    for (int wd = 0; wd < kPerLane; ++wd) {
+        uint32_t b = bits[lane * kPerLane + wd];
+        while (b) {
+            const int k = (lane * kPerLane + wd) * 32 + __ffs(b) - 1;
+            b &= b - 1;
+            int bw;
+            const float sn = bit_snr(p, rc, Q, c0, k, wi, delay, bw);
+            if (open && k == prev + 1) {
+                if (sn > cur.best) {
+                    cur.best   = sn;
+                    cur.best_k = k;
+                    cur.best_w = bw;
+                }
+                cur.last_k = k;
+            } else {
+                if (open)
+                    finish(cur);
+                cur  = Seg{k, k, k, bw, sn};
+                open = true;
+            }
+            prev = k;
+        }
+    }
+    if (open) {
+        if (cur.last_k == kend - 1) {
+            has_right = true;
+            right     = cur;
+            if (cur.first_k == kbeg) {
+                whole    = true;
+                left     = cur;
+                has_left = true;
+            }
+        } else {
+            finish(cur);
+        }
+    }
+    // lane 0 joins the share-end runs in time order
+    uint32_t ev = __ballot_sync(0xFFFFFFFFU, has_left || has_right);
+    RunState r    = run;
+    int64_t last  = r.open ? c0 - 1 : -2; // tile column of the run's last sample
+    while (ev) {
+        const int L = __ffs(static_cast<int>(ev)) - 1;
+        ev &= ev - 1;
+        const bool hl = __shfl_sync(0xFFFFFFFFU, has_left, L);
+        const bool hr = __shfl_sync(0xFFFFFFFFU, has_right, L);
+        const bool wh = __shfl_sync(0xFFFFFFFFU, whole, L);
+        const Seg gl  = shfl_seg(left, L);
+        const Seg gr  = shfl_seg(right, L);
+        if (lane != 0)
+            continue;
+        const int64_t lstart = c0 + L * kPerLane * 32;
+        if (hl) {
+            if (r.open && last == lstart - 1) {
+                if (gl.best > r.best) {
+                    r.best   = gl.best;
+                    r.best_t = rc.tile_t0 + c0 + gl.best_k;
+                    r.best_w = gl.best_w;
+                }
+                r.last_t = rc.tile_t0 + c0 + gl.last_k;
+            } else {
+                if (r.open)
+                    emit(p, row, r, count);
+                r = run_of(rc, c0, gl);
+            }
+            last = c0 + gl.last_k;
+            if (!wh) {
+                emit(p, row, r, count);
+                r.open = 0;
+            }
+        }
+        if (hr && !wh) {
+            if (r.open)
+                emit(p, row, r, count);
+            r    = run_of(rc, c0, gr);
+            last = c0 + gr.last_k;
+        }
+    }
+    if (lane == 0) {
+        // a run that does not reach the chunk's last valid column has closed
+        const int64_t chunk_end = min(c0 + CH, static_cast<int64_t>(p.n_valid));
+        if (r.open && last != chunk_end - 1) {
+            emit(p, row, r, count);
+            r.open = 0;
+        }
+        run = r;
     }
 }
 
@@ -371,11 +508,8 @@ __device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float
                                            float& m1) {
     constexpr int W = 1 << WI;
     if constexpr (W == 1) {
-        float m = q[0] - pm1;
-#pragma unroll
-        for (int e = 1; e < P; ++e)
-            m = fmaxf(m, q[e] - q[e - 1]);
-        m1 = m; // the largest width-1 sum of the thread's samples
+        const float m = max_diffs<P, 1>(q, q[0] - pm1);
+        m1             = m; // the largest width-1 sum of the thread's samples
         return m > T;
     } else if constexpr (W == 2) {
         // Every width-2 window sum is, before rounding, the sum of two of the
@@ -388,10 +522,7 @@ __device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float
         const float d = fmaxf(m1, pm1 - pm2);
         if (T > 0.0F && 2.0F * d * (1.0F + 0x1p-20F) <= T)
             return false;
-        float m = fmaxf(q[0] - pm2, q[1] - pm1);
-#pragma unroll
-        for (int e = 2; e < P; ++e)
-            m = fmaxf(m, q[e] - q[e - 2]);
+        const float m = max_diffs<P, 2>(q, fmaxf(q[0] - pm2, q[1] - pm1));
         return m > T;
     } else {
         if constexpr (W >= 4 * P) {
@@ -417,10 +548,11 @@ __device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float
             const float e[4] = {a.x, a.y, b.x, b.y};
             pick_lows<R, 2, 4>(e, false, lo);
         }
-        float m = gmx[0] - lo[0];
-#pragma unroll
-        for (int g = 1; g < NG; ++g)
-            m = fmaxf(m, gmx[g] - lo[g]);
+        float m;
+        if constexpr (NG == 4)
+            m = fmaxf(fmax3(gmx[0] - lo[0], gmx[1] - lo[1], gmx[2] - lo[2]), gmx[3] - lo[3]);
+        else
+            m = fmaxf(gmx[0] - lo[0], gmx[1] - lo[1]);
         return m > T;
     }
 }
@@ -636,14 +768,16 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             float gmx[NG], gmn[NG];
 #pragma unroll
             for (int gq = 0; gq < NG; ++gq) {
-                gmx[gq] = fmaxf(fmaxf(q[4 * gq], q[4 * gq + 1]), fmaxf(q[4 * gq + 2], q[4 * gq + 3]));
-                gmn[gq] = fminf(fminf(q[4 * gq], q[4 * gq + 1]), fminf(q[4 * gq + 2], q[4 * gq + 3]));
+                gmx[gq] = fmaxf(fmax3(q[4 * gq], q[4 * gq + 1], q[4 * gq + 2]), q[4 * gq + 3]);
+                gmn[gq] = fminf(fmin3(q[4 * gq], q[4 * gq + 1], q[4 * gq + 2]), q[4 * gq + 3]);
             }
-            float bmax = gmx[0], bmin = gmn[0];
-#pragma unroll
-            for (int gq = 1; gq < NG; ++gq) {
-                bmax = fmaxf(bmax, gmx[gq]);
-                bmin = fminf(bmin, gmn[gq]);
+            float bmax, bmin;
+            if constexpr (NG == 4) {
+                bmax = fmaxf(fmax3(gmx[0], gmx[1], gmx[2]), gmx[3]);
+                bmin = fminf(fmin3(gmn[0], gmn[1], gmn[2]), gmn[3]);
+            } else {
+                bmax = fmaxf(gmx[0], gmx[1]);
+                bmin = fminf(gmn[0], gmn[1]);
             }
             if constexpr (NG == 4)
                 reinterpret_cast<float4*>(gmin + halo / 4)[threadIdx.x] = make_float4(gmn[0], gmn[1], gmn[2], gmn[3]);
@@ -846,15 +980,16 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                 }
                 __syncthreads();
             }
-            // Widths are independent (each has its own run state): lane 0 of
-            // warp w walks widths w, w + 8, ... Candidates of different widths
-            // may therefore reach the output in any order (results are sorted
-            // afterwards; only which ones a per-DM cap drops can vary).
-            if (all && lane == 0) {
+            // Widths are independent (each has its own run state): warp w
+            // walks widths w, w + 8, ..., its lanes over the chunk's samples.
+            // Candidates may therefore reach the output in any order (results
+            // are sorted afterwards; only which ones a per-DM cap drops can
+            // vary).
+            if (all) {
                 for (int wi = warp; wi < nw; wi += kThreads / 32) {
                     if (((fw >> wi) & 1U) == 0U)
                         continue;
-                    for (int wd = 0; wd < (CH / 32); ++wd) {
+                    for (int wd = lane; wd < (CH / 32); wd += 32) {
                         uint32_t m = bits[wi * (CH / 32) + wd];
                         while (m) {
                             const int k = wd * 32 + __ffs(m) - 1;
@@ -867,14 +1002,14 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                         }
                     }
                 }
-            } else if (!all && !across && lane == 0) {
+            } else if (!across) {
                 for (int wi = warp; wi < nw; wi += kThreads / 32)
                     if (((fw >> wi) & 1U) != 0U || runs[wi].open)
-                        walk_runs<CH>(p, rc, Q, c0, row.delay, bits + wi * (CH / 32), wi, runs[wi], row,
-                                  &local_count);
+                        walk_runs_warp<CH>(p, rc, Q, c0, row.delay, bits + wi * (CH / 32), wi, runs[wi], row,
+                                           &local_count);
             }
-            if (across && threadIdx.x == 0 && (fw != 0U || runs[0].open))
-                walk_runs<CH>(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
+            if (across && warp == 0 && (fw != 0U || runs[0].open))
+                walk_runs_warp<CH>(p, rc, Q, c0, row.delay, any_bits, -1, runs[0], row, &local_count);
             __syncthreads();
         }
         if (abort_flag) {

@@ -477,7 +477,12 @@ int frost_search_plane_data(const frost_search* s,
  * (CUDA events on the engine's stream), the stage profile frost keeps in
  * RunProfile (include/frost/pipeline/profile.hpp:27-61) at kernel level.
  * `algorithmic_level_bytes` counts one read of every input row and one write
- * of every output row of the FDMT levels >= 2 (the HBM roofline's traffic). */
+ * of every output row of the FDMT levels >= 2 (the HBM roofline's traffic).
+ * `unfused_model_bytes` is the schedule-independent figure of the FDMT and
+ * search per gulp of T samples: every level l = 1..L read and written once
+ * with its history, sum_l (R_{l-1} + R_l) (T + H_l) s, plus one read of every
+ * searched plane row, sum_p R_p T s (R_0 = channels, s = the plane element
+ * size); fusing levels moves fewer bytes than it counts. */
 typedef struct {
     double level1_ms;
     double level_ms;
@@ -491,6 +496,7 @@ typedef struct {
     uint64_t algorithmic_level1_bytes;
     uint64_t algorithmic_search_bytes;
     uint64_t executes;
+    uint64_t unfused_model_bytes;
 } frost_search_timing;
 
 /* No counterpart in the reference (dmt launches per call). With `enable`

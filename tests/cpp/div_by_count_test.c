@@ -1,7 +1,10 @@
 // Correctly rounded a / n (n a positive integer count) from a precomputed
-// y = RN(1/n) with one fused multiply-add correction, the division the
-// Welford kernel uses (frost_b200/csrc/rfi_kernels.cu: div_by_count),
-// checked bit for bit against IEEE division on random operands.
+// two-term reciprocal y_hi = RN(1/n), y_lo = RN((1 - n y_hi) / n):
+// q = RN(a y_hi + RN(a y_lo)), the division the Welford kernel uses
+// (frost_b200/csrc/rfi_kernels.cu: WelfordAcc::step_recip), checked bit for
+// bit against IEEE division on random operands. A zero numerator may give
+// a zero of the other sign; the kernel adds q to a mean that is never -0,
+// so only the value of a zero quotient matters there.
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -15,20 +18,17 @@ static uint64_t next(void) {
     return state;
 }
 
-static double div_by_count(double a, double n, double y) {
-    if (a == 0.0)
-        return a;
-    if (!(fabs(a) > 0x1p-900))
-        return a / n;
-    const double q0 = a * y;
-    const double r  = fma(-q0, n, a);
-    return fma(r, y, q0);
+static double div_by_count(double a, double n, double yh, double yl) {
+    double q = fma(a, yh, a * yl);
+    if (!(fabs(a) > 0x1p-900) && a != 0.0)
+        q = a / n;
+    return q;
 }
 
 int main(void) {
     long bad = 0, tested = 0;
     for (long i = 0; i < 30000000L; ++i) {
-        const uint64_t n = 1 + next() % 262144;
+        const uint64_t n = 1 + ((i % 11 == 0) ? next() % 4294967296ULL : next() % 262144);
         double a;
         if (i % 3 == 0) {
             a = ((double)(int64_t)next() / 9.2e18) * 100.0; // typical deviations
@@ -42,10 +42,13 @@ int main(void) {
             if (i % 7 == 0)
                 a = (i % 2) ? 0.0 : -0.0;
         }
-        const double y = 1.0 / (double)n;
-        const double q = div_by_count(a, (double)n, y), t = a / (double)n;
+        const double dn = (double)n;
+        const double yh = 1.0 / dn;
+        const double yl = fma(-dn, yh, 1.0) / dn;
+        const double q = div_by_count(a, dn, yh, yl), t = a / dn;
         ++tested;
-        if (memcmp(&q, &t, sizeof q) != 0) {
+        const int same = (a == 0.0) ? (q == 0.0) : (memcmp(&q, &t, sizeof q) == 0);
+        if (!same) {
             if (bad < 10)
                 printf("a=%a n=%lu got %a want %a\n", a, (unsigned long)n, q, t);
             ++bad;

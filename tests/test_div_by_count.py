@@ -1,7 +1,8 @@
-"""The correction-step division of the Welford kernel (div_by_count in
-frost_b200/csrc/rfi_kernels.cu) restated in C and compared bit for bit with
-IEEE double division on 30 M random operands and window counts up to
-262 144; the GPU RFI parity tests check the kernel itself."""
+"""The two-term-reciprocal division of the Welford kernel
+(WelfordAcc::step_recip in frost_b200/csrc/rfi_kernels.cu) restated in C and
+compared bit for bit with IEEE double division on 30 M random operands and
+counts up to 262 144 (and up to 2^32 for one operand in eleven); the GPU RFI
+parity tests check the kernel itself."""
 
 import os
 import subprocess
