@@ -7,8 +7,11 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 #include <cuda_runtime_api.h>
 
@@ -46,6 +49,28 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
 }
 
 #define FB_CUDA(call) ::fb::cuda_check((call), #call, __FILE__, __LINE__)
+
+/** Lets kernel `fn` launch with up to the device's opt-in shared memory per
+ * block. The attribute is process-wide state of the function: setting it to
+ * each launch's own size would race between host threads launching the
+ * same kernel with different sizes (served beams, batched cleaners), so it
+ * is set once, to the largest value, per function and device. */
+inline void allow_large_smem(const void* fn) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count({fn, dev}) != 0)
+        return;
+    cudaFuncAttributes a{};
+    FB_CUDA(cudaFuncGetAttributes(&a, fn));
+    int optin = 0;
+    FB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    FB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 optin - static_cast<int>(a.sharedSizeBytes)));
+    done.insert({fn, dev});
+}
 #define FB_LAUNCH_CHECK() ::fb::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
 
 void set_last_error(const std::string& msg);

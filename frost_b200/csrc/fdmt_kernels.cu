@@ -699,14 +699,12 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
     if (smem > 200 * 1024)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "level1: leaf windows too long for shared memory");
     if (out.fp16) {
-        FB_CUDA(cudaFuncSetAttribute(k_level1<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+        allow_large_smem(reinterpret_cast<const void*>(&k_level1<__half>));
         k_level1<__half><<<grid, kThreads, smem, s>>>(
             ops, node_first_op, nnodes, ntiles, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
             input_hist, hist_len, static_cast<__half*>(out.data), out.pitch, out.base);
     } else {
-        FB_CUDA(cudaFuncSetAttribute(k_level1<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+        allow_large_smem(reinterpret_cast<const void*>(&k_level1<float>));
         k_level1<float><<<grid, kThreads, smem, s>>>(
             ops, node_first_op, nnodes, ntiles, max_node_delay, waterfall, waterfall_pitch, t0, n_valid,
             input_hist, hist_len, static_cast<float*>(out.data), out.pitch, out.base);
@@ -765,8 +763,7 @@ LevelSegTable<K> seg_table(LevelSeg* segs, int n, int64_t* total) {
 template <class S, int NS, int K>
 void level2_go(const LevelSegTable<K>& t, int64_t total, cudaStream_t s, int32_t ctas, long long wait_limit) {
     const size_t smem = NS * (4 * kTimePerCta * sizeof(S) + 48);
-    FB_CUDA(cudaFuncSetAttribute(k_level2_pipe<S, NS, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
+    allow_large_smem(reinterpret_cast<const void*>(&k_level2_pipe<S, NS, K>));
     k_level2_pipe<S, NS, K><<<grid_for(total, ctas), kThreads, smem, s>>>(t, wait_limit);
 }
 
@@ -775,8 +772,7 @@ void level_go(const LevelSegTable<K>& t, int64_t total, bool fused, int32_t stag
               long long wait_limit) {
     if (!fused) {
         const size_t smem = kStages * (2 * kTimePerCta * sizeof(S) + 16);
-        FB_CUDA(cudaFuncSetAttribute(k_level_pipe<S, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+        allow_large_smem(reinterpret_cast<const void*>(&k_level_pipe<S, K>));
         k_level_pipe<S, K><<<grid_for(total, ctas), kThreads, smem, s>>>(t, wait_limit);
         return;
     }

@@ -1130,8 +1130,7 @@ void launch_seeded(const frost_giant* rows, const u32* tord, const u32* sord, co
     const size_t smem           = bitmap_words * sizeof(u32);
     if (smem <= kSmemLimit) {
         if (smem > 48 * 1024)
-            FB_CUDA(cudaFuncSetAttribute(k_seeded<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem)));
+            allow_large_smem(reinterpret_cast<const void*>(&k_seeded<true>));
         k_seeded<true><<<nseg, kThreads, smem, s>>>(rows, tord, sord, rank_of, lo, hi, tol, label, nullptr,
                                                     bitmap_words);
     } else {

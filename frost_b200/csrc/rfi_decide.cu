@@ -950,8 +950,7 @@ void launch_sorts(const SortJobs& j, const ChannelScratch& w, const float* x, co
         return;
     const size_t smem = j.use_smem ? j.P * sizeof(double) : 0;
     if (smem > 48 * 1024)
-        FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(&k_channel_sorts),
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_large_smem(reinterpret_cast<const void*>(&k_channel_sorts));
     k_channel_sorts<<<static_cast<unsigned>(jobs), kBlock, smem, s>>>(j, w, x, ign);
     FB_DECIDE_LAUNCH();
 }

@@ -669,7 +669,7 @@ constexpr int kScanChans = 64;  // channel tile staged in shared memory
 struct ScanRowAcc {
     double sum_det = 0.0, sum_keep = 0.0, sx = 0.0, sxx = 0.0;
     uint32_t n_keep = 0, n_meas = 0; // counts (exact as doubles when used)
-    KadaneState sp = KadaneState::make(), sn = KadaneState::make();
+    KadaneBest sp, sn; // rows are scanned whole: only the best runs are needed
     __device__ __forceinline__ void step(uint64_t c, float x, float l, float ic, float clip, int kspec) {
         ++n_meas;
         const float zc = (x - l) * ic;
@@ -682,8 +682,8 @@ struct ScanRowAcc {
         sx += x;
         sxx += static_cast<double>(x) * x;
         if (kspec) {
-            sp.append(static_cast<int64_t>(c), cl);
-            sn.append(static_cast<int64_t>(c), -cl);
+            sp.append(static_cast<int32_t>(c), cl);
+            sn.append(static_cast<int32_t>(c), -cl);
         }
     }
     __device__ void finish(const Dims& d, uint64_t t, const KspecParams& kp,
@@ -717,8 +717,8 @@ struct ScanRowAcc {
                 return false;
             };
             Span32 a, b;
-            bool whole     = accept(sp.best, a);
-            whole          = accept(sn.best, b) || whole;
+            bool whole     = accept(sp.best(), a);
+            whole          = accept(sn.best(), b) || whole;
             kspec_pos[t]   = a;
             kspec_neg[t]   = b;
             kspec_whole[t] = whole ? 1 : 0;
@@ -867,7 +867,7 @@ struct ScanColAcc {
     float l = 0.0F, iv = 0.0F, cm = 0.0F, ci = 0.0F;
     float cmin = FLT_MAX, cmax = -FLT_MAX;
     ZdotSums zs{0, 0, 0, 0, 0};
-    KadaneState kpos = KadaneState::make(), kneg = KadaneState::make();
+    KadaneState32 kpos, kneg; // widened when stored
     __device__ __forceinline__ void step(float x, uint64_t t) {
         if (t >= wend) {
             w                = window_of(t, d->window, d->nwin);
@@ -898,8 +898,8 @@ struct ScanColAcc {
         }
         if (kchan) {
             const double u = outlier ? 0.0 : static_cast<double>((z - cm) * ci);
-            kpos.append(static_cast<int64_t>(t), u);
-            kneg.append(static_cast<int64_t>(t), -u);
+            kpos.append(static_cast<int32_t>(t), u);
+            kneg.append(static_cast<int32_t>(t), -u);
         }
     }
     __device__ __forceinline__ void store(uint64_t k, float* cmin_out, float* cmax_out,
@@ -911,8 +911,8 @@ struct ScanColAcc {
         if (zdot)
             zs_out[o] = zs;
         if (kchan) {
-            kp_out[o] = kpos;
-            kn_out[o] = kneg;
+            kp_out[o] = kpos.widen();
+            kn_out[o] = kneg.widen();
         }
     }
 };
@@ -1037,10 +1037,14 @@ __device__ __forceinline__ float level_of(const ApplyParams& p, float loc, float
     return p.equalize ? p.eq_loc + (p.eq_scale * v) : loc + (scale * v);
 }
 
-// Unflagged rows (lib/cpu/rfi_cpu.cpp:537-624): one CTA per row; the row's
-// samples and cell states are staged in shared memory so neighbour draws
-// read them without touching HBM again. Masked cells are not written: the
-// normalized output zeroes them, so their fill values are never observed.
+// Unflagged rows (lib/cpu/rfi_cpu.cpp:537-624): each CTA takes kApplyRows
+// consecutive rows in turn (their per-window constants then come from L1);
+// a row's samples and cell states are staged in shared memory so neighbour
+// draws read them without touching HBM again. Masked cells are not written:
+// the normalized output zeroes them, so their fill values are never
+// observed.
+constexpr int kApplyRows = 8;
+
 template <int D, int V>
 __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restrict__ raw,
                                   const float* __restrict__ loc, const float* __restrict__ scale,
@@ -1062,142 +1066,145 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
     __shared__ unsigned long long cnt[kCountSlots];
     if (threadIdx.x < kCountSlots)
         cnt[threadIdx.x] = 0;
+    unsigned long long narrow = 0, nks = 0, nkc = 0, fallbacks = 0;
+    const uint64_t t_end = min(static_cast<uint64_t>(blockIdx.x + 1) * kApplyRows, d.nsamps);
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * kApplyRows; t < t_end; ++t) {
+        if (time_flags[t] != 0)
+            continue;
+        const uint64_t w  = window_of(t, d.window, d.nwin);
+        const float* lw   = loc + w * n;
+        const float* sw   = scale + w * n;
+        const float* iw   = inv + w * n;
+        const uint8_t* in = raw + t * d.row_bytes;
+        float* out        = work + t * n;
+        const float sk    = s_keep_f[t];
+        const Span32 ksp  = p.kspec ? kspec_pos[t] : Span32{-1, -1};
+        const Span32 ksn  = p.kspec ? kspec_neg[t] : Span32{-1, -1};
+        auto span_has     = [](const Span32& s, uint64_t c) {
+            return s.lo >= 0 && static_cast<int32_t>(c) >= s.lo && static_cast<int32_t>(c) <= s.hi;
+        };
+        auto seg_has = [](const Segment& s, uint64_t tt) {
+            const int64_t i = static_cast<int64_t>(tt);
+            return i >= s.start && i <= s.end;
+        };
 
-    const uint64_t t = blockIdx.x;
-    if (time_flags[t] != 0)
-        return;
-    const uint64_t w  = window_of(t, d.window, d.nwin);
-    const float* lw   = loc + w * n;
-    const float* sw   = scale + w * n;
-    const float* iw   = inv + w * n;
-    const uint8_t* in = raw + t * d.row_bytes;
-    float* out        = work + t * n;
-    const float sk    = s_keep_f[t];
-    const Span32 ksp  = p.kspec ? kspec_pos[t] : Span32{-1, -1};
-    const Span32 ksn  = p.kspec ? kspec_neg[t] : Span32{-1, -1};
-    auto span_has     = [](const Span32& s, uint64_t c) {
-        return s.lo >= 0 && static_cast<int32_t>(c) >= s.lo && static_cast<int32_t>(c) <= s.hi;
-    };
-    auto seg_has = [](const Segment& s, uint64_t tt) {
-        const int64_t i = static_cast<int64_t>(tt);
-        return i >= s.start && i <= s.end;
-    };
-
-    // V consecutive channels per thread (V = 4: 16-byte loads of the
-    // per-window constants and stores of the row, when nchans % 4 == 0);
-    // channel indices fit 32 bits (the launcher checks)
-    const uint32_t n32 = static_cast<uint32_t>(n);
-    bool dirty         = false; // a cell of this thread's needs a fill
-    for (uint32_t cb = threadIdx.x * V; cb < n32; cb += blockDim.x * V) {
-        float xs[V], ls[V], ss[V], is[V], outv[V];
-        uint8_t ms[V], ka[V];
-        if constexpr (V == 4) {
-            const float4 l4 = *reinterpret_cast<const float4*>(lw + cb);
-            const float4 s4 = *reinterpret_cast<const float4*>(sw + cb);
-            const float4 i4 = *reinterpret_cast<const float4*>(iw + cb);
-            const uchar4 m4 = *reinterpret_cast<const uchar4*>(mask + cb);
-            ls[0] = l4.x; ls[1] = l4.y; ls[2] = l4.z; ls[3] = l4.w;
-            ss[0] = s4.x; ss[1] = s4.y; ss[2] = s4.z; ss[3] = s4.w;
-            is[0] = i4.x; is[1] = i4.y; is[2] = i4.z; is[3] = i4.w;
-            ms[0] = m4.x; ms[1] = m4.y; ms[2] = m4.z; ms[3] = m4.w;
-            if (p.kchan) {
-                const uchar4 k4 = *reinterpret_cast<const uchar4*>(kchan_any + cb);
-                ka[0] = k4.x; ka[1] = k4.y; ka[2] = k4.z; ka[3] = k4.w;
-            } else {
-                ka[0] = ka[1] = ka[2] = ka[3] = 0;
-            }
-            if constexpr (D == FROST_UINT8) {
-                const uchar4 x4 = *reinterpret_cast<const uchar4*>(in + cb);
-                xs[0] = static_cast<float>(x4.x); xs[1] = static_cast<float>(x4.y);
-                xs[2] = static_cast<float>(x4.z); xs[3] = static_cast<float>(x4.w);
-            } else {
-#pragma unroll
-                for (int e = 0; e < V; ++e)
-                    xs[e] = rd<D>(in, cb + e);
-            }
-        } else {
-            ls[0] = lw[cb];
-            ss[0] = sw[cb];
-            is[0] = iw[cb];
-            ms[0] = mask[cb];
-            ka[0] = p.kchan ? kchan_any[cb] : 0;
-            xs[0] = rd<D>(in, cb);
-        }
-#pragma unroll
-        for (int e = 0; e < V; ++e) {
-            const uint32_t c = cb + e;
-            const float x    = xs[e];
-            uint8_t st;
-            float v = 0.0F;
-            outv[e] = 0.0F;
-            if (ms[e] == 0) {
-                st = kMasked;
-            } else if (is[e] == 0.0F) {
-                st      = kUnmeasured;
-                outv[e] = x;
-            } else {
-                const float z = (x - ls[e]) * is[e];
-                if (p.narrow_active && fabsf(z) > p.clip) {
-                    st = kNarrow;
-                } else if (p.kspec && (span_has(ksp, c) || span_has(ksn, c))) {
-                    st = kKadaneSpectrum;
-                } else if (ka[e] != 0 && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
-                    st = kKadaneChannel;
+        // V consecutive channels per thread (V = 4: 16-byte loads of the
+        // per-window constants and stores of the row, when nchans % 4 == 0);
+        // channel indices fit 32 bits (the launcher checks)
+        const uint32_t n32 = static_cast<uint32_t>(n);
+        bool dirty         = false; // a cell of this thread's needs a fill
+        for (uint32_t cb = threadIdx.x * V; cb < n32; cb += blockDim.x * V) {
+            float xs[V], ls[V], ss[V], is[V], outv[V];
+            uint8_t ms[V], ka[V];
+            if constexpr (V == 4) {
+                const float4 l4 = *reinterpret_cast<const float4*>(lw + cb);
+                const float4 s4 = *reinterpret_cast<const float4*>(sw + cb);
+                const float4 i4 = *reinterpret_cast<const float4*>(iw + cb);
+                const uchar4 m4 = *reinterpret_cast<const uchar4*>(mask + cb);
+                ls[0] = l4.x; ls[1] = l4.y; ls[2] = l4.z; ls[3] = l4.w;
+                ss[0] = s4.x; ss[1] = s4.y; ss[2] = s4.z; ss[3] = s4.w;
+                is[0] = i4.x; is[1] = i4.y; is[2] = i4.z; is[3] = i4.w;
+                ms[0] = m4.x; ms[1] = m4.y; ms[2] = m4.z; ms[3] = m4.w;
+                if (p.kchan) {
+                    const uchar4 k4 = *reinterpret_cast<const uchar4*>(kchan_any + cb);
+                    ka[0] = k4.x; ka[1] = k4.y; ka[2] = k4.z; ka[3] = k4.w;
                 } else {
-                    st = kClean;
-                    float term = 0.0F;
-                    if (p.zero_dm == FROST_ZERO_DM_SUBTRACT)
-                        term = sk;
-                    else if (p.zero_dm == FROST_ZERO_DM_ZDOT)
-                        term = (zdot_a[c] * sk) + zdot_b[c];
-                    v       = z - term;
-                    outv[e] = p.transform ? level_of(p, ls[e], ss[e], v) : x;
+                    ka[0] = ka[1] = ka[2] = ka[3] = 0;
+                }
+                if constexpr (D == FROST_UINT8) {
+                    const uchar4 x4 = *reinterpret_cast<const uchar4*>(in + cb);
+                    xs[0] = static_cast<float>(x4.x); xs[1] = static_cast<float>(x4.y);
+                    xs[2] = static_cast<float>(x4.z); xs[3] = static_cast<float>(x4.w);
+                } else {
+    #pragma unroll
+                    for (int e = 0; e < V; ++e)
+                        xs[e] = rd<D>(in, cb + e);
+                }
+            } else {
+                ls[0] = lw[cb];
+                ss[0] = sw[cb];
+                is[0] = iw[cb];
+                ms[0] = mask[cb];
+                ka[0] = p.kchan ? kchan_any[cb] : 0;
+                xs[0] = rd<D>(in, cb);
+            }
+    #pragma unroll
+            for (int e = 0; e < V; ++e) {
+                const uint32_t c = cb + e;
+                const float x    = xs[e];
+                uint8_t st;
+                float v = 0.0F;
+                outv[e] = 0.0F;
+                if (ms[e] == 0) {
+                    st = kMasked;
+                } else if (is[e] == 0.0F) {
+                    st      = kUnmeasured;
+                    outv[e] = x;
+                } else {
+                    const float z = (x - ls[e]) * is[e];
+                    if (p.narrow_active && fabsf(z) > p.clip) {
+                        st = kNarrow;
+                    } else if (p.kspec && (span_has(ksp, c) || span_has(ksn, c))) {
+                        st = kKadaneSpectrum;
+                    } else if (ka[e] != 0 && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
+                        st = kKadaneChannel;
+                    } else {
+                        st = kClean;
+                        float term = 0.0F;
+                        if (p.zero_dm == FROST_ZERO_DM_SUBTRACT)
+                            term = sk;
+                        else if (p.zero_dm == FROST_ZERO_DM_ZDOT)
+                            term = (zdot_a[c] * sk) + zdot_b[c];
+                        v       = z - term;
+                        outv[e] = p.transform ? level_of(p, ls[e], ss[e], v) : x;
+                    }
+                }
+                state[c] = st;
+                sv[c]    = v;
+                dirty    = dirty || st == kNarrow || st == kKadaneSpectrum || st == kKadaneChannel;
+            }
+            // masked and flagged cells are (re)written below or never read
+            if constexpr (V == 4)
+                *reinterpret_cast<float4*>(out + cb) = make_float4(outv[0], outv[1], outv[2], outv[3]);
+            else
+                out[cb] = outv[0];
+        }
+        // a row with no cell to fill (almost every row) is done; the barrier
+        // also orders this row's shared-memory writes after the last row's reads
+        if (!__syncthreads_or(dirty))
+            continue;
+
+        for (uint32_t c = threadIdx.x; c < n32; c += blockDim.x) {
+            const uint8_t st = state[c];
+            if (st == kClean || st == kUnmeasured || st == kMasked)
+                continue;
+            if (st == kNarrow)
+                ++narrow;
+            else if (st == kKadaneSpectrum)
+                ++nks;
+            else
+                ++nkc;
+            if (!p.neighbour) {
+                const float v = p.noise ? normal_deviate(draw(p, kStreamNoise, t, c, 0)) : 0.0F;
+                out[c]        = level_of(p, lw[c], sw[c], v);
+                continue;
+            }
+            const uint64_t r  = p.chan_fill_radius;
+            const uint64_t lo = c > r ? c - r : 0;
+            const uint64_t hi = (c + r < n - 1) ? c + r : n - 1;
+            float value       = 0.0F;
+            bool found        = false;
+            for (int a = 0; a < kMaxDraws && !found; ++a) {
+                const uint64_t src = uniform_index(draw(p, kStreamCell, t, c, a), lo, hi);
+                if (state[src] == kClean) {
+                    value = sv[src];
+                    found = true;
                 }
             }
-            state[c] = st;
-            sv[c]    = v;
-            dirty    = dirty || st == kNarrow || st == kKadaneSpectrum || st == kKadaneChannel;
+            fallbacks += found ? 0 : 1;
+            out[c] = level_of(p, lw[c], sw[c], value);
         }
-        // masked and flagged cells are (re)written below or never read
-        if constexpr (V == 4)
-            *reinterpret_cast<float4*>(out + cb) = make_float4(outv[0], outv[1], outv[2], outv[3]);
-        else
-            out[cb] = outv[0];
-    }
-    // a row with no cell to fill (almost every row) is done
-    if (!__syncthreads_or(dirty))
-        return;
-
-    unsigned long long narrow = 0, nks = 0, nkc = 0, fallbacks = 0;
-    for (uint32_t c = threadIdx.x; c < n32; c += blockDim.x) {
-        const uint8_t st = state[c];
-        if (st == kClean || st == kUnmeasured || st == kMasked)
-            continue;
-        if (st == kNarrow)
-            ++narrow;
-        else if (st == kKadaneSpectrum)
-            ++nks;
-        else
-            ++nkc;
-        if (!p.neighbour) {
-            const float v = p.noise ? normal_deviate(draw(p, kStreamNoise, t, c, 0)) : 0.0F;
-            out[c]        = level_of(p, lw[c], sw[c], v);
-            continue;
-        }
-        const uint64_t r  = p.chan_fill_radius;
-        const uint64_t lo = c > r ? c - r : 0;
-        const uint64_t hi = (c + r < n - 1) ? c + r : n - 1;
-        float value       = 0.0F;
-        bool found        = false;
-        for (int a = 0; a < kMaxDraws && !found; ++a) {
-            const uint64_t src = uniform_index(draw(p, kStreamCell, t, c, a), lo, hi);
-            if (state[src] == kClean) {
-                value = sv[src];
-                found = true;
-            }
-        }
-        fallbacks += found ? 0 : 1;
-        out[c] = level_of(p, lw[c], sw[c], value);
+        __syncthreads(); // the fills read this row's states before the next row rewrites them
     }
     if (narrow | nks | nkc | fallbacks) {
         atomicAdd(&cnt[kCountNarrow], narrow);
@@ -1668,8 +1675,7 @@ uint64_t launch_counter() { return g_launches.load(std::memory_order_relaxed); }
 
 static void set_smem(const void* fn, size_t bytes) {
     if (bytes > 48 * 1024)
-        FB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(bytes)));
+        allow_large_smem(fn);
 }
 
 void launch_check_finite(const uint8_t* raw, uint64_t nwords, unsigned long long* first_bad,
@@ -1781,6 +1787,8 @@ void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const
                       float* chunk_max, ZdotSums* chunk_zdot, KadaneState* chunk_kpos,
                       KadaneState* chunk_kneg, float* lo, float* hi, ZdotSums* zdot_sum,
                       Run* kpos_best, Run* kneg_best, cudaStream_t s) {
+    if (d.nsamps >= (uint64_t{1} << 31))
+        throw Error(FROST_ERR_INVALID_ARGUMENT, "scan: too many samples for 32-bit time indices");
     const StageGeom g = stage_geom(raw, d.row_bytes, bits_of(d.dtype));
     if (g.seg_bytes == 0) {
         const dim3 grid(grid1(d.nchans, 64), static_cast<unsigned>(d.nchunks));
@@ -1822,12 +1830,12 @@ void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* 
     FB_DISPATCH(d.dtype, {
         if (vec) {
             set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 4>), smem);
-            k_apply_unflagged<D, 4><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
+            k_apply_unflagged<D, 4><<<static_cast<unsigned>((d.nsamps + kApplyRows - 1) / kApplyRows), 256, smem, s>>>(
                 d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
                 kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, work, counters);
         } else {
             set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 1>), smem);
-            k_apply_unflagged<D, 1><<<static_cast<unsigned>(d.nsamps), 256, smem, s>>>(
+            k_apply_unflagged<D, 1><<<static_cast<unsigned>((d.nsamps + kApplyRows - 1) / kApplyRows), 256, smem, s>>>(
                 d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
                 kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, work, counters);
         }

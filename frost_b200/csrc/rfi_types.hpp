@@ -164,6 +164,93 @@ struct KadaneState {
     }
 };
 
+/** KadaneState::append with 32-bit positions (a block's samples and
+ * channels stay below 2^31): the same sums, comparisons and runs, fewer
+ * integer instructions in the per-sample scans; widened for storage. */
+struct KadaneState32 {
+    struct Run32 {
+        double sum;
+        int32_t start, end;
+    };
+    double total = 0.0;
+    int32_t first = 0, last = -1;
+    bool empty    = true;
+    Run32 prefix{0.0, 0, -1}, suffix{0.0, 0, -1}, best{0.0, 0, -1};
+
+    FB_HD void append(int32_t i, double u) {
+        if (empty) {
+            empty  = false;
+            first  = i;
+            prefix = {0.0, i, i - 1};
+            suffix = {0.0, i, i - 1};
+            best   = suffix;
+        }
+        last = i;
+        total += u;
+        if (total > prefix.sum)
+            prefix = {total, first, i};
+        const double s = suffix.sum + u;
+        if (s > 0.0) {
+            if (suffix.end < suffix.start)
+                suffix.start = i;
+            suffix.sum = s;
+            suffix.end = i;
+        } else {
+            suffix = {0.0, i + 1, i};
+        }
+        if (suffix.sum > best.sum)
+            best = suffix;
+    }
+    FB_HD static Run wide(const Run32& r) { return {r.sum, r.start, r.end}; }
+    FB_HD KadaneState widen() const {
+        KadaneState k = KadaneState::make();
+        k.total       = total;
+        k.first       = first;
+        k.last        = last;
+        k.empty       = empty ? 1 : 0;
+        k.prefix      = wide(prefix);
+        k.suffix      = wide(suffix);
+        k.best        = wide(best);
+        return k;
+    }
+};
+
+/** The best run of KadaneState::append over a sequence that is never
+ * combined with another: only the open (suffix) run and the best one are
+ * kept, with 32-bit positions. */
+struct KadaneBest {
+    double ssum = 0.0, bsum = 0.0;
+    int32_t sstart = 0, send = -1, bstart = 0, bend = -1;
+    bool started = false;
+
+    FB_HD void append(int32_t i, double u) {
+        if (!started) {
+            started = true;
+            sstart  = i;
+            send    = i - 1;
+            bstart  = i;
+            bend    = i - 1;
+        }
+        const double s = ssum + u;
+        if (s > 0.0) {
+            if (send < sstart)
+                sstart = i;
+            ssum = s;
+            send = i;
+        } else {
+            ssum   = 0.0;
+            sstart = i + 1;
+            send   = i;
+        }
+        if (ssum > bsum) {
+            bsum   = ssum;
+            bstart = sstart;
+            bend   = send;
+        }
+    }
+    FB_HD Run best() const { return {bsum, bstart, bend}; }
+};
+
 /** Largest power of five not above `count` (0 for 0). */
 FB_HD uint64_t largest_power_of_five_leq(uint64_t count) {
     if (count == 0)

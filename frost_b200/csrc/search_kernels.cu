@@ -285,7 +285,7 @@ __device__ __forceinline__ Seg shfl_seg(const Seg& g, int src) {
 // strict comparison keeps the earliest maximum), emits the closed ones and
 // leaves `run` open when it reaches the chunk's last valid sample.
 template <int CH>
-__device__ __noinline__ void walk_runs_warp(const SearchParams& p, const RowConst& rc, const float* Q, int64_t c0,
+__device__ __forceinline__ void walk_runs_warp(const SearchParams& p, const RowConst& rc, const float* Q, int64_t c0,
                                int32_t delay, const uint32_t* bits, int wi, RunState& run,
                                const SearchRow& row, uint32_t* count) {
     constexpr int kPerLane = CH / 32 / 32; // mask words per lane
@@ -1133,8 +1133,7 @@ void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t
                         sizeof(uint32_t) * search_bits_words(p0.nwidths, chunk) + 2 * es * seg;
     const dim3 grid(static_cast<unsigned>(ctas > 0 ? std::min<int64_t>(rows, ctas) : rows));
     auto go = [&](auto kernel) {
-        FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+        allow_large_smem(reinterpret_cast<const void*>(kernel));
         kernel<<<grid, kThreads, smem, s>>>(t);
     };
     // widths 1, 2, 4, ... (no trapezoid): the unrolled steady-state tests
