@@ -177,15 +177,19 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch():
-    """Level-kernel DRAM bytes per launch from the committed ncu summary
-    (profiles/fdmt_level_config2.json), scaled to the full gulp, or None."""
-    path = os.path.join(ROOT, "profiles", "fdmt_level_config2.json")
+def ncu_traffic_per_launch(algorithmic_per_launch):
+    """Level-kernel DRAM bytes per launch at full size, scaled from the
+    committed small-case ncu capture (profiles/fdmt_level_config1.json: the
+    1024-channel gulp's measured DRAM bytes over its algorithmic bytes, the
+    level kernels' traffic growing in proportion to the rows and samples
+    they stream), or None."""
+    path = os.path.join(ROOT, "profiles", "fdmt_level_config1.json")
     try:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch_full_gulp")
-    except (OSError, ValueError):
+            ratio = float(json.load(f)["traffic_over_algorithmic"])
+    except (OSError, ValueError, KeyError):
         return None
+    return int(ratio * algorithmic_per_launch)
 
 
 def beam_seed(rank, beam):
@@ -412,7 +416,7 @@ def run_gpu(args):
     t = single16["timing"]
     peak, peak_kind = measured_peaks()
     level_gbs = t["algorithmic_level_bytes"] / (t["level_ms"] / 1e3) / 1e9 if t["level_ms"] else 0.0
-    traffic = ncu_traffic_per_launch()
+    traffic = ncu_traffic_per_launch(t["algorithmic_level_bytes"] / max(t["level_launches"], 1))
     roofline = {
         "bound": "hbm",
         "kernel": ("FDMT level phase: k_level2_pipe<__half> (two levels per pass) + k_level_pipe<__half> "
@@ -983,6 +987,51 @@ def run_config3(args):
     print(json.dumps(line), flush=True)
 
 
+def run_pipeline(args):
+    """One plain FP16 pipeline (RFI, FDMT, search) over the seeded gulp of
+    `--pipeline-config` (config1: 1024 channels, 65536 samples; config2: the
+    headline gulp), W warm-up gulps then K timed ones, with the engine's
+    per-phase CUDA-event times. The small case for multi-pass ncu captures
+    of the FDMT and search kernels; not the headline metric."""
+    import numpy as np
+    import torch
+
+    from frost_b200.config import Storage
+    from frost_b200.pipeline import GulpPipeline, plan_for
+
+    select_workload(args.pipeline_config)
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    lay = layout()
+    raw = torch.from_numpy(np.ascontiguousarray(make_gulp(0x46524F5354)).reshape(-1)).to("cuda")
+    pipe = GulpPipeline(rfi_config(), lay, 2.0, plan_for(lay, 0.0, DM_MAX, DEPTH), search_config(Storage.FP16),
+                        device=local)
+    for _ in range(args.warmup):
+        pipe.execute_device(raw.data_ptr(), GULP, on_device=True)
+    torch.cuda.synchronize()
+    pipe.search.enable_timing(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(args.steps):
+        res = pipe.execute_device(raw.data_ptr(), GULP, on_device=True)
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    t = pipe.search.timing()
+    print(json.dumps({"metric": "plain FP16 pipeline, beam-s searched per second",
+                      "value": round(GULP * TSAMP / (ms / 1e3), 3), "unit": UNIT, "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f32 (fp16 plane storage)", "data": "synthetic",
+                      "config": {"workload": WORKLOAD}, "candidates": int(res.candidates.size),
+                      "phase_ms_per_step": {k: round(t[k] / args.steps, 3) for k in
+                                            ("level1_ms", "level_ms", "search_ms", "history_ms")},
+                      "algorithmic_level_bytes_per_launch":
+                          int(t["algorithmic_level_bytes"] / max(t["level_launches"], 1))}), flush=True)
+
+
 def run_rfi(args):
     """The RFI stage of the headline gulp alone (4096 channels, uint8, the
     config-2 RFI recipe and strategies: bandpass, moments, IQRM, Kadane in
@@ -1032,18 +1081,22 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["frost", "reference"], default="frost")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "postprocess", "rfi", "config3"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "postprocess", "rfi", "config3",
+                                                              "pipeline"],
                     default="config2",
                     help="config2 (headline), config1 (1024-channel profiling case), serving "
                          "(64 beams at real-time cadence), postprocess (candidate clustering and "
                          "dedup of the headline gulp's detections), rfi (the RFI stage alone, a "
-                         "profiling case) or config3 (32 uneven beams searched as one batch)")
+                         "profiling case), pipeline (one plain FP16 pipeline, a profiling case) or "
+                         "config3 (32 uneven beams searched as one batch)")
     ap.add_argument("--beams", type=int, default=3, help="served beams per GPU (admitted by memory)")
     ap.add_argument("--staging", type=int, default=0,
                     help="e2e leg: staging blocks (and gulps in flight) per beam; 0 = one gulp in flight, "
                          "uploaded when it is processed")
     ap.add_argument("--served-tile", type=int, default=0,
                     help="FDMT tile of the served beams in samples (0 = the whole gulp)")
+    ap.add_argument("--pipeline-config", choices=sorted(WORKLOADS), default="config1",
+                    help="the pipeline workload's gulp geometry")
     ap.add_argument("--rfi-nsamps", type=int, default=131072,
                     help="samples of the headline gulp the rfi workload cleans per step")
     args = ap.parse_args()
@@ -1052,6 +1105,9 @@ def main():
         return
     if args.workload == "rfi":
         run_rfi(args)
+        return
+    if args.workload == "pipeline":
+        run_pipeline(args)
         return
     if args.workload == "serving":
         run_serving(args)

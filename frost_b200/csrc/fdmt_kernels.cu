@@ -30,22 +30,26 @@ template <class S> __device__ __forceinline__ float ld(const S* p);
 template <> __device__ __forceinline__ float ld<float>(const float* p) { return *p; }
 template <> __device__ __forceinline__ float ld<__half>(const __half* p) { return __half2float(*p); }
 
-template <class S> __device__ __forceinline__ void st(S* p, float v);
-template <> __device__ __forceinline__ void st<float>(float* p, float v) { *p = v; }
-// FP16 storage saturates at the largest finite half instead of overflowing
-// to infinity (a strong unexcised burst must not poison a whole DM row).
-template <> __device__ __forceinline__ void st<__half>(__half* p, float v) {
-    *p = __float2half_rn(fminf(fmaxf(v, -65504.0F), 65504.0F));
-}
-
 // Two sums of finite fp16 level values (at most four of them, so finite
 // floats) rounded to an fp16 pair, lo in the low half: the saturating
-// convert gives st<__half>'s clamp-then-round bit for bit for finite
-// inputs (a magnitude past 65504 becomes 65504), in one instruction.
+// convert gives clamp-to-+-65504-then-round bit for bit for finite inputs
+// (a magnitude past 65504 becomes 65504), in one instruction.
 __device__ __forceinline__ uint32_t pack_sat(float lo, float hi) {
     uint32_t r;
     asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
     return r;
+}
+
+// Stores a level value. FP16 storage saturates at the largest finite half
+// instead of overflowing to infinity (a strong unexcised burst must not
+// poison a whole DM row): one saturating convert, which for finite values
+// gives clamp-then-round bit for bit (as pack_sat does for pairs).
+template <class S> __device__ __forceinline__ void st_sat(S* p, float v);
+template <> __device__ __forceinline__ void st_sat<float>(float* p, float v) { *p = v; }
+template <> __device__ __forceinline__ void st_sat<__half>(__half* p, float v) {
+    unsigned short h;
+    asm("cvt.rn.satfinite.f16.f32 %0, %1;" : "=h"(h) : "f"(v));
+    *reinterpret_cast<unsigned short*>(p) = h;
 }
 
 // Level 1 with the leaf initialisation: row (d_lo, d_hi) of a two-channel
@@ -56,17 +60,20 @@ __device__ __forceinline__ uint32_t pack_sat(float lo, float hi) {
 // double (every window sum is then its exact value to ~1e-16 relative,
 // however long the tile, and rounds once to float). The two channels' tile
 // segments, with the H samples before the tile, sit in shared memory as
-// floats; thread t owns samples t, t + 256, ... of the tile.
+// doubles (converted once); thread t owns samples t, t + 256, ... of the
+// tile.
+constexpr int kFill = 8; // tile elements each thread loads at once (the H + 1 more follow)
+
 template <class S>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 5)
     k_level1(const LeafOp* __restrict__ ops, const int32_t* __restrict__ node_first_op, int32_t nnodes,
              int32_t ntiles, int32_t H, const float* __restrict__ wf, int64_t wpitch, int64_t t0,
              int32_t n_valid, const float* __restrict__ hist, int32_t hist_len, S* __restrict__ out,
              int64_t pitch, int32_t base) {
-    extern __shared__ float smem_x[];
+    extern __shared__ double smem_x[];
     const int32_t N = kTimePerCta + H + 1;
-    float* Xa       = smem_x;
-    float* Xb       = smem_x + N;
+    double* Xa      = smem_x;
+    double* Xb      = smem_x + N;
     // Work items (node, tile), nodes fastest; a CTA takes items blockIdx.x,
     // blockIdx.x + gridDim.x, ...
     const int64_t nitems = static_cast<int64_t>(nnodes) * ntiles;
@@ -76,11 +83,14 @@ __global__ void __launch_bounds__(kThreads)
         const int32_t ca  = ops[op0].chan_lo;
         const int32_t cb  = ops[op0].chan_hi;
         const int32_t k0  = static_cast<int32_t>(item / nnodes) * kTimePerCta;
-        // x(i) for tile-relative time t = k0 + i - H - 1 (index 0 unused)
-        for (int i = threadIdx.x; i < N; i += kThreads) {
+        // x(i) for tile-relative time t = k0 + i - H - 1 (index 0 unused):
+        // the first kFill elements of each thread are all loaded before any
+        // is stored, so a fill waits for one round trip, not one per element
+        auto fetch = [&](int i, float& a, float& b) {
             const int64_t t = static_cast<int64_t>(k0) + i - H - 1;
-            float a = 0.0F, b = 0.0F;
-            if (i > 0) {
+            a = 0.0F;
+            b = 0.0F;
+            if (i > 0 && i < N) {
                 if (t < 0) {
                     a = hist[static_cast<int64_t>(ca) * hist_len + hist_len + t];
                     if (cb >= 0)
@@ -91,8 +101,26 @@ __global__ void __launch_bounds__(kThreads)
                         b = wf[static_cast<int64_t>(cb) * wpitch + t0 + t];
                 }
             }
-            Xa[i] = a;
-            Xb[i] = b;
+        };
+        {
+            float ra[kFill], rb[kFill];
+#pragma unroll
+            for (int u = 0; u < kFill; ++u)
+                fetch(threadIdx.x + u * kThreads, ra[u], rb[u]);
+#pragma unroll
+            for (int u = 0; u < kFill; ++u) {
+                const int i = threadIdx.x + u * kThreads;
+                if (i < N) {
+                    Xa[i] = static_cast<double>(ra[u]);
+                    Xb[i] = static_cast<double>(rb[u]);
+                }
+            }
+            for (int i = threadIdx.x + kFill * kThreads; i < N; i += kThreads) {
+                float a, b;
+                fetch(i, a, b);
+                Xa[i] = static_cast<double>(a);
+                Xb[i] = static_cast<double>(b);
+            }
         }
         __syncthreads();
         // window state per owned sample: A = sum a[t - dl .. t],
@@ -120,7 +148,7 @@ __global__ void __launch_bounds__(kThreads)
             for (int32_t q = from; q <= op.d_lo; ++q)
 #pragma unroll
                 for (int j = 0; j < kPer; ++j)
-                    A[j] += static_cast<double>(Xa[i0 + j * kThreads - q]);
+                    A[j] += Xa[i0 + j * kThreads - q];
             if (cb >= 0) {
                 // B's window moves from back offsets [dl, dl + dh] to
                 // [op.d_lo, op.d_lo + op.d_hi]: drop the top, add the bottom,
@@ -133,21 +161,21 @@ __global__ void __launch_bounds__(kThreads)
                     for (int32_t q = op.d_lo; q <= nb; ++q)
 #pragma unroll
                         for (int j = 0; j < kPer; ++j)
-                            B[j] += static_cast<double>(Xb[i0 + j * kThreads - q]);
+                            B[j] += Xb[i0 + j * kThreads - q];
                 } else {
                     for (int32_t q = dl; q < op.d_lo; ++q)
 #pragma unroll
                         for (int j = 0; j < kPer; ++j)
-                            B[j] -= static_cast<double>(Xb[i0 + j * kThreads - q]);
+                            B[j] -= Xb[i0 + j * kThreads - q];
                     for (int32_t q = ob + 1; q <= nb; ++q)
 #pragma unroll
                         for (int j = 0; j < kPer; ++j)
-                            B[j] += static_cast<double>(Xb[i0 + j * kThreads - q]);
+                            B[j] += Xb[i0 + j * kThreads - q];
                 }
             }
 #pragma unroll
             for (int j = 0; j < kPer; ++j)
-                st<S>(row + j * kThreads, static_cast<float>(A[j] + B[j]));
+                st_sat<S>(row + j * kThreads, static_cast<float>(A[j] + B[j]));
             dl = op.d_lo;
             dh = op.d_hi;
         }
@@ -695,7 +723,7 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
         throw Error(FROST_ERR_INTERNAL, "level1: bad geometry");
     const int32_t ntiles = ncols / kTimePerCta;
     const dim3 grid(grid_for(static_cast<int64_t>(nnodes) * ntiles, ctas));
-    const size_t smem = 2 * sizeof(float) * (kTimePerCta + max_node_delay + 1);
+    const size_t smem = 2 * sizeof(double) * (kTimePerCta + max_node_delay + 1);
     if (smem > 200 * 1024)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "level1: leaf windows too long for shared memory");
     if (out.fp16) {

@@ -1038,12 +1038,12 @@ __device__ __forceinline__ float level_of(const ApplyParams& p, float loc, float
 }
 
 // Unflagged rows (lib/cpu/rfi_cpu.cpp:537-624): each CTA takes kApplyRows
-// consecutive rows in turn (their per-window constants then come from L1);
-// a row's samples and cell states are staged in shared memory so neighbour
-// draws read them without touching HBM again. Masked cells are not written:
-// the normalized output zeroes them, so their fill values are never
-// observed.
-constexpr int kApplyRows = 8;
+// consecutive rows in turn (one: more rows per CTA measured slower, 3.1 vs
+// 2.9 ms at 8); a row's samples and cell states are staged in shared
+// memory so neighbour draws read them without touching HBM again. Masked
+// cells are not written: the normalized output zeroes them, so their fill
+// values are never observed.
+constexpr int kApplyRows = 1;
 
 template <int D, int V>
 __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restrict__ raw,

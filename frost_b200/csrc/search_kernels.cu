@@ -805,18 +805,20 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                         nh[halo + halo / 4 + halo / P] = q[P - 1];
                 }
                 if (!direct_halo) {
-                    // this chunk's halo from the previous chunk's, rebased so that Q[-1] = 0
+                    // this chunk's halo from the previous chunk's, rebased so
+                    // that Q[-1] = 0: the group and thread minima and Q[-2],
+                    // Q[-1] now (the bound tests read them); the halo's other
+                    // prefix sums only when Q is stored (store_q)
                     const float* ph  = nh0 + ((ci - 1) & 1) * nh_len;
-                    const int n      = halo + halo / 4 + halo / P;
-                    const float last = ph[n];
-                    for (int i = threadIdx.x; i < n; i += kThreads) {
-                        const float v = ph[i] - last;
-                        if (i < halo)
-                            Q[i - halo] = v;
-                        else if (i < halo + halo / 4)
-                            gmin[i - halo] = v;
+                    const int n      = halo / 4 + halo / P;
+                    const float last = ph[halo + n];
+                    for (int i = threadIdx.x; i < n + 2; i += kThreads) {
+                        if (i < halo / 4)
+                            gmin[i] = ph[halo + i] - last;
+                        else if (i < n)
+                            tmin[i - halo / 4] = ph[halo + i] - last;
                         else
-                            tmin[i - halo - halo / 4] = v;
+                            Q[i - n - 2] = ph[halo + i - n - 2] - last;
                     }
                 }
             }
@@ -827,6 +829,13 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
 #pragma unroll
                 for (int i = 0; i < P / 4; ++i)
                     d[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+                if (carry_halo && !direct_halo) {
+                    // the rest of the halo's prefix sums, rebased (Q[-2], Q[-1] are)
+                    const float* ph  = nh0 + ((ci - 1) & 1) * nh_len;
+                    const float last = ph[halo + halo / 4 + halo / P];
+                    for (int i = threadIdx.x; i < halo - 2; i += kThreads)
+                        Q[i - halo] = ph[i] - last;
+                }
                 for (int i = threadIdx.x; i < nw * (CH / 32); i += kThreads)
                     bits[i] = 0U;
                 if (threadIdx.x == 0)
