@@ -64,4 +64,11 @@ __device__ __forceinline__ void load(void* dst, const void* src, uint32_t bytes,
         : "memory");
 }
 
+/** Starts fetching global [src, src + bytes) into L2 (no shared memory, no
+ * completion to wait for): a later bulk copy of the range then waits for
+ * L2, not HBM. 16-byte aligned, a multiple of 16 bytes. */
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 } // namespace fb::bulk

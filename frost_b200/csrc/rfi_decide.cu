@@ -165,11 +165,30 @@ __device__ float block_select(const float* __restrict__ x, uint64_t count, uint6
         for (int i = threadIdx.x; i < 256; i += blockDim.x)
             hist[i] = 0;
         __syncthreads();
-        for (uint64_t i = threadIdx.x; i < count; i += blockDim.x) {
-            const float v    = ABS ? fabsf(x[i]) : x[i];
-            const uint32_t k = order_key(v);
-            if ((k & pmask) == prefix)
-                atomicAdd(&hist[(k >> shift) & 255U], 1U);
+        // eight loads in flight per thread (one CTA streams the whole
+        // series), then one shared-memory atomic per bin a warp's keys fall
+        // in (most keys share their top bytes)
+        constexpr int kU = 8;
+        for (uint64_t base = 0; base < count; base += static_cast<uint64_t>(blockDim.x) * kU) {
+            float v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const uint64_t i = base + static_cast<uint64_t>(u) * blockDim.x + threadIdx.x;
+                v[u]             = i < count ? x[i] : 0.0F;
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const uint64_t i = base + static_cast<uint64_t>(u) * blockDim.x + threadIdx.x;
+                uint32_t bin     = 256U; // none
+                if (i < count) {
+                    const uint32_t k = order_key(ABS ? fabsf(v[u]) : v[u]);
+                    if ((k & pmask) == prefix)
+                        bin = (k >> shift) & 255U;
+                }
+                const unsigned peers = __match_any_sync(0xFFFFFFFFU, bin);
+                if (bin < 256U && static_cast<int>(threadIdx.x & 31U) == __ffs(static_cast<int>(peers)) - 1)
+                    atomicAdd(&hist[bin], static_cast<uint32_t>(__popc(peers)));
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -190,6 +209,44 @@ __device__ float block_select(const float* __restrict__ x, uint64_t count, uint6
         __syncthreads();
     }
     return key_value(prefix);
+}
+
+/** The element of rank `rank - 1` given the element `v` of rank `rank`
+ * (|x| when ABS): v itself when fewer than `rank` elements lie below it,
+ * else the largest element below it (one pass instead of a second
+ * selection). */
+template <bool ABS>
+__device__ float block_select_prev(const float* __restrict__ x, uint64_t count, uint64_t rank, float v,
+                                   unsigned long long* red, uint32_t* s_max) {
+    const uint32_t K       = order_key(v);
+    unsigned long long below = 0;
+    uint32_t best          = 0U;
+    constexpr int kU = 8; // loads in flight per thread
+    for (uint64_t base = 0; base < count; base += static_cast<uint64_t>(blockDim.x) * kU) {
+        float v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint64_t i = base + static_cast<uint64_t>(u) * blockDim.x + threadIdx.x;
+            v[u]             = i < count ? x[i] : 0.0F;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint64_t i = base + static_cast<uint64_t>(u) * blockDim.x + threadIdx.x;
+            const uint32_t k = order_key(ABS ? fabsf(v[u]) : v[u]);
+            if (i < count && k < K) {
+                ++below;
+                best = max(best, k);
+            }
+        }
+    }
+    if (threadIdx.x == 0)
+        *s_max = 0U;
+    below = block_sum(below, red); // its barriers also order the reset above
+    atomicMax(s_max, best);
+    __syncthreads();
+    const uint32_t m = *s_max;
+    __syncthreads();
+    return below >= rank ? key_value(m) : v;
 }
 
 // ---- channel mask --------------------------------------------------------
@@ -625,11 +682,13 @@ __global__ void __launch_bounds__(kBlock)
     __shared__ uint32_t hist[256];
     __shared__ uint64_t s_rank;
     __shared__ uint32_t s_bin;
+    __shared__ unsigned long long red[32];
+    __shared__ uint32_t s_max;
     if (none_good(good_prefix, n))
         return;
     float med = block_select<true>(x, count, count / 2, hist, &s_rank, &s_bin);
     if (count % 2 == 0) {
-        const float lower = block_select<true>(x, count, count / 2 - 1, hist, &s_rank, &s_bin);
+        const float lower = block_select_prev<true>(x, count, count / 2, med, red, &s_max);
         med               = 0.5F * lower + 0.5F * med;
     }
     if (threadIdx.x == 0)
@@ -864,16 +923,49 @@ __global__ void __launch_bounds__(kBlock)
     k_flag_list(uint64_t count, uint64_t n, const uint8_t* __restrict__ flags, const uint8_t* __restrict__ mask,
                 uint64_t* __restrict__ flagged, unsigned long long* __restrict__ counters) {
     __shared__ unsigned long long red[32];
-    const uint64_t per       = (count + blockDim.x - 1) / blockDim.x;
-    const uint64_t t0        = threadIdx.x * per;
-    const uint64_t t1        = t0 + per < count ? t0 + per : count;
-    unsigned long long local = 0, total = 0;
-    for (uint64_t t = t0; t < t1; ++t)
-        local += flags[t] != 0 ? 1 : 0;
-    unsigned long long at = block_exclusive_scan(local, red, &total);
-    for (uint64_t t = t0; t < t1; ++t)
-        if (flags[t] != 0)
-            flagged[at++] = t;
+    // each warp takes one contiguous span (a multiple of 32 samples) and
+    // walks it 32 samples at a time, eight ballots per step (loads in
+    // flight); pass 1 counts, the warps' counts are scanned, pass 2 writes
+    // each flagged sample at its rank: increasing order without a barrier
+    // per step
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t below_lane = (1U << lane) - 1U;
+    const uint64_t span       = ((count + nwarps - 1) / nwarps + 31) / 32 * 32;
+    const uint64_t w0         = min(static_cast<uint64_t>(warp) * span, count);
+    const uint64_t w1         = min(w0 + span, count);
+    constexpr int kU          = 8;
+    auto step = [&](uint64_t base, uint32_t (&bal)[kU]) {
+        bool f[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint64_t t = base + 32 * u + lane;
+            f[u]             = t < w1 && flags[t] != 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            bal[u] = __ballot_sync(0xFFFFFFFFU, f[u]);
+    };
+    unsigned long long mine = 0;
+    for (uint64_t base = w0; base < w1; base += 32 * kU) {
+        uint32_t bal[kU];
+        step(base, bal);
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            mine += static_cast<unsigned long long>(__popc(bal[u]));
+    }
+    unsigned long long total = 0;
+    unsigned long long at    = block_exclusive_scan(lane == 0 ? mine : 0ULL, red, &total);
+    at                       = __shfl_sync(0xFFFFFFFFU, at, 0);
+    for (uint64_t base = w0; base < w1; base += 32 * kU) {
+        uint32_t bal[kU];
+        step(base, bal);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if ((bal[u] >> lane) & 1U)
+                flagged[at + static_cast<uint32_t>(__popc(bal[u] & below_lane))] = base + 32 * u + lane;
+            at += static_cast<unsigned long long>(__popc(bal[u]));
+        }
+    }
     unsigned long long kept = 0;
     for (uint64_t c = threadIdx.x; c < n; c += blockDim.x)
         kept += mask[c] != 0 ? 1 : 0;

@@ -140,20 +140,23 @@ __global__ void k_check_finite(const uint32_t* __restrict__ w, uint64_t n,
 
 // ---- bandpass -------------------------------------------------------------
 
+// The evenly spaced sample rows of each window (row i of window w is block
+// row b + i * len / m, lib/cpu/spectra_cpu.cpp:96-104), decoded to float:
+// one CTA per (row, window), its threads across the channels.
 template <int D>
 __global__ void k_sample_rows(Dims d, const uint8_t* __restrict__ raw, float* __restrict__ out) {
-    const uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    const uint64_t i = blockIdx.y;
-    const uint64_t w = blockIdx.z;
-    if (c >= d.nchans)
-        return;
+    const uint64_t i   = blockIdx.x;
+    const uint64_t w   = blockIdx.y;
     const uint64_t b   = window_begin(w, d.window);
     const uint64_t len = window_end(w, d) - b;
     const uint64_t m   = largest_power_of_five_leq(len < kMaxBandpassRows ? len : kMaxBandpassRows);
     if (i >= m)
         return;
-    const uint64_t t = b + (i * len) / m;
-    out[(w * kMaxBandpassRows + i) * d.nchans + c] = rd<D>(raw + t * d.row_bytes, c);
+    const uint64_t t  = b + (i * len) / m;
+    const uint8_t* in = raw + t * d.row_bytes;
+    float* dst        = out + (w * kMaxBandpassRows + i) * d.nchans;
+    for (uint64_t c = threadIdx.x; c < d.nchans; c += blockDim.x)
+        dst[c] = rd<D>(in, c);
 }
 
 // Recursive median-of-5 over m = 5^k values streamed in order: the same
@@ -1688,8 +1691,8 @@ void launch_check_finite(const uint8_t* raw, uint64_t nwords, unsigned long long
 }
 
 void launch_sample_rows(const Dims& d, const uint8_t* raw, float* samples, cudaStream_t s) {
-    const dim3 grid(grid1(d.nchans, 128), kMaxBandpassRows, static_cast<unsigned>(d.nwin));
-    FB_DISPATCH(d.dtype, k_sample_rows<D><<<grid, 128, 0, s>>>(d, raw, samples));
+    const dim3 grid(kMaxBandpassRows, static_cast<unsigned>(d.nwin));
+    FB_DISPATCH(d.dtype, k_sample_rows<D><<<grid, 256, 0, s>>>(d, raw, samples));
     FB_COUNT_LAUNCH();
 }
 

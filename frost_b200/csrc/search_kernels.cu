@@ -40,6 +40,7 @@ namespace fb::fdmt {
 namespace {
 
 constexpr int kThreads   = 256;
+static_assert(kThreads == 256, "the warp offsets read the 8 warp totals as two float4");
 constexpr int kMaxWidths = 32;
 // widths 1, 2, ..., 2^15 take the unrolled steady-state tests
 constexpr int kMaxPow2Widths = 16;
@@ -78,7 +79,7 @@ __device__ __forceinline__ float max_diffs(const float (&q)[P], float m) {
 }
 
 __device__ void scan_inplace(float* a, int n) {
-    __shared__ float warp_tot[kThreads / 32];
+    __shared__ __align__(16) float warp_tot[kThreads / 32];
     const int per = (n + kThreads - 1) / kThreads;
     const int beg = threadIdx.x * per;
     const int end = min(beg + per, n);
@@ -712,6 +713,11 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             const uint32_t bytes = static_cast<uint32_t>((seg_cols - off) * sizeof(S));
             bulk::mbar_expect(&bar[b], bytes);
             bulk::load(stage0 + b * seg_cols + off, src + static_cast<int64_t>(ci) * CH - halo + off, bytes, &bar[b]);
+            // two buffers hold one chunk in flight: the chunk staged two
+            // issues later is fetched into L2 meanwhile (the same columns its
+            // copy reads), so that copy waits for L2, not HBM
+            if (ci + 2 < nchunks)
+                bulk::prefetch_l2(src + static_cast<int64_t>(ci + 2) * CH, static_cast<uint32_t>(CH * sizeof(S)));
         };
         if (threadIdx.x == 0)
             for (int ci = 0; ci < min(2, nchunks); ++ci)
@@ -757,9 +763,15 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             // every thread has read this chunk's staging buffer: refill it
             if (threadIdx.x == 0 && ci + 2 < nchunks)
                 issue(ci + 2);
-            float woff = 0.0F;
-            for (int w = 0; w < warp; ++w)
-                woff += warp_tot[w];
+            // the totals of the warps before this one, in warp order (the
+            // later terms add +0, which leaves the sum's bits unchanged)
+            const float4 ta = reinterpret_cast<const float4*>(warp_tot)[0];
+            const float4 tb = reinterpret_cast<const float4*>(warp_tot)[1];
+            const float tw[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+            float woff        = 0.0F;
+#pragma unroll
+            for (int w = 0; w < kThreads / 32 - 1; ++w)
+                woff += w < warp ? tw[w] : 0.0F;
             const float off = excl + woff;
 #pragma unroll
             for (int e = 0; e < P; ++e)
