@@ -438,9 +438,16 @@ template <class S, int P> __device__ __forceinline__ void ld_cols(const S* p, fl
 // at `p` (16-byte aligned); fp16 samples are added with mixed-precision
 // adds (`add.rn.f32.f16`: the widening is exact, so the same bits as
 // widening first).
-template <class S, int P> __device__ __forceinline__ void scan_cols(const S* p, float (&q)[P]) {
+template <class S, int P> __device__ __forceinline__ void scan_cols(const S* p, float (&q)[P], float& xmax) {
     if constexpr (sizeof(S) == 4) {
         ld_cols<S, P>(p, q);
+        float m = q[0];
+#pragma unroll
+        for (int e = 1; e + 1 < P; e += 2)
+            m = fmax3(m, q[e], q[e + 1]);
+        if constexpr (P % 2 == 0)
+            m = fmaxf(m, q[P - 1]);
+        xmax = m;
 #pragma unroll
         for (int e = 1; e < P; ++e)
             q[e] += q[e - 1];
@@ -451,6 +458,12 @@ template <class S, int P> __device__ __forceinline__ void scan_cols(const S* p, 
             const uint4 u = reinterpret_cast<const uint4*>(p)[i];
             w[4 * i] = u.x, w[4 * i + 1] = u.y, w[4 * i + 2] = u.z, w[4 * i + 3] = u.w;
         }
+        // the largest sample: packed fp16 maxima (exact), then one widening
+        __half2 hm = *reinterpret_cast<const __half2*>(&w[0]);
+#pragma unroll
+        for (int i = 1; i < P / 2; ++i)
+            hm = __hmax2(hm, *reinterpret_cast<const __half2*>(&w[i]));
+        xmax = fmaxf(__low2float(hm), __high2float(hm));
         q[0] = __half2float(__ushort_as_half(static_cast<unsigned short>(w[0] & 0xFFFFU)));
 #pragma unroll
         for (int e = 1; e < P; ++e) {
@@ -458,6 +471,19 @@ template <class S, int P> __device__ __forceinline__ void scan_cols(const S* p, 
             asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(q[e]) : "h"(h), "f"(q[e - 1]));
         }
     }
+}
+
+// q[e] += off for every e, two lanes per instruction (add.rn.f32x2: each
+// lane rounds as a scalar add).
+template <int P> __device__ __forceinline__ void add_offset(float (&q)[P], float off) {
+#pragma unroll
+    for (int e = 0; e + 1 < P; e += 2)
+        asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%0, %1};\n mov.b64 b, {%2, %2};\n"
+            " add.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
+            : "+f"(q[e]), "+f"(q[e + 1])
+            : "f"(off));
+    if constexpr (P % 2 != 0)
+        q[P - 1] += off;
 }
 
 template <int R, int NG, int N>
@@ -509,9 +535,9 @@ __device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float
                                            float& m1) {
     constexpr int W = 1 << WI;
     if constexpr (W == 1) {
-        const float m = max_diffs<P, 1>(q, q[0] - pm1);
-        m1             = m; // the largest width-1 sum of the thread's samples
-        return m > T;
+        // m1 arrives as an upper bound of every width-1 sum of the thread's
+        // samples (see the caller)
+        return m1 > T;
     } else if constexpr (W == 2) {
         // Every width-2 window sum is, before rounding, the sum of two of the
         // thread's width-1 sums (or of its first one and the one ending just
@@ -558,15 +584,18 @@ __device__ __forceinline__ bool pow2_maybe(const float (&q)[P], float pm1, float
     }
 }
 
-template <int P, int NG, int WI>
-__device__ __forceinline__ void pow2_all(uint32_t& cand, int nw, const float (&q)[P], float pm1, float pm2,
-                                         const float (&gmx)[NG], float bmax, const float* gmin,
-                                         const float* tmin, int halo, const WidthTest* wt, float& m1) {
-    if constexpr (WI < kMaxPow2Widths) {
+// The steady-state tests of the widths 2^WI .. 2^(WI1 - 1) that are below nw
+// (one by one: a test of a set of widths against its smallest threshold,
+// bounded by the set's least window start, measured slower).
+template <int P, int NG, int WI, int WI1>
+__device__ __forceinline__ void pow2_range(uint32_t& cand, const float (&q)[P], float pm1, float pm2,
+                                           const float (&gmx)[NG], float bmax, const float* gmin,
+                                           const float* tmin, int halo, const WidthTest* wt, int nw, float& m1) {
+    if constexpr (WI < WI1) {
         if (WI < nw) {
             if (pow2_maybe<P, NG, WI>(q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt[WI].T, m1))
                 cand |= 1U << WI;
-            pow2_all<P, NG, WI + 1>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt, m1);
+            pow2_range<P, NG, WI + 1, WI1>(cand, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt, nw, m1);
         }
     }
 }
@@ -746,7 +775,8 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             // ---- prefix sums of the thread's P columns: serial, then across the
             // warp (shuffles), then across warps (one offset per warp)
             float q[P];
-            scan_cols<S, P>(seg + halo + P * threadIdx.x, q);
+            float xmax; // the thread's largest sample
+            scan_cols<S, P>(seg + halo + P * threadIdx.x, q, xmax);
             float incl = q[P - 1];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -773,9 +803,7 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             for (int w = 0; w < kThreads / 32 - 1; ++w)
                 woff += w < warp ? tw[w] : 0.0F;
             const float off = excl + woff;
-#pragma unroll
-            for (int e = 0; e < P; ++e)
-                q[e] += off;
+            add_offset<P>(q, off);
             // ---- group and block extremes (registers; the minima to shared memory)
             float gmx[NG], gmn[NG];
 #pragma unroll
@@ -871,8 +899,17 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                 }
                 uint32_t cand = 0U;
                 if constexpr (POW2) {
-                    float m1 = FB_POS_INF; // set by the width-1 test
-                    pow2_all<P, NG, 0>(cand, nw, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt, m1);
+                    // A width-1 window sum Q[k] - Q[k-1] inside the thread's
+                    // samples (k >= 1) differs from the sample x[k] by four
+                    // roundings (the local prefix, the offset twice, the
+                    // difference), each at most 2^-24 of a magnitude below
+                    // max|Q| + |off| (Q within [bmin, bmax]): 2^-20 of that
+                    // bounds their sum. The first sample's sum reaches back
+                    // into the previous thread's prefix (the block scan's own
+                    // rounding) and is taken exactly.
+                    const float qmag = fmaxf(fabsf(bmax), fabsf(bmin)) + fabsf(off);
+                    float m1         = fmaxf(xmax + qmag * 0x1p-20F, q[0] - pm1);
+                    pow2_range<P, NG, 0, kMaxPow2Widths>(cand, q, pm1, pm2, gmx, bmax, gmin, tmin, halo, wt, nw, m1);
                 }
                 else {
                     for (int wi = 0; wi < nw; ++wi) {
