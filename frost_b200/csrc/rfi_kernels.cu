@@ -105,7 +105,11 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) {
 }
 
 __device__ __forceinline__ uint64_t window_of(uint64_t t, uint64_t window, uint64_t nwin) {
-    const uint64_t w = t / window;
+    // a 32-bit division when both fit (a 64-bit one is a long software
+    // sequence, paid per thread and row in the row-parallel kernels)
+    const uint64_t w = (t | window) < (uint64_t{1} << 32)
+                           ? static_cast<uint64_t>(static_cast<uint32_t>(t) / static_cast<uint32_t>(window))
+                           : t / window;
     return w < nwin - 1 ? w : nwin - 1;
 }
 
@@ -666,11 +670,19 @@ __global__ void __launch_bounds__(kStageChans)
 constexpr int kScanRows  = 128; // rows per CTA (one thread each)
 constexpr int kScanChans = 64;  // channel tile staged in shared memory
 
+template <int D> constexpr bool kIntRow = D != FROST_FLOAT32 && kBitsOf<D> <= 16;
+
 // One row of the row scan (lib/cpu/rfi_cpu_measure.cpp:305-446), fed its
 // channels in ascending order: the detection series sums and the Kadane
 // states across frequency.
+// With integer samples of at most 16 bits (INT) the row's sum and sum of
+// squares are kept as integers: every partial double sum of such values is
+// an integer below 2^53, so the reference's double sums are exact and equal
+// the integer ones whatever the order.
+template <bool INT>
 struct ScanRowAcc {
     double sum_det = 0.0, sum_keep = 0.0, sx = 0.0, sxx = 0.0;
+    uint64_t isx = 0, isxx = 0;
     uint32_t n_keep = 0, n_meas = 0; // counts (exact as doubles when used)
     KadaneBest sp, sn; // rows are scanned whole: only the best runs are needed
     __device__ __forceinline__ void step(uint64_t c, float x, float l, float ic, float clip, int kspec) {
@@ -682,8 +694,14 @@ struct ScanRowAcc {
             sum_keep += zc;
             ++n_keep;
         }
-        sx += x;
-        sxx += static_cast<double>(x) * x;
+        if constexpr (INT) {
+            const uint32_t xi = static_cast<uint32_t>(x);
+            isx += xi;
+            isxx += static_cast<uint64_t>(xi) * xi;
+        } else {
+            sx += x;
+            sxx += static_cast<double>(x) * x;
+        }
         if (kspec) {
             sp.append(static_cast<int32_t>(c), cl);
             sn.append(static_cast<int32_t>(c), -cl);
@@ -696,6 +714,8 @@ struct ScanRowAcc {
                            Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole) const {
         const double dn     = n_meas > 1 ? static_cast<double>(n_meas) : 1.0;
         const double s_keep = n_keep > 0 ? sum_keep / static_cast<double>(n_keep) : 0.0;
+        const double sx     = INT ? static_cast<double>(isx) : this->sx;
+        const double sxx    = INT ? static_cast<double>(isxx) : this->sxx;
         s_det[t]            = static_cast<float>(sum_det / dn);
         s_keep_f[t]         = static_cast<float>(s_keep);
         s_keep_d[t]         = s_keep;
@@ -745,7 +765,7 @@ __global__ void __launch_bounds__(kScanRows)
     const uint64_t w     = active ? window_of(t, d.window, d.nwin) : 0;
     const float* lw      = loc + w * n;
     const float* iw      = inv + w * n;
-    ScanRowAcc acc;
+    ScanRowAcc<kIntRow<D>> acc;
     for (uint64_t c0 = 0; c0 < n; c0 += kScanChans) {
         const unsigned cl_ = threadIdx.x % kScanChans;
         const uint64_t cc  = c0 + cl_;
@@ -797,6 +817,9 @@ __global__ void __launch_bounds__(kScanRows)
     const uint64_t w  = active ? window_of(t, d.window, d.nwin) : 0;
     const float* lw   = loc + w * n;
     const float* iw   = inv + w * n;
+    // 16-byte loads of the window constants and mask need 16-byte aligned rows
+    const bool vec_consts = (reinterpret_cast<uintptr_t>(lw) | reinterpret_cast<uintptr_t>(iw) |
+                             reinterpret_cast<uintptr_t>(mask)) % 16 == 0;
     const int nrows   = static_cast<int>(d.nsamps - t0 < kScanRows ? d.nsamps - t0 : kScanRows);
     const int ntiles  = static_cast<int>((d.row_bytes + kRowTileBytes - 1) / kRowTileBytes);
     auto issue = [&](int j) {
@@ -812,7 +835,7 @@ __global__ void __launch_bounds__(kScanRows)
     issue(0);
     if (ntiles > 1)
         issue(1);
-    ScanRowAcc acc;
+    ScanRowAcc<kIntRow<D>> acc;
     for (int j = 0; j < ntiles; ++j) {
         if (j + 1 < ntiles)
             stage::wait_pending<1>();
@@ -829,6 +852,30 @@ __global__ void __launch_bounds__(kScanRows)
                     uint8_t b[16];
                 } u;
                 u.v = *reinterpret_cast<const uint4*>(row + (q - cb) * kBitsOf<D> / 8);
+                if constexpr (kPerChunk == 16) {
+                    if (vec_consts && q + kPerChunk <= ce) {
+                        // a whole chunk: its mask bytes and window constants
+                        // as 16-byte loads (the same for every row of the CTA)
+                        union {
+                            uint4 v;
+                            uint8_t b[16];
+                        } mk;
+                        mk.v = *reinterpret_cast<const uint4*>(mask + q);
+                        float ls[16], is[16];
+#pragma unroll
+                        for (int v4 = 0; v4 < 4; ++v4) {
+                            const float4 a = reinterpret_cast<const float4*>(lw + q)[v4];
+                            const float4 b = reinterpret_cast<const float4*>(iw + q)[v4];
+                            ls[4 * v4] = a.x, ls[4 * v4 + 1] = a.y, ls[4 * v4 + 2] = a.z, ls[4 * v4 + 3] = a.w;
+                            is[4 * v4] = b.x, is[4 * v4 + 1] = b.y, is[4 * v4 + 2] = b.z, is[4 * v4 + 3] = b.w;
+                        }
+#pragma unroll
+                        for (int e = 0; e < 16; ++e)
+                            if (mk.b[e] != 0 && is[e] != 0.0F)
+                                acc.step(q + e, rd<D>(u.b, static_cast<uint64_t>(e)), ls[e], is[e], clip, kp.enabled);
+                        continue;
+                    }
+                }
 #pragma unroll
                 for (int e = 0; e < kPerChunk; ++e) {
                     const uint32_t c = q + e;
@@ -870,6 +917,7 @@ struct ScanColAcc {
     float l = 0.0F, iv = 0.0F, cm = 0.0F, ci = 0.0F;
     float cmin = FLT_MAX, cmax = -FLT_MAX;
     ZdotSums zs{0, 0, 0, 0, 0};
+    uint32_t zn = 0;
     KadaneState32 kpos, kneg; // widened when stored
     __device__ __forceinline__ void step(float x, uint64_t t) {
         if (t >= wend) {
@@ -893,7 +941,7 @@ struct ScanColAcc {
         const bool outlier = fabsf(z) > clip;
         if (zdot && !outlier && iv != 0.0F) {
             const double sk = s_keep_d[t];
-            zs.n += 1.0;
+            ++zn; // the count, exact as an integer (stored as a double)
             zs.sz += z;
             zs.ss += sk;
             zs.sss += sk * sk;
@@ -911,8 +959,11 @@ struct ScanColAcc {
         const uint64_t o = k * d->nchans + c;
         cmin_out[o]      = cmin;
         cmax_out[o]      = cmax;
-        if (zdot)
-            zs_out[o] = zs;
+        if (zdot) {
+            ZdotSums z = zs;
+            z.n        = static_cast<double>(zn);
+            zs_out[o]  = z;
+        }
         if (kchan) {
             kp_out[o] = kpos.widen();
             kn_out[o] = kneg.widen();
