@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 
 #include <cuda_runtime.h>
 
@@ -1146,7 +1147,13 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
         // per-window constants and stores of the row, when nchans % 4 == 0);
         // channel indices fit 32 bits (the launcher checks)
         const uint32_t n32 = static_cast<uint32_t>(n);
-        bool dirty         = false; // a cell of this thread's needs a fill
+        // One pass over the thread's cells: classify each, then either write
+        // the row's values (STATES false: every row) or the cell states and
+        // zero-DM-corrected values the fills draw from (STATES true: only a
+        // row with a cell to fill, recomputed the same way).
+        auto cells = [&](auto states_tag) -> bool {
+        constexpr bool STATES = decltype(states_tag)::value;
+        bool dirty = false; // a cell of this thread's needs a fill
         for (uint32_t cb = threadIdx.x * V; cb < n32; cb += blockDim.x * V) {
             float xs[V], ls[V], ss[V], is[V], outv[V];
             uint8_t ms[V], ka[V];
@@ -1213,20 +1220,27 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
                         outv[e] = p.transform ? level_of(p, ls[e], ss[e], v) : x;
                     }
                 }
-                state[c] = st;
-                sv[c]    = v;
-                dirty    = dirty || st == kNarrow || st == kKadaneSpectrum || st == kKadaneChannel;
+                if constexpr (STATES) {
+                    state[c] = st;
+                    sv[c]    = v;
+                }
+                dirty = dirty || st == kNarrow || st == kKadaneSpectrum || st == kKadaneChannel;
             }
             // masked and flagged cells are (re)written below or never read
-            if constexpr (V == 4)
-                *reinterpret_cast<float4*>(out + cb) = make_float4(outv[0], outv[1], outv[2], outv[3]);
-            else
-                out[cb] = outv[0];
+            if constexpr (!STATES) {
+                if constexpr (V == 4)
+                    *reinterpret_cast<float4*>(out + cb) = make_float4(outv[0], outv[1], outv[2], outv[3]);
+                else
+                    out[cb] = outv[0];
+            }
         }
-        // a row with no cell to fill (almost every row) is done; the barrier
-        // also orders this row's shared-memory writes after the last row's reads
-        if (!__syncthreads_or(dirty))
+        return dirty;
+        };
+        // a row with no cell to fill (almost every row) is done
+        if (!__syncthreads_or(cells(std::false_type{})))
             continue;
+        cells(std::true_type{});
+        __syncthreads(); // every cell state is written before the fills read them
 
         for (uint32_t c = threadIdx.x; c < n32; c += blockDim.x) {
             const uint8_t st = state[c];
