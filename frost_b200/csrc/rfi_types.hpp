@@ -187,17 +187,20 @@ struct KadaneState32 {
         }
         last = i;
         total += u;
-        if (total > prefix.sum)
-            prefix = {total, first, i};
+        if (total > prefix.sum) { // the prefix run always starts at `first`
+            prefix.sum = total;
+            prefix.end = i;
+        }
         const double s = suffix.sum + u;
         if (s > 0.0) {
             if (suffix.end < suffix.start)
                 suffix.start = i;
             suffix.sum = s;
-            suffix.end = i;
         } else {
-            suffix = {0.0, i + 1, i};
+            suffix.sum   = 0.0;
+            suffix.start = i + 1;
         }
+        suffix.end = i;
         if (suffix.sum > best.sum)
             best = suffix;
     }
