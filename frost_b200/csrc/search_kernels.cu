@@ -1103,43 +1103,70 @@ __global__ void k_flush(SearchParams p, int64_t nrows) {
     }
 }
 
-__global__ void k_variance(const SearchRow* __restrict__ rows, const PlaneInfo* __restrict__ planes,
-                           const int64_t* __restrict__ leaf_offset,
-                           const uint16_t* __restrict__ leaf_len, int64_t nrows,
-                           const double* __restrict__ gtab, int32_t max_len, int32_t nw,
-                           const uint8_t* __restrict__ mask, const uint8_t* __restrict__ mask_or,
-                           double* __restrict__ var, float* __restrict__ inv,
-                           float* __restrict__ inv_or) {
-    const int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+// Noise tables: for every searched row and width, the sum over the row's
+// channels of the boxcar variance of a channel's leaf run (masked and
+// OR-masked). A warp per row: the lanes take every 32nd channel, each
+// accumulates its share of the sums of eight widths at a time, and the warp
+// adds the lanes' sums by a butterfly (the same terms as a sequential sum in
+// another order: within a few ulp of it).
+__global__ void __launch_bounds__(256)
+    k_variance_warp(const SearchRow* __restrict__ rows, const PlaneInfo* __restrict__ planes,
+                    const int64_t* __restrict__ leaf_offset, const uint16_t* __restrict__ leaf_len, int64_t nrows,
+                    const double* __restrict__ gtab, int32_t max_len, int32_t nw,
+                    const uint8_t* __restrict__ mask, const uint8_t* __restrict__ mask_or,
+                    double* __restrict__ var, float* __restrict__ inv, float* __restrict__ inv_or) {
+    const int lane  = threadIdx.x & 31;
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (g >= nrows)
-        return;
+        return; // the whole warp
     const SearchRow r   = rows[g];
     const PlaneInfo pl  = planes[r.plane];
     const int32_t nch   = static_cast<int32_t>(pl.chan_end - pl.chan_begin);
     const uint16_t* len = leaf_len + leaf_offset[g];
-    double v[kMaxWidths], vo[kMaxWidths];
-    for (int w = 0; w < nw; ++w) {
-        v[w]  = 0.0;
-        vo[w] = 0.0;
-    }
-    for (int32_t c = 0; c < nch; ++c) {
-        const int L     = min(static_cast<int>(len[c]), max_len);
-        const bool on   = mask[pl.chan_begin + c] != 0;
-        const bool on_o = mask_or[pl.chan_begin + c] != 0;
-        if (!on && !on_o)
-            continue;
-        const double* gt = gtab + static_cast<int64_t>(L) * nw;
-        for (int w = 0; w < nw; ++w) {
-            if (on)
-                v[w] += gt[w];
-            if (on_o)
-                vo[w] += gt[w];
+    constexpr int kW = 8;
+    for (int w0 = 0; w0 < nw; w0 += kW) {
+        double v[kW], vo[kW];
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            v[j]  = 0.0;
+            vo[j] = 0.0;
         }
-    }
-    for (int w = 0; w < nw; ++w) {
-        var[g * nw + w]    = v[w];
-        inv[g * nw + w]    = v[w] > 0.0 ? static_cast<float>(1.0 / sqrt(v[w])) : 0.0F;
-        inv_or[g * nw + w] = vo[w] > 0.0 ? static_cast<float>(1.0 / sqrt(vo[w])) : 0.0F;
+        for (int32_t c = lane; c < nch; c += 32) {
+            const bool on   = mask[pl.chan_begin + c] != 0;
+            const bool on_o = mask_or[pl.chan_begin + c] != 0;
+            if (!on && !on_o)
+                continue;
+            const int L      = min(static_cast<int>(len[c]), max_len);
+            const double* gt = gtab + static_cast<int64_t>(L) * nw + w0;
+#pragma unroll
+            for (int j = 0; j < kW; ++j) {
+                if (w0 + j < nw) {
+                    const double x = gt[j];
+                    if (on)
+                        v[j] += x;
+                    if (on_o)
+                        vo[j] += x;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            for (int o = 16; o > 0; o >>= 1) {
+                v[j] += __shfl_xor_sync(0xFFFFFFFFU, v[j], o);
+                vo[j] += __shfl_xor_sync(0xFFFFFFFFU, vo[j], o);
+            }
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < kW; ++j) {
+                const int w = w0 + j;
+                if (w < nw) {
+                    var[g * nw + w]    = v[j];
+                    inv[g * nw + w]    = v[j] > 0.0 ? static_cast<float>(1.0 / sqrt(v[j])) : 0.0F;
+                    inv_or[g * nw + w] = vo[j] > 0.0 ? static_cast<float>(1.0 / sqrt(vo[j])) : 0.0F;
+                }
+            }
+        }
     }
 }
 
@@ -1253,7 +1280,7 @@ void launch_variance(const SearchRow* rows, const PlaneInfo* planes, const int64
         return;
     if (nwidths > kMaxWidths)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "variance: more than 32 boxcar widths");
-    k_variance<<<static_cast<unsigned>((nrows + 127) / 128), 128, 0, s>>>(
+    k_variance_warp<<<static_cast<unsigned>((nrows + 7) / 8), 256, 0, s>>>(
         rows, planes, leaf_offset, leaf_len, nrows, gtab, max_len, nwidths, mask, mask_or, var,
         inv_sigma, inv_sigma_or);
     FB_LAUNCH_CHECK();
