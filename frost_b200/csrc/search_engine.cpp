@@ -9,6 +9,7 @@
 #include <string>
 
 #include "dedisp.hpp"
+#include "postprocess_kernels.hpp"
 
 namespace fb::fdmt {
 
@@ -21,6 +22,19 @@ template <class T> void upload(DeviceBuffer& b, const std::vector<T>& v, cudaStr
 }
 
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Bits that hold every value 0..v.
+int bits_of(uint64_t v) {
+    int b = 0;
+    while (v != 0) {
+        ++b;
+        v >>= 1;
+    }
+    return b;
+}
+
+// Digit histograms of the candidate radix sort for up to n keys.
+SizeType sort_hist_bytes(SizeType n) { return 256 * ((n + pp::kTile - 1) / pp::kTile) * sizeof(uint32_t); }
 
 PlanConfig plan_config(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc) {
     float f_min = 0, f_max = 0;
@@ -152,6 +166,26 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     m_row_counts.reserve(std::max<SizeType>(m_nsearch * sizeof(uint32_t), 16));
     const SizeType maxc = std::max<uint64_t>(bc.max_candidates, 1);
     m_cands.reserve(maxc * sizeof(frost_candidate));
+    for (int i = 0; i < 2; ++i) {
+        m_sort_keys[i].reserve(maxc * sizeof(uint64_t));
+        m_sort_vals[i].reserve(maxc * sizeof(uint32_t));
+    }
+    m_sort_hist.reserve(sort_hist_bytes(maxc));
+    m_cands_sorted.reserve(maxc * sizeof(frost_candidate));
+    m_cand_range.reserve(2 * sizeof(unsigned long long));
+    {
+        uint32_t max_level = 0, max_idx = 0, max_dm = 0;
+        for (const PlaneInfo& pi : pinfo) {
+            max_level = std::max(max_level, pi.subband_level);
+            max_idx   = std::max(max_idx, pi.subband_idx);
+        }
+        for (const auto& p : planes)
+            max_dm = std::max<uint32_t>(max_dm, static_cast<uint32_t>(std::max<size_t>(p.delay.size(), 1) - 1));
+        m_key_level_bits  = bits_of(max_level);
+        m_key_idx_bits    = bits_of(max_idx);
+        m_key_dm_bits     = bits_of(max_dm);
+        m_key_filter_bits = bits_of(static_cast<uint64_t>(std::max<SizeType>(nw, 1) - 1));
+    }
     m_counters.reserve(4 * sizeof(unsigned long long));
     m_clock.reserve(sizeof(GulpClock));
     m_clock_h.reserve(sizeof(GulpClock));
@@ -241,7 +275,13 @@ Engine::Footprint Engine::estimate(const frost_dedisp_plan_config& dd, const fro
                     nsearch * nw * (sizeof(double) + 2 * sizeof(float)) + b16(nsearch * nruns * sizeof(RunState)) +
                     b16(nsearch * sizeof(uint32_t)) + 4 * sizeof(unsigned long long) + sizeof(GulpClock) +
                     sizeof(unsigned long long) + 2 * static_cast<SizeType>(C);
-    f.candidate_bytes = std::max<SizeType>(bc.max_candidates, 1) * sizeof(frost_candidate);
+    {
+        const SizeType maxc = std::max<SizeType>(bc.max_candidates, 1);
+        // detections, their sorted copy, the sort's keys and positions
+        // (two of each), its histograms and the peak range
+        f.candidate_bytes = maxc * (2 * sizeof(frost_candidate) + 2 * sizeof(uint64_t) + 2 * sizeof(uint32_t)) +
+                            sort_hist_bytes(maxc) + 2 * sizeof(unsigned long long);
+    }
     // level buffers and histories of the fused and single-level schedules
     int64_t tile = bc.tile_nsamps != 0 ? static_cast<int64_t>(bc.tile_nsamps) : static_cast<int64_t>(dd.block_nsamps);
     tile                = round_up(std::min<int64_t>(tile, static_cast<int64_t>(dd.block_nsamps)), kTileQuantum);
@@ -738,7 +778,8 @@ SizeType Engine::plan_bytes(int64_t tile) const {
         bytes += static_cast<SizeType>(m_plan.level_rows(h)) * m_hist_len[h] * es;
     bytes += 2 * static_cast<SizeType>(m_plan.nchans()) * m_plan.level_history(0) * sizeof(float);
     bytes += m_leaf_len.bytes() + m_rows.bytes() + m_var.bytes() + m_inv.bytes() * 2 +
-             m_carry.bytes() + m_cands.bytes() + m_row_ops.bytes() + m_leaf_ops.bytes();
+             m_carry.bytes() + m_cands.bytes() + m_row_ops.bytes() + m_leaf_ops.bytes() +
+             m_cands_sorted.bytes() + m_sort_keys[0].bytes() * 2 + m_sort_vals[0].bytes() * 2 + m_sort_hist.bytes();
     return bytes;
 }
 
@@ -783,7 +824,9 @@ SizeType Engine::device_bytes() const {
                                   &m_node_first_op_d, &m_row_ops, &m_fused_ops, &m_rows, &m_planes,
                                   &m_widths, &m_leaf_len, &m_leaf_offset, &m_gtab, &m_var, &m_inv,
                                   &m_inv_or, &m_mask_d, &m_mask_or_d, &m_carry, &m_row_counts, &m_cands,
-                                  &m_counters, &m_clock, &m_frontier, &m_capture_rows};
+                                  &m_counters, &m_clock, &m_frontier, &m_capture_rows,
+                                  &m_sort_keys[0], &m_sort_keys[1], &m_sort_vals[0], &m_sort_vals[1],
+                                  &m_sort_hist, &m_cands_sorted, &m_cand_range};
     for (const auto* b : rest)
         total += b->bytes();
     for (const auto& b : m_capture)
@@ -1017,19 +1060,46 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
 }
 
 void Engine::collect(cudaStream_t s) {
-    unsigned long long counters[4];
-    FB_CUDA(cudaMemcpyAsync(counters, m_counters.get(), sizeof(counters), cudaMemcpyDeviceToHost, s));
+    const uint64_t cap = std::max<uint64_t>(m_cfg.max_candidates, 1);
+    const frost_candidate* cands = m_cands.as<frost_candidate>();
+    launch_cand_range(cands, m_counters.as<unsigned long long>(), cap, m_cand_range.as<unsigned long long>(), s);
+    m_launches += 1;
+    unsigned long long counters[6];
+    FB_CUDA(cudaMemcpyAsync(counters, m_counters.get(), 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaMemcpyAsync(counters + 4, m_cand_range.get(), 2 * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, s));
     FB_CUDA(cudaStreamSynchronize(s));
     if (counters[3] != 0)
         throw Error(FROST_ERR_TIMEOUT, "search: a level or search kernel's bounded wait for its bulk copies ran "
                                        "out; this call's results are incomplete");
-    const uint64_t n = std::min<uint64_t>(counters[0], m_cfg.max_candidates);
+    const uint64_t n = std::min<uint64_t>(counters[0], cap);
     m_results.resize(n);
-    if (n)
-        FB_CUDA(cudaMemcpy(m_results.data(), m_cands.get(), n * sizeof(frost_candidate),
-                           cudaMemcpyDeviceToHost));
     m_dropped_global = counters[1];
     m_dropped_per_dm = counters[2];
+    if (n == 0)
+        return;
+    // Order (level, sub-band, DM row, peak, width): one packed key when the
+    // fields fit in 64 bits (always for real plans: the peaks of one call
+    // span about a gulp), else a comparison sort on the host.
+    const int peak_bits = bits_of(counters[5] - counters[4]);
+    const int key_bits  = m_key_level_bits + m_key_idx_bits + m_key_dm_bits + peak_bits + m_key_filter_bits;
+    if (n >= 2 && key_bits <= 64) {
+        const CandKeySpec spec{counters[4], m_key_idx_bits, m_key_dm_bits, peak_bits, m_key_filter_bits};
+        uint64_t* keys     = m_sort_keys[0].as<uint64_t>();
+        uint64_t* keys_alt = m_sort_keys[1].as<uint64_t>();
+        uint32_t* vals     = m_sort_vals[0].as<uint32_t>();
+        uint32_t* vals_alt = m_sort_vals[1].as<uint32_t>();
+        launch_cand_keys(cands, n, spec, keys, vals, s);
+        pp::radix_sort(keys, vals, keys_alt, vals_alt, n, key_bits, m_sort_hist.as<uint32_t>(), s);
+        launch_cand_gather(cands, vals, n, m_cands_sorted.as<frost_candidate>(), s);
+        m_launches += 2 + 3 * static_cast<uint64_t>((key_bits + 7) / 8);
+        FB_CUDA(cudaMemcpyAsync(m_results.data(), m_cands_sorted.get(), n * sizeof(frost_candidate),
+                                cudaMemcpyDeviceToHost, s));
+        FB_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    FB_CUDA(cudaMemcpyAsync(m_results.data(), cands, n * sizeof(frost_candidate), cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
     std::sort(m_results.begin(), m_results.end(), [](const frost_candidate& a, const frost_candidate& b) {
         if (a.subband_level != b.subband_level)
             return a.subband_level < b.subband_level;

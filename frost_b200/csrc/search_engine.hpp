@@ -131,6 +131,11 @@ private:
     DeviceBuffer m_leaf_ops, m_node_first_op_d, m_row_ops, m_rows, m_planes, m_widths, m_leaf_len,
         m_leaf_offset, m_gtab, m_var, m_inv, m_inv_or, m_mask_d, m_mask_or_d, m_carry,
         m_row_counts, m_cands, m_counters, m_frontier, m_capture_rows;
+    // Candidate ordering: packed keys and their positions (ping-ponged by
+    // the radix sort), its digit histograms, the sorted copy and the
+    // smallest / largest peak sample of a call.
+    DeviceBuffer m_sort_keys[2], m_sort_vals[2], m_sort_hist, m_cands_sorted, m_cand_range;
+    int m_key_level_bits = 0, m_key_idx_bits = 0, m_key_dm_bits = 0, m_key_filter_bits = 0;
     std::vector<int64_t> m_row_op_offset;
     /** One FDMT step: level `out` from level `in` = out - 1 (single) or
      * out - 2 (fused: the level between is never stored). Step 0 is level 1

@@ -1293,4 +1293,102 @@ void launch_flush_runs(const SearchParams& p, int64_t nrows, cudaStream_t s) {
     FB_LAUNCH_CHECK();
 }
 
+// ---- candidate ordering ------------------------------------------------------
+//
+// The search kernels append detections in whatever order their CTAs reach
+// them; results are returned sorted by (sub-band level, sub-band, DM row,
+// peak sample, width). The five fields pack into one 64-bit key (field
+// widths from the plan, the peak relative to the smallest peak of the
+// call), so the order is a stable radix sort of the keys followed by a
+// gather.
+
+namespace {
+
+__global__ void __launch_bounds__(256)
+    k_cand_range(const frost_candidate* __restrict__ c, const unsigned long long* __restrict__ count,
+                 uint64_t cap, unsigned long long* __restrict__ range) {
+    const uint64_t n = min(static_cast<uint64_t>(*count), cap);
+    unsigned long long lo = ~0ULL, hi = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long p = c[i].peak_sample;
+        lo = p < lo ? p : lo;
+        hi = p > hi ? p : hi;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long l2 = __shfl_xor_sync(0xFFFFFFFFU, lo, o);
+        const unsigned long long h2 = __shfl_xor_sync(0xFFFFFFFFU, hi, o);
+        lo = l2 < lo ? l2 : lo;
+        hi = h2 > hi ? h2 : hi;
+    }
+    __shared__ unsigned long long s_lo[8], s_hi[8];
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        s_lo[warp] = lo;
+        s_hi[warp] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) {
+            lo = s_lo[w] < lo ? s_lo[w] : lo;
+            hi = s_hi[w] > hi ? s_hi[w] : hi;
+        }
+        if (lo <= hi) {
+            atomicMin(&range[0], lo);
+            atomicMax(&range[1], hi);
+        }
+    }
+}
+
+__global__ void k_cand_keys(const frost_candidate* __restrict__ c, uint64_t n, CandKeySpec k,
+                            uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n)
+        return;
+    const frost_candidate& x = c[i];
+    uint64_t key             = x.subband_level;
+    key                      = (key << k.idx_bits) | x.subband_idx;
+    key                      = (key << k.dm_bits) | x.dm_idx;
+    key                      = (key << k.peak_bits) | (x.peak_sample - k.peak_base);
+    key                      = (key << k.filter_bits) | x.filter_idx;
+    keys[i]                  = key;
+    idx[i]                   = static_cast<uint32_t>(i);
+}
+
+__global__ void k_cand_gather(const frost_candidate* __restrict__ c, const uint32_t* __restrict__ perm,
+                              uint64_t n, frost_candidate* __restrict__ out) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i < n)
+        out[i] = c[perm[i]];
+}
+
+unsigned blocks256(uint64_t n) { return static_cast<unsigned>((n + 255) / 256); }
+
+} // namespace
+
+void launch_cand_range(const frost_candidate* c, const unsigned long long* count, uint64_t cap,
+                       unsigned long long* range, cudaStream_t s) {
+    FB_CUDA(cudaMemsetAsync(range, 0xFF, sizeof(unsigned long long), s));
+    FB_CUDA(cudaMemsetAsync(range + 1, 0, sizeof(unsigned long long), s));
+    const uint64_t grid = std::min<uint64_t>(blocks256(cap), 4 * 148);
+    k_cand_range<<<static_cast<unsigned>(grid), 256, 0, s>>>(c, count, cap, range);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_cand_keys(const frost_candidate* c, uint64_t n, const CandKeySpec& k, uint64_t* keys,
+                      uint32_t* idx, cudaStream_t s) {
+    if (n == 0)
+        return;
+    k_cand_keys<<<blocks256(n), 256, 0, s>>>(c, n, k, keys, idx);
+    FB_LAUNCH_CHECK();
+}
+
+void launch_cand_gather(const frost_candidate* c, const uint32_t* perm, uint64_t n, frost_candidate* out,
+                        cudaStream_t s) {
+    if (n == 0)
+        return;
+    k_cand_gather<<<blocks256(n), 256, 0, s>>>(c, perm, n, out);
+    FB_LAUNCH_CHECK();
+}
+
 } // namespace fb::fdmt

@@ -129,4 +129,22 @@ void launch_variance(const SearchRow* rows, const PlaneInfo* planes, const int64
 /** Emits every open run as a candidate and closes it (drain). */
 void launch_flush_runs(const SearchParams& p, int64_t nrows, cudaStream_t s);
 
+/** Bit widths of the packed candidate order key (level, sub-band, DM row,
+ * peak - peak_base, width index; most significant first). */
+struct CandKeySpec {
+    uint64_t peak_base;
+    int idx_bits, dm_bits, peak_bits, filter_bits;
+};
+
+/** range[0] = smallest, range[1] = largest peak sample of the first
+ * min(*count, cap) candidates (~0 and 0 when there are none). */
+void launch_cand_range(const frost_candidate* c, const unsigned long long* count, uint64_t cap,
+                       unsigned long long* range, cudaStream_t s);
+/** keys[i] = packed order key of c[i], idx[i] = i. */
+void launch_cand_keys(const frost_candidate* c, uint64_t n, const CandKeySpec& k, uint64_t* keys,
+                      uint32_t* idx, cudaStream_t s);
+/** out[i] = c[perm[i]]. */
+void launch_cand_gather(const frost_candidate* c, const uint32_t* perm, uint64_t n, frost_candidate* out,
+                        cudaStream_t s);
+
 } // namespace fb::fdmt
