@@ -84,6 +84,8 @@ SIGNATURES = {
     "frost_search_set_launch_shape": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "frost_search_set_residency": (C.c_int, [_vp, C.c_int]),
     "frost_search_get_residency": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "frost_search_set_fused_search": (C.c_int, [_vp, C.c_int]),
+    "frost_search_get_fused_search": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "frost_search_get_launch_shape": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                                 C.POINTER(C.c_int)]),
     "frost_search_enable_timing": (C.c_int, [_vp, C.c_int]),

@@ -776,6 +776,22 @@ int frost_search_get_residency(const frost_search* s, int* ctas_per_sm) {
     });
 }
 
+int frost_search_set_fused_search(frost_search* s, int on) {
+    return guarded([&] {
+        if (s == nullptr)
+            invalid("frost_search_set_fused_search: null handle");
+        s->impl.set_fused_search(on != 0);
+    });
+}
+
+int frost_search_get_fused_search(const frost_search* s, int* on) {
+    return guarded([&] {
+        if (s == nullptr || on == nullptr)
+            invalid("frost_search_get_fused_search: null argument");
+        *on = s->impl.fused_search_on() ? 1 : 0;
+    });
+}
+
 int frost_search_set_wait_limit(frost_search* s, int64_t tries) {
     return guarded([&] {
         if (s == nullptr)

@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kThreads)
         const int32_t in_base = G.in_base, out_base = G.out_base;
         unsigned* err          = G.err;
         const int64_t local    = item - sbeg;
-        const int64_t r        = local % G.nrows;
+        const int64_t r        = G.rows != nullptr ? G.rows[local % G.nrows] : local % G.nrows;
         const RowOp op         = ops[r];
         const int tile0        = static_cast<int>(local / G.nrows) * G.tpc;
         const int nt           = min(G.tpc, G.ntiles - tile0);
@@ -741,7 +741,8 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
 }
 
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
-                  unsigned* err, cudaStream_t s, int32_t tpc, int32_t ctas, long long wait_limit) {
+                  unsigned* err, cudaStream_t s, int32_t tpc, int32_t ctas, long long wait_limit,
+                  const int32_t* row_map) {
     if (nrows == 0)
         return;
     if (ncols % kTimePerCta != 0 || in.base % 8 != 0 || in.pitch % 8 != 0 || out.base % 8 != 0 ||
@@ -750,6 +751,8 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
     const int ntiles = ncols / kTimePerCta;
     if (tpc < 1 || tpc > 128)
         throw Error(FROST_ERR_INTERNAL, "level: tiles per CTA must be in [1, 128]");
+    if (err == nullptr && row_map != nullptr)
+        throw Error(FROST_ERR_INTERNAL, "level: a row map needs the pipelined kernel");
     if (err == nullptr) {
         // direct form (no bulk copies): one CTA per (row, tile)
         const dim3 grid(static_cast<unsigned>(nrows), static_cast<unsigned>(ntiles));
@@ -764,20 +767,20 @@ void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, 
         FB_LAUNCH_CHECK();
         return;
     }
-    LevelSeg g{ops, in.data, out.data, in.pitch, out.pitch, in.base, out.base, ntiles, tpc, nrows, 0, err};
+    LevelSeg g{ops, in.data, out.data, in.pitch, out.pitch, in.base, out.base, ntiles, tpc, nrows, 0, err, row_map};
     launch_level_segs(&g, 1, false, out.fp16 != 0, 0, s, ctas, wait_limit);
 }
 
 namespace {
 
 template <int K>
-LevelSegTable<K> seg_table(LevelSeg* segs, int n, int64_t* total) {
+LevelSegTable<K> seg_table(LevelSeg* segs, int n, int64_t* total, bool fused) {
     LevelSegTable<K> t{};
     t.n       = n;
     int64_t e = 0;
     for (int i = 0; i < n; ++i) {
         LevelSeg& g = segs[i];
-        if (g.tpc < 1 || g.tpc > 128 || g.ntiles < 1 || g.nrows < 1 || g.err == nullptr ||
+        if (g.tpc < 1 || g.tpc > 128 || g.ntiles < 1 || g.nrows < 1 || g.err == nullptr || (fused && g.rows) ||
             g.in_base % 8 != 0 || g.in_pitch % 8 != 0 || g.out_base % 8 != 0 || g.out_pitch % 8 != 0)
             throw Error(FROST_ERR_INTERNAL, "level: bad segment geometry");
         e += g.nrows * ((g.ntiles + g.tpc - 1) / g.tpc);
@@ -821,7 +824,7 @@ template <int K>
 void launch_table(LevelSeg* segs, int n, bool fused, bool fp16, int32_t stages, cudaStream_t s, int32_t ctas,
                   long long wait_limit) {
     int64_t total = 0;
-    const LevelSegTable<K> t = seg_table<K>(segs, n, &total);
+    const LevelSegTable<K> t = seg_table<K>(segs, n, &total, fused);
     if (fp16)
         level_go<__half, K>(t, total, fused, stages, s, ctas, wait_limit);
     else

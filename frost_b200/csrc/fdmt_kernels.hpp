@@ -39,6 +39,9 @@ struct LevelSeg {
     int64_t nrows;
     int64_t item_end;
     unsigned* err;
+    // single levels: output rows rows[0 .. nrows) of the level (their ops
+    // ops[rows[i]]); nullptr: rows 0 .. nrows - 1
+    const int32_t* rows;
 };
 constexpr int kMaxLevelSegs = 48;
 template <int K> struct LevelSegTable {
@@ -63,13 +66,14 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
                    int64_t t0, int32_t n_valid, const float* input_hist, int32_t hist_len,
                    LevelView out, int32_t ncols, cudaStream_t s, int32_t ctas = 0);
 
-/** Level h >= 2: out[row] = in[lo] + in[hi] shifted. With `err` non-null
+/** Level h >= 2: out[row] = in[lo] + in[hi] shifted (only the rows
+ * row_map[0 .. nrows) when a map is given; the pipelined kernel only). With `err` non-null
  * the TMA-pipelined kernel runs (each CTA takes `tiles_per_cta` tiles of
  * 2048 columns) and sets *err if a bounded wait ran out; with `err` null
  * the direct (one CTA per row and tile) kernel runs. */
 void launch_level(const RowOp* ops, int64_t nrows, LevelView in, LevelView out, int32_t ncols,
                   unsigned* err, cudaStream_t s, int32_t tiles_per_cta = 16, int32_t ctas = 0,
-                  long long wait_limit = kDefaultWaitLimit);
+                  long long wait_limit = kDefaultWaitLimit, const int32_t* row_map = nullptr);
 
 /** A row of level h+1 from four rows of level h-1: the sum of row[j] read at
  * t - shift[j] (shift[0] = 0), grouped (row0 + row1) + (row2 + row3); a

@@ -33,6 +33,22 @@ int bits_of(uint64_t v) {
     return b;
 }
 
+// Rows of level h that no plane searches (ascending): with the single
+// level step into h fused with the search, the level kernel computes only
+// these.
+std::vector<int32_t> unsearched_rows(const Plan& plan, int h) {
+    std::vector<char> searched(static_cast<size_t>(plan.level_rows(h)), 0);
+    for (const auto& p : plan.planes())
+        if (p.height == h)
+            for (const auto r : p.level_row)
+                searched[static_cast<size_t>(r)] = 1;
+    std::vector<int32_t> out;
+    for (size_t r = 0; r < searched.size(); ++r)
+        if (searched[r] == 0)
+            out.push_back(static_cast<int32_t>(r));
+    return out;
+}
+
 // Digit histograms of the candidate radix sort for up to n keys.
 SizeType sort_hist_bytes(SizeType n) { return 256 * ((n + pp::kTile - 1) / pp::kTile) * sizeof(uint32_t); }
 
@@ -147,6 +163,33 @@ Engine::Engine(const frost_dedisp_plan_config& dd, const frost_boxcar_config& bc
     upload(m_leaf_offset, leaf_off, s);
     upload(m_widths, m_plan.widths(), s);
 
+    // Single level steps fused with the search: the op of every searched
+    // row's level row, and per searched height the rows no plane searches.
+    {
+        std::vector<RowOp> fs_ops(m_nsearch, RowOp{0, -1, 0, 0});
+        for (SizeType g = 0; g < m_nsearch; ++g) {
+            const int h = planes[static_cast<size_t>(rows[g].plane)].height;
+            if (h >= 2)
+                fs_ops[g] = m_plan.row_ops(h)[static_cast<size_t>(rows[g].level_row)];
+        }
+        upload(m_fs_ops, fs_ops, s);
+        std::vector<int32_t> fs_rows;
+        m_fs_rows_off.assign(L + 1, 0);
+        m_fs_rows_n.assign(L + 1, 0);
+        for (int h = 2; h <= L; ++h) {
+            if (m_height_g1[h] <= m_height_g0[h])
+                continue;
+            const auto r     = unsearched_rows(m_plan, h);
+            m_fs_rows_off[h] = static_cast<int64_t>(fs_rows.size());
+            m_fs_rows_n[h]   = static_cast<int64_t>(r.size());
+            fs_rows.insert(fs_rows.end(), r.begin(), r.end());
+        }
+        upload(m_fs_rows, fs_rows, s);
+        // on by default for fp16 storage; fp32 doubles the staged children,
+        // and the fused search then holds fewer CTAs an SM than it saves
+        m_fs_on = m_fp16;
+    }
+
     // Window-box variance table g[L][w].
     m_max_len          = m_plan.max_leaf_length();
     const auto& widths = m_plan.widths();
@@ -259,18 +302,22 @@ Engine::Footprint Engine::estimate(const frost_dedisp_plan_config& dd, const fro
         row_op_offset[h] = static_cast<int64_t>(nrow_ops);
         nrow_ops += plan.row_ops(h).size();
     }
-    SizeType nsearch = 0, nleaf = 0;
+    SizeType nsearch = 0, nleaf = 0, nfs_rows = 0;
     std::vector<char> searched(L + 1, 0);
     for (const auto& p : plan.planes()) {
         nsearch += p.delay.size();
         nleaf += p.delay.size() * static_cast<SizeType>(p.chan_end - p.chan_begin);
         searched[p.height] = 1;
     }
+    for (int h = 2; h <= L; ++h)
+        if (searched[h])
+            nfs_rows += unsearched_rows(plan, h).size();
     const SizeType nruns = bc.peak_mode == FROST_PEAK_ACROSS_WIDTHS ? 1 : nw;
     f.table_bytes = b16(leaf.size() * sizeof(LeafOp)) + b16((nodes + 1) * sizeof(int32_t)) +
                     b16(nrow_ops * sizeof(RowOp)) + b16(nsearch * sizeof(SearchRow)) +
                     b16(plan.planes().size() * sizeof(PlaneInfo)) + b16(nleaf * sizeof(uint16_t)) +
                     b16(nsearch * sizeof(int64_t)) + b16(nw * sizeof(int32_t)) +
+                    b16(nsearch * sizeof(RowOp)) + b16(nfs_rows * sizeof(int32_t)) +
                     b16((static_cast<SizeType>(plan.max_leaf_length()) + 1) * nw * sizeof(double)) +
                     nsearch * nw * (sizeof(double) + 2 * sizeof(float)) + b16(nsearch * nruns * sizeof(RunState)) +
                     b16(nsearch * sizeof(uint32_t)) + 4 * sizeof(unsigned long long) + sizeof(GulpClock) +
@@ -409,7 +456,8 @@ Engine::Tuned Engine::autotune() {
     m_timing_on           = false;
     cudaStream_t s = m_stream;
     std::string key = std::to_string(m_plan.nchans()) + "|" + std::to_string(m_ncols) + "|" +
-                      std::to_string(m_fp16) + "|" + std::to_string(m_plan.widths().back());
+                      std::to_string(m_fp16) + "|" + std::to_string(m_plan.widths().back()) + "|" +
+                      std::to_string(m_fs_on);
     for (int h = 1; h <= m_plan.levels(); ++h)
         key += "|" + std::to_string(m_plan.level_rows(h));
     for (const auto& p : m_plan.planes())
@@ -518,6 +566,17 @@ void Engine::set_residency(int32_t ctas_per_sm) {
     m_ctas_per_sm = ctas_per_sm;
 }
 
+void Engine::set_fused_search(bool on) {
+    DeviceGuard g(m_device);
+    FB_CUDA(cudaStreamSynchronize(m_stream));
+    if (m_graph != nullptr) {
+        // the captured launches follow the old schedule
+        FB_CUDA(cudaGraphExecDestroy(m_graph));
+        m_graph = nullptr;
+    }
+    m_fs_on = on;
+}
+
 void Engine::set_wait_limit(long long tries) {
     DeviceGuard g(m_device);
     FB_CUDA(cudaStreamSynchronize(m_stream));
@@ -609,7 +668,8 @@ int Engine::batch_pre(int64_t round, cudaStream_t s, RoundWork& w) {
                                   m_level_tpc,
                                   static_cast<int64_t>(m_plan.level_rows(st.out)),
                                   0,
-                                  err};
+                                  err,
+                                  nullptr};
     m_launches += 1;
     return 0;
 }
@@ -826,7 +886,7 @@ SizeType Engine::device_bytes() const {
                                   &m_inv_or, &m_mask_d, &m_mask_or_d, &m_carry, &m_row_counts, &m_cands,
                                   &m_counters, &m_clock, &m_frontier, &m_capture_rows,
                                   &m_sort_keys[0], &m_sort_keys[1], &m_sort_vals[0], &m_sort_vals[1],
-                                  &m_sort_hist, &m_cands_sorted, &m_cand_range};
+                                  &m_sort_hist, &m_cands_sorted, &m_cand_range, &m_fs_ops, &m_fs_rows};
     for (const auto* b : rest)
         total += b->bytes();
     for (const auto& b : m_capture)
@@ -1007,6 +1067,19 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                 m_timing.algorithmic_level1_bytes +=
                     static_cast<uint64_t>(C) * m_ncols * sizeof(float) +
                     static_cast<uint64_t>(m_plan.level_rows(1)) * m_ncols * es;
+            } else if (fused_search(st)) {
+                // only the rows no plane searches; the search computes the rest
+                const int64_t n = m_fs_rows_n[h];
+                if (n > 0) {
+                    timed(kLevel, s, [&] {
+                        launch_level(m_row_ops.as<RowOp>() + st.op_offset, n, view(st.in), out,
+                                     static_cast<int32_t>(m_ncols), err, s, m_level_tpc, cta_cap(), m_wait_limit,
+                                     m_fs_rows.as<int32_t>() + m_fs_rows_off[h]);
+                    });
+                    m_launches += 1;
+                    m_timing.level_launches += 1;
+                    m_timing.algorithmic_level_bytes += static_cast<uint64_t>(3 * n) * m_ncols * es;
+                }
             } else {
                 timed(kLevel, s, [&] {
                     if (st.fused)
@@ -1027,12 +1100,21 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                 launch_load_history(out, m_plan.level_rows(h), m_hist_len[h], m_hist[h].get(), s);
             });
             if (m_height_g1[h] > m_height_g0[h]) {
-                timed(kSearch, s,
-                      [&] { launch_search(sp, out, m_height_g0[h], m_height_g1[h], s, m_search_chunk, cta_cap()); });
+                const bool fs   = si > 0 && fused_search(st);
+                const int64_t g = m_height_g1[h] - m_height_g0[h];
+                timed(kSearch, s, [&] {
+                    if (fs)
+                        launch_search_fused(sp, view(st.in), out, m_fs_ops.as<RowOp>(), m_height_g0[h],
+                                            m_height_g1[h], s, m_search_chunk, cta_cap());
+                    else
+                        launch_search(sp, out, m_height_g0[h], m_height_g1[h], s, m_search_chunk, cta_cap());
+                });
                 m_launches += 1;
                 m_timing.search_launches += 1;
+                // fused: the searched rows' children (at most two rows each) are
+                // read and the rows written, instead of the rows read
                 m_timing.algorithmic_search_bytes +=
-                    static_cast<uint64_t>(m_height_g1[h] - m_height_g0[h]) * m_ncols * es;
+                    static_cast<uint64_t>(fs ? 3 * g : g) * m_ncols * es;
                 if (m_capture_on) {
                     for (size_t p = 0; p < planes.size(); ++p) {
                         if (planes[p].height != h)

@@ -135,6 +135,12 @@ private:
     // the radix sort), its digit histograms, the sorted copy and the
     // smallest / largest peak sample of a call.
     DeviceBuffer m_sort_keys[2], m_sort_vals[2], m_sort_hist, m_cands_sorted, m_cand_range;
+    // Single level steps fused with the search of their level: the RowOp of
+    // each searched row [g], and per height the rows the level kernel still
+    // computes (m_fs_rows[m_fs_rows_off[h] ..][m_fs_rows_n[h]]).
+    DeviceBuffer m_fs_ops, m_fs_rows;
+    std::vector<int64_t> m_fs_rows_off, m_fs_rows_n;
+    bool m_fs_on = false; // set for fp16 storage by the constructor
     int m_key_level_bits = 0, m_key_idx_bits = 0, m_key_dm_bits = 0, m_key_filter_bits = 0;
     std::vector<int64_t> m_row_op_offset;
     /** One FDMT step: level `out` from level `in` = out - 1 (single) or
@@ -146,6 +152,11 @@ private:
         int64_t op_offset; // into m_row_ops (single) or m_fused_ops (fused)
     };
     std::vector<Step> m_steps;
+    /** The step's level is searched in the same pass (fused single step). */
+    bool fused_search(const Step& st) const {
+        return m_fs_on && !st.fused && st.out >= 2 && m_height_g1[st.out] > m_height_g0[st.out] &&
+               search_halo(m_plan.widths().back()) <= m_search_chunk;
+    }
     std::vector<int> m_buf_of;         // level -> level buffer (-1: not stored)
     std::vector<int32_t> m_hist_len;   // level -> history columns kept
     struct Schedule {
@@ -188,6 +199,10 @@ private:
      * beams' kernels overlap); results do not depend on it. */
     void set_residency(int32_t ctas_per_sm);
     int32_t residency() const { return m_ctas_per_sm; }
+    /** Fuses each single level step into a searched level with its search
+     * (default on; identical results). Waits for the engine's stream. */
+    void set_fused_search(bool on);
+    bool fused_search_on() const { return m_fs_on; }
 
     /** Device bytes an engine for (dd, bc) allocates, computed on the host
      * from its plan without allocating anything: level buffers (under

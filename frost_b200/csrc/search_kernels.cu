@@ -434,23 +434,45 @@ template <class S, int P> __device__ __forceinline__ void ld_cols(const S* p, fl
     }
 }
 
-// q[e] = x[0] + ... + x[e] (left to right, float) of the P staged samples
-// at `p` (16-byte aligned); fp16 samples are added with mixed-precision
-// adds (`add.rn.f32.f16`: the widening is exact, so the same bits as
-// widening first).
+// q[e] = x[0] + ... + x[e] (left to right, float) of P samples already in
+// q; xmax = the largest of them.
+template <int P> __device__ __forceinline__ void scan_floats(float (&q)[P], float& xmax) {
+    float m = q[0];
+#pragma unroll
+    for (int e = 1; e + 1 < P; e += 2)
+        m = fmax3(m, q[e], q[e + 1]);
+    if constexpr (P % 2 == 0)
+        m = fmaxf(m, q[P - 1]);
+    xmax = m;
+#pragma unroll
+    for (int e = 1; e < P; ++e)
+        q[e] += q[e - 1];
+}
+
+// The same for P fp16 samples packed in pairs (sample 2i in the low half of
+// w[i]), added with mixed-precision adds (`add.rn.f32.f16`: the widening is
+// exact, so the same bits as widening first).
+template <int P>
+__device__ __forceinline__ void scan_halves(const uint32_t (&w)[P / 2], float (&q)[P], float& xmax) {
+    // the largest sample: packed fp16 maxima (exact), then one widening
+    __half2 hm = *reinterpret_cast<const __half2*>(&w[0]);
+#pragma unroll
+    for (int i = 1; i < P / 2; ++i)
+        hm = __hmax2(hm, *reinterpret_cast<const __half2*>(&w[i]));
+    xmax = fmaxf(__low2float(hm), __high2float(hm));
+    q[0] = __half2float(__ushort_as_half(static_cast<unsigned short>(w[0] & 0xFFFFU)));
+#pragma unroll
+    for (int e = 1; e < P; ++e) {
+        const uint16_t h = static_cast<uint16_t>((e & 1) ? (w[e / 2] >> 16) : (w[e / 2] & 0xFFFFU));
+        asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(q[e]) : "h"(h), "f"(q[e - 1]));
+    }
+}
+
+// Prefix sums of the P staged samples at `p` (16-byte aligned).
 template <class S, int P> __device__ __forceinline__ void scan_cols(const S* p, float (&q)[P], float& xmax) {
     if constexpr (sizeof(S) == 4) {
         ld_cols<S, P>(p, q);
-        float m = q[0];
-#pragma unroll
-        for (int e = 1; e + 1 < P; e += 2)
-            m = fmax3(m, q[e], q[e + 1]);
-        if constexpr (P % 2 == 0)
-            m = fmaxf(m, q[P - 1]);
-        xmax = m;
-#pragma unroll
-        for (int e = 1; e < P; ++e)
-            q[e] += q[e - 1];
+        scan_floats<P>(q, xmax);
     } else {
         uint32_t w[P / 2];
 #pragma unroll
@@ -458,18 +480,90 @@ template <class S, int P> __device__ __forceinline__ void scan_cols(const S* p, 
             const uint4 u = reinterpret_cast<const uint4*>(p)[i];
             w[4 * i] = u.x, w[4 * i + 1] = u.y, w[4 * i + 2] = u.z, w[4 * i + 3] = u.w;
         }
-        // the largest sample: packed fp16 maxima (exact), then one widening
-        __half2 hm = *reinterpret_cast<const __half2*>(&w[0]);
+        scan_halves<P>(w, q, xmax);
+    }
+}
+
+// Fused level step: this thread's P columns of a searched row computed from
+// the level below, out = lo + hi shifted, bit for bit as the single-level
+// kernel computes them, stored to the row in global memory and
+// prefix-summed. `lo` is the staged unshifted child segment at the thread's
+// first column and `hi` the staged 16-byte-aligned superset of the shifted
+// child at the same place, the thread's first shifted sample `hoff`
+// elements in (hi == nullptr: the row copies its low child); both buffers
+// hold at least 16 bytes past the thread's P columns.
+// fp16: the level kernel rounds the float sum of two fp16 values with the
+// saturating convert. That float sum is exact when their exponents differ
+// by at most 12 (11-bit significands: the sum needs at most 24 bits), and
+// otherwise the smaller operand is below a quarter of the larger one's fp16
+// spacing, so that both roundings return the larger operand; the fp16 add
+// (round to nearest even of the exact sum) gives the same bits, with a
+// clamp to +-65504 for the saturation (sums past it round to infinity).
+template <class S, int P>
+__device__ __forceinline__ void merge_scan(const S* lo, const S* hi, int hoff, S* dst, float (&q)[P],
+                                           float& xmax) {
+    if constexpr (sizeof(S) == 4) {
+        ld_cols<S, P>(lo, q);
+        if (hi != nullptr) {
+            float h[P + 4];
 #pragma unroll
-        for (int i = 1; i < P / 2; ++i)
-            hm = __hmax2(hm, *reinterpret_cast<const __half2*>(&w[i]));
-        xmax = fmaxf(__low2float(hm), __high2float(hm));
-        q[0] = __half2float(__ushort_as_half(static_cast<unsigned short>(w[0] & 0xFFFFU)));
-#pragma unroll
-        for (int e = 1; e < P; ++e) {
-            const uint16_t h = static_cast<uint16_t>((e & 1) ? (w[e / 2] >> 16) : (w[e / 2] & 0xFFFFU));
-            asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(q[e]) : "h"(h), "f"(q[e - 1]));
+            for (int i = 0; i < P / 4 + 1; ++i) {
+                const float4 v = reinterpret_cast<const float4*>(hi)[i];
+                h[4 * i] = v.x, h[4 * i + 1] = v.y, h[4 * i + 2] = v.z, h[4 * i + 3] = v.w;
+            }
+            switch (hoff) {
+#define FB_SHIFTED(O)                                                                             \
+    case O:                                                                                       \
+        _Pragma("unroll") for (int e = 0; e < P; ++e) q[e] = q[e] + h[O + e];                      \
+        break;
+                FB_SHIFTED(0) FB_SHIFTED(1) FB_SHIFTED(2) FB_SHIFTED(3)
+#undef FB_SHIFTED
+            }
         }
+#pragma unroll
+        for (int i = 0; i < P / 4; ++i)
+            reinterpret_cast<float4*>(dst)[i] = make_float4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+        scan_floats<P>(q, xmax);
+    } else {
+        uint32_t w[P / 2];
+#pragma unroll
+        for (int i = 0; i < P / 8; ++i) {
+            const uint4 u = reinterpret_cast<const uint4*>(lo)[i];
+            w[4 * i] = u.x, w[4 * i + 1] = u.y, w[4 * i + 2] = u.z, w[4 * i + 3] = u.w;
+        }
+        if (hi != nullptr) {
+            uint32_t W[P / 2 + 4];
+#pragma unroll
+            for (int i = 0; i < P / 8 + 1; ++i) {
+                const uint4 u = reinterpret_cast<const uint4*>(hi)[i];
+                W[4 * i] = u.x, W[4 * i + 1] = u.y, W[4 * i + 2] = u.z, W[4 * i + 3] = u.w;
+            }
+            // the shifted pairs: whole words hoff / 2 on, shifted by a half
+            // when hoff is odd
+            const uint32_t sh = (hoff & 1) * 16U;
+            uint32_t g[P / 2];
+            switch (hoff >> 1) {
+#define FB_SHIFTED(K)                                                                             \
+    case K:                                                                                       \
+        _Pragma("unroll") for (int i = 0; i < P / 2; ++i) g[i] = __funnelshift_r(W[K + i], W[K + i + 1], sh); \
+        break;
+                FB_SHIFTED(0) FB_SHIFTED(1) FB_SHIFTED(2) FB_SHIFTED(3)
+#undef FB_SHIFTED
+            }
+            const __half2 top = __float2half2_rn(65504.0F);
+            const __half2 bot = __float2half2_rn(-65504.0F);
+#pragma unroll
+            for (int i = 0; i < P / 2; ++i) {
+                const __half2 x = __hadd2(*reinterpret_cast<const __half2*>(&w[i]),
+                                          *reinterpret_cast<const __half2*>(&g[i]));
+                const __half2 c = __hmin2(__hmax2(x, bot), top);
+                w[i]            = *reinterpret_cast<const uint32_t*>(&c);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < P / 8; ++i)
+            reinterpret_cast<uint4*>(dst)[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+        scan_halves<P>(w, q, xmax);
     }
 }
 
@@ -626,8 +720,8 @@ __device__ void scan_halo(const S* seg, int halo, int jmin, float* Q, float* gmi
         H[i] -= last;
 }
 
-template <class S, int CH, bool POW2, int K>
-__global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
+template <class S, int CH, bool POW2, bool FS, int K>
+__global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2048 ? 5 : 4))
     k_search(const __grid_constant__ SearchSegTable<K> tab) {
     // The search shape (widths, halo, peak mode, valid columns) is the same
     // in every segment; the rows, tables and outputs are each segment's.
@@ -646,6 +740,10 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
     //   bits   uint32 [nw][CH / 32]: per-width masks of the samples that fired
     //   stage  S [2][halo + CH]: the raw row segment, bulk-copied one chunk
     //          ahead (the halo columns only for the first chunk)
+    // With the level step fused (FS), the stage instead holds the row's
+    // halo columns (first chunk) and, for each of two chunks in flight, the
+    // chunk's unshifted child segment and the aligned superset of its
+    // shifted one: S [halo] + [2][CH + CH + 16 / es].
     extern __shared__ __align__(16) float Ps[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int abort_flag;
@@ -736,6 +834,46 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
         __syncthreads();
 
         const S* src = level + row.level_row * pitch + base;
+        // fused level step: the row's op, its children's segments and the
+        // offset of the shifted one inside its 16-byte-aligned superset
+        constexpr int VEC  = 16 / static_cast<int>(sizeof(S));
+        S* const fs_halo   = stage0;
+        auto fs_lo         = [&](int b) { return stage0 + halo + b * (2 * CH + VEC); };
+        auto fs_hi         = [&](int b) { return stage0 + halo + b * (2 * CH + VEC) + CH; };
+        const S* lo_src    = nullptr;
+        const S* hi_src    = nullptr;
+        int hoff           = 0;
+        uint32_t hi_bytes  = 0;
+        if constexpr (FS) {
+            const RowOp op      = SG.ops[g];
+            const S* in         = static_cast<const S*>(SG.in);
+            lo_src              = in + static_cast<int64_t>(op.lo_row) * SG.in_pitch + SG.in_base;
+            const int64_t first = static_cast<int64_t>(SG.in_base) - op.shift;
+            hoff                = static_cast<int>(((first % VEC) + VEC) % VEC);
+            if (op.hi_row >= 0) {
+                hi_src   = in + static_cast<int64_t>(op.hi_row) * SG.in_pitch + (first - hoff);
+                hi_bytes = static_cast<uint32_t>((CH / VEC + (hoff > 0 ? 1 : 0)) * 16);
+            }
+        }
+        auto issue_fs = [&](int ci) {
+            const int b    = static_cast<int>((cc + ci) & 1);
+            uint32_t bytes = static_cast<uint32_t>(CH * sizeof(S)) + hi_bytes;
+            if (ci == 0)
+                bytes += static_cast<uint32_t>(halo * sizeof(S));
+            bulk::mbar_expect(&bar[b], bytes);
+            if (ci == 0)
+                bulk::load(fs_halo, src - halo, static_cast<uint32_t>(halo * sizeof(S)), &bar[b]);
+            bulk::load(fs_lo(b), lo_src + static_cast<int64_t>(ci) * CH, static_cast<uint32_t>(CH * sizeof(S)),
+                       &bar[b]);
+            if (hi_bytes != 0)
+                bulk::load(fs_hi(b), hi_src + static_cast<int64_t>(ci) * CH, hi_bytes, &bar[b]);
+            // the chunk staged two issues later is fetched into L2 meanwhile
+            if (ci + 2 < nchunks) {
+                bulk::prefetch_l2(lo_src + static_cast<int64_t>(ci + 2) * CH, static_cast<uint32_t>(CH * sizeof(S)));
+                if (hi_bytes != 0)
+                    bulk::prefetch_l2(hi_src + static_cast<int64_t>(ci + 2) * CH, hi_bytes);
+            }
+        };
         auto issue = [&](int ci) {
             const int b          = static_cast<int>((cc + ci) & 1);
             const int off        = (ci == 0 || !carry_halo) ? 0 : halo;
@@ -748,9 +886,15 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             if (ci + 2 < nchunks)
                 bulk::prefetch_l2(src + static_cast<int64_t>(ci + 2) * CH, static_cast<uint32_t>(CH * sizeof(S)));
         };
-        if (threadIdx.x == 0)
-            for (int ci = 0; ci < min(2, nchunks); ++ci)
-                issue(ci);
+        if (threadIdx.x == 0) {
+            if constexpr (FS) {
+                for (int ci = 0; ci < min(2, nchunks); ++ci)
+                    issue_fs(ci);
+            } else {
+                for (int ci = 0; ci < min(2, nchunks); ++ci)
+                    issue(ci);
+            }
+        }
         const int jmin     = halo - wmax + 1; // earlier columns never enter a window
         const int64_t warm = static_cast<int64_t>(row.delay) + wmax - 1;
         auto close_runs = [&]() {
@@ -768,7 +912,7 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             __syncthreads();
             if (abort_flag)
                 break;
-            const S* seg           = stage0 + ((cc + ci) & 1) * seg_cols;
+            const S* seg           = FS ? fs_halo : stage0 + ((cc + ci) & 1) * seg_cols;
             const bool direct_halo = ci == 0 || !carry_halo;
             if (direct_halo)
                 scan_halo<S, P>(seg, halo, jmin, Q, gmin, tmin);
@@ -776,7 +920,13 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
             // warp (shuffles), then across warps (one offset per warp)
             float q[P];
             float xmax; // the thread's largest sample
-            scan_cols<S, P>(seg + halo + P * threadIdx.x, q, xmax);
+            if constexpr (FS) {
+                const int b = static_cast<int>((cc + ci) & 1);
+                merge_scan<S, P>(fs_lo(b) + P * threadIdx.x, hi_bytes != 0 ? fs_hi(b) + P * threadIdx.x : nullptr,
+                                 hoff, const_cast<S*>(src) + c0 + P * threadIdx.x, q, xmax);
+            }
+            else
+                scan_cols<S, P>(seg + halo + P * threadIdx.x, q, xmax);
             float incl = q[P - 1];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -791,8 +941,13 @@ __global__ void __launch_bounds__(kThreads, CH == 2048 ? 5 : 4)
                 warp_tot[warp] = incl;
             __syncthreads();
             // every thread has read this chunk's staging buffer: refill it
-            if (threadIdx.x == 0 && ci + 2 < nchunks)
-                issue(ci + 2);
+            if constexpr (FS) {
+                if (threadIdx.x == 0 && ci + 2 < nchunks)
+                    issue_fs(ci + 2);
+            } else {
+                if (threadIdx.x == 0 && ci + 2 < nchunks)
+                    issue(ci + 2);
+            }
             // the totals of the warps before this one, in warp order (the
             // later terms add +0, which leaves the sum's bits unchanged)
             const float4 ta = reinterpret_cast<const float4*>(warp_tot)[0];
@@ -1199,11 +1354,15 @@ void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t
     t.n            = n;
     int64_t rows   = 0;
     const auto& p0 = segs[0].p;
+    const bool fs  = segs[0].in != nullptr;
     for (int i = 0; i < n; ++i) {
         SearchSeg& g = segs[i];
         check_search(g.p, g.pitch, g.base, chunk);
-        if (!same_shape(g.p, p0) || g.fp16 != segs[0].fp16)
+        if (!same_shape(g.p, p0) || g.fp16 != segs[0].fp16 || (g.in != nullptr) != fs)
             throw Error(FROST_ERR_INTERNAL, "search: segments of one launch differ in shape");
+        if (fs && (K != 1 || g.ops == nullptr || g.p.halo > chunk || g.in_base % 8 != 0 || g.in_pitch % 8 != 0 ||
+                   g.base % 8 != 0 || g.pitch % 8 != 0))
+            throw Error(FROST_ERR_INTERNAL, "search: bad fused level step geometry");
         rows += g.nrows;
         g.row_end = rows;
         t.s[i]    = g;
@@ -1214,8 +1373,11 @@ void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t
     // masks and the staging buffers (the kernel's layout)
     const size_t per  = static_cast<size_t>(chunk) / kThreads; // columns per thread
     const size_t nh   = static_cast<size_t>(p0.halo) + p0.halo / 4 + p0.halo / per + 4;
+    // staging: two raw row segments, or (fused level step) the halo and
+    // two pairs of child segments
+    const size_t stage_elems = fs ? p0.halo + 2 * (2 * static_cast<size_t>(chunk) + 16 / es) : 2 * seg;
     const size_t smem = sizeof(float) * ((4 + seg + 4) + (seg / 4 + 4) + seg / per + 2 * nh) +
-                        sizeof(uint32_t) * search_bits_words(p0.nwidths, chunk) + 2 * es * seg;
+                        sizeof(uint32_t) * search_bits_words(p0.nwidths, chunk) + es * stage_elems;
     const dim3 grid(static_cast<unsigned>(ctas > 0 ? std::min<int64_t>(rows, ctas) : rows));
     auto go = [&](auto kernel) {
         allow_large_smem(reinterpret_cast<const void*>(kernel));
@@ -1225,10 +1387,19 @@ void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t
     const bool pow2 = p0.pow2_widths != 0 && !p0.trapezoid && p0.nwidths <= kMaxPow2Widths;
     auto typed = [&](auto tag) {
         using S = decltype(tag);
+        if constexpr (K == 1) {
+            if (fs) {
+                if (chunk == 2048)
+                    pow2 ? go(k_search<S, 2048, true, true, K>) : go(k_search<S, 2048, false, true, K>);
+                else
+                    pow2 ? go(k_search<S, 4096, true, true, K>) : go(k_search<S, 4096, false, true, K>);
+                return;
+            }
+        }
         if (chunk == 2048)
-            pow2 ? go(k_search<S, 2048, true, K>) : go(k_search<S, 2048, false, K>);
+            pow2 ? go(k_search<S, 2048, true, false, K>) : go(k_search<S, 2048, false, false, K>);
         else
-            pow2 ? go(k_search<S, 4096, true, K>) : go(k_search<S, 4096, false, K>);
+            pow2 ? go(k_search<S, 4096, true, false, K>) : go(k_search<S, 4096, false, false, K>);
     };
     if (segs[0].fp16)
         typed(__half{});
@@ -1269,6 +1440,27 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
     g.fp16  = level.fp16;
     g.g0    = g0;
     g.nrows = g1 - g0;
+    launch_search_segs(&g, 1, s, chunk, ctas);
+}
+
+void launch_search_fused(const SearchParams& p, LevelView in, LevelView level, const RowOp* ops, int64_t g0,
+                         int64_t g1, cudaStream_t s, int32_t chunk, int32_t ctas) {
+    if (g1 <= g0 || p.n_valid <= 0)
+        return;
+    if (in.fp16 != level.fp16)
+        throw Error(FROST_ERR_INTERNAL, "search: fused level step between storage types");
+    SearchSeg g{};
+    g.p        = p;
+    g.level    = level.data;
+    g.pitch    = level.pitch;
+    g.base     = level.base;
+    g.fp16     = level.fp16;
+    g.g0       = g0;
+    g.nrows    = g1 - g0;
+    g.in       = in.data;
+    g.in_pitch = in.pitch;
+    g.in_base  = in.base;
+    g.ops      = ops;
     launch_search_segs(&g, 1, s, chunk, ctas);
 }
 

@@ -97,6 +97,15 @@ struct SearchSeg {
     int64_t g0;
     int64_t nrows;
     int64_t row_end;
+    // Fused single level step (in != nullptr): each searched row of `level`
+    // is computed in the same pass from the level below, out = in[lo] +
+    // in[hi] shifted by its op (ops[g] for searched row g), written to
+    // `level` and searched; its halo columns are already in `level`.
+    const void* in;
+    int64_t in_pitch;
+    int32_t in_base;
+    int32_t pad;
+    const RowOp* ops;
 };
 constexpr int kMaxSearchSegs = 32;
 template <int K> struct SearchSegTable {
@@ -116,6 +125,12 @@ void launch_search_segs(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk = 
  * looping over rows (0: one CTA per row). */
 void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g1,
                    cudaStream_t s, int32_t chunk = kSearchChunk, int32_t ctas = 0);
+
+/** launch_search with the single level step into `level` fused: searched
+ * row g is first computed from `in` by ops[g] (the step's RowOp of its
+ * level row) and written to `level`. The halo must not exceed the chunk. */
+void launch_search_fused(const SearchParams& p, LevelView in, LevelView level, const RowOp* ops, int64_t g0,
+                         int64_t g1, cudaStream_t s, int32_t chunk = kSearchChunk, int32_t ctas = 0);
 
 /** Exact variance of every searched row and width for `mask` and for
  * `mask_or`: var = sum over active channels of g[L_c][w]; writes

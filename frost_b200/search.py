@@ -225,6 +225,16 @@ class FDMTBoxcar:
         check(lib().frost_search_get_residency(self._h, C.byref(v)))
         return v.value
 
+    def set_fused_search(self, on: bool = True):
+        """Fuses each single FDMT level step into a searched level with that
+        level's search (default on). Results are identical either way."""
+        check(lib().frost_search_set_fused_search(self._h, 1 if on else 0))
+
+    def fused_search(self) -> bool:
+        v = C.c_int()
+        check(lib().frost_search_get_fused_search(self._h, C.byref(v)))
+        return bool(v.value)
+
     def set_wait_limit(self, tries: int = -1):
         """Bound (mbarrier tries) of the kernels' first wait on each bulk
         copy; negative restores the default, 0 gives up at once. A

@@ -564,6 +564,16 @@ int frost_search_set_launch_shape(frost_search* s, int fused, int tiles_per_cta,
 int frost_search_set_residency(frost_search* s, int ctas_per_sm);
 int frost_search_get_residency(const frost_search* s, int* ctas_per_sm);
 
+/* No counterpart in the reference. With `on` (the default) every single
+ * FDMT level step into a searched level is fused with that level's
+ * search: the search kernel computes each searched row from the level
+ * below (the same float adds and fp16 rounding as the level kernel),
+ * writes it and searches it in one pass, and the level kernel computes
+ * only the rows no plane searches. Results are identical either way.
+ * Waits for the engine's stream. */
+int frost_search_set_fused_search(frost_search* s, int on);
+int frost_search_get_fused_search(const frost_search* s, int* on);
+
 /* Enables (and zeroes) or disables per-phase timing. */
 int frost_search_enable_timing(frost_search* s, int enable);
 int frost_search_get_timing(const frost_search* s, frost_search_timing* out);

@@ -348,6 +348,34 @@ def test_residency_caps_keep_the_candidates(storage):
         FDMTBoxcar(pc, bc).set_residency(-1)
 
 
+@pytest.mark.parametrize("storage", [Storage.FP32, Storage.FP16])
+def test_fused_level_search_steps_are_bit_identical(storage):
+    """A single level step into a searched level fused with its search (the
+    search kernel computes, writes and searches each searched row; the level
+    kernel computes only the rows no plane searches) gives the candidates and
+    planes of the separate level and search launches bit for bit, over
+    several gulps (the next levels and gulps read the fused rows), for single
+    and two-level schedules and both search chunks."""
+    from frost_b200.search import FDMTBoxcar
+    pc = plan_config(depth=2, gulp=8192)
+    stream = make_stream(pc, 3, seed=131, pulses=PULSES)
+    bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0, storage=storage)
+    for fused, chunk in ((True, 4096), (False, 4096), (True, 2048)):
+        outs, planes = [], []
+        for on in (False, True):
+            eng = FDMTBoxcar(pc, bc)
+            eng.set_launch_shape(fused, 4, 2 if fused else 0, chunk)
+            eng.set_fused_search(on)
+            assert eng.fused_search() == on
+            eng.capture_planes(True)
+            outs.append(np.concatenate([run_engine(eng, stream, pc.block_nsamps, drain=False),
+                                        eng.drain().candidates]))
+            planes.append([eng.plane_data(p, pc.block_nsamps) for p in range(len(eng.get_search_plans()))])
+        assert outs[0].size > 0
+        assert np.array_equal(outs[1], outs[0]), (fused, chunk)
+        assert all(np.array_equal(a, b) for a, b in zip(planes[1], planes[0])), (fused, chunk)
+
+
 def test_uneven_widths_match_oracle():
     """Widths that are not powers of two (wtsp 1.5: 1, 2, 3, 5, ..., 93)
     take the table-driven steady-state tests (window starts straddling two
