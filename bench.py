@@ -420,7 +420,8 @@ def run_gpu(args):
     roofline = {
         "bound": "hbm",
         "kernel": ("FDMT level phase: k_level2_pipe<__half> (two levels per pass) + k_level_pipe<__half> "
-                   "(single levels), plain FP16 single-beam run"),
+                   "(the rows no plane searches of single steps into searched levels; their searched rows are "
+                   "computed inside the search kernel), plain FP16 single-beam run"),
         "achieved": round(level_gbs, 1),
         "peak": peak,
         "unit": "GB/s",
