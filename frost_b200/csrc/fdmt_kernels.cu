@@ -11,6 +11,7 @@
 // directly, coalesced. Storage is float or __half; arithmetic is float.
 
 #include <algorithm>
+#include <type_traits>
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -56,24 +57,29 @@ template <> __device__ __forceinline__ void st_sat<__half>(__half* p, float v) {
 // node at time t is sum_{s=0..d_lo} a[t - s] + sum_{s=0..d_hi} b[t - d_lo - s]
 // (one channel: the first term). The node's rows have non-decreasing d_lo
 // and d_hi (ascending delays), so each thread walks them in order and moves
-// its two windows by the samples that enter or leave them, accumulating in
-// double (every window sum is then its exact value to ~1e-16 relative,
-// however long the tile, and rounds once to float). The two channels' tile
-// segments, with the H samples before the tile, sit in shared memory as
-// doubles (converted once); thread t owns samples t, t + 256, ... of the
-// tile.
+// its two windows by the samples that enter or leave them. FP32 storage
+// accumulates in double (every window sum is then its exact value to ~1e-16
+// relative, however long the tile, and rounds once to float); FP16 storage
+// in float, the precision variant's FP32 accumulation (a window of a few
+// tens of unit-variance samples moved a few tens of times carries an error
+// some 1e-5 of an fp16 step). The two channels' tile segments, with the H
+// samples before the tile, sit in shared memory in the accumulator's type
+// (converted once); thread t owns samples t, t + 256, ... of the tile.
 constexpr int kFill = 8; // tile elements each thread loads at once (the H + 1 more follow)
 
+template <class S> using Level1Acc = std::conditional_t<sizeof(S) == 2, float, double>;
+
 template <class S>
-__global__ void __launch_bounds__(kThreads, 5)
+__global__ void __launch_bounds__(kThreads, sizeof(S) == 2 ? 6 : 5)
     k_level1(const LeafOp* __restrict__ ops, const int32_t* __restrict__ node_first_op, int32_t nnodes,
              int32_t ntiles, int32_t H, const float* __restrict__ wf, int64_t wpitch, int64_t t0,
              int32_t n_valid, const float* __restrict__ hist, int32_t hist_len, S* __restrict__ out,
              int64_t pitch, int32_t base) {
-    extern __shared__ double smem_x[];
+    using Acc = Level1Acc<S>;
+    extern __shared__ __align__(16) unsigned char smem_l1[];
     const int32_t N = kTimePerCta + H + 1;
-    double* Xa      = smem_x;
-    double* Xb      = smem_x + N;
+    Acc* Xa         = reinterpret_cast<Acc*>(smem_l1);
+    Acc* Xb         = Xa + N;
     // Work items (node, tile), nodes fastest; a CTA takes items blockIdx.x,
     // blockIdx.x + gridDim.x, ...
     const int64_t nitems = static_cast<int64_t>(nnodes) * ntiles;
@@ -111,25 +117,25 @@ __global__ void __launch_bounds__(kThreads, 5)
             for (int u = 0; u < kFill; ++u) {
                 const int i = threadIdx.x + u * kThreads;
                 if (i < N) {
-                    Xa[i] = static_cast<double>(ra[u]);
-                    Xb[i] = static_cast<double>(rb[u]);
+                    Xa[i] = static_cast<Acc>(ra[u]);
+                    Xb[i] = static_cast<Acc>(rb[u]);
                 }
             }
             for (int i = threadIdx.x + kFill * kThreads; i < N; i += kThreads) {
                 float a, b;
                 fetch(i, a, b);
-                Xa[i] = static_cast<double>(a);
-                Xb[i] = static_cast<double>(b);
+                Xa[i] = static_cast<Acc>(a);
+                Xb[i] = static_cast<Acc>(b);
             }
         }
         __syncthreads();
         // window state per owned sample: A = sum a[t - dl .. t],
         // B = sum b[t - dl - dh .. t - dl]; (dl, dh) = (-1, -1): both empty
-        double A[kPer], B[kPer];
+        Acc A[kPer], B[kPer];
 #pragma unroll
         for (int j = 0; j < kPer; ++j) {
-            A[j] = 0.0;
-            B[j] = 0.0;
+            A[j] = 0;
+            B[j] = 0;
         }
         int32_t dl = -1, dh = -1;
         const int i0 = threadIdx.x + H + 1; // index of the thread's first sample
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(kThreads, 5)
             if (op.d_lo < dl) {
 #pragma unroll
                 for (int j = 0; j < kPer; ++j)
-                    A[j] = 0.0;
+                    A[j] = 0;
                 from = 0;
             }
             for (int32_t q = from; q <= op.d_lo; ++q)
@@ -157,7 +163,7 @@ __global__ void __launch_bounds__(kThreads, 5)
                 if (dh < 0 || op.d_lo > ob || nb < ob || op.d_lo < dl) {
 #pragma unroll
                     for (int j = 0; j < kPer; ++j)
-                        B[j] = 0.0;
+                        B[j] = 0;
                     for (int32_t q = op.d_lo; q <= nb; ++q)
 #pragma unroll
                         for (int j = 0; j < kPer; ++j)
@@ -723,7 +729,8 @@ void launch_level1(const LeafOp* ops, const int32_t* node_first_op, int32_t nnod
         throw Error(FROST_ERR_INTERNAL, "level1: bad geometry");
     const int32_t ntiles = ncols / kTimePerCta;
     const dim3 grid(grid_for(static_cast<int64_t>(nnodes) * ntiles, ctas));
-    const size_t smem = 2 * sizeof(double) * (kTimePerCta + max_node_delay + 1);
+    const size_t acc  = out.fp16 ? sizeof(float) : sizeof(double); // Level1Acc
+    const size_t smem = 2 * acc * (kTimePerCta + max_node_delay + 1);
     if (smem > 200 * 1024)
         throw Error(FROST_ERR_INVALID_ARGUMENT, "level1: leaf windows too long for shared memory");
     if (out.fp16) {
