@@ -780,7 +780,7 @@ int frost_search_set_fused_search(frost_search* s, int on) {
     return guarded([&] {
         if (s == nullptr)
             invalid("frost_search_set_fused_search: null handle");
-        s->impl.set_fused_search(on != 0);
+        s->impl.set_fused_search(on);
     });
 }
 
@@ -788,7 +788,7 @@ int frost_search_get_fused_search(const frost_search* s, int* on) {
     return guarded([&] {
         if (s == nullptr || on == nullptr)
             invalid("frost_search_get_fused_search: null argument");
-        *on = s->impl.fused_search_on() ? 1 : 0;
+        *on = s->impl.fused_search_mode();
     });
 }
 

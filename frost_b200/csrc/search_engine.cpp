@@ -457,7 +457,7 @@ Engine::Tuned Engine::autotune() {
     cudaStream_t s = m_stream;
     std::string key = std::to_string(m_plan.nchans()) + "|" + std::to_string(m_ncols) + "|" +
                       std::to_string(m_fp16) + "|" + std::to_string(m_plan.widths().back()) + "|" +
-                      std::to_string(m_fs_on);
+                      std::to_string(fused_search_mode());
     for (int h = 1; h <= m_plan.levels(); ++h)
         key += "|" + std::to_string(m_plan.level_rows(h));
     for (const auto& p : m_plan.planes())
@@ -566,7 +566,9 @@ void Engine::set_residency(int32_t ctas_per_sm) {
     m_ctas_per_sm = ctas_per_sm;
 }
 
-void Engine::set_fused_search(bool on) {
+void Engine::set_fused_search(int32_t mode) {
+    if (mode < 0 || mode > 2)
+        invalid("search: fused search mode must be 0, 1 or 2");
     DeviceGuard g(m_device);
     FB_CUDA(cudaStreamSynchronize(m_stream));
     if (m_graph != nullptr) {
@@ -574,7 +576,9 @@ void Engine::set_fused_search(bool on) {
         FB_CUDA(cudaGraphExecDestroy(m_graph));
         m_graph = nullptr;
     }
-    m_fs_on = on;
+    m_fs_on = mode != 0;
+    if (mode != 0)
+        m_fs_buffers = mode;
 }
 
 void Engine::set_wait_limit(long long tries) {
@@ -1105,7 +1109,7 @@ void Engine::run_tiles(const float* wf, SizeType nsamps, cudaStream_t s) {
                 timed(kSearch, s, [&] {
                     if (fs)
                         launch_search_fused(sp, view(st.in), out, m_fs_ops.as<RowOp>(), m_height_g0[h],
-                                            m_height_g1[h], s, m_search_chunk, cta_cap());
+                                            m_height_g1[h], s, m_search_chunk, cta_cap(), m_fs_buffers);
                     else
                         launch_search(sp, out, m_height_g0[h], m_height_g1[h], s, m_search_chunk, cta_cap());
                 });

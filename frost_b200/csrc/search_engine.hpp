@@ -141,6 +141,7 @@ private:
     DeviceBuffer m_fs_ops, m_fs_rows;
     std::vector<int64_t> m_fs_rows_off, m_fs_rows_n;
     bool m_fs_on = false; // set for fp16 storage by the constructor
+    int32_t m_fs_buffers = 1;
     int m_key_level_bits = 0, m_key_idx_bits = 0, m_key_dm_bits = 0, m_key_filter_bits = 0;
     std::vector<int64_t> m_row_op_offset;
     /** One FDMT step: level `out` from level `in` = out - 1 (single) or
@@ -200,9 +201,10 @@ private:
     void set_residency(int32_t ctas_per_sm);
     int32_t residency() const { return m_ctas_per_sm; }
     /** Fuses each single level step into a searched level with its search
-     * (default on; identical results). Waits for the engine's stream. */
-    void set_fused_search(bool on);
-    bool fused_search_on() const { return m_fs_on; }
+     * (mode 0: off; 1 or 2: on, that many chunks staged at once); identical
+     * results. Waits for the engine's stream. */
+    void set_fused_search(int32_t mode);
+    int32_t fused_search_mode() const { return m_fs_on ? m_fs_buffers : 0; }
 
     /** Device bytes an engine for (dd, bc) allocates, computed on the host
      * from its plan without allocating anything: level buffers (under

@@ -720,9 +720,10 @@ __device__ void scan_halo(const S* seg, int halo, int jmin, float* Q, float* gmi
         H[i] -= last;
 }
 
-template <class S, int CH, bool POW2, bool FS, int K>
-__global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2048 ? 5 : 4))
+template <class S, int CH, bool POW2, int FSB, int K>
+__global__ void __launch_bounds__(kThreads, FSB == 2 ? (CH == 2048 ? 4 : 3) : (CH == 2048 ? 5 : 4))
     k_search(const __grid_constant__ SearchSegTable<K> tab) {
+    constexpr bool FS = FSB > 0; // fused level step, FSB chunks staged at once
     // The search shape (widths, halo, peak mode, valid columns) is the same
     // in every segment; the rows, tables and outputs are each segment's.
     const SearchParams& p = tab.s[0].p;
@@ -741,9 +742,11 @@ __global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2
     //   stage  S [2][halo + CH]: the raw row segment, bulk-copied one chunk
     //          ahead (the halo columns only for the first chunk)
     // With the level step fused (FS), the stage instead holds the row's
-    // halo columns (first chunk) and, for each of two chunks in flight, the
-    // chunk's unshifted child segment and the aligned superset of its
-    // shifted one: S [halo] + [2][CH + CH + 16 / es].
+    // halo columns (first chunk) and, for each of the FSB chunks in flight
+    // (one or two), the chunk's unshifted child segment and the aligned
+    // superset of its shifted one: S [halo] + [FSB][CH + CH + 16 / es]. With
+    // one, the next chunk's copies start once every thread has merged this
+    // one (no more shared memory than the two raw buffers).
     extern __shared__ __align__(16) float Ps[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int abort_flag;
@@ -856,22 +859,23 @@ __global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2
             }
         }
         auto issue_fs = [&](int ci) {
-            const int b    = static_cast<int>((cc + ci) & 1);
+            const int b    = static_cast<int>((cc + ci) & 1); // barrier
+            const int sb   = FSB == 2 ? b : 0;                  // staging buffers
             uint32_t bytes = static_cast<uint32_t>(CH * sizeof(S)) + hi_bytes;
             if (ci == 0)
                 bytes += static_cast<uint32_t>(halo * sizeof(S));
             bulk::mbar_expect(&bar[b], bytes);
             if (ci == 0)
                 bulk::load(fs_halo, src - halo, static_cast<uint32_t>(halo * sizeof(S)), &bar[b]);
-            bulk::load(fs_lo(b), lo_src + static_cast<int64_t>(ci) * CH, static_cast<uint32_t>(CH * sizeof(S)),
+            bulk::load(fs_lo(sb), lo_src + static_cast<int64_t>(ci) * CH, static_cast<uint32_t>(CH * sizeof(S)),
                        &bar[b]);
             if (hi_bytes != 0)
-                bulk::load(fs_hi(b), hi_src + static_cast<int64_t>(ci) * CH, hi_bytes, &bar[b]);
-            // the chunk staged two issues later is fetched into L2 meanwhile
-            if (ci + 2 < nchunks) {
-                bulk::prefetch_l2(lo_src + static_cast<int64_t>(ci + 2) * CH, static_cast<uint32_t>(CH * sizeof(S)));
+                bulk::load(fs_hi(sb), hi_src + static_cast<int64_t>(ci) * CH, hi_bytes, &bar[b]);
+            // the chunk staged next after those in flight is fetched into L2 meanwhile
+            if (ci + FSB < nchunks) {
+                bulk::prefetch_l2(lo_src + static_cast<int64_t>(ci + FSB) * CH, static_cast<uint32_t>(CH * sizeof(S)));
                 if (hi_bytes != 0)
-                    bulk::prefetch_l2(hi_src + static_cast<int64_t>(ci + 2) * CH, hi_bytes);
+                    bulk::prefetch_l2(hi_src + static_cast<int64_t>(ci + FSB) * CH, hi_bytes);
             }
         };
         auto issue = [&](int ci) {
@@ -888,7 +892,7 @@ __global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2
         };
         if (threadIdx.x == 0) {
             if constexpr (FS) {
-                for (int ci = 0; ci < min(2, nchunks); ++ci)
+                for (int ci = 0; ci < min(FSB, nchunks); ++ci)
                     issue_fs(ci);
             } else {
                 for (int ci = 0; ci < min(2, nchunks); ++ci)
@@ -921,7 +925,7 @@ __global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2
             float q[P];
             float xmax; // the thread's largest sample
             if constexpr (FS) {
-                const int b = static_cast<int>((cc + ci) & 1);
+                const int b = FSB == 2 ? static_cast<int>((cc + ci) & 1) : 0;
                 merge_scan<S, P>(fs_lo(b) + P * threadIdx.x, hi_bytes != 0 ? fs_hi(b) + P * threadIdx.x : nullptr,
                                  hoff, const_cast<S*>(src) + c0 + P * threadIdx.x, q, xmax);
             }
@@ -942,8 +946,8 @@ __global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2
             __syncthreads();
             // every thread has read this chunk's staging buffer: refill it
             if constexpr (FS) {
-                if (threadIdx.x == 0 && ci + 2 < nchunks)
-                    issue_fs(ci + 2);
+                if (threadIdx.x == 0 && ci + FSB < nchunks)
+                    issue_fs(ci + FSB);
             } else {
                 if (threadIdx.x == 0 && ci + 2 < nchunks)
                     issue(ci + 2);
@@ -1229,7 +1233,7 @@ __global__ void __launch_bounds__(kThreads, FS ? (CH == 2048 ? 4 : 3) : (CH == 2
             // a segment never landed: report it and let the copies in flight end
             if (threadIdx.x == 0) {
                 atomicOr(p.err, 1U);
-                for (int j = ci; j < min(ci + 2, nchunks); ++j)
+                for (int j = ci; j < min(ci + (FSB == 1 ? 1 : 2), nchunks); ++j)
                     (void)bulk::mbar_wait(&bar[(cc + j) & 1], static_cast<uint32_t>(((cc + j) >> 1) & 1));
             }
             return;
@@ -1355,12 +1359,13 @@ void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t
     int64_t rows   = 0;
     const auto& p0 = segs[0].p;
     const bool fs  = segs[0].in != nullptr;
+    const int fsb  = segs[0].fs_buffers;
     for (int i = 0; i < n; ++i) {
         SearchSeg& g = segs[i];
         check_search(g.p, g.pitch, g.base, chunk);
-        if (!same_shape(g.p, p0) || g.fp16 != segs[0].fp16 || (g.in != nullptr) != fs)
+        if (!same_shape(g.p, p0) || g.fp16 != segs[0].fp16 || (g.in != nullptr) != fs || g.fs_buffers != fsb)
             throw Error(FROST_ERR_INTERNAL, "search: segments of one launch differ in shape");
-        if (fs && (K != 1 || g.ops == nullptr || g.p.halo > chunk || g.in_base % 8 != 0 || g.in_pitch % 8 != 0 ||
+        if (fs && (K != 1 || g.ops == nullptr || (fsb != 1 && fsb != 2) || g.p.halo > chunk || g.in_base % 8 != 0 || g.in_pitch % 8 != 0 ||
                    g.base % 8 != 0 || g.pitch % 8 != 0))
             throw Error(FROST_ERR_INTERNAL, "search: bad fused level step geometry");
         rows += g.nrows;
@@ -1375,7 +1380,7 @@ void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t
     const size_t nh   = static_cast<size_t>(p0.halo) + p0.halo / 4 + p0.halo / per + 4;
     // staging: two raw row segments, or (fused level step) the halo and
     // two pairs of child segments
-    const size_t stage_elems = fs ? p0.halo + 2 * (2 * static_cast<size_t>(chunk) + 16 / es) : 2 * seg;
+    const size_t stage_elems = fs ? p0.halo + fsb * (2 * static_cast<size_t>(chunk) + 16 / es) : 2 * seg;
     const size_t smem = sizeof(float) * ((4 + seg + 4) + (seg / 4 + 4) + seg / per + 2 * nh) +
                         sizeof(uint32_t) * search_bits_words(p0.nwidths, chunk) + es * stage_elems;
     const dim3 grid(static_cast<unsigned>(ctas > 0 ? std::min<int64_t>(rows, ctas) : rows));
@@ -1388,18 +1393,25 @@ void search_table(SearchSeg* segs, int n, cudaStream_t s, int32_t chunk, int32_t
     auto typed = [&](auto tag) {
         using S = decltype(tag);
         if constexpr (K == 1) {
+            if (fs && fsb == 1) {
+                if (chunk == 2048)
+                    pow2 ? go(k_search<S, 2048, true, 1, K>) : go(k_search<S, 2048, false, 1, K>);
+                else
+                    pow2 ? go(k_search<S, 4096, true, 1, K>) : go(k_search<S, 4096, false, 1, K>);
+                return;
+            }
             if (fs) {
                 if (chunk == 2048)
-                    pow2 ? go(k_search<S, 2048, true, true, K>) : go(k_search<S, 2048, false, true, K>);
+                    pow2 ? go(k_search<S, 2048, true, 2, K>) : go(k_search<S, 2048, false, 2, K>);
                 else
-                    pow2 ? go(k_search<S, 4096, true, true, K>) : go(k_search<S, 4096, false, true, K>);
+                    pow2 ? go(k_search<S, 4096, true, 2, K>) : go(k_search<S, 4096, false, 2, K>);
                 return;
             }
         }
         if (chunk == 2048)
-            pow2 ? go(k_search<S, 2048, true, false, K>) : go(k_search<S, 2048, false, false, K>);
+            pow2 ? go(k_search<S, 2048, true, 0, K>) : go(k_search<S, 2048, false, 0, K>);
         else
-            pow2 ? go(k_search<S, 4096, true, false, K>) : go(k_search<S, 4096, false, false, K>);
+            pow2 ? go(k_search<S, 4096, true, 0, K>) : go(k_search<S, 4096, false, 0, K>);
     };
     if (segs[0].fp16)
         typed(__half{});
@@ -1444,7 +1456,7 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
 }
 
 void launch_search_fused(const SearchParams& p, LevelView in, LevelView level, const RowOp* ops, int64_t g0,
-                         int64_t g1, cudaStream_t s, int32_t chunk, int32_t ctas) {
+                         int64_t g1, cudaStream_t s, int32_t chunk, int32_t ctas, int32_t buffers) {
     if (g1 <= g0 || p.n_valid <= 0)
         return;
     if (in.fp16 != level.fp16)
@@ -1460,7 +1472,8 @@ void launch_search_fused(const SearchParams& p, LevelView in, LevelView level, c
     g.in       = in.data;
     g.in_pitch = in.pitch;
     g.in_base  = in.base;
-    g.ops      = ops;
+    g.ops        = ops;
+    g.fs_buffers = buffers;
     launch_search_segs(&g, 1, s, chunk, ctas);
 }
 

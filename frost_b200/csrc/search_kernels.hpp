@@ -104,7 +104,7 @@ struct SearchSeg {
     const void* in;
     int64_t in_pitch;
     int32_t in_base;
-    int32_t pad;
+    int32_t fs_buffers; // chunks staged at once: 1 or 2 (two: fewer CTAs an SM)
     const RowOp* ops;
 };
 constexpr int kMaxSearchSegs = 32;
@@ -128,9 +128,11 @@ void launch_search(const SearchParams& p, LevelView level, int64_t g0, int64_t g
 
 /** launch_search with the single level step into `level` fused: searched
  * row g is first computed from `in` by ops[g] (the step's RowOp of its
- * level row) and written to `level`. The halo must not exceed the chunk. */
+ * level row) and written to `level`; `buffers` (1 or 2) chunks are staged
+ * at once. The halo must not exceed the chunk. */
 void launch_search_fused(const SearchParams& p, LevelView in, LevelView level, const RowOp* ops, int64_t g0,
-                         int64_t g1, cudaStream_t s, int32_t chunk = kSearchChunk, int32_t ctas = 0);
+                         int64_t g1, cudaStream_t s, int32_t chunk = kSearchChunk, int32_t ctas = 0,
+                         int32_t buffers = 1);
 
 /** Exact variance of every searched row and width for `mask` and for
  * `mask_or`: var = sum over active channels of g[L_c][w]; writes

@@ -225,15 +225,16 @@ class FDMTBoxcar:
         check(lib().frost_search_get_residency(self._h, C.byref(v)))
         return v.value
 
-    def set_fused_search(self, on: bool = True):
+    def set_fused_search(self, mode: int = 1):
         """Fuses each single FDMT level step into a searched level with that
-        level's search (default on). Results are identical either way."""
-        check(lib().frost_search_set_fused_search(self._h, 1 if on else 0))
+        level's search (mode 1 or 2: chunks staged at once; 0: off; default
+        1 for fp16 storage, 0 for fp32). Results are identical either way."""
+        check(lib().frost_search_set_fused_search(self._h, int(mode)))
 
-    def fused_search(self) -> bool:
+    def fused_search(self) -> int:
         v = C.c_int()
         check(lib().frost_search_get_fused_search(self._h, C.byref(v)))
-        return bool(v.value)
+        return v.value
 
     def set_wait_limit(self, tries: int = -1):
         """Bound (mbarrier tries) of the kernels' first wait on each bulk

@@ -564,13 +564,15 @@ int frost_search_set_launch_shape(frost_search* s, int fused, int tiles_per_cta,
 int frost_search_set_residency(frost_search* s, int ctas_per_sm);
 int frost_search_get_residency(const frost_search* s, int* ctas_per_sm);
 
-/* No counterpart in the reference. With `on` (the default) every single
- * FDMT level step into a searched level is fused with that level's
- * search: the search kernel computes each searched row from the level
- * below (the same float adds and fp16 rounding as the level kernel),
- * writes it and searches it in one pass, and the level kernel computes
- * only the rows no plane searches. Results are identical either way.
- * Waits for the engine's stream. */
+/* No counterpart in the reference. With `on` = 1 or 2 every single FDMT
+ * level step into a searched level is fused with that level's search: the
+ * search kernel computes each searched row from the level below (the same
+ * sums and fp16 rounding as the level kernel), writes it and searches it in
+ * one pass, staging `on` chunks of the row's two children at once, and the
+ * level kernel computes only the rows no plane searches; 0 turns it off.
+ * Results are identical either way. The default is 1 for fp16 storage and
+ * 0 for fp32. FROST_ERR_INVALID_ARGUMENT outside 0..2. Waits for the
+ * engine's stream. */
 int frost_search_set_fused_search(frost_search* s, int on);
 int frost_search_get_fused_search(const frost_search* s, int* on);
 

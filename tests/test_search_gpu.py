@@ -362,18 +362,21 @@ def test_fused_level_search_steps_are_bit_identical(storage):
     bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0, storage=storage)
     for fused, chunk in ((True, 4096), (False, 4096), (True, 2048)):
         outs, planes = [], []
-        for on in (False, True):
+        for mode in (0, 1, 2):  # off; one or two chunks staged at once
             eng = FDMTBoxcar(pc, bc)
             eng.set_launch_shape(fused, 4, 2 if fused else 0, chunk)
-            eng.set_fused_search(on)
-            assert eng.fused_search() == on
+            eng.set_fused_search(mode)
+            assert eng.fused_search() == mode
             eng.capture_planes(True)
             outs.append(np.concatenate([run_engine(eng, stream, pc.block_nsamps, drain=False),
                                         eng.drain().candidates]))
             planes.append([eng.plane_data(p, pc.block_nsamps) for p in range(len(eng.get_search_plans()))])
         assert outs[0].size > 0
-        assert np.array_equal(outs[1], outs[0]), (fused, chunk)
-        assert all(np.array_equal(a, b) for a, b in zip(planes[1], planes[0])), (fused, chunk)
+        for k in (1, 2):
+            assert np.array_equal(outs[k], outs[0]), (fused, chunk, k)
+            assert all(np.array_equal(a, b) for a, b in zip(planes[k], planes[0])), (fused, chunk, k)
+    with pytest.raises(ValueError):
+        FDMTBoxcar(pc, bc).set_fused_search(3)
 
 
 def test_uneven_widths_match_oracle():
