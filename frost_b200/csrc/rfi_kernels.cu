@@ -51,6 +51,23 @@ template <int D> __device__ __forceinline__ float rd(const uint8_t* __restrict__
     }
 }
 
+// The integer code of sample c of an integer dtype D (rd<D> is its float).
+template <int D> __device__ __forceinline__ uint32_t rdi(const uint8_t* __restrict__ row, uint64_t c) {
+    if constexpr (D == FROST_UINT8) {
+        return row[c];
+    } else if constexpr (D == FROST_UINT16) {
+        return reinterpret_cast<const uint16_t*>(row)[c];
+    } else if constexpr (D == FROST_UINT32) {
+        return reinterpret_cast<const uint32_t*>(row)[c];
+    } else {
+        static_assert(D != FROST_FLOAT32, "rdi: integer dtypes only");
+        constexpr unsigned kBits = D == FROST_UINT1 ? 1U : D == FROST_UINT2 ? 2U : 4U;
+        constexpr unsigned kMask = (1U << kBits) - 1U;
+        const uint64_t bit       = c * kBits;
+        return (row[bit >> 3U] >> (bit & 7U)) & kMask;
+    }
+}
+
 // Bits per packed sample of dtype D (usable in device code).
 template <int D>
 constexpr uint64_t kBitsOf = D == FROST_UINT1 ? 1 : D == FROST_UINT2 ? 2 : D == FROST_UINT4 ? 4
@@ -680,13 +697,16 @@ template <int D> constexpr bool kIntRow = D != FROST_FLOAT32 && kBitsOf<D> <= 16
 // squares are kept as integers: every partial double sum of such values is
 // an integer below 2^53, so the reference's double sums are exact and equal
 // the integer ones whatever the order.
-template <bool INT>
+template <bool INT, bool W32 = false>
 struct ScanRowAcc {
     double sum_det = 0.0, sum_keep = 0.0, sx = 0.0, sxx = 0.0;
     uint64_t isx = 0, isxx = 0;
+    uint32_t tsx = 0, tsxx = 0;      // W32: the current tile's integer sums
     uint32_t n_keep = 0, n_meas = 0; // counts (exact as doubles when used)
     KadaneBest sp, sn; // rows are scanned whole: only the best runs are needed
-    __device__ __forceinline__ void step(uint64_t c, float x, float l, float ic, float clip, int kspec) {
+    // xi: the sample's integer code (INT: x == xi exactly)
+    __device__ __forceinline__ void step(uint64_t c, float x, uint32_t xi, float l, float ic, float clip,
+                                         int kspec) {
         ++n_meas;
         const float zc = (x - l) * ic;
         const float cl = clampf(zc, -clip, clip);
@@ -695,8 +715,10 @@ struct ScanRowAcc {
             sum_keep += zc;
             ++n_keep;
         }
-        if constexpr (INT) {
-            const uint32_t xi = static_cast<uint32_t>(x);
+        if constexpr (INT && W32) {
+            tsx += xi;
+            tsxx += xi * xi;
+        } else if constexpr (INT) {
             isx += xi;
             isxx += static_cast<uint64_t>(xi) * xi;
         } else {
@@ -708,6 +730,17 @@ struct ScanRowAcc {
             sn.append(static_cast<int32_t>(c), -cl);
         }
     }
+    __device__ __forceinline__ void step(uint64_t c, float x, float l, float ic, float clip, int kspec) {
+        step(c, x, INT ? static_cast<uint32_t>(x) : 0U, l, ic, clip, kspec);
+    }
+    // W32: moves the tile's integer sums into the 64-bit ones (exact: a tile
+    // of at most 128 8-bit samples sums below 2^32 even squared)
+    __device__ __forceinline__ void flush() {
+        isx += tsx;
+        isxx += tsxx;
+        tsx  = 0;
+        tsxx = 0;
+    }
     __device__ void finish(const Dims& d, uint64_t t, const KspecParams& kp,
                            const uint64_t* __restrict__ good_prefix, float* __restrict__ s_det,
                            double* __restrict__ s_keep_d, float* __restrict__ s_keep_f,
@@ -715,8 +748,8 @@ struct ScanRowAcc {
                            Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole) const {
         const double dn     = n_meas > 1 ? static_cast<double>(n_meas) : 1.0;
         const double s_keep = n_keep > 0 ? sum_keep / static_cast<double>(n_keep) : 0.0;
-        const double sx     = INT ? static_cast<double>(isx) : this->sx;
-        const double sxx    = INT ? static_cast<double>(isxx) : this->sxx;
+        const double sx     = INT ? static_cast<double>(isx + tsx) : this->sx;
+        const double sxx    = INT ? static_cast<double>(isxx + tsxx) : this->sxx;
         s_det[t]            = static_cast<float>(sum_det / dn);
         s_keep_f[t]         = static_cast<float>(s_keep);
         s_keep_d[t]         = s_keep;
@@ -836,7 +869,9 @@ __global__ void __launch_bounds__(kScanRows)
     issue(0);
     if (ntiles > 1)
         issue(1);
-    ScanRowAcc<kIntRow<D>> acc;
+    // 8-bit and narrower samples: the integer sums of a tile in 32 bits
+    constexpr bool kW32 = kIntRow<D> && kBitsOf<D> <= 8;
+    ScanRowAcc<kIntRow<D>, kW32> acc;
     for (int j = 0; j < ntiles; ++j) {
         if (j + 1 < ntiles)
             stage::wait_pending<1>();
@@ -872,8 +907,10 @@ __global__ void __launch_bounds__(kScanRows)
                         }
 #pragma unroll
                         for (int e = 0; e < 16; ++e)
-                            if (mk.b[e] != 0 && is[e] != 0.0F)
-                                acc.step(q + e, rd<D>(u.b, static_cast<uint64_t>(e)), ls[e], is[e], clip, kp.enabled);
+                            if (mk.b[e] != 0 && is[e] != 0.0F) {
+                                const uint32_t xi = rdi<D>(u.b, static_cast<uint64_t>(e));
+                                acc.step(q + e, static_cast<float>(xi), xi, ls[e], is[e], clip, kp.enabled);
+                            }
                         continue;
                     }
                 }
@@ -890,6 +927,8 @@ __global__ void __launch_bounds__(kScanRows)
                     acc.step(c, rd<D>(u.b, static_cast<uint64_t>(e)), lw[c], ic, clip, kp.enabled);
                 }
             }
+            if constexpr (kW32)
+                acc.flush();
         }
         __syncthreads(); // every thread is done with this tile's buffer
         if (j + 2 < ntiles)
@@ -1135,6 +1174,9 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
         const float sk    = s_keep_f[t];
         const Span32 ksp  = p.kspec ? kspec_pos[t] : Span32{-1, -1};
         const Span32 ksn  = p.kspec ? kspec_neg[t] : Span32{-1, -1};
+        // a row with no Kadane span across frequency (almost every row)
+        // skips the per-cell span tests
+        const bool row_kspec = ksp.lo >= 0 || ksn.lo >= 0;
         auto span_has     = [](const Span32& s, uint64_t c) {
             return s.lo >= 0 && static_cast<int32_t>(c) >= s.lo && static_cast<int32_t>(c) <= s.hi;
         };
@@ -1205,7 +1247,7 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
                     const float z = (x - ls[e]) * is[e];
                     if (p.narrow_active && fabsf(z) > p.clip) {
                         st = kNarrow;
-                    } else if (p.kspec && (span_has(ksp, c) || span_has(ksn, c))) {
+                    } else if (row_kspec && (span_has(ksp, c) || span_has(ksn, c))) {
                         st = kKadaneSpectrum;
                     } else if (ka[e] != 0 && (seg_has(kchan_pos[c], t) || seg_has(kchan_neg[c], t))) {
                         st = kKadaneChannel;

@@ -191,18 +191,20 @@ struct KadaneState32 {
             prefix.sum = total;
             prefix.end = i;
         }
+        // The open (suffix) run always ends at the last position, so its end
+        // is `last` (filled in by widen) and it is empty exactly when its
+        // sum is zero (a kept run has a positive sum).
         const double s = suffix.sum + u;
         if (s > 0.0) {
-            if (suffix.end < suffix.start)
+            if (suffix.sum == 0.0)
                 suffix.start = i;
             suffix.sum = s;
         } else {
             suffix.sum   = 0.0;
             suffix.start = i + 1;
         }
-        suffix.end = i;
         if (suffix.sum > best.sum)
-            best = suffix;
+            best = {suffix.sum, suffix.start, i};
     }
     FB_HD static Run wide(const Run32& r) { return {r.sum, r.start, r.end}; }
     FB_HD KadaneState widen() const {
@@ -212,7 +214,7 @@ struct KadaneState32 {
         k.last        = last;
         k.empty       = empty ? 1 : 0;
         k.prefix      = wide(prefix);
-        k.suffix      = wide(suffix);
+        k.suffix      = {suffix.sum, suffix.start, empty ? suffix.end : last};
         k.best        = wide(best);
         return k;
     }
@@ -220,35 +222,29 @@ struct KadaneState32 {
 
 /** The best run of KadaneState::append over a sequence that is never
  * combined with another: only the open (suffix) run and the best one are
- * kept, with 32-bit positions. */
+ * kept, with 32-bit positions. The open run always ends at the position
+ * just appended and is empty exactly when its sum is zero. When no run
+ * ever has a positive sum the best run is empty (length 0) and reported at
+ * position 0 rather than at the first position appended; callers use only
+ * a best run's length when it is empty. */
 struct KadaneBest {
     double ssum = 0.0, bsum = 0.0;
-    int32_t sstart = 0, send = -1, bstart = 0, bend = -1;
-    bool started = false;
+    int32_t sstart = 0, bstart = 0, bend = -1;
 
     FB_HD void append(int32_t i, double u) {
-        if (!started) {
-            started = true;
-            sstart  = i;
-            send    = i - 1;
-            bstart  = i;
-            bend    = i - 1;
-        }
         const double s = ssum + u;
         if (s > 0.0) {
-            if (send < sstart)
+            if (ssum == 0.0)
                 sstart = i;
             ssum = s;
-            send = i;
         } else {
             ssum   = 0.0;
             sstart = i + 1;
-            send   = i;
         }
         if (ssum > bsum) {
             bsum   = ssum;
             bstart = sstart;
-            bend   = send;
+            bend   = i;
         }
     }
     FB_HD Run best() const { return {bsum, bstart, bend}; }
