@@ -376,9 +376,10 @@ __global__ void __launch_bounds__(kThreads)
 // A row of level h+1 is a row of level h plus a shifted one, and each of
 // those is a row of level h-1 plus a shifted one, so it is the sum of up to
 // four level h-1 rows read at shifts 0, s1, s2, s3 (FusedOp). Computing
-// (x0 + x1) + (x2 + x3) in float is what the two single levels compute
-// (with float storage the same bits; with fp16 storage the middle sums stay
-// in float), and level h is never written or read back. Staging as in
+// (x0 + x1) + (x2 + x3) is what the two single levels compute, bit for bit
+// (float storage: float adds; fp16 storage: each sum rounded to fp16 with
+// saturation, as a stored middle level would be), and level h is never
+// written or read back. Staging as in
 // k_level_pipe: one unshifted segment and up to three 16-byte-aligned
 // supersets of the shifted ones per tile, kStages2 tiles in flight.
 
@@ -405,60 +406,44 @@ __device__ __forceinline__ void pick8h(const __half* stage, int e, int off, uint
     }
 }
 
-// f + h in float, h an fp16 value: the widening is exact, so this is
-// float(h) + f rounded to nearest, in one mixed-precision add.
-__device__ __forceinline__ float add_h(uint16_t h, float f) {
-    float r;
-    asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(h), "f"(f));
-    return r;
-}
-
-// 8 consecutive values starting at element off + e of a staged aligned
-// segment (off < 16 / sizeof(S)), as float.
-template <class S>
-__device__ __forceinline__ void load8(const S* stage, int e, int off, float (&x)[8]) {
-    if constexpr (sizeof(S) == 4) {
-        const float4* h4 = reinterpret_cast<const float4*>(stage) + e / 4;
-        const float4 b0 = h4[0], b1 = h4[1], b2 = h4[2]; // b2 unused when off == 0
-        const float h[12] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
-        switch (off) {
+// 8 consecutive floats starting at element off + e of a staged aligned
+// segment (off < 4).
+__device__ __forceinline__ void load8(const float* stage, int e, int off, float (&x)[8]) {
+    const float4* h4 = reinterpret_cast<const float4*>(stage) + e / 4;
+    const float4 b0 = h4[0], b1 = h4[1], b2 = h4[2]; // b2 unused when off == 0
+    const float h[12] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
+    switch (off) {
 #define FB_PICK(O)                                                                                \
     case O:                                                                                       \
         _Pragma("unroll") for (int i = 0; i < 8; ++i) x[i] = h[O + i];                             \
         break;
-            FB_PICK(0) FB_PICK(1) FB_PICK(2) FB_PICK(3)
+        FB_PICK(0) FB_PICK(1) FB_PICK(2) FB_PICK(3)
 #undef FB_PICK
-        }
-    } else {
-        uint32_t g[4];
-        pick8h(stage, e, off, g);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&g[i]));
-            x[2 * i]       = f.x;
-            x[2 * i + 1]   = f.y;
-        }
     }
 }
 
-// acc[q] = acc[q] + (value q of load8), the same float sums; fp16 values are
-// added with mixed-precision adds instead of being widened first.
-template <class S>
-__device__ __forceinline__ void add8(const S* stage, int e, int off, float (&acc)[8]) {
-    if constexpr (sizeof(S) == 4) {
-        float x[8];
-        load8<S>(stage, e, off, x);
+// acc[q] = acc[q] + (value q of load8).
+__device__ __forceinline__ void add8(const float* stage, int e, int off, float (&acc)[8]) {
+    float x[8];
+    load8(stage, e, off, x);
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
-            acc[q] = acc[q] + x[q];
-    } else {
-        uint32_t g[4];
-        pick8h(stage, e, off, g);
+    for (int q = 0; q < 8; ++q)
+        acc[q] = acc[q] + x[q];
+}
+
+// a[i] = a[i] + b[i] for four packed fp16 pairs as the single-level kernel
+// rounds it: the float sum of two fp16 values is exact when their exponents
+// differ by at most 12 and otherwise rounds to the larger one, as the fp16
+// add does; the clamp to +-65504 is the saturating convert's (sums past it
+// round to infinity).
+__device__ __forceinline__ void add_sat4(uint32_t (&a)[4], const uint32_t (&b)[4]) {
+    const __half2 top = __float2half2_rn(65504.0F);
+    const __half2 bot = __float2half2_rn(-65504.0F);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            acc[2 * i]     = add_h(static_cast<uint16_t>(g[i] & 0xFFFFU), acc[2 * i]);
-            acc[2 * i + 1] = add_h(static_cast<uint16_t>(g[i] >> 16), acc[2 * i + 1]);
-        }
+    for (int i = 0; i < 4; ++i) {
+        const __half2 x = __hadd2(*reinterpret_cast<const __half2*>(&a[i]), *reinterpret_cast<const __half2*>(&b[i]));
+        const __half2 c = __hmin2(__hmax2(x, bot), top);
+        a[i]            = *reinterpret_cast<const uint32_t*>(&c);
     }
 }
 
@@ -549,31 +534,48 @@ __global__ void __launch_bounds__(kThreads)
             if (abort_flag)
                 break;
             const unsigned char* sb = pipe2_smem + st * kStageBytes;
-            float a[8];
-            load8<S>(reinterpret_cast<const S*>(sb), e, 0, a);
-            if (bytes[1] != 0U)
-                add8<S>(reinterpret_cast<const S*>(sb + kLoBytes), e, off[1], a);
-            if (bytes[2] != 0U) {
-                float b[8];
-                load8<S>(reinterpret_cast<const S*>(sb + kLoBytes + kHiBytes), e, off[2], b);
-                if (bytes[3] != 0U)
-                    add8<S>(reinterpret_cast<const S*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], b);
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    a[q] = a[q] + b[q];
-            }
             S* dst = dst_row + static_cast<int64_t>(tile0 + i) * kTimePerCta + e;
             if constexpr (sizeof(S) == 4) {
+                float a[8];
+                load8(reinterpret_cast<const float*>(sb), e, 0, a);
+                if (bytes[1] != 0U)
+                    add8(reinterpret_cast<const float*>(sb + kLoBytes), e, off[1], a);
+                if (bytes[2] != 0U) {
+                    float b[8];
+                    load8(reinterpret_cast<const float*>(sb + kLoBytes + kHiBytes), e, off[2], b);
+                    if (bytes[3] != 0U)
+                        add8(reinterpret_cast<const float*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], b);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        a[q] = a[q] + b[q];
+                }
                 float4* d4 = reinterpret_cast<float4*>(dst);
                 d4[0]      = make_float4(a[0], a[1], a[2], a[3]);
                 d4[1]      = make_float4(a[4], a[5], a[6], a[7]);
             } else {
-                uint32_t r[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    r[q] = pack_sat(a[2 * q], a[2 * q + 1]);
+                // fp16 storage: each of the three sums is the single-level
+                // kernel's (the float sum of two fp16 values rounded with
+                // saturation), as fp16 adds clamped to +-65504, so two levels
+                // in one pass give the bits of two single steps
+                uint32_t a[4], b[4];
+                {
+                    const uint4 u = *reinterpret_cast<const uint4*>(reinterpret_cast<const S*>(sb) + e);
+                    a[0] = u.x, a[1] = u.y, a[2] = u.z, a[3] = u.w;
                 }
-                *reinterpret_cast<uint4*>(dst) = make_uint4(r[0], r[1], r[2], r[3]);
+                if (bytes[1] != 0U) {
+                    pick8h(reinterpret_cast<const __half*>(sb + kLoBytes), e, off[1], b);
+                    add_sat4(a, b);
+                }
+                if (bytes[2] != 0U) {
+                    pick8h(reinterpret_cast<const __half*>(sb + kLoBytes + kHiBytes), e, off[2], b);
+                    if (bytes[3] != 0U) {
+                        uint32_t c[4];
+                        pick8h(reinterpret_cast<const __half*>(sb + kLoBytes + 2 * kHiBytes), e, off[3], c);
+                        add_sat4(b, c);
+                    }
+                    add_sat4(a, b);
+                }
+                *reinterpret_cast<uint4*>(dst) = make_uint4(a[0], a[1], a[2], a[3]);
             }
             __syncthreads(); // every thread is done with stage st
             if (threadIdx.x == 0 && i + NS < nt)

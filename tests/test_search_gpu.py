@@ -289,18 +289,18 @@ def test_autotune_keeps_results_and_caches_choice():
 @pytest.mark.parametrize("peak_mode", [PeakMode.PER_WIDTH, PeakMode.ACROSS_WIDTHS, PeakMode.ALL])
 def test_every_launch_shape_gives_the_same_candidates(peak_mode):
     """Launch shapes (fused steps or single levels, tiles per CTA, bulk-copy
-    stages) change how the work is cut, not the arithmetic: with float
-    planes every shape with the same search chunk reports identical
-    candidates, trapezoid and cold prefix included, and with fp16 planes
-    every fused shape does; the two search chunks agree within the S/N
-    rounding of their prefix origins."""
+    stages) change how the work is cut, not the arithmetic: every shape with
+    the same search chunk reports identical candidates, trapezoid and cold
+    prefix included, with float planes and with fp16 planes (a fused step
+    rounds its middle level as a stored one would be); the two search
+    chunks agree within the S/N rounding of their prefix origins."""
     from frost_b200.search import FDMTBoxcar
     pc = plan_config(depth=1, gulp=8192)
     stream = make_stream(pc, 3, seed=93, pulses=PULSES)
     for storage, shapes in ((Storage.FP32, [(False, 4, 0, 4096), (True, 8, 2, 2048), (True, 32, 3, 2048),
                                             (True, 16, 0, 4096), (False, 16, 0, 2048)]),
                             (Storage.FP16, [(True, 16, 0, 4096), (True, 4, 2, 2048), (True, 32, 4, 2048),
-                                            (True, 8, 3, 4096)])):
+                                            (True, 8, 3, 4096), (False, 4, 0, 4096), (False, 16, 0, 2048)])):
         bc = BoxcarConfig(max_boxcar=16, detect_thresh=6.0, use_trapezoid=True, peak_mode=peak_mode,
                           storage=storage)
         ref = {}
