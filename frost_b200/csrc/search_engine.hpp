@@ -140,7 +140,7 @@ private:
     // computes (m_fs_rows[m_fs_rows_off[h] ..][m_fs_rows_n[h]]).
     DeviceBuffer m_fs_ops, m_fs_rows;
     std::vector<int64_t> m_fs_rows_off, m_fs_rows_n;
-    bool m_fs_on = false; // set for fp16 storage by the constructor
+    bool m_fs_on = true;
     int32_t m_fs_buffers = 1;
     int m_key_level_bits = 0, m_key_idx_bits = 0, m_key_dm_bits = 0, m_key_filter_bits = 0;
     std::vector<int64_t> m_row_op_offset;

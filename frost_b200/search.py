@@ -228,7 +228,7 @@ class FDMTBoxcar:
     def set_fused_search(self, mode: int = 1):
         """Fuses each single FDMT level step into a searched level with that
         level's search (mode 1 or 2: chunks staged at once; 0: off; default
-        1 for fp16 storage, 0 for fp32). Results are identical either way."""
+        1). Results are identical either way."""
         check(lib().frost_search_set_fused_search(self._h, int(mode)))
 
     def fused_search(self) -> int:

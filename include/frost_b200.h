@@ -570,9 +570,9 @@ int frost_search_get_residency(const frost_search* s, int* ctas_per_sm);
  * sums and fp16 rounding as the level kernel), writes it and searches it in
  * one pass, staging `on` chunks of the row's two children at once, and the
  * level kernel computes only the rows no plane searches; 0 turns it off.
- * Results are identical either way. The default is 1 for fp16 storage and
- * 0 for fp32. FROST_ERR_INVALID_ARGUMENT outside 0..2. Waits for the
- * engine's stream. */
+ * Results are identical either way. The default is 1. Two staged chunks
+ * hold fewer CTAs an SM and measured slower. FROST_ERR_INVALID_ARGUMENT
+ * outside 0..2. Waits for the engine's stream. */
 int frost_search_set_fused_search(frost_search* s, int on);
 int frost_search_get_fused_search(const frost_search* s, int* on);
 
