@@ -311,7 +311,7 @@ SizeType Cleaner::memory_usage() const {
         &m_raw, &m_samples, &m_loc, &m_scale, &m_inv, &m_loc2, &m_scale2, &m_unmeasured,
         &m_moments, &m_clip_mean, &m_clip_inv, &m_mask_d, &m_static_mask_d, &m_good_prefix,
         &m_s_det, &m_s_keep_d, &m_s_keep_f, &m_row_std, &m_kspec_pos, &m_kspec_neg,
-        &m_kspec_whole, &m_chunk_min, &m_chunk_max, &m_chunk_zdot, &m_chunk_kpos, &m_chunk_kneg,
+        &m_kspec_whole, &m_row_clip, &m_row_kchan, &m_slow_rows, &m_nslow, &m_chunk_min, &m_chunk_max, &m_chunk_zdot, &m_chunk_kpos, &m_chunk_kneg,
         &m_lo, &m_hi, &m_zdot_sum, &m_kpos_best, &m_kneg_best, &m_time_flags_d, &m_zdot_a_d,
         &m_zdot_b_d, &m_kchan_pos_d, &m_kchan_neg_d, &m_kchan_any_d, &m_flagged_d, &m_work, &m_out, &m_counters,
         &m_first_bad, &m_tail_loc, &m_tail_scale, &m_tail_out_loc, &m_tail_out_scale, &m_recip,
@@ -354,6 +354,7 @@ SizeType Cleaner::estimate_memory(const frost_rfi_config& cfg, const frost_block
     total += nwin * kMaxBandpassRows * n * f + n * sizeof(uint32_t);
     total += (moments ? nwin * n * sizeof(MomentSums) : 0) + 2 * std::max<SizeType>(moments ? nwin * n * f : 0, f);
     total += T * (f + sizeof(double) + f + f) + 2 * T1 * sizeof(Span32) + 2 * T1;
+    total += 2 * T1 + T1 * sizeof(uint32_t) + 16; // row_clip, row_kchan, the listed rows and their count
     total += 2 * nck * f + std::max<SizeType>(zdot ? nck : 1, 1) * sizeof(ZdotSums) +
              2 * std::max<SizeType>(kchan ? nck : 1, 1) * sizeof(KadaneState);
     total += 2 * n * f + n * sizeof(ZdotSums) + 2 * n * sizeof(Run);
@@ -603,6 +604,10 @@ void Cleaner::reserve_phase_buffers(const Dims& d) {
     m_kspec_pos.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
     m_kspec_neg.reserve(std::max<SizeType>(T, 1) * sizeof(Span32));
     m_kspec_whole.reserve(std::max<SizeType>(T, 1));
+    m_row_clip.reserve(std::max<SizeType>(T, 1));
+    m_row_kchan.reserve(std::max<SizeType>(T, 1));
+    m_slow_rows.reserve(std::max<SizeType>(T, 1) * sizeof(uint32_t));
+    m_nslow.reserve(16);
     m_time_flags_d.reserve(std::max<SizeType>(T, 1));
     const SizeType nck = d.nchunks * n;
     m_chunk_min.reserve(nck * sizeof(float));
@@ -714,7 +719,7 @@ void Cleaner::run_full(const Dims& d, cudaStream_t s) {
     launch_scan_rows(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(), m_clip, kp,
                      m_good_prefix.as<uint64_t>(), m_s_det.as<float>(), m_s_keep_d.as<double>(),
                      m_s_keep_f.as<float>(), m_row_std.as<float>(), m_kspec_pos.as<Span32>(),
-                     m_kspec_neg.as<Span32>(), m_kspec_whole.as<uint8_t>(), s);
+                     m_kspec_neg.as<Span32>(), m_kspec_whole.as<uint8_t>(), m_row_clip.as<uint8_t>(), s);
     launch_scan_cols(d, raw, m_loc.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(), m_clip,
                      m_s_keep_d.as<double>(), zdot ? 1 : 0, kchan ? 1 : 0, m_clip_mean.as<float>(),
                      m_clip_inv.as<float>(), m_chunk_min.as<float>(), m_chunk_max.as<float>(),
@@ -735,11 +740,15 @@ void Cleaner::run_full(const Dims& d, cudaStream_t s) {
 
     // ---- apply (lib/cpu/rfi_cpu.cpp:526-720) ----
     const ApplyParams p = apply_params();
+    if (kchan)
+        launch_kchan_rows(d, m_kchan_pos_d.as<Segment>(), m_kchan_neg_d.as<Segment>(), m_kchan_any_d.as<uint8_t>(),
+                          m_row_kchan.as<uint8_t>(), s);
     launch_apply_unflagged(d, p, raw, m_loc.as<float>(), m_scale.as<float>(), m_inv.as<float>(),
                            m_mask_d.as<uint8_t>(), m_time_flags_d.as<uint8_t>(), m_kspec_pos.as<Span32>(),
                            m_kspec_neg.as<Span32>(), m_kchan_pos_d.as<Segment>(), m_kchan_neg_d.as<Segment>(),
                            m_kchan_any_d.as<uint8_t>(), m_s_keep_f.as<float>(), m_zdot_a_d.as<float>(),
-                           m_zdot_b_d.as<float>(), m_work.as<float>(), counters, s);
+                           m_zdot_b_d.as<float>(), m_row_clip.as<uint8_t>(), m_row_kchan.as<uint8_t>(),
+                           m_slow_rows.as<uint32_t>(), m_nslow.as<unsigned int>(), m_work.as<float>(), counters, s);
     launch_apply_flagged(d, p, m_flagged_d.as<uint64_t>(), counters + kRepFlagged, m_loc.as<float>(),
                          m_scale.as<float>(), m_inv.as<float>(), m_mask_d.as<uint8_t>(),
                          m_time_flags_d.as<uint8_t>(), m_work.as<float>(), counters, s);

@@ -112,7 +112,7 @@ private:
     // Device workspace.
     DeviceBuffer m_raw, m_samples, m_loc, m_scale, m_inv, m_loc2, m_scale2, m_unmeasured,
         m_moments, m_clip_mean, m_clip_inv, m_mask_d, m_static_mask_d, m_good_prefix, m_s_det,
-        m_s_keep_d, m_s_keep_f, m_row_std, m_kspec_pos, m_kspec_neg, m_kspec_whole, m_chunk_min,
+        m_s_keep_d, m_s_keep_f, m_row_std, m_kspec_pos, m_kspec_neg, m_kspec_whole, m_row_clip, m_row_kchan, m_slow_rows, m_nslow, m_chunk_min,
         m_chunk_max, m_chunk_zdot, m_chunk_kpos, m_chunk_kneg, m_lo, m_hi, m_zdot_sum, m_kpos_best,
         m_kneg_best, m_time_flags_d, m_zdot_a_d, m_zdot_b_d, m_kchan_pos_d, m_kchan_neg_d, m_kchan_any_d,
         m_flagged_d, m_work, m_out, m_counters, m_first_bad, m_tail_loc, m_tail_scale,

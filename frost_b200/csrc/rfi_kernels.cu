@@ -745,7 +745,8 @@ struct ScanRowAcc {
                            const uint64_t* __restrict__ good_prefix, float* __restrict__ s_det,
                            double* __restrict__ s_keep_d, float* __restrict__ s_keep_f,
                            float* __restrict__ row_std, Span32* __restrict__ kspec_pos,
-                           Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole) const {
+                           Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole,
+                           uint8_t* __restrict__ row_clip) const {
         const double dn     = n_meas > 1 ? static_cast<double>(n_meas) : 1.0;
         const double s_keep = n_keep > 0 ? sum_keep / static_cast<double>(n_keep) : 0.0;
         const double sx     = INT ? static_cast<double>(isx + tsx) : this->sx;
@@ -753,6 +754,10 @@ struct ScanRowAcc {
         s_det[t]            = static_cast<float>(sum_det / dn);
         s_keep_f[t]         = static_cast<float>(s_keep);
         s_keep_d[t]         = s_keep;
+        // a measured cell of this row is past the clip (a narrow-band cell
+        // for the apply pass, which computes the same z from the same row,
+        // constants and clip)
+        row_clip[t] = n_keep != n_meas ? 1 : 0;
         const double mx     = sx / dn;
         const double var    = (sxx / dn) - (mx * mx);
         row_std[t]          = static_cast<float>(sqrt(var < 0.0 ? 0.0 : var));
@@ -790,7 +795,7 @@ __global__ void __launch_bounds__(kScanRows)
                 KspecParams kp, const uint64_t* __restrict__ good_prefix, float* __restrict__ s_det,
                 double* __restrict__ s_keep_d, float* __restrict__ s_keep_f,
                 float* __restrict__ row_std, Span32* __restrict__ kspec_pos,
-                Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole) {
+                Span32* __restrict__ kspec_neg, uint8_t* __restrict__ kspec_whole, uint8_t* __restrict__ row_clip) {
     __shared__ float tile[kScanRows][kScanChans + 1];
     const uint64_t t0    = static_cast<uint64_t>(blockIdx.x) * kScanRows;
     const uint64_t t     = t0 + threadIdx.x;
@@ -823,7 +828,7 @@ __global__ void __launch_bounds__(kScanRows)
     }
     if (active)
         acc.finish(d, t, kp, good_prefix, s_det, s_keep_d, s_keep_f, row_std, kspec_pos, kspec_neg,
-                   kspec_whole);
+                   kspec_whole, row_clip);
 }
 
 // The same rows with 128-byte column tiles of all 128 rows bulk-copied
@@ -840,7 +845,7 @@ __global__ void __launch_bounds__(kScanRows)
                        float* __restrict__ s_det, double* __restrict__ s_keep_d,
                        float* __restrict__ s_keep_f, float* __restrict__ row_std,
                        Span32* __restrict__ kspec_pos, Span32* __restrict__ kspec_neg,
-                       uint8_t* __restrict__ kspec_whole) {
+                       uint8_t* __restrict__ kspec_whole, uint8_t* __restrict__ row_clip) {
     extern __shared__ __align__(16) uint8_t tiles[]; // [2][kScanRows][kRowTileStride]
     constexpr int kPerChunk = static_cast<int>(128 / kBitsOf<D>); // channels per 16 bytes
     constexpr int kTileCh   = static_cast<int>(kRowTileBytes * 8 / kBitsOf<D>);
@@ -936,7 +941,7 @@ __global__ void __launch_bounds__(kScanRows)
     }
     if (active)
         acc.finish(d, t, kp, good_prefix, s_det, s_keep_d, s_keep_f, row_std, kspec_pos, kspec_neg,
-                   kspec_whole);
+                   kspec_whole, row_clip);
 }
 
 // One (chunk, channel) sequence of the column scan
@@ -1131,13 +1136,99 @@ __device__ __forceinline__ float level_of(const ApplyParams& p, float loc, float
     return p.equalize ? p.eq_loc + (p.eq_scale * v) : loc + (scale * v);
 }
 
-// Unflagged rows (lib/cpu/rfi_cpu.cpp:537-624): each CTA takes kApplyRows
-// consecutive rows in turn (one: more rows per CTA measured slower, 3.1 vs
-// 2.9 ms at 8); a row's samples and cell states are staged in shared
-// memory so neighbour draws read them without touching HBM again. Masked
-// cells are not written: the normalized output zeroes them, so their fill
-// values are never observed.
-constexpr int kApplyRows = 1;
+// Unflagged rows (lib/cpu/rfi_cpu.cpp:537-624) in two kernels. Every
+// measured cell of a row is clean when the row has no span across
+// frequency, no cell past the clip (the row scan computed the same z of
+// every measured cell from the same row, constants and clip; masks only
+// grow after it, so a cell it did not clip is never clipped here) and no
+// Kadane-along-time segment covering it. k_apply_clean writes those rows'
+// clean values (a CTA per row, no cell states, few registers) and lists
+// the others; k_apply_unflagged classifies the listed rows' cells, writes
+// their values and, where a cell needs one, the fills: a row's samples and
+// cell states are staged in shared memory so neighbour draws read them
+// without touching HBM again. Masked cells are not written: the normalized
+// output zeroes them, so their fill values are never observed.
+template <int D, int V>
+__global__ void __launch_bounds__(256)
+    k_apply_clean(Dims d, ApplyParams p, const uint8_t* __restrict__ raw, const float* __restrict__ loc,
+                  const float* __restrict__ scale, const float* __restrict__ inv,
+                  const uint8_t* __restrict__ mask, const uint8_t* __restrict__ time_flags,
+                  const Span32* __restrict__ kspec_pos, const Span32* __restrict__ kspec_neg,
+                  const float* __restrict__ s_keep_f, const float* __restrict__ zdot_a,
+                  const float* __restrict__ zdot_b, const uint8_t* __restrict__ row_clip,
+                  const uint8_t* __restrict__ row_kchan, float* __restrict__ work,
+                  uint32_t* __restrict__ slow_rows, unsigned int* __restrict__ nslow) {
+    const uint64_t t = blockIdx.x;
+    if (t >= d.nsamps || time_flags[t] != 0)
+        return;
+    const bool row_kspec = p.kspec && (kspec_pos[t].lo >= 0 || kspec_neg[t].lo >= 0);
+    if (row_kspec || (p.narrow_active && row_clip[t] != 0) || (p.kchan && row_kchan[t] != 0)) {
+        if (threadIdx.x == 0)
+            slow_rows[atomicAdd(nslow, 1U)] = static_cast<uint32_t>(t);
+        return;
+    }
+    const uint64_t n   = d.nchans;
+    const uint32_t n32 = static_cast<uint32_t>(n);
+    const uint64_t w   = window_of(t, d.window, d.nwin);
+    const float* lw    = loc + w * n;
+    const float* sw    = scale + w * n;
+    const float* iw    = inv + w * n;
+    const uint8_t* in  = raw + t * d.row_bytes;
+    float* out         = work + t * n;
+    const float sk     = s_keep_f[t];
+    for (uint32_t cb = threadIdx.x * V; cb < n32; cb += blockDim.x * V) {
+        float xs[V], ls[V], ss[V], is[V], outv[V];
+        uint8_t ms[V];
+        if constexpr (V == 4) {
+            const float4 l4 = *reinterpret_cast<const float4*>(lw + cb);
+            const float4 s4 = *reinterpret_cast<const float4*>(sw + cb);
+            const float4 i4 = *reinterpret_cast<const float4*>(iw + cb);
+            const uchar4 m4 = *reinterpret_cast<const uchar4*>(mask + cb);
+            ls[0] = l4.x; ls[1] = l4.y; ls[2] = l4.z; ls[3] = l4.w;
+            ss[0] = s4.x; ss[1] = s4.y; ss[2] = s4.z; ss[3] = s4.w;
+            is[0] = i4.x; is[1] = i4.y; is[2] = i4.z; is[3] = i4.w;
+            ms[0] = m4.x; ms[1] = m4.y; ms[2] = m4.z; ms[3] = m4.w;
+            if constexpr (D == FROST_UINT8) {
+                const uchar4 x4 = *reinterpret_cast<const uchar4*>(in + cb);
+                xs[0] = static_cast<float>(x4.x); xs[1] = static_cast<float>(x4.y);
+                xs[2] = static_cast<float>(x4.z); xs[3] = static_cast<float>(x4.w);
+            } else {
+#pragma unroll
+                for (int e = 0; e < V; ++e)
+                    xs[e] = rd<D>(in, cb + e);
+            }
+        } else {
+            ls[0] = lw[cb];
+            ss[0] = sw[cb];
+            is[0] = iw[cb];
+            ms[0] = mask[cb];
+            xs[0] = rd<D>(in, cb);
+        }
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const uint32_t c = cb + e;
+            const float x    = xs[e];
+            if (ms[e] == 0) {
+                outv[e] = 0.0F;
+            } else if (is[e] == 0.0F) {
+                outv[e] = x;
+            } else {
+                const float z = (x - ls[e]) * is[e];
+                float term    = 0.0F;
+                if (p.zero_dm == FROST_ZERO_DM_SUBTRACT)
+                    term = sk;
+                else if (p.zero_dm == FROST_ZERO_DM_ZDOT)
+                    term = (zdot_a[c] * sk) + zdot_b[c];
+                const float v = z - term;
+                outv[e]       = p.transform ? level_of(p, ls[e], ss[e], v) : x;
+            }
+        }
+        if constexpr (V == 4)
+            *reinterpret_cast<float4*>(out + cb) = make_float4(outv[0], outv[1], outv[2], outv[3]);
+        else
+            out[cb] = outv[0];
+    }
+}
 
 template <int D, int V>
 __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restrict__ raw,
@@ -1151,7 +1242,8 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
                                   const uint8_t* __restrict__ kchan_any,
                                   const float* __restrict__ s_keep_f,
                                   const float* __restrict__ zdot_a,
-                                  const float* __restrict__ zdot_b, float* __restrict__ work,
+                                  const float* __restrict__ zdot_b, const uint32_t* __restrict__ slow_rows,
+                                  const unsigned int* __restrict__ nslow, float* __restrict__ work,
                                   unsigned long long* __restrict__ counters) {
     extern __shared__ unsigned char smem[];
     const uint64_t n = d.nchans;
@@ -1161,10 +1253,9 @@ __global__ void k_apply_unflagged(Dims d, ApplyParams p, const uint8_t* __restri
     if (threadIdx.x < kCountSlots)
         cnt[threadIdx.x] = 0;
     unsigned long long narrow = 0, nks = 0, nkc = 0, fallbacks = 0;
-    const uint64_t t_end = min(static_cast<uint64_t>(blockIdx.x + 1) * kApplyRows, d.nsamps);
-    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * kApplyRows; t < t_end; ++t) {
-        if (time_flags[t] != 0)
-            continue;
+    const unsigned int nrows = *nslow;
+    for (unsigned int i = blockIdx.x; i < nrows; i += gridDim.x) {
+        const uint64_t t = slow_rows[i];
         const uint64_t w  = window_of(t, d.window, d.nwin);
         const float* lw   = loc + w * n;
         const float* sw   = scale + w * n;
@@ -1871,21 +1962,21 @@ void launch_scan_rows(const Dims& d, const uint8_t* raw, const float* loc, const
                       const uint8_t* mask, float clip, const KspecParams& kp,
                       const uint64_t* good_prefix, float* s_det, double* s_keep_d, float* s_keep_f,
                       float* row_std, Span32* kspec_pos, Span32* kspec_neg, uint8_t* kspec_whole,
-                      cudaStream_t s) {
+                      uint8_t* row_clip, cudaStream_t s) {
     if (d.nchans >= (uint64_t{1} << 31))
         throw Error(FROST_ERR_INVALID_ARGUMENT, "scan: too many channels for 32-bit channel indices");
     const unsigned grid = grid1(d.nsamps, kScanRows);
     if (d.row_bytes % 16 != 0 || reinterpret_cast<uintptr_t>(raw) % 16 != 0) {
         FB_DISPATCH(d.dtype, k_scan_rows<D><<<grid, kScanRows, 0, s>>>(
                                  d, raw, loc, inv, mask, clip, kp, good_prefix, s_det, s_keep_d,
-                                 s_keep_f, row_std, kspec_pos, kspec_neg, kspec_whole));
+                                 s_keep_f, row_std, kspec_pos, kspec_neg, kspec_whole, row_clip));
     } else {
         const size_t smem = 2 * static_cast<size_t>(kScanRows) * kRowTileStride;
         FB_DISPATCH(d.dtype, {
             set_smem(reinterpret_cast<const void*>(&k_scan_rows_staged<D>), smem);
             k_scan_rows_staged<D><<<grid, kScanRows, smem, s>>>(
                 d, raw, loc, inv, mask, clip, kp, good_prefix, s_det, s_keep_d, s_keep_f, row_std,
-                kspec_pos, kspec_neg, kspec_whole);
+                kspec_pos, kspec_neg, kspec_whole, row_clip);
         });
     }
     FB_COUNT_LAUNCH();
@@ -1921,35 +2012,78 @@ void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const
 }
 
 
+namespace {
+// row_kchan[t] = 1 for the rows a channel's Kadane-along-time segment
+// covers (the caller zeroes it): CTA 2c + k takes channel c's positive
+// (k = 0) or negative segment.
+__global__ void __launch_bounds__(256)
+    k_kchan_rows(uint64_t nchans, uint64_t nsamps, const Segment* __restrict__ kchan_pos,
+                 const Segment* __restrict__ kchan_neg, const uint8_t* __restrict__ kchan_any,
+                 uint8_t* __restrict__ row_kchan) {
+    const uint64_t c = blockIdx.x >> 1;
+    if (c >= nchans || kchan_any[c] == 0)
+        return;
+    const Segment g  = (blockIdx.x & 1) == 0 ? kchan_pos[c] : kchan_neg[c];
+    const int64_t lo = g.start < 0 ? 0 : g.start;
+    const int64_t hi = g.end < static_cast<int64_t>(nsamps) ? g.end : static_cast<int64_t>(nsamps) - 1;
+    for (int64_t t = lo + threadIdx.x; t <= hi; t += blockDim.x)
+        row_kchan[t] = 1;
+}
+} // namespace
+
+void launch_kchan_rows(const Dims& d, const Segment* kchan_pos, const Segment* kchan_neg,
+                       const uint8_t* kchan_any, uint8_t* row_kchan, cudaStream_t s) {
+    FB_CUDA(cudaMemsetAsync(row_kchan, 0, d.nsamps, s));
+    if (d.nsamps == 0 || d.nchans == 0)
+        return;
+    k_kchan_rows<<<static_cast<unsigned>(2 * d.nchans), 256, 0, s>>>(d.nchans, d.nsamps, kchan_pos, kchan_neg,
+                                                                     kchan_any, row_kchan);
+    FB_COUNT_LAUNCH();
+}
+
 void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* raw,
                             const float* loc, const float* scale, const float* inv,
                             const uint8_t* mask, const uint8_t* time_flags, const Span32* kspec_pos,
                             const Span32* kspec_neg, const Segment* kchan_pos,
                             const Segment* kchan_neg, const uint8_t* kchan_any,
                             const float* s_keep_f, const float* zdot_a,
-                            const float* zdot_b, float* work, unsigned long long* counters,
-                            cudaStream_t s) {
+                            const float* zdot_b, const uint8_t* row_clip, const uint8_t* row_kchan,
+                            uint32_t* slow_rows, unsigned int* nslow, float* work,
+                            unsigned long long* counters, cudaStream_t s) {
     const size_t smem = d.nchans * (sizeof(float) + 1);
     if (d.nsamps == 0)
         return;
-    if (d.nchans >= (uint64_t{1} << 31))
-        throw Error(FROST_ERR_INVALID_ARGUMENT, "apply: too many channels for one row's block");
+    if (d.nchans >= (uint64_t{1} << 31) || d.nsamps >= (uint64_t{1} << 31))
+        throw Error(FROST_ERR_INVALID_ARGUMENT, "apply: too many channels or samples for one block");
+    FB_CUDA(cudaMemsetAsync(nslow, 0, sizeof(unsigned int), s));
     // 4-channel vectors need nchans % 4 == 0 and, for the byte loads of the
     // raw row, a 4-byte aligned block
     const bool vec = d.nchans % 4 == 0 && reinterpret_cast<uintptr_t>(raw) % 4 == 0;
+    int dev = 0, sms = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    FB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // the listed rows: a few CTAs an SM loop over them (the count is read on the device)
+    const unsigned slow_grid = static_cast<unsigned>(std::min<uint64_t>(d.nsamps, static_cast<uint64_t>(sms) * 4));
     FB_DISPATCH(d.dtype, {
         if (vec) {
+            k_apply_clean<D, 4><<<static_cast<unsigned>(d.nsamps), 256, 0, s>>>(
+                d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, s_keep_f, zdot_a, zdot_b,
+                row_clip, row_kchan, work, slow_rows, nslow);
             set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 4>), smem);
-            k_apply_unflagged<D, 4><<<static_cast<unsigned>((d.nsamps + kApplyRows - 1) / kApplyRows), 256, smem, s>>>(
+            k_apply_unflagged<D, 4><<<slow_grid, 256, smem, s>>>(
                 d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
-                kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, work, counters);
+                kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, slow_rows, nslow, work, counters);
         } else {
+            k_apply_clean<D, 1><<<static_cast<unsigned>(d.nsamps), 256, 0, s>>>(
+                d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, s_keep_f, zdot_a, zdot_b,
+                row_clip, row_kchan, work, slow_rows, nslow);
             set_smem(reinterpret_cast<const void*>(&k_apply_unflagged<D, 1>), smem);
-            k_apply_unflagged<D, 1><<<static_cast<unsigned>((d.nsamps + kApplyRows - 1) / kApplyRows), 256, smem, s>>>(
+            k_apply_unflagged<D, 1><<<slow_grid, 256, smem, s>>>(
                 d, p, raw, loc, scale, inv, mask, time_flags, kspec_pos, kspec_neg, kchan_pos,
-                kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, work, counters);
+                kchan_neg, kchan_any, s_keep_f, zdot_a, zdot_b, slow_rows, nslow, work, counters);
         }
     });
+    FB_COUNT_LAUNCH();
     FB_COUNT_LAUNCH();
 }
 

@@ -75,12 +75,13 @@ void launch_bandpass(const Dims& d, const float* samples, float* loc, float* sca
 void launch_moments(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
                     const uint8_t* static_mask, float clip, MomentSums* out, cudaStream_t s);
 
-// Per-row detection series and the Kadane-across-frequency spans.
+// Per-row detection series and the Kadane-across-frequency spans;
+// row_clip[t] = 1 when a measured cell of row t is past the clip.
 void launch_scan_rows(const Dims& d, const uint8_t* raw, const float* loc, const float* inv,
                       const uint8_t* mask, float clip, const KspecParams& kp,
                       const uint64_t* good_prefix, float* s_det, double* s_keep_d, float* s_keep_f,
                       float* row_std, Span32* kspec_pos, Span32* kspec_neg, uint8_t* kspec_whole,
-                      cudaStream_t s);
+                      uint8_t* row_clip, cudaStream_t s);
 
 // Per (chunk, channel): min/max of unmeasured cells, zdot sums and the
 // Kadane-along-time states; then combined over chunks per channel in chunk
@@ -92,17 +93,26 @@ void launch_scan_cols(const Dims& d, const uint8_t* raw, const float* loc, const
                       KadaneState* chunk_kneg, float* lo, float* hi, ZdotSums* zdot_sum,
                       Run* kpos_best, Run* kneg_best, cudaStream_t s);
 
+// row_kchan[t] = 1 for the rows some channel's Kadane-along-time segment
+// covers, else 0.
+void launch_kchan_rows(const Dims& d, const Segment* kchan_pos, const Segment* kchan_neg,
+                       const uint8_t* kchan_any, uint8_t* row_kchan, cudaStream_t s);
+
 // Cleans unflagged rows into work[nsamps][nchans] (float). kchan_any[c]
 // marks the channels with a Kadane-along-time segment (only those read
-// their segments).
+// their segments); a row with no clipped cell (row_clip), no segment
+// (row_kchan) and no span across frequency writes its clean values
+// without classifying its cells, the others are listed in slow_rows
+// (*nslow of them; nsamps entries of room) and cleaned cell by cell.
 void launch_apply_unflagged(const Dims& d, const ApplyParams& p, const uint8_t* raw,
                             const float* loc, const float* scale, const float* inv,
                             const uint8_t* mask, const uint8_t* time_flags, const Span32* kspec_pos,
                             const Span32* kspec_neg, const Segment* kchan_pos,
                             const Segment* kchan_neg, const uint8_t* kchan_any,
                             const float* s_keep_f, const float* zdot_a,
-                            const float* zdot_b, float* work, unsigned long long* counters,
-                            cudaStream_t s);
+                            const float* zdot_b, const uint8_t* row_clip, const uint8_t* row_kchan,
+                            uint32_t* slow_rows, unsigned int* nslow, float* work,
+                            unsigned long long* counters, cudaStream_t s);
 
 // Refills the flagged rows flagged[0 .. *nflagged) of work from unflagged
 // rows (the count is read on the device).
