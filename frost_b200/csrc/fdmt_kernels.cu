@@ -67,6 +67,47 @@ template <> __device__ __forceinline__ void st_sat<__half>(__half* p, float v) {
 // (converted once); thread t owns samples t, t + 256, ... of the tile.
 constexpr int kFill = 8; // tile elements each thread loads at once (the H + 1 more follow)
 
+// acc[j] += x[i + j * kThreads] (SIGN = 1) or -= (SIGN = -1) for j < kPer:
+// float accumulators two lanes per instruction (add/sub.rn.f32x2: each lane
+// rounds as the scalar operation), doubles one at a time.
+// a[j] += b[j], two lanes per instruction.
+template <int N> __device__ __forceinline__ void slide_regs(float (&a)[N], const float (&b)[N]) {
+#pragma unroll
+    for (int j = 0; j < N; j += 2)
+        asm("{\n .reg .b64 p, q;\n mov.b64 p, {%0, %1};\n mov.b64 q, {%2, %3};\n"
+            " add.rn.f32x2 p, p, q;\n mov.b64 {%0, %1}, p;\n}"
+            : "+f"(a[j]), "+f"(a[j + 1])
+            : "f"(b[j]), "f"(b[j + 1]));
+}
+
+template <int SIGN, class Acc, int N>
+__device__ __forceinline__ void slide(Acc (&acc)[N], const Acc* x, int i) {
+    if constexpr (sizeof(Acc) == 4) {
+#pragma unroll
+        for (int j = 0; j < N; j += 2) {
+            const float a = x[i + j * kThreads], b = x[i + (j + 1) * kThreads];
+            if constexpr (SIGN > 0)
+                asm("{\n .reg .b64 p, q;\n mov.b64 p, {%0, %1};\n mov.b64 q, {%2, %3};\n"
+                    " add.rn.f32x2 p, p, q;\n mov.b64 {%0, %1}, p;\n}"
+                    : "+f"(acc[j]), "+f"(acc[j + 1])
+                    : "f"(a), "f"(b));
+            else
+                asm("{\n .reg .b64 p, q;\n mov.b64 p, {%0, %1};\n mov.b64 q, {%2, %3};\n"
+                    " sub.rn.f32x2 p, p, q;\n mov.b64 {%0, %1}, p;\n}"
+                    : "+f"(acc[j]), "+f"(acc[j + 1])
+                    : "f"(a), "f"(b));
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            if constexpr (SIGN > 0)
+                acc[j] += x[i + j * kThreads];
+            else
+                acc[j] -= x[i + j * kThreads];
+        }
+    }
+}
+
 template <class S> using Level1Acc = std::conditional_t<sizeof(S) == 2, float, double>;
 
 template <class S>
@@ -152,9 +193,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(S) == 2 ? 6 : 5)
                 from = 0;
             }
             for (int32_t q = from; q <= op.d_lo; ++q)
-#pragma unroll
-                for (int j = 0; j < kPer; ++j)
-                    A[j] += Xa[i0 + j * kThreads - q];
+                slide<1>(A, Xa, i0 - q);
             if (cb >= 0) {
                 // B's window moves from back offsets [dl, dl + dh] to
                 // [op.d_lo, op.d_lo + op.d_hi]: drop the top, add the bottom,
@@ -165,23 +204,28 @@ __global__ void __launch_bounds__(kThreads, sizeof(S) == 2 ? 6 : 5)
                     for (int j = 0; j < kPer; ++j)
                         B[j] = 0;
                     for (int32_t q = op.d_lo; q <= nb; ++q)
-#pragma unroll
-                        for (int j = 0; j < kPer; ++j)
-                            B[j] += Xb[i0 + j * kThreads - q];
+                        slide<1>(B, Xb, i0 - q);
                 } else {
                     for (int32_t q = dl; q < op.d_lo; ++q)
-#pragma unroll
-                        for (int j = 0; j < kPer; ++j)
-                            B[j] -= Xb[i0 + j * kThreads - q];
+                        slide<-1>(B, Xb, i0 - q);
                     for (int32_t q = ob + 1; q <= nb; ++q)
-#pragma unroll
-                        for (int j = 0; j < kPer; ++j)
-                            B[j] += Xb[i0 + j * kThreads - q];
+                        slide<1>(B, Xb, i0 - q);
                 }
             }
+            if constexpr (sizeof(Acc) == 4) {
+                float sum[kPer];
 #pragma unroll
-            for (int j = 0; j < kPer; ++j)
-                st_sat<S>(row + j * kThreads, static_cast<float>(A[j] + B[j]));
+                for (int j = 0; j < kPer; ++j)
+                    sum[j] = A[j];
+                slide_regs(sum, B);
+#pragma unroll
+                for (int j = 0; j < kPer; ++j)
+                    st_sat<S>(row + j * kThreads, sum[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < kPer; ++j)
+                    st_sat<S>(row + j * kThreads, static_cast<float>(A[j] + B[j]));
+            }
             dl = op.d_lo;
             dh = op.d_hi;
         }
