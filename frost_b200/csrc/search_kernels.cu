@@ -25,6 +25,18 @@
 // extending or closing the run carried from the previous chunk (and tile,
 // and gulp) and emitting each closed run's peak. The DM-time rows are never
 // re-read and the run state is the only thing carried between calls.
+//
+// When the FDMT step into the searched level is a single level step, the
+// same kernel also performs it for its rows (the fused level step): each
+// chunk stages the row's two children from the level below instead of the
+// row, adds them as the level kernel would, writes the row back for the
+// next levels and the history, and searches it; the level kernel then
+// computes only the rows no plane searches.
+//
+// Results are ordered on the device afterwards (k_cand_range, k_cand_keys,
+// a radix sort of packed keys, k_cand_gather), so the candidates of one
+// call come back in (level, sub-band, DM row, peak, width) order whatever
+// order the CTAs appended them in.
 
 #include <algorithm>
 
