@@ -963,7 +963,13 @@ struct ScanColAcc {
     float cmin = FLT_MAX, cmax = -FLT_MAX;
     ZdotSums zs{0, 0, 0, 0, 0};
     uint32_t zn = 0;
-    KadaneState32 kpos, kneg; // widened when stored
+    KadanePair32 kk; // Kadane along time of u and -u, widened when stored
+    // the first sample of an active channel's chunk (every later sample of
+    // the chunk follows in order)
+    __device__ __forceinline__ void begin(uint64_t t0) {
+        if (kchan)
+            kk.begin(static_cast<int32_t>(t0));
+    }
     __device__ __forceinline__ void step(float x, uint64_t t) {
         if (t >= wend) {
             w                = window_of(t, d->window, d->nwin);
@@ -994,8 +1000,7 @@ struct ScanColAcc {
         }
         if (kchan) {
             const double u = outlier ? 0.0 : static_cast<double>((z - cm) * ci);
-            kpos.append(static_cast<int32_t>(t), u);
-            kneg.append(static_cast<int32_t>(t), -u);
+            kk.append(static_cast<int32_t>(t), u);
         }
     }
     __device__ __forceinline__ void store(uint64_t k, float* cmin_out, float* cmax_out,
@@ -1010,8 +1015,11 @@ struct ScanColAcc {
             zs_out[o]  = z;
         }
         if (kchan) {
-            kp_out[o] = kpos.widen();
-            kn_out[o] = kneg.widen();
+            // an active channel appended every sample of the chunk
+            const uint64_t t1   = (k + 1) * d->chunk < d->nsamps ? (k + 1) * d->chunk : d->nsamps;
+            const int32_t last  = static_cast<int32_t>(t1) - 1;
+            kp_out[o] = kk.widen_pos(last);
+            kn_out[o] = kk.widen_neg(last);
         }
     }
 };
@@ -1032,6 +1040,8 @@ __global__ void k_scan_cols(Dims d, const uint8_t* __restrict__ raw, const float
     if (mask[c] != 0) {
         const uint64_t t0 = k * d.chunk;
         const uint64_t t1 = (t0 + d.chunk < d.nsamps) ? t0 + d.chunk : d.nsamps;
+        if (t0 < t1)
+            acc.begin(t0);
         for (uint64_t tb = t0; tb < t1; tb += kBlock) {
             // fetch kBlock rows ahead of their sequential use
             float xs[kBlock];
@@ -1071,6 +1081,8 @@ __global__ void __launch_bounds__(kStageChans)
     const uint64_t left = d.row_bytes - off;
     const int copy      = static_cast<int>(left < static_cast<uint64_t>(seg_bytes) ? left : seg_bytes);
     stage::Stager st(stage_buf, raw + off, d.row_bytes, seg_bytes, copy, rows, t0, t1);
+    if (active && t0 < t1)
+        acc.begin(t0);
     st.start();
     for (int kb = 0; kb < st.nblk; ++kb) {
         st.wait(kb);

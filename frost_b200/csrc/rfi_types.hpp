@@ -220,6 +220,82 @@ struct KadaneState32 {
     }
 };
 
+/** The two KadaneState32 of one sequence u and its negation -u, appended
+ * together from a known first position (`begin`) with 32-bit positions:
+ * the states of -u share the running total (negated: the sums of -u are
+ * the exact negations of those of u) and compare it for their own best
+ * prefix; the open runs' ends are the last position (`widen_*(last)`). The
+ * same sums, comparisons and runs as two KadaneState32 appends. */
+struct KadanePair32 {
+    struct Side {
+        double psum = 0.0, ssum = 0.0, bsum = 0.0;
+        int32_t pend = -1, sstart = 0, bstart = 0, bend = -1;
+    };
+    double total = 0.0; // of u
+    int32_t first = 0;
+    bool empty    = true;
+    Side pos, neg;
+
+    FB_HD static void begin_side(Side& sd, int32_t i) {
+        sd.pend   = i - 1;
+        sd.sstart = i;
+        sd.bstart = i;
+        sd.bend   = i - 1;
+    }
+    FB_HD void begin(int32_t i) {
+        empty = false;
+        first = i;
+        begin_side(pos, i);
+        begin_side(neg, i);
+    }
+    FB_HD static void open_run(Side& sd, int32_t i, double s) {
+        if (s > 0.0) {
+            if (sd.ssum == 0.0)
+                sd.sstart = i;
+            sd.ssum = s;
+        } else {
+            sd.ssum   = 0.0;
+            sd.sstart = i + 1;
+        }
+        if (sd.ssum > sd.bsum) {
+            sd.bsum   = sd.ssum;
+            sd.bstart = sd.sstart;
+            sd.bend   = i;
+        }
+    }
+    FB_HD void append(int32_t i, double u) {
+        total += u;
+        if (total > pos.psum) { // the prefix runs start at `first`
+            pos.psum = total;
+            pos.pend = i;
+        }
+        if (-total > neg.psum) {
+            neg.psum = -total;
+            neg.pend = i;
+        }
+        open_run(pos, i, pos.ssum + u);
+        open_run(neg, i, neg.ssum - u);
+    }
+    FB_HD KadaneState widen(const Side& sd, double tot, int32_t last) const {
+        KadaneState k = KadaneState::make();
+        if (empty)
+            return k;
+        k.total  = tot;
+        k.first  = first;
+        k.last   = last;
+        k.empty  = 0;
+        k.prefix = {sd.psum, first, sd.pend};
+        k.suffix = {sd.ssum, sd.sstart, last};
+        k.best   = {sd.bsum, sd.bstart, sd.bend};
+        return k;
+    }
+    /** The state of u after appends up to position `last`. */
+    FB_HD KadaneState widen_pos(int32_t last) const { return widen(pos, total, last); }
+    /** The state of -u (its total is 0 - total: +0 rather than -0 for a
+     * zero total, as the sum of -u would be). */
+    FB_HD KadaneState widen_neg(int32_t last) const { return widen(neg, 0.0 - total, last); }
+};
+
 /** The best run of KadaneState::append over a sequence that is never
  * combined with another: only the open (suffix) run and the best one are
  * kept, with 32-bit positions. The open run always ends at the position

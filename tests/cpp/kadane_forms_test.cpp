@@ -1,6 +1,7 @@
 // The reduced Kadane forms of the RFI scans (KadaneState32: 32-bit
 // positions, the open run's end implied; KadaneBest: open and best runs
-// only) against the full KadaneState on random sequences: integer values
+// only; KadanePair32: the states of u and -u together) against the full
+// KadaneState on random sequences: integer values
 // (exact zero sums and ties), small and large floats, runs of equal values,
 // gaps in the positions. Prints "bad N" with N the mismatches.
 
@@ -30,9 +31,11 @@ int main() {
     for (int trial = 0; trial < 200000; ++trial) {
         const int n    = static_cast<int>(rng() % 40);
         const int kind = static_cast<int>(rng() % 4);
-        KadaneState full = KadaneState::make();
+        KadaneState full = KadaneState::make(), fneg = KadaneState::make();
         KadaneState32 k32;
         KadaneBest kb;
+        KadanePair32 pair;
+        int32_t last = -1;
         int32_t pos = static_cast<int32_t>(rng() % 5);
         for (int i = 0; i < n; ++i) {
             double u = 0.0;
@@ -43,13 +46,23 @@ int main() {
             default: u = (rng() % 3 == 0) ? 0.0 : std::ldexp(static_cast<double>(static_cast<int>(rng() % 5) - 2), static_cast<int>(rng() % 60) - 30); break;
             }
             full.append(pos, u);
+            fneg.append(pos, -u);
             k32.append(pos, u);
             kb.append(pos, u);
+            if (i == 0)
+                pair.begin(pos);
+            pair.append(pos, u);
+            last = pos;
             pos += 1 + static_cast<int32_t>(rng() % 3 == 0 ? rng() % 4 : 0);
         }
         ++cases;
         const KadaneState w = k32.widen();
         if (!same_state(w, full))
+            ++bad;
+        // bit-level equality of the totals (the sign of a zero included)
+        const KadaneState pp = pair.widen_pos(last), pn = pair.widen_neg(last);
+        if (!same_state(pp, full) || !same_state(pn, fneg) ||
+            std::signbit(pp.total) != std::signbit(full.total) || std::signbit(pn.total) != std::signbit(fneg.total))
             ++bad;
         const Run b = kb.best();
         if (full.best.length() > 0 ? !same(b, full.best) : (b.length() > 0 || b.sum != full.best.sum))

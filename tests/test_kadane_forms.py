@@ -1,5 +1,6 @@
-"""The reduced Kadane forms the RFI scan kernels run (KadaneState32 in the
-time scan, KadaneBest in the frequency scan; frost_b200/csrc/rfi_types.hpp,
+"""The reduced Kadane forms the RFI scan kernels run (KadaneState32 and
+KadanePair32, the states of u and -u together, in the time scan,
+KadaneBest in the frequency scan; frost_b200/csrc/rfi_types.hpp,
 host-compiled) agree with the full KadaneState append field for field on
 200 000 random sequences (exact zero sums, ties, gaps in the positions); the
 GPU RFI parity tests check the kernels against frost's own cleaner."""
